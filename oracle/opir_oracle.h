@@ -1,0 +1,113 @@
+/* CPU oracle for the OnionPIRv2 server hot path (PirServer::make_query).
+ *
+ * TEST INFRASTRUCTURE ONLY. This is a plain-C restatement of the reference's
+ * algorithm, used by tests/, __graft_entry__.smoke() and the cpu_baseline leg
+ * of bench.py as the checker. Nothing in the product links or calls it.
+ *
+ * Parameter set: CONFIG_N2048_K1_COMP (database_constants.h:77-94): N = 2048,
+ * logical q = q1*q2 (two 29-bit NTT primes), t = generate_prime(13),
+ * small_q = 22-bit NTT prime, L_EP = 6, L_KEY = 10, L_KS = 8.
+ *
+ * Layouts (all little-endian u64, values canonical in [0, q)):
+ *   ciphertext   : [c0 (N)][c1 (N)]                                 (rlwe.h:17-31)
+ *   BV keys      : [level i < h][row j < L_KS][b (N)][a (N)], NTT form,
+ *                  galois_k(level i) = (N >> i) + 1             (bv_keyswitch.h:48-66)
+ *   RGSW (GSWCt) : [row r < 2l][c0 (N)][c1 (N)], NTT form          (gsw.h:8-17)
+ */
+#ifndef OPIR_ORACLE_H
+#define OPIR_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  uint32_t N;
+  uint64_t q, q1, q2;           /* logical modulus and its CRT factors   */
+  uint64_t w1, w2, w_crt;       /* minimal 2N-th roots mod q1, q2; CRT   */
+  uint64_t q1_inv_mod_q2;
+  uint64_t t, small_q;
+  uint32_t small_q_width;
+  uint32_t ct_mod_width;        /* 58: sum of configured limb bit widths */
+  uint32_t l_ep, l_key, l_ks;
+  uint32_t base_ep, base_key, base_ks;
+  uint64_t target_num_pt, num_pt, fst_dim_sz, other_dim_sz;
+  uint32_t num_dims, expansion_height, fst_dim_pow2;
+} opir_oracle_params;
+
+/* ---- parameters (pir.cpp, utils.cpp) ---- */
+int oracle_is_prime(uint64_t n);
+uint64_t oracle_generate_prime(uint32_t bit_width);
+int oracle_ntt_primes(const uint32_t *bit_widths, uint32_t count, uint32_t N,
+                      uint64_t *out);
+uint64_t oracle_min_primitive_root(uint64_t degree, uint64_t q);
+int oracle_calc_db_shape(uint64_t target, uint64_t l, uint32_t h, int pow2,
+                         uint64_t *fst_dim_sz, uint64_t *num_dims);
+int oracle_params_init(uint64_t target_num_pt, uint32_t expansion_height,
+                       int fst_dim_pow2, opir_oracle_params *out);
+
+/* ---- ring primitives ---- */
+void oracle_ntt_fwd(uint64_t *a, uint32_t N, uint64_t q, uint64_t root);
+void oracle_ntt_inv(uint64_t *a, uint32_t N, uint64_t q, uint64_t root);
+void oracle_automorphism(const uint64_t *in, uint32_t N, uint32_t k, uint64_t q,
+                         uint64_t *out);
+void oracle_negacyclic_shift(const uint64_t *in, uint32_t N, uint64_t shift,
+                             uint64_t q, uint64_t *out);
+uint64_t oracle_rescale(uint64_t a, uint64_t inp_mod, uint64_t out_mod);
+void oracle_signed_decompose(uint64_t val, uint32_t base_log2, uint64_t q,
+                             uint64_t *out, uint32_t num_digits);
+
+/* ---- seeded client (the reference client with seeded generators) ---- */
+uint64_t oracle_mt_test(uint64_t seed, uint64_t skip);
+uint64_t oracle_db_coeff(uint64_t seed, uint64_t pt, uint64_t c, uint64_t N,
+                         uint64_t t);
+void oracle_db_plaintext(uint64_t seed, uint64_t pt, const opir_oracle_params *p,
+                         uint16_t *out);
+
+typedef struct oracle_client oracle_client;
+oracle_client *oracle_client_new(const opir_oracle_params *p, uint64_t seed);
+void oracle_client_free(oracle_client *c);
+void oracle_client_bv_keys(const oracle_client *c, uint64_t *out);
+void oracle_client_gsw_key(const oracle_client *c, uint64_t *out);
+int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out);
+void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp,
+                           uint64_t *pt_out);
+
+/* ---- server (server.cpp, gsw.cpp, bv_keyswitch.cpp, matrix.cpp) ---- */
+typedef struct oracle_server oracle_server;
+oracle_server *oracle_server_new(const opir_oracle_params *p);
+void oracle_server_free(oracle_server *s);
+int oracle_server_load_seeded(oracle_server *s, uint64_t logical_num_pt,
+                              uint64_t seed);
+int oracle_server_load(oracle_server *s, uint64_t logical_num_pt,
+                       const uint16_t *coeffs);
+int oracle_server_set_keys(oracle_server *s, const uint64_t *bv_keys,
+                           const uint64_t *gsw_key);
+int oracle_server_expand(const oracle_server *s, const uint64_t *query,
+                         uint64_t *out);
+int oracle_server_complete_selectors(const oracle_server *s,
+                                     const uint64_t *expanded, uint64_t *out);
+int oracle_server_first_dim(const oracle_server *s, const uint64_t *fst_query,
+                            uint64_t *out);
+int oracle_server_other_dim(const oracle_server *s, uint64_t *mid,
+                            const uint64_t *selectors, uint64_t *out);
+int oracle_server_make_query(const oracle_server *s, const uint64_t *query,
+                             uint64_t *resp);
+void oracle_mod_switch(const opir_oracle_params *p, uint64_t *ct);
+size_t oracle_serialize(const opir_oracle_params *p, const uint64_t *resp,
+                        uint8_t *out);
+void oracle_external_product(const opir_oracle_params *p, const uint64_t *rgsw,
+                             uint32_t l, uint32_t base_log2,
+                             const uint64_t *ct, uint64_t *out);
+void oracle_bv_apply_galois(const opir_oracle_params *p, uint64_t *ct,
+                            uint32_t galois_k, const uint64_t *key_rows);
+void oracle_level_mat_mat_32(const uint32_t *A, const uint32_t *B, uint64_t *out,
+                             uint64_t m, uint64_t n, uint64_t levels, uint64_t q);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,233 @@
+"""ctypes view of the CPU oracle (libopir_oracle.so). TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
+this module, and only as the checker. The library restates the reference
+server path in plain C (oracle/opir_oracle.c); see that file for the
+file:line map into the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libopir_oracle.so")
+_u64p = C.POINTER(C.c_uint64)
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("N", C.c_uint32),
+        ("q", C.c_uint64), ("q1", C.c_uint64), ("q2", C.c_uint64),
+        ("w1", C.c_uint64), ("w2", C.c_uint64), ("w_crt", C.c_uint64),
+        ("q1_inv_mod_q2", C.c_uint64),
+        ("t", C.c_uint64), ("small_q", C.c_uint64),
+        ("small_q_width", C.c_uint32), ("ct_mod_width", C.c_uint32),
+        ("l_ep", C.c_uint32), ("l_key", C.c_uint32), ("l_ks", C.c_uint32),
+        ("base_ep", C.c_uint32), ("base_key", C.c_uint32), ("base_ks", C.c_uint32),
+        ("target_num_pt", C.c_uint64), ("num_pt", C.c_uint64),
+        ("fst_dim_sz", C.c_uint64), ("other_dim_sz", C.c_uint64),
+        ("num_dims", C.c_uint32), ("expansion_height", C.c_uint32),
+        ("fst_dim_pow2", C.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+    @property
+    def useful(self) -> int:
+        return self.fst_dim_sz + self.l_ep * (self.num_dims - 1)
+
+
+def build() -> str:
+    """Compile libopir_oracle.so (the C restatement) if it is missing."""
+    if not os.path.exists(_LIB_PATH):
+        subprocess.run(["make", "-C", _HERE, "libopir_oracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(build())
+        L.oracle_params_init.argtypes = [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(Params)]
+        L.oracle_client_new.argtypes = [C.POINTER(Params), C.c_uint64]
+        L.oracle_client_new.restype = C.c_void_p
+        L.oracle_client_free.argtypes = [C.c_void_p]
+        L.oracle_client_bv_keys.argtypes = [C.c_void_p, _u64p]
+        L.oracle_client_gsw_key.argtypes = [C.c_void_p, _u64p]
+        L.oracle_client_query.argtypes = [C.c_void_p, C.c_uint64, _u64p]
+        L.oracle_client_decrypt.argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_server_new.argtypes = [C.POINTER(Params)]
+        L.oracle_server_new.restype = C.c_void_p
+        L.oracle_server_free.argtypes = [C.c_void_p]
+        L.oracle_server_load_seeded.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
+        L.oracle_server_load.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint16)]
+        L.oracle_server_set_keys.argtypes = [C.c_void_p, _u64p, _u64p]
+        for f in ("oracle_server_expand", "oracle_server_complete_selectors",
+                  "oracle_server_first_dim", "oracle_server_make_query"):
+            getattr(L, f).argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_server_other_dim.argtypes = [C.c_void_p, _u64p, _u64p, _u64p]
+        L.oracle_mod_switch.argtypes = [C.POINTER(Params), _u64p]
+        L.oracle_serialize.argtypes = [C.POINTER(Params), _u64p, C.POINTER(C.c_uint8)]
+        L.oracle_serialize.restype = C.c_size_t
+        L.oracle_ntt_fwd.argtypes = [_u64p, C.c_uint32, C.c_uint64, C.c_uint64]
+        L.oracle_ntt_inv.argtypes = [_u64p, C.c_uint32, C.c_uint64, C.c_uint64]
+        L.oracle_min_primitive_root.argtypes = [C.c_uint64, C.c_uint64]
+        L.oracle_min_primitive_root.restype = C.c_uint64
+        L.oracle_generate_prime.argtypes = [C.c_uint32]
+        L.oracle_generate_prime.restype = C.c_uint64
+        L.oracle_is_prime.argtypes = [C.c_uint64]
+        L.oracle_calc_db_shape.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_int,
+                                           _u64p, _u64p]
+        L.oracle_rescale.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
+        L.oracle_rescale.restype = C.c_uint64
+        L.oracle_signed_decompose.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, _u64p, C.c_uint32]
+        L.oracle_mt_test.argtypes = [C.c_uint64, C.c_uint64]
+        L.oracle_mt_test.restype = C.c_uint64
+        L.oracle_db_coeff.argtypes = [C.c_uint64] * 5
+        L.oracle_db_coeff.restype = C.c_uint64
+        L.oracle_db_plaintext.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(Params),
+                                          C.POINTER(C.c_uint16)]
+        L.oracle_level_mat_mat_32.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                              _u64p, C.c_uint64, C.c_uint64, C.c_uint64,
+                                              C.c_uint64]
+        L.oracle_external_product.argtypes = [C.POINTER(Params), _u64p, C.c_uint32, C.c_uint32,
+                                              _u64p, _u64p]
+        L.oracle_bv_apply_galois.argtypes = [C.POINTER(Params), _u64p, C.c_uint32, _u64p]
+        _lib = L
+    return _lib
+
+
+def ptr(a: np.ndarray, ctype=C.c_uint64):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def params(target: int, height: int, pow2: bool = True) -> Params:
+    p = Params()
+    rc = lib().oracle_params_init(target, height, 1 if pow2 else 0, C.byref(p))
+    if rc != 0:
+        raise ValueError(f"invalid layout target={target} height={height}")
+    return p
+
+
+def db_plaintext(seed: int, pt: int, p: Params) -> np.ndarray:
+    out = np.empty(p.N, dtype=np.uint16)
+    lib().oracle_db_plaintext(seed, pt, C.byref(p), ptr(out, C.c_uint16))
+    return out
+
+
+class Client:
+    """Seeded client: the reference client with seeded generators."""
+
+    def __init__(self, p: Params, seed: int):
+        self.p = p
+        self.h = lib().oracle_client_new(C.byref(p), seed)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_client_free(self.h)
+            self.h = None
+
+    def bv_keys(self) -> np.ndarray:
+        p = self.p
+        out = np.zeros((max(p.expansion_height, 0), p.l_ks, 2, p.N), dtype=np.uint64)
+        if p.expansion_height:
+            lib().oracle_client_bv_keys(self.h, ptr(out))
+        return out
+
+    def gsw_key(self) -> np.ndarray:
+        p = self.p
+        out = np.zeros((2 * p.l_key, 2, p.N), dtype=np.uint64)
+        lib().oracle_client_gsw_key(self.h, ptr(out))
+        return out
+
+    def query(self, idx: int) -> np.ndarray:
+        out = np.zeros((2, self.p.N), dtype=np.uint64)
+        if lib().oracle_client_query(self.h, idx, ptr(out)) != 0:
+            raise IndexError("plaintext index outside the layout")
+        return out
+
+    def decrypt(self, resp: np.ndarray) -> np.ndarray:
+        resp = np.ascontiguousarray(resp, dtype=np.uint64)
+        out = np.zeros(self.p.N, dtype=np.uint64)
+        lib().oracle_client_decrypt(self.h, ptr(resp), ptr(out))
+        return out
+
+
+class Server:
+    def __init__(self, p: Params):
+        self.p = p
+        self.h = lib().oracle_server_new(C.byref(p))
+        if not self.h:
+            raise MemoryError("oracle server allocation failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_server_free(self.h)
+            self.h = None
+
+    def load_seeded(self, logical: int, seed: int):
+        assert lib().oracle_server_load_seeded(self.h, logical, seed) == 0
+
+    def load(self, coeffs: np.ndarray, logical: int | None = None):
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.uint16)
+        n = coeffs.shape[0] if logical is None else logical
+        rc = lib().oracle_server_load(self.h, n, ptr(coeffs, C.c_uint16))
+        if rc != 0:
+            raise ValueError("plaintext source rejected")
+
+    def set_keys(self, bv: np.ndarray, gsw: np.ndarray):
+        bv = np.ascontiguousarray(bv, dtype=np.uint64)
+        gsw = np.ascontiguousarray(gsw, dtype=np.uint64)
+        lib().oracle_server_set_keys(self.h, ptr(bv), ptr(gsw))
+
+    def expand(self, query: np.ndarray) -> np.ndarray:
+        out = np.zeros((self.p.useful, 2, self.p.N), dtype=np.uint64)
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        assert lib().oracle_server_expand(self.h, ptr(q), ptr(out)) == 0
+        return out
+
+    def complete_selectors(self, expanded: np.ndarray) -> np.ndarray:
+        p = self.p
+        out = np.zeros((max(p.num_dims - 1, 1), 2 * p.l_ep, 2, p.N), dtype=np.uint64)
+        e = np.ascontiguousarray(expanded, dtype=np.uint64)
+        assert lib().oracle_server_complete_selectors(self.h, ptr(e), ptr(out)) == 0
+        return out[: p.num_dims - 1]
+
+    def first_dim(self, fst_query: np.ndarray) -> np.ndarray:
+        p = self.p
+        out = np.zeros((p.other_dim_sz, 2, p.N), dtype=np.uint64)
+        f = np.ascontiguousarray(fst_query[: p.fst_dim_sz], dtype=np.uint64)
+        assert lib().oracle_server_first_dim(self.h, ptr(f), ptr(out)) == 0
+        return out
+
+    def other_dim(self, mid: np.ndarray, selectors: np.ndarray) -> np.ndarray:
+        out = np.zeros((2, self.p.N), dtype=np.uint64)
+        m = np.array(mid, dtype=np.uint64, copy=True, order="C")
+        s = np.ascontiguousarray(selectors, dtype=np.uint64)
+        if s.size == 0:
+            s = np.zeros(1, dtype=np.uint64)
+        assert lib().oracle_server_other_dim(self.h, ptr(m), ptr(s), ptr(out)) == 0
+        return out
+
+    def make_query(self, query: np.ndarray) -> np.ndarray:
+        out = np.zeros((2, self.p.N), dtype=np.uint64)
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        assert lib().oracle_server_make_query(self.h, ptr(q), ptr(out)) == 0
+        return out
+
+
+def serialize(p: Params, resp: np.ndarray) -> bytes:
+    r = np.ascontiguousarray(resp, dtype=np.uint64)
+    buf = np.zeros(2 * p.N * 8, dtype=np.uint8)
+    n = lib().oracle_serialize(C.byref(p), ptr(r), ptr(buf, C.c_uint8))
+    return buf[:n].tobytes()

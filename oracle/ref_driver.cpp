@@ -1,0 +1,306 @@
+// Seeded driver over the OnionPIRv2 reference's public API. Test
+// infrastructure: it is linked with the unmodified reference sources (and the
+// HEXL stand-in in oracle/hexl_standin) into oracle/_ref/opir_ref, and is used
+//   (1) to generate the golden responses under tests/golden/ (mode "golden"),
+//   (2) as the timed CPU baseline of PirServer::make_query (mode "time").
+//
+// The reference's own client seeds itself from std::random_device
+// (client.cpp:20-23, bv_keyswitch.cpp:267, server.cpp:55). This driver keeps
+// every algorithm of the reference and only supplies seeded generators:
+//   * database: PirServer::load_data (server.cpp:80-203) with a seeded
+//     counter-based PlaintextSource, coefficient = mix64(seed, pt*N+c) % t;
+//   * secret key: gen_secret_key_rns (rlwe.cpp:219-228) on rng(client_seed);
+//   * BV keys: bvks::gen_bv_ks_key (bv_keyswitch.cpp:222-259) for
+//     galois_k = (N >> i) + 1, i < h (bv_keyswitch.cpp:270-274) on
+//     rng(client_seed ^ kBvSalt) -- the reference draws these from a
+//     generator separate from the client's own;
+//   * RGSW(s): GSWEval::plain_to_gsw (gsw.cpp:359-422) as in
+//     PirClient::generate_gsw_from_key (client.cpp:25-38) on rng(client_seed);
+//   * query: PirClient::fast_generate_query / add_gsw_to_query
+//     (client.cpp:48-225) restated over the same public helpers on
+//     rng(client_seed), continuing after the RGSW key draws.
+#include "bv_keyswitch.h"
+#include "client.h"
+#include "gsw.h"
+#include "pir.h"
+#include "rlwe.h"
+#include "server.h"
+#include "utils.h"
+#include "hexl/hexl.hpp"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr uint64_t kBvSalt = 0x5BD1E9955BD1E995ULL;
+constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ULL;
+
+uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+uint64_t db_coeff(uint64_t seed, uint64_t pt, uint64_t c, uint64_t n, uint64_t t) {
+  return mix64(seed + (pt * n + c + 1) * kGolden) % t;
+}
+
+struct Client {
+  RlweSk sk;
+  bvks::BvGaloisKeys bv;
+  GSWCt gsw;
+  std::mt19937_64 rng;
+};
+
+Client make_client(const PirParams &p, uint64_t seed) {
+  constexpr size_t N = DBConsts::PolyDegree;
+  Client c{{}, {}, {}, std::mt19937_64(seed)};
+  const std::vector<uint64_t> qs(p.get_rns_mods().begin(), p.get_rns_mods().end());
+  c.sk = gen_secret_key_rns(N, qs, c.rng);
+  std::mt19937_64 rng_bv(seed ^ kBvSalt);
+  for (size_t i = 0; i < p.get_expan_height(); ++i) {
+    const uint32_t galois_k = static_cast<uint32_t>((N >> i) + 1);
+    c.bv.keys.push_back(bvks::gen_bv_ks_key(p, c.sk, galois_k, rng_bv));
+  }
+  std::vector<uint64_t> sk_coef(c.sk.data.begin(), c.sk.data.begin() + N);
+  utils::ntt_inv(sk_coef.data(), N, qs[0]);
+  GSWEval key_gsw(p, p.get_l_key(), p.get_base_log2_key());
+  c.gsw = key_gsw.plain_to_gsw(sk_coef, c.sk, c.rng);
+  return c;
+}
+
+// client.cpp:48-98
+std::vector<size_t> query_indices(const PirParams &p, size_t pt_idx) {
+  const size_t col = pt_idx % p.get_fst_dim_sz();
+  const size_t row = pt_idx / p.get_fst_dim_sz();
+  const size_t other = p.get_other_dim_sz();
+  const size_t d = p.get_num_dims();
+  std::vector<size_t> out = {col};
+  if (d == 1) return out;
+  const size_t h = d - 1;
+  const size_t r = 2 * other - (size_t{1} << h);
+  const size_t sl = other - r;
+  size_t perfect;
+  if (row < sl) {
+    out.push_back(0);
+    perfect = row;
+  } else {
+    const size_t corrected = row - sl;
+    out.push_back(corrected % 2);
+    perfect = sl + corrected / 2;
+  }
+  if (h > 1) {
+    for (size_t k = h - 2; k + 1 > 0; k--) {
+      out.push_back((perfect >> k) & 1ULL);
+      if (k == 0) break;
+    }
+  }
+  return out;
+}
+
+// client.cpp:107-225 (K == 1 branch: every config here is single-limb)
+RlweCt make_query(const PirParams &p, Client &c, size_t pt_idx) {
+  constexpr size_t N = DBConsts::PolyDegree;
+  const std::vector<uint64_t> qs(p.get_rns_mods().begin(), p.get_rns_mods().end());
+  const uint64_t t = p.get_plain_mod();
+  const std::vector<size_t> qi = query_indices(p, pt_idx);
+  const size_t h = p.get_expan_height();
+  const size_t capacity = size_t{1} << h;
+  uint64_t inverse = 0;
+  utils::try_invert_uint_mod(capacity, t, inverse);
+  const size_t rev = utils::bit_reverse(qi[0], h);
+  RlweCt query;
+  encrypt_zero_rns(c.sk, N, qs, p.get_noise_std_dev(), c.rng, query, false);
+  const uint64_t Q = qs[0];
+  const uint64_t scaled = utils::round_div_u128((uint128_t)Q * inverse, t) % Q;
+  query.c0[rev] = (query.c0[rev] + scaled) % Q;
+  if (qi.size() > 1) {
+    uint64_t inv_cap = 0;
+    utils::try_invert_uint_mod(capacity, Q, inv_cap);
+    const auto gadget = utils::gsw_gadget(p.get_l(), p.get_base_log2(), qs);
+    for (size_t i = 1; i < qi.size(); i++) {
+      if (qi[i] != 1) continue;
+      for (size_t k = 0; k < p.get_l(); k++) {
+        const size_t pos = p.get_fst_dim_sz() + (i - 1) * p.get_l() + k;
+        const size_t ridx = utils::bit_reverse(pos, h);
+        const uint64_t coef = (uint64_t)((uint128_t)gadget[0][k] * inv_cap % Q);
+        query.c0[ridx] = (uint64_t)(((uint128_t)query.c0[ridx] + coef) % Q);
+      }
+    }
+  }
+  return query;
+}
+
+// client.cpp:364-430, decryption under small_q.
+RlwePt decrypt_small_q(const PirParams &p, const Client &c, const RlweCt &ct) {
+  constexpr size_t N = DBConsts::PolyDegree;
+  const uint64_t q = p.get_small_q();
+  const uint64_t t = p.get_plain_mod();
+  std::vector<uint64_t> sk_coef(c.sk.data.begin(), c.sk.data.begin() + N);
+  utils::ntt_inv(sk_coef.data(), N, p.get_rns_mods()[0]);
+  std::vector<uint64_t> sks(N), c0(N), c1(N), phase(N);
+  for (size_t i = 0; i < N; i++) sks[i] = (sk_coef[i] > 1) ? (q - 1) : sk_coef[i];
+  utils::ntt_fwd(sks.data(), N, q);
+  for (size_t i = 0; i < N; i++) { c0[i] = ct.c0[i] % q; c1[i] = ct.c1[i] % q; }
+  utils::ntt_fwd(c1.data(), N, q);
+  intel::hexl::EltwiseMultMod(phase.data(), c1.data(), sks.data(), N, q, 1);
+  utils::ntt_inv(phase.data(), N, q);
+  intel::hexl::EltwiseAddMod(phase.data(), phase.data(), c0.data(), N, q);
+  RlwePt out;
+  out.data.resize(N);
+  for (size_t i = 0; i < N; i++)
+    out.data[i] = utils::round_div_u128((uint128_t)phase[i] * t, q) % t;
+  return out;
+}
+
+void write_u64(const std::string &path, const std::vector<uint64_t> &v) {
+  std::ofstream f(path, std::ios::binary);
+  f.write(reinterpret_cast<const char *>(v.data()), v.size() * 8);
+}
+
+struct Args {
+  std::string mode = "golden";
+  size_t target = 16384, height = 9;
+  bool pow2 = true;
+  uint64_t db_seed = 1, client_seed = 2;
+  size_t index = 0;
+  size_t queries = 1, warmup = 0;
+  std::string out;
+  bool dump_inputs = false;
+};
+
+Args parse(int argc, char **argv) {
+  Args a;
+  for (int i = 1; i < argc; ++i) {
+    std::string k = argv[i];
+    auto val = [&]() -> std::string {
+      if (i + 1 >= argc) throw std::invalid_argument("missing value for " + k);
+      return argv[++i];
+    };
+    if (k == "--mode") a.mode = val();
+    else if (k == "--target") a.target = std::stoull(val());
+    else if (k == "--height") a.height = std::stoull(val());
+    else if (k == "--pow2") a.pow2 = std::stoull(val()) != 0;
+    else if (k == "--db-seed") a.db_seed = std::stoull(val());
+    else if (k == "--client-seed") a.client_seed = std::stoull(val());
+    else if (k == "--index") a.index = std::stoull(val());
+    else if (k == "--queries") a.queries = std::stoull(val());
+    else if (k == "--warmup") a.warmup = std::stoull(val());
+    else if (k == "--out") a.out = val();
+    else if (k == "--dump-inputs") a.dump_inputs = true;
+    else throw std::invalid_argument("unknown option " + k);
+  }
+  return a;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  try {
+    const Args a = parse(argc, argv);
+    constexpr size_t N = DBConsts::PolyDegree;
+    PirParams params = PirParams().with_layout({a.target, a.height, a.pow2});
+    const uint64_t t = params.get_plain_mod();
+    PirServer server(params);
+    const uint64_t seed = a.db_seed;
+    PlaintextSource source = [&](size_t idx, RlwePt &out) {
+      out.data.resize(N);
+      for (size_t c = 0; c < N; ++c) out.data[c] = db_coeff(seed, idx, c, N, t);
+    };
+    const auto t_load0 = std::chrono::steady_clock::now();
+    std::vector<size_t> record;
+    if (a.mode == "golden") record.push_back(a.index);
+    server.load_data(a.target, source, record);
+    const double load_s = std::chrono::duration<double>(
+        std::chrono::steady_clock::now() - t_load0).count();
+
+    if (a.mode == "golden") {
+      Client c = make_client(params, a.client_seed);
+      server.set_client_bv_galois_key(1, c.bv);
+      server.set_client_gsw_key(1, c.gsw);
+      RlweCt query = make_query(params, c, a.index);
+      RlweCt query_copy = query;
+      RlweCt resp = server.make_query(1, query);
+      std::stringstream ss;
+      const size_t nbytes = server.save_resp_to_stream(resp, ss);
+      const std::string stream = ss.str();
+      RlwePt dec = decrypt_small_q(params, c, resp);
+      RlwePt want = server.direct_get_original_plaintext(a.index);
+      const bool ok = dec.data == want.data;
+      if (!a.out.empty()) {
+        std::vector<uint64_t> r(resp.c0);
+        r.insert(r.end(), resp.c1.begin(), resp.c1.end());
+        write_u64(a.out + "/response.u64", r);
+        std::ofstream(a.out + "/response.bin", std::ios::binary).write(stream.data(), stream.size());
+        if (a.dump_inputs) {
+          std::vector<uint64_t> qv(query_copy.c0);
+          qv.insert(qv.end(), query_copy.c1.begin(), query_copy.c1.end());
+          write_u64(a.out + "/query.u64", qv);
+          std::vector<uint64_t> kv;
+          for (const auto &key : c.bv.keys)
+            for (const auto &row : key.cts) {
+              kv.insert(kv.end(), row.b.begin(), row.b.end());
+              kv.insert(kv.end(), row.a.begin(), row.a.end());
+            }
+          write_u64(a.out + "/bv_keys.u64", kv);
+          std::vector<uint64_t> gv;
+          for (const auto &row : c.gsw) gv.insert(gv.end(), row.begin(), row.end());
+          write_u64(a.out + "/gsw_key.u64", gv);
+        }
+      }
+      const auto &crt = params.get_composite_rns();
+      std::printf(
+          "{\"ok\": %s, \"num_pt\": %zu, \"fst_dim_sz\": %zu, \"num_dims\": %zu, "
+          "\"other_dim_sz\": %zu, \"q\": %llu, \"q1\": %llu, \"q2\": %llu, \"w1\": %llu, "
+          "\"w2\": %llu, \"t\": %llu, \"small_q\": %llu, \"resp_bytes\": %zu, \"load_s\": %.3f}\n",
+          ok ? "true" : "false", params.get_num_pt(), params.get_fst_dim_sz(),
+          params.get_num_dims(), params.get_other_dim_sz(),
+          (unsigned long long)params.get_rns_mods()[0], (unsigned long long)crt.q1,
+          (unsigned long long)crt.q2, (unsigned long long)crt.w1,
+          (unsigned long long)crt.w2, (unsigned long long)t,
+          (unsigned long long)params.get_small_q(), nbytes, load_s);
+      return ok ? 0 : 3;
+    }
+
+    if (a.mode == "time") {
+      // The timer boundary is make_query only (merkle_benchmark.cpp:549-553).
+      std::vector<double> ms;
+      size_t failures = 0;
+      for (size_t q = 0; q < a.warmup + a.queries; ++q) {
+        Client c = make_client(params, a.client_seed + q);
+        server.set_client_bv_galois_key(q + 1, c.bv);
+        server.set_client_gsw_key(q + 1, c.gsw);
+        const size_t idx = static_cast<size_t>(mix64(a.client_seed * 7919 + q) % a.target);
+        RlweCt query = make_query(params, c, idx);
+        const auto t0 = std::chrono::steady_clock::now();
+        RlweCt resp = server.make_query(q + 1, query);
+        const double dt = std::chrono::duration<double, std::milli>(
+            std::chrono::steady_clock::now() - t0).count();
+        RlwePt dec = decrypt_small_q(params, c, resp);
+        for (size_t i = 0; i < N; ++i)
+          if (dec.data[i] != db_coeff(seed, idx, i, N, t)) { ++failures; break; }
+        if (q >= a.warmup) ms.push_back(dt);
+      }
+      double sum = 0;
+      for (double v : ms) sum += v;
+      std::printf("{\"mean_ms\": %.3f, \"queries\": %zu, \"failures\": %zu, \"load_s\": %.3f, \"samples_ms\": [",
+                  ms.empty() ? 0.0 : sum / ms.size(), ms.size(), failures, load_s);
+      for (size_t i = 0; i < ms.size(); ++i) std::printf("%s%.3f", i ? ", " : "", ms[i]);
+      std::printf("]}\n");
+      return failures ? 3 : 0;
+    }
+    throw std::invalid_argument("unknown mode " + a.mode);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "opir_ref error: %s\n", e.what());
+    return 1;
+  }
+}

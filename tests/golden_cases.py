@@ -1,0 +1,27 @@
+"""Loader for the reference-generated golden fixtures in tests/golden/."""
+import hashlib
+import json
+import os
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def cases():
+    with open(os.path.join(GOLDEN_DIR, "golden.json")) as f:
+        return json.load(f)["cases"]
+
+
+def case(name):
+    for c in cases():
+        if c["name"] == name:
+            return c
+    raise KeyError(name)
+
+
+def stream(c):
+    with open(os.path.join(GOLDEN_DIR, c["name"] + ".resp.bin"), "rb") as f:
+        return f.read()
+
+
+def sha256(arr) -> str:
+    return hashlib.sha256(memoryview(arr).cast("B")).hexdigest()
