@@ -1,0 +1,220 @@
+/* onionpir_b200.h -- C ABI of the B200 OnionPIRv2 server hot path.
+ *
+ * This library replaces the reference's PirServer query-processing path
+ * (src/server.cpp, src/gsw.cpp, src/bv_keyswitch.cpp, src/matrix.cpp of
+ * zcy05331/OnionPIRv2) with hand-written sm_100a CUDA kernels. Every entry
+ * point below names the reference interface it replaces (paths relative to
+ * the reference's src/). The parameter set is CONFIG_N2048_K1_COMP
+ * (includes/database_constants.h:77-94): N = 2048, logical q = q1*q2 with two
+ * 29-bit NTT primes, t = 4099, small_q = 4169729, L_EP = 6, L_KEY = 10,
+ * L_KS = 8.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only. Host buffers unless a name ends in
+ *     _device, in which case the pointers are CUDA device pointers.
+ *   - Every call returns an opir_status (0 = OK). A non-zero status never
+ *     leaves a CUDA error pending; opir_server_last_error() describes it. The
+ *     status codes map onto the exception types the reference throws.
+ *   - Ciphertexts are [c0 (N u64)][c1 (N u64)], coefficients canonical in
+ *     [0, q) (includes/rlwe.h:17-31, K = 1). Key rows are in the NTT domain of
+ *     the reference's NTT (HEXL ordering: forward output bit-reversed,
+ *     root = CRT of the minimal primitive 2N-th roots mod q1 and q2).
+ *   - A server handle owns its device memory (database, client keys, scratch
+ *     arena) on the device it was created on. Calls on one handle must not
+ *     run concurrently; distinct handles are independent.
+ */
+#ifndef ONIONPIR_B200_H
+#define ONIONPIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  OPIR_OK = 0,
+  OPIR_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  OPIR_ERR_OUT_OF_RANGE = 2,     /* std::out_of_range (unknown client, index) */
+  OPIR_ERR_RUNTIME = 3,          /* std::runtime_error */
+  OPIR_ERR_CUDA = 4,             /* CUDA launch/runtime failure */
+  OPIR_ERR_NO_MEMORY = 5,        /* device allocation failed / HBM budget */
+  OPIR_ERR_OVERFLOW = 6          /* std::overflow_error */
+} opir_status;
+
+/* PirLayoutConfig (includes/pir.h:199-203). */
+typedef struct {
+  uint64_t target_num_pt;
+  uint32_t expansion_height;
+  uint32_t fst_dim_pow2;
+} opir_layout;
+
+/* Derived runtime parameters: the values PirParams exposes through its
+ * getters (includes/pir.h:237-277, src/pir.cpp:14-134). */
+typedef struct {
+  uint32_t poly_degree;           /* N */
+  uint32_t num_limbs;             /* K (1: logical single modulus)       */
+  uint64_t q;                     /* logical ciphertext modulus q1*q2    */
+  uint64_t q1, q2;                /* composite first-dim limbs           */
+  uint64_t w1, w2, w_crt;         /* 2N-th roots: q1, q2 and CRT (mod q) */
+  uint64_t q1_inv_mod_q2;
+  uint64_t plain_mod;             /* t                                   */
+  uint64_t small_q;               /* modulus-switch target               */
+  uint32_t small_q_width;         /* response bits per coefficient       */
+  uint32_t ct_mod_width;          /* 58                                  */
+  uint32_t l_ep, l_key, l_ks;     /* gadget lengths                      */
+  uint32_t base_log2, base_log2_key, base_log2_ks;
+  uint64_t target_num_pt, num_pt, fst_dim_sz, other_dim_sz;
+  uint32_t num_dims, expansion_height, fst_dim_pow2;
+  uint32_t reserved;
+} opir_params;
+
+typedef struct opir_server opir_server;
+
+/* Plaintext source callback: fill out_coeffs[0..N) (each < t) for the given
+ * logical plaintext index. Returns 0 on success. Replaces PlaintextSource
+ * (includes/server.h:13). */
+typedef int (*opir_plaintext_source)(void *user, uint64_t logical_index,
+                                     uint64_t *out_coeffs);
+
+/* ---- parameters ---------------------------------------------------------- */
+
+/* PirParams().with_layout(layout) (src/pir.cpp:49-134). */
+opir_status opir_params_init(const opir_layout *layout, opir_params *out);
+
+/* Bytes of the serialized response: ceil(2 N small_q_width / 8). */
+size_t opir_response_bytes(const opir_params *params);
+
+/* ---- server lifetime ------------------------------------------------------ */
+
+/* PirServer::PirServer(const PirParams&) (src/server.cpp:29-46). Allocates
+ * the device database on CUDA device `device`. */
+opir_status opir_server_create(const opir_params *params, int device,
+                               opir_server **out);
+/* PirServer::~PirServer (src/server.cpp:48-49). NULL is a no-op. */
+void opir_server_destroy(opir_server *server);
+/* Human-readable description of the last failure on this handle. */
+const char *opir_server_last_error(const opir_server *server);
+/* The parameters the server was created with. */
+opir_status opir_server_params(const opir_server *server, opir_params *out);
+
+/* ---- database ------------------------------------------------------------- */
+
+/* PirServer::load_data (src/server.cpp:80-203) with the plaintexts given as
+ * one host array: logical_num_pt x N coefficients, each < t. The rounded
+ * tail [logical_num_pt, num_pt) is zero. NTT, CRT split and the transpose
+ * into the coefficient-major first-dimension layout run on the device. */
+opir_status opir_server_load_db(opir_server *server, uint64_t logical_num_pt,
+                                const uint64_t *coeffs);
+/* Same, 16-bit coefficients (t < 2^16), halving the host->device bytes. */
+opir_status opir_server_load_db_u16(opir_server *server,
+                                    uint64_t logical_num_pt,
+                                    const uint16_t *coeffs);
+/* Same, pulling plaintexts through a callback like the reference's
+ * PlaintextSource; the callback is called once per logical index, in order. */
+opir_status opir_server_load_db_source(opir_server *server,
+                                       uint64_t logical_num_pt,
+                                       opir_plaintext_source source,
+                                       void *user);
+/* Synthetic database generated on the device from a seed:
+ * coefficient(pt, c) = mix64(seed + (pt*N + c + 1) * 0x9E3779B97F4A7C15) % t
+ * (SplitMix64 finaliser). Used by benchmarks and tests. */
+opir_status opir_server_load_db_seeded(opir_server *server,
+                                       uint64_t logical_num_pt, uint64_t seed);
+
+/* ---- client keys ---------------------------------------------------------- */
+
+/* PirServer::set_client_bv_galois_key + set_client_gsw_key
+ * (src/server.cpp:857-863) / set_client_session_keys (:865-875).
+ *   bv_keys : n_keys x L_KS rows x [b (N)][a (N)] u64, NTT form
+ *             (bvks::BvKeySwitchKey, includes/bv_keyswitch.h:48-66)
+ *   galois_ks: n_keys automorphism exponents; every (N >> i) + 1 for
+ *             i < expansion_height must be present
+ *   gsw_key : 2 L_KEY rows x [c0 (N)][c1 (N)] u64, NTT form (GSWCt RGSW(s))
+ * Re-registering a client id replaces its keys. */
+opir_status opir_server_set_client_keys(opir_server *server, uint64_t client_id,
+                                        const uint64_t *bv_keys,
+                                        const uint32_t *galois_ks,
+                                        uint32_t n_keys,
+                                        const uint64_t *gsw_key);
+opir_status opir_server_remove_client(opir_server *server, uint64_t client_id);
+
+/* ---- query processing ----------------------------------------------------- */
+
+/* PirServer::make_query (src/server.cpp:895-947): expansion, selector
+ * completion, first dimension, remaining dimensions, modulus switch.
+ *   query    : [c0 (N)][c1 (N)] u64 coefficient form mod q
+ *   response : [c0 (N)][c1 (N)] u64 coefficient form mod small_q
+ * Unknown client_id -> OPIR_ERR_OUT_OF_RANGE (the reference's map::at). */
+opir_status opir_server_make_query(opir_server *server, uint64_t client_id,
+                                   const uint64_t *query, uint64_t *response);
+
+/* Batched form: n independent queries (each with its own client) answered
+ * in one pass, the first-dimension scan reading the database once for the
+ * whole batch. queries: n x 2N u64; responses: n x 2N u64. */
+opir_status opir_server_make_query_batch(opir_server *server, uint32_t n,
+                                         const uint64_t *client_ids,
+                                         const uint64_t *queries,
+                                         uint64_t *responses);
+
+/* Batched form on device-resident buffers, enqueued on `stream`
+ * (a cudaStream_t; NULL = the handle's own stream). client_ids is a host
+ * array. The call returns after enqueueing; synchronise the stream before
+ * reading d_responses. */
+opir_status opir_server_make_query_batch_device(opir_server *server, uint32_t n,
+                                                const uint64_t *client_ids,
+                                                const uint64_t *d_queries,
+                                                uint64_t *d_responses,
+                                                void *stream);
+
+/* Per-stage device times (ms) of the last make_query / batch call, in the
+ * reference's TimerLogger sections (includes/logging.h:34-78):
+ * [0] Expand, [1] Convert, [2] First dim, [3] Other dim, [4] Modulus switching.
+ * Stage timing must have been enabled with opir_server_set_stage_timing. */
+opir_status opir_server_set_stage_timing(opir_server *server, int enabled);
+opir_status opir_server_stage_times(const opir_server *server, float *ms_out);
+
+/* ---- individual stages (public PirServer methods used by tests and by the
+ *      reference's tree-PIR callers) --------------------------------------- */
+
+/* PirServer::expand_query (src/server.cpp:818-821): useful leaves
+ * u = fst_dim_sz + L_EP (num_dims - 1), out: u x 2N u64 coefficient form. */
+opir_status opir_server_expand_query(opir_server *server, uint64_t client_id,
+                                     const uint64_t *query, uint64_t *out);
+/* PirServer::complete_selectors (src/server.cpp:823-855): expanded is the
+ * expand_query output; out: (num_dims-1) x 2 L_EP rows x 2N u64, NTT form. */
+opir_status opir_server_complete_selectors(opir_server *server,
+                                           uint64_t client_id,
+                                           const uint64_t *expanded,
+                                           uint64_t *out);
+/* PirServer::evaluate_first_dim (src/server.cpp:313-405): fst_query is
+ * fst_dim_sz x 2N u64 coefficient form; out: other_dim_sz x 2N u64
+ * coefficient form. */
+opir_status opir_server_evaluate_first_dim(opir_server *server,
+                                           const uint64_t *fst_query,
+                                           uint64_t *out);
+/* PirServer::evaluate_other_dim (src/server.cpp:599-649): mid is
+ * other_dim_sz x 2N coefficient form, selectors as produced by
+ * complete_selectors; out: 2N u64 (before the modulus switch). */
+opir_status opir_server_evaluate_other_dim(opir_server *server,
+                                           const uint64_t *mid,
+                                           const uint64_t *selectors,
+                                           uint64_t *out);
+
+/* ---- response codec ------------------------------------------------------- */
+
+/* PirServer::save_resp_to_stream (src/server.cpp:950-1009): c0 then c1,
+ * small_q_width bits per coefficient, LSB-first, zero-padded last byte.
+ * Returns the byte count, or 0 if cap is too small. Host-only helper (the
+ * device path writes the same bytes in its modulus-switch kernel). */
+size_t opir_save_response(const opir_params *params, const uint64_t *response,
+                          uint8_t *out, size_t cap);
+
+/* Library version string. */
+const char *opir_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ONIONPIR_B200_H */

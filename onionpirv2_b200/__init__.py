@@ -1,0 +1,10 @@
+"""B200-native (sm_100a) OnionPIRv2 server hot path.
+
+The compute lives in libonionpir_b200.so (CUDA kernels behind a C ABI, see
+include/onionpir_b200.h); this package is the host-side mirror of the
+reference's PirParams / PirServer interface over that ABI.
+"""
+from .server import (DeviceError, OutOfRange, PirParams, PirServer,  # noqa: F401
+                     save_response)
+
+__all__ = ["PirParams", "PirServer", "save_response", "OutOfRange", "DeviceError"]

@@ -1,0 +1,612 @@
+// sm_100a kernels of the OnionPIRv2 server path. Every kernel runs 256
+// threads per block; polynomial kernels keep their working planes in shared
+// memory (8 KiB per residue plane) and run the block-cooperative NTT of
+// opir_device.cuh. Thread t owns coefficient positions t + 256 s, s < 8, for
+// every per-coefficient step, so global reads of planes are coalesced.
+#include "opir_kernels.h"
+
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+namespace opir {
+
+namespace {
+
+constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ull;
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ ResidueTables pick(const DevParams &P, int res) {
+  return res ? P.r[1] : P.r[0];
+}
+
+void check_launch(const char *what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Raise a kernel's dynamic shared-memory limit once per (device, kernel,
+// size); cudaFuncSetAttribute applies to the current device.
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> granted;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_pair(dev, reinterpret_cast<const void *>(kernel));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = granted.find(key);
+  if (it != granted.end() && it->second >= bytes) return;
+  const cudaError_t e = cudaFuncSetAttribute(
+      kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  granted[key] = bytes;
+}
+
+// ------------------------------------------------------------ split/compose
+__global__ void k_split_u64(DevParams P, const uint64_t *__restrict__ in,
+                            uint32_t *__restrict__ out, uint64_t n, uint64_t per_item,
+                            uint64_t stride) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = i >> kLogN, j = i & (kN - 1);
+    const uint64_t item = p / per_item, pp = p % per_item;
+    const uint64_t v = in[i];
+    uint32_t *o = out + item * stride + pp * 2 * kN + j;
+    o[0] = reduce64(v, P.q1, P.r[0].mu);
+    o[kN] = reduce64(v, P.q2, P.r[1].mu);
+  }
+}
+
+__global__ void k_compose_u64(DevParams P, const uint32_t *__restrict__ in, uint64_t stride,
+                              uint64_t *__restrict__ out, uint64_t n, uint64_t per_item) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = i >> kLogN, j = i & (kN - 1);
+    const uint64_t item = p / per_item, pp = p % per_item;
+    const uint32_t *s = in + item * stride + pp * 2 * kN + j;
+    out[i] = crt_compose(s[0], s[kN], P);
+  }
+}
+
+// --------------------------------------------------------- DB preprocessing
+constexpr int kDbTile = 8;
+
+__global__ void __launch_bounds__(kThreads)
+k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
+                uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
+                uint64_t logical, uint64_t num_pt, uint64_t pt_begin,
+                uint64_t pt_end, uint32_t *__restrict__ db) {
+  extern __shared__ uint32_t sm[];
+  const int res = blockIdx.y;
+  const ResidueTables T = pick(P, res);
+  const uint64_t pt0 = pt_begin + (uint64_t)blockIdx.x * kDbTile;
+  for (int idx = threadIdx.x; idx < kDbTile * kN; idx += kThreads) {
+    const int p = idx >> kLogN, c = idx & (kN - 1);
+    const uint64_t pt = pt0 + p;
+    uint32_t v = 0;
+    if (pt < pt_end && pt < logical) {
+      if (coeffs != nullptr)
+        v = coeffs[(pt - coeff_pt_begin) * kN + c];
+      else
+        v = static_cast<uint32_t>(mix64(seed + (pt * kN + c + 1) * kGolden) % t);
+    }
+    sm[idx] = v;  // v < t < q_res: already canonical
+  }
+  __syncthreads();
+  ntt_fwd_planes(sm, kDbTile, T);
+  uint32_t *dbr = db + (uint64_t)res * kN * num_pt;
+  for (int idx = threadIdx.x; idx < kDbTile * kN; idx += kThreads) {
+    const int c = idx / kDbTile, p = idx % kDbTile;
+    const uint64_t pt = pt0 + p;
+    if (pt < pt_end) dbr[(uint64_t)c * num_pt + pt] = sm[p * kN + c];
+  }
+}
+
+// ----------------------------------------------------------- expansion level
+// One heap node (and one residue) per block: BV key switch of the node's
+// ciphertext (bv_keyswitch.cpp:296-367) then the two children
+// (server.cpp:794-809): left = c + c', right = (c - c') X^-k.
+__global__ void __launch_bounds__(kThreads, 2)
+k_expand_level(DevParams P, uint32_t galois, uint32_t kshift, int base_ks, int l_ks,
+               const uint32_t *__restrict__ in, uint64_t in_stride,
+               uint32_t *__restrict__ out, uint64_t out_stride,
+               const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  extern __shared__ uint32_t sm[];
+  uint32_t *sc1 = sm;            // sigma(c1), both residues
+  uint32_t *sc0 = sm + 2 * kN;   // sigma(c0), own residue
+  uint32_t *D = sm + 3 * kN;     // digit planes
+  const int node = blockIdx.x, res = blockIdx.y, b = blockIdx.z;
+  const ResidueTables T = pick(P, res);
+  const uint32_t q = T.q;
+  const uint32_t *ct = in + ((uint64_t)b * in_stride + node) * kCtWords;
+  const uint32_t *c0 = ct + res * kN;
+  const uint32_t *c1 = ct + 2 * kN + res * kN;
+
+  // sigma_k on c1 (both residues) and c0 (own residue), utils.cpp:58-72
+  for (int i = threadIdx.x; i < kN; i += kThreads) {
+    uint32_t dest = (static_cast<uint32_t>(i) * galois) & (2 * kN - 1);
+    const bool neg = dest >= kN;
+    dest &= kN - 1;
+    const uint32_t a0 = ct[2 * kN + i], a1 = ct[3 * kN + i], z = c0[i];
+    sc1[dest] = neg ? neg_mod(a0, P.q1) : a0;
+    sc1[kN + dest] = neg ? neg_mod(a1, P.q2) : a1;
+    sc0[dest] = neg ? neg_mod(z, q) : z;
+  }
+  __syncthreads();
+  // signed base-2^base_ks decomposition of sigma(c1) (mod q), digits LSB first
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    int64_t d = centre(crt_compose(sc1[j], sc1[kN + j], P), P);
+    for (int t = 0; t < l_ks; ++t) D[t * kN + j] = digit_residue(next_digit(d, base_ks), q);
+  }
+  __syncthreads();
+  ntt_fwd_planes(D, l_ks, T);
+  // inner product with the key rows (row t encrypts sigma(s) B^t)
+  const uint32_t *key = bv_keys[b] + bv_level_off + res * kN;
+  uint32_t rb[kPer], ra[kPer];
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    uint64_t ab = 0, aa = 0;
+    for (int t = 0; t < l_ks; ++t) {
+      const uint64_t dv = D[t * kN + j];
+      ab += dv * __ldg(key + (uint64_t)(t * 4 + 0) * kN + j);
+      aa += dv * __ldg(key + (uint64_t)(t * 4 + 2) * kN + j);
+    }
+    rb[s] = reduce64(ab, q, T.mu);
+    ra[s] = reduce64(aa, q, T.mu);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    D[j] = rb[s];
+    D[kN + j] = ra[s];
+  }
+  __syncthreads();
+  ntt_inv_planes(D, 2, T);
+  uint32_t *outL = out + ((uint64_t)b * out_stride + 2 * (uint64_t)node) * kCtWords;
+  uint32_t *outR = outL + kCtWords;
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    const uint32_t n0v = add_mod(sc0[j], D[j], q);   // c0' = sigma(c0) + delta_b
+    const uint32_t n1v = D[kN + j];                  // c1' = delta_a
+    const uint32_t o0 = c0[j], o1 = c1[j];
+    outL[res * kN + j] = add_mod(o0, n0v, q);
+    outL[2 * kN + res * kN + j] = add_mod(o1, n1v, q);
+    const uint32_t d0 = sub_mod(o0, n0v, q), d1 = sub_mod(o1, n1v, q);
+    int dst = j - static_cast<int>(kshift);
+    const bool wrap = dst < 0;
+    if (wrap) dst += kN;
+    outR[res * kN + dst] = wrap ? neg_mod(d0, q) : d0;
+    outR[2 * kN + res * kN + dst] = wrap ? neg_mod(d1, q) : d1;
+  }
+}
+
+// Shared gadget product of a coefficient-form ciphertext (both residues read
+// from `x` / optional `y`: the decomposed value is y - x, or x when y is
+// null) against NTT-form RGSW rows: acc_k += sum_rows digit * rgsw[row][k].
+// Digit i (LSB first) of poly p meets row p*l + (l - 1 - i) (gsw.cpp:283-293).
+__device__ __forceinline__ void gadget_mac(const DevParams &P, const ResidueTables &T,
+                                           int res, const uint32_t *x, const uint32_t *y,
+                                           const uint32_t *rgsw, int l, int base_log2,
+                                           uint32_t *D, uint64_t (&acc0)[kPer],
+                                           uint64_t (&acc1)[kPer]) {
+  const uint32_t q = T.q;
+#pragma unroll 1
+  for (int p = 0; p < 2; ++p) {
+#pragma unroll
+    for (int s = 0; s < kPer; ++s) {
+      const int j = threadIdx.x + s * kThreads;
+      uint32_t v1 = x[(p * 2 + 0) * kN + j], v2 = x[(p * 2 + 1) * kN + j];
+      if (y != nullptr) {
+        v1 = sub_mod(y[(p * 2 + 0) * kN + j], v1, P.q1);
+        v2 = sub_mod(y[(p * 2 + 1) * kN + j], v2, P.q2);
+      }
+      int64_t d = centre(crt_compose(v1, v2, P), P);
+      for (int i = 0; i < l; ++i) D[i * kN + j] = digit_residue(next_digit(d, base_log2), q);
+    }
+    __syncthreads();
+    ntt_fwd_planes(D, l, T);
+#pragma unroll
+    for (int s = 0; s < kPer; ++s) {
+      const int j = threadIdx.x + s * kThreads;
+      uint64_t a0 = acc0[s], a1 = acc1[s];
+      for (int i = 0; i < l; ++i) {
+        const int row = p * l + (l - 1 - i);
+        const uint64_t dv = D[i * kN + j];
+        const uint32_t *R = rgsw + (uint64_t)row * kCtWords + res * kN + j;
+        a0 += dv * __ldg(R);
+        a1 += dv * __ldg(R + 2 * kN);
+      }
+      acc0[s] = a0;
+      acc1[s] = a1;
+    }
+    __syncthreads();
+  }
+}
+
+// -------------------------------------------------------- selector completion
+__global__ void __launch_bounds__(kThreads, 2)
+k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
+            const uint32_t *const *__restrict__ gsw_keys, uint32_t *__restrict__ sel) {
+  extern __shared__ uint32_t D[];
+  const int row_id = blockIdx.x, res = blockIdx.y, b = blockIdx.z;
+  const int selno = row_id / S.l_ep, r = row_id % S.l_ep;
+  const ResidueTables T = pick(P, res);
+  const uint32_t *ct = leaves + ((uint64_t)b * leaf_stride + S.n0 + row_id) * kCtWords;
+  uint32_t *out = sel + ((uint64_t)b * (S.num_dims - 1) + selno) * 2 * S.l_ep * kCtWords;
+  uint64_t acc0[kPer], acc1[kPer];
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) acc0[s] = acc1[s] = 0;
+  // bottom row: ExtProd(RGSW(s), row) with the key gadget (gsw.cpp:119-182)
+  gadget_mac(P, T, res, ct, nullptr, gsw_keys[b], S.l_key, S.base_key, D, acc0, acc1);
+  uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords;
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    bot[res * kN + j] = reduce64(acc0[s], T.q, T.mu);
+    bot[2 * kN + res * kN + j] = reduce64(acc1[s], T.q, T.mu);
+    D[j] = ct[res * kN + j];
+    D[kN + j] = ct[2 * kN + res * kN + j];
+  }
+  __syncthreads();
+  // top row: the expanded row itself in NTT form (gsw.cpp:330-338)
+  ntt_fwd_planes(D, 2, T);
+  uint32_t *top = out + (uint64_t)r * kCtWords;
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    top[res * kN + j] = D[j];
+    top[2 * kN + res * kN + j] = D[kN + j];
+  }
+}
+
+// ------------------------------------------------------- first-dim query prep
+constexpr int kFstTile = 4;  // ciphertexts per block (8 planes)
+
+__global__ void __launch_bounds__(kThreads)
+k_fst_prep(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
+           uint32_t *__restrict__ qmat, uint32_t ncols) {
+  extern __shared__ uint32_t sm[];
+  const int res = blockIdx.y, b = blockIdx.z;
+  const uint32_t k0 = blockIdx.x * kFstTile;
+  const ResidueTables T = pick(P, res);
+  for (int idx = threadIdx.x; idx < 2 * kFstTile * kN; idx += kThreads) {
+    const int e = idx >> kLogN, j = idx & (kN - 1);
+    const uint32_t k = k0 + (e >> 1);
+    const int p = e & 1;
+    sm[idx] = k < S.n0 ? leaves[((uint64_t)b * leaf_stride + k) * kCtWords + (p * 2 + res) * kN + j] : 0u;
+  }
+  __syncthreads();
+  ntt_fwd_planes(sm, 2 * kFstTile, T);
+  for (int idx = threadIdx.x; idx < 2 * kFstTile * kN; idx += kThreads) {
+    const int l = idx / (2 * kFstTile), e = idx % (2 * kFstTile);
+    const uint32_t k = k0 + (e >> 1);
+    const int p = e & 1;
+    if (k < S.n0)
+      qmat[(((uint64_t)res * kN + l) * S.n0 + k) * ncols + 2 * b + p] = sm[e * kN + l];
+  }
+}
+
+// ------------------------------------------------------------ first-dim scan
+// Block = (column tile, NTT level, residue). A warp owns one database row at a
+// time; its lanes split the first dimension k, accumulate exact 64-bit sums
+// of 29x29-bit products (at most 64 per lane, so no overflow), reduce them
+// mod q and finish with a shuffle tree of modular adds. The query tile is
+// staged transposed in shared memory ([column][k]) so each lane reads its
+// four k values per column with one 16-byte load.
+template <int NCT, bool VEC>
+__global__ void __launch_bounds__(kThreads)
+k_scan(DevParams P, uint32_t n0, uint32_t m, const uint32_t *__restrict__ db,
+       uint64_t num_pt, const uint32_t *__restrict__ qmat, uint32_t ncols,
+       uint32_t *__restrict__ cmat) {
+  extern __shared__ __align__(16) uint32_t qs[];  // [NCT][n0]
+  const int ct0 = blockIdx.x * NCT;
+  const int l = blockIdx.y, res = blockIdx.z;
+  const uint32_t q = res ? P.q2 : P.q1;
+  const uint64_t mu = res ? P.r[1].mu : P.r[0].mu;
+  const uint32_t *Q = qmat + ((uint64_t)res * kN + l) * n0 * ncols;
+  for (uint32_t idx = threadIdx.x; idx < n0 * NCT; idx += kThreads) {
+    const uint32_t k = idx / NCT, c = idx % NCT;
+    qs[c * n0 + k] = (ct0 + c < (int)ncols) ? Q[(uint64_t)k * ncols + ct0 + c] : 0u;
+  }
+  __syncthreads();
+  const uint32_t *A = db + ((uint64_t)res * kN + l) * num_pt;
+  uint32_t *C = cmat + ((uint64_t)res * kN + l) * m * ncols;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t r = warp; r < m; r += kThreads / 32) {
+    const uint32_t *Ar = A + (uint64_t)r * n0;
+    uint64_t acc[NCT];
+#pragma unroll
+    for (int c = 0; c < NCT; ++c) acc[c] = 0;
+    if (VEC) {
+      for (uint32_t k = 4 * lane; k < n0; k += 128) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4 *>(Ar + k));
+#pragma unroll
+        for (int c = 0; c < NCT; ++c) {
+          const uint4 b = *reinterpret_cast<const uint4 *>(qs + c * n0 + k);
+          acc[c] += (uint64_t)a.x * b.x + (uint64_t)a.y * b.y;
+          acc[c] += (uint64_t)a.z * b.z + (uint64_t)a.w * b.w;
+        }
+      }
+    } else {
+      for (uint32_t k = lane; k < n0; k += 32) {
+        const uint64_t a = __ldg(Ar + k);
+#pragma unroll
+        for (int c = 0; c < NCT; ++c) acc[c] += a * qs[c * n0 + k];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NCT; ++c) {
+      uint32_t v = reduce64(acc[c], q, mu);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v = add_mod(v, __shfl_xor_sync(0xffffffffu, v, off), q);
+      if (lane == c && ct0 + c < (int)ncols) C[(uint64_t)r * ncols + ct0 + c] = v;
+    }
+  }
+}
+
+// ----------------------------------------------------------- scan epilogue
+constexpr int kEpiTile = 4;  // candidates per block (8 planes)
+
+__global__ void __launch_bounds__(kThreads)
+k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_t ncols,
+                uint32_t *__restrict__ mid, uint64_t mid_stride) {
+  extern __shared__ uint32_t sm[];
+  const int res = blockIdx.y, b = blockIdx.z;
+  const uint32_t r0 = blockIdx.x * kEpiTile;
+  const ResidueTables T = pick(P, res);
+  for (int idx = threadIdx.x; idx < 2 * kEpiTile * kN; idx += kThreads) {
+    const int l = idx / (2 * kEpiTile), e = idx % (2 * kEpiTile);
+    const uint32_t r = r0 + (e >> 1);
+    const int p = e & 1;
+    sm[e * kN + l] = r < S.other
+        ? cmat[(((uint64_t)res * kN + l) * S.other + r) * ncols + 2 * b + p] : 0u;
+  }
+  __syncthreads();
+  ntt_inv_planes(sm, 2 * kEpiTile, T);
+  for (int idx = threadIdx.x; idx < 2 * kEpiTile * kN; idx += kThreads) {
+    const int e = idx >> kLogN, j = idx & (kN - 1);
+    const uint32_t r = r0 + (e >> 1);
+    const int p = e & 1;
+    if (r < S.other)
+      mid[((uint64_t)b * mid_stride + r) * kCtWords + (p * 2 + res) * kN + j] = sm[idx];
+  }
+}
+
+// --------------------------------------------------------------- MUX level
+// ext_prod_mux (server.cpp:652-722): out = x + INTT(ExtProd(sel, y - x)).
+__global__ void __launch_bounds__(kThreads, 2)
+k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t offset,
+            uint32_t half, const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+            uint64_t mid_stride, const uint32_t *__restrict__ sel) {
+  extern __shared__ uint32_t D[];
+  const int res = blockIdx.y, b = blockIdx.z;
+  const uint32_t i = blockIdx.x;
+  const uint32_t *base_in = in + (uint64_t)b * mid_stride * kCtWords;
+  uint32_t *base_out = out + (uint64_t)b * mid_stride * kCtWords;
+  if (i >= n_pairs) {  // level 0: carry the unpaired prefix over unchanged
+    const uint32_t c = i - n_pairs;
+    for (int j = threadIdx.x; j < kN; j += kThreads) {
+      base_out[(uint64_t)c * kCtWords + res * kN + j] = base_in[(uint64_t)c * kCtWords + res * kN + j];
+      base_out[(uint64_t)c * kCtWords + 2 * kN + res * kN + j] =
+          base_in[(uint64_t)c * kCtWords + 2 * kN + res * kN + j];
+    }
+    return;
+  }
+  uint32_t xi, yi, oi;
+  if (level == 0) { xi = offset + 2 * i; yi = xi + 1; oi = offset + i; }
+  else { xi = i; yi = i + half; oi = i; }
+  const ResidueTables T = pick(P, res);
+  const uint32_t *x = base_in + (uint64_t)xi * kCtWords;
+  const uint32_t *y = base_in + (uint64_t)yi * kCtWords;
+  const uint32_t *rgsw = sel + ((uint64_t)b * (S.num_dims - 1) + level) * 2 * S.l_ep * kCtWords;
+  uint64_t acc0[kPer], acc1[kPer];
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) acc0[s] = acc1[s] = 0;
+  gadget_mac(P, T, res, x, y, rgsw, S.l_ep, S.base_ep, D, acc0, acc1);
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    D[j] = reduce64(acc0[s], T.q, T.mu);
+    D[kN + j] = reduce64(acc1[s], T.q, T.mu);
+  }
+  __syncthreads();
+  ntt_inv_planes(D, 2, T);
+  uint32_t *o = base_out + (uint64_t)oi * kCtWords;
+#pragma unroll
+  for (int s = 0; s < kPer; ++s) {
+    const int j = threadIdx.x + s * kThreads;
+    o[res * kN + j] = add_mod(x[res * kN + j], D[j], T.q);
+    o[2 * kN + res * kN + j] = add_mod(x[2 * kN + res * kN + j], D[kN + j], T.q);
+  }
+}
+
+// ------------------------------------------------ modulus switch + packing
+// utils.cpp:445-462: centred round(v * out / inp), inp = q, out = small_q.
+__device__ __forceinline__ uint64_t rescale_dev(uint64_t v, uint64_t inp, uint64_t outm) {
+  const int64_t inp_i = static_cast<int64_t>(inp);
+  int64_t c = static_cast<int64_t>(v);
+  if (c >= inp_i / 2) c -= inp_i;
+  const bool neg = c < 0;
+  const uint64_t mag = neg ? static_cast<uint64_t>(-c) : static_cast<uint64_t>(c);
+  const unsigned __int128 num =
+      static_cast<unsigned __int128>(mag) * outm + static_cast<uint64_t>(inp_i / 2);
+  const uint64_t quo = static_cast<uint64_t>(num / inp) % outm;
+  return neg ? (quo ? outm - quo : 0) : quo;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_modswitch(DevParams P, const uint32_t *__restrict__ ct_all, uint64_t ct_stride,
+            uint64_t *__restrict__ resp, uint8_t *__restrict__ bytes, uint32_t resp_bytes) {
+  __shared__ uint32_t vals[2 * kN];
+  const int b = blockIdx.x;
+  const uint32_t *ct = ct_all + (uint64_t)b * ct_stride * kCtWords;
+  for (int idx = threadIdx.x; idx < 2 * kN; idx += kThreads) {
+    const int p = idx >> kLogN, j = idx & (kN - 1);
+    const uint64_t v = crt_compose(ct[(p * 2 + 0) * kN + j], ct[(p * 2 + 1) * kN + j], P);
+    const uint64_t r = rescale_dev(v, P.q, P.small_q);
+    resp[(uint64_t)b * 2 * kN + idx] = r;
+    vals[idx] = static_cast<uint32_t>(r & ((1ull << P.small_q_width) - 1));
+  }
+  if (bytes == nullptr) return;
+  __syncthreads();
+  const uint32_t w = P.small_q_width;
+  for (uint32_t B = threadIdx.x; B < resp_bytes; B += kThreads) {
+    const uint64_t bit0 = 8ull * B;
+    const uint32_t i = static_cast<uint32_t>(bit0 / w), o = static_cast<uint32_t>(bit0 % w);
+    uint64_t v = vals[i] >> o;
+    const uint32_t have = w - o;
+    if (have < 8 && i + 1 < 2 * kN) v |= static_cast<uint64_t>(vals[i + 1]) << have;
+    bytes[(uint64_t)b * resp_bytes + B] = static_cast<uint8_t>(v & 0xFF);
+  }
+}
+
+inline unsigned grid1d(uint64_t n) {
+  const uint64_t g = (n + kThreads - 1) / kThreads;
+  return static_cast<unsigned>(g < 65535ull * 16 ? g : 65535ull * 16);
+}
+
+}  // namespace
+
+// ===================================================================== launchers
+void launch_split_u64(const DevParams &P, const uint64_t *in, uint32_t *out, uint64_t n_items,
+                      uint64_t per_item, uint64_t out_item_stride, cudaStream_t st) {
+  const uint64_t n = n_items * per_item * kN;
+  if (n == 0) return;
+  k_split_u64<<<grid1d(n), kThreads, 0, st>>>(P, in, out, n, per_item, out_item_stride);
+  check_launch("k_split_u64");
+}
+
+void launch_compose_u64(const DevParams &P, const uint32_t *in, uint64_t in_item_stride,
+                        uint64_t *out, uint64_t n_items, uint64_t per_item, cudaStream_t st) {
+  const uint64_t n = n_items * per_item * kN;
+  if (n == 0) return;
+  k_compose_u64<<<grid1d(n), kThreads, 0, st>>>(P, in, in_item_stride, out, n, per_item);
+  check_launch("k_compose_u64");
+}
+
+void launch_db_preprocess(const DevParams &P, const uint16_t *coeffs, uint64_t coeff_pt_begin,
+                          uint64_t seed, uint64_t t, uint64_t logical, uint64_t num_pt,
+                          uint64_t pt_begin, uint64_t pt_end, uint32_t *db, cudaStream_t st) {
+  if (pt_end <= pt_begin) return;
+  const size_t smem = kDbTile * kN * sizeof(uint32_t);
+  set_smem(k_db_preprocess, smem);
+  const uint64_t tiles = (pt_end - pt_begin + kDbTile - 1) / kDbTile;
+  dim3 grid(static_cast<unsigned>(tiles), 2);
+  k_db_preprocess<<<grid, kThreads, smem, st>>>(P, coeffs, coeff_pt_begin, seed, t, logical,
+                                                 num_pt, pt_begin, pt_end, db);
+  check_launch("k_db_preprocess");
+}
+
+void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const uint32_t *in,
+                         uint64_t in_stride, uint32_t *out, uint64_t out_stride,
+                         const uint32_t *const *bv_keys, uint64_t bv_level_stride,
+                         uint32_t batch, cudaStream_t st) {
+  const uint32_t nodes = expand_nodes(s, d);
+  const size_t smem = (3 + s.l_ks) * kN * sizeof(uint32_t);
+  set_smem(k_expand_level, smem);
+  const uint32_t k = 1u << d;
+  const uint32_t galois = kN / k + 1;
+  dim3 grid(nodes, 2, batch);
+  k_expand_level<<<grid, kThreads, smem, st>>>(P, galois, k, s.base_ks, s.l_ks, in, in_stride,
+                                                out, out_stride, bv_keys, d * bv_level_stride);
+  check_launch("k_expand_level");
+}
+
+void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves,
+                      uint64_t leaf_stride, const uint32_t *const *gsw_keys, uint32_t *sel,
+                      uint32_t batch, cudaStream_t st) {
+  if (s.num_dims <= 1) return;
+  const size_t smem = s.l_key * kN * sizeof(uint32_t);
+  set_smem(k_selectors, smem);
+  dim3 grid((s.num_dims - 1) * s.l_ep, 2, batch);
+  k_selectors<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
+  check_launch("k_selectors");
+}
+
+void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
+                     uint64_t leaf_stride, uint32_t *qmat, uint32_t batch, cudaStream_t st) {
+  const size_t smem = 2 * kFstTile * kN * sizeof(uint32_t);
+  set_smem(k_fst_prep, smem);
+  dim3 grid((s.n0 + kFstTile - 1) / kFstTile, 2, batch);
+  k_fst_prep<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, qmat, 2 * batch);
+  check_launch("k_fst_prep");
+}
+
+template <int NCT>
+static void scan_dispatch(const DevParams &P, const Shape &s, const uint32_t *db,
+                          const uint32_t *qmat, uint32_t *cmat, uint32_t ncols,
+                          cudaStream_t st) {
+  const size_t smem = (size_t)NCT * s.n0 * sizeof(uint32_t);
+  dim3 grid((ncols + NCT - 1) / NCT, kN, 2);
+  if (s.n0 % 128 == 0) {
+    set_smem(k_scan<NCT, true>, smem);
+    k_scan<NCT, true><<<grid, kThreads, smem, st>>>(P, s.n0, s.other, db, s.num_pt, qmat, ncols, cmat);
+  } else {
+    set_smem(k_scan<NCT, false>, smem);
+    k_scan<NCT, false><<<grid, kThreads, smem, st>>>(P, s.n0, s.other, db, s.num_pt, qmat, ncols, cmat);
+  }
+  check_launch("k_scan");
+}
+
+void launch_scan(const DevParams &P, const Shape &s, const uint32_t *db, const uint32_t *qmat,
+                 uint32_t *cmat, uint32_t batch, cudaStream_t st) {
+  const uint32_t ncols = 2 * batch;
+  if (ncols <= 2) scan_dispatch<2>(P, s, db, qmat, cmat, ncols, st);
+  else if (ncols <= 4) scan_dispatch<4>(P, s, db, qmat, cmat, ncols, st);
+  else if (ncols <= 8) scan_dispatch<8>(P, s, db, qmat, cmat, ncols, st);
+  else scan_dispatch<16>(P, s, db, qmat, cmat, ncols, st);
+}
+
+void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cmat, uint32_t *mid,
+                          uint64_t mid_stride, uint32_t batch, cudaStream_t st) {
+  const size_t smem = 2 * kEpiTile * kN * sizeof(uint32_t);
+  set_smem(k_scan_epilogue, smem);
+  dim3 grid((s.other + kEpiTile - 1) / kEpiTile, 2, batch);
+  k_scan_epilogue<<<grid, kThreads, smem, st>>>(P, s, cmat, 2 * batch, mid, mid_stride);
+  check_launch("k_scan_epilogue");
+}
+
+void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, const uint32_t *in,
+                      uint32_t *out, uint64_t mid_stride, const uint32_t *sel, uint32_t batch,
+                      cudaStream_t st) {
+  const uint32_t h = s.num_dims - 1;
+  uint32_t n_pairs, offset = 0, half = 0, copies = 0;
+  if (level == 0) {
+    const uint32_t last = 2 * s.other - (1u << h);
+    offset = s.other - last;
+    n_pairs = last / 2;
+    copies = offset;
+  } else {
+    half = (1u << (h - level)) >> 1;
+    n_pairs = half;
+  }
+  const size_t smem = s.l_ep * kN * sizeof(uint32_t);
+  set_smem(k_mux_level, smem);
+  dim3 grid(n_pairs + copies, 2, batch);
+  k_mux_level<<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,
+                                             mid_stride, sel);
+  check_launch("k_mux_level");
+}
+
+void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride, uint64_t *resp,
+                      uint8_t *bytes, uint32_t resp_bytes, uint32_t batch, cudaStream_t st) {
+  k_modswitch<<<batch, kThreads, 0, st>>>(P, ct, ct_stride, resp, bytes, resp_bytes);
+  check_launch("k_modswitch");
+}
+
+}  // namespace opir

@@ -1,0 +1,100 @@
+// Host-callable launchers for the sm_100a kernels of the OnionPIRv2 server
+// path. All launches are asynchronous on the given stream.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "opir_device.cuh"
+
+namespace opir {
+
+// Shape of one make_query call (derived from PirParams).
+struct Shape {
+  uint32_t n0;          // fst_dim_sz
+  uint32_t other;       // other_dim_sz
+  uint32_t num_dims;
+  uint32_t h;           // expansion height
+  uint32_t useful;      // n0 + l_ep (num_dims - 1)
+  uint32_t l_ep, l_key, l_ks;
+  uint32_t base_ep, base_key, base_ks;
+  uint64_t num_pt;
+};
+
+// Number of heap nodes processed at expansion level d (nodes whose leftmost
+// leaf is below `useful`, src/server.cpp:786-792).
+inline uint32_t expand_nodes(const Shape &s, uint32_t d) {
+  const uint64_t span = 1ull << (s.h - d);
+  return static_cast<uint32_t>((s.useful + span - 1) / span);
+}
+
+// u64 (mod q) arrays -> residue pairs. in: n_items x per_item polys x N u64
+// (contiguous); out: item i at out + i * out_item_stride u32 words, each item
+// per_item x 2 x N u32.
+void launch_split_u64(const DevParams &P, const uint64_t *in, uint32_t *out,
+                      uint64_t n_items, uint64_t per_item, uint64_t out_item_stride,
+                      cudaStream_t st);
+// residue pairs -> u64 (mod q); the inverse of launch_split_u64.
+void launch_compose_u64(const DevParams &P, const uint32_t *in, uint64_t in_item_stride,
+                        uint64_t *out, uint64_t n_items, uint64_t per_item,
+                        cudaStream_t st);
+
+// Database preprocessing (src/server.cpp:80-171): plaintexts [pt][N] (u16,
+// or generated from `seed` when coeffs == nullptr) -> NTT -> residues ->
+// db[res][coeff][pt]. Covers plaintexts [pt_begin, pt_end) of a database of
+// num_pt plaintexts; rows >= logical are zero.
+void launch_db_preprocess(const DevParams &P, const uint16_t *coeffs,
+                          uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
+                          uint64_t logical, uint64_t num_pt, uint64_t pt_begin,
+                          uint64_t pt_end, uint32_t *db, cudaStream_t st);
+
+// One expansion level d over `batch` queries. in: batch x in_stride cts,
+// out: batch x out_stride cts. bv_level[b] points at the (galois level d) key
+// block of query b: L_KS x [b|a] x 2 residues x N u32, NTT form.
+void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d,
+                         const uint32_t *in, uint64_t in_stride, uint32_t *out,
+                         uint64_t out_stride, const uint32_t *const *bv_keys,
+                         uint64_t bv_level_stride, uint32_t batch, cudaStream_t st);
+
+// Selector completion (src/server.cpp:823-855, src/gsw.cpp:317-357).
+// leaves: batch x leaf_stride cts; gsw[b]: 2 L_KEY rows x 2 polys x 2 res x N;
+// sel: batch x (num_dims-1) x 2 L_EP rows x 2 x 2 x N (NTT form).
+void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves,
+                      uint64_t leaf_stride, const uint32_t *const *gsw_keys,
+                      uint32_t *sel, uint32_t batch, cudaStream_t st);
+
+// First-dimension query matrix (src/server.cpp:332-346 + 264-304): NTT of the
+// first n0 leaves of each query, written as qmat[res][level][k][2*batch].
+void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
+                     uint64_t leaf_stride, uint32_t *qmat, uint32_t batch,
+                     cudaStream_t st);
+
+// First-dimension scan (matrix.cpp:240-350): per residue and NTT level,
+// C[res][l][r][c] = sum_k db[res][l][r*n0 + k] * qmat[res][l][k][c] mod q_res,
+// c < 2*batch.
+void launch_scan(const DevParams &P, const Shape &s, const uint32_t *db,
+                 const uint32_t *qmat, uint32_t *cmat, uint32_t batch,
+                 cudaStream_t st);
+
+// Gather + INTT of the scan output into candidate ciphertexts
+// (src/server.cpp:529-597). mid: batch x mid_stride cts (coefficient form).
+void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cmat,
+                          uint32_t *mid, uint64_t mid_stride, uint32_t batch,
+                          cudaStream_t st);
+
+// One MUX level of evaluate_other_dim (src/server.cpp:599-722).
+// level 0: pairs (offset + 2i, offset + 2i + 1) -> out[offset + i], and
+//          out[0, offset) = in[0, offset);
+// level a >= 1: pairs (i, i + half) -> out[i], i < half.
+void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level,
+                      const uint32_t *in, uint32_t *out, uint64_t mid_stride,
+                      const uint32_t *sel, uint32_t batch, cudaStream_t st);
+
+// Modulus switch (src/server.cpp:1025-1043) + response bit packing
+// (src/server.cpp:950-1009). ct: batch x ct_stride cts; resp: batch x 2N u64;
+// bytes: batch x resp_bytes (may be nullptr).
+void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride,
+                      uint64_t *resp, uint8_t *bytes, uint32_t resp_bytes,
+                      uint32_t batch, cudaStream_t st);
+
+}  // namespace opir

@@ -1,0 +1,32 @@
+// Host-side parameter derivation for CONFIG_N2048_K1_COMP: primes, roots,
+// gadget bases, database shape, NTT twiddle tables for the two CRT limbs.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/onionpir_b200.h"
+
+namespace opir {
+
+bool is_prime_u64(uint64_t n);
+uint64_t generate_prime(uint32_t bit_width);
+std::vector<uint64_t> ntt_friendly_primes(const std::vector<uint32_t> &bit_widths,
+                                          uint32_t n);
+uint64_t min_primitive_root(uint64_t degree, uint64_t q);
+bool invert_mod(uint64_t v, uint64_t m, uint64_t &out);
+// {fst_dim_sz, num_dims}; throws std::invalid_argument / std::runtime_error.
+std::pair<uint64_t, uint64_t> calc_db_shape(uint64_t target, uint64_t l, uint32_t h,
+                                            bool pow2);
+// PirParams().with_layout(layout); throws like the reference.
+opir_params derive_params(const opir_layout &layout);
+
+// Per-limb NTT tables (u32 values and Shoup companions).
+struct LimbTables {
+  uint32_t q = 0, n_inv = 0, n_inv_sh = 0;
+  uint64_t mu = 0;
+  std::vector<uint32_t> fw, fw_sh, iw, iw_sh;
+};
+LimbTables make_limb_tables(uint32_t n, uint32_t q, uint32_t root);
+
+}  // namespace opir

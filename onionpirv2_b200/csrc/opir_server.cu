@@ -1,0 +1,720 @@
+// C-ABI implementation: the server handle that replaces PirServer's query
+// path (src/server.cpp). Host code orchestrates the sm_100a kernels of
+// opir_kernels.cu on one CUDA stream per handle; there is no CPU compute
+// path -- every arithmetic step of make_query runs in a kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/onionpir_b200.h"
+#include "opir_kernels.h"
+#include "opir_params.h"
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    reset();
+    if (count == 0) return;
+    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      throw std::bad_alloc();
+    }
+    n = count;
+  }
+};
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) ck(cudaSetDevice(dev), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+struct ClientKeys {
+  DevBuf<uint32_t> bv;   // h x L_KS x 2 polys x 2 residues x N
+  DevBuf<uint32_t> gsw;  // 2 L_KEY x 2 polys x 2 residues x N
+};
+
+constexpr int kStages = 5;
+
+}  // namespace
+
+struct opir_server {
+  opir_params params{};
+  opir::Shape shape{};
+  opir::DevParams dp{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf<uint32_t> tables;
+  DevBuf<uint32_t> db;
+  bool db_loaded = false;
+  std::unordered_map<uint64_t, ClientKeys> clients;
+  std::string last_error;
+  // scratch arena (sized for `cap` queries)
+  uint32_t cap = 0;
+  uint64_t lvl_slots = 1;   // ciphertext slots per query in an expansion buffer
+  DevBuf<uint64_t> q_u64, resp_u64;
+  DevBuf<uint8_t> resp_bytes;
+  DevBuf<uint32_t> lvl[2], sel, qmat, cmat, mid[2];
+  DevBuf<const uint32_t *> keyptrs;
+  std::vector<const uint32_t *> host_keyptrs;
+  // stage timing
+  bool timing = false;
+  cudaEvent_t ev[kStages + 1] = {};
+  float stage_ms[kStages] = {0, 0, 0, 0, 0};
+};
+
+namespace {
+
+using opir::kCtWords;
+using opir::kN;
+
+opir_status fail(opir_server *s, opir_status code, const std::string &msg) {
+  if (s) s->last_error = msg;
+  return code;
+}
+
+template <typename F>
+opir_status guarded(opir_server *s, F &&f) {
+  try {
+    f();
+    if (s) s->last_error.clear();
+    return OPIR_OK;
+  } catch (const std::invalid_argument &e) {
+    return fail(s, OPIR_ERR_INVALID_ARGUMENT, e.what());
+  } catch (const std::out_of_range &e) {
+    return fail(s, OPIR_ERR_OUT_OF_RANGE, e.what());
+  } catch (const std::overflow_error &e) {
+    return fail(s, OPIR_ERR_OVERFLOW, e.what());
+  } catch (const std::bad_alloc &) {
+    return fail(s, OPIR_ERR_NO_MEMORY, "device or host allocation failed");
+  } catch (const CudaError &e) {
+    cudaGetLastError();
+    return fail(s, OPIR_ERR_CUDA, e.what());
+  } catch (const std::runtime_error &e) {
+    cudaGetLastError();
+    return fail(s, OPIR_ERR_RUNTIME, e.what());
+  } catch (...) {
+    return fail(s, OPIR_ERR_RUNTIME, "unknown error");
+  }
+}
+
+uint32_t resp_bytes_of(const opir_params &p) {
+  return static_cast<uint32_t>((2ull * p.poly_degree * p.small_q_width + 7) / 8);
+}
+
+void setup_device_params(opir_server *s) {
+  const opir_params &p = s->params;
+  const auto t1 = opir::make_limb_tables(kN, static_cast<uint32_t>(p.q1), static_cast<uint32_t>(p.w1));
+  const auto t2 = opir::make_limb_tables(kN, static_cast<uint32_t>(p.q2), static_cast<uint32_t>(p.w2));
+  std::vector<uint32_t> host(8 * kN);
+  const opir::LimbTables *ts[2] = {&t1, &t2};
+  for (int r = 0; r < 2; ++r) {
+    std::copy(ts[r]->fw.begin(), ts[r]->fw.end(), host.begin() + (r * 4 + 0) * kN);
+    std::copy(ts[r]->fw_sh.begin(), ts[r]->fw_sh.end(), host.begin() + (r * 4 + 1) * kN);
+    std::copy(ts[r]->iw.begin(), ts[r]->iw.end(), host.begin() + (r * 4 + 2) * kN);
+    std::copy(ts[r]->iw_sh.begin(), ts[r]->iw_sh.end(), host.begin() + (r * 4 + 3) * kN);
+  }
+  s->tables.alloc(host.size());
+  ck(cudaMemcpy(s->tables.p, host.data(), host.size() * 4, cudaMemcpyHostToDevice), "tables");
+  opir::DevParams &d = s->dp;
+  for (int r = 0; r < 2; ++r) {
+    d.r[r].fw = s->tables.p + (r * 4 + 0) * kN;
+    d.r[r].fw_sh = s->tables.p + (r * 4 + 1) * kN;
+    d.r[r].iw = s->tables.p + (r * 4 + 2) * kN;
+    d.r[r].iw_sh = s->tables.p + (r * 4 + 3) * kN;
+    d.r[r].q = ts[r]->q;
+    d.r[r].n_inv = ts[r]->n_inv;
+    d.r[r].n_inv_sh = ts[r]->n_inv_sh;
+    d.r[r].mu = ts[r]->mu;
+  }
+  d.q = p.q;
+  d.half_q = p.q >> 1;
+  d.q1 = static_cast<uint32_t>(p.q1);
+  d.q2 = static_cast<uint32_t>(p.q2);
+  d.q1_inv = static_cast<uint32_t>(p.q1_inv_mod_q2);
+  d.q1_inv_sh = static_cast<uint32_t>((static_cast<uint64_t>(d.q1_inv) << 32) / d.q2);
+  d.small_q = p.small_q;
+  d.small_q_width = p.small_q_width;
+
+  opir::Shape &sh = s->shape;
+  sh.n0 = static_cast<uint32_t>(p.fst_dim_sz);
+  sh.other = static_cast<uint32_t>(p.other_dim_sz);
+  sh.num_dims = p.num_dims;
+  sh.h = p.expansion_height;
+  sh.useful = static_cast<uint32_t>(p.fst_dim_sz + static_cast<uint64_t>(p.l_ep) * (p.num_dims - 1));
+  sh.l_ep = p.l_ep;
+  sh.l_key = p.l_key;
+  sh.l_ks = p.l_ks;
+  sh.base_ep = p.base_log2;
+  sh.base_key = p.base_log2_key;
+  sh.base_ks = p.base_log2_ks;
+  sh.num_pt = p.num_pt;
+  uint64_t slots = 1;
+  for (uint32_t d2 = 0; d2 < sh.h; ++d2) slots = std::max<uint64_t>(slots, 2ull * opir::expand_nodes(sh, d2));
+  s->lvl_slots = std::max<uint64_t>(slots, sh.useful);
+}
+
+void ensure_capacity(opir_server *s, uint32_t n) {
+  if (n <= s->cap) return;
+  const opir::Shape &sh = s->shape;
+  const uint64_t ct = kCtWords;
+  const uint64_t nsel = sh.num_dims > 1 ? sh.num_dims - 1 : 0;
+  s->q_u64.alloc(static_cast<size_t>(n) * 2 * kN);
+  s->resp_u64.alloc(static_cast<size_t>(n) * 2 * kN);
+  s->resp_bytes.alloc(static_cast<size_t>(n) * resp_bytes_of(s->params));
+  for (auto &b : s->lvl) b.alloc(n * s->lvl_slots * ct);
+  s->sel.alloc(std::max<uint64_t>(1, n * nsel * 2 * sh.l_ep * ct));
+  s->qmat.alloc(2ull * kN * sh.n0 * 2 * n);
+  s->cmat.alloc(2ull * kN * sh.other * 2 * n);
+  for (auto &b : s->mid) b.alloc(static_cast<size_t>(n) * sh.other * ct);
+  s->keyptrs.alloc(2ull * n);
+  s->cap = n;
+}
+
+const ClientKeys &client(const opir_server *s, uint64_t id) {
+  auto it = s->clients.find(id);
+  if (it == s->clients.end()) throw std::out_of_range("unknown client id " + std::to_string(id));
+  return it->second;
+}
+
+// Uploads the per-query key pointer table (bv pointers then gsw pointers).
+void upload_keyptrs(opir_server *s, const uint64_t *client_ids, uint32_t n) {
+  s->host_keyptrs.resize(2ull * n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const ClientKeys &k = client(s, client_ids[i]);
+    s->host_keyptrs[i] = k.bv.p;
+    s->host_keyptrs[n + i] = k.gsw.p;
+  }
+  ck(cudaMemcpyAsync(s->keyptrs.p, s->host_keyptrs.data(), 2ull * n * sizeof(void *),
+                     cudaMemcpyHostToDevice, s->stream), "key pointers");
+}
+
+void mark(opir_server *s, int i) {
+  if (s->timing) ck(cudaEventRecord(s->ev[i], s->stream), "cudaEventRecord");
+}
+
+// Expansion (Algorithm 2) over n queries whose residue pairs sit in slot 0 of
+// lvl[0]; returns the buffer holding the leaves.
+uint32_t *run_expand(opir_server *s, uint32_t n) {
+  const opir::Shape &sh = s->shape;
+  const uint64_t bv_level_stride = static_cast<uint64_t>(sh.l_ks) * 4 * kN;
+  for (uint32_t d = 0; d < sh.h; ++d)
+    opir::launch_expand_level(s->dp, sh, d, s->lvl[d & 1].p, s->lvl_slots, s->lvl[(d + 1) & 1].p,
+                              s->lvl_slots, s->keyptrs.p, bv_level_stride, n, s->stream);
+  return s->lvl[sh.h & 1].p;
+}
+
+// First dimension: NTT + transpose of the first n0 leaves, scan, gather + INTT.
+void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n) {
+  const opir::Shape &sh = s->shape;
+  opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, s->qmat.p, n, s->stream);
+  opir::launch_scan(s->dp, sh, s->db.p, s->qmat.p, s->cmat.p, n, s->stream);
+  opir::launch_scan_epilogue(s->dp, sh, s->cmat.p, s->mid[0].p, sh.other, n, s->stream);
+}
+
+// Remaining dimensions: returns the buffer whose slot 0 holds the result.
+uint32_t *run_other_dims(opir_server *s, uint32_t n) {
+  const opir::Shape &sh = s->shape;
+  if (sh.num_dims <= 1) return s->mid[0].p;
+  const uint32_t levels = sh.num_dims - 1;
+  for (uint32_t a = 0; a < levels; ++a)
+    opir::launch_mux_level(s->dp, sh, a, s->mid[a & 1].p, s->mid[(a + 1) & 1].p, sh.other,
+                           s->sel.p, n, s->stream);
+  return s->mid[levels & 1].p;
+}
+
+void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
+                  const uint64_t *d_queries, uint64_t *d_resp, uint8_t *d_bytes) {
+  if (!s->db_loaded) throw std::runtime_error("make_query before load_data");
+  if (n == 0) return;
+  ensure_capacity(s, n);
+  upload_keyptrs(s, client_ids, n);
+  const opir::Shape &sh = s->shape;
+  mark(s, 0);
+  opir::launch_split_u64(s->dp, d_queries, s->lvl[0].p, n, 2, s->lvl_slots * kCtWords, s->stream);
+  const uint32_t *leaves = run_expand(s, n);
+  mark(s, 1);
+  opir::launch_selectors(s->dp, sh, leaves, s->lvl_slots, s->keyptrs.p + n, s->sel.p, n, s->stream);
+  mark(s, 2);
+  run_first_dim(s, leaves, n);
+  mark(s, 3);
+  const uint32_t *res = run_other_dims(s, n);
+  mark(s, 4);
+  opir::launch_modswitch(s->dp, res, sh.other, d_resp, d_bytes, resp_bytes_of(s->params), n,
+                         s->stream);
+  mark(s, 5);
+}
+
+void finish(opir_server *s) {
+  ck(cudaStreamSynchronize(s->stream), "make_query");
+  if (s->timing)
+    for (int i = 0; i < kStages; ++i)
+      ck(cudaEventElapsedTime(&s->stage_ms[i], s->ev[i], s->ev[i + 1]), "cudaEventElapsedTime");
+}
+
+void check_query_values(const opir_server *s, const uint64_t *q, size_t count) {
+  for (size_t i = 0; i < count; ++i)
+    if (q[i] >= s->params.q) throw std::invalid_argument("query coefficient not reduced mod q");
+}
+
+// Database upload in tiles of plaintexts (u16 coefficients).
+template <typename Fill>
+void load_tiles(opir_server *s, uint64_t logical, Fill &&fill) {
+  const opir_params &p = s->params;
+  if (logical > p.num_pt)
+    throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
+  const uint64_t tile = 16384;
+  std::vector<uint16_t> host(tile * kN);
+  DevBuf<uint16_t> dev;
+  dev.alloc(tile * kN);
+  s->db_loaded = false;
+  for (uint64_t pb = 0; pb < p.num_pt; pb += tile) {
+    const uint64_t pe = std::min<uint64_t>(p.num_pt, pb + tile);
+    const uint64_t real_end = std::min<uint64_t>(pe, logical);
+    if (pb < real_end) {
+      fill(pb, real_end, host.data());
+      ck(cudaMemcpyAsync(dev.p, host.data(), (real_end - pb) * kN * 2, cudaMemcpyHostToDevice,
+                         s->stream), "db upload");
+    }
+    opir::launch_db_preprocess(s->dp, dev.p, pb, 0, p.plain_mod, logical, p.num_pt, pb, pe,
+                               s->db.p, s->stream);
+    ck(cudaStreamSynchronize(s->stream), "db preprocess");
+  }
+  s->db_loaded = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *opir_version(void) { return "onionpir_b200 0.1 (sm_100a)"; }
+
+opir_status opir_params_init(const opir_layout *layout, opir_params *out) {
+  if (!layout || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] { *out = opir::derive_params(*layout); });
+}
+
+size_t opir_response_bytes(const opir_params *params) {
+  return params ? resp_bytes_of(*params) : 0;
+}
+
+opir_status opir_server_create(const opir_params *params, int device, opir_server **out) {
+  if (!params || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  opir_server *s = new (std::nothrow) opir_server();
+  if (!s) return OPIR_ERR_NO_MEMORY;
+  const opir_status st = guarded(s, [&] {
+    if (params->poly_degree != static_cast<uint32_t>(kN) || params->num_limbs != 1)
+      throw std::invalid_argument("only CONFIG_N2048_K1_COMP parameters are supported");
+    opir_layout lay{params->target_num_pt, params->expansion_height, params->fst_dim_pow2};
+    const opir_params check = opir::derive_params(lay);
+    if (check.num_pt != params->num_pt || check.q != params->q)
+      throw std::invalid_argument("params do not match their layout");
+    s->params = check;
+    s->device = device;
+    DeviceGuard g(device);
+    ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto &e : s->ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+    setup_device_params(s);
+    s->db.alloc(2ull * kN * s->params.num_pt);
+    ck(cudaMemsetAsync(s->db.p, 0, 2ull * kN * s->params.num_pt * 4, s->stream), "db memset");
+    ck(cudaStreamSynchronize(s->stream), "create");
+  });
+  if (st != OPIR_OK) {
+    opir_server_destroy(s);
+    return st;
+  }
+  *out = s;
+  return OPIR_OK;
+}
+
+void opir_server_destroy(opir_server *s) {
+  if (!s) return;
+  {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    s->clients.clear();
+    s->tables.reset();
+    s->db.reset();
+    s->q_u64.reset();
+    s->resp_u64.reset();
+    s->resp_bytes.reset();
+    for (auto &b : s->lvl) b.reset();
+    s->sel.reset();
+    s->qmat.reset();
+    s->cmat.reset();
+    for (auto &b : s->mid) b.reset();
+    s->keyptrs.reset();
+    for (auto &e : s->ev)
+      if (e) cudaEventDestroy(e);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  delete s;
+}
+
+const char *opir_server_last_error(const opir_server *s) {
+  return s ? s->last_error.c_str() : "null server handle";
+}
+
+opir_status opir_server_params(const opir_server *s, opir_params *out) {
+  if (!s || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  *out = s->params;
+  return OPIR_OK;
+}
+
+opir_status opir_server_load_db_u16(opir_server *s, uint64_t logical, const uint16_t *coeffs) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
+    DeviceGuard g(s->device);
+    const uint64_t t = s->params.plain_mod;
+    load_tiles(s, logical, [&](uint64_t b, uint64_t e, uint16_t *dst) {
+      const uint16_t *src = coeffs + b * kN;
+      for (uint64_t i = 0; i < (e - b) * kN; ++i) {
+        if (src[i] >= t)
+          throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
+        dst[i] = src[i];
+      }
+    });
+  });
+}
+
+opir_status opir_server_load_db(opir_server *s, uint64_t logical, const uint64_t *coeffs) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
+    DeviceGuard g(s->device);
+    const uint64_t t = s->params.plain_mod;
+    load_tiles(s, logical, [&](uint64_t b, uint64_t e, uint16_t *dst) {
+      const uint64_t *src = coeffs + b * kN;
+      for (uint64_t i = 0; i < (e - b) * kN; ++i) {
+        if (src[i] >= t)
+          throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
+        dst[i] = static_cast<uint16_t>(src[i]);
+      }
+    });
+  });
+}
+
+opir_status opir_server_load_db_source(opir_server *s, uint64_t logical,
+                                       opir_plaintext_source source, void *user) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!source) throw std::invalid_argument("PirServer::load_data requires a source");
+    DeviceGuard g(s->device);
+    const uint64_t t = s->params.plain_mod;
+    std::vector<uint64_t> pt(kN);
+    load_tiles(s, logical, [&](uint64_t b, uint64_t e, uint16_t *dst) {
+      for (uint64_t idx = b; idx < e; ++idx) {
+        if (source(user, idx, pt.data()) != 0)
+          throw std::invalid_argument("Plaintext source failed");
+        for (int c = 0; c < kN; ++c) {
+          if (pt[c] >= t)
+            throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
+          dst[(idx - b) * kN + c] = static_cast<uint16_t>(pt[c]);
+        }
+      }
+    });
+  });
+}
+
+opir_status opir_server_load_db_seeded(opir_server *s, uint64_t logical, uint64_t seed) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    DeviceGuard g(s->device);
+    const opir_params &p = s->params;
+    if (logical > p.num_pt)
+      throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
+    s->db_loaded = false;
+    const uint64_t chunk = 1ull << 20;
+    for (uint64_t pb = 0; pb < p.num_pt; pb += chunk)
+      opir::launch_db_preprocess(s->dp, nullptr, 0, seed, p.plain_mod, logical, p.num_pt, pb,
+                                 std::min<uint64_t>(p.num_pt, pb + chunk), s->db.p, s->stream);
+    ck(cudaStreamSynchronize(s->stream), "db preprocess");
+    s->db_loaded = true;
+  });
+}
+
+opir_status opir_server_set_client_keys(opir_server *s, uint64_t client_id,
+                                        const uint64_t *bv_keys, const uint32_t *galois_ks,
+                                        uint32_t n_keys, const uint64_t *gsw_key) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    const opir_params &p = s->params;
+    const uint32_t h = p.expansion_height;
+    if (!gsw_key) throw std::invalid_argument("PirServer session key bundle cannot be null");
+    if (n_keys < h) throw std::invalid_argument("PirServer session lacks keys for its expansion height");
+    if (n_keys && (!bv_keys || !galois_ks)) throw std::invalid_argument("null BV key arrays");
+    const size_t key_words = static_cast<size_t>(p.l_ks) * 2 * kN;  // one BvKeySwitchKey, u64
+    std::vector<uint64_t> ordered(static_cast<size_t>(h) * key_words);
+    for (uint32_t d = 0; d < h; ++d) {
+      const uint32_t want = kN / (1u << d) + 1;
+      int found = -1;
+      for (uint32_t i = 0; i < n_keys; ++i)
+        if (galois_ks[i] == want) { found = static_cast<int>(i); break; }
+      if (found < 0) throw std::out_of_range("BvGaloisKeys::get: galois_k not found");
+      std::memcpy(ordered.data() + d * key_words, bv_keys + found * key_words, key_words * 8);
+    }
+    const size_t gsw_words = static_cast<size_t>(2) * p.l_key * 2 * kN;
+    for (uint64_t v : ordered)
+      if (v >= p.q) throw std::invalid_argument("BV key value not reduced mod q");
+    for (size_t i = 0; i < gsw_words; ++i)
+      if (gsw_key[i] >= p.q) throw std::invalid_argument("RGSW key value not reduced mod q");
+    DeviceGuard g(s->device);
+    ClientKeys k;
+    DevBuf<uint64_t> tmp;
+    tmp.alloc(std::max(ordered.size(), gsw_words));
+    k.bv.alloc(std::max<size_t>(1, ordered.size() * 2));
+    k.gsw.alloc(gsw_words * 2);
+    if (!ordered.empty()) {
+      ck(cudaMemcpyAsync(tmp.p, ordered.data(), ordered.size() * 8, cudaMemcpyHostToDevice, s->stream), "bv upload");
+      opir::launch_split_u64(s->dp, tmp.p, k.bv.p, 1, ordered.size() / kN, 0, s->stream);
+      ck(cudaStreamSynchronize(s->stream), "bv split");
+    }
+    ck(cudaMemcpyAsync(tmp.p, gsw_key, gsw_words * 8, cudaMemcpyHostToDevice, s->stream), "gsw upload");
+    opir::launch_split_u64(s->dp, tmp.p, k.gsw.p, 1, gsw_words / kN, 0, s->stream);
+    ck(cudaStreamSynchronize(s->stream), "gsw split");
+    ClientKeys &slot = s->clients[client_id];
+    std::swap(slot.bv.p, k.bv.p); std::swap(slot.bv.n, k.bv.n);
+    std::swap(slot.gsw.p, k.gsw.p); std::swap(slot.gsw.n, k.gsw.n);
+  });
+}
+
+opir_status opir_server_remove_client(opir_server *s, uint64_t client_id) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    DeviceGuard g(s->device);
+    ck(cudaStreamSynchronize(s->stream), "remove_client");
+    if (s->clients.erase(client_id) == 0) throw std::out_of_range("unknown client id");
+  });
+}
+
+opir_status opir_server_make_query_batch(opir_server *s, uint32_t n, const uint64_t *client_ids,
+                                         const uint64_t *queries, uint64_t *responses) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (n && (!client_ids || !queries || !responses)) throw std::invalid_argument("null argument");
+    check_query_values(s, queries, static_cast<size_t>(n) * 2 * kN);
+    DeviceGuard g(s->device);
+    ensure_capacity(s, n);
+    ck(cudaMemcpyAsync(s->q_u64.p, queries, static_cast<size_t>(n) * 2 * kN * 8,
+                       cudaMemcpyHostToDevice, s->stream), "query upload");
+    run_pipeline(s, client_ids, n, s->q_u64.p, s->resp_u64.p, nullptr);
+    ck(cudaMemcpyAsync(responses, s->resp_u64.p, static_cast<size_t>(n) * 2 * kN * 8,
+                       cudaMemcpyDeviceToHost, s->stream), "response download");
+    finish(s);
+  });
+}
+
+opir_status opir_server_make_query(opir_server *s, uint64_t client_id, const uint64_t *query,
+                                   uint64_t *response) {
+  return opir_server_make_query_batch(s, 1, &client_id, query, response);
+}
+
+opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
+                                                const uint64_t *client_ids,
+                                                const uint64_t *d_queries, uint64_t *d_responses,
+                                                void *stream) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (n && (!client_ids || !d_queries || !d_responses)) throw std::invalid_argument("null argument");
+    DeviceGuard g(s->device);
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    if (user) {  // order after the caller's prior work on its stream
+      cudaEvent_t e;
+      ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      ck(cudaEventRecord(e, user), "event record");
+      ck(cudaStreamWaitEvent(s->stream, e, 0), "wait");
+      cudaEventDestroy(e);
+    }
+    run_pipeline(s, client_ids, n, d_queries, d_responses, nullptr);
+    if (user) {
+      cudaEvent_t e;
+      ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      ck(cudaEventRecord(e, s->stream), "event record");
+      ck(cudaStreamWaitEvent(user, e, 0), "wait");
+      cudaEventDestroy(e);
+    }
+  });
+}
+
+opir_status opir_server_set_stage_timing(opir_server *s, int enabled) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  s->timing = enabled != 0;
+  return OPIR_OK;
+}
+
+opir_status opir_server_stage_times(const opir_server *s, float *ms_out) {
+  if (!s || !ms_out) return OPIR_ERR_INVALID_ARGUMENT;
+  std::memcpy(ms_out, s->stage_ms, sizeof(s->stage_ms));
+  return OPIR_OK;
+}
+
+opir_status opir_server_expand_query(opir_server *s, uint64_t client_id, const uint64_t *query,
+                                     uint64_t *out) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!query || !out) throw std::invalid_argument("null argument");
+    check_query_values(s, query, 2 * kN);
+    DeviceGuard g(s->device);
+    ensure_capacity(s, 1);
+    upload_keyptrs(s, &client_id, 1);
+    ck(cudaMemcpyAsync(s->q_u64.p, query, 2 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    opir::launch_split_u64(s->dp, s->q_u64.p, s->lvl[0].p, 1, 2, 0, s->stream);
+    const uint32_t *leaves = run_expand(s, 1);
+    DevBuf<uint64_t> o;
+    o.alloc(static_cast<size_t>(s->shape.useful) * 2 * kN);
+    opir::launch_compose_u64(s->dp, leaves, 0, o.p, 1, 2ull * s->shape.useful, s->stream);
+    ck(cudaMemcpyAsync(out, o.p, o.n * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    ck(cudaStreamSynchronize(s->stream), "expand_query");
+  });
+}
+
+opir_status opir_server_complete_selectors(opir_server *s, uint64_t client_id,
+                                           const uint64_t *expanded, uint64_t *out) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!expanded || !out) throw std::invalid_argument("null argument");
+    const opir::Shape &sh = s->shape;
+    check_query_values(s, expanded, static_cast<size_t>(sh.useful) * 2 * kN);
+    DeviceGuard g(s->device);
+    ensure_capacity(s, 1);
+    upload_keyptrs(s, &client_id, 1);
+    const uint32_t nsel = sh.num_dims - 1;
+    if (nsel == 0) return;
+    DevBuf<uint64_t> in;
+    in.alloc(static_cast<size_t>(sh.useful) * 2 * kN);
+    ck(cudaMemcpyAsync(in.p, expanded, in.n * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    opir::launch_split_u64(s->dp, in.p, s->lvl[0].p, 1, 2ull * sh.useful, 0, s->stream);
+    opir::launch_selectors(s->dp, sh, s->lvl[0].p, s->lvl_slots, s->keyptrs.p + 1, s->sel.p, 1,
+                           s->stream);
+    const uint64_t polys = 2ull * nsel * 2 * sh.l_ep;
+    DevBuf<uint64_t> o;
+    o.alloc(polys * kN);
+    opir::launch_compose_u64(s->dp, s->sel.p, 0, o.p, 1, polys, s->stream);
+    ck(cudaMemcpyAsync(out, o.p, o.n * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    ck(cudaStreamSynchronize(s->stream), "complete_selectors");
+  });
+}
+
+opir_status opir_server_evaluate_first_dim(opir_server *s, const uint64_t *fst_query, uint64_t *out) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!fst_query || !out) throw std::invalid_argument("null argument");
+    if (!s->db_loaded) throw std::runtime_error("evaluate_first_dim before load_data");
+    const opir::Shape &sh = s->shape;
+    check_query_values(s, fst_query, static_cast<size_t>(sh.n0) * 2 * kN);
+    DeviceGuard g(s->device);
+    ensure_capacity(s, 1);
+    DevBuf<uint64_t> in;
+    in.alloc(static_cast<size_t>(sh.n0) * 2 * kN);
+    ck(cudaMemcpyAsync(in.p, fst_query, in.n * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    opir::launch_split_u64(s->dp, in.p, s->lvl[0].p, 1, 2ull * sh.n0, 0, s->stream);
+    run_first_dim(s, s->lvl[0].p, 1);
+    DevBuf<uint64_t> o;
+    o.alloc(static_cast<size_t>(sh.other) * 2 * kN);
+    opir::launch_compose_u64(s->dp, s->mid[0].p, 0, o.p, 1, 2ull * sh.other, s->stream);
+    ck(cudaMemcpyAsync(out, o.p, o.n * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    ck(cudaStreamSynchronize(s->stream), "evaluate_first_dim");
+  });
+}
+
+opir_status opir_server_evaluate_other_dim(opir_server *s, const uint64_t *mid,
+                                           const uint64_t *selectors, uint64_t *out) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    const opir::Shape &sh = s->shape;
+    const uint32_t nsel = sh.num_dims - 1;
+    if (!mid || !out || (nsel && !selectors)) throw std::invalid_argument("null argument");
+    if (nsel && sh.other < (1u << (nsel - 1)))
+      throw std::invalid_argument("evaluate_other_dim: layout has fewer candidates than its selector tree");
+    check_query_values(s, mid, static_cast<size_t>(sh.other) * 2 * kN);
+    DeviceGuard g(s->device);
+    ensure_capacity(s, 1);
+    DevBuf<uint64_t> in;
+    const uint64_t sel_polys = 2ull * nsel * 2 * sh.l_ep;
+    in.alloc(std::max<uint64_t>(static_cast<uint64_t>(sh.other) * 2, sel_polys) * kN);
+    ck(cudaMemcpyAsync(in.p, mid, static_cast<size_t>(sh.other) * 2 * kN * 8,
+                       cudaMemcpyHostToDevice, s->stream), "upload");
+    opir::launch_split_u64(s->dp, in.p, s->mid[0].p, 1, 2ull * sh.other, 0, s->stream);
+    if (nsel) {
+      ck(cudaStreamSynchronize(s->stream), "upload");
+      ck(cudaMemcpyAsync(in.p, selectors, sel_polys * kN * 8, cudaMemcpyHostToDevice, s->stream),
+         "upload");
+      opir::launch_split_u64(s->dp, in.p, s->sel.p, 1, sel_polys, 0, s->stream);
+    }
+    const uint32_t *r = run_other_dims(s, 1);
+    DevBuf<uint64_t> o;
+    o.alloc(2 * kN);
+    opir::launch_compose_u64(s->dp, r, 0, o.p, 1, 2, s->stream);
+    ck(cudaMemcpyAsync(out, o.p, 2 * kN * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    ck(cudaStreamSynchronize(s->stream), "evaluate_other_dim");
+  });
+}
+
+size_t opir_save_response(const opir_params *params, const uint64_t *resp, uint8_t *out,
+                          size_t cap) {
+  if (!params || !resp || !out) return 0;
+  const uint32_t w = params->small_q_width;
+  const size_t need = resp_bytes_of(*params);
+  if (cap < need) return 0;
+  uint8_t buf = 0;
+  uint32_t filled = 0;
+  size_t nb = 0;
+  for (uint32_t i = 0; i < 2 * params->poly_degree; ++i) {
+    const uint64_t c = resp[i] & ((1ull << w) - 1);
+    uint32_t written = 0;
+    while (written < w) {
+      const uint32_t room = 8 - filled;
+      const uint32_t take = std::min(room, w - written);
+      buf |= static_cast<uint8_t>(((c >> written) & ((1ull << take) - 1)) << filled);
+      filled += take;
+      written += take;
+      if (filled == 8) { out[nb++] = buf; buf = 0; filled = 0; }
+    }
+  }
+  if (filled) out[nb++] = buf;
+  return nb;
+}
+
+}  // extern "C"

@@ -1,0 +1,275 @@
+"""Python mirror of the reference's PirParams / PirServer interface over the
+C ABI (include/onionpir_b200.h).
+
+Names, argument meaning and error behaviour follow the reference
+(src/includes/pir.h, src/includes/server.h): invalid layouts and inputs raise
+ValueError (std::invalid_argument), unknown clients raise KeyError-compatible
+IndexError subclass OutOfRange (std::out_of_range), device failures raise
+RuntimeError. Ciphertexts are numpy uint64 arrays shaped (2, N) = (c0, c1).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, Iterable, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+OPIR_OK = 0
+OPIR_ERR_INVALID_ARGUMENT = 1
+OPIR_ERR_OUT_OF_RANGE = 2
+OPIR_ERR_RUNTIME = 3
+OPIR_ERR_CUDA = 4
+OPIR_ERR_NO_MEMORY = 5
+OPIR_ERR_OVERFLOW = 6
+
+
+class OutOfRange(IndexError, KeyError):
+    """std::out_of_range in the reference (unknown client, missing key)."""
+
+
+class DeviceError(RuntimeError):
+    """CUDA failure reported by the library."""
+
+
+def _raise(code: int, msg: str):
+    if code == OPIR_ERR_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    if code == OPIR_ERR_OUT_OF_RANGE:
+        raise OutOfRange(msg)
+    if code == OPIR_ERR_OVERFLOW:
+        raise OverflowError(msg)
+    if code == OPIR_ERR_NO_MEMORY:
+        raise MemoryError(msg)
+    if code == OPIR_ERR_CUDA:
+        raise DeviceError(msg)
+    raise RuntimeError(msg)
+
+
+def _ptr(a: np.ndarray, t=C.c_uint64):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class PirParams:
+    """PirParams().with_layout({target_num_pt, expansion_height, fst_dim_pow2})."""
+
+    def __init__(self, target_num_pt: int = 43690, expansion_height: int = 10,
+                 fst_dim_pow2: bool = True):
+        self._layout = L.Layout(target_num_pt, expansion_height, 1 if fst_dim_pow2 else 0)
+        self._p = L.Params()
+        rc = L.load().opir_params_init(C.byref(self._layout), C.byref(self._p))
+        if rc != OPIR_OK:
+            _raise(rc, f"invalid layout {target_num_pt}/{expansion_height}/{fst_dim_pow2}")
+
+    def with_layout(self, target_num_pt: int, expansion_height: int,
+                    fst_dim_pow2: bool = True) -> "PirParams":
+        return PirParams(target_num_pt, expansion_height, fst_dim_pow2)
+
+    def __getattr__(self, name):
+        p = self.__dict__.get("_p")
+        if p is not None and name in dict(L.Params._fields_):
+            return getattr(p, name)
+        raise AttributeError(name)
+
+    # getters named as in includes/pir.h
+    def get_num_pt(self): return self._p.num_pt
+    def get_fst_dim_sz(self): return self._p.fst_dim_sz
+    def get_other_dim_sz(self): return self._p.other_dim_sz
+    def get_num_dims(self): return self._p.num_dims
+    def get_expan_height(self): return self._p.expansion_height
+    def get_plain_mod(self): return self._p.plain_mod
+    def get_small_q(self): return self._p.small_q
+    def get_rns_mods(self): return [self._p.q]
+    def get_poly_degree(self): return self._p.poly_degree
+    def get_l(self): return self._p.l_ep
+    def get_l_key(self): return self._p.l_key
+    def get_target_num_pt(self): return self._p.target_num_pt
+
+    @property
+    def N(self) -> int:
+        return self._p.poly_degree
+
+    @property
+    def useful(self) -> int:
+        return self._p.fst_dim_sz + self._p.l_ep * (self._p.num_dims - 1)
+
+    def response_bytes(self) -> int:
+        return int(L.load().opir_response_bytes(C.byref(self._p)))
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self._p, f) for f, _ in L.Params._fields_ if f != "reserved"}
+
+
+class PirServer:
+    """Device-resident OnionPIRv2 server (PirServer, includes/server.h:15-172)."""
+
+    def __init__(self, params: PirParams, device: int = 0):
+        self.params = params
+        self._lib = L.load()
+        h = C.c_void_p()
+        rc = self._lib.opir_server_create(C.byref(params._p), device, C.byref(h))
+        if rc != OPIR_OK:
+            _raise(rc, f"opir_server_create failed (status {rc})")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.opir_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != OPIR_OK:
+            msg = self._lib.opir_server_last_error(self._h)
+            _raise(rc, msg.decode() if msg else f"status {rc}")
+
+    # ---- database
+    def load_data(self, logical_num_pt: int,
+                  source: Callable[[int], Sequence[int]] | np.ndarray):
+        """load_data(logical_num_pt, source): source is either an array
+        (logical_num_pt, N) of coefficients < t or a callable index -> N
+        coefficients (the reference's PlaintextSource)."""
+        N = self.params.N
+        if isinstance(source, np.ndarray):
+            arr = np.ascontiguousarray(source)
+            if arr.shape != (logical_num_pt, N):
+                raise ValueError("Plaintext source returned the wrong coefficient count")
+            if arr.dtype == np.uint16:
+                self._check(self._lib.opir_server_load_db_u16(self._h, logical_num_pt, _ptr(arr, C.c_uint16)))
+            else:
+                a64 = np.ascontiguousarray(arr, dtype=np.uint64)
+                self._check(self._lib.opir_server_load_db(self._h, logical_num_pt, _ptr(a64)))
+            return
+        err: list[BaseException] = []
+
+        def cb(_user, idx, out):
+            try:
+                vals = np.asarray(source(int(idx)), dtype=np.uint64)
+                if vals.shape != (N,):
+                    raise ValueError("Plaintext source returned the wrong coefficient count")
+                C.memmove(out, vals.ctypes.data, N * 8)
+                return 0
+            except BaseException as e:  # propagate after the C call returns
+                err.append(e)
+                return 1
+
+        cfun = L.SOURCE_CB(cb)
+        rc = self._lib.opir_server_load_db_source(self._h, logical_num_pt, cfun, None)
+        if err:
+            raise err[0]
+        self._check(rc)
+
+    def load_data_seeded(self, logical_num_pt: int, seed: int):
+        self._check(self._lib.opir_server_load_db_seeded(self._h, logical_num_pt, seed))
+
+    # ---- keys
+    def set_client_keys(self, client_id: int, bv_keys: np.ndarray, gsw_key: np.ndarray,
+                        galois_ks: Iterable[int] | None = None):
+        """set_client_bv_galois_key + set_client_gsw_key. bv_keys: (n_keys, L_KS,
+        2, N) NTT form [b, a]; galois_ks defaults to (N >> i) + 1."""
+        N = self.params.N
+        bv = np.ascontiguousarray(bv_keys, dtype=np.uint64)
+        n_keys = bv.shape[0] if bv.size else 0
+        if galois_ks is None:
+            galois_ks = [(N >> i) + 1 for i in range(n_keys)]
+        gk = np.ascontiguousarray(np.asarray(list(galois_ks), dtype=np.uint32))
+        if gk.size == 0:
+            gk = np.zeros(1, dtype=np.uint32)
+        if bv.size == 0:
+            bv = np.zeros(1, dtype=np.uint64)
+        g = np.ascontiguousarray(gsw_key, dtype=np.uint64)
+        self._check(self._lib.opir_server_set_client_keys(
+            self._h, client_id, _ptr(bv), _ptr(gk, C.c_uint32), n_keys, _ptr(g)))
+
+    def remove_client(self, client_id: int):
+        self._check(self._lib.opir_server_remove_client(self._h, client_id))
+
+    # ---- query path
+    def make_query(self, client_id: int, query: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        if q.shape != (2, self.params.N):
+            raise ValueError("query must be (2, N)")
+        out = np.zeros((2, self.params.N), dtype=np.uint64)
+        self._check(self._lib.opir_server_make_query(self._h, client_id, _ptr(q), _ptr(out)))
+        return out
+
+    def make_query_batch(self, client_ids: Sequence[int], queries: np.ndarray) -> np.ndarray:
+        ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
+        q = np.ascontiguousarray(queries, dtype=np.uint64)
+        n = ids.size
+        if q.shape != (n, 2, self.params.N):
+            raise ValueError("queries must be (n, 2, N)")
+        out = np.zeros_like(q)
+        self._check(self._lib.opir_server_make_query_batch(self._h, n, _ptr(ids), _ptr(q), _ptr(out)))
+        return out
+
+    def make_query_batch_device(self, client_ids: Sequence[int], d_queries: int,
+                                d_responses: int, stream: int = 0):
+        """Enqueue on device pointers (ints), e.g. torch tensors' data_ptr()."""
+        ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
+        self._check(self._lib.opir_server_make_query_batch_device(
+            self._h, ids.size, _ptr(ids), C.c_void_p(d_queries), C.c_void_p(d_responses),
+            C.c_void_p(stream) if stream else None))
+
+    def set_stage_timing(self, enabled: bool):
+        self._check(self._lib.opir_server_set_stage_timing(self._h, 1 if enabled else 0))
+
+    def stage_times(self) -> dict:
+        buf = (C.c_float * 5)()
+        self._check(self._lib.opir_server_stage_times(self._h, buf))
+        names = ["Expand", "Convert", "First dim", "Other dim", "Modulus switching"]
+        return dict(zip(names, list(buf)))
+
+    # ---- individual stages (public PirServer methods)
+    def expand_query(self, client_id: int, query: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        out = np.zeros((self.params.useful, 2, self.params.N), dtype=np.uint64)
+        self._check(self._lib.opir_server_expand_query(self._h, client_id, _ptr(q), _ptr(out)))
+        return out
+
+    def complete_selectors(self, client_id: int, expanded: np.ndarray) -> np.ndarray:
+        p = self.params
+        e = np.ascontiguousarray(expanded, dtype=np.uint64)
+        out = np.zeros((max(p.num_dims - 1, 1), 2 * p.l_ep, 2, p.N), dtype=np.uint64)
+        self._check(self._lib.opir_server_complete_selectors(self._h, client_id, _ptr(e), _ptr(out)))
+        return out[: p.num_dims - 1]
+
+    def evaluate_first_dim(self, fst_query: np.ndarray) -> np.ndarray:
+        p = self.params
+        f = np.ascontiguousarray(fst_query[: p.fst_dim_sz], dtype=np.uint64)
+        out = np.zeros((p.other_dim_sz, 2, p.N), dtype=np.uint64)
+        self._check(self._lib.opir_server_evaluate_first_dim(self._h, _ptr(f), _ptr(out)))
+        return out
+
+    def evaluate_other_dim(self, mid: np.ndarray, selectors: np.ndarray) -> np.ndarray:
+        m = np.ascontiguousarray(mid, dtype=np.uint64)
+        s = np.ascontiguousarray(selectors, dtype=np.uint64)
+        if s.size == 0:
+            s = np.zeros(1, dtype=np.uint64)
+        out = np.zeros((2, self.params.N), dtype=np.uint64)
+        self._check(self._lib.opir_server_evaluate_other_dim(self._h, _ptr(m), _ptr(s), _ptr(out)))
+        return out
+
+    def save_resp_to_stream(self, response: np.ndarray) -> bytes:
+        return save_response(self.params, response)
+
+
+def save_response(params: PirParams, response: np.ndarray) -> bytes:
+    """PirServer::save_resp_to_stream (server.cpp:950-1009)."""
+    r = np.ascontiguousarray(response, dtype=np.uint64)
+    cap = params.response_bytes()
+    buf = np.zeros(cap, dtype=np.uint8)
+    n = L.load().opir_save_response(C.byref(params._p), _ptr(r), _ptr(buf, C.c_uint8), cap)
+    return buf[:n].tobytes()

@@ -1,0 +1,153 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle and the
+reference-generated goldens. Integer work, so every comparison is bit-exact.
+
+Stage tests mirror the reference's public PirServer methods
+(expand_query, complete_selectors, evaluate_first_dim, evaluate_other_dim);
+end-to-end tests compare make_query responses (u64 arrays and the 22-bit
+serialized stream) with the golden responses the reference itself produced,
+and check that the client decrypts the requested plaintext.
+"""
+import functools
+
+import numpy as np
+import pytest
+
+from onionpirv2_b200 import OutOfRange, PirParams, PirServer, save_response
+from oracle import oracle as O
+from tests import golden_cases as G
+
+pytestmark = pytest.mark.gpu
+
+SMALL = [c["name"] for c in G.cases() if c["num_pt"] <= 20000]
+LARGE = [c["name"] for c in G.cases() if c["num_pt"] > 20000]
+
+
+@functools.lru_cache(maxsize=None)
+def setup(name):
+    c = G.case(name)
+    op = O.params(c["target_num_pt"], c["expansion_height"], c["fst_dim_pow2"])
+    cl = O.Client(op, c["client_seed"])
+    bv, gsw = cl.bv_keys(), cl.gsw_key()
+    q = cl.query(c["index"])
+    gp = PirParams(c["target_num_pt"], c["expansion_height"], c["fst_dim_pow2"])
+    srv = PirServer(gp)
+    srv.load_data_seeded(c["target_num_pt"], c["db_seed"])
+    srv.set_client_keys(7, bv, gsw)
+    return c, op, cl, bv, gsw, q, gp, srv
+
+
+@functools.lru_cache(maxsize=None)
+def oracle_server(name):
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    s = O.Server(op)
+    s.load_seeded(c["target_num_pt"], c["db_seed"])
+    s.set_keys(bv, gsw)
+    return s
+
+
+def _check_response(c, cl, op, resp):
+    assert G.sha256(resp) == c["sha256_response_u64"]
+    assert save_response(PirParams(c["target_num_pt"], c["expansion_height"], c["fst_dim_pow2"]),
+                         resp) == G.stream(c)
+    want = (O.db_plaintext(c["db_seed"], c["index"], op) if c["index"] < c["target_num_pt"]
+            else np.zeros(op.N, np.uint16))
+    assert np.array_equal(cl.decrypt(resp), want.astype(np.uint64))
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_expand_query_matches_oracle(name):
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    got = srv.expand_query(7, q)
+    want = oracle_server(name).expand(q)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_complete_selectors_matches_oracle(name):
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    exp = oracle_server(name).expand(q)
+    got = srv.complete_selectors(7, exp)
+    want = oracle_server(name).complete_selectors(exp)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_first_dim_matches_oracle(name):
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    exp = oracle_server(name).expand(q)
+    got = srv.evaluate_first_dim(exp)
+    want = oracle_server(name).first_dim(exp)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_other_dim_matches_oracle(name):
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    os_ = oracle_server(name)
+    exp = os_.expand(q)
+    sel = os_.complete_selectors(exp)
+    mid = os_.first_dim(exp)
+    got = srv.evaluate_other_dim(mid, sel)
+    want = os_.other_dim(mid, sel)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("name", SMALL + LARGE)
+def test_make_query_matches_reference_golden(name):
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    _check_response(c, cl, op, srv.make_query(7, q))
+
+
+def test_batch_equals_single_queries():
+    name = "c1_16384_h9"
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    rng = np.random.default_rng(5)
+    clients, queries, idxs = [], [], []
+    for i in range(5):
+        k = O.Client(op, 1000 + i)
+        srv.set_client_keys(100 + i, k.bv_keys(), k.gsw_key())
+        idx = int(rng.integers(0, op.num_pt))
+        clients.append(k); idxs.append(idx); queries.append(k.query(idx))
+    ids = [100 + i for i in range(5)]
+    batch = srv.make_query_batch(ids, np.stack(queries))
+    for i in range(5):
+        single = srv.make_query(ids[i], queries[i])
+        assert np.array_equal(batch[i], single)
+        assert np.array_equal(clients[i].decrypt(batch[i]),
+                              O.db_plaintext(c["db_seed"], idxs[i], op).astype(np.uint64))
+    # the batch mixes in the golden client and still matches the golden
+    mixed = srv.make_query_batch([ids[0], 7, ids[1]], np.stack([queries[0], q, queries[1]]))
+    _check_response(c, cl, op, mixed[1])
+
+
+def test_load_paths_agree():
+    name = "small_1000_h7"
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    pts = np.stack([O.db_plaintext(c["db_seed"], i, op) for i in range(c["target_num_pt"])])
+    for src in (pts, pts.astype(np.uint64), lambda i: pts[i]):
+        s2 = PirServer(gp)
+        s2.load_data(c["target_num_pt"], src)
+        s2.set_client_keys(7, bv, gsw)
+        _check_response(c, cl, op, s2.make_query(7, q))
+        s2.close()
+
+
+def test_errors_follow_the_reference():
+    name = "ragged_43_h5"
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    with pytest.raises(OutOfRange):
+        srv.make_query(12345, q)                      # map::at on an unknown client
+    bad = np.stack([O.db_plaintext(1, i, op) for i in range(c["target_num_pt"])]).astype(np.uint64)
+    bad[3, 17] = op.t
+    s2 = PirServer(gp)
+    with pytest.raises(ValueError):                   # server.cpp:134-137
+        s2.load_data(c["target_num_pt"], bad)
+    with pytest.raises(ValueError):                   # server.cpp:85-88
+        s2.load_data_seeded(op.num_pt + 1, 1)
+    with pytest.raises(ValueError):                   # fewer keys than the height
+        s2.set_client_keys(1, bv[:1], gsw)
+    with pytest.raises(OutOfRange):                   # BvGaloisKeys::get
+        s2.set_client_keys(1, bv, gsw, galois_ks=[3] * bv.shape[0])
+    s2.close()
+    # the handle stays usable after errors
+    _check_response(c, cl, op, srv.make_query(7, q))
