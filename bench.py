@@ -1,0 +1,383 @@
+"""Benchmark of the B200 OnionPIRv2 server path (PirServer::make_query).
+
+Workload: k1_comp parameters (N = 2048, q = q1 q2 ~ 2^58, t = 4099), a
+2^18-plaintext database (872 MB of 13-bit coefficients; 4 GiB in NTT form on
+the device), first dimension 512 x 9 further binary dimensions. A step is one
+batch of B independent queries (each with its own client keys) answered by
+one pass of the path; the first-dimension scan reads the database once per
+batch. The database is larger than L2 (126 MB), so every step streams it from
+HBM; no L2 flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+    python bench.py --impl reference ...      # the reference's CPU server
+
+N > 1 runs one rank per GPU (torchrun), each holding a replica of the
+database and serving its own queries (queries are independent: replicas
+only, no collective on the data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import platform
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "queries/s and DB GB/s at 1 GB DB, batched vs plain GPU (bit-exact); p50/p99 ms"
+TARGET, HEIGHT = 262144, 10
+DB_SEED = 20261203
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-queries", type=int, default=3)
+    ap.add_argument("--target", type=int, default=TARGET,
+                    help="plaintexts (smaller layouts are for profiling captures)")
+    ap.add_argument("--height", type=int, default=HEIGHT)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Max of a per-rank float over all ranks (identity when world == 1)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device=None):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier(device_ids=[device.index] if device is not None and device.type == "cuda" else None)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic() -> dict | None:
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+def synthetic_inputs(params, batch: int, seed: int):
+    """Seeded uniform ciphertexts and key material mod q. make_query's work
+    is data-independent, so uniform inputs time the same arithmetic as
+    genuine client queries (parity is proven by tests/)."""
+    N, q = params.N, params.q
+    rng = np.random.default_rng(seed)
+    queries = rng.integers(0, q, (batch, 2, N), dtype=np.uint64)
+    keys = []
+    for b in range(batch):
+        bv = rng.integers(0, q, (params.expansion_height, params.l_ks, 2, N), dtype=np.uint64)
+        gsw = rng.integers(0, q, (2 * params.l_key, 2, N), dtype=np.uint64)
+        keys.append((bv, gsw))
+    return queries, keys
+
+
+def ref_binary() -> str | None:
+    d = os.path.join(ROOT, "oracle", "_ref")
+    fast, port = os.path.join(d, "opir_ref_avx512"), os.path.join(d, "opir_ref")
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+    except OSError:
+        flags = ""
+    if os.path.exists(fast) and "avx512f" in flags and "avx512dq" in flags and "avx512bw" in flags:
+        return fast
+    return port if os.path.exists(port) else None
+
+
+def run_reference(queries: int, warmup: int, procs: int, seed: int) -> dict:
+    exe = ref_binary()
+    if exe is None:
+        raise FileNotFoundError("oracle/_ref is not built")
+    cmd = [exe, "--mode", "time", "--target", str(TARGET), "--height", str(HEIGHT),
+           "--db-seed", str(DB_SEED), "--client-seed", str(seed), "--queries", str(queries),
+           "--warmup", str(warmup), "--procs", str(procs)]
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True)
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    res["binary"] = os.path.basename(exe)
+    return res
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor()
+
+
+# ---------------------------------------------------------------- reference arm
+def bench_reference(args, world, rank):
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    try:
+        res = run_reference(args.steps, args.warmup, procs, 7)
+    except Exception as e:  # reference binary missing or failed
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU server: {e}"}))
+        return
+    qps = res["qps"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["mean_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"k1_comp N=2048, {TARGET} plaintexts, first dim 512 x 9 binary dims",
+                   "batch": 1, "parallelism": f"{procs} host processes"},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": procs, "kind": "reference",
+                         "sample": (f"reference make_query (oracle/_ref/{res['binary']}, HEXL stand-in) "
+                                    f"on {procs} forked processes x {args.steps} queries after one load_data; "
+                                    f"CPU {cpu_model()}")},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- our arm
+def bench_ours(args, world, rank, local):
+    import torch
+    from onionpirv2_b200 import PirParams, PirServer
+    from onionpirv2_b200.server import launch_count
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=device)
+    params = PirParams(args.target, args.height)
+    N = params.N
+    B = args.batch
+    srv = PirServer(params, device=local)
+    t0 = time.perf_counter()
+    srv.load_data_seeded(args.target, DB_SEED)
+    load_s = time.perf_counter() - t0
+    queries, keys = synthetic_inputs(params, B, 1000 + rank)
+    for b, (bv, gsw) in enumerate(keys):
+        srv.set_client_keys(b, bv, gsw)
+    ids = list(range(B))
+    # a dedicated (non-default) stream: the library orders its own stream
+    # after this one and this one after its work, so events recorded here
+    # bracket the whole batch
+    stream = torch.cuda.Stream(device)
+    d_q = torch.from_numpy(queries.view(np.int64)).to(device)
+    d_r = torch.empty_like(d_q)
+
+    def step(n, qbuf, rbuf):
+        srv.make_query_batch_device(ids[:n], qbuf.data_ptr(), rbuf.data_ptr(), stream.cuda_stream)
+
+    def timed(n, steps, warm):
+        qb, rb = d_q[:n].contiguous(), d_r[:n].contiguous()
+        for _ in range(warm):
+            step(n, qb, rb)
+        torch.cuda.synchronize(device)
+        barrier(world, device)
+        torch.cuda.synchronize(device)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        srv.set_stage_timing(True)
+        l0 = launch_count()
+        evs[0].record(stream)
+        for i in range(steps):
+            step(n, qb, rb)
+            evs[i + 1].record(stream)
+        torch.cuda.synchronize(device)
+        launches = launch_count() - l0
+        barrier(world, device)
+        per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+        total = evs[0].elapsed_time(evs[-1])
+        stages = srv.stage_times()
+        srv.set_stage_timing(False)
+        return total, per, stages, launches
+
+    # plain single-query path (B = 1)
+    plain_total, plain_per, plain_stages, _ = timed(1, args.steps, args.warmup)
+    plain_total = max_over_ranks(plain_total, world, device)
+    # batched path (headline), clocks sampled during the timed region
+    with ClockSampler(local) as clk:
+        total, per, stages, launches = timed(B, args.steps, args.warmup)
+    total_max = max_over_ranks(total, world, device)
+    queries_done = world * B * args.steps
+    qps = queries_done / (total_max / 1e3)
+
+    # end to end through the host-buffer C ABI call (pinned host memory)
+    hq = torch.from_numpy(queries.view(np.int64)).pin_memory()
+    hr = torch.empty_like(hq).pin_memory()
+    hq_np, hr_np = hq.numpy().view(np.uint64), hr.numpy().view(np.uint64)
+    for _ in range(args.warmup):
+        srv.make_query_batch(ids, hq_np, out=hr_np)
+    barrier(world, device)
+    te = time.perf_counter()
+    for _ in range(args.steps):
+        srv.make_query_batch(ids, hq_np, out=hr_np)
+    e2e_s = max_over_ranks(time.perf_counter() - te, world, device)
+    e2e_qps = queries_done / e2e_s
+
+    if rank != 0:
+        srv.close()
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    peaks = measured_peaks()
+    db_phys = 2 * N * params.num_pt * 4
+    qmat_bytes = 2 * N * params.fst_dim_sz * 2 * B * 4
+    cmat_bytes = 2 * N * params.other_dim_sz * 2 * B * 4
+    alg_bytes = db_phys + qmat_bytes + cmat_bytes
+    core_ms = stages["Core"]
+    achieved = alg_bytes / (core_ms / 1e3) / 1e9
+    traffic = ncu_traffic()
+    logical_db = params.num_pt * N * 13 / 8
+    line = {
+        "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded DB coefficients < t generated on device; seeded uniform "
+                "ciphertexts and keys mod q -- the path is data-independent)",
+        "config": {"workload": f"k1_comp N=2048, {args.target} plaintexts ({logical_db / 1e6:.1f} MB "
+                               f"at 13 bits, {db_phys} B NTT form), first dim {params.fst_dim_sz} x "
+                               f"{params.num_dims - 1} binary dims",
+                   "batch": B, "num_pt": params.num_pt, "fst_dim_sz": params.fst_dim_sz,
+                   "num_dims": params.num_dims,
+                   "l2": "inputs larger than L2: the 4 GiB database streams from HBM every step",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "db_gbs": logical_db * queries_done / (total_max / 1e3) / 1e9,
+        "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+        "stages_ms": {k: round(v, 4) for k, v in stages.items() if k != "calls"},
+        "plain": {"batch": 1, "value": world * args.steps / (plain_total / 1e3), "unit": "queries/s",
+                  "latency_ms": {"p50": float(np.percentile(plain_per, 50)),
+                                 "p99": float(np.percentile(plain_per, 99))},
+                  "db_gbs": logical_db * world * args.steps / (plain_total / 1e3) / 1e9,
+                  "stages_ms": {k: round(v, 4) for k, v in plain_stages.items() if k != "calls"}},
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * 2 * N * 8,
+                "d2h_bytes_per_step": B * 2 * N * 8},
+        "roofline": {"bound": "hbm", "kernel": "k_scan (first-dimension scan)",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "algorithmic_bytes": alg_bytes,
+                     "traffic": (traffic or {}).get(f"batch_{B}")},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+        "setup": {"db_load_s": round(load_s, 3), "gpu": torch.cuda.get_device_name(device)},
+    }
+    if world == 1 and not args.no_cpu_baseline and args.target == TARGET:
+        try:
+            res = run_reference(args.cpu_queries, 0, 1, 7)
+            line["cpu_baseline"] = {
+                "value": 1000.0 / res["mean_ms"], "unit": "queries/s", "cores": 1,
+                "kind": "reference",
+                "sample": (f"reference make_query (oracle/_ref/{res['binary']}, HEXL stand-in), "
+                           f"{res['queries']} queries on the same layout after one untimed "
+                           f"load_data ({res['load_s']:.1f} s); CPU {cpu_model()}")}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unit": "queries/s", "cores": 0,
+                                    "kind": "reference", "sample": f"unavailable: {e}"}
+    print(json.dumps(line))
+    srv.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        bench_reference(args, world, rank)
+        return
+    bench_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

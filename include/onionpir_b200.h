@@ -168,12 +168,19 @@ opir_status opir_server_make_query_batch_device(opir_server *server, uint32_t n,
                                                 uint64_t *d_responses,
                                                 void *stream);
 
-/* Per-stage device times (ms) of the last make_query / batch call, in the
- * reference's TimerLogger sections (includes/logging.h:34-78):
- * [0] Expand, [1] Convert, [2] First dim, [3] Other dim, [4] Modulus switching.
- * Stage timing must have been enabled with opir_server_set_stage_timing. */
+/* Per-stage device times (ms), averaged over the make_query / batch calls
+ * made since stage timing was (re-)enabled, in the reference's TimerLogger
+ * sections (includes/logging.h:34-78): [0] Expand, [1] Convert,
+ * [2] First dim, [3] Other dim, [4] Modulus switching, [5] Core (the
+ * first-dimension scan kernel alone, the reference's CORE_TIME). Timing uses
+ * CUDA events on the handle's stream; opir_server_stage_times synchronises
+ * that stream. *calls receives the number of calls averaged (may be NULL). */
 opir_status opir_server_set_stage_timing(opir_server *server, int enabled);
-opir_status opir_server_stage_times(const opir_server *server, float *ms_out);
+opir_status opir_server_stage_times(opir_server *server, float *ms_out,
+                                    uint32_t *calls);
+
+/* Total kernel launches issued by this library in this process. */
+uint64_t opir_launch_count(void);
 
 /* ---- individual stages (public PirServer methods used by tests and by the
  *      reference's tree-PIR callers) --------------------------------------- */

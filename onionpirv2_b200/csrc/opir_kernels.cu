@@ -5,6 +5,7 @@
 // every per-coefficient step, so global reads of planes are coalesced.
 #include "opir_kernels.h"
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <stdexcept>
@@ -27,7 +28,10 @@ __device__ __forceinline__ ResidueTables pick(const DevParams &P, int res) {
   return res ? P.r[1] : P.r[0];
 }
 
+std::atomic<uint64_t> g_launches{0};
+
 void check_launch(const char *what) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -483,6 +487,8 @@ inline unsigned grid1d(uint64_t n) {
 }  // namespace
 
 // ===================================================================== launchers
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 void launch_split_u64(const DevParams &P, const uint64_t *in, uint32_t *out, uint64_t n_items,
                       uint64_t per_item, uint64_t out_item_stride, cudaStream_t st) {
   const uint64_t n = n_items * per_item * kN;

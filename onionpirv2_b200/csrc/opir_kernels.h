@@ -97,4 +97,7 @@ void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride
                       uint64_t *resp, uint8_t *bytes, uint32_t resp_bytes,
                       uint32_t batch, cudaStream_t st);
 
+// Kernel launches issued so far by this library (all launchers count).
+uint64_t launch_count();
+
 }  // namespace opir

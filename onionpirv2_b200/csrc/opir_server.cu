@@ -72,6 +72,8 @@ struct ClientKeys {
 };
 
 constexpr int kStages = 5;
+constexpr int kEvents = kStages + 3;   // 6 stage boundaries + scan begin/end
+constexpr int kTimingSlots = 512;
 
 }  // namespace
 
@@ -94,10 +96,11 @@ struct opir_server {
   DevBuf<uint32_t> lvl[2], sel, qmat, cmat, mid[2];
   DevBuf<const uint32_t *> keyptrs;
   std::vector<const uint32_t *> host_keyptrs;
-  // stage timing
+  // stage timing: one event set per timed call, averaged on request
   bool timing = false;
-  cudaEvent_t ev[kStages + 1] = {};
-  float stage_ms[kStages] = {0, 0, 0, 0, 0};
+  std::vector<std::vector<cudaEvent_t>> ev_pool;
+  uint32_t timed_calls = 0;
+  cudaEvent_t *cur_ev = nullptr;
 };
 
 namespace {
@@ -226,8 +229,19 @@ void upload_keyptrs(opir_server *s, const uint64_t *client_ids, uint32_t n) {
                      cudaMemcpyHostToDevice, s->stream), "key pointers");
 }
 
+void begin_timed_call(opir_server *s) {
+  s->cur_ev = nullptr;
+  if (!s->timing || s->timed_calls >= kTimingSlots) return;
+  if (s->ev_pool.size() <= s->timed_calls) {
+    std::vector<cudaEvent_t> evs(kEvents);
+    for (auto &e : evs) ck(cudaEventCreate(&e), "cudaEventCreate");
+    s->ev_pool.push_back(std::move(evs));
+  }
+  s->cur_ev = s->ev_pool[s->timed_calls++].data();
+}
+
 void mark(opir_server *s, int i) {
-  if (s->timing) ck(cudaEventRecord(s->ev[i], s->stream), "cudaEventRecord");
+  if (s->cur_ev) ck(cudaEventRecord(s->cur_ev[i], s->stream), "cudaEventRecord");
 }
 
 // Expansion (Algorithm 2) over n queries whose residue pairs sit in slot 0 of
@@ -245,7 +259,9 @@ uint32_t *run_expand(opir_server *s, uint32_t n) {
 void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n) {
   const opir::Shape &sh = s->shape;
   opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, s->qmat.p, n, s->stream);
+  mark(s, kStages + 1);
   opir::launch_scan(s->dp, sh, s->db.p, s->qmat.p, s->cmat.p, n, s->stream);
+  mark(s, kStages + 2);
   opir::launch_scan_epilogue(s->dp, sh, s->cmat.p, s->mid[0].p, sh.other, n, s->stream);
 }
 
@@ -267,6 +283,7 @@ void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
   ensure_capacity(s, n);
   upload_keyptrs(s, client_ids, n);
   const opir::Shape &sh = s->shape;
+  begin_timed_call(s);
   mark(s, 0);
   opir::launch_split_u64(s->dp, d_queries, s->lvl[0].p, n, 2, s->lvl_slots * kCtWords, s->stream);
   const uint32_t *leaves = run_expand(s, n);
@@ -280,14 +297,10 @@ void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
   opir::launch_modswitch(s->dp, res, sh.other, d_resp, d_bytes, resp_bytes_of(s->params), n,
                          s->stream);
   mark(s, 5);
+  s->cur_ev = nullptr;
 }
 
-void finish(opir_server *s) {
-  ck(cudaStreamSynchronize(s->stream), "make_query");
-  if (s->timing)
-    for (int i = 0; i < kStages; ++i)
-      ck(cudaEventElapsedTime(&s->stage_ms[i], s->ev[i], s->ev[i + 1]), "cudaEventElapsedTime");
-}
+void finish(opir_server *s) { ck(cudaStreamSynchronize(s->stream), "make_query"); }
 
 void check_query_values(const opir_server *s, const uint64_t *q, size_t count) {
   for (size_t i = 0; i < count; ++i)
@@ -351,7 +364,6 @@ opir_status opir_server_create(const opir_params *params, int device, opir_serve
     s->device = device;
     DeviceGuard g(device);
     ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    for (auto &e : s->ev) ck(cudaEventCreate(&e), "cudaEventCreate");
     setup_device_params(s);
     s->db.alloc(2ull * kN * s->params.num_pt);
     ck(cudaMemsetAsync(s->db.p, 0, 2ull * kN * s->params.num_pt * 4, s->stream), "db memset");
@@ -384,8 +396,8 @@ void opir_server_destroy(opir_server *s) {
     s->cmat.reset();
     for (auto &b : s->mid) b.reset();
     s->keyptrs.reset();
-    for (auto &e : s->ev)
-      if (e) cudaEventDestroy(e);
+    for (auto &evs : s->ev_pool)
+      for (auto &e : evs) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
     if (prev >= 0) cudaSetDevice(prev);
   }
@@ -581,14 +593,33 @@ opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
 opir_status opir_server_set_stage_timing(opir_server *s, int enabled) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   s->timing = enabled != 0;
+  s->timed_calls = 0;
   return OPIR_OK;
 }
 
-opir_status opir_server_stage_times(const opir_server *s, float *ms_out) {
+opir_status opir_server_stage_times(opir_server *s, float *ms_out, uint32_t *calls) {
   if (!s || !ms_out) return OPIR_ERR_INVALID_ARGUMENT;
-  std::memcpy(ms_out, s->stage_ms, sizeof(s->stage_ms));
-  return OPIR_OK;
+  return guarded(s, [&] {
+    DeviceGuard g(s->device);
+    ck(cudaStreamSynchronize(s->stream), "stage_times");
+    double sum[kStages + 1] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t c = 0; c < s->timed_calls; ++c) {
+      const cudaEvent_t *e = s->ev_pool[c].data();
+      float ms = 0;
+      for (int i = 0; i < kStages; ++i) {
+        ck(cudaEventElapsedTime(&ms, e[i], e[i + 1]), "cudaEventElapsedTime");
+        sum[i] += ms;
+      }
+      ck(cudaEventElapsedTime(&ms, e[kStages + 1], e[kStages + 2]), "cudaEventElapsedTime");
+      sum[kStages] += ms;
+    }
+    for (int i = 0; i <= kStages; ++i)
+      ms_out[i] = s->timed_calls ? static_cast<float>(sum[i] / s->timed_calls) : 0.f;
+    if (calls) *calls = s->timed_calls;
+  });
 }
+
+uint64_t opir_launch_count(void) { return opir::launch_count(); }
 
 opir_status opir_server_expand_query(opir_server *s, uint64_t client_id, const uint64_t *query,
                                      uint64_t *out) {

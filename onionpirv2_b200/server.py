@@ -205,13 +205,19 @@ class PirServer:
         self._check(self._lib.opir_server_make_query(self._h, client_id, _ptr(q), _ptr(out)))
         return out
 
-    def make_query_batch(self, client_ids: Sequence[int], queries: np.ndarray) -> np.ndarray:
+    def make_query_batch(self, client_ids: Sequence[int], queries: np.ndarray,
+                         out: np.ndarray | None = None) -> np.ndarray:
+        """n queries in one pass; `out` (n, 2, N) uint64 may be supplied (e.g.
+        pinned host memory)."""
         ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
         q = np.ascontiguousarray(queries, dtype=np.uint64)
         n = ids.size
         if q.shape != (n, 2, self.params.N):
             raise ValueError("queries must be (n, 2, N)")
-        out = np.zeros_like(q)
+        if out is None:
+            out = np.zeros_like(q)
+        elif out.shape != q.shape or out.dtype != np.uint64 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous (n, 2, N) uint64 array")
         self._check(self._lib.opir_server_make_query_batch(self._h, n, _ptr(ids), _ptr(q), _ptr(out)))
         return out
 
@@ -227,10 +233,15 @@ class PirServer:
         self._check(self._lib.opir_server_set_stage_timing(self._h, 1 if enabled else 0))
 
     def stage_times(self) -> dict:
-        buf = (C.c_float * 5)()
-        self._check(self._lib.opir_server_stage_times(self._h, buf))
-        names = ["Expand", "Convert", "First dim", "Other dim", "Modulus switching"]
-        return dict(zip(names, list(buf)))
+        """Average per-stage device ms since set_stage_timing(True); "Core" is
+        the first-dimension scan kernel alone."""
+        buf = (C.c_float * 6)()
+        calls = C.c_uint32()
+        self._check(self._lib.opir_server_stage_times(self._h, buf, C.byref(calls)))
+        names = ["Expand", "Convert", "First dim", "Other dim", "Modulus switching", "Core"]
+        out = dict(zip(names, [float(x) for x in buf]))
+        out["calls"] = calls.value
+        return out
 
     # ---- individual stages (public PirServer methods)
     def expand_query(self, client_id: int, query: np.ndarray) -> np.ndarray:
@@ -264,6 +275,11 @@ class PirServer:
 
     def save_resp_to_stream(self, response: np.ndarray) -> bytes:
         return save_response(self.params, response)
+
+
+def launch_count() -> int:
+    """Kernel launches issued by the library in this process."""
+    return int(L.load().opir_launch_count())
 
 
 def save_response(params: PirParams, response: np.ndarray) -> bytes:

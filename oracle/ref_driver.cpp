@@ -28,6 +28,7 @@
 #include "utils.h"
 #include "hexl/hexl.hpp"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -38,6 +39,9 @@
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <sys/wait.h>
+#include <unistd.h>
 
 namespace {
 
@@ -173,7 +177,7 @@ struct Args {
   bool pow2 = true;
   uint64_t db_seed = 1, client_seed = 2;
   size_t index = 0;
-  size_t queries = 1, warmup = 0;
+  size_t queries = 1, warmup = 0, procs = 1;
   std::string out;
   bool dump_inputs = false;
 };
@@ -195,6 +199,7 @@ Args parse(int argc, char **argv) {
     else if (k == "--index") a.index = std::stoull(val());
     else if (k == "--queries") a.queries = std::stoull(val());
     else if (k == "--warmup") a.warmup = std::stoull(val());
+    else if (k == "--procs") a.procs = std::stoull(val());
     else if (k == "--out") a.out = val();
     else if (k == "--dump-inputs") a.dump_inputs = true;
     else throw std::invalid_argument("unknown option " + k);
@@ -273,29 +278,74 @@ int main(int argc, char **argv) {
 
     if (a.mode == "time") {
       // The timer boundary is make_query only (merkle_benchmark.cpp:549-553).
-      std::vector<double> ms;
-      size_t failures = 0;
-      for (size_t q = 0; q < a.warmup + a.queries; ++q) {
-        Client c = make_client(params, a.client_seed + q);
-        server.set_client_bv_galois_key(q + 1, c.bv);
-        server.set_client_gsw_key(q + 1, c.gsw);
-        const size_t idx = static_cast<size_t>(mix64(a.client_seed * 7919 + q) % a.target);
-        RlweCt query = make_query(params, c, idx);
-        const auto t0 = std::chrono::steady_clock::now();
-        RlweCt resp = server.make_query(q + 1, query);
-        const double dt = std::chrono::duration<double, std::milli>(
-            std::chrono::steady_clock::now() - t0).count();
-        RlwePt dec = decrypt_small_q(params, c, resp);
-        for (size_t i = 0; i < N; ++i)
-          if (dec.data[i] != db_coeff(seed, idx, i, N, t)) { ++failures; break; }
-        if (q >= a.warmup) ms.push_back(dt);
+      // P processes are forked after load_data so the preprocessed database
+      // is shared copy-on-write; each runs its own clients and queries.
+      const int P = static_cast<int>(a.procs < 1 ? 1 : a.procs);
+      std::vector<int> fds(P);
+      std::vector<pid_t> pids(P);
+      for (int p = 0; p < P; ++p) {
+        int fd[2];
+        if (pipe(fd) != 0) throw std::runtime_error("pipe");
+        const pid_t pid = fork();
+        if (pid < 0) throw std::runtime_error("fork");
+        if (pid == 0) {
+          close(fd[0]);
+          double sum_ms = 0, wall_ms = 0;
+          size_t failures = 0, timed = 0;
+          std::chrono::steady_clock::time_point wall0;
+          for (size_t q = 0; q < a.warmup + a.queries; ++q) {
+            const uint64_t cseed = a.client_seed + 1000003ull * p + q;
+            Client c = make_client(params, cseed);
+            server.set_client_bv_galois_key(q + 1, c.bv);
+            server.set_client_gsw_key(q + 1, c.gsw);
+            const size_t idx = static_cast<size_t>(mix64(cseed * 7919) % a.target);
+            RlweCt query = make_query(params, c, idx);
+            if (q == a.warmup) wall0 = std::chrono::steady_clock::now();
+            const auto t0 = std::chrono::steady_clock::now();
+            RlweCt resp = server.make_query(q + 1, query);
+            const double dt = std::chrono::duration<double, std::milli>(
+                std::chrono::steady_clock::now() - t0).count();
+            RlwePt dec = decrypt_small_q(params, c, resp);
+            for (size_t i = 0; i < N; ++i)
+              if (dec.data[i] != db_coeff(seed, idx, i, N, t)) { ++failures; break; }
+            if (q >= a.warmup) { sum_ms += dt; ++timed; }
+          }
+          if (timed) wall_ms = std::chrono::duration<double, std::milli>(
+              std::chrono::steady_clock::now() - wall0).count();
+          char buf[256];
+          const int n = std::snprintf(buf, sizeof buf, "%.6f %.6f %zu %zu\n", sum_ms, wall_ms,
+                                      timed, failures);
+          if (write(fd[1], buf, n) != n) _exit(2);
+          close(fd[1]);
+          _exit(0);
+        }
+        close(fd[1]);
+        fds[p] = fd[0];
+        pids[p] = pid;
       }
-      double sum = 0;
-      for (double v : ms) sum += v;
-      std::printf("{\"mean_ms\": %.3f, \"queries\": %zu, \"failures\": %zu, \"load_s\": %.3f, \"samples_ms\": [",
-                  ms.empty() ? 0.0 : sum / ms.size(), ms.size(), failures, load_s);
-      for (size_t i = 0; i < ms.size(); ++i) std::printf("%s%.3f", i ? ", " : "", ms[i]);
-      std::printf("]}\n");
+      double sum_ms = 0, wall_max = 0;
+      size_t timed = 0, failures = 0;
+      for (int p = 0; p < P; ++p) {
+        char buf[256] = {0};
+        const ssize_t n = read(fds[p], buf, sizeof buf - 1);
+        close(fds[p]);
+        int status = 0;
+        waitpid(pids[p], &status, 0);
+        double s1 = 0, w1 = 0;
+        size_t t1 = 0, f1 = 0;
+        if (n <= 0 || std::sscanf(buf, "%lf %lf %zu %zu", &s1, &w1, &t1, &f1) != 4 ||
+            !WIFEXITED(status) || WEXITSTATUS(status) != 0)
+          throw std::runtime_error("timing child failed");
+        sum_ms += s1;
+        timed += t1;
+        failures += f1;
+        wall_max = std::max(wall_max, w1);
+      }
+      const double mean = timed ? sum_ms / timed : 0.0;
+      const double qps = wall_max > 0 ? timed / (wall_max / 1000.0) : 0.0;
+      std::printf("{\"mean_ms\": %.3f, \"qps\": %.4f, \"queries\": %zu, \"procs\": %d, "
+                  "\"failures\": %zu, \"load_s\": %.3f}\n",
+                  mean, qps, timed, P, failures, load_s);
       return failures ? 3 : 0;
     }
     throw std::invalid_argument("unknown mode " + a.mode);
