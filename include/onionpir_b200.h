@@ -218,6 +218,35 @@ opir_status opir_server_evaluate_other_dim(opir_server *server,
 size_t opir_save_response(const opir_params *params, const uint64_t *response,
                           uint8_t *out, size_t cap);
 
+/* ---- allocation-free MUX ------------------------------------------------- */
+
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory when they run a MUX step (a host that pre-budgets and owns all
+ * device memory, or a request loop that must not touch the CUDA allocator
+ * because an allocation can synchronise the device): n independent MUX
+ * steps out_i = x_i + b_i * (y_i - x_i), exactly PirServer::ext_prod_mux
+ * (src/server.cpp:652-722), with no server handle and no allocation.
+ *   d_x, d_y      : n x 2N u64 device arrays, coefficient form mod q
+ *   d_selectors   : n x 2 L_EP rows x 2N u64 device array, RGSW selector in
+ *                   NTT form (the complete_selectors layout)
+ *   d_out         : n x 2N u64 device array (may not alias the inputs)
+ *   stream        : cudaStream_t to enqueue on (NULL = legacy default stream)
+ * Working memory is one fixed array inside the library (about 3.9 MiB per
+ * device that loads the library, held until process exit); n above
+ * OPIR_NOALLOC_MAX_MUX is rejected with OPIR_ERR_INVALID_ARGUMENT. The first
+ * call on each device sets up that device (looks up the array's device
+ * address and copies the NTT tables into it with a synchronous cudaMemcpy),
+ * so make the first call before any stream capture. Every call shares the
+ * same array: calls whose work overlaps on the GPU (different streams, or
+ * different host threads) race and must be serialised by the caller. Each
+ * call overwrites every scratch word it reads, so nothing depends on what an
+ * earlier call left behind. Only the CONFIG_N2048_K1_COMP parameter set. */
+#define OPIR_NOALLOC_MAX_MUX 8
+opir_status opir_ext_prod_mux_noalloc(const opir_params *params, uint32_t n,
+                                      const uint64_t *d_x, const uint64_t *d_y,
+                                      const uint64_t *d_selectors, uint64_t *d_out,
+                                      void *stream);
+
 /* Library version string. */
 const char *opir_version(void);
 
