@@ -83,36 +83,50 @@ __global__ void k_compose_u64(DevParams P, const uint32_t *__restrict__ in, uint
 }
 
 // --------------------------------------------------------- DB preprocessing
-constexpr int kDbTile = 8;
+constexpr int kDbTile = 8;  // plaintexts per block (one padded plane each)
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
                 uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
                 uint64_t logical, uint64_t num_pt, uint64_t pt_begin,
                 uint64_t pt_end, uint32_t *__restrict__ db) {
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y;
+  const int res = blockIdx.y, tid = threadIdx.x;
   const ResidueTables T = pick(P, res);
   const uint64_t pt0 = pt_begin + (uint64_t)blockIdx.x * kDbTile;
-  for (int idx = threadIdx.x; idx < kDbTile * kN; idx += kThreads) {
-    const int p = idx >> kLogN, c = idx & (kN - 1);
-    const uint64_t pt = pt0 + p;
-    uint32_t v = 0;
-    if (pt < pt_end && pt < logical) {
-      if (coeffs != nullptr)
-        v = coeffs[(pt - coeff_pt_begin) * kN + c];
-      else
-        v = static_cast<uint32_t>(mix64(seed + (pt * kN + c + 1) * kGolden) % t);
+  for (int e = 0; e < kDbTile; ++e) {
+    const uint64_t pt = pt0 + e;
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int c = posA(tid, k);
+      uint32_t x = 0;
+      if (pt < pt_end && pt < logical) {
+        if (coeffs != nullptr)
+          x = coeffs[(pt - coeff_pt_begin) * kN + c];
+        else
+          x = static_cast<uint32_t>(mix64(seed + (pt * kN + c + 1) * kGolden) % t);
+      }
+      v[k] = x;  // x < t < q_res: canonical
     }
-    sm[idx] = v;  // v < t < q_res: already canonical
+    fwdA(v, T);
+    st_plane<0>(sm + e * kPad, v, tid);
   }
   __syncthreads();
-  ntt_fwd_planes(sm, kDbTile, T);
+  fwd_mid(sm, kDbTile, T);
+  uint32_t out[kDbTile][8];
+#pragma unroll
+  for (int e = 0; e < kDbTile; ++e) {
+    ld_plane<3>(sm + e * kPad, out[e], tid);
+    fwdD(out[e], T, tid);
+  }
   uint32_t *dbr = db + (uint64_t)res * kN * num_pt;
-  for (int idx = threadIdx.x; idx < kDbTile * kN; idx += kThreads) {
-    const int c = idx / kDbTile, p = idx % kDbTile;
-    const uint64_t pt = pt0 + p;
-    if (pt < pt_end) dbr[(uint64_t)c * num_pt + pt] = sm[p * kN + c];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    uint32_t *row = dbr + (uint64_t)posD(tid, k) * num_pt + pt0;
+#pragma unroll
+    for (int e = 0; e < kDbTile; ++e)
+      if (pt0 + e < pt_end) row[e] = out[e][k];
   }
 }
 
@@ -120,73 +134,87 @@ k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
 // One heap node (and one residue) per block: BV key switch of the node's
 // ciphertext (bv_keyswitch.cpp:296-367) then the two children
 // (server.cpp:794-809): left = c + c', right = (c - c') X^-k.
+// sigma_k is applied as a gather: sigma(c)[j] = +-c[j k^-1 mod 2N].
 __global__ void __launch_bounds__(kThreads, 2)
-k_expand_level(DevParams P, uint32_t galois, uint32_t kshift, int base_ks, int l_ks,
+k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, int l_ks,
                const uint32_t *__restrict__ in, uint64_t in_stride,
                uint32_t *__restrict__ out, uint64_t out_stride,
                const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
   extern __shared__ uint32_t sm[];
-  uint32_t *sc1 = sm;            // sigma(c1), both residues
-  uint32_t *sc0 = sm + 2 * kN;   // sigma(c0), own residue
-  uint32_t *D = sm + 3 * kN;     // digit planes
-  const int node = blockIdx.x, res = blockIdx.y, b = blockIdx.z;
+  const int node = blockIdx.x, res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
   const ResidueTables T = pick(P, res);
   const uint32_t q = T.q;
   const uint32_t *ct = in + ((uint64_t)b * in_stride + node) * kCtWords;
   const uint32_t *c0 = ct + res * kN;
   const uint32_t *c1 = ct + 2 * kN + res * kN;
 
-  // sigma_k on c1 (both residues) and c0 (own residue), utils.cpp:58-72
-  for (int i = threadIdx.x; i < kN; i += kThreads) {
-    uint32_t dest = (static_cast<uint32_t>(i) * galois) & (2 * kN - 1);
-    const bool neg = dest >= kN;
-    dest &= kN - 1;
-    const uint32_t a0 = ct[2 * kN + i], a1 = ct[3 * kN + i], z = c0[i];
-    sc1[dest] = neg ? neg_mod(a0, P.q1) : a0;
-    sc1[kN + dest] = neg ? neg_mod(a1, P.q2) : a1;
-    sc0[dest] = neg ? neg_mod(z, q) : z;
-  }
-  __syncthreads();
-  // signed base-2^base_ks decomposition of sigma(c1) (mod q), digits LSB first
+  // sigma_k(c0) (own residue) and the centred sigma_k(c1) at A-order positions
+  uint32_t s0[8];
+  int64_t d[8];
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    int64_t d = centre(crt_compose(sc1[j], sc1[kN + j], P), P);
-    for (int t = 0; t < l_ks; ++t) D[t * kN + j] = digit_residue(next_digit(d, base_ks), q);
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t j = posA(tid, k);
+    const uint32_t u = (j * galois_inv) & (2 * kN - 1);
+    const bool neg = u >= kN;
+    const uint32_t src = u & (kN - 1);
+    const uint32_t z = c0[src], a0 = ct[2 * kN + src], a1 = ct[3 * kN + src];
+    s0[k] = neg ? neg_mod(z, q) : z;
+    d[k] = centre(crt_compose(neg ? neg_mod(a0, P.q1) : a0, neg ? neg_mod(a1, P.q2) : a1, P), P);
+  }
+  // digit planes: decompose, pass A in registers
+  for (int i = 0; i < l_ks; ++i) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = digit_residue(next_digit(d[k], base_ks), q);
+    fwdA(v, T);
+    st_plane<0>(sm + i * kPad, v, tid);
   }
   __syncthreads();
-  ntt_fwd_planes(D, l_ks, T);
-  // inner product with the key rows (row t encrypts sigma(s) B^t)
+  fwd_mid(sm, l_ks, T);
+  // inner product with the key rows (row t encrypts sigma(s) B^t), D-order
   const uint32_t *key = bv_keys[b] + bv_level_off + res * kN;
-  uint32_t rb[kPer], ra[kPer];
+  uint64_t ab[8], aa[8];
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    uint64_t ab = 0, aa = 0;
-    for (int t = 0; t < l_ks; ++t) {
-      const uint64_t dv = D[t * kN + j];
-      ab += dv * __ldg(key + (uint64_t)(t * 4 + 0) * kN + j);
-      aa += dv * __ldg(key + (uint64_t)(t * 4 + 2) * kN + j);
+  for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
+  for (int i = 0; i < l_ks; ++i) {
+    uint32_t v[8];
+    ld_plane<3>(sm + i * kPad, v, tid);
+    fwdD(v, T, tid);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j0 = 4 * (tid + 256 * h);
+      const uint4 kb = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(i * 4 + 0) * kN + j0));
+      const uint4 ka = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(i * 4 + 2) * kN + j0));
+      ab[4 * h + 0] += (uint64_t)v[4 * h + 0] * kb.x; aa[4 * h + 0] += (uint64_t)v[4 * h + 0] * ka.x;
+      ab[4 * h + 1] += (uint64_t)v[4 * h + 1] * kb.y; aa[4 * h + 1] += (uint64_t)v[4 * h + 1] * ka.y;
+      ab[4 * h + 2] += (uint64_t)v[4 * h + 2] * kb.z; aa[4 * h + 2] += (uint64_t)v[4 * h + 2] * ka.z;
+      ab[4 * h + 3] += (uint64_t)v[4 * h + 3] * kb.w; aa[4 * h + 3] += (uint64_t)v[4 * h + 3] * ka.w;
     }
-    rb[s] = reduce64(ab, q, T.mu);
-    ra[s] = reduce64(aa, q, T.mu);
   }
   __syncthreads();
+  {
+    uint32_t v[8], w[8];
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    D[j] = rb[s];
-    D[kN + j] = ra[s];
+    for (int k = 0; k < 8; ++k) { v[k] = reduce64(ab[k], q, T.mu); w[k] = reduce64(aa[k], q, T.mu); }
+    invD(v, T, tid);
+    invD(w, T, tid);
+    st_plane<3>(sm, v, tid);
+    st_plane<3>(sm + kPad, w, tid);
   }
   __syncthreads();
-  ntt_inv_planes(D, 2, T);
+  inv_mid(sm, 2, T);
+  uint32_t db_[8], da[8];
+  ld_plane<0>(sm, db_, tid);
+  ld_plane<0>(sm + kPad, da, tid);
+  invA(db_, T);
+  invA(da, T);
   uint32_t *outL = out + ((uint64_t)b * out_stride + 2 * (uint64_t)node) * kCtWords;
   uint32_t *outR = outL + kCtWords;
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    const uint32_t n0v = add_mod(sc0[j], D[j], q);   // c0' = sigma(c0) + delta_b
-    const uint32_t n1v = D[kN + j];                  // c1' = delta_a
+  for (int k = 0; k < 8; ++k) {
+    const int j = posA(tid, k);
+    const uint32_t n0v = add_mod(s0[k], db_[k], q);  // c0' = sigma(c0) + delta_b
+    const uint32_t n1v = da[k];                      // c1' = delta_a
     const uint32_t o0 = c0[j], o1 = c1[j];
     outL[res * kN + j] = add_mod(o0, n0v, q);
     outL[2 * kN + res * kN + j] = add_mod(o1, n1v, q);
@@ -201,42 +229,54 @@ k_expand_level(DevParams P, uint32_t galois, uint32_t kshift, int base_ks, int l
 
 // Shared gadget product of a coefficient-form ciphertext (both residues read
 // from `x` / optional `y`: the decomposed value is y - x, or x when y is
-// null) against NTT-form RGSW rows: acc_k += sum_rows digit * rgsw[row][k].
-// Digit i (LSB first) of poly p meets row p*l + (l - 1 - i) (gsw.cpp:283-293).
+// null) against NTT-form RGSW rows: acc_k += sum_rows digit * rgsw[row][k],
+// accumulated at this thread's D-order positions. Digit i (LSB first) of
+// poly p meets row p*l + (l - 1 - i) (gsw.cpp:283-293). Uses l padded planes.
 __device__ __forceinline__ void gadget_mac(const DevParams &P, const ResidueTables &T,
                                            int res, const uint32_t *x, const uint32_t *y,
                                            const uint32_t *rgsw, int l, int base_log2,
-                                           uint32_t *D, uint64_t (&acc0)[kPer],
-                                           uint64_t (&acc1)[kPer]) {
+                                           uint32_t *sm, uint64_t (&acc0)[8],
+                                           uint64_t (&acc1)[8]) {
   const uint32_t q = T.q;
+  const int tid = threadIdx.x;
 #pragma unroll 1
   for (int p = 0; p < 2; ++p) {
+    int64_t d[8];
 #pragma unroll
-    for (int s = 0; s < kPer; ++s) {
-      const int j = threadIdx.x + s * kThreads;
+    for (int k = 0; k < 8; ++k) {
+      const int j = posA(tid, k);
       uint32_t v1 = x[(p * 2 + 0) * kN + j], v2 = x[(p * 2 + 1) * kN + j];
       if (y != nullptr) {
         v1 = sub_mod(y[(p * 2 + 0) * kN + j], v1, P.q1);
         v2 = sub_mod(y[(p * 2 + 1) * kN + j], v2, P.q2);
       }
-      int64_t d = centre(crt_compose(v1, v2, P), P);
-      for (int i = 0; i < l; ++i) D[i * kN + j] = digit_residue(next_digit(d, base_log2), q);
+      d[k] = centre(crt_compose(v1, v2, P), P);
+    }
+    for (int i = 0; i < l; ++i) {
+      uint32_t v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = digit_residue(next_digit(d[k], base_log2), q);
+      fwdA(v, T);
+      st_plane<0>(sm + i * kPad, v, tid);
     }
     __syncthreads();
-    ntt_fwd_planes(D, l, T);
+    fwd_mid(sm, l, T);
+    for (int i = 0; i < l; ++i) {
+      uint32_t v[8];
+      ld_plane<3>(sm + i * kPad, v, tid);
+      fwdD(v, T, tid);
+      const int row = p * l + (l - 1 - i);
+      const uint32_t *R0 = rgsw + (uint64_t)row * kCtWords + res * kN;
 #pragma unroll
-    for (int s = 0; s < kPer; ++s) {
-      const int j = threadIdx.x + s * kThreads;
-      uint64_t a0 = acc0[s], a1 = acc1[s];
-      for (int i = 0; i < l; ++i) {
-        const int row = p * l + (l - 1 - i);
-        const uint64_t dv = D[i * kN + j];
-        const uint32_t *R = rgsw + (uint64_t)row * kCtWords + res * kN + j;
-        a0 += dv * __ldg(R);
-        a1 += dv * __ldg(R + 2 * kN);
+      for (int h = 0; h < 2; ++h) {
+        const int j0 = 4 * (tid + 256 * h);
+        const uint4 r0 = __ldg(reinterpret_cast<const uint4 *>(R0 + j0));
+        const uint4 r1 = __ldg(reinterpret_cast<const uint4 *>(R0 + 2 * kN + j0));
+        acc0[4 * h + 0] += (uint64_t)v[4 * h + 0] * r0.x; acc1[4 * h + 0] += (uint64_t)v[4 * h + 0] * r1.x;
+        acc0[4 * h + 1] += (uint64_t)v[4 * h + 1] * r0.y; acc1[4 * h + 1] += (uint64_t)v[4 * h + 1] * r1.y;
+        acc0[4 * h + 2] += (uint64_t)v[4 * h + 2] * r0.z; acc1[4 * h + 2] += (uint64_t)v[4 * h + 2] * r1.z;
+        acc0[4 * h + 3] += (uint64_t)v[4 * h + 3] * r0.w; acc1[4 * h + 3] += (uint64_t)v[4 * h + 3] * r1.w;
       }
-      acc0[s] = a0;
-      acc1[s] = a1;
     }
     __syncthreads();
   }
@@ -246,62 +286,87 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const ResidueTabl
 __global__ void __launch_bounds__(kThreads, 2)
 k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
             const uint32_t *const *__restrict__ gsw_keys, uint32_t *__restrict__ sel) {
-  extern __shared__ uint32_t D[];
-  const int row_id = blockIdx.x, res = blockIdx.y, b = blockIdx.z;
+  extern __shared__ uint32_t sm[];
+  const int row_id = blockIdx.x, res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
   const int selno = row_id / S.l_ep, r = row_id % S.l_ep;
   const ResidueTables T = pick(P, res);
   const uint32_t *ct = leaves + ((uint64_t)b * leaf_stride + S.n0 + row_id) * kCtWords;
   uint32_t *out = sel + ((uint64_t)b * (S.num_dims - 1) + selno) * 2 * S.l_ep * kCtWords;
-  uint64_t acc0[kPer], acc1[kPer];
+  uint64_t acc0[8], acc1[8];
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) acc0[s] = acc1[s] = 0;
+  for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
   // bottom row: ExtProd(RGSW(s), row) with the key gadget (gsw.cpp:119-182)
-  gadget_mac(P, T, res, ct, nullptr, gsw_keys[b], S.l_key, S.base_key, D, acc0, acc1);
-  uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords;
+  gadget_mac(P, T, res, ct, nullptr, gsw_keys[b], S.l_key, S.base_key, sm, acc0, acc1);
+  uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords + res * kN;
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    bot[res * kN + j] = reduce64(acc0[s], T.q, T.mu);
-    bot[2 * kN + res * kN + j] = reduce64(acc1[s], T.q, T.mu);
-    D[j] = ct[res * kN + j];
-    D[kN + j] = ct[2 * kN + res * kN + j];
+  for (int h = 0; h < 2; ++h) {
+    const int j0 = 4 * (tid + 256 * h);
+    uint4 o0, o1;
+    o0.x = reduce64(acc0[4 * h + 0], T.q, T.mu); o0.y = reduce64(acc0[4 * h + 1], T.q, T.mu);
+    o0.z = reduce64(acc0[4 * h + 2], T.q, T.mu); o0.w = reduce64(acc0[4 * h + 3], T.q, T.mu);
+    o1.x = reduce64(acc1[4 * h + 0], T.q, T.mu); o1.y = reduce64(acc1[4 * h + 1], T.q, T.mu);
+    o1.z = reduce64(acc1[4 * h + 2], T.q, T.mu); o1.w = reduce64(acc1[4 * h + 3], T.q, T.mu);
+    *reinterpret_cast<uint4 *>(bot + j0) = o0;
+    *reinterpret_cast<uint4 *>(bot + 2 * kN + j0) = o1;
+  }
+  // top row: the expanded row itself in NTT form (gsw.cpp:330-338)
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = ct[(p * 2 + res) * kN + posA(tid, k)];
+    fwdA(v, T);
+    st_plane<0>(sm + p * kPad, v, tid);
   }
   __syncthreads();
-  // top row: the expanded row itself in NTT form (gsw.cpp:330-338)
-  ntt_fwd_planes(D, 2, T);
-  uint32_t *top = out + (uint64_t)r * kCtWords;
+  fwd_mid(sm, 2, T);
+  uint32_t *top = out + (uint64_t)r * kCtWords + res * kN;
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    top[res * kN + j] = D[j];
-    top[2 * kN + res * kN + j] = D[kN + j];
+  for (int p = 0; p < 2; ++p) {
+    uint32_t v[8];
+    ld_plane<3>(sm + p * kPad, v, tid);
+    fwdD(v, T, tid);
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      *reinterpret_cast<uint4 *>(top + p * 2 * kN + 4 * (tid + 256 * h)) =
+          make_uint4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
   }
 }
 
 // ------------------------------------------------------- first-dim query prep
 constexpr int kFstTile = 4;  // ciphertexts per block (8 planes)
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_fst_prep(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
            uint32_t *__restrict__ qmat, uint32_t ncols) {
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y, b = blockIdx.z;
+  const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
   const uint32_t k0 = blockIdx.x * kFstTile;
   const ResidueTables T = pick(P, res);
-  for (int idx = threadIdx.x; idx < 2 * kFstTile * kN; idx += kThreads) {
-    const int e = idx >> kLogN, j = idx & (kN - 1);
-    const uint32_t k = k0 + (e >> 1);
+  for (int e = 0; e < 2 * kFstTile; ++e) {
+    const uint32_t kk = k0 + (e >> 1);
     const int p = e & 1;
-    sm[idx] = k < S.n0 ? leaves[((uint64_t)b * leaf_stride + k) * kCtWords + (p * 2 + res) * kN + j] : 0u;
+    uint32_t v[8];
+    const uint32_t *src = leaves + ((uint64_t)b * leaf_stride + kk) * kCtWords + (p * 2 + res) * kN;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = kk < S.n0 ? src[posA(tid, k)] : 0u;
+    fwdA(v, T);
+    st_plane<0>(sm + e * kPad, v, tid);
   }
   __syncthreads();
-  ntt_fwd_planes(sm, 2 * kFstTile, T);
-  for (int idx = threadIdx.x; idx < 2 * kFstTile * kN; idx += kThreads) {
-    const int l = idx / (2 * kFstTile), e = idx % (2 * kFstTile);
-    const uint32_t k = k0 + (e >> 1);
-    const int p = e & 1;
-    if (k < S.n0)
-      qmat[(((uint64_t)res * kN + l) * S.n0 + k) * ncols + 2 * b + p] = sm[e * kN + l];
+  fwd_mid(sm, 2 * kFstTile, T);
+  uint32_t o[2 * kFstTile][8];
+#pragma unroll
+  for (int e = 0; e < 2 * kFstTile; ++e) {
+    ld_plane<3>(sm + e * kPad, o[e], tid);
+    fwdD(o[e], T, tid);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    uint32_t *dst = qmat + (((uint64_t)res * kN + posD(tid, k)) * S.n0 + k0) * ncols + 2 * b;
+#pragma unroll
+    for (int e = 0; e < 2 * kFstTile; ++e)
+      if (k0 + (e >> 1) < S.n0) dst[(e >> 1) * ncols + (e & 1)] = o[e][k];
   }
 }
 
@@ -366,28 +431,39 @@ k_scan(DevParams P, uint32_t n0, uint32_t m, const uint32_t *__restrict__ db,
 // ----------------------------------------------------------- scan epilogue
 constexpr int kEpiTile = 4;  // candidates per block (8 planes)
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_t ncols,
                 uint32_t *__restrict__ mid, uint64_t mid_stride) {
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y, b = blockIdx.z;
+  const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
   const uint32_t r0 = blockIdx.x * kEpiTile;
   const ResidueTables T = pick(P, res);
-  for (int idx = threadIdx.x; idx < 2 * kEpiTile * kN; idx += kThreads) {
-    const int l = idx / (2 * kEpiTile), e = idx % (2 * kEpiTile);
-    const uint32_t r = r0 + (e >> 1);
-    const int p = e & 1;
-    sm[e * kN + l] = r < S.other
-        ? cmat[(((uint64_t)res * kN + l) * S.other + r) * ncols + 2 * b + p] : 0u;
+  uint32_t v[2 * kEpiTile][8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t *src = cmat + (((uint64_t)res * kN + posD(tid, k)) * S.other + r0) * ncols + 2 * b;
+#pragma unroll
+    for (int e = 0; e < 2 * kEpiTile; ++e)
+      v[e][k] = r0 + (e >> 1) < S.other ? src[(e >> 1) * ncols + (e & 1)] : 0u;
+  }
+#pragma unroll
+  for (int e = 0; e < 2 * kEpiTile; ++e) {
+    invD(v[e], T, tid);
+    st_plane<3>(sm + e * kPad, v[e], tid);
   }
   __syncthreads();
-  ntt_inv_planes(sm, 2 * kEpiTile, T);
-  for (int idx = threadIdx.x; idx < 2 * kEpiTile * kN; idx += kThreads) {
-    const int e = idx >> kLogN, j = idx & (kN - 1);
+  inv_mid(sm, 2 * kEpiTile, T);
+  for (int e = 0; e < 2 * kEpiTile; ++e) {
     const uint32_t r = r0 + (e >> 1);
     const int p = e & 1;
-    if (r < S.other)
-      mid[((uint64_t)b * mid_stride + r) * kCtWords + (p * 2 + res) * kN + j] = sm[idx];
+    uint32_t w[8];
+    ld_plane<0>(sm + e * kPad, w, tid);
+    invA(w, T);
+    if (r < S.other) {
+      uint32_t *dst = mid + ((uint64_t)b * mid_stride + r) * kCtWords + (p * 2 + res) * kN;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) dst[posA(tid, k)] = w[k];
+    }
   }
 }
 
@@ -397,14 +473,14 @@ __global__ void __launch_bounds__(kThreads, 2)
 k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t offset,
             uint32_t half, const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
             uint64_t mid_stride, const uint32_t *__restrict__ sel) {
-  extern __shared__ uint32_t D[];
-  const int res = blockIdx.y, b = blockIdx.z;
+  extern __shared__ uint32_t sm[];
+  const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
   const uint32_t i = blockIdx.x;
   const uint32_t *base_in = in + (uint64_t)b * mid_stride * kCtWords;
   uint32_t *base_out = out + (uint64_t)b * mid_stride * kCtWords;
   if (i >= n_pairs) {  // level 0: carry the unpaired prefix over unchanged
     const uint32_t c = i - n_pairs;
-    for (int j = threadIdx.x; j < kN; j += kThreads) {
+    for (int j = tid; j < kN; j += kThreads) {
       base_out[(uint64_t)c * kCtWords + res * kN + j] = base_in[(uint64_t)c * kCtWords + res * kN + j];
       base_out[(uint64_t)c * kCtWords + 2 * kN + res * kN + j] =
           base_in[(uint64_t)c * kCtWords + 2 * kN + res * kN + j];
@@ -418,24 +494,32 @@ k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t off
   const uint32_t *x = base_in + (uint64_t)xi * kCtWords;
   const uint32_t *y = base_in + (uint64_t)yi * kCtWords;
   const uint32_t *rgsw = sel + ((uint64_t)b * (S.num_dims - 1) + level) * 2 * S.l_ep * kCtWords;
-  uint64_t acc0[kPer], acc1[kPer];
+  uint64_t acc0[8], acc1[8];
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) acc0[s] = acc1[s] = 0;
-  gadget_mac(P, T, res, x, y, rgsw, S.l_ep, S.base_ep, D, acc0, acc1);
+  for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
+  gadget_mac(P, T, res, x, y, rgsw, S.l_ep, S.base_ep, sm, acc0, acc1);
+  {
+    uint32_t v[8], w[8];
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    D[j] = reduce64(acc0[s], T.q, T.mu);
-    D[kN + j] = reduce64(acc1[s], T.q, T.mu);
+    for (int k = 0; k < 8; ++k) { v[k] = reduce64(acc0[k], T.q, T.mu); w[k] = reduce64(acc1[k], T.q, T.mu); }
+    invD(v, T, tid);
+    invD(w, T, tid);
+    st_plane<3>(sm, v, tid);
+    st_plane<3>(sm + kPad, w, tid);
   }
   __syncthreads();
-  ntt_inv_planes(D, 2, T);
+  inv_mid(sm, 2, T);
   uint32_t *o = base_out + (uint64_t)oi * kCtWords;
 #pragma unroll
-  for (int s = 0; s < kPer; ++s) {
-    const int j = threadIdx.x + s * kThreads;
-    o[res * kN + j] = add_mod(x[res * kN + j], D[j], T.q);
-    o[2 * kN + res * kN + j] = add_mod(x[2 * kN + res * kN + j], D[kN + j], T.q);
+  for (int p = 0; p < 2; ++p) {
+    uint32_t v[8];
+    ld_plane<0>(sm + p * kPad, v, tid);
+    invA(v, T);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int j = posA(tid, k);
+      o[(p * 2 + res) * kN + j] = add_mod(x[(p * 2 + res) * kN + j], v[k], T.q);
+    }
   }
 }
 
@@ -509,7 +593,7 @@ void launch_db_preprocess(const DevParams &P, const uint16_t *coeffs, uint64_t c
                           uint64_t seed, uint64_t t, uint64_t logical, uint64_t num_pt,
                           uint64_t pt_begin, uint64_t pt_end, uint32_t *db, cudaStream_t st) {
   if (pt_end <= pt_begin) return;
-  const size_t smem = kDbTile * kN * sizeof(uint32_t);
+  const size_t smem = kDbTile * kPad * sizeof(uint32_t);
   set_smem(k_db_preprocess, smem);
   const uint64_t tiles = (pt_end - pt_begin + kDbTile - 1) / kDbTile;
   dim3 grid(static_cast<unsigned>(tiles), 2);
@@ -523,13 +607,16 @@ void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const u
                          const uint32_t *const *bv_keys, uint64_t bv_level_stride,
                          uint32_t batch, cudaStream_t st) {
   const uint32_t nodes = expand_nodes(s, d);
-  const size_t smem = (3 + s.l_ks) * kN * sizeof(uint32_t);
+  const size_t smem = s.l_ks * kPad * sizeof(uint32_t);
   set_smem(k_expand_level, smem);
   const uint32_t k = 1u << d;
   const uint32_t galois = kN / k + 1;
+  uint32_t galois_inv = 1;  // galois^-1 mod 2N (galois is odd)
+  while (((galois_inv * galois) & (2 * kN - 1)) != 1) galois_inv += 2;
   dim3 grid(nodes, 2, batch);
-  k_expand_level<<<grid, kThreads, smem, st>>>(P, galois, k, s.base_ks, s.l_ks, in, in_stride,
-                                                out, out_stride, bv_keys, d * bv_level_stride);
+  k_expand_level<<<grid, kThreads, smem, st>>>(P, galois_inv, k, s.base_ks, s.l_ks, in,
+                                                in_stride, out, out_stride, bv_keys,
+                                                d * bv_level_stride);
   check_launch("k_expand_level");
 }
 
@@ -537,7 +624,7 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
                       uint64_t leaf_stride, const uint32_t *const *gsw_keys, uint32_t *sel,
                       uint32_t batch, cudaStream_t st) {
   if (s.num_dims <= 1) return;
-  const size_t smem = s.l_key * kN * sizeof(uint32_t);
+  const size_t smem = s.l_key * kPad * sizeof(uint32_t);
   set_smem(k_selectors, smem);
   dim3 grid((s.num_dims - 1) * s.l_ep, 2, batch);
   k_selectors<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
@@ -546,7 +633,7 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
 
 void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
                      uint64_t leaf_stride, uint32_t *qmat, uint32_t batch, cudaStream_t st) {
-  const size_t smem = 2 * kFstTile * kN * sizeof(uint32_t);
+  const size_t smem = 2 * kFstTile * kPad * sizeof(uint32_t);
   set_smem(k_fst_prep, smem);
   dim3 grid((s.n0 + kFstTile - 1) / kFstTile, 2, batch);
   k_fst_prep<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, qmat, 2 * batch);
@@ -580,7 +667,7 @@ void launch_scan(const DevParams &P, const Shape &s, const uint32_t *db, const u
 
 void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cmat, uint32_t *mid,
                           uint64_t mid_stride, uint32_t batch, cudaStream_t st) {
-  const size_t smem = 2 * kEpiTile * kN * sizeof(uint32_t);
+  const size_t smem = 2 * kEpiTile * kPad * sizeof(uint32_t);
   set_smem(k_scan_epilogue, smem);
   dim3 grid((s.other + kEpiTile - 1) / kEpiTile, 2, batch);
   k_scan_epilogue<<<grid, kThreads, smem, st>>>(P, s, cmat, 2 * batch, mid, mid_stride);
@@ -601,7 +688,7 @@ void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, const 
     half = (1u << (h - level)) >> 1;
     n_pairs = half;
   }
-  const size_t smem = s.l_ep * kN * sizeof(uint32_t);
+  const size_t smem = s.l_ep * kPad * sizeof(uint32_t);
   set_smem(k_mux_level, smem);
   dim3 grid(n_pairs + copies, 2, batch);
   k_mux_level<<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,

@@ -146,25 +146,40 @@ void setup_device_params(opir_server *s) {
   const opir_params &p = s->params;
   const auto t1 = opir::make_limb_tables(kN, static_cast<uint32_t>(p.q1), static_cast<uint32_t>(p.w1));
   const auto t2 = opir::make_limb_tables(kN, static_cast<uint32_t>(p.q2), static_cast<uint32_t>(p.w2));
-  std::vector<uint32_t> host(8 * kN);
+  // per residue: fw, fw_sh, iw, iw_sh (kN each), then (fw, fw_sh) and
+  // (iw, iw_sh) interleaved (2 kN each)
+  std::vector<uint32_t> host(16 * kN);
   const opir::LimbTables *ts[2] = {&t1, &t2};
   for (int r = 0; r < 2; ++r) {
-    std::copy(ts[r]->fw.begin(), ts[r]->fw.end(), host.begin() + (r * 4 + 0) * kN);
-    std::copy(ts[r]->fw_sh.begin(), ts[r]->fw_sh.end(), host.begin() + (r * 4 + 1) * kN);
-    std::copy(ts[r]->iw.begin(), ts[r]->iw.end(), host.begin() + (r * 4 + 2) * kN);
-    std::copy(ts[r]->iw_sh.begin(), ts[r]->iw_sh.end(), host.begin() + (r * 4 + 3) * kN);
+    uint32_t *h = host.data() + r * 8 * kN;
+    std::copy(ts[r]->fw.begin(), ts[r]->fw.end(), h + 0 * kN);
+    std::copy(ts[r]->fw_sh.begin(), ts[r]->fw_sh.end(), h + 1 * kN);
+    std::copy(ts[r]->iw.begin(), ts[r]->iw.end(), h + 2 * kN);
+    std::copy(ts[r]->iw_sh.begin(), ts[r]->iw_sh.end(), h + 3 * kN);
+    for (int i = 0; i < kN; ++i) {
+      h[4 * kN + 2 * i] = ts[r]->fw[i];
+      h[4 * kN + 2 * i + 1] = ts[r]->fw_sh[i];
+      h[6 * kN + 2 * i] = ts[r]->iw[i];
+      h[6 * kN + 2 * i + 1] = ts[r]->iw_sh[i];
+    }
   }
   s->tables.alloc(host.size());
   ck(cudaMemcpy(s->tables.p, host.data(), host.size() * 4, cudaMemcpyHostToDevice), "tables");
   opir::DevParams &d = s->dp;
   for (int r = 0; r < 2; ++r) {
-    d.r[r].fw = s->tables.p + (r * 4 + 0) * kN;
-    d.r[r].fw_sh = s->tables.p + (r * 4 + 1) * kN;
-    d.r[r].iw = s->tables.p + (r * 4 + 2) * kN;
-    d.r[r].iw_sh = s->tables.p + (r * 4 + 3) * kN;
+    uint32_t *base = s->tables.p + r * 8 * kN;
+    d.r[r].fw = base + 0 * kN;
+    d.r[r].fw_sh = base + 1 * kN;
+    d.r[r].iw = base + 2 * kN;
+    d.r[r].iw_sh = base + 3 * kN;
+    d.r[r].fwt = reinterpret_cast<const uint2 *>(base + 4 * kN);
+    d.r[r].iwt = reinterpret_cast<const uint2 *>(base + 6 * kN);
     d.r[r].q = ts[r]->q;
     d.r[r].n_inv = ts[r]->n_inv;
     d.r[r].n_inv_sh = ts[r]->n_inv_sh;
+    const uint32_t w1n = static_cast<uint32_t>(static_cast<uint64_t>(ts[r]->iw[1]) * ts[r]->n_inv % ts[r]->q);
+    d.r[r].w1_ninv = w1n;
+    d.r[r].w1_ninv_sh = static_cast<uint32_t>((static_cast<uint64_t>(w1n) << 32) / ts[r]->q);
     d.r[r].mu = ts[r]->mu;
   }
   d.q = p.q;
