@@ -14,8 +14,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libonionpir_b200.so")
-SOURCES = ["opir_kernels.cu", "opir_server.cu", "opir_params.cpp", "opir_noalloc.cu"]
-HEADERS = ["opir_device.cuh", "opir_kernels.h", "opir_params.h"]
+SOURCES = ["opir_kernels.cu", "opir_server.cu", "opir_params.cpp", "opir_noalloc.cu",
+           "opir_scan_tc.cu"]
+HEADERS = ["opir_device.cuh", "opir_kernels.h", "opir_params.h", "opir_scan_tc.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
                      "--expt-relaxed-constexpr"]

@@ -88,8 +88,8 @@ constexpr int kDbTile = 8;  // plaintexts per block (one padded plane each)
 __global__ void __launch_bounds__(kThreads, 2)
 k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
                 uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
-                uint64_t logical, uint64_t num_pt, uint64_t pt_begin,
-                uint64_t pt_end, uint32_t *__restrict__ db) {
+                uint64_t logical, uint32_t n0, uint32_t n0p, uint32_t other,
+                uint64_t pt_begin, uint64_t pt_end, uint8_t *__restrict__ db8) {
   extern __shared__ uint32_t sm[];
   const int res = blockIdx.y, tid = threadIdx.x;
   const ResidueTables T = pick(P, res);
@@ -120,13 +120,31 @@ k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
     ld_plane<3>(sm + e * kPad, out[e], tid);
     fwdD(out[e], T, tid);
   }
-  uint32_t *dbr = db + (uint64_t)res * kN * num_pt;
+  // byte planes: db8[((res N + level) 4 + plane) other + row][n0p], pt = row n0 + k
+  const bool packed = (n0 % kDbTile) == 0 && pt0 + kDbTile <= pt_end;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    uint32_t *row = dbr + (uint64_t)posD(tid, k) * num_pt + pt0;
+    const uint64_t zl = (uint64_t)res * kN + posD(tid, k);
 #pragma unroll
-    for (int e = 0; e < kDbTile; ++e)
-      if (pt0 + e < pt_end) row[e] = out[e][k];
+    for (int j = 0; j < 4; ++j) {
+      uint8_t *plane = db8 + (zl * 4 + j) * (uint64_t)other * n0p;
+      if (packed) {
+        const uint64_t row = pt0 / n0, col = pt0 % n0;
+        uint32_t lo = 0, hi = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          lo |= ((out[e][k] >> (8 * j)) & 0xFFu) << (8 * e);
+          hi |= ((out[e + 4][k] >> (8 * j)) & 0xFFu) << (8 * e);
+        }
+        *reinterpret_cast<uint2 *>(plane + row * n0p + col) = make_uint2(lo, hi);
+      } else {
+        for (int e = 0; e < kDbTile; ++e) {
+          const uint64_t pt = pt0 + e;
+          if (pt < pt_end)
+            plane[(pt / n0) * n0p + pt % n0] = static_cast<uint8_t>(out[e][k] >> (8 * j));
+        }
+      }
+    }
   }
 }
 
@@ -338,7 +356,7 @@ constexpr int kFstTile = 4;  // ciphertexts per block (8 planes)
 
 __global__ void __launch_bounds__(kThreads, 2)
 k_fst_prep(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
-           uint32_t *__restrict__ qmat, uint32_t ncols) {
+           uint8_t *__restrict__ qb, uint32_t ncols, uint32_t n0p) {
   extern __shared__ uint32_t sm[];
   const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
   const uint32_t k0 = blockIdx.x * kFstTile;
@@ -361,61 +379,101 @@ k_fst_prep(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t l
     ld_plane<3>(sm + e * kPad, o[e], tid);
     fwdD(o[e], T, tid);
   }
+  // qb[((res N + level) 4 + plane) ncols + column][n0p]: the four first-
+  // dimension indices k0..k0+3 of one column pack into one 32-bit word
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    uint32_t *dst = qmat + (((uint64_t)res * kN + posD(tid, k)) * S.n0 + k0) * ncols + 2 * b;
+    const uint64_t zl = (uint64_t)res * kN + posD(tid, k);
 #pragma unroll
-    for (int e = 0; e < 2 * kFstTile; ++e)
-      if (k0 + (e >> 1) < S.n0) dst[(e >> 1) * ncols + (e & 1)] = o[e][k];
+    for (int p = 0; p < 2; ++p) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int kk = 0; kk < kFstTile; ++kk) w |= ((o[kk * 2 + p][k] >> (8 * j)) & 0xFFu) << (8 * kk);
+        *reinterpret_cast<uint32_t *>(qb + ((zl * 4 + j) * ncols + 2 * b + p) * n0p + k0) = w;
+      }
+    }
   }
 }
 
 // ------------------------------------------------------------ first-dim scan
-// Block = (column tile, NTT level, residue). A warp owns one database row at a
-// time; its lanes split the first dimension k, accumulate exact 64-bit sums
-// of 29x29-bit products (at most 64 per lane, so no overflow), reduce them
-// mod q and finish with a shuffle tree of modular adds. The query tile is
-// staged transposed in shared memory ([column][k]) so each lane reads its
-// four k values per column with one 16-byte load.
+// CUDA-core form (used for small batches): block = (column tile, residue x
+// level); a warp owns one database row at a time, its lanes split the first
+// dimension, accumulate exact 64-bit sums of 29x29-bit products (at most 64
+// per lane, so no overflow), reduce mod q and finish with a shuffle tree of
+// modular adds. Operands are the byte planes also used by the tensor-core
+// form; values are rebuilt with byte permutes.
+__device__ __forceinline__ void unpack16(const uint4 &p0, const uint4 &p1, const uint4 &p2,
+                                         const uint4 &p3, uint32_t (&a)[16]) {
+  const uint32_t x0[4] = {p0.x, p0.y, p0.z, p0.w}, x1[4] = {p1.x, p1.y, p1.z, p1.w};
+  const uint32_t x2[4] = {p2.x, p2.y, p2.z, p2.w}, x3[4] = {p3.x, p3.y, p3.z, p3.w};
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const uint32_t lo01 = __byte_perm(x0[w], x1[w], 0x5140), lo23 = __byte_perm(x2[w], x3[w], 0x5140);
+    const uint32_t hi01 = __byte_perm(x0[w], x1[w], 0x7362), hi23 = __byte_perm(x2[w], x3[w], 0x7362);
+    a[4 * w + 0] = __byte_perm(lo01, lo23, 0x5410);
+    a[4 * w + 1] = __byte_perm(lo01, lo23, 0x7632);
+    a[4 * w + 2] = __byte_perm(hi01, hi23, 0x5410);
+    a[4 * w + 3] = __byte_perm(hi01, hi23, 0x7632);
+  }
+}
+
 template <int NCT, bool VEC>
 __global__ void __launch_bounds__(kThreads)
-k_scan(DevParams P, uint32_t n0, uint32_t m, const uint32_t *__restrict__ db,
-       uint64_t num_pt, const uint32_t *__restrict__ qmat, uint32_t ncols,
-       uint32_t *__restrict__ cmat) {
-  extern __shared__ __align__(16) uint32_t qs[];  // [NCT][n0]
+k_scan(DevParams P, uint32_t n0, uint32_t n0p, uint32_t m, const uint8_t *__restrict__ db8,
+       const uint8_t *__restrict__ qb, uint32_t ncols, uint32_t *__restrict__ cmat) {
+  extern __shared__ __align__(16) uint32_t qs[];  // [NCT][n0p]
   const int ct0 = blockIdx.x * NCT;
-  const int l = blockIdx.y, res = blockIdx.z;
+  const uint32_t z = blockIdx.y;
+  const int res = z >= kN ? 1 : 0;
   const uint32_t q = res ? P.q2 : P.q1;
   const uint64_t mu = res ? P.r[1].mu : P.r[0].mu;
-  const uint32_t *Q = qmat + ((uint64_t)res * kN + l) * n0 * ncols;
-  for (uint32_t idx = threadIdx.x; idx < n0 * NCT; idx += kThreads) {
-    const uint32_t k = idx / NCT, c = idx % NCT;
-    qs[c * n0 + k] = (ct0 + c < (int)ncols) ? Q[(uint64_t)k * ncols + ct0 + c] : 0u;
+  for (uint32_t idx = threadIdx.x; idx < n0p * NCT; idx += kThreads) {
+    const uint32_t c = idx / n0p, k = idx % n0p;
+    uint32_t v = 0;
+    if (ct0 + c < ncols && k < n0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        v |= static_cast<uint32_t>(qb[(((uint64_t)z * 4 + j) * ncols + ct0 + c) * n0p + k]) << (8 * j);
+    }
+    qs[c * n0p + k] = v;
   }
   __syncthreads();
-  const uint32_t *A = db + ((uint64_t)res * kN + l) * num_pt;
-  uint32_t *C = cmat + ((uint64_t)res * kN + l) * m * ncols;
+  const uint64_t plane_stride = (uint64_t)m * n0p;
+  const uint8_t *A = db8 + (uint64_t)z * 4 * plane_stride;
+  uint32_t *C = cmat + (uint64_t)z * m * ncols;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint32_t r = warp; r < m; r += kThreads / 32) {
-    const uint32_t *Ar = A + (uint64_t)r * n0;
+    const uint8_t *Ar = A + (uint64_t)r * n0p;
     uint64_t acc[NCT];
 #pragma unroll
     for (int c = 0; c < NCT; ++c) acc[c] = 0;
     if (VEC) {
-      for (uint32_t k = 4 * lane; k < n0; k += 128) {
-        const uint4 a = __ldg(reinterpret_cast<const uint4 *>(Ar + k));
+      for (uint32_t k = 16 * lane; k < n0p; k += 512) {
+        const uint4 p0 = __ldg(reinterpret_cast<const uint4 *>(Ar + k));
+        const uint4 p1 = __ldg(reinterpret_cast<const uint4 *>(Ar + plane_stride + k));
+        const uint4 p2 = __ldg(reinterpret_cast<const uint4 *>(Ar + 2 * plane_stride + k));
+        const uint4 p3 = __ldg(reinterpret_cast<const uint4 *>(Ar + 3 * plane_stride + k));
+        uint32_t a[16];
+        unpack16(p0, p1, p2, p3, a);
 #pragma unroll
         for (int c = 0; c < NCT; ++c) {
-          const uint4 b = *reinterpret_cast<const uint4 *>(qs + c * n0 + k);
-          acc[c] += (uint64_t)a.x * b.x + (uint64_t)a.y * b.y;
-          acc[c] += (uint64_t)a.z * b.z + (uint64_t)a.w * b.w;
+#pragma unroll
+          for (int w = 0; w < 4; ++w) {
+            const uint4 b = *reinterpret_cast<const uint4 *>(qs + c * n0p + k + 4 * w);
+            acc[c] += (uint64_t)a[4 * w] * b.x + (uint64_t)a[4 * w + 1] * b.y;
+            acc[c] += (uint64_t)a[4 * w + 2] * b.z + (uint64_t)a[4 * w + 3] * b.w;
+          }
         }
       }
     } else {
       for (uint32_t k = lane; k < n0; k += 32) {
-        const uint64_t a = __ldg(Ar + k);
+        const uint64_t a = Ar[k] | (uint32_t)Ar[plane_stride + k] << 8 |
+                           (uint32_t)Ar[2 * plane_stride + k] << 16 |
+                           (uint32_t)Ar[3 * plane_stride + k] << 24;
 #pragma unroll
-        for (int c = 0; c < NCT; ++c) acc[c] += a * qs[c * n0 + k];
+        for (int c = 0; c < NCT; ++c) acc[c] += a * qs[c * n0p + k];
       }
     }
 #pragma unroll
@@ -589,16 +647,16 @@ void launch_compose_u64(const DevParams &P, const uint32_t *in, uint64_t in_item
   check_launch("k_compose_u64");
 }
 
-void launch_db_preprocess(const DevParams &P, const uint16_t *coeffs, uint64_t coeff_pt_begin,
-                          uint64_t seed, uint64_t t, uint64_t logical, uint64_t num_pt,
-                          uint64_t pt_begin, uint64_t pt_end, uint32_t *db, cudaStream_t st) {
+void launch_db_preprocess(const DevParams &P, const Shape &s, const uint16_t *coeffs,
+                          uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
+                          uint64_t pt_begin, uint64_t pt_end, uint8_t *db8, cudaStream_t st) {
   if (pt_end <= pt_begin) return;
   const size_t smem = kDbTile * kPad * sizeof(uint32_t);
   set_smem(k_db_preprocess, smem);
   const uint64_t tiles = (pt_end - pt_begin + kDbTile - 1) / kDbTile;
   dim3 grid(static_cast<unsigned>(tiles), 2);
-  k_db_preprocess<<<grid, kThreads, smem, st>>>(P, coeffs, coeff_pt_begin, seed, t, logical,
-                                                 num_pt, pt_begin, pt_end, db);
+  k_db_preprocess<<<grid, kThreads, smem, st>>>(P, coeffs, coeff_pt_begin, seed, t, logical, s.n0,
+                                                 s.n0p, s.other, pt_begin, pt_end, db8);
   check_launch("k_db_preprocess");
 }
 
@@ -632,37 +690,36 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
 }
 
 void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
-                     uint64_t leaf_stride, uint32_t *qmat, uint32_t batch, cudaStream_t st) {
+                     uint64_t leaf_stride, uint8_t *qb, uint32_t batch, cudaStream_t st) {
   const size_t smem = 2 * kFstTile * kPad * sizeof(uint32_t);
   set_smem(k_fst_prep, smem);
   dim3 grid((s.n0 + kFstTile - 1) / kFstTile, 2, batch);
-  k_fst_prep<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, qmat, 2 * batch);
+  k_fst_prep<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, qb, 2 * batch, s.n0p);
   check_launch("k_fst_prep");
 }
 
 template <int NCT>
-static void scan_dispatch(const DevParams &P, const Shape &s, const uint32_t *db,
-                          const uint32_t *qmat, uint32_t *cmat, uint32_t ncols,
-                          cudaStream_t st) {
-  const size_t smem = (size_t)NCT * s.n0 * sizeof(uint32_t);
-  dim3 grid((ncols + NCT - 1) / NCT, kN, 2);
-  if (s.n0 % 128 == 0) {
+static void scan_dispatch(const DevParams &P, const Shape &s, const uint8_t *db8, const uint8_t *qb,
+                          uint32_t *cmat, uint32_t ncols, cudaStream_t st) {
+  const size_t smem = (size_t)NCT * s.n0p * sizeof(uint32_t);
+  dim3 grid((ncols + NCT - 1) / NCT, 2 * kN);
+  if (s.n0 % 16 == 0) {
     set_smem(k_scan<NCT, true>, smem);
-    k_scan<NCT, true><<<grid, kThreads, smem, st>>>(P, s.n0, s.other, db, s.num_pt, qmat, ncols, cmat);
+    k_scan<NCT, true><<<grid, kThreads, smem, st>>>(P, s.n0, s.n0p, s.other, db8, qb, ncols, cmat);
   } else {
     set_smem(k_scan<NCT, false>, smem);
-    k_scan<NCT, false><<<grid, kThreads, smem, st>>>(P, s.n0, s.other, db, s.num_pt, qmat, ncols, cmat);
+    k_scan<NCT, false><<<grid, kThreads, smem, st>>>(P, s.n0, s.n0p, s.other, db8, qb, ncols, cmat);
   }
   check_launch("k_scan");
 }
 
-void launch_scan(const DevParams &P, const Shape &s, const uint32_t *db, const uint32_t *qmat,
+void launch_scan(const DevParams &P, const Shape &s, const uint8_t *db8, const uint8_t *qb,
                  uint32_t *cmat, uint32_t batch, cudaStream_t st) {
   const uint32_t ncols = 2 * batch;
-  if (ncols <= 2) scan_dispatch<2>(P, s, db, qmat, cmat, ncols, st);
-  else if (ncols <= 4) scan_dispatch<4>(P, s, db, qmat, cmat, ncols, st);
-  else if (ncols <= 8) scan_dispatch<8>(P, s, db, qmat, cmat, ncols, st);
-  else scan_dispatch<16>(P, s, db, qmat, cmat, ncols, st);
+  if (ncols <= 2) scan_dispatch<2>(P, s, db8, qb, cmat, ncols, st);
+  else if (ncols <= 4) scan_dispatch<4>(P, s, db8, qb, cmat, ncols, st);
+  else if (ncols <= 8) scan_dispatch<8>(P, s, db8, qb, cmat, ncols, st);
+  else scan_dispatch<16>(P, s, db8, qb, cmat, ncols, st);
 }
 
 void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cmat, uint32_t *mid,

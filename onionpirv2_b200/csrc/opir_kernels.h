@@ -18,6 +18,7 @@ struct Shape {
   uint32_t useful;      // n0 + l_ep (num_dims - 1)
   uint32_t l_ep, l_key, l_ks;
   uint32_t base_ep, base_key, base_ks;
+  uint32_t n0p;         // n0 rounded up to 16 (byte-plane row length)
   uint64_t num_pt;
 };
 
@@ -41,12 +42,13 @@ void launch_compose_u64(const DevParams &P, const uint32_t *in, uint64_t in_item
 
 // Database preprocessing (src/server.cpp:80-171): plaintexts [pt][N] (u16,
 // or generated from `seed` when coeffs == nullptr) -> NTT -> residues ->
-// db[res][coeff][pt]. Covers plaintexts [pt_begin, pt_end) of a database of
-// num_pt plaintexts; rows >= logical are zero.
-void launch_db_preprocess(const DevParams &P, const uint16_t *coeffs,
+// byte planes db8[((res N + level) 4 + plane) other + row][n0p] with
+// pt = row n0 + k. Covers plaintexts [pt_begin, pt_end); rows >= logical are
+// zero. Padding bytes (k >= n0) are never written: the buffer starts zeroed.
+void launch_db_preprocess(const DevParams &P, const Shape &s, const uint16_t *coeffs,
                           uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
-                          uint64_t logical, uint64_t num_pt, uint64_t pt_begin,
-                          uint64_t pt_end, uint32_t *db, cudaStream_t st);
+                          uint64_t logical, uint64_t pt_begin, uint64_t pt_end,
+                          uint8_t *db8, cudaStream_t st);
 
 // One expansion level d over `batch` queries. in: batch x in_stride cts,
 // out: batch x out_stride cts. bv_level[b] points at the (galois level d) key
@@ -64,16 +66,17 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
                       uint32_t *sel, uint32_t batch, cudaStream_t st);
 
 // First-dimension query matrix (src/server.cpp:332-346 + 264-304): NTT of the
-// first n0 leaves of each query, written as qmat[res][level][k][2*batch].
+// first n0 leaves of each query, written as byte planes
+// qb[((res N + level) 4 + plane) 2 batch + column][n0p], column = 2 b + poly.
 void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
-                     uint64_t leaf_stride, uint32_t *qmat, uint32_t batch,
+                     uint64_t leaf_stride, uint8_t *qb, uint32_t batch,
                      cudaStream_t st);
 
-// First-dimension scan (matrix.cpp:240-350): per residue and NTT level,
-// C[res][l][r][c] = sum_k db[res][l][r*n0 + k] * qmat[res][l][k][c] mod q_res,
-// c < 2*batch.
-void launch_scan(const DevParams &P, const Shape &s, const uint32_t *db,
-                 const uint32_t *qmat, uint32_t *cmat, uint32_t batch,
+// First-dimension scan on CUDA cores (matrix.cpp:240-350): per residue and
+// NTT level, C[res][l][r][c] = sum_k A[r][k] Q[k][c] mod q_res, c < 2 batch,
+// with A and Q rebuilt from their byte planes.
+void launch_scan(const DevParams &P, const Shape &s, const uint8_t *db8,
+                 const uint8_t *qb, uint32_t *cmat, uint32_t batch,
                  cudaStream_t st);
 
 // Gather + INTT of the scan output into candidate ciphertexts

@@ -1,0 +1,371 @@
+// First-dimension scan on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Per residue r and NTT level l the scan is C = A . Q mod q_r with
+// A = database rows [other x n0] and Q = query columns [n0 x 2B], all values
+// < 2^29 (matrix.cpp:240-350, the reference's level_mat_mat_32). Both operands
+// are stored as four byte planes (A = sum_i 2^(8i) A_i, Q = sum_j 2^(8j) Q_j),
+// so C = sum_{i,j} 2^(8(i+j)) A_i . Q_j. Every A_i . Q_j is an exact
+// unsigned-int8 MMA with int32 accumulation (n0 <= 2048 so a sum of at most
+// 2048 products of 255 x 255 stays below 2^31 per byte pair; pairs with the
+// same shift s = i + j share one accumulator, at most 4 pairs: < 2^31 for
+// n0 <= 8192). The epilogue recombines the seven accumulators
+// sum_s P_s 2^(8s) mod q in exact 64-bit arithmetic.
+//
+// Structure: persistent CTAs (one per SM), 6 warps:
+//   warp 0      TMA producer: 3-D tiled loads (128B swizzle) of 4 A planes
+//               [128 rows x 128 B] and 4 Q planes [ntile x 128 B] per stage
+//   warp 1      TMEM owner + MMA issuer (one elected lane)
+//   warps 2..5  epilogue: tcgen05.ld of the accumulators, recombination,
+//               modular reduction, stores of C
+// Two smem stages ring between producer and MMA; one TMEM accumulator set
+// (7 x ntile columns) rings between MMA and epilogue. Every mbarrier wait is
+// bounded in time; on timeout the kernel records an error code, drains its
+// own in-flight copies and MMAs, frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "opir_scan_tc.h"
+
+namespace opir {
+
+namespace {
+
+constexpr int kM = 128;          // MMA M / rows per tile
+constexpr int kKT = 128;         // K bytes per stage (one 128B swizzle atom)
+constexpr int kStages = 2;
+constexpr int kThreadsTc = 192;
+constexpr uint32_t kTmemCols = 512;
+constexpr long long kWaitCycles = 1ll << 31;  // ~1 s at 2 GHz
+
+__device__ __forceinline__ uint32_t sa(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(sa(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false on timeout or when another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag) {
+  const long long t0 = clock64();
+  while (!mbar_try(b, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa(b)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(sa(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(sa(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Shared-memory matrix descriptor: K-major, 128B swizzle, 8-row groups of
+// 128-byte rows (SBO = 1024 B), Blackwell descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>(1) << 16;              // LBO (unused when swizzled)
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;      // SBO
+  d |= static_cast<uint64_t>(1) << 46;              // version
+  d |= static_cast<uint64_t>(2) << 61;              // SWIZZLE_128B
+  return d;
+}
+__device__ __forceinline__ void mma_u8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sa(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t (&r)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
+      : "r"(addr)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t reduce64_tc(uint64_t x, uint32_t q, uint64_t mu) {
+  const uint64_t qhat = __umul64hi(x, mu);
+  uint64_t r = x - qhat * q;
+  if (r >= q) r -= q;
+  if (r >= q) r -= q;
+  return static_cast<uint32_t>(r);
+}
+
+__global__ void __launch_bounds__(kThreadsTc, 1)
+k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmQ,
+          TcScanArgs a) {
+  extern __shared__ __align__(1024) uint8_t smraw[];
+  uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smraw) + 1023) &
+                                            ~static_cast<uintptr_t>(1023));
+  const uint32_t a_plane = kM * kKT;               // 16 KiB
+  const uint32_t q_plane = a.ntile * kKT;          // ntile * 128 B
+  const uint32_t stage_bytes = 4 * a_plane + 4 * q_plane;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + kStages * stage_bytes);
+  uint64_t *empty = full + kStages;
+  uint64_t *acc_full = empty + kStages;
+  uint64_t *acc_empty = acc_full + 1;
+  uint64_t *drain = acc_empty + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 128);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     sa(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t per_z = a.col_tiles * a.m_tiles;
+  const uint32_t n_items = per_z * a.zcount;
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    uint32_t stage = 0, phase = 0, issued[kStages] = {0, 0};
+    bool ok = true;
+    for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+      const uint32_t ct = it % a.col_tiles, mt = (it / a.col_tiles) % a.m_tiles, z = it / per_z;
+      for (uint32_t kt = 0; ok && kt < a.k_tiles; ++kt) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) { ok = false; break; }
+        if (lane == 0) {
+          uint8_t *st = sm + stage * stage_bytes;
+          mbar_expect_tx(&full[stage], stage_bytes);
+          for (int pl = 0; pl < 4; ++pl)
+            tma_load_3d(st + pl * a_plane, &tmA, &full[stage], kt * kKT, mt * kM, z * 4 + pl);
+          for (int pl = 0; pl < 4; ++pl)
+            tma_load_3d(st + 4 * a_plane + pl * q_plane, &tmQ, &full[stage], kt * kKT,
+                        ct * a.ntile, z * 4 + pl);
+        }
+        __syncwarp();
+        ++issued[stage];
+        if (++stage == kStages) { stage = 0; phase ^= 1; }
+      }
+    }
+    if (!ok) {
+      if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 1u); }
+    }
+    // own copies in flight must land before the CTA may exit
+    for (int s = 0; s < kStages; ++s) {
+      if (issued[s] == 0) continue;
+      const long long t0 = clock64();
+      while (!mbar_try(&full[s], (issued[s] - 1) & 1)) {
+        if (clock64() - t0 > kWaitCycles) { if (lane == 0) atomicOr(a.err, 8u); break; }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------- MMA issuer
+    const uint32_t idesc = (2u << 4)                                  // D: s32
+                           | (static_cast<uint32_t>(a.ntile >> 3) << 17)  // N
+                           | (static_cast<uint32_t>(kM >> 4) << 24);       // M
+    // A, B: unsigned 8-bit, K-major, dense
+    uint32_t stage = 0, phase = 0, acc_phase = 0;
+    bool ok = true;
+    for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
+      if (!mbar_wait(acc_empty, acc_phase ^ 1, abort_flag)) { ok = false; break; }
+      fence_after();
+      for (uint32_t kt = 0; kt < a.k_tiles; ++kt) {
+        if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
+        fence_after();
+        if (lane == 0) {
+          const uint32_t base = sa(sm + stage * stage_bytes);
+#pragma unroll
+          for (int ks = 0; ks < kKT / 32; ++ks) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const int s = i + j;
+                const int first_i = s > 3 ? s - 3 : 0;
+                const uint32_t acc = (kt | ks) != 0 || i != first_i;
+                const uint64_t da = sw128_desc(base + i * a_plane + ks * 32);
+                const uint64_t db = sw128_desc(base + 4 * a_plane + j * q_plane + ks * 32);
+                mma_u8(tmem + s * a.ntile, da, db, idesc, acc);
+              }
+            }
+          }
+          mma_commit(&empty[stage]);  // frees the stage when these MMAs finish
+        }
+        __syncwarp();
+        if (++stage == kStages) { stage = 0; phase ^= 1; }
+      }
+      if (!ok) break;
+      if (lane == 0) mma_commit(acc_full);
+      __syncwarp();
+      acc_phase ^= 1;
+    }
+    if (!ok && lane == 0) { *abort_flag = 1; atomicOr(a.err, 2u); }
+    // all MMAs issued by this thread must finish before TMEM is released
+    if (lane == 0) mma_commit(drain);
+    __syncwarp();
+    const long long t0 = clock64();
+    while (!mbar_try(drain, 0)) {
+      if (clock64() - t0 > kWaitCycles) { if (lane == 0) atomicOr(a.err, 16u); break; }
+    }
+  } else {
+    // --------------------------------------------------------- epilogue
+    const int quad = warp & 3;             // TMEM lane quadrant of this warp
+    const int row = quad * 32 + lane;
+    uint32_t acc_phase = 0;
+    for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+      if (!mbar_wait(acc_full, acc_phase, abort_flag)) {
+        if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 4u); }
+        break;
+      }
+      fence_after();
+      const uint32_t ct = it % a.col_tiles, mt = (it / a.col_tiles) % a.m_tiles, z = it / per_z;
+      const int res = z >= a.levels_per_res ? 1 : 0;
+      const uint32_t q = a.q[res];
+      const uint64_t mu = a.mu[res];
+      const uint32_t m = mt * kM + row;
+      uint32_t *dst = a.cmat + (static_cast<uint64_t>(z) * a.other + m) * a.ncols;
+      const uint32_t col0 = ct * a.ntile;
+      for (uint32_t c0 = 0; c0 < a.ntile; c0 += 8) {
+        uint32_t P[7][8];
+#pragma unroll
+        for (int s = 0; s < 7; ++s)
+          tmem_ld8(tmem + (static_cast<uint32_t>(quad * 32) << 16) + s * a.ntile + c0, P[s]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          uint64_t acc = 0;
+#pragma unroll
+          for (int s = 0; s < 7; ++s) acc += static_cast<uint64_t>(P[s][c]) * a.w[res][s];
+          const uint32_t col = col0 + c0 + c;
+          if (m < a.other && col < a.ncols) dst[col] = reduce64_tc(acc, q, mu);
+        }
+      }
+      fence_before();
+      mbar_arrive(acc_empty);
+      acc_phase ^= 1;
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || p == nullptr)
+      throw std::runtime_error("cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+// 3-D byte tensor [planes][rows][k] (k innermost, row stride = k_bytes),
+// boxes of [1][box_rows][128] with 128B swizzle; out-of-range rows read 0.
+void make_plane_map(CUtensorMap *map, const uint8_t *base, uint64_t k_bytes, uint64_t rows,
+                    uint64_t planes, uint32_t box_rows) {
+  if (k_bytes % 16 != 0) throw std::invalid_argument("plane row stride must be a multiple of 16");
+  const cuuint64_t dims[3] = {k_bytes, rows, planes};
+  const cuuint64_t strides[2] = {k_bytes, k_bytes * rows};
+  const cuuint32_t box[3] = {static_cast<cuuint32_t>(kKT), box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
+                                 const_cast<uint8_t *>(base), dims, strides, box, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string(static_cast<int>(r)));
+}
+
+size_t scan_tc_smem(uint32_t ntile) {
+  return 1024 + kStages * (4ull * kM * kKT + 4ull * ntile * kKT) + 128;
+}
+
+void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcScanArgs &args,
+                    int sm_count, cudaStream_t st) {
+  const size_t smem = scan_tc_smem(args.ntile);
+  static int configured_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (configured_dev != dev) {
+    const cudaError_t e = cudaFuncSetAttribute(k_scan_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(scan_tc_smem(64)));
+    if (e != cudaSuccess)
+      throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    configured_dev = dev;
+  }
+  const uint64_t items = static_cast<uint64_t>(args.col_tiles) * args.m_tiles * args.zcount;
+  const unsigned grid = static_cast<unsigned>(items < static_cast<uint64_t>(sm_count) ? items : sm_count);
+  k_scan_tc<<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw std::runtime_error(std::string("k_scan_tc: ") + cudaGetErrorString(e));
+}
+
+}  // namespace opir

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -15,6 +16,7 @@
 #include "../../include/onionpir_b200.h"
 #include "opir_kernels.h"
 #include "opir_params.h"
+#include "opir_scan_tc.h"
 
 namespace {
 
@@ -84,8 +86,12 @@ struct opir_server {
   int device = 0;
   cudaStream_t stream = nullptr;
   DevBuf<uint32_t> tables;
-  DevBuf<uint32_t> db;
+  DevBuf<uint8_t> db8;       // byte-plane database, see opir_kernels.h
   bool db_loaded = false;
+  CUtensorMap map_db{};      // TMA view of db8 for the tensor-core scan
+  int sm_count = 148;
+  int scan_mode = 0;         // 0 auto, 1 tensor cores, 2 CUDA cores
+  DevBuf<uint32_t> err;      // device error word of the tensor-core scan
   std::unordered_map<uint64_t, ClientKeys> clients;
   std::string last_error;
   // scratch arena (sized for `cap` queries)
@@ -93,7 +99,8 @@ struct opir_server {
   uint64_t lvl_slots = 1;   // ciphertext slots per query in an expansion buffer
   DevBuf<uint64_t> q_u64, resp_u64;
   DevBuf<uint8_t> resp_bytes;
-  DevBuf<uint32_t> lvl[2], sel, qmat, cmat, mid[2];
+  DevBuf<uint32_t> lvl[2], sel, cmat, mid[2];
+  DevBuf<uint8_t> qb;        // byte-plane first-dimension query matrix
   DevBuf<const uint32_t *> keyptrs;
   std::vector<const uint32_t *> host_keyptrs;
   // stage timing: one event set per timed call, averaged on request
@@ -204,6 +211,7 @@ void setup_device_params(opir_server *s) {
   sh.base_key = p.base_log2_key;
   sh.base_ks = p.base_log2_ks;
   sh.num_pt = p.num_pt;
+  sh.n0p = static_cast<uint32_t>((p.fst_dim_sz + 15) / 16 * 16);
   uint64_t slots = 1;
   for (uint32_t d2 = 0; d2 < sh.h; ++d2) slots = std::max<uint64_t>(slots, 2ull * opir::expand_nodes(sh, d2));
   s->lvl_slots = std::max<uint64_t>(slots, sh.useful);
@@ -219,7 +227,7 @@ void ensure_capacity(opir_server *s, uint32_t n) {
   s->resp_bytes.alloc(static_cast<size_t>(n) * resp_bytes_of(s->params));
   for (auto &b : s->lvl) b.alloc(n * s->lvl_slots * ct);
   s->sel.alloc(std::max<uint64_t>(1, n * nsel * 2 * sh.l_ep * ct));
-  s->qmat.alloc(2ull * kN * sh.n0 * 2 * n);
+  s->qb.alloc(2ull * kN * 4 * 2 * n * sh.n0p);
   s->cmat.alloc(2ull * kN * sh.other * 2 * n);
   for (auto &b : s->mid) b.alloc(static_cast<size_t>(n) * sh.other * ct);
   s->keyptrs.alloc(2ull * n);
@@ -270,12 +278,50 @@ uint32_t *run_expand(opir_server *s, uint32_t n) {
   return s->lvl[sh.h & 1].p;
 }
 
+// Batch sizes from which the tensor-core scan is used in auto mode.
+constexpr uint32_t kTcMinBatch = 2;
+
+void launch_scan_any(opir_server *s, uint32_t n) {
+  const opir::Shape &sh = s->shape;
+  const uint32_t ncols = 2 * n;
+  const bool tc = s->scan_mode == 1 || (s->scan_mode == 0 && n >= kTcMinBatch);
+  if (!tc) {
+    opir::launch_scan(s->dp, sh, s->db8.p, s->qb.p, s->cmat.p, n, s->stream);
+    return;
+  }
+  opir::TcScanArgs a{};
+  a.ntile = ncols <= 64 ? (ncols + 15) / 16 * 16 : 64;
+  a.col_tiles = (ncols + a.ntile - 1) / a.ntile;
+  a.k_tiles = (sh.n0p + 127) / 128;
+  a.other = sh.other;
+  a.m_tiles = (sh.other + 127) / 128;
+  a.ncols = ncols;
+  a.zcount = 2 * kN;
+  a.levels_per_res = kN;
+  for (int r = 0; r < 2; ++r) {
+    a.q[r] = s->dp.r[r].q;
+    a.mu[r] = s->dp.r[r].mu;
+    uint64_t w = 1;
+    for (int sft = 0; sft < 7; ++sft) {
+      a.w[r][sft] = static_cast<uint32_t>(w);
+      w = (w << 8) % a.q[r];
+    }
+  }
+  a.cmat = s->cmat.p;
+  a.err = s->err.p;
+  CUtensorMap map_q;
+  opir::make_plane_map(&map_q, s->qb.p, sh.n0p, ncols, 2ull * kN * 4, a.ntile);
+  opir::launch_scan_tc(s->map_db, map_q, a, s->sm_count, s->stream);
+}
+
 // First dimension: NTT + transpose of the first n0 leaves, scan, gather + INTT.
 void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n) {
   const opir::Shape &sh = s->shape;
-  opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, s->qmat.p, n, s->stream);
+  if (sh.n0p != sh.n0)  // keep the padded tail of every query row zero
+    ck(cudaMemsetAsync(s->qb.p, 0, 2ull * kN * 4 * 2 * n * sh.n0p, s->stream), "qb memset");
+  opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, s->qb.p, n, s->stream);
   mark(s, kStages + 1);
-  opir::launch_scan(s->dp, sh, s->db.p, s->qmat.p, s->cmat.p, n, s->stream);
+  launch_scan_any(s, n);
   mark(s, kStages + 2);
   opir::launch_scan_epilogue(s->dp, sh, s->cmat.p, s->mid[0].p, sh.other, n, s->stream);
 }
@@ -315,7 +361,20 @@ void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
   s->cur_ev = nullptr;
 }
 
-void finish(opir_server *s) { ck(cudaStreamSynchronize(s->stream), "make_query"); }
+// Reads and clears the tensor-core scan's error word (stream must be idle).
+void check_device_error(opir_server *s) {
+  uint32_t e = 0;
+  ck(cudaMemcpy(&e, s->err.p, sizeof(e), cudaMemcpyDeviceToHost), "error word");
+  if (e != 0) {
+    ck(cudaMemset(s->err.p, 0, sizeof(e)), "error word");
+    throw std::runtime_error("tensor-core scan timed out (code " + std::to_string(e) + ")");
+  }
+}
+
+void finish(opir_server *s) {
+  ck(cudaStreamSynchronize(s->stream), "make_query");
+  check_device_error(s);
+}
 
 void check_query_values(const opir_server *s, const uint64_t *q, size_t count) {
   for (size_t i = 0; i < count; ++i)
@@ -341,8 +400,8 @@ void load_tiles(opir_server *s, uint64_t logical, Fill &&fill) {
       ck(cudaMemcpyAsync(dev.p, host.data(), (real_end - pb) * kN * 2, cudaMemcpyHostToDevice,
                          s->stream), "db upload");
     }
-    opir::launch_db_preprocess(s->dp, dev.p, pb, 0, p.plain_mod, logical, p.num_pt, pb, pe,
-                               s->db.p, s->stream);
+    opir::launch_db_preprocess(s->dp, s->shape, dev.p, pb, 0, p.plain_mod, logical, pb, pe,
+                               s->db8.p, s->stream);
     ck(cudaStreamSynchronize(s->stream), "db preprocess");
   }
   s->db_loaded = true;
@@ -380,8 +439,18 @@ opir_status opir_server_create(const opir_params *params, int device, opir_serve
     DeviceGuard g(device);
     ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     setup_device_params(s);
-    s->db.alloc(2ull * kN * s->params.num_pt);
-    ck(cudaMemsetAsync(s->db.p, 0, 2ull * kN * s->params.num_pt * 4, s->stream), "db memset");
+    const opir::Shape &sh = s->shape;
+    const uint64_t db_bytes = 2ull * kN * 4 * sh.other * sh.n0p;
+    s->db8.alloc(db_bytes);
+    ck(cudaMemsetAsync(s->db8.p, 0, db_bytes, s->stream), "db memset");
+    opir::make_plane_map(&s->map_db, s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128);
+    s->err.alloc(1);
+    ck(cudaMemsetAsync(s->err.p, 0, sizeof(uint32_t), s->stream), "err memset");
+    ck(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
+    if (const char *m = std::getenv("OPIR_SCAN")) {
+      if (std::strcmp(m, "tc") == 0) s->scan_mode = 1;
+      else if (std::strcmp(m, "cuda") == 0) s->scan_mode = 2;
+    }
     ck(cudaStreamSynchronize(s->stream), "create");
   });
   if (st != OPIR_OK) {
@@ -401,13 +470,14 @@ void opir_server_destroy(opir_server *s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     s->clients.clear();
     s->tables.reset();
-    s->db.reset();
+    s->db8.reset();
+    s->err.reset();
     s->q_u64.reset();
     s->resp_u64.reset();
     s->resp_bytes.reset();
     for (auto &b : s->lvl) b.reset();
     s->sel.reset();
-    s->qmat.reset();
+    s->qb.reset();
     s->cmat.reset();
     for (auto &b : s->mid) b.reset();
     s->keyptrs.reset();
@@ -495,8 +565,8 @@ opir_status opir_server_load_db_seeded(opir_server *s, uint64_t logical, uint64_
     s->db_loaded = false;
     const uint64_t chunk = 1ull << 20;
     for (uint64_t pb = 0; pb < p.num_pt; pb += chunk)
-      opir::launch_db_preprocess(s->dp, nullptr, 0, seed, p.plain_mod, logical, p.num_pt, pb,
-                                 std::min<uint64_t>(p.num_pt, pb + chunk), s->db.p, s->stream);
+      opir::launch_db_preprocess(s->dp, s->shape, nullptr, 0, seed, p.plain_mod, logical, pb,
+                                 std::min<uint64_t>(p.num_pt, pb + chunk), s->db8.p, s->stream);
     ck(cudaStreamSynchronize(s->stream), "db preprocess");
     s->db_loaded = true;
   });

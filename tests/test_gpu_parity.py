@@ -151,3 +151,35 @@ def test_errors_follow_the_reference():
     s2.close()
     # the handle stays usable after errors
     _check_response(c, cl, op, srv.make_query(7, q))
+
+
+@pytest.mark.parametrize("mode", ["tc", "cuda"])
+@pytest.mark.parametrize("name", SMALL + LARGE)
+def test_both_scan_kernels_match_golden(name, mode, monkeypatch):
+    """Force the tensor-core (tcgen05) or the CUDA-core first-dimension scan."""
+    c, op, cl, bv, gsw, q, gp, _ = setup(name)
+    monkeypatch.setenv("OPIR_SCAN", mode)
+    with PirServer(gp) as srv:
+        srv.load_data_seeded(c["target_num_pt"], c["db_seed"])
+        srv.set_client_keys(7, bv, gsw)
+        _check_response(c, cl, op, srv.make_query(7, q))
+
+
+@pytest.mark.parametrize("mode,batch", [("tc", 40), ("cuda", 9), ("tc", 3)])
+def test_batched_scan_kernels(mode, batch, monkeypatch):
+    """Batches that need several column tiles (tc: 80 columns > 64; cuda:
+    18 columns > 16) against the single-query answers."""
+    name = "small_1000_h7"
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    rng = np.random.default_rng(batch)
+    idx = [int(i) for i in rng.integers(0, c["target_num_pt"], batch)]
+    monkeypatch.setenv("OPIR_SCAN", mode)
+    with PirServer(gp) as s2:
+        s2.load_data_seeded(c["target_num_pt"], c["db_seed"])
+        s2.set_client_keys(7, bv, gsw)
+        queries = np.stack([cl.query(i) for i in idx])
+        out = s2.make_query_batch([7] * batch, queries)
+    for i in range(batch):
+        assert np.array_equal(out[i], srv.make_query(7, queries[i]))
+        assert np.array_equal(cl.decrypt(out[i]),
+                              O.db_plaintext(c["db_seed"], idx[i], op).astype(np.uint64))
