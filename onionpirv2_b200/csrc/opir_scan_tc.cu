@@ -5,11 +5,13 @@
 // < 2^29 (matrix.cpp:240-350, the reference's level_mat_mat_32). Both operands
 // are stored as four byte planes (A = sum_i 2^(8i) A_i, Q = sum_j 2^(8j) Q_j),
 // so C = sum_{i,j} 2^(8(i+j)) A_i . Q_j. Every A_i . Q_j is an exact
-// unsigned-int8 MMA with int32 accumulation (n0 <= 2048 so a sum of at most
-// 2048 products of 255 x 255 stays below 2^31 per byte pair; pairs with the
-// same shift s = i + j share one accumulator, at most 4 pairs: < 2^31 for
-// n0 <= 8192). The epilogue recombines the seven accumulators
-// sum_s P_s 2^(8s) mod q in exact 64-bit arithmetic.
+// unsigned-int8 product with int32 accumulation (n0 <= 2048 so a sum of at
+// most 2048 products of 255 x 255 stays below 2^31). One MMA per A plane and
+// K step multiplies A_i by the four Q planes at once (they sit next to each
+// other in shared memory, so they form one B operand of N = 4 ntile rows):
+// each A tile is read from shared memory once per K step. The epilogue
+// recombines the 16 partial products sum_{i,j} P_ij 2^(8(i+j)) mod q in exact
+// 64-bit arithmetic (16 terms < 2^27 x 2^29).
 //
 // Structure: persistent CTAs (one per SM), 6 warps:
 //   warp 0      TMA producer: 3-D tiled loads (128B swizzle) of 4 A planes
@@ -17,8 +19,10 @@
 //   warp 1      TMEM owner + MMA issuer (one elected lane)
 //   warps 2..5  epilogue: tcgen05.ld of the accumulators, recombination,
 //               modular reduction, stores of C
-// Two smem stages ring between producer and MMA; one TMEM accumulator set
-// (7 x ntile columns) rings between MMA and epilogue. Every mbarrier wait is
+// Two smem stages ring between producer and MMA. An accumulator set is
+// 4 planes x 4 ntile columns of TMEM; with ntile = 16 two sets (columns 0 and
+// 256) ring between MMA and epilogue so the MMA warp does not wait for the
+// previous tile's epilogue, with ntile = 32 one set fills TMEM. Every mbarrier wait is
 // bounded in time; on timeout the kernel records an error code, drains its
 // own in-flight copies and MMAs, frees TMEM and returns.
 #include <cuda.h>
@@ -143,9 +147,9 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
   const uint32_t stage_bytes = 4 * a_plane + 4 * q_plane;
   uint64_t *full = reinterpret_cast<uint64_t *>(sm + kStages * stage_bytes);
   uint64_t *empty = full + kStages;
-  uint64_t *acc_full = empty + kStages;
-  uint64_t *acc_empty = acc_full + 1;
-  uint64_t *drain = acc_empty + 1;
+  uint64_t *acc_full = empty + kStages;   // [2]
+  uint64_t *acc_empty = acc_full + 2;     // [2]
+  uint64_t *drain = acc_empty + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -155,8 +159,10 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 128);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 128);
+    }
     mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -210,15 +216,18 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     }
   } else if (warp == 1) {
     // ------------------------------------------------------- MMA issuer
+    const uint32_t nb = 4 * a.ntile;  // B operand rows: the four Q planes
     const uint32_t idesc = (2u << 4)                                  // D: s32
-                           | (static_cast<uint32_t>(a.ntile >> 3) << 17)  // N
-                           | (static_cast<uint32_t>(kM >> 4) << 24);       // M
+                           | (static_cast<uint32_t>(nb >> 3) << 17)   // N
+                           | (static_cast<uint32_t>(kM >> 4) << 24);  // M
     // A, B: unsigned 8-bit, K-major, dense
-    uint32_t stage = 0, phase = 0, acc_phase = 0;
+    const uint32_t nbufs = 4 * nb <= 256 ? 2 : 1;
+    uint32_t stage = 0, phase = 0, acc_phase[2] = {0, 0}, buf = 0;
     bool ok = true;
     for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
-      if (!mbar_wait(acc_empty, acc_phase ^ 1, abort_flag)) { ok = false; break; }
+      if (!mbar_wait(&acc_empty[buf], acc_phase[buf] ^ 1, abort_flag)) { ok = false; break; }
       fence_after();
+      const uint32_t acc_base = tmem + buf * 256;  // 4 accumulators of nb columns
       for (uint32_t kt = 0; kt < a.k_tiles; ++kt) {
         if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
         fence_after();
@@ -226,17 +235,11 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
           const uint32_t base = sa(sm + stage * stage_bytes);
 #pragma unroll
           for (int ks = 0; ks < kKT / 32; ++ks) {
+            const uint64_t db = sw128_desc(base + 4 * a_plane + ks * 32);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-#pragma unroll
-              for (int j = 0; j < 4; ++j) {
-                const int s = i + j;
-                const int first_i = s > 3 ? s - 3 : 0;
-                const uint32_t acc = (kt | ks) != 0 || i != first_i;
-                const uint64_t da = sw128_desc(base + i * a_plane + ks * 32);
-                const uint64_t db = sw128_desc(base + 4 * a_plane + j * q_plane + ks * 32);
-                mma_u8(tmem + s * a.ntile, da, db, idesc, acc);
-              }
+              const uint64_t da = sw128_desc(base + i * a_plane + ks * 32);
+              mma_u8(acc_base + i * nb, da, db, idesc, (kt | ks) != 0);
             }
           }
           mma_commit(&empty[stage]);  // frees the stage when these MMAs finish
@@ -245,9 +248,10 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         if (++stage == kStages) { stage = 0; phase ^= 1; }
       }
       if (!ok) break;
-      if (lane == 0) mma_commit(acc_full);
+      if (lane == 0) mma_commit(&acc_full[buf]);
       __syncwarp();
-      acc_phase ^= 1;
+      acc_phase[buf] ^= 1;
+      if (nbufs == 2) buf ^= 1;
     }
     if (!ok && lane == 0) { *abort_flag = 1; atomicOr(a.err, 2u); }
     // all MMAs issued by this thread must finish before TMEM is released
@@ -261,9 +265,9 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     // --------------------------------------------------------- epilogue
     const int quad = warp & 3;             // TMEM lane quadrant of this warp
     const int row = quad * 32 + lane;
-    uint32_t acc_phase = 0;
+    uint32_t acc_phase[2] = {0, 0}, buf = 0;
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-      if (!mbar_wait(acc_full, acc_phase, abort_flag)) {
+      if (!mbar_wait(&acc_full[buf], acc_phase[buf], abort_flag)) {
         if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 4u); }
         break;
       }
@@ -272,27 +276,43 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
       const int res = z >= a.levels_per_res ? 1 : 0;
       const uint32_t q = a.q[res];
       const uint64_t mu = a.mu[res];
+      uint32_t w[7];
+#pragma unroll
+      for (int s2 = 0; s2 < 7; ++s2) w[s2] = a.w[res][s2];
       const uint32_t m = mt * kM + row;
       uint32_t *dst = a.cmat + (static_cast<uint64_t>(z) * a.other + m) * a.ncols;
       const uint32_t col0 = ct * a.ntile;
+      const uint32_t nb = 4 * a.ntile;
+      const uint32_t tbase = tmem + buf * 256 + (static_cast<uint32_t>(quad * 32) << 16);
+      uint32_t outv[32];
       for (uint32_t c0 = 0; c0 < a.ntile; c0 += 8) {
-        uint32_t P[7][8];
+        uint64_t acc[8];
 #pragma unroll
-        for (int s = 0; s < 7; ++s)
-          tmem_ld8(tmem + (static_cast<uint32_t>(quad * 32) << 16) + s * a.ntile + c0, P[s]);
-        tmem_wait_ld();
+        for (int c = 0; c < 8; ++c) acc[c] = 0;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          uint64_t acc = 0;
+        for (int i = 0; i < 4; ++i) {
+          uint32_t P[4][8];
 #pragma unroll
-          for (int s = 0; s < 7; ++s) acc += static_cast<uint64_t>(P[s][c]) * a.w[res][s];
-          const uint32_t col = col0 + c0 + c;
-          if (m < a.other && col < a.ncols) dst[col] = reduce64_tc(acc, q, mu);
+          for (int j = 0; j < 4; ++j) tmem_ld8(tbase + i * nb + j * a.ntile + c0, P[j]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[c] += static_cast<uint64_t>(P[j][c]) * w[i + j];
         }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) outv[(c0 + c) & 31] = reduce64_tc(acc[c], q, mu);
       }
+      // the accumulators are in registers: hand the TMEM set back first
       fence_before();
-      mbar_arrive(acc_empty);
-      acc_phase ^= 1;
+      mbar_arrive(&acc_empty[buf]);
+      acc_phase[buf] ^= 1;
+      if (16 * a.ntile <= 256) buf ^= 1;
+      if (m < a.other) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+          if (c < static_cast<int>(a.ntile) && col0 + c < a.ncols) dst[col0 + c] = outv[c];
+      }
     }
   }
   fence_before();
@@ -356,7 +376,7 @@ void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcSc
   cudaGetDevice(&dev);
   if (configured_dev != dev) {
     const cudaError_t e = cudaFuncSetAttribute(k_scan_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(scan_tc_smem(64)));
+                                               static_cast<int>(scan_tc_smem(32)));
     if (e != cudaSuccess)
       throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     configured_dev = dev;

@@ -279,7 +279,7 @@ uint32_t *run_expand(opir_server *s, uint32_t n) {
 }
 
 // Batch sizes from which the tensor-core scan is used in auto mode.
-constexpr uint32_t kTcMinBatch = 2;
+constexpr uint32_t kTcMinBatch = 1;
 
 void launch_scan_any(opir_server *s, uint32_t n) {
   const opir::Shape &sh = s->shape;
@@ -290,7 +290,7 @@ void launch_scan_any(opir_server *s, uint32_t n) {
     return;
   }
   opir::TcScanArgs a{};
-  a.ntile = ncols <= 64 ? (ncols + 15) / 16 * 16 : 64;
+  a.ntile = ncols <= 16 ? 16 : 32;  // two 7 x ntile TMEM sets must fit 512 columns
   a.col_tiles = (ncols + a.ntile - 1) / a.ntile;
   a.k_tiles = (sh.n0p + 127) / 128;
   a.other = sh.other;
