@@ -160,13 +160,37 @@ opir_status opir_server_make_query_batch(opir_server *server, uint32_t n,
 
 /* Batched form on device-resident buffers, enqueued on `stream`
  * (a cudaStream_t; NULL = the handle's own stream). client_ids is a host
- * array. The call returns after enqueueing; synchronise the stream before
- * reading d_responses. */
+ * array. The call returns after enqueueing (it does not wait for earlier work
+ * on the device; if the scratch arena must grow for n it allocates, see
+ * opir_server_reserve); synchronise the stream before reading d_responses.
+ * The next call on the same handle may be enqueued before this one has
+ * finished: calls on one handle run in order on the handle's stream. */
 opir_status opir_server_make_query_batch_device(opir_server *server, uint32_t n,
                                                 const uint64_t *client_ids,
                                                 const uint64_t *d_queries,
                                                 uint64_t *d_responses,
                                                 void *stream);
+
+/* ---- device memory planning ---------------------------------------------
+ * No counterpart in the reference (its server grows host vectors as it
+ * goes). The device bytes a handle requests from the CUDA allocator (which
+ * rounds each allocation up to its page size), so that a request loop can
+ * admit databases, clients and in-flight batches against an HBM budget before
+ * it allocates anything. Registering a client also holds a transient upload
+ * buffer of max(BV, RGSW) key bytes / 2 for the duration of the call. */
+typedef struct {
+  uint64_t database_bytes;          /* byte-plane database, NTT tables, error word */
+  uint64_t client_key_bytes;        /* one registered client's BV + RGSW keys */
+  uint64_t scratch_bytes_per_query; /* scratch arena bytes per query of a batch */
+  uint64_t scratch_bytes_fixed;     /* scratch arena bytes independent of the batch */
+} opir_memory_plan;
+opir_status opir_plan_memory(const opir_params *params, opir_memory_plan *out);
+
+/* Grows the handle's scratch arena to max_batch queries now (a no-op when it
+ * is already that large), so that later query calls with n <= max_batch
+ * allocate no device memory and never wait on the CUDA allocator. The arena
+ * then holds scratch_bytes_fixed + max_batch * scratch_bytes_per_query. */
+opir_status opir_server_reserve(opir_server *server, uint32_t max_batch);
 
 /* Per-stage device times (ms), averaged over the make_query / batch calls
  * made since stage timing was (re-)enabled, in the reference's TimerLogger

@@ -5,6 +5,7 @@ include/onionpir_b200.h); this package is the host-side mirror of the
 reference's PirParams / PirServer interface over that ABI.
 """
 from .server import (DeviceError, OutOfRange, PirParams, PirServer,  # noqa: F401
-                     save_response)
+                     plan_memory, save_response)
 
-__all__ = ["PirParams", "PirServer", "save_response", "OutOfRange", "DeviceError"]
+__all__ = ["PirParams", "PirServer", "save_response", "plan_memory", "OutOfRange",
+           "DeviceError"]

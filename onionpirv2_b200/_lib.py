@@ -39,6 +39,11 @@ class Params(C.Structure):
     ]
 
 
+class MemoryPlan(C.Structure):
+    _fields_ = [("database_bytes", C.c_uint64), ("client_key_bytes", C.c_uint64),
+                ("scratch_bytes_per_query", C.c_uint64), ("scratch_bytes_fixed", C.c_uint64)]
+
+
 SOURCE_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, u64p)
 
 _SIGS = {
@@ -59,6 +64,8 @@ _SIGS = {
     "opir_server_make_query_batch": ([C.c_void_p, C.c_uint32, u64p, u64p, u64p], C.c_int),
     "opir_server_make_query_batch_device": ([C.c_void_p, C.c_uint32, u64p, C.c_void_p,
                                              C.c_void_p, C.c_void_p], C.c_int),
+    "opir_plan_memory": ([C.POINTER(Params), C.POINTER(MemoryPlan)], C.c_int),
+    "opir_server_reserve": ([C.c_void_p, C.c_uint32], C.c_int),
     "opir_server_set_stage_timing": ([C.c_void_p, C.c_int], C.c_int),
     "opir_server_stage_times": ([C.c_void_p, C.POINTER(C.c_float), u32p], C.c_int),
     "opir_launch_count": ([], C.c_uint64),

@@ -28,6 +28,9 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
+
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -331,17 +334,32 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_
                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
+  static const EncodeTiledFn fn = [] {  // initialised once, thread-safe
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
             cudaSuccess ||
         q != cudaDriverEntryPointSuccess || p == nullptr)
-      throw std::runtime_error("cuTensorMapEncodeTiled unavailable");
-    fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
+      return static_cast<EncodeTiledFn>(nullptr);
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  if (!fn) throw std::runtime_error("cuTensorMapEncodeTiled unavailable");
   return fn;
+}
+
+// Raises the kernel's dynamic shared memory limit once per device.
+void configure_scan_tc() {
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(dev)) return;
+  const cudaError_t e = cudaFuncSetAttribute(k_scan_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(scan_tc_smem(32)));
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  done.insert(dev);
 }
 
 }  // namespace
@@ -371,16 +389,7 @@ size_t scan_tc_smem(uint32_t ntile) {
 void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcScanArgs &args,
                     int sm_count, cudaStream_t st) {
   const size_t smem = scan_tc_smem(args.ntile);
-  static int configured_dev = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (configured_dev != dev) {
-    const cudaError_t e = cudaFuncSetAttribute(k_scan_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(scan_tc_smem(32)));
-    if (e != cudaSuccess)
-      throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-    configured_dev = dev;
-  }
+  configure_scan_tc();
   const uint64_t items = static_cast<uint64_t>(args.col_tiles) * args.m_tiles * args.zcount;
   const unsigned grid = static_cast<unsigned>(items < static_cast<uint64_t>(sm_count) ? items : sm_count);
   k_scan_tc<<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);

@@ -77,6 +77,15 @@ constexpr int kStages = 5;
 constexpr int kEvents = kStages + 3;   // 6 stage boundaries + scan begin/end
 constexpr int kTimingSlots = 512;
 
+// Pinned staging slot for one call's key-pointer table, so that its upload is
+// an asynchronous copy; `done` marks when the copy that read it has run.
+struct KeyPtrSlot {
+  const uint32_t **host = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;
+};
+constexpr int kKeyPtrSlots = 4;
+
 }  // namespace
 
 struct opir_server {
@@ -103,6 +112,8 @@ struct opir_server {
   DevBuf<uint8_t> qb;        // byte-plane first-dimension query matrix
   DevBuf<const uint32_t *> keyptrs;
   std::vector<const uint32_t *> host_keyptrs;
+  KeyPtrSlot kp_ring[kKeyPtrSlots];
+  uint32_t kp_next = 0;
   // stage timing: one event set per timed call, averaged on request
   bool timing = false;
   std::vector<std::vector<cudaEvent_t>> ev_pool;
@@ -147,6 +158,56 @@ opir_status guarded(opir_server *s, F &&f) {
 
 uint32_t resp_bytes_of(const opir_params &p) {
   return static_cast<uint32_t>((2ull * p.poly_degree * p.small_q_width + 7) / 8);
+}
+
+// Kernel-facing shape of a layout; *lvl_slots receives the ciphertext slots
+// per query that an expansion buffer needs (the widest tree level, at least
+// the useful leaves).
+opir::Shape make_shape(const opir_params &p, uint64_t *lvl_slots) {
+  opir::Shape sh{};
+  sh.n0 = static_cast<uint32_t>(p.fst_dim_sz);
+  sh.other = static_cast<uint32_t>(p.other_dim_sz);
+  sh.num_dims = p.num_dims;
+  sh.h = p.expansion_height;
+  sh.useful = static_cast<uint32_t>(p.fst_dim_sz + static_cast<uint64_t>(p.l_ep) * (p.num_dims - 1));
+  sh.l_ep = p.l_ep;
+  sh.l_key = p.l_key;
+  sh.l_ks = p.l_ks;
+  sh.base_ep = p.base_log2;
+  sh.base_key = p.base_log2_key;
+  sh.base_ks = p.base_log2_ks;
+  sh.num_pt = p.num_pt;
+  sh.n0p = static_cast<uint32_t>((p.fst_dim_sz + 15) / 16 * 16);
+  uint64_t slots = 1;
+  for (uint32_t d2 = 0; d2 < sh.h; ++d2) slots = std::max<uint64_t>(slots, 2ull * opir::expand_nodes(sh, d2));
+  *lvl_slots = std::max<uint64_t>(slots, sh.useful);
+  return sh;
+}
+
+// Element counts of every scratch-arena buffer for n queries; the single
+// source for ensure_capacity and opir_plan_memory.
+struct ScratchPlan {
+  size_t q_u64, resp_u64, resp_bytes, lvl, sel, qb, cmat, mid, keyptrs;
+  uint64_t bytes() const {
+    return (q_u64 + resp_u64) * 8 + resp_bytes + 2 * lvl * 4 + sel * 4 + qb + cmat * 4 +
+           2 * mid * 4 + keyptrs * sizeof(void *);
+  }
+};
+
+ScratchPlan plan_scratch(const opir::Shape &sh, uint64_t lvl_slots, uint32_t resp_bytes, uint32_t n) {
+  const uint64_t ct = kCtWords;
+  const uint64_t nsel = sh.num_dims > 1 ? sh.num_dims - 1 : 0;
+  ScratchPlan pl{};
+  pl.q_u64 = static_cast<size_t>(n) * 2 * kN;
+  pl.resp_u64 = pl.q_u64;
+  pl.resp_bytes = static_cast<size_t>(n) * resp_bytes;
+  pl.lvl = n * lvl_slots * ct;
+  pl.sel = std::max<uint64_t>(1, n * nsel * 2 * sh.l_ep * ct);
+  pl.qb = 2ull * kN * 4 * 2 * n * sh.n0p;
+  pl.cmat = 2ull * kN * sh.other * 2 * n;
+  pl.mid = static_cast<size_t>(n) * sh.other * ct;
+  pl.keyptrs = 2ull * n;
+  return pl;
 }
 
 void setup_device_params(opir_server *s) {
@@ -198,39 +259,21 @@ void setup_device_params(opir_server *s) {
   d.small_q = p.small_q;
   d.small_q_width = p.small_q_width;
 
-  opir::Shape &sh = s->shape;
-  sh.n0 = static_cast<uint32_t>(p.fst_dim_sz);
-  sh.other = static_cast<uint32_t>(p.other_dim_sz);
-  sh.num_dims = p.num_dims;
-  sh.h = p.expansion_height;
-  sh.useful = static_cast<uint32_t>(p.fst_dim_sz + static_cast<uint64_t>(p.l_ep) * (p.num_dims - 1));
-  sh.l_ep = p.l_ep;
-  sh.l_key = p.l_key;
-  sh.l_ks = p.l_ks;
-  sh.base_ep = p.base_log2;
-  sh.base_key = p.base_log2_key;
-  sh.base_ks = p.base_log2_ks;
-  sh.num_pt = p.num_pt;
-  sh.n0p = static_cast<uint32_t>((p.fst_dim_sz + 15) / 16 * 16);
-  uint64_t slots = 1;
-  for (uint32_t d2 = 0; d2 < sh.h; ++d2) slots = std::max<uint64_t>(slots, 2ull * opir::expand_nodes(sh, d2));
-  s->lvl_slots = std::max<uint64_t>(slots, sh.useful);
+  s->shape = make_shape(p, &s->lvl_slots);
 }
 
 void ensure_capacity(opir_server *s, uint32_t n) {
   if (n <= s->cap) return;
-  const opir::Shape &sh = s->shape;
-  const uint64_t ct = kCtWords;
-  const uint64_t nsel = sh.num_dims > 1 ? sh.num_dims - 1 : 0;
-  s->q_u64.alloc(static_cast<size_t>(n) * 2 * kN);
-  s->resp_u64.alloc(static_cast<size_t>(n) * 2 * kN);
-  s->resp_bytes.alloc(static_cast<size_t>(n) * resp_bytes_of(s->params));
-  for (auto &b : s->lvl) b.alloc(n * s->lvl_slots * ct);
-  s->sel.alloc(std::max<uint64_t>(1, n * nsel * 2 * sh.l_ep * ct));
-  s->qb.alloc(2ull * kN * 4 * 2 * n * sh.n0p);
-  s->cmat.alloc(2ull * kN * sh.other * 2 * n);
-  for (auto &b : s->mid) b.alloc(static_cast<size_t>(n) * sh.other * ct);
-  s->keyptrs.alloc(2ull * n);
+  const ScratchPlan pl = plan_scratch(s->shape, s->lvl_slots, resp_bytes_of(s->params), n);
+  s->q_u64.alloc(pl.q_u64);
+  s->resp_u64.alloc(pl.resp_u64);
+  s->resp_bytes.alloc(pl.resp_bytes);
+  for (auto &b : s->lvl) b.alloc(pl.lvl);
+  s->sel.alloc(pl.sel);
+  s->qb.alloc(pl.qb);
+  s->cmat.alloc(pl.cmat);
+  for (auto &b : s->mid) b.alloc(pl.mid);
+  s->keyptrs.alloc(pl.keyptrs);
   s->cap = n;
 }
 
@@ -240,7 +283,23 @@ const ClientKeys &client(const opir_server *s, uint64_t id) {
   return it->second;
 }
 
-// Uploads the per-query key pointer table (bv pointers then gsw pointers).
+// Makes every pinned key-pointer slot hold at least `entries` pointers.
+void grow_keyptr_slots(opir_server *s, size_t entries) {
+  for (KeyPtrSlot &sl : s->kp_ring) {
+    if (!sl.done) ck(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "event");
+    if (sl.cap >= entries) continue;
+    ck(cudaEventSynchronize(sl.done), "key pointer slot");
+    if (sl.host) cudaFreeHost(sl.host);
+    sl.host = nullptr;
+    sl.cap = 0;
+    ck(cudaMallocHost(reinterpret_cast<void **>(&sl.host), entries * sizeof(void *)), "cudaMallocHost");
+    sl.cap = entries;
+  }
+}
+
+// Uploads the per-query key pointer table (bv pointers then gsw pointers)
+// from a pinned slot of a small ring; a slot is refilled only after the copy
+// that last read it has executed, which in steady state has long happened.
 void upload_keyptrs(opir_server *s, const uint64_t *client_ids, uint32_t n) {
   s->host_keyptrs.resize(2ull * n);
   for (uint32_t i = 0; i < n; ++i) {
@@ -248,8 +307,13 @@ void upload_keyptrs(opir_server *s, const uint64_t *client_ids, uint32_t n) {
     s->host_keyptrs[i] = k.bv.p;
     s->host_keyptrs[n + i] = k.gsw.p;
   }
-  ck(cudaMemcpyAsync(s->keyptrs.p, s->host_keyptrs.data(), 2ull * n * sizeof(void *),
-                     cudaMemcpyHostToDevice, s->stream), "key pointers");
+  grow_keyptr_slots(s, 2ull * n);
+  KeyPtrSlot &sl = s->kp_ring[s->kp_next++ % kKeyPtrSlots];
+  ck(cudaEventSynchronize(sl.done), "key pointer slot");
+  std::copy(s->host_keyptrs.begin(), s->host_keyptrs.end(), sl.host);
+  ck(cudaMemcpyAsync(s->keyptrs.p, sl.host, 2ull * n * sizeof(void *), cudaMemcpyHostToDevice,
+                     s->stream), "key pointers");
+  ck(cudaEventRecord(sl.done, s->stream), "event record");
 }
 
 void begin_timed_call(opir_server *s) {
@@ -481,6 +545,10 @@ void opir_server_destroy(opir_server *s) {
     s->cmat.reset();
     for (auto &b : s->mid) b.reset();
     s->keyptrs.reset();
+    for (KeyPtrSlot &sl : s->kp_ring) {
+      if (sl.host) cudaFreeHost(sl.host);
+      if (sl.done) cudaEventDestroy(sl.done);
+    }
     for (auto &evs : s->ev_pool)
       for (auto &e : evs) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -672,6 +740,33 @@ opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
       ck(cudaStreamWaitEvent(user, e, 0), "wait");
       cudaEventDestroy(e);
     }
+  });
+}
+
+opir_status opir_plan_memory(const opir_params *params, opir_memory_plan *out) {
+  if (!params || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] {
+    if (params->poly_degree != static_cast<uint32_t>(kN) || params->num_limbs != 1)
+      throw std::invalid_argument("only CONFIG_N2048_K1_COMP parameters are supported");
+    uint64_t slots = 0;
+    const opir::Shape sh = make_shape(*params, &slots);
+    const uint32_t rb = resp_bytes_of(*params);
+    const uint64_t one = plan_scratch(sh, slots, rb, 1).bytes();
+    const uint64_t two = plan_scratch(sh, slots, rb, 2).bytes();
+    out->database_bytes = 2ull * kN * 4 * sh.other * sh.n0p + 16ull * kN * 4 + sizeof(uint32_t);
+    out->client_key_bytes =
+        (static_cast<uint64_t>(sh.h) * sh.l_ks * 2 * kN + 2ull * sh.l_key * 2 * kN) * 2 * 4;
+    out->scratch_bytes_per_query = two - one;
+    out->scratch_bytes_fixed = 2 * one - two;
+  });
+}
+
+opir_status opir_server_reserve(opir_server *s, uint32_t max_batch) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    DeviceGuard g(s->device);
+    ensure_capacity(s, max_batch);
+    grow_keyptr_slots(s, 2ull * max_batch);
   });
 }
 

@@ -229,6 +229,11 @@ class PirServer:
             self._h, ids.size, _ptr(ids), C.c_void_p(d_queries), C.c_void_p(d_responses),
             C.c_void_p(stream) if stream else None))
 
+    def reserve(self, max_batch: int):
+        """Size the device scratch arena for batches of up to max_batch now, so
+        that later calls of that size allocate no device memory."""
+        self._check(self._lib.opir_server_reserve(self._h, int(max_batch)))
+
     def set_stage_timing(self, enabled: bool):
         self._check(self._lib.opir_server_set_stage_timing(self._h, 1 if enabled else 0))
 
@@ -275,6 +280,16 @@ class PirServer:
 
     def save_resp_to_stream(self, response: np.ndarray) -> bytes:
         return save_response(self.params, response)
+
+
+def plan_memory(params: PirParams) -> dict:
+    """Device bytes a server of these parameters requests: database, one
+    client's keys, and scratch = fixed + batch * per_query."""
+    plan = L.MemoryPlan()
+    rc = L.load().opir_plan_memory(C.byref(params._p), C.byref(plan))
+    if rc != OPIR_OK:
+        _raise(rc, "opir_plan_memory failed")
+    return {f: int(getattr(plan, f)) for f, _ in L.MemoryPlan._fields_}
 
 
 def launch_count() -> int:
