@@ -352,11 +352,14 @@ k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t 
 }
 
 // ------------------------------------------------------- first-dim query prep
+// Forward NTT of the first n0 leaves (prep_query_composite, server.cpp:
+// 264-304) into `out`, same ciphertext layout as the leaves, stored as
+// coalesced quads; k_fst_pack then turns them into byte planes.
 constexpr int kFstTile = 4;  // ciphertexts per block (8 planes)
 
 __global__ void __launch_bounds__(kThreads, 2)
-k_fst_prep(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
-           uint8_t *__restrict__ qb, uint32_t ncols, uint32_t n0p) {
+k_fst_ntt(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
+          uint32_t *__restrict__ out, uint64_t out_stride) {
   extern __shared__ uint32_t sm[];
   const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
   const uint32_t k0 = blockIdx.x * kFstTile;
@@ -373,27 +376,64 @@ k_fst_prep(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t l
   }
   __syncthreads();
   fwd_mid(sm, 2 * kFstTile, T);
-  uint32_t o[2 * kFstTile][8];
 #pragma unroll
   for (int e = 0; e < 2 * kFstTile; ++e) {
-    ld_plane<3>(sm + e * kPad, o[e], tid);
-    fwdD(o[e], T, tid);
+    const uint32_t kk = k0 + (e >> 1);
+    if (kk >= S.n0) continue;  // uniform over the block
+    const int p = e & 1;
+    uint32_t v[8];
+    ld_plane<3>(sm + e * kPad, v, tid);
+    fwdD(v, T, tid);
+    uint32_t *dst = out + ((uint64_t)b * out_stride + kk) * kCtWords + (p * 2 + res) * kN;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      *reinterpret_cast<uint4 *>(dst + 4 * (tid + 256 * h)) =
+          make_uint4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
   }
-  // qb[((res N + level) 4 + plane) ncols + column][n0p]: the four first-
-  // dimension indices k0..k0+3 of one column pack into one 32-bit word
+}
+
+// Byte-plane packing of the NTT-form query matrix:
+//   qb[((res N + z) 4 + j) ncols + col][k] = byte j of ntt[b][k][p][res][z],
+//   col = 2 b + p, zero for n0 <= k < n0p.
+// Block = (128 leaves, 32 levels of one residue, one column). Reads are 128-B
+// rows of 32 levels per leaf; the tile is transposed through shared memory
+// (33-word pitch: conflict-free both ways) and written as 128-B rows of
+// leaves per (level, byte plane).
+constexpr int kPackK = 128, kPackZ = 32, kPackPitch = kPackK / 4 + 1;
+
+__global__ void __launch_bounds__(kThreads)
+k_fst_pack(const uint32_t *__restrict__ ntt, uint64_t ntt_stride, uint32_t n0, uint32_t n0p,
+           uint8_t *__restrict__ qb, uint32_t ncols) {
+  __shared__ uint32_t sw[4][kPackZ][kPackPitch];
+  const uint32_t k0 = blockIdx.x * kPackK;
+  const uint32_t zt = blockIdx.y;
+  const int res = zt >= kN / kPackZ ? 1 : 0;
+  const uint32_t z0 = (zt - res * (kN / kPackZ)) * kPackZ;
+  const uint32_t col = blockIdx.z, b = col >> 1, p = col & 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t *src = ntt + (uint64_t)b * ntt_stride * kCtWords + (p * 2 + res) * kN + z0 + lane;
+  // warp w packs leaves 4w' .. 4w'+3 (w' = w, w + 8, ...) of level z0 + lane
+  for (int kq = warp; kq < kPackK / 4; kq += kThreads / 32) {
+    uint32_t v[4];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const uint64_t zl = (uint64_t)res * kN + posD(tid, k);
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        uint32_t w = 0;
-#pragma unroll
-        for (int kk = 0; kk < kFstTile; ++kk) w |= ((o[kk * 2 + p][k] >> (8 * j)) & 0xFFu) << (8 * kk);
-        *reinterpret_cast<uint32_t *>(qb + ((zl * 4 + j) * ncols + 2 * b + p) * n0p + k0) = w;
-      }
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t k = k0 + 4 * kq + i;
+      v[i] = k < n0 ? src[(uint64_t)k * kCtWords] : 0u;
     }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      sw[j][lane][kq] = __byte_perm(__byte_perm(v[0], v[1], 0x40 + 0x11 * j),
+                                    __byte_perm(v[2], v[3], 0x40 + 0x11 * j), 0x5410);
+  }
+  __syncthreads();
+  // each thread writes 16 leaves (one uint4) of one (byte plane, level) row
+  for (int i = tid; i < 4 * kPackZ * (kPackK / 16); i += kThreads) {
+    const int c = i & 7, row = i >> 3, j = row / kPackZ, z = row % kPackZ;
+    const uint32_t k = k0 + 16 * c;
+    if (k >= n0p) continue;
+    const uint32_t *w = &sw[j][z][4 * c];
+    *reinterpret_cast<uint4 *>(qb + (((uint64_t)(res * kN + z0 + z) * 4 + j) * ncols + col) * n0p + k) =
+        make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -487,41 +527,60 @@ k_scan(DevParams P, uint32_t n0, uint32_t n0p, uint32_t m, const uint8_t *__rest
 }
 
 // ----------------------------------------------------------- scan epilogue
-constexpr int kEpiTile = 4;  // candidates per block (8 planes)
-
+// inter_to_cts_composite (server.cpp:529-597): INTT of every candidate of
+// the scan. A block transforms 8 planes of one residue: R rows x G adjacent
+// columns (R G = 8, G = 8 when the batch has at least 8 columns), so that the
+// G words it reads per (level, row) are one contiguous run of cmat (a full
+// 32-B sector for G = 8).
+template <int G, bool VEC>
 __global__ void __launch_bounds__(kThreads, 2)
 k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_t ncols,
                 uint32_t *__restrict__ mid, uint64_t mid_stride) {
+  constexpr int R = 8 / G;
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
-  const uint32_t r0 = blockIdx.x * kEpiTile;
+  const int res = blockIdx.y, tid = threadIdx.x;
+  const uint32_t r0 = blockIdx.x * R, c0 = blockIdx.z * G;
   const ResidueTables T = pick(P, res);
-  uint32_t v[2 * kEpiTile][8];
+  uint32_t v[8][8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const uint32_t *src = cmat + (((uint64_t)res * kN + posD(tid, k)) * S.other + r0) * ncols + 2 * b;
+    const uint32_t *src = cmat + (((uint64_t)res * kN + posD(tid, k)) * S.other + r0) * ncols + c0;
 #pragma unroll
-    for (int e = 0; e < 2 * kEpiTile; ++e)
-      v[e][k] = r0 + (e >> 1) < S.other ? src[(e >> 1) * ncols + (e & 1)] : 0u;
+    for (int i = 0; i < R; ++i) {
+      const bool row_ok = r0 + i < S.other;
+      if (VEC) {
+#pragma unroll
+        for (int g = 0; g < G; g += 4) {
+          uint4 w = make_uint4(0, 0, 0, 0);
+          if (row_ok && c0 + g < ncols) w = __ldg(reinterpret_cast<const uint4 *>(src + i * ncols + g));
+          v[i * G + g][k] = w.x;
+          v[i * G + g + 1][k] = w.y;
+          v[i * G + g + 2][k] = w.z;
+          v[i * G + g + 3][k] = w.w;
+        }
+      } else {
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+          v[i * G + g][k] = row_ok && c0 + g < ncols ? __ldg(src + i * ncols + g) : 0u;
+      }
+    }
   }
 #pragma unroll
-  for (int e = 0; e < 2 * kEpiTile; ++e) {
+  for (int e = 0; e < 8; ++e) {
     invD(v[e], T, tid);
     st_plane<3>(sm + e * kPad, v[e], tid);
   }
   __syncthreads();
-  inv_mid(sm, 2 * kEpiTile, T);
-  for (int e = 0; e < 2 * kEpiTile; ++e) {
-    const uint32_t r = r0 + (e >> 1);
-    const int p = e & 1;
+  inv_mid(sm, 8, T);
+  for (int e = 0; e < 8; ++e) {
+    const uint32_t r = r0 + e / G, c = c0 + e % G;
+    if (r >= S.other || c >= ncols) continue;  // uniform over the block
     uint32_t w[8];
     ld_plane<0>(sm + e * kPad, w, tid);
     invA(w, T);
-    if (r < S.other) {
-      uint32_t *dst = mid + ((uint64_t)b * mid_stride + r) * kCtWords + (p * 2 + res) * kN;
+    uint32_t *dst = mid + ((uint64_t)(c >> 1) * mid_stride + r) * kCtWords + ((c & 1) * 2 + res) * kN;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) dst[posA(tid, k)] = w[k];
-    }
+    for (int k = 0; k < 8; ++k) dst[posA(tid, k)] = w[k];
   }
 }
 
@@ -690,12 +749,16 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
 }
 
 void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
-                     uint64_t leaf_stride, uint8_t *qb, uint32_t batch, cudaStream_t st) {
+                     uint64_t leaf_stride, uint32_t *ntt, uint64_t ntt_stride, uint8_t *qb,
+                     uint32_t batch, cudaStream_t st) {
   const size_t smem = 2 * kFstTile * kPad * sizeof(uint32_t);
-  set_smem(k_fst_prep, smem);
+  set_smem(k_fst_ntt, smem);
   dim3 grid((s.n0 + kFstTile - 1) / kFstTile, 2, batch);
-  k_fst_prep<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, qb, 2 * batch, s.n0p);
-  check_launch("k_fst_prep");
+  k_fst_ntt<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, ntt, ntt_stride);
+  check_launch("k_fst_ntt");
+  dim3 pgrid((s.n0p + kPackK - 1) / kPackK, 2 * kN / kPackZ, 2 * batch);
+  k_fst_pack<<<pgrid, kThreads, 0, st>>>(ntt, ntt_stride, s.n0, s.n0p, qb, 2 * batch);
+  check_launch("k_fst_pack");
 }
 
 template <int NCT>
@@ -722,13 +785,26 @@ void launch_scan(const DevParams &P, const Shape &s, const uint8_t *db8, const u
   else scan_dispatch<16>(P, s, db8, qb, cmat, ncols, st);
 }
 
+template <int G, bool VEC>
+static void epilogue_launch(const DevParams &P, const Shape &s, const uint32_t *cmat, uint32_t *mid,
+                            uint64_t mid_stride, uint32_t ncols, cudaStream_t st) {
+  const size_t smem = 8 * kPad * sizeof(uint32_t);
+  set_smem(k_scan_epilogue<G, VEC>, smem);
+  dim3 grid((s.other + 8 / G - 1) / (8 / G), 2, (ncols + G - 1) / G);
+  k_scan_epilogue<G, VEC><<<grid, kThreads, smem, st>>>(P, s, cmat, ncols, mid, mid_stride);
+  check_launch("k_scan_epilogue");
+}
+
 void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cmat, uint32_t *mid,
                           uint64_t mid_stride, uint32_t batch, cudaStream_t st) {
-  const size_t smem = 2 * kEpiTile * kPad * sizeof(uint32_t);
-  set_smem(k_scan_epilogue, smem);
-  dim3 grid((s.other + kEpiTile - 1) / kEpiTile, 2, batch);
-  k_scan_epilogue<<<grid, kThreads, smem, st>>>(P, s, cmat, 2 * batch, mid, mid_stride);
-  check_launch("k_scan_epilogue");
+  const uint32_t ncols = 2 * batch;
+  const bool vec = ncols % 4 == 0;
+  if (ncols <= 2) epilogue_launch<2, false>(P, s, cmat, mid, mid_stride, ncols, st);
+  else if (ncols <= 6) {
+    if (vec) epilogue_launch<4, true>(P, s, cmat, mid, mid_stride, ncols, st);
+    else epilogue_launch<4, false>(P, s, cmat, mid, mid_stride, ncols, st);
+  } else if (vec) epilogue_launch<8, true>(P, s, cmat, mid, mid_stride, ncols, st);
+  else epilogue_launch<8, false>(P, s, cmat, mid, mid_stride, ncols, st);
 }
 
 void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, const uint32_t *in,

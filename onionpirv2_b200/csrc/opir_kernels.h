@@ -69,8 +69,8 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
 // first n0 leaves of each query, written as byte planes
 // qb[((res N + level) 4 + plane) 2 batch + column][n0p], column = 2 b + poly.
 void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
-                     uint64_t leaf_stride, uint8_t *qb, uint32_t batch,
-                     cudaStream_t st);
+                     uint64_t leaf_stride, uint32_t *ntt, uint64_t ntt_stride, uint8_t *qb,
+                     uint32_t batch, cudaStream_t st);
 
 // First-dimension scan on CUDA cores (matrix.cpp:240-350): per residue and
 // NTT level, C[res][l][r][c] = sum_k A[r][k] Q[k][c] mod q_res, c < 2 batch,

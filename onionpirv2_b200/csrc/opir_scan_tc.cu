@@ -4,14 +4,21 @@
 // A = database rows [other x n0] and Q = query columns [n0 x 2B], all values
 // < 2^29 (matrix.cpp:240-350, the reference's level_mat_mat_32). Both operands
 // are stored as four byte planes (A = sum_i 2^(8i) A_i, Q = sum_j 2^(8j) Q_j),
-// so C = sum_{i,j} 2^(8(i+j)) A_i . Q_j. Every A_i . Q_j is an exact
-// unsigned-int8 product with int32 accumulation (n0 <= 2048 so a sum of at
-// most 2048 products of 255 x 255 stays below 2^31). One MMA per A plane and
-// K step multiplies A_i by the four Q planes at once (they sit next to each
-// other in shared memory, so they form one B operand of N = 4 ntile rows):
-// each A tile is read from shared memory once per K step. The epilogue
-// recombines the 16 partial products sum_{i,j} P_ij 2^(8(i+j)) mod q in exact
-// 64-bit arithmetic (16 terms < 2^27 x 2^29).
+// so C = sum_s 2^(8s) S_s with S_s = sum_{i+j=s} A_i . Q_j, s = 0..6. Every
+// A_i . Q_j is an exact unsigned-int8 product with int32 accumulation; an S_s
+// sums at most four of them, so n0 <= 8192 keeps it below 2^31
+// (4 x 8192 x 255 x 255 < 2^31).
+//
+// One MMA per A plane and K step multiplies A_i by the four Q planes at once
+// (they sit next to each other in shared memory and form one B operand of
+// N = 4 ntile rows), writing TMEM columns [i ntile, (i + 4) ntile): the
+// accumulator of S_s is columns [s ntile, (s + 1) ntile), shared by the MMAs
+// of every (i, j) with i + j = s. Each A tile is read from shared memory once
+// per K step, and an accumulator set is 7 ntile columns. The first K step of
+// a tile initialises every column exactly once: A_0 Q_0..3 (overwrite s 0-3),
+// A_3 Q_1..3 (overwrite s 4-6), then A_3 Q_0, A_1 Q_0..3 and A_2 Q_0..3
+// accumulate. The epilogue recombines sum_s S_s 2^(8s) mod q in exact 64-bit
+// arithmetic (7 terms < 2^31 x 2^29).
 //
 // Structure: persistent CTAs (one per SM), 6 warps:
 //   warp 0      TMA producer: 3-D tiled loads (128B swizzle) of 4 A planes
@@ -19,12 +26,12 @@
 //   warp 1      TMEM owner + MMA issuer (one elected lane)
 //   warps 2..5  epilogue: tcgen05.ld of the accumulators, recombination,
 //               modular reduction, stores of C
-// Two smem stages ring between producer and MMA. An accumulator set is
-// 4 planes x 4 ntile columns of TMEM; with ntile = 16 two sets (columns 0 and
-// 256) ring between MMA and epilogue so the MMA warp does not wait for the
-// previous tile's epilogue, with ntile = 32 one set fills TMEM. Every mbarrier wait is
-// bounded in time; on timeout the kernel records an error code, drains its
-// own in-flight copies and MMAs, frees TMEM and returns.
+// Two smem stages ring between producer and MMA. With ntile = 16 or 32 two
+// accumulator sets (TMEM columns 0 and 256) ring between MMA and epilogue so
+// the MMA warp does not wait for the previous tile's epilogue; ntile = 64 (a
+// batch of 32 queries in one pass over the database) uses one set. Every
+// mbarrier wait is bounded in time; on timeout the kernel records an error
+// code, drains its own in-flight copies and MMAs, frees TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -186,7 +193,7 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
 
   if (warp == 0) {
     // ---------------------------------------------------------- producer
-    uint32_t stage = 0, phase = 0, issued[kStages] = {0, 0};
+    uint32_t stage = 0, phase = 0, total = 0;  // total: stage loads issued
     bool ok = true;
     for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
       const uint32_t ct = it % a.col_tiles, mt = (it / a.col_tiles) % a.m_tiles, z = it / per_z;
@@ -202,7 +209,7 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                         ct * a.ntile, z * 4 + pl);
         }
         __syncwarp();
-        ++issued[stage];
+        ++total;
         if (++stage == kStages) { stage = 0; phase ^= 1; }
       }
     }
@@ -210,27 +217,29 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
       if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 1u); }
     }
     // own copies in flight must land before the CTA may exit
-    for (int s = 0; s < kStages; ++s) {
-      if (issued[s] == 0) continue;
+    for (uint32_t s = 0; s < static_cast<uint32_t>(kStages); ++s) {
+      const uint32_t issued = (total + kStages - 1 - s) / kStages;  // loads into stage s
+      if (issued == 0) continue;
       const long long t0 = clock64();
-      while (!mbar_try(&full[s], (issued[s] - 1) & 1)) {
+      while (!mbar_try(&full[s], (issued - 1) & 1)) {
         if (clock64() - t0 > kWaitCycles) { if (lane == 0) atomicOr(a.err, 8u); break; }
       }
     }
   } else if (warp == 1) {
     // ------------------------------------------------------- MMA issuer
-    const uint32_t nb = 4 * a.ntile;  // B operand rows: the four Q planes
-    const uint32_t idesc = (2u << 4)                                  // D: s32
-                           | (static_cast<uint32_t>(nb >> 3) << 17)   // N
-                           | (static_cast<uint32_t>(kM >> 4) << 24);  // M
-    // A, B: unsigned 8-bit, K-major, dense
-    const uint32_t nbufs = 4 * nb <= 256 ? 2 : 1;
-    uint32_t stage = 0, phase = 0, acc_phase[2] = {0, 0}, buf = 0;
+    const uint32_t nt = a.ntile;
+    // A, B: unsigned 8-bit, K-major, dense; D: s32; M = 128; N as given
+    auto idesc_n = [](uint32_t n) {
+      return (2u << 4) | ((n >> 3) << 17) | (static_cast<uint32_t>(kM >> 4) << 24);
+    };
+    const uint32_t id4 = idesc_n(4 * nt), id3 = idesc_n(3 * nt), id1 = idesc_n(nt);
+    const uint32_t nbufs = 2 * 7 * nt <= 512 ? 2 : 1;
+    uint32_t stage = 0, phase = 0, acc_phases = 0, buf = 0;  // bit b: phase of set b
     bool ok = true;
     for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
-      if (!mbar_wait(&acc_empty[buf], acc_phase[buf] ^ 1, abort_flag)) { ok = false; break; }
+      if (!mbar_wait(&acc_empty[buf], ((acc_phases >> buf) & 1) ^ 1, abort_flag)) { ok = false; break; }
       fence_after();
-      const uint32_t acc_base = tmem + buf * 256;  // 4 accumulators of nb columns
+      const uint32_t acc = tmem + buf * 256;  // S_s at columns acc + s nt
       for (uint32_t kt = 0; kt < a.k_tiles; ++kt) {
         if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
         fence_after();
@@ -238,11 +247,20 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
           const uint32_t base = sa(sm + stage * stage_bytes);
 #pragma unroll
           for (int ks = 0; ks < kKT / 32; ++ks) {
-            const uint64_t db = sw128_desc(base + 4 * a_plane + ks * 32);
+            const uint32_t qa = base + 4 * a_plane + ks * 32;  // Q planes 0..3
+            const uint64_t db = sw128_desc(qa);
+            if (kt == 0 && ks == 0) {
+              const uint64_t a0 = sw128_desc(base + ks * 32), a3 = sw128_desc(base + 3 * a_plane + ks * 32);
+              mma_u8(acc, a0, db, id4, 0);                                // S_0..3  = A_0 Q_0..3
+              mma_u8(acc + 4 * nt, a3, sw128_desc(qa + q_plane), id3, 0); // S_4..6  = A_3 Q_1..3
+              mma_u8(acc + 3 * nt, a3, db, id1, 1);                       // S_3    += A_3 Q_0
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const uint64_t da = sw128_desc(base + i * a_plane + ks * 32);
-              mma_u8(acc_base + i * nb, da, db, idesc, (kt | ks) != 0);
+              for (int i = 1; i < 3; ++i)
+                mma_u8(acc + i * nt, sw128_desc(base + i * a_plane + ks * 32), db, id4, 1);
+            } else {
+#pragma unroll
+              for (int i = 0; i < 4; ++i)
+                mma_u8(acc + i * nt, sw128_desc(base + i * a_plane + ks * 32), db, id4, 1);
             }
           }
           mma_commit(&empty[stage]);  // frees the stage when these MMAs finish
@@ -253,7 +271,7 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
       if (!ok) break;
       if (lane == 0) mma_commit(&acc_full[buf]);
       __syncwarp();
-      acc_phase[buf] ^= 1;
+      acc_phases ^= 1u << buf;
       if (nbufs == 2) buf ^= 1;
     }
     if (!ok && lane == 0) { *abort_flag = 1; atomicOr(a.err, 2u); }
@@ -268,53 +286,59 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     // --------------------------------------------------------- epilogue
     const int quad = warp & 3;             // TMEM lane quadrant of this warp
     const int row = quad * 32 + lane;
-    uint32_t acc_phase[2] = {0, 0}, buf = 0;
+    uint32_t acc_phases = 0, buf = 0;  // bit b: phase of set b
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-      if (!mbar_wait(&acc_full[buf], acc_phase[buf], abort_flag)) {
+      if (!mbar_wait(&acc_full[buf], (acc_phases >> buf) & 1, abort_flag)) {
         if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 4u); }
         break;
       }
       fence_after();
       const uint32_t ct = it % a.col_tiles, mt = (it / a.col_tiles) % a.m_tiles, z = it / per_z;
       const int res = z >= a.levels_per_res ? 1 : 0;
-      const uint32_t q = a.q[res];
-      const uint64_t mu = a.mu[res];
+      const uint32_t q = res ? a.q[1] : a.q[0];
+      const uint64_t mu = res ? a.mu[1] : a.mu[0];
       uint32_t w[7];
 #pragma unroll
-      for (int s2 = 0; s2 < 7; ++s2) w[s2] = a.w[res][s2];
+      for (int s2 = 0; s2 < 7; ++s2) w[s2] = res ? a.w[1][s2] : a.w[0][s2];
       const uint32_t m = mt * kM + row;
       uint32_t *dst = a.cmat + (static_cast<uint64_t>(z) * a.other + m) * a.ncols;
       const uint32_t col0 = ct * a.ntile;
-      const uint32_t nb = 4 * a.ntile;
+      const uint32_t nt = a.ntile;
       const uint32_t tbase = tmem + buf * 256 + (static_cast<uint32_t>(quad * 32) << 16);
+      // columns in halves of 32: the second half's values stay in registers
+      // while the TMEM set is handed back, then both halves are stored
       uint32_t outv[32];
-      for (uint32_t c0 = 0; c0 < a.ntile; c0 += 8) {
-        uint64_t acc[8];
+      for (uint32_t h0 = 0; h0 < nt; h0 += 32) {
+        const bool last = h0 + 32 >= nt;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = 0;
+        for (int cc = 0; cc < 4; ++cc) {
+          const uint32_t c0 = h0 + 8 * cc;
+          if (c0 >= nt) break;
+          uint32_t P[7][8];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          uint32_t P[4][8];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) tmem_ld8(tbase + i * nb + j * a.ntile + c0, P[j]);
+          for (int s2 = 0; s2 < 7; ++s2) tmem_ld8(tbase + s2 * nt + c0, P[s2]);
           tmem_wait_ld();
+          uint64_t acc[8];
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
+          for (int c = 0; c < 8; ++c) {
+            acc[c] = static_cast<uint64_t>(P[0][c]) * w[0];
 #pragma unroll
-            for (int c = 0; c < 8; ++c) acc[c] += static_cast<uint64_t>(P[j][c]) * w[i + j];
+            for (int s2 = 1; s2 < 7; ++s2) acc[c] += static_cast<uint64_t>(P[s2][c]) * w[s2];
+          }
+#pragma unroll
+          for (int c = 0; c < 8; ++c) outv[8 * cc + c] = reduce64_tc(acc[c], q, mu);
         }
+        if (last) {  // the accumulators are in registers: hand the TMEM set back first
+          fence_before();
+          mbar_arrive(&acc_empty[buf]);
+          acc_phases ^= 1u << buf;
+          if (2 * 7 * nt <= 512) buf ^= 1;
+        }
+        if (m < a.other) {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) outv[(c0 + c) & 31] = reduce64_tc(acc[c], q, mu);
-      }
-      // the accumulators are in registers: hand the TMEM set back first
-      fence_before();
-      mbar_arrive(&acc_empty[buf]);
-      acc_phase[buf] ^= 1;
-      if (16 * a.ntile <= 256) buf ^= 1;
-      if (m < a.other) {
-#pragma unroll
-        for (int c = 0; c < 32; ++c)
-          if (c < static_cast<int>(a.ntile) && col0 + c < a.ncols) dst[col0 + c] = outv[c];
+          for (int c = 0; c < 32; ++c)
+            if (h0 + c < nt && col0 + h0 + c < a.ncols) dst[col0 + h0 + c] = outv[c];
+        }
       }
     }
   }
@@ -356,7 +380,7 @@ void configure_scan_tc() {
   std::lock_guard<std::mutex> lock(mu);
   if (done.count(dev)) return;
   const cudaError_t e = cudaFuncSetAttribute(k_scan_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(scan_tc_smem(32)));
+                                             static_cast<int>(scan_tc_smem(64)));
   if (e != cudaSuccess)
     throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   done.insert(dev);

@@ -14,7 +14,7 @@ struct TcScanArgs {
   uint32_t other;           // rows per level (candidates)
   uint32_t m_tiles;         // ceil(other / 128)
   uint32_t ncols;           // real output columns (2 x batch)
-  uint32_t ntile;           // MMA N: columns per tile, 16 or 32
+  uint32_t ntile;           // query columns per tile: 16, 32 or 64
   uint32_t col_tiles;       // ceil(ncols / ntile)
   uint32_t zcount;          // residues x levels
   uint32_t levels_per_res;  // N

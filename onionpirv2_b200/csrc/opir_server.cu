@@ -348,13 +348,18 @@ constexpr uint32_t kTcMinBatch = 1;
 void launch_scan_any(opir_server *s, uint32_t n) {
   const opir::Shape &sh = s->shape;
   const uint32_t ncols = 2 * n;
-  const bool tc = s->scan_mode == 1 || (s->scan_mode == 0 && n >= kTcMinBatch);
+  // the tensor-core form needs n0 <= 8192 (int32 accumulators, see
+  // opir_scan_tc.cu); larger first dimensions use the CUDA-core form
+  const bool tc_ok = sh.n0p <= 8192;
+  const bool tc = tc_ok && (s->scan_mode == 1 || (s->scan_mode == 0 && n >= kTcMinBatch));
   if (!tc) {
     opir::launch_scan(s->dp, sh, s->db8.p, s->qb.p, s->cmat.p, n, s->stream);
     return;
   }
   opir::TcScanArgs a{};
-  a.ntile = ncols <= 16 ? 16 : 32;  // two 7 x ntile TMEM sets must fit 512 columns
+  // ntile <= 32: two accumulator sets of 7 ntile columns ring in TMEM;
+  // ntile = 64: one set, a batch of 32 queries in one pass over the database
+  a.ntile = ncols <= 16 ? 16 : ncols <= 32 ? 32 : 64;
   a.col_tiles = (ncols + a.ntile - 1) / a.ntile;
   a.k_tiles = (sh.n0p + 127) / 128;
   a.other = sh.other;
@@ -381,9 +386,9 @@ void launch_scan_any(opir_server *s, uint32_t n) {
 // First dimension: NTT + transpose of the first n0 leaves, scan, gather + INTT.
 void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n) {
   const opir::Shape &sh = s->shape;
-  if (sh.n0p != sh.n0)  // keep the padded tail of every query row zero
-    ck(cudaMemsetAsync(s->qb.p, 0, 2ull * kN * 4 * 2 * n * sh.n0p, s->stream), "qb memset");
-  opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, s->qb.p, n, s->stream);
+  // the NTT-form leaves go to whichever expansion buffer does not hold them
+  uint32_t *ntt = leaves == s->lvl[0].p ? s->lvl[1].p : s->lvl[0].p;
+  opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, ntt, s->lvl_slots, s->qb.p, n, s->stream);
   mark(s, kStages + 1);
   launch_scan_any(s, n);
   mark(s, kStages + 2);

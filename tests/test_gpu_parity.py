@@ -165,10 +165,12 @@ def test_both_scan_kernels_match_golden(name, mode, monkeypatch):
         _check_response(c, cl, op, srv.make_query(7, q))
 
 
-@pytest.mark.parametrize("mode,batch", [("tc", 40), ("cuda", 9), ("tc", 3)])
+@pytest.mark.parametrize("mode,batch", [("tc", 40), ("cuda", 9), ("tc", 3), ("tc", 16),
+                                        ("tc", 32), ("tc", 12)])
 def test_batched_scan_kernels(mode, batch, monkeypatch):
-    """Batches that need several column tiles (tc: 80 columns > 64; cuda:
-    18 columns > 16) against the single-query answers."""
+    """Every tensor-core tile width (16, 32, 64 columns; 80 columns = two
+    tiles of 64) and a CUDA-core batch over several column tiles (18 > 16),
+    against the single-query answers."""
     name = "small_1000_h7"
     c, op, cl, bv, gsw, q, gp, srv = setup(name)
     rng = np.random.default_rng(batch)
