@@ -250,6 +250,9 @@ def bench_ours(args, world, rank, local):
     queries, keys = synthetic_inputs(params, B, 1000 + rank)
     for b, (bv, gsw) in enumerate(keys):
         srv.set_client_keys(b, bv, gsw)
+    t0 = time.perf_counter()
+    srv.autotune(B)                      # scan tiling per batch bucket (setup, untimed)
+    tune_s = time.perf_counter() - t0
     ids = list(range(B))
     # a dedicated (non-default) stream: the library orders its own stream
     # after this one and this one after its work, so events recorded here
@@ -353,7 +356,9 @@ def bench_ours(args, world, rank, local):
                      "traffic": (traffic or {}).get(f"batch_{B}")},
         "clocks": clk.summary(),
         "gpu_launches": launches,
-        "setup": {"db_load_s": round(load_s, 3), "gpu": torch.cuda.get_device_name(device)},
+        "setup": {"db_load_s": round(load_s, 3), "autotune_s": round(tune_s, 3),
+                  "scan_tile": srv.scan_tile(B), "scan_tile_plain": srv.scan_tile(1),
+                  "gpu": torch.cuda.get_device_name(device)},
     }
     if world == 1 and not args.no_cpu_baseline and args.target == TARGET:
         try:

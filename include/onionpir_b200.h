@@ -192,6 +192,20 @@ opir_status opir_plan_memory(const opir_params *params, opir_memory_plan *out);
  * then holds scratch_bytes_fixed + max_batch * scratch_bytes_per_query. */
 opir_status opir_server_reserve(opir_server *server, uint32_t max_batch);
 
+/* No counterpart in the reference (its matrix.cpp kernels have one fixed
+ * blocking). Times the tilings of the tensor-core first-dimension scan --
+ * query columns per tile (16, 32, 64), K bytes per pipeline stage (128 with
+ * 128-byte swizzle, 64 with 64-byte swizzle) and pipeline depth -- on this
+ * handle's database for batches of 1, 2, 4, ... up to max_batch queries, and
+ * keeps the fastest per batch-size bucket. Every tiling computes the same
+ * result; only the speed differs. Synchronises the handle's stream and
+ * overwrites its scratch arena: no query may be in flight on the handle. */
+opir_status opir_server_autotune(opir_server *server, uint32_t max_batch);
+/* The scan tiling a batch of n queries uses (autotuned, else the default). */
+opir_status opir_server_scan_tile(const opir_server *server, uint32_t n,
+                                  uint32_t *ntile, uint32_t *kt,
+                                  uint32_t *stages);
+
 /* Per-stage device times (ms), averaged over the make_query / batch calls
  * made since stage timing was (re-)enabled, in the reference's TimerLogger
  * sections (includes/logging.h:34-78): [0] Expand, [1] Convert,

@@ -521,48 +521,36 @@ k_scan(DevParams P, uint32_t n0, uint32_t n0p, uint32_t m, const uint8_t *__rest
       uint32_t v = reduce64(acc[c], q, mu);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) v = add_mod(v, __shfl_xor_sync(0xffffffffu, v, off), q);
-      if (lane == c && ct0 + c < (int)ncols) C[(uint64_t)r * ncols + ct0 + c] = v;
+      if (lane == c && ct0 + c < (int)ncols) C[(uint64_t)(ct0 + c) * m + r] = v;
     }
   }
 }
 
 // ----------------------------------------------------------- scan epilogue
 // inter_to_cts_composite (server.cpp:529-597): INTT of every candidate of
-// the scan. A block transforms 8 planes of one residue: R rows x G adjacent
-// columns (R G = 8, G = 8 when the batch has at least 8 columns), so that the
-// G words it reads per (level, row) are one contiguous run of cmat (a full
-// 32-B sector for G = 8).
-template <int G, bool VEC>
+// the scan. cmat is [residue x level][column][row]; a block transforms 8
+// adjacent rows of one column and one residue, so the 8 words it reads per
+// level are one contiguous 32-byte sector.
+template <bool VEC>
 __global__ void __launch_bounds__(kThreads, 2)
 k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_t ncols,
                 uint32_t *__restrict__ mid, uint64_t mid_stride) {
-  constexpr int R = 8 / G;
   extern __shared__ uint32_t sm[];
   const int res = blockIdx.y, tid = threadIdx.x;
-  const uint32_t r0 = blockIdx.x * R, c0 = blockIdx.z * G;
+  const uint32_t r0 = blockIdx.x * 8, c = blockIdx.z;
   const ResidueTables T = pick(P, res);
   uint32_t v[8][8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const uint32_t *src = cmat + (((uint64_t)res * kN + posD(tid, k)) * S.other + r0) * ncols + c0;
+    const uint32_t *src = cmat + (((uint64_t)res * kN + posD(tid, k)) * ncols + c) * S.other + r0;
+    if (VEC && r0 + 8 <= S.other) {
+      const uint4 lo = __ldg(reinterpret_cast<const uint4 *>(src));
+      const uint4 hi = __ldg(reinterpret_cast<const uint4 *>(src + 4));
+      v[0][k] = lo.x; v[1][k] = lo.y; v[2][k] = lo.z; v[3][k] = lo.w;
+      v[4][k] = hi.x; v[5][k] = hi.y; v[6][k] = hi.z; v[7][k] = hi.w;
+    } else {
 #pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const bool row_ok = r0 + i < S.other;
-      if (VEC) {
-#pragma unroll
-        for (int g = 0; g < G; g += 4) {
-          uint4 w = make_uint4(0, 0, 0, 0);
-          if (row_ok && c0 + g < ncols) w = __ldg(reinterpret_cast<const uint4 *>(src + i * ncols + g));
-          v[i * G + g][k] = w.x;
-          v[i * G + g + 1][k] = w.y;
-          v[i * G + g + 2][k] = w.z;
-          v[i * G + g + 3][k] = w.w;
-        }
-      } else {
-#pragma unroll
-        for (int g = 0; g < G; ++g)
-          v[i * G + g][k] = row_ok && c0 + g < ncols ? __ldg(src + i * ncols + g) : 0u;
-      }
+      for (int e = 0; e < 8; ++e) v[e][k] = r0 + e < S.other ? __ldg(src + e) : 0u;
     }
   }
 #pragma unroll
@@ -572,13 +560,14 @@ k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_
   }
   __syncthreads();
   inv_mid(sm, 8, T);
+  uint32_t *dst0 = mid + (uint64_t)(c >> 1) * mid_stride * kCtWords + ((c & 1) * 2 + res) * kN;
   for (int e = 0; e < 8; ++e) {
-    const uint32_t r = r0 + e / G, c = c0 + e % G;
-    if (r >= S.other || c >= ncols) continue;  // uniform over the block
+    const uint32_t r = r0 + e;
+    if (r >= S.other) break;  // uniform over the block
     uint32_t w[8];
     ld_plane<0>(sm + e * kPad, w, tid);
     invA(w, T);
-    uint32_t *dst = mid + ((uint64_t)(c >> 1) * mid_stride + r) * kCtWords + ((c & 1) * 2 + res) * kN;
+    uint32_t *dst = dst0 + (uint64_t)r * kCtWords;
 #pragma unroll
     for (int k = 0; k < 8; ++k) dst[posA(tid, k)] = w[k];
   }
@@ -785,26 +774,19 @@ void launch_scan(const DevParams &P, const Shape &s, const uint8_t *db8, const u
   else scan_dispatch<16>(P, s, db8, qb, cmat, ncols, st);
 }
 
-template <int G, bool VEC>
-static void epilogue_launch(const DevParams &P, const Shape &s, const uint32_t *cmat, uint32_t *mid,
-                            uint64_t mid_stride, uint32_t ncols, cudaStream_t st) {
-  const size_t smem = 8 * kPad * sizeof(uint32_t);
-  set_smem(k_scan_epilogue<G, VEC>, smem);
-  dim3 grid((s.other + 8 / G - 1) / (8 / G), 2, (ncols + G - 1) / G);
-  k_scan_epilogue<G, VEC><<<grid, kThreads, smem, st>>>(P, s, cmat, ncols, mid, mid_stride);
-  check_launch("k_scan_epilogue");
-}
-
 void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cmat, uint32_t *mid,
                           uint64_t mid_stride, uint32_t batch, cudaStream_t st) {
+  const size_t smem = 8 * kPad * sizeof(uint32_t);
   const uint32_t ncols = 2 * batch;
-  const bool vec = ncols % 4 == 0;
-  if (ncols <= 2) epilogue_launch<2, false>(P, s, cmat, mid, mid_stride, ncols, st);
-  else if (ncols <= 6) {
-    if (vec) epilogue_launch<4, true>(P, s, cmat, mid, mid_stride, ncols, st);
-    else epilogue_launch<4, false>(P, s, cmat, mid, mid_stride, ncols, st);
-  } else if (vec) epilogue_launch<8, true>(P, s, cmat, mid, mid_stride, ncols, st);
-  else epilogue_launch<8, false>(P, s, cmat, mid, mid_stride, ncols, st);
+  dim3 grid((s.other + 7) / 8, 2, ncols);
+  if (s.other % 4 == 0) {
+    set_smem(k_scan_epilogue<true>, smem);
+    k_scan_epilogue<true><<<grid, kThreads, smem, st>>>(P, s, cmat, ncols, mid, mid_stride);
+  } else {
+    set_smem(k_scan_epilogue<false>, smem);
+    k_scan_epilogue<false><<<grid, kThreads, smem, st>>>(P, s, cmat, ncols, mid, mid_stride);
+  }
+  check_launch("k_scan_epilogue");
 }
 
 void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, const uint32_t *in,

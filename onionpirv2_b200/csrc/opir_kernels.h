@@ -73,8 +73,9 @@ void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
                      uint32_t batch, cudaStream_t st);
 
 // First-dimension scan on CUDA cores (matrix.cpp:240-350): per residue and
-// NTT level, C[res][l][r][c] = sum_k A[r][k] Q[k][c] mod q_res, c < 2 batch,
-// with A and Q rebuilt from their byte planes.
+// NTT level, C[res][l][c][r] = sum_k A[r][k] Q[k][c] mod q_res, c < 2 batch,
+// with A and Q rebuilt from their byte planes (the tensor-core form writes
+// the same [res x level][column][row] layout).
 void launch_scan(const DevParams &P, const Shape &s, const uint8_t *db8,
                  const uint8_t *qb, uint32_t *cmat, uint32_t batch,
                  cudaStream_t st);

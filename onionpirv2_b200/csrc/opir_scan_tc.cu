@@ -20,11 +20,12 @@
 // accumulate. The epilogue recombines sum_s S_s 2^(8s) mod q in exact 64-bit
 // arithmetic (7 terms < 2^31 x 2^29).
 //
-// Structure: persistent CTAs (one per SM), 6 warps:
+// Structure: persistent CTAs (one per SM), 10 warps:
 //   warp 0      TMA producer: 3-D tiled loads (128B swizzle) of 4 A planes
 //               [128 rows x 128 B] and 4 Q planes [ntile x 128 B] per stage
 //   warp 1      TMEM owner + MMA issuer (one elected lane)
-//   warps 2..5  epilogue: tcgen05.ld of the accumulators, recombination,
+//   warps 2..9  epilogue, two warps per TMEM lane quadrant (each takes half
+//               of the tile's columns): tcgen05.ld of the accumulators, recombination,
 //               modular reduction, stores of C
 // Two smem stages ring between producer and MMA. With ntile = 16 or 32 two
 // accumulator sets (TMEM columns 0 and 256) ring between MMA and epilogue so
@@ -49,9 +50,10 @@ namespace opir {
 namespace {
 
 constexpr int kM = 128;          // MMA M / rows per tile
-constexpr int kKT = 128;         // K bytes per stage (one 128B swizzle atom)
-constexpr int kStages = 2;
-constexpr int kThreadsTc = 192;
+constexpr int kMaxStages = 8;
+constexpr int kThreadsTc = 320;
+constexpr int kEpilogueThreads = 256;
+constexpr size_t kBarrierBytes = 256;  // mbarriers, TMEM slot, abort flag
 constexpr uint32_t kTmemCols = 512;
 constexpr long long kWaitCycles = 1ll << 31;  // ~1 s at 2 GHz
 
@@ -102,14 +104,16 @@ __device__ __forceinline__ void fence_before() {
 __device__ __forceinline__ void fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
-// Shared-memory matrix descriptor: K-major, 128B swizzle, 8-row groups of
-// 128-byte rows (SBO = 1024 B), Blackwell descriptor version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// Shared-memory matrix descriptor, K-major, KT-byte swizzle (KT = 128: 128B
+// swizzle; KT = 64: 64B swizzle): 8-row groups of KT-byte rows (SBO = 8 KT
+// bytes), Blackwell descriptor version 1.
+template <int KT>
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
   uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
-  d |= static_cast<uint64_t>(1) << 16;              // LBO (unused when swizzled)
-  d |= static_cast<uint64_t>(1024 >> 4) << 32;      // SBO
-  d |= static_cast<uint64_t>(1) << 46;              // version
-  d |= static_cast<uint64_t>(2) << 61;              // SWIZZLE_128B
+  d |= static_cast<uint64_t>(1) << 16;                     // LBO (unused when swizzled)
+  d |= static_cast<uint64_t>((8 * KT) >> 4) << 32;         // SBO
+  d |= static_cast<uint64_t>(1) << 46;                     // version
+  d |= static_cast<uint64_t>(KT == 128 ? 2 : 4) << 61;     // SWIZZLE_128B / SWIZZLE_64B
   return d;
 }
 __device__ __forceinline__ void mma_u8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
@@ -146,32 +150,34 @@ __device__ __forceinline__ uint32_t reduce64_tc(uint64_t x, uint32_t q, uint64_t
   return static_cast<uint32_t>(r);
 }
 
+template <int KT>
 __global__ void __launch_bounds__(kThreadsTc, 1)
 k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmQ,
           TcScanArgs a) {
   extern __shared__ __align__(1024) uint8_t smraw[];
   uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smraw) + 1023) &
                                             ~static_cast<uintptr_t>(1023));
-  const uint32_t a_plane = kM * kKT;               // 16 KiB
-  const uint32_t q_plane = a.ntile * kKT;          // ntile * 128 B
+  const uint32_t stages = a.stages;
+  const uint32_t a_plane = kM * KT;                // 16 or 8 KiB
+  const uint32_t q_plane = a.ntile * KT;
   const uint32_t stage_bytes = 4 * a_plane + 4 * q_plane;
-  uint64_t *full = reinterpret_cast<uint64_t *>(sm + kStages * stage_bytes);
-  uint64_t *empty = full + kStages;
-  uint64_t *acc_full = empty + kStages;   // [2]
-  uint64_t *acc_empty = acc_full + 2;     // [2]
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + stages * stage_bytes);
+  uint64_t *empty = full + kMaxStages;
+  uint64_t *acc_full = empty + kMaxStages;  // [2]
+  uint64_t *acc_empty = acc_full + 2;       // [2]
   uint64_t *drain = acc_empty + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (uint32_t s = 0; s < stages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 128);
+      mbar_init(&acc_empty[b], kEpilogueThreads);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -203,22 +209,22 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
           uint8_t *st = sm + stage * stage_bytes;
           mbar_expect_tx(&full[stage], stage_bytes);
           for (int pl = 0; pl < 4; ++pl)
-            tma_load_3d(st + pl * a_plane, &tmA, &full[stage], kt * kKT, mt * kM, z * 4 + pl);
+            tma_load_3d(st + pl * a_plane, &tmA, &full[stage], kt * KT, mt * kM, z * 4 + pl);
           for (int pl = 0; pl < 4; ++pl)
-            tma_load_3d(st + 4 * a_plane + pl * q_plane, &tmQ, &full[stage], kt * kKT,
+            tma_load_3d(st + 4 * a_plane + pl * q_plane, &tmQ, &full[stage], kt * KT,
                         ct * a.ntile, z * 4 + pl);
         }
         __syncwarp();
         ++total;
-        if (++stage == kStages) { stage = 0; phase ^= 1; }
+        if (++stage == stages) { stage = 0; phase ^= 1; }
       }
     }
     if (!ok) {
       if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 1u); }
     }
     // own copies in flight must land before the CTA may exit
-    for (uint32_t s = 0; s < static_cast<uint32_t>(kStages); ++s) {
-      const uint32_t issued = (total + kStages - 1 - s) / kStages;  // loads into stage s
+    for (uint32_t s = 0; s < stages; ++s) {
+      const uint32_t issued = (total + stages - 1 - s) / stages;  // loads into stage s
       if (issued == 0) continue;
       const long long t0 = clock64();
       while (!mbar_try(&full[s], (issued - 1) & 1)) {
@@ -246,27 +252,27 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         if (lane == 0) {
           const uint32_t base = sa(sm + stage * stage_bytes);
 #pragma unroll
-          for (int ks = 0; ks < kKT / 32; ++ks) {
+          for (int ks = 0; ks < KT / 32; ++ks) {
             const uint32_t qa = base + 4 * a_plane + ks * 32;  // Q planes 0..3
-            const uint64_t db = sw128_desc(qa);
+            const uint64_t db = smem_desc<KT>(qa);
             if (kt == 0 && ks == 0) {
-              const uint64_t a0 = sw128_desc(base + ks * 32), a3 = sw128_desc(base + 3 * a_plane + ks * 32);
-              mma_u8(acc, a0, db, id4, 0);                                // S_0..3  = A_0 Q_0..3
-              mma_u8(acc + 4 * nt, a3, sw128_desc(qa + q_plane), id3, 0); // S_4..6  = A_3 Q_1..3
-              mma_u8(acc + 3 * nt, a3, db, id1, 1);                       // S_3    += A_3 Q_0
+              const uint64_t a0 = smem_desc<KT>(base), a3 = smem_desc<KT>(base + 3 * a_plane);
+              mma_u8(acc, a0, db, id4, 0);                                   // S_0..3  = A_0 Q_0..3
+              mma_u8(acc + 4 * nt, a3, smem_desc<KT>(qa + q_plane), id3, 0); // S_4..6  = A_3 Q_1..3
+              mma_u8(acc + 3 * nt, a3, db, id1, 1);                          // S_3    += A_3 Q_0
 #pragma unroll
               for (int i = 1; i < 3; ++i)
-                mma_u8(acc + i * nt, sw128_desc(base + i * a_plane + ks * 32), db, id4, 1);
+                mma_u8(acc + i * nt, smem_desc<KT>(base + i * a_plane), db, id4, 1);
             } else {
 #pragma unroll
               for (int i = 0; i < 4; ++i)
-                mma_u8(acc + i * nt, sw128_desc(base + i * a_plane + ks * 32), db, id4, 1);
+                mma_u8(acc + i * nt, smem_desc<KT>(base + i * a_plane + ks * 32), db, id4, 1);
             }
           }
           mma_commit(&empty[stage]);  // frees the stage when these MMAs finish
         }
         __syncwarp();
-        if (++stage == kStages) { stage = 0; phase ^= 1; }
+        if (++stage == stages) { stage = 0; phase ^= 1; }
       }
       if (!ok) break;
       if (lane == 0) mma_commit(&acc_full[buf]);
@@ -285,6 +291,7 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
   } else {
     // --------------------------------------------------------- epilogue
     const int quad = warp & 3;             // TMEM lane quadrant of this warp
+    const uint32_t half = (warp - 2) >> 2;   // which half of the tile's columns
     const int row = quad * 32 + lane;
     uint32_t acc_phases = 0, buf = 0;  // bit b: phase of set b
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
@@ -301,19 +308,22 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
 #pragma unroll
       for (int s2 = 0; s2 < 7; ++s2) w[s2] = res ? a.w[1][s2] : a.w[0][s2];
       const uint32_t m = mt * kM + row;
-      uint32_t *dst = a.cmat + (static_cast<uint64_t>(z) * a.other + m) * a.ncols;
+      // cmat[z][column][row]: a warp's 32 rows of one column are 128
+      // contiguous bytes
+      uint32_t *dst = a.cmat + static_cast<uint64_t>(z) * a.ncols * a.other + m;
       const uint32_t col0 = ct * a.ntile;
       const uint32_t nt = a.ntile;
       const uint32_t tbase = tmem + buf * 256 + (static_cast<uint32_t>(quad * 32) << 16);
-      // columns in halves of 32: the second half's values stay in registers
-      // while the TMEM set is handed back, then both halves are stored
+      // this warp's nt / 2 (<= 32) columns are read and reduced into
+      // registers, the TMEM set is handed back, then the values are stored
       uint32_t outv[32];
-      for (uint32_t h0 = 0; h0 < nt; h0 += 32) {
-        const bool last = h0 + 32 >= nt;
+      const uint32_t cbeg = half * (nt / 2), cend = cbeg + nt / 2;  // nt / 2 <= 32
+      for (uint32_t h0 = cbeg; h0 < cend; h0 += 32) {
+        const bool last = h0 + 32 >= cend;
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
           const uint32_t c0 = h0 + 8 * cc;
-          if (c0 >= nt) break;
+          if (c0 >= cend) break;
           uint32_t P[7][8];
 #pragma unroll
           for (int s2 = 0; s2 < 7; ++s2) tmem_ld8(tbase + s2 * nt + c0, P[s2]);
@@ -337,7 +347,8 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         if (m < a.other) {
 #pragma unroll
           for (int c = 0; c < 32; ++c)
-            if (h0 + c < nt && col0 + h0 + c < a.ncols) dst[col0 + h0 + c] = outv[c];
+            if (h0 + c < cend && col0 + h0 + c < a.ncols)
+              dst[static_cast<uint64_t>(col0 + h0 + c) * a.other] = outv[c];
         }
       }
     }
@@ -371,7 +382,10 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// Raises the kernel's dynamic shared memory limit once per device.
+// Largest dynamic shared memory a block may opt into on sm_100.
+constexpr size_t kSmemLimit = 227 * 1024;
+
+// Raises the kernels' dynamic shared memory limit once per device.
 void configure_scan_tc() {
   static std::mutex mu;
   static std::set<int> done;
@@ -379,44 +393,63 @@ void configure_scan_tc() {
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lock(mu);
   if (done.count(dev)) return;
-  const cudaError_t e = cudaFuncSetAttribute(k_scan_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(scan_tc_smem(64)));
-  if (e != cudaSuccess)
-    throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  for (const void *k : {reinterpret_cast<const void *>(k_scan_tc<128>),
+                        reinterpret_cast<const void *>(k_scan_tc<64>)}) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(kSmemLimit));
+    if (e != cudaSuccess)
+      throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  }
   done.insert(dev);
 }
 
 }  // namespace
 
 // 3-D byte tensor [planes][rows][k] (k innermost, row stride = k_bytes),
-// boxes of [1][box_rows][128] with 128B swizzle; out-of-range rows read 0.
+// boxes of [1][box_rows][box_k] with box_k-byte swizzle (128 or 64); rows and
+// k past the extents read as zero.
 void make_plane_map(CUtensorMap *map, const uint8_t *base, uint64_t k_bytes, uint64_t rows,
-                    uint64_t planes, uint32_t box_rows) {
+                    uint64_t planes, uint32_t box_rows, uint32_t box_k) {
   if (k_bytes % 16 != 0) throw std::invalid_argument("plane row stride must be a multiple of 16");
+  if (box_k != 128 && box_k != 64) throw std::invalid_argument("box_k must be 128 or 64");
   const cuuint64_t dims[3] = {k_bytes, rows, planes};
   const cuuint64_t strides[2] = {k_bytes, k_bytes * rows};
-  const cuuint32_t box[3] = {static_cast<cuuint32_t>(kKT), box_rows, 1};
+  const cuuint32_t box[3] = {box_k, box_rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
                                  const_cast<uint8_t *>(base), dims, strides, box, estr,
-                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 box_k == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
     throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string(static_cast<int>(r)));
 }
 
-size_t scan_tc_smem(uint32_t ntile) {
-  return 1024 + kStages * (4ull * kM * kKT + 4ull * ntile * kKT) + 128;
+size_t scan_tc_smem(uint32_t ntile, uint32_t kt, uint32_t stages) {
+  return 1024 + static_cast<size_t>(stages) * (4ull * kM * kt + 4ull * ntile * kt) + kBarrierBytes;
+}
+
+uint32_t scan_tc_max_stages(uint32_t ntile, uint32_t kt) {
+  const size_t stage = 4ull * kM * kt + 4ull * ntile * kt;
+  const size_t n = (kSmemLimit - 1024 - kBarrierBytes) / stage;
+  return static_cast<uint32_t>(n < static_cast<size_t>(kMaxStages) ? n : kMaxStages);
 }
 
 void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcScanArgs &args,
                     int sm_count, cudaStream_t st) {
-  const size_t smem = scan_tc_smem(args.ntile);
+  if ((args.kt != 128 && args.kt != 64) || args.stages < 2 ||
+      args.stages > scan_tc_max_stages(args.ntile, args.kt) ||
+      (args.ntile != 16 && args.ntile != 32 && args.ntile != 64))
+    throw std::invalid_argument("tensor-core scan: unsupported tile configuration");
+  const size_t smem = scan_tc_smem(args.ntile, args.kt, args.stages);
   configure_scan_tc();
   const uint64_t items = static_cast<uint64_t>(args.col_tiles) * args.m_tiles * args.zcount;
   const unsigned grid = static_cast<unsigned>(items < static_cast<uint64_t>(sm_count) ? items : sm_count);
-  k_scan_tc<<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
+  if (args.kt == 128)
+    k_scan_tc<128><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
+  else
+    k_scan_tc<64><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw std::runtime_error(std::string("k_scan_tc: ") + cudaGetErrorString(e));
 }

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -86,6 +87,18 @@ struct KeyPtrSlot {
 };
 constexpr int kKeyPtrSlots = 4;
 
+// Tiling of the tensor-core scan for one batch-size bucket (batches of
+// 2^(b-1) < n <= 2^b queries; the last bucket takes every larger batch).
+struct ScanTile {
+  uint32_t ntile = 0, kt = 0, stages = 0;  // ntile 0: pick by the default rule
+};
+constexpr int kTileBuckets = 10;
+int tile_bucket(uint32_t n) {
+  int b = 0;
+  while (b + 1 < kTileBuckets && (1u << b) < n) ++b;
+  return b;
+}
+
 }  // namespace
 
 struct opir_server {
@@ -97,7 +110,8 @@ struct opir_server {
   DevBuf<uint32_t> tables;
   DevBuf<uint8_t> db8;       // byte-plane database, see opir_kernels.h
   bool db_loaded = false;
-  CUtensorMap map_db{};      // TMA view of db8 for the tensor-core scan
+  CUtensorMap map_db[2]{};   // TMA views of db8 for the tensor-core scan: 128 B / 64 B swizzle
+  ScanTile tile[kTileBuckets];  // tensor-core scan tiling per batch bucket (autotuned)
   int sm_count = 148;
   int scan_mode = 0;         // 0 auto, 1 tensor cores, 2 CUDA cores
   DevBuf<uint32_t> err;      // device error word of the tensor-core scan
@@ -345,23 +359,16 @@ uint32_t *run_expand(opir_server *s, uint32_t n) {
 // Batch sizes from which the tensor-core scan is used in auto mode.
 constexpr uint32_t kTcMinBatch = 1;
 
-void launch_scan_any(opir_server *s, uint32_t n) {
+// Tensor-core scan of n queries with an explicit tiling.
+void launch_scan_tc_tile(opir_server *s, uint32_t n, const ScanTile &t) {
   const opir::Shape &sh = s->shape;
   const uint32_t ncols = 2 * n;
-  // the tensor-core form needs n0 <= 8192 (int32 accumulators, see
-  // opir_scan_tc.cu); larger first dimensions use the CUDA-core form
-  const bool tc_ok = sh.n0p <= 8192;
-  const bool tc = tc_ok && (s->scan_mode == 1 || (s->scan_mode == 0 && n >= kTcMinBatch));
-  if (!tc) {
-    opir::launch_scan(s->dp, sh, s->db8.p, s->qb.p, s->cmat.p, n, s->stream);
-    return;
-  }
   opir::TcScanArgs a{};
-  // ntile <= 32: two accumulator sets of 7 ntile columns ring in TMEM;
-  // ntile = 64: one set, a batch of 32 queries in one pass over the database
-  a.ntile = ncols <= 16 ? 16 : ncols <= 32 ? 32 : 64;
+  a.ntile = t.ntile;
+  a.kt = t.kt;
+  a.stages = t.stages;
   a.col_tiles = (ncols + a.ntile - 1) / a.ntile;
-  a.k_tiles = (sh.n0p + 127) / 128;
+  a.k_tiles = (sh.n0p + a.kt - 1) / a.kt;
   a.other = sh.other;
   a.m_tiles = (sh.other + 127) / 128;
   a.ncols = ncols;
@@ -379,8 +386,39 @@ void launch_scan_any(opir_server *s, uint32_t n) {
   a.cmat = s->cmat.p;
   a.err = s->err.p;
   CUtensorMap map_q;
-  opir::make_plane_map(&map_q, s->qb.p, sh.n0p, ncols, 2ull * kN * 4, a.ntile);
-  opir::launch_scan_tc(s->map_db, map_q, a, s->sm_count, s->stream);
+  opir::make_plane_map(&map_q, s->qb.p, sh.n0p, ncols, 2ull * kN * 4, a.ntile, a.kt);
+  opir::launch_scan_tc(s->map_db[a.kt == 128 ? 0 : 1], map_q, a, s->sm_count, s->stream);
+}
+
+// The tiling a batch of n queries uses: the OPIR_SCAN_TILE override
+// ("ntile,kt,stages"), else the autotuned bucket, else the default rule.
+ScanTile effective_tile(const opir_server *s, uint32_t n) {
+  if (const char *e = std::getenv("OPIR_SCAN_TILE")) {
+    unsigned a0 = 0, a1 = 0, a2 = 0;
+    if (std::sscanf(e, "%u,%u,%u", &a0, &a1, &a2) == 3) return ScanTile{a0, a1, a2};
+  }
+  ScanTile t = s->tile[tile_bucket(n)];
+  if (t.ntile != 0) return t;
+  // ntile <= 32: two accumulator sets of 7 ntile columns ring in TMEM;
+  // ntile = 64: one set, a batch of 32 queries in one pass over the database
+  const uint32_t ncols = 2 * n;
+  t.ntile = ncols <= 16 ? 16 : ncols <= 32 ? 32 : 64;
+  t.kt = 128;
+  t.stages = opir::scan_tc_max_stages(t.ntile, t.kt);
+  return t;
+}
+
+void launch_scan_any(opir_server *s, uint32_t n) {
+  const opir::Shape &sh = s->shape;
+  // the tensor-core form needs n0 <= 8192 (int32 accumulators, see
+  // opir_scan_tc.cu); larger first dimensions use the CUDA-core form
+  const bool tc_ok = sh.n0p <= 8192;
+  const bool tc = tc_ok && (s->scan_mode == 1 || (s->scan_mode == 0 && n >= kTcMinBatch));
+  if (!tc) {
+    opir::launch_scan(s->dp, sh, s->db8.p, s->qb.p, s->cmat.p, n, s->stream);
+    return;
+  }
+  launch_scan_tc_tile(s, n, effective_tile(s, n));
 }
 
 // First dimension: NTT + transpose of the first n0 leaves, scan, gather + INTT.
@@ -512,7 +550,8 @@ opir_status opir_server_create(const opir_params *params, int device, opir_serve
     const uint64_t db_bytes = 2ull * kN * 4 * sh.other * sh.n0p;
     s->db8.alloc(db_bytes);
     ck(cudaMemsetAsync(s->db8.p, 0, db_bytes, s->stream), "db memset");
-    opir::make_plane_map(&s->map_db, s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128);
+    opir::make_plane_map(&s->map_db[0], s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128, 128);
+    opir::make_plane_map(&s->map_db[1], s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128, 64);
     s->err.alloc(1);
     ck(cudaMemsetAsync(s->err.p, 0, sizeof(uint32_t), s->stream), "err memset");
     ck(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
@@ -773,6 +812,61 @@ opir_status opir_server_reserve(opir_server *s, uint32_t max_batch) {
     ensure_capacity(s, max_batch);
     grow_keyptr_slots(s, 2ull * max_batch);
   });
+}
+
+opir_status opir_server_autotune(opir_server *s, uint32_t max_batch) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!s->db_loaded) throw std::runtime_error("autotune before load_data");
+    if (max_batch == 0) throw std::invalid_argument("max_batch must be positive");
+    if (s->shape.n0p > 8192) return;  // the CUDA-core scan has no tiling to tune
+    DeviceGuard g(s->device);
+    ensure_capacity(s, max_batch);
+    std::vector<ScanTile> cands;
+    for (uint32_t kt : {128u, 64u})
+      for (uint32_t nt : {16u, 32u, 64u}) {
+        const uint32_t hi = opir::scan_tc_max_stages(nt, kt);
+        for (uint32_t st = std::max(2u, hi > 2 ? hi - 1 : 2u); st <= hi; ++st) cands.push_back({nt, kt, st});
+      }
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    try {
+      for (int b = 0; b < kTileBuckets; ++b) {
+        const uint32_t n = std::min<uint32_t>(1u << b, max_batch);
+        float best = 1e30f;
+        for (const ScanTile &c : cands) {
+          if (c.ntile > 16 && 2 * n <= c.ntile / 2) continue;  // mostly empty tiles
+          launch_scan_tc_tile(s, n, c);
+          ck(cudaEventRecord(e0, s->stream), "event record");
+          for (int r = 0; r < 3; ++r) launch_scan_tc_tile(s, n, c);
+          ck(cudaEventRecord(e1, s->stream), "event record");
+          ck(cudaEventSynchronize(e1), "autotune");
+          float ms = 0;
+          ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+          if (ms < best) { best = ms; s->tile[b] = c; }
+        }
+        check_device_error(s);
+        if (n == max_batch) break;
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  });
+}
+
+opir_status opir_server_scan_tile(const opir_server *s, uint32_t n, uint32_t *ntile, uint32_t *kt,
+                                  uint32_t *stages) {
+  if (!s || !ntile || !kt || !stages || n == 0) return OPIR_ERR_INVALID_ARGUMENT;
+  const ScanTile t = effective_tile(s, n);
+  *ntile = t.ntile;
+  *kt = t.kt;
+  *stages = t.stages;
+  return OPIR_OK;
 }
 
 opir_status opir_server_set_stage_timing(opir_server *s, int enabled) {

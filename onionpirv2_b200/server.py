@@ -234,6 +234,18 @@ class PirServer:
         that later calls of that size allocate no device memory."""
         self._check(self._lib.opir_server_reserve(self._h, int(max_batch)))
 
+    def autotune(self, max_batch: int):
+        """Time the tensor-core scan's tilings on this database for batches
+        up to max_batch and keep the fastest per batch-size bucket."""
+        self._check(self._lib.opir_server_autotune(self._h, int(max_batch)))
+
+    def scan_tile(self, n: int) -> dict:
+        """Tiling of the first-dimension scan for a batch of n queries."""
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self._check(self._lib.opir_server_scan_tile(self._h, int(n), C.byref(a), C.byref(b),
+                                                    C.byref(c)))
+        return {"ntile": a.value, "kt": b.value, "stages": c.value}
+
     def set_stage_timing(self, enabled: bool):
         self._check(self._lib.opir_server_set_stage_timing(self._h, 1 if enabled else 0))
 

@@ -185,3 +185,47 @@ def test_batched_scan_kernels(mode, batch, monkeypatch):
         assert np.array_equal(out[i], srv.make_query(7, queries[i]))
         assert np.array_equal(cl.decrypt(out[i]),
                               O.db_plaintext(c["db_seed"], idx[i], op).astype(np.uint64))
+
+
+TILINGS = [(16, 128, 2), (16, 128, 3), (32, 128, 2), (64, 128, 2), (16, 64, 6), (32, 64, 5),
+           (64, 64, 4), (64, 64, 3)]
+
+
+@pytest.mark.parametrize("tiling", TILINGS, ids=lambda t: "x".join(map(str, t)))
+def test_every_scan_tiling_matches(tiling, monkeypatch):
+    """Each tensor-core tiling the autotuner may pick (query columns per tile,
+    K bytes per stage with its swizzle, pipeline depth), on a batch that
+    spans two column tiles of 16 and on the single query, against the
+    reference golden and the single-query answers."""
+    name = "c1_16384_h9"
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    monkeypatch.setenv("OPIR_SCAN_TILE", ",".join(map(str, tiling)))
+    rng = np.random.default_rng(sum(tiling))
+    idx = [int(i) for i in rng.integers(0, c["target_num_pt"], 11)]
+    queries = np.stack([q] + [cl.query(i) for i in idx])
+    with PirServer(gp) as s2:
+        s2.load_data_seeded(c["target_num_pt"], c["db_seed"])
+        s2.set_client_keys(7, bv, gsw)
+        assert s2.scan_tile(12) == dict(zip(("ntile", "kt", "stages"), tiling))
+        _check_response(c, cl, op, s2.make_query(7, q))
+        out = s2.make_query_batch([7] * len(queries), queries)
+    _check_response(c, cl, op, out[0])
+    for i in range(len(idx)):
+        assert np.array_equal(cl.decrypt(out[i + 1]),
+                              O.db_plaintext(c["db_seed"], idx[i], op).astype(np.uint64))
+
+
+def test_autotune_keeps_results():
+    name = "c1_16384_h9"
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    with PirServer(gp) as s2:
+        s2.load_data_seeded(c["target_num_pt"], c["db_seed"])
+        s2.set_client_keys(7, bv, gsw)
+        s2.autotune(8)
+        for n in (1, 2, 5, 8):
+            t = s2.scan_tile(n)
+            assert t["ntile"] in (16, 32, 64) and t["kt"] in (64, 128) and t["stages"] >= 2
+        _check_response(c, cl, op, s2.make_query(7, q))
+        out = s2.make_query_batch([7] * 5, np.stack([q] * 5))
+        for i in range(5):
+            _check_response(c, cl, op, out[i])
