@@ -37,7 +37,7 @@ DB_SEED = 20261203
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--target", type=int, default=TARGET,
                     help="plaintexts (smaller layouts are for profiling captures)")
     ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default scan tiling (or OPIR_SCAN_TILE)")
     ap.add_argument("--serve", action="store_true",
                     help="serving loop: Poisson arrivals over three resident databases")
     ap.add_argument("--rates", default="50,500,2000", help="offered queries/s (--serve)")
@@ -94,7 +96,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -205,8 +207,11 @@ def bench_reference(args, world, rank):
     if rank != 0:
         return
     procs = os.cpu_count() or 1
+    # a bounded sample: at most 8 timed queries (and 1 warm-up) per process,
+    # ~2 s each on one core, so the run ends within a few minutes
+    n_q, n_w = min(args.steps, 8), min(args.warmup, 1)
     try:
-        res = run_reference(args.steps, args.warmup, procs, 7)
+        res = run_reference(n_q, n_w, procs, 7)
     except Exception as e:  # reference binary missing or failed
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU server: {e}"}))
         return
@@ -220,7 +225,8 @@ def bench_reference(args, world, rank):
                    "batch": 1, "parallelism": f"{procs} host processes"},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": procs, "kind": "reference",
                          "sample": (f"reference make_query (oracle/_ref/{res['binary']}, HEXL stand-in) "
-                                    f"on {procs} forked processes x {args.steps} queries after one load_data; "
+                                    f"on {procs} forked processes x {n_q} queries ({n_w} warm-up) after one "
+                                    f"load_data; "
                                     f"CPU {cpu_model()}")},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -251,7 +257,8 @@ def bench_ours(args, world, rank, local):
     for b, (bv, gsw) in enumerate(keys):
         srv.set_client_keys(b, bv, gsw)
     t0 = time.perf_counter()
-    srv.autotune(B)                      # scan tiling per batch bucket (setup, untimed)
+    if not args.no_autotune:
+        srv.autotune(B)                  # scan tiling per batch bucket (setup, untimed)
     tune_s = time.perf_counter() - t0
     ids = list(range(B))
     # a dedicated (non-default) stream: the library orders its own stream
@@ -264,6 +271,14 @@ def bench_ours(args, world, rank, local):
     def step(n, qbuf, rbuf):
         srv.make_query_batch_device(ids[:n], qbuf.data_ptr(), rbuf.data_ptr(), stream.cuda_stream)
 
+    def nvtx(name):
+        """NVTX range around a timed loop (lets a profiler select it)."""
+        import contextlib
+        try:
+            return torch.cuda.nvtx.range(name)
+        except Exception:
+            return contextlib.nullcontext()
+
     def timed(n, steps, warm):
         qb, rb = d_q[:n].contiguous(), d_r[:n].contiguous()
         for _ in range(warm):
@@ -274,11 +289,12 @@ def bench_ours(args, world, rank, local):
         evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
         srv.set_stage_timing(True)
         l0 = launch_count()
-        evs[0].record(stream)
-        for i in range(steps):
-            step(n, qb, rb)
-            evs[i + 1].record(stream)
-        torch.cuda.synchronize(device)
+        with nvtx(f"timed_b{n}"):
+            evs[0].record(stream)
+            for i in range(steps):
+                step(n, qb, rb)
+                evs[i + 1].record(stream)
+            torch.cuda.synchronize(device)
         launches = launch_count() - l0
         barrier(world, device)
         per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
