@@ -4,10 +4,12 @@
 // opir_device.cuh. Thread t owns coefficient positions t + 256 s, s < 8, for
 // every per-coefficient step, so global reads of planes are coalesced.
 #include "opir_kernels.h"
+#include "opir_ntt.cuh"
 
 #include <atomic>
 #include <map>
 #include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -22,10 +24,6 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
-}
-
-__device__ __forceinline__ ResidueTables pick(const DevParams &P, int res) {
-  return res ? P.r[1] : P.r[0];
 }
 
 std::atomic<uint64_t> g_launches{0};
@@ -85,14 +83,15 @@ __global__ void k_compose_u64(DevParams P, const uint32_t *__restrict__ in, uint
 // --------------------------------------------------------- DB preprocessing
 constexpr int kDbTile = 8;  // plaintexts per block (one padded plane each)
 
-__global__ void __launch_bounds__(kThreads, 2)
-k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
-                uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
-                uint64_t logical, uint32_t n0, uint32_t n0p, uint32_t other,
-                uint64_t pt_begin, uint64_t pt_end, uint8_t *__restrict__ db8) {
+template <int RES>
+__device__ __forceinline__ void db_preprocess_body(const DevParams &P, const uint16_t *coeffs,
+                                                   uint64_t coeff_pt_begin, uint64_t seed,
+                                                   uint64_t t, uint64_t logical, uint32_t n0,
+                                                   uint32_t n0p, uint32_t other, uint64_t pt_begin,
+                                                   uint64_t pt_end, uint8_t *db8) {
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y, tid = threadIdx.x;
-  const ResidueTables T = pick(P, res);
+  const int tid = threadIdx.x;
+  const ResidueTables &T = P.r[RES];
   const uint64_t pt0 = pt_begin + (uint64_t)blockIdx.x * kDbTile;
   for (int e = 0; e < kDbTile; ++e) {
     const uint64_t pt = pt0 + e;
@@ -109,22 +108,28 @@ k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
       }
       v[k] = x;  // x < t < q_res: canonical
     }
-    fwdA(v, T);
+    fA<RES>(v);
     st_plane<0>(sm + e * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid(sm, kDbTile, T);
+  fwd_mid_r<RES>(sm, kDbTile, T.fwt);
   uint32_t out[kDbTile][8];
+  {
+    uint2 wd[6];
+    fload_d(wd, T.fwt, tid);
 #pragma unroll
-  for (int e = 0; e < kDbTile; ++e) {
-    ld_plane<3>(sm + e * kPad, out[e], tid);
-    fwdD(out[e], T, tid);
+    for (int e = 0; e < kDbTile; ++e) {
+      ld_plane<3>(sm + e * kPad, out[e], tid);
+      fD<RES>(out[e], wd);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) out[e][k] = canon8<RES>(out[e][k]);
+    }
   }
   // byte planes: db8[((res N + level) 4 + plane) other + row][n0p], pt = row n0 + k
   const bool packed = (n0 % kDbTile) == 0 && pt0 + kDbTile <= pt_end;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const uint64_t zl = (uint64_t)res * kN + posD(tid, k);
+    const uint64_t zl = (uint64_t)RES * kN + posD(tid, k);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       uint8_t *plane = db8 + (zl * 4 + j) * (uint64_t)other * n0p;
@@ -148,23 +153,38 @@ k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
   }
 }
 
+__global__ void __launch_bounds__(kThreads, 2)
+k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
+                uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
+                uint64_t logical, uint32_t n0, uint32_t n0p, uint32_t other,
+                uint64_t pt_begin, uint64_t pt_end, uint8_t *__restrict__ db8) {
+  if (blockIdx.y == 0)
+    db_preprocess_body<0>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin,
+                          pt_end, db8);
+  else
+    db_preprocess_body<1>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin,
+                          pt_end, db8);
+}
+
 // ----------------------------------------------------------- expansion level
 // One heap node (and one residue) per block: BV key switch of the node's
 // ciphertext (bv_keyswitch.cpp:296-367) then the two children
 // (server.cpp:794-809): left = c + c', right = (c - c') X^-k.
 // sigma_k is applied as a gather: sigma(c)[j] = +-c[j k^-1 mod 2N].
-__global__ void __launch_bounds__(kThreads, 2)
-k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, int l_ks,
-               const uint32_t *__restrict__ in, uint64_t in_stride,
-               uint32_t *__restrict__ out, uint64_t out_stride,
-               const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+template <int RES>
+__device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t galois_inv,
+                                                  uint32_t kshift, int base_ks, int l_ks,
+                                                  const uint32_t *in, uint64_t in_stride,
+                                                  uint32_t *out, uint64_t out_stride,
+                                                  const uint32_t *const *bv_keys,
+                                                  uint64_t bv_level_off) {
   extern __shared__ uint32_t sm[];
-  const int node = blockIdx.x, res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
-  const ResidueTables T = pick(P, res);
-  const uint32_t q = T.q;
+  constexpr uint32_t q = Res<RES>::q;
+  const int node = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
+  const ResidueTables &T = P.r[RES];
   const uint32_t *ct = in + ((uint64_t)b * in_stride + node) * kCtWords;
-  const uint32_t *c0 = ct + res * kN;
-  const uint32_t *c1 = ct + 2 * kN + res * kN;
+  const uint32_t *c0 = ct + RES * kN;
+  const uint32_t *c1 = ct + 2 * kN + RES * kN;
 
   // sigma_k(c0) (own residue) and the centred sigma_k(c1) at A-order positions
   uint32_t s0[8];
@@ -184,48 +204,58 @@ k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, i
     uint32_t v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) v[k] = digit_residue(next_digit(d[k], base_ks), q);
-    fwdA(v, T);
+    fA<RES>(v);
     st_plane<0>(sm + i * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid(sm, l_ks, T);
-  // inner product with the key rows (row t encrypts sigma(s) B^t), D-order
-  const uint32_t *key = bv_keys[b] + bv_level_off + res * kN;
+  fwd_mid_r<RES>(sm, l_ks, T.fwt);
+  // inner product with the key rows (row t encrypts sigma(s) B^t), D-order;
+  // digit NTT values stay in [0, 4q) when l_ks <= 8 (sum < 2^64), else canonical
+  const uint32_t *key = bv_keys[b] + bv_level_off + RES * kN;
+  const bool lazy = l_ks <= 8;
   uint64_t ab[8], aa[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
-  for (int i = 0; i < l_ks; ++i) {
-    uint32_t v[8];
-    ld_plane<3>(sm + i * kPad, v, tid);
-    fwdD(v, T, tid);
+  {
+    uint2 wd[6];
+    fload_d(wd, T.fwt, tid);
+    for (int i = 0; i < l_ks; ++i) {
+      uint32_t v[8];
+      ld_plane<3>(sm + i * kPad, v, tid);
+      fD<RES>(v, wd);
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int j0 = 4 * (tid + 256 * h);
-      const uint4 kb = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(i * 4 + 0) * kN + j0));
-      const uint4 ka = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(i * 4 + 2) * kN + j0));
-      ab[4 * h + 0] += (uint64_t)v[4 * h + 0] * kb.x; aa[4 * h + 0] += (uint64_t)v[4 * h + 0] * ka.x;
-      ab[4 * h + 1] += (uint64_t)v[4 * h + 1] * kb.y; aa[4 * h + 1] += (uint64_t)v[4 * h + 1] * ka.y;
-      ab[4 * h + 2] += (uint64_t)v[4 * h + 2] * kb.z; aa[4 * h + 2] += (uint64_t)v[4 * h + 2] * ka.z;
-      ab[4 * h + 3] += (uint64_t)v[4 * h + 3] * kb.w; aa[4 * h + 3] += (uint64_t)v[4 * h + 3] * ka.w;
+      for (int k = 0; k < 8; ++k) v[k] = lazy ? to4q<RES>(v[k]) : canon8<RES>(v[k]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j0 = 4 * (tid + 256 * h);
+        const uint4 kb = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(i * 4 + 0) * kN + j0));
+        const uint4 ka = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(i * 4 + 2) * kN + j0));
+        ab[4 * h + 0] += (uint64_t)v[4 * h + 0] * kb.x; aa[4 * h + 0] += (uint64_t)v[4 * h + 0] * ka.x;
+        ab[4 * h + 1] += (uint64_t)v[4 * h + 1] * kb.y; aa[4 * h + 1] += (uint64_t)v[4 * h + 1] * ka.y;
+        ab[4 * h + 2] += (uint64_t)v[4 * h + 2] * kb.z; aa[4 * h + 2] += (uint64_t)v[4 * h + 2] * ka.z;
+        ab[4 * h + 3] += (uint64_t)v[4 * h + 3] * kb.w; aa[4 * h + 3] += (uint64_t)v[4 * h + 3] * ka.w;
+      }
     }
   }
   __syncthreads();
   {
+    uint2 wd[6];
+    iload_d(wd, T.iwt, tid);
     uint32_t v[8], w[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { v[k] = reduce64(ab[k], q, T.mu); w[k] = reduce64(aa[k], q, T.mu); }
-    invD(v, T, tid);
-    invD(w, T, tid);
+    for (int k = 0; k < 8; ++k) { v[k] = red64<RES>(ab[k]); w[k] = red64<RES>(aa[k]); }
+    iD<RES>(v, wd);
+    iD<RES>(w, wd);
     st_plane<3>(sm, v, tid);
     st_plane<3>(sm + kPad, w, tid);
   }
   __syncthreads();
-  inv_mid(sm, 2, T);
+  inv_mid_r<RES>(sm, 2, T.iwt);
   uint32_t db_[8], da[8];
   ld_plane<0>(sm, db_, tid);
   ld_plane<0>(sm + kPad, da, tid);
-  invA(db_, T);
-  invA(da, T);
+  iA<RES>(db_);
+  iA<RES>(da);
   uint32_t *outL = out + ((uint64_t)b * out_stride + 2 * (uint64_t)node) * kCtWords;
   uint32_t *outR = outL + kCtWords;
 #pragma unroll
@@ -234,15 +264,28 @@ k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, i
     const uint32_t n0v = add_mod(s0[k], db_[k], q);  // c0' = sigma(c0) + delta_b
     const uint32_t n1v = da[k];                      // c1' = delta_a
     const uint32_t o0 = c0[j], o1 = c1[j];
-    outL[res * kN + j] = add_mod(o0, n0v, q);
-    outL[2 * kN + res * kN + j] = add_mod(o1, n1v, q);
+    outL[RES * kN + j] = add_mod(o0, n0v, q);
+    outL[2 * kN + RES * kN + j] = add_mod(o1, n1v, q);
     const uint32_t d0 = sub_mod(o0, n0v, q), d1 = sub_mod(o1, n1v, q);
     int dst = j - static_cast<int>(kshift);
     const bool wrap = dst < 0;
     if (wrap) dst += kN;
-    outR[res * kN + dst] = wrap ? neg_mod(d0, q) : d0;
-    outR[2 * kN + res * kN + dst] = wrap ? neg_mod(d1, q) : d1;
+    outR[RES * kN + dst] = wrap ? neg_mod(d0, q) : d0;
+    outR[2 * kN + RES * kN + dst] = wrap ? neg_mod(d1, q) : d1;
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, int l_ks,
+               const uint32_t *__restrict__ in, uint64_t in_stride,
+               uint32_t *__restrict__ out, uint64_t out_stride,
+               const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  if (blockIdx.y == 0)
+    expand_level_body<0>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
+                         bv_keys, bv_level_off);
+  else
+    expand_level_body<1>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
+                         bv_keys, bv_level_off);
 }
 
 // Shared gadget product of a coefficient-form ciphertext (both residues read
@@ -250,13 +293,17 @@ k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, i
 // null) against NTT-form RGSW rows: acc_k += sum_rows digit * rgsw[row][k],
 // accumulated at this thread's D-order positions. Digit i (LSB first) of
 // poly p meets row p*l + (l - 1 - i) (gsw.cpp:283-293). Uses l padded planes.
-__device__ __forceinline__ void gadget_mac(const DevParams &P, const ResidueTables &T,
-                                           int res, const uint32_t *x, const uint32_t *y,
-                                           const uint32_t *rgsw, int l, int base_log2,
-                                           uint32_t *sm, uint64_t (&acc0)[8],
+// Digit NTT values enter the MAC in [0, 4q) when 2 l <= 16 (a sum of 2 l
+// products below 4q x q < 2^60 stays below 2^64), else canonical.
+template <int RES>
+__device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x,
+                                           const uint32_t *y, const uint32_t *rgsw, int l,
+                                           int base_log2, uint32_t *sm, uint64_t (&acc0)[8],
                                            uint64_t (&acc1)[8]) {
-  const uint32_t q = T.q;
+  constexpr uint32_t q = Res<RES>::q;
+  const ResidueTables &T = P.r[RES];
   const int tid = threadIdx.x;
+  const bool lazy = l <= 8;
 #pragma unroll 1
   for (int p = 0; p < 2; ++p) {
     int64_t d[8];
@@ -274,17 +321,21 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const ResidueTabl
       uint32_t v[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) v[k] = digit_residue(next_digit(d[k], base_log2), q);
-      fwdA(v, T);
+      fA<RES>(v);
       st_plane<0>(sm + i * kPad, v, tid);
     }
     __syncthreads();
-    fwd_mid(sm, l, T);
+    fwd_mid_r<RES>(sm, l, T.fwt);
+    uint2 wd[6];
+    fload_d(wd, T.fwt, tid);
     for (int i = 0; i < l; ++i) {
       uint32_t v[8];
       ld_plane<3>(sm + i * kPad, v, tid);
-      fwdD(v, T, tid);
+      fD<RES>(v, wd);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = lazy ? to4q<RES>(v[k]) : canon8<RES>(v[k]);
       const int row = p * l + (l - 1 - i);
-      const uint32_t *R0 = rgsw + (uint64_t)row * kCtWords + res * kN;
+      const uint32_t *R0 = rgsw + (uint64_t)row * kCtWords + RES * kN;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int j0 = 4 * (tid + 256 * h);
@@ -301,29 +352,30 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const ResidueTabl
 }
 
 // -------------------------------------------------------- selector completion
-__global__ void __launch_bounds__(kThreads, 2)
-k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
-            const uint32_t *const *__restrict__ gsw_keys, uint32_t *__restrict__ sel) {
+template <int RES>
+__device__ __forceinline__ void selectors_body(const DevParams &P, const Shape &S,
+                                               const uint32_t *leaves, uint64_t leaf_stride,
+                                               const uint32_t *const *gsw_keys, uint32_t *sel) {
   extern __shared__ uint32_t sm[];
-  const int row_id = blockIdx.x, res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
+  const int row_id = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
   const int selno = row_id / S.l_ep, r = row_id % S.l_ep;
-  const ResidueTables T = pick(P, res);
+  const ResidueTables &T = P.r[RES];
   const uint32_t *ct = leaves + ((uint64_t)b * leaf_stride + S.n0 + row_id) * kCtWords;
   uint32_t *out = sel + ((uint64_t)b * (S.num_dims - 1) + selno) * 2 * S.l_ep * kCtWords;
   uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
   // bottom row: ExtProd(RGSW(s), row) with the key gadget (gsw.cpp:119-182)
-  gadget_mac(P, T, res, ct, nullptr, gsw_keys[b], S.l_key, S.base_key, sm, acc0, acc1);
-  uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords + res * kN;
+  gadget_mac<RES>(P, ct, nullptr, gsw_keys[b], S.l_key, S.base_key, sm, acc0, acc1);
+  uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords + RES * kN;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int j0 = 4 * (tid + 256 * h);
     uint4 o0, o1;
-    o0.x = reduce64(acc0[4 * h + 0], T.q, T.mu); o0.y = reduce64(acc0[4 * h + 1], T.q, T.mu);
-    o0.z = reduce64(acc0[4 * h + 2], T.q, T.mu); o0.w = reduce64(acc0[4 * h + 3], T.q, T.mu);
-    o1.x = reduce64(acc1[4 * h + 0], T.q, T.mu); o1.y = reduce64(acc1[4 * h + 1], T.q, T.mu);
-    o1.z = reduce64(acc1[4 * h + 2], T.q, T.mu); o1.w = reduce64(acc1[4 * h + 3], T.q, T.mu);
+    o0.x = red64<RES>(acc0[4 * h + 0]); o0.y = red64<RES>(acc0[4 * h + 1]);
+    o0.z = red64<RES>(acc0[4 * h + 2]); o0.w = red64<RES>(acc0[4 * h + 3]);
+    o1.x = red64<RES>(acc1[4 * h + 0]); o1.y = red64<RES>(acc1[4 * h + 1]);
+    o1.z = red64<RES>(acc1[4 * h + 2]); o1.w = red64<RES>(acc1[4 * h + 3]);
     *reinterpret_cast<uint4 *>(bot + j0) = o0;
     *reinterpret_cast<uint4 *>(bot + 2 * kN + j0) = o1;
   }
@@ -332,23 +384,36 @@ k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t 
   for (int p = 0; p < 2; ++p) {
     uint32_t v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = ct[(p * 2 + res) * kN + posA(tid, k)];
-    fwdA(v, T);
+    for (int k = 0; k < 8; ++k) v[k] = ct[(p * 2 + RES) * kN + posA(tid, k)];
+    fA<RES>(v);
     st_plane<0>(sm + p * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid(sm, 2, T);
-  uint32_t *top = out + (uint64_t)r * kCtWords + res * kN;
+  fwd_mid_r<RES>(sm, 2, T.fwt);
+  uint32_t *top = out + (uint64_t)r * kCtWords + RES * kN;
+  uint2 wd[6];
+  fload_d(wd, T.fwt, tid);
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
     uint32_t v[8];
     ld_plane<3>(sm + p * kPad, v, tid);
-    fwdD(v, T, tid);
+    fD<RES>(v, wd);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = canon8<RES>(v[k]);
 #pragma unroll
     for (int h = 0; h < 2; ++h)
       *reinterpret_cast<uint4 *>(top + p * 2 * kN + 4 * (tid + 256 * h)) =
           make_uint4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
+            const uint32_t *const *__restrict__ gsw_keys, uint32_t *__restrict__ sel) {
+  if (blockIdx.y == 0)
+    selectors_body<0>(P, S, leaves, leaf_stride, gsw_keys, sel);
+  else
+    selectors_body<1>(P, S, leaves, leaf_stride, gsw_keys, sel);
 }
 
 // ------------------------------------------------------- first-dim query prep
@@ -357,25 +422,28 @@ k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t 
 // coalesced quads; k_fst_pack then turns them into byte planes.
 constexpr int kFstTile = 4;  // ciphertexts per block (8 planes)
 
-__global__ void __launch_bounds__(kThreads, 2)
-k_fst_ntt(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
-          uint32_t *__restrict__ out, uint64_t out_stride) {
+template <int RES>
+__device__ __forceinline__ void fst_ntt_body(const DevParams &P, const Shape &S,
+                                             const uint32_t *leaves, uint64_t leaf_stride,
+                                             uint32_t *out, uint64_t out_stride) {
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
+  const int b = blockIdx.z, tid = threadIdx.x;
   const uint32_t k0 = blockIdx.x * kFstTile;
-  const ResidueTables T = pick(P, res);
+  const ResidueTables &T = P.r[RES];
   for (int e = 0; e < 2 * kFstTile; ++e) {
     const uint32_t kk = k0 + (e >> 1);
     const int p = e & 1;
     uint32_t v[8];
-    const uint32_t *src = leaves + ((uint64_t)b * leaf_stride + kk) * kCtWords + (p * 2 + res) * kN;
+    const uint32_t *src = leaves + ((uint64_t)b * leaf_stride + kk) * kCtWords + (p * 2 + RES) * kN;
 #pragma unroll
     for (int k = 0; k < 8; ++k) v[k] = kk < S.n0 ? src[posA(tid, k)] : 0u;
-    fwdA(v, T);
+    fA<RES>(v);
     st_plane<0>(sm + e * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid(sm, 2 * kFstTile, T);
+  fwd_mid_r<RES>(sm, 2 * kFstTile, T.fwt);
+  uint2 wd[6];
+  fload_d(wd, T.fwt, tid);
 #pragma unroll
   for (int e = 0; e < 2 * kFstTile; ++e) {
     const uint32_t kk = k0 + (e >> 1);
@@ -383,13 +451,24 @@ k_fst_ntt(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t le
     const int p = e & 1;
     uint32_t v[8];
     ld_plane<3>(sm + e * kPad, v, tid);
-    fwdD(v, T, tid);
-    uint32_t *dst = out + ((uint64_t)b * out_stride + kk) * kCtWords + (p * 2 + res) * kN;
+    fD<RES>(v, wd);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = canon8<RES>(v[k]);
+    uint32_t *dst = out + ((uint64_t)b * out_stride + kk) * kCtWords + (p * 2 + RES) * kN;
 #pragma unroll
     for (int h = 0; h < 2; ++h)
       *reinterpret_cast<uint4 *>(dst + 4 * (tid + 256 * h)) =
           make_uint4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_fst_ntt(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
+          uint32_t *__restrict__ out, uint64_t out_stride) {
+  if (blockIdx.y == 0)
+    fst_ntt_body<0>(P, S, leaves, leaf_stride, out, out_stride);
+  else
+    fst_ntt_body<1>(P, S, leaves, leaf_stride, out, out_stride);
 }
 
 // Byte-plane packing of the NTT-form query matrix:
@@ -531,18 +610,18 @@ k_scan(DevParams P, uint32_t n0, uint32_t n0p, uint32_t m, const uint8_t *__rest
 // the scan. cmat is [residue x level][column][row]; a block transforms 8
 // adjacent rows of one column and one residue, so the 8 words it reads per
 // level are one contiguous 32-byte sector.
-template <bool VEC>
-__global__ void __launch_bounds__(kThreads, 2)
-k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_t ncols,
-                uint32_t *__restrict__ mid, uint64_t mid_stride) {
+template <int RES, bool VEC>
+__device__ __forceinline__ void scan_epilogue_body(const DevParams &P, const Shape &S,
+                                                   const uint32_t *cmat, uint32_t ncols,
+                                                   uint32_t *mid, uint64_t mid_stride) {
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y, tid = threadIdx.x;
+  const int tid = threadIdx.x;
   const uint32_t r0 = blockIdx.x * 8, c = blockIdx.z;
-  const ResidueTables T = pick(P, res);
+  const ResidueTables &T = P.r[RES];
   uint32_t v[8][8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const uint32_t *src = cmat + (((uint64_t)res * kN + posD(tid, k)) * ncols + c) * S.other + r0;
+    const uint32_t *src = cmat + (((uint64_t)RES * kN + posD(tid, k)) * ncols + c) * S.other + r0;
     if (VEC && r0 + 8 <= S.other) {
       const uint4 lo = __ldg(reinterpret_cast<const uint4 *>(src));
       const uint4 hi = __ldg(reinterpret_cast<const uint4 *>(src + 4));
@@ -553,80 +632,108 @@ k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_
       for (int e = 0; e < 8; ++e) v[e][k] = r0 + e < S.other ? __ldg(src + e) : 0u;
     }
   }
+  {
+    uint2 wd[6];
+    iload_d(wd, T.iwt, tid);
 #pragma unroll
-  for (int e = 0; e < 8; ++e) {
-    invD(v[e], T, tid);
-    st_plane<3>(sm + e * kPad, v[e], tid);
+    for (int e = 0; e < 8; ++e) {
+      iD<RES>(v[e], wd);
+      st_plane<3>(sm + e * kPad, v[e], tid);
+    }
   }
   __syncthreads();
-  inv_mid(sm, 8, T);
-  uint32_t *dst0 = mid + (uint64_t)(c >> 1) * mid_stride * kCtWords + ((c & 1) * 2 + res) * kN;
+  inv_mid_r<RES>(sm, 8, T.iwt);
+  uint32_t *dst0 = mid + (uint64_t)(c >> 1) * mid_stride * kCtWords + ((c & 1) * 2 + RES) * kN;
   for (int e = 0; e < 8; ++e) {
     const uint32_t r = r0 + e;
     if (r >= S.other) break;  // uniform over the block
     uint32_t w[8];
     ld_plane<0>(sm + e * kPad, w, tid);
-    invA(w, T);
+    iA<RES>(w);
     uint32_t *dst = dst0 + (uint64_t)r * kCtWords;
 #pragma unroll
     for (int k = 0; k < 8; ++k) dst[posA(tid, k)] = w[k];
   }
 }
 
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads, 2)
+k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_t ncols,
+                uint32_t *__restrict__ mid, uint64_t mid_stride) {
+  if (blockIdx.y == 0)
+    scan_epilogue_body<0, VEC>(P, S, cmat, ncols, mid, mid_stride);
+  else
+    scan_epilogue_body<1, VEC>(P, S, cmat, ncols, mid, mid_stride);
+}
+
 // --------------------------------------------------------------- MUX level
 // ext_prod_mux (server.cpp:652-722): out = x + INTT(ExtProd(sel, y - x)).
-__global__ void __launch_bounds__(kThreads, 2)
-k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t offset,
-            uint32_t half, const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-            uint64_t mid_stride, const uint32_t *__restrict__ sel) {
+template <int RES>
+__device__ __forceinline__ void mux_level_body(const DevParams &P, const Shape &S, uint32_t level,
+                                               uint32_t n_pairs, uint32_t offset, uint32_t half,
+                                               const uint32_t *in, uint32_t *out,
+                                               uint64_t mid_stride, const uint32_t *sel) {
   extern __shared__ uint32_t sm[];
-  const int res = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
+  constexpr uint32_t q = Res<RES>::q;
+  const int b = blockIdx.z, tid = threadIdx.x;
   const uint32_t i = blockIdx.x;
   const uint32_t *base_in = in + (uint64_t)b * mid_stride * kCtWords;
   uint32_t *base_out = out + (uint64_t)b * mid_stride * kCtWords;
   if (i >= n_pairs) {  // level 0: carry the unpaired prefix over unchanged
     const uint32_t c = i - n_pairs;
     for (int j = tid; j < kN; j += kThreads) {
-      base_out[(uint64_t)c * kCtWords + res * kN + j] = base_in[(uint64_t)c * kCtWords + res * kN + j];
-      base_out[(uint64_t)c * kCtWords + 2 * kN + res * kN + j] =
-          base_in[(uint64_t)c * kCtWords + 2 * kN + res * kN + j];
+      base_out[(uint64_t)c * kCtWords + RES * kN + j] = base_in[(uint64_t)c * kCtWords + RES * kN + j];
+      base_out[(uint64_t)c * kCtWords + 2 * kN + RES * kN + j] =
+          base_in[(uint64_t)c * kCtWords + 2 * kN + RES * kN + j];
     }
     return;
   }
   uint32_t xi, yi, oi;
   if (level == 0) { xi = offset + 2 * i; yi = xi + 1; oi = offset + i; }
   else { xi = i; yi = i + half; oi = i; }
-  const ResidueTables T = pick(P, res);
+  const ResidueTables &T = P.r[RES];
   const uint32_t *x = base_in + (uint64_t)xi * kCtWords;
   const uint32_t *y = base_in + (uint64_t)yi * kCtWords;
   const uint32_t *rgsw = sel + ((uint64_t)b * (S.num_dims - 1) + level) * 2 * S.l_ep * kCtWords;
   uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
-  gadget_mac(P, T, res, x, y, rgsw, S.l_ep, S.base_ep, sm, acc0, acc1);
+  gadget_mac<RES>(P, x, y, rgsw, S.l_ep, S.base_ep, sm, acc0, acc1);
   {
+    uint2 wd[6];
+    iload_d(wd, T.iwt, tid);
     uint32_t v[8], w[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { v[k] = reduce64(acc0[k], T.q, T.mu); w[k] = reduce64(acc1[k], T.q, T.mu); }
-    invD(v, T, tid);
-    invD(w, T, tid);
+    for (int k = 0; k < 8; ++k) { v[k] = red64<RES>(acc0[k]); w[k] = red64<RES>(acc1[k]); }
+    iD<RES>(v, wd);
+    iD<RES>(w, wd);
     st_plane<3>(sm, v, tid);
     st_plane<3>(sm + kPad, w, tid);
   }
   __syncthreads();
-  inv_mid(sm, 2, T);
+  inv_mid_r<RES>(sm, 2, T.iwt);
   uint32_t *o = base_out + (uint64_t)oi * kCtWords;
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
     uint32_t v[8];
     ld_plane<0>(sm + p * kPad, v, tid);
-    invA(v, T);
+    iA<RES>(v);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int j = posA(tid, k);
-      o[(p * 2 + res) * kN + j] = add_mod(x[(p * 2 + res) * kN + j], v[k], T.q);
+      o[(p * 2 + RES) * kN + j] = add_mod(x[(p * 2 + RES) * kN + j], v[k], q);
     }
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t offset,
+            uint32_t half, const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+            uint64_t mid_stride, const uint32_t *__restrict__ sel) {
+  if (blockIdx.y == 0)
+    mux_level_body<0>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
+  else
+    mux_level_body<1>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
 }
 
 // ------------------------------------------------ modulus switch + packing
@@ -678,6 +785,34 @@ inline unsigned grid1d(uint64_t n) {
 
 // ===================================================================== launchers
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+void upload_ntt_constants(const uint32_t q[2], const uint32_t *const fw[2],
+                          const uint32_t *const fw_sh[2], const uint32_t *const iw[2],
+                          const uint32_t *const iw_sh[2], const uint32_t nscale[2][4]) {
+  if (q[0] != kQ1 || q[1] != kQ2)
+    throw std::invalid_argument("the kernels are compiled for the CONFIG_N2048_K1_COMP moduli");
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(dev)) return;
+  uint2 f[2][64], i[2][64];
+  uint4 sc[2];
+  for (int r = 0; r < 2; ++r) {
+    for (int k = 0; k < 64; ++k) {
+      f[r][k] = make_uint2(fw[r][k], fw_sh[r][k]);
+      i[r][k] = make_uint2(iw[r][k], iw_sh[r][k]);
+    }
+    sc[r] = make_uint4(nscale[r][0], nscale[r][1], nscale[r][2], nscale[r][3]);
+  }
+  cudaError_t e = cudaMemcpyToSymbol(c_fwt, f, sizeof(f));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_iwt, i, sizeof(i));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_nscale, sc, sizeof(sc));
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("NTT constants: ") + cudaGetErrorString(e));
+  done.insert(dev);
+}
 
 void launch_split_u64(const DevParams &P, const uint64_t *in, uint32_t *out, uint64_t n_items,
                       uint64_t per_item, uint64_t out_item_stride, cudaStream_t st) {

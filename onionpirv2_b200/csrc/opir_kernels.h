@@ -65,6 +65,15 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
                       uint64_t leaf_stride, const uint32_t *const *gsw_keys,
                       uint32_t *sel, uint32_t batch, cudaStream_t st);
 
+// Twiddles with index < 64 (value and Shoup companion, forward and inverse)
+// and {N^-1, Shoup, iw[1] N^-1, Shoup} of both residues, copied to the
+// kernels' constant memory on the current device. Once per device; later
+// calls are no-ops. Throws if q differs from the moduli the kernels are
+// compiled for.
+void upload_ntt_constants(const uint32_t q[2], const uint32_t *const fw[2],
+                          const uint32_t *const fw_sh[2], const uint32_t *const iw[2],
+                          const uint32_t *const iw_sh[2], const uint32_t nscale[2][4]);
+
 // First-dimension query matrix (src/server.cpp:332-346 + 264-304): NTT of the
 // first n0 leaves of each query, written as byte planes
 // qb[((res N + level) 4 + plane) 2 batch + column][n0p], column = 2 b + poly.

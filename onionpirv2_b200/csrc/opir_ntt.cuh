@@ -1,0 +1,264 @@
+// Residue-specialised register NTT for the query-path kernels.
+//
+// Same transform, layout and positions as the register-resident NTT of
+// opir_device.cuh (radix 8/8/8/4, A/B/C/D thread positions, padded planes),
+// with three changes that cut instructions per butterfly:
+//   * the residue is a template parameter, so q is an immediate;
+//   * twiddles with index < 64 (passes A and B, uniform over a warp) and the
+//     inverse scaling constants live in constant memory; the per-thread
+//     twiddles of passes C and D are loaded once per plane loop instead of
+//     once per plane;
+//   * forward butterflies correct X only where the bound needs it. With
+//     canonical inputs and Shoup products t in [0, 2q), an uncorrected
+//     butterfly maps [0, b q) to [0, (b + 2) q) and a corrected one (X taken
+//     to [0, 4q) first) maps [0, 8q) to [0, 6q); correcting stages 4, 6, 8
+//     and 10 keeps every value below 8q < 2^32 (q < 2^29), and the output
+//     lies in [0, 8q).
+// This header defines constant-memory arrays and is included by one
+// translation unit only (opir_kernels.cu), which uploads them per device.
+#pragma once
+
+#include "opir_device.cuh"
+
+namespace opir {
+
+constexpr uint32_t kQ1 = 536813569u;  // CONFIG_N2048_K1_COMP composite limbs
+constexpr uint32_t kQ2 = 536752129u;
+
+template <int RES>
+struct Res {
+  static constexpr uint32_t q = RES ? kQ2 : kQ1;
+  static constexpr uint64_t mu = ~0ull / q;  // floor(2^64 / q) (q odd, > 1)
+};
+
+// (w, floor(w 2^32 / q)) for twiddle indices < 64: [residue][index]
+static __constant__ uint2 c_fwt[2][64];
+static __constant__ uint2 c_iwt[2][64];
+// {N^-1, its Shoup companion, iw[1] N^-1, its Shoup companion} per residue
+static __constant__ uint4 c_nscale[2];
+
+template <int RES>
+__device__ __forceinline__ uint32_t red64(uint64_t x) {  // any x -> [0, q)
+  constexpr uint32_t Q = Res<RES>::q;
+  const uint64_t qhat = __umul64hi(x, Res<RES>::mu);
+  uint32_t r = static_cast<uint32_t>(x - qhat * Q);  // < 3q < 2^32
+  r = min(r, r - 2 * Q);
+  return min(r, r - Q);
+}
+template <int RES>
+__device__ __forceinline__ uint32_t canon8(uint32_t x) {  // [0, 8q) -> [0, q)
+  constexpr uint32_t Q = Res<RES>::q;
+  x = min(x, x - 4 * Q);
+  x = min(x, x - 2 * Q);
+  return min(x, x - Q);
+}
+template <int RES>
+__device__ __forceinline__ uint32_t to4q(uint32_t x) {  // [0, 8q) -> [0, 4q)
+  return min(x, x - 4 * Res<RES>::q);
+}
+
+// --------------------------------------------------------------- forward
+template <uint32_t Q, bool C>
+__device__ __forceinline__ void fbf(uint32_t &X, uint32_t &Y, uint2 w) {
+  uint32_t x = X;
+  if (C) x = min(x, x - 4 * Q);
+  const uint32_t t = Y * w.x - __umulhi(Y, w.y) * Q;
+  X = x + t;
+  Y = x - t + 2 * Q;
+}
+template <uint32_t Q, bool C1, bool C2, bool C3>
+__device__ __forceinline__ void fpass8(uint32_t (&v)[8], const uint2 (&w)[7]) {
+  fbf<Q, C1>(v[0], v[4], w[0]); fbf<Q, C1>(v[1], v[5], w[0]);
+  fbf<Q, C1>(v[2], v[6], w[0]); fbf<Q, C1>(v[3], v[7], w[0]);
+  fbf<Q, C2>(v[0], v[2], w[1]); fbf<Q, C2>(v[1], v[3], w[1]);
+  fbf<Q, C2>(v[4], v[6], w[2]); fbf<Q, C2>(v[5], v[7], w[2]);
+  fbf<Q, C3>(v[0], v[1], w[3]); fbf<Q, C3>(v[2], v[3], w[4]);
+  fbf<Q, C3>(v[4], v[5], w[5]); fbf<Q, C3>(v[6], v[7], w[6]);
+}
+// pass A (stages 1-3), canonical input; twiddles 1..7 from constant memory
+template <int RES>
+__device__ __forceinline__ void fA(uint32_t (&v)[8]) {
+  const uint2 w[7] = {c_fwt[RES][1], c_fwt[RES][2], c_fwt[RES][3], c_fwt[RES][4],
+                      c_fwt[RES][5], c_fwt[RES][6], c_fwt[RES][7]};
+  fpass8<Res<RES>::q, false, false, false>(v, w);
+}
+// per-thread twiddles of passes B (warp-uniform, constant memory), C and D
+template <int RES>
+__device__ __forceinline__ void fload_b(uint2 (&w)[7], int t) {
+  const int g = t >> 5;
+  w[0] = c_fwt[RES][8 + g];
+  w[1] = c_fwt[RES][16 + 2 * g];
+  w[2] = c_fwt[RES][17 + 2 * g];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w[3 + i] = c_fwt[RES][32 + 4 * g + i];
+}
+__device__ __forceinline__ void fload_c(uint2 (&w)[7], const uint2 *fwt, int t) {
+  const int g = t & 63;
+  w[0] = __ldg(fwt + 64 + g);
+  w[1] = __ldg(fwt + 128 + 2 * g);
+  w[2] = __ldg(fwt + 129 + 2 * g);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w[3 + i] = __ldg(fwt + 256 + 4 * g + i);
+}
+__device__ __forceinline__ void fload_d(uint2 (&w)[6], const uint2 *fwt, int t) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int b4 = t + 256 * h;
+    w[3 * h] = __ldg(fwt + 512 + b4);
+    w[3 * h + 1] = __ldg(fwt + 1024 + 2 * b4);
+    w[3 * h + 2] = __ldg(fwt + 1025 + 2 * b4);
+  }
+}
+// pass D (stages 10-11): output in [0, 8q)
+template <int RES>
+__device__ __forceinline__ void fD(uint32_t (&v)[8], const uint2 (&w)[6]) {
+  constexpr uint32_t Q = Res<RES>::q;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint32_t *u = v + 4 * h;
+    fbf<Q, true>(u[0], u[2], w[3 * h]);
+    fbf<Q, true>(u[1], u[3], w[3 * h]);
+    fbf<Q, false>(u[0], u[1], w[3 * h + 1]);
+    fbf<Q, false>(u[2], u[3], w[3 * h + 2]);
+  }
+}
+// Passes B and C over `np` padded planes stored in A-order after fA, up to a
+// __syncthreads; ends synchronised. The caller then loads D-order and runs fD.
+template <int RES>
+__device__ __forceinline__ void fwd_mid_r(uint32_t *sm, int np, const uint2 *fwt) {
+  constexpr uint32_t Q = Res<RES>::q;
+  const int t = threadIdx.x;
+  {
+    uint2 w[7];
+    fload_b<RES>(w, t);
+    for (int i = 0; i < np; ++i) {
+      uint32_t v[8];
+      ld_plane<1>(sm + i * kPad, v, t);
+      fpass8<Q, true, false, true>(v, w);
+      st_plane<1>(sm + i * kPad, v, t);
+    }
+  }
+  __syncthreads();
+  {
+    uint2 w[7];
+    fload_c(w, fwt, t);
+    for (int i = 0; i < np; ++i) {
+      uint32_t v[8];
+      ld_plane<2>(sm + i * kPad, v, t);
+      fpass8<Q, false, true, false>(v, w);
+      st_plane<2>(sm + i * kPad, v, t);
+    }
+  }
+  __syncthreads();
+}
+
+// --------------------------------------------------------------- inverse
+// Gentleman-Sande, inputs and outputs in [0, 2q) between passes.
+template <uint32_t Q>
+__device__ __forceinline__ void ibf(uint32_t &X, uint32_t &Y, uint2 w) {
+  uint32_t u = X + Y;
+  u = min(u, u - 2 * Q);
+  const uint32_t d = X - Y + 2 * Q;
+  Y = d * w.x - __umulhi(d, w.y) * Q;
+  X = u;
+}
+template <uint32_t Q>
+__device__ __forceinline__ void ipass8(uint32_t (&v)[8], const uint2 (&w)[7]) {
+  ibf<Q>(v[0], v[1], w[3]); ibf<Q>(v[2], v[3], w[4]);
+  ibf<Q>(v[4], v[5], w[5]); ibf<Q>(v[6], v[7], w[6]);
+  ibf<Q>(v[0], v[2], w[1]); ibf<Q>(v[1], v[3], w[1]);
+  ibf<Q>(v[4], v[6], w[2]); ibf<Q>(v[5], v[7], w[2]);
+  ibf<Q>(v[0], v[4], w[0]); ibf<Q>(v[1], v[5], w[0]);
+  ibf<Q>(v[2], v[6], w[0]); ibf<Q>(v[3], v[7], w[0]);
+}
+// twiddles of the inverse passes in the same [base + g, 2 base + 2 g (+1),
+// 4 base + 4 g (+0..3)] arrangement as the forward ones
+template <int RES>
+__device__ __forceinline__ void iload_b(uint2 (&w)[7], int t) {
+  const int g = t >> 5;
+  w[0] = c_iwt[RES][8 + g];
+  w[1] = c_iwt[RES][16 + 2 * g];
+  w[2] = c_iwt[RES][17 + 2 * g];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w[3 + i] = c_iwt[RES][32 + 4 * g + i];
+}
+__device__ __forceinline__ void iload_c(uint2 (&w)[7], const uint2 *iwt, int t) {
+  const int g = t & 63;
+  w[0] = __ldg(iwt + 64 + g);
+  w[1] = __ldg(iwt + 128 + 2 * g);
+  w[2] = __ldg(iwt + 129 + 2 * g);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w[3 + i] = __ldg(iwt + 256 + 4 * g + i);
+}
+__device__ __forceinline__ void iload_d(uint2 (&w)[6], const uint2 *iwt, int t) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int b4 = t + 256 * h;
+    w[3 * h] = __ldg(iwt + 512 + b4);
+    w[3 * h + 1] = __ldg(iwt + 1024 + 2 * b4);
+    w[3 * h + 2] = __ldg(iwt + 1025 + 2 * b4);
+  }
+}
+// first inverse pass (stages t = 1, 2) on D-order values in [0, 2q)
+template <int RES>
+__device__ __forceinline__ void iD(uint32_t (&v)[8], const uint2 (&w)[6]) {
+  constexpr uint32_t Q = Res<RES>::q;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint32_t *u = v + 4 * h;
+    ibf<Q>(u[0], u[1], w[3 * h + 1]);
+    ibf<Q>(u[2], u[3], w[3 * h + 2]);
+    ibf<Q>(u[0], u[2], w[3 * h]);
+    ibf<Q>(u[1], u[3], w[3 * h]);
+  }
+}
+// last inverse pass (t = 256, 512, then 1024 with N^-1 folded in); canonical
+template <int RES>
+__device__ __forceinline__ void iA(uint32_t (&v)[8]) {
+  constexpr uint32_t Q = Res<RES>::q;
+  ibf<Q>(v[0], v[1], c_iwt[RES][4]); ibf<Q>(v[2], v[3], c_iwt[RES][5]);
+  ibf<Q>(v[4], v[5], c_iwt[RES][6]); ibf<Q>(v[6], v[7], c_iwt[RES][7]);
+  ibf<Q>(v[0], v[2], c_iwt[RES][2]); ibf<Q>(v[1], v[3], c_iwt[RES][2]);
+  ibf<Q>(v[4], v[6], c_iwt[RES][3]); ibf<Q>(v[5], v[7], c_iwt[RES][3]);
+  const uint4 s = c_nscale[RES];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t X = v[k], Y = v[k + 4];
+    const uint32_t a = X + Y, d = X - Y + 2 * Q;
+    const uint32_t ra = a * s.x - __umulhi(a, s.y) * Q;
+    const uint32_t rb = d * s.z - __umulhi(d, s.w) * Q;
+    v[k] = min(ra, ra - Q);
+    v[k + 4] = min(rb, rb - Q);
+  }
+}
+// Passes C and B over `np` planes holding D-order values after iD, up to a
+// __syncthreads; ends synchronised. The caller then loads A-order and runs iA.
+template <int RES>
+__device__ __forceinline__ void inv_mid_r(uint32_t *sm, int np, const uint2 *iwt) {
+  constexpr uint32_t Q = Res<RES>::q;
+  const int t = threadIdx.x;
+  {
+    uint2 w[7];
+    iload_c(w, iwt, t);
+    for (int i = 0; i < np; ++i) {
+      uint32_t v[8];
+      ld_plane<2>(sm + i * kPad, v, t);
+      ipass8<Q>(v, w);
+      st_plane<2>(sm + i * kPad, v, t);
+    }
+  }
+  __syncthreads();
+  {
+    uint2 w[7];
+    iload_b<RES>(w, t);
+    for (int i = 0; i < np; ++i) {
+      uint32_t v[8];
+      ld_plane<1>(sm + i * kPad, v, t);
+      ipass8<Q>(v, w);
+      st_plane<1>(sm + i * kPad, v, t);
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace opir

@@ -264,6 +264,21 @@ void setup_device_params(opir_server *s) {
     d.r[r].w1_ninv_sh = static_cast<uint32_t>((static_cast<uint64_t>(w1n) << 32) / ts[r]->q);
     d.r[r].mu = ts[r]->mu;
   }
+  {
+    const uint32_t qs[2] = {ts[0]->q, ts[1]->q};
+    const uint32_t *fw[2] = {ts[0]->fw.data(), ts[1]->fw.data()};
+    const uint32_t *fw_sh[2] = {ts[0]->fw_sh.data(), ts[1]->fw_sh.data()};
+    const uint32_t *iw[2] = {ts[0]->iw.data(), ts[1]->iw.data()};
+    const uint32_t *iw_sh[2] = {ts[0]->iw_sh.data(), ts[1]->iw_sh.data()};
+    uint32_t nscale[2][4];
+    for (int r = 0; r < 2; ++r) {
+      nscale[r][0] = d.r[r].n_inv;
+      nscale[r][1] = d.r[r].n_inv_sh;
+      nscale[r][2] = d.r[r].w1_ninv;
+      nscale[r][3] = d.r[r].w1_ninv_sh;
+    }
+    opir::upload_ntt_constants(qs, fw, fw_sh, iw, iw_sh, nscale);
+  }
   d.q = p.q;
   d.half_q = p.q >> 1;
   d.q1 = static_cast<uint32_t>(p.q1);
