@@ -188,7 +188,7 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
 
   // sigma_k(c0) (own residue) and the centred sigma_k(c1) at A-order positions
   uint32_t s0[8];
-  int64_t d[8];
+  uint64_t d[8];  // centred sigma_k(c1) + digit offset
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const uint32_t j = posA(tid, k);
@@ -197,29 +197,31 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
     const uint32_t src = u & (kN - 1);
     const uint32_t z = c0[src], a0 = ct[2 * kN + src], a1 = ct[3 * kN + src];
     s0[k] = neg ? neg_mod(z, q) : z;
-    d[k] = centre(crt_compose(neg ? neg_mod(a0, P.q1) : a0, neg ? neg_mod(a1, P.q2) : a1, P), P);
+    d[k] = digit_source<kLKs, kBaseKs>(compose_c(neg ? neg_mod(a0, kQ1) : a0,
+                                                 neg ? neg_mod(a1, kQ2) : a1));
   }
   // digit planes: decompose, pass A in registers
-  for (int i = 0; i < l_ks; ++i) {
+#pragma unroll
+  for (int i = 0; i < kLKs; ++i) {
     uint32_t v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = digit_residue(next_digit(d[k], base_ks), q);
+    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, kBaseKs>(d[k], i);
     fA<RES>(v);
     st_plane<0>(sm + i * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid_r<RES>(sm, l_ks, T.fwt);
+  fwd_mid_r<RES>(sm, kLKs, T.fwt);
   // inner product with the key rows (row t encrypts sigma(s) B^t), D-order;
   // digit NTT values stay in [0, 4q) when l_ks <= 8 (sum < 2^64), else canonical
   const uint32_t *key = bv_keys[b] + bv_level_off + RES * kN;
-  const bool lazy = l_ks <= 8;
+  constexpr bool lazy = kLKs <= 8;
   uint64_t ab[8], aa[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
   {
     uint2 wd[6];
     fload_d(wd, T.fwt, tid);
-    for (int i = 0; i < l_ks; ++i) {
+    for (int i = 0; i < kLKs; ++i) {
       uint32_t v[8];
       ld_plane<3>(sm + i * kPad, v, tid);
       fD<RES>(v, wd);
@@ -295,32 +297,34 @@ k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, i
 // poly p meets row p*l + (l - 1 - i) (gsw.cpp:283-293). Uses l padded planes.
 // Digit NTT values enter the MAC in [0, 4q) when 2 l <= 16 (a sum of 2 l
 // products below 4q x q < 2^60 stays below 2^64), else canonical.
-template <int RES>
+template <int RES, int L, int B>
 __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x,
-                                           const uint32_t *y, const uint32_t *rgsw, int l,
-                                           int base_log2, uint32_t *sm, uint64_t (&acc0)[8],
+                                           const uint32_t *y, const uint32_t *rgsw,
+                                           uint32_t *sm, uint64_t (&acc0)[8],
                                            uint64_t (&acc1)[8]) {
   constexpr uint32_t q = Res<RES>::q;
+  constexpr int l = L;
+  constexpr bool lazy = L <= 8;
   const ResidueTables &T = P.r[RES];
   const int tid = threadIdx.x;
-  const bool lazy = l <= 8;
 #pragma unroll 1
   for (int p = 0; p < 2; ++p) {
-    int64_t d[8];
+    uint64_t d[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int j = posA(tid, k);
       uint32_t v1 = x[(p * 2 + 0) * kN + j], v2 = x[(p * 2 + 1) * kN + j];
       if (y != nullptr) {
-        v1 = sub_mod(y[(p * 2 + 0) * kN + j], v1, P.q1);
-        v2 = sub_mod(y[(p * 2 + 1) * kN + j], v2, P.q2);
+        v1 = sub_mod(y[(p * 2 + 0) * kN + j], v1, kQ1);
+        v2 = sub_mod(y[(p * 2 + 1) * kN + j], v2, kQ2);
       }
-      d[k] = centre(crt_compose(v1, v2, P), P);
+      d[k] = digit_source<L, B>(compose_c(v1, v2));
     }
+#pragma unroll
     for (int i = 0; i < l; ++i) {
       uint32_t v[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = digit_residue(next_digit(d[k], base_log2), q);
+      for (int k = 0; k < 8; ++k) v[k] = digit_res<q, B>(d[k], i);
       fA<RES>(v);
       st_plane<0>(sm + i * kPad, v, tid);
     }
@@ -366,7 +370,7 @@ __device__ __forceinline__ void selectors_body(const DevParams &P, const Shape &
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
   // bottom row: ExtProd(RGSW(s), row) with the key gadget (gsw.cpp:119-182)
-  gadget_mac<RES>(P, ct, nullptr, gsw_keys[b], S.l_key, S.base_key, sm, acc0, acc1);
+  gadget_mac<RES, kLKey, kBaseKey>(P, ct, nullptr, gsw_keys[b], sm, acc0, acc1);
   uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords + RES * kN;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -698,7 +702,7 @@ __device__ __forceinline__ void mux_level_body(const DevParams &P, const Shape &
   uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
-  gadget_mac<RES>(P, x, y, rgsw, S.l_ep, S.base_ep, sm, acc0, acc1);
+  gadget_mac<RES, kLEp, kBaseEp>(P, x, y, rgsw, sm, acc0, acc1);
   {
     uint2 wd[6];
     iload_d(wd, T.iwt, tid);
@@ -843,10 +847,18 @@ void launch_db_preprocess(const DevParams &P, const Shape &s, const uint16_t *co
   check_launch("k_db_preprocess");
 }
 
+// The kernels are compiled for the CONFIG_N2048_K1_COMP gadget shapes.
+static void check_gadgets(const Shape &s) {
+  if (s.l_ep != kLEp || s.base_ep != kBaseEp || s.l_key != kLKey || s.base_key != kBaseKey ||
+      s.l_ks != kLKs || s.base_ks != kBaseKs)
+    throw std::invalid_argument("the kernels are compiled for the CONFIG_N2048_K1_COMP gadgets");
+}
+
 void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const uint32_t *in,
                          uint64_t in_stride, uint32_t *out, uint64_t out_stride,
                          const uint32_t *const *bv_keys, uint64_t bv_level_stride,
                          uint32_t batch, cudaStream_t st) {
+  check_gadgets(s);
   const uint32_t nodes = expand_nodes(s, d);
   const size_t smem = s.l_ks * kPad * sizeof(uint32_t);
   set_smem(k_expand_level, smem);
@@ -864,6 +876,7 @@ void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const u
 void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves,
                       uint64_t leaf_stride, const uint32_t *const *gsw_keys, uint32_t *sel,
                       uint32_t batch, cudaStream_t st) {
+  check_gadgets(s);
   if (s.num_dims <= 1) return;
   const size_t smem = s.l_key * kPad * sizeof(uint32_t);
   set_smem(k_selectors, smem);
@@ -927,6 +940,7 @@ void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cm
 void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, const uint32_t *in,
                       uint32_t *out, uint64_t mid_stride, const uint32_t *sel, uint32_t batch,
                       cudaStream_t st) {
+  check_gadgets(s);
   const uint32_t h = s.num_dims - 1;
   uint32_t n_pairs, offset = 0, half = 0, copies = 0;
   if (level == 0) {

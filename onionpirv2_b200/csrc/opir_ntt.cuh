@@ -57,6 +57,56 @@ __device__ __forceinline__ uint32_t to4q(uint32_t x) {  // [0, 8q) -> [0, 4q)
   return min(x, x - 4 * Res<RES>::q);
 }
 
+// ------------------------------------------------------ gadget digits
+// Gadget shapes of CONFIG_N2048_K1_COMP (digits x log2 base): data RGSW
+// (L_EP), key RGSW (L_KEY), BV key switching (L_KS).
+constexpr int kLEp = 6, kBaseEp = 10, kLKey = 10, kBaseKey = 6, kLKs = 8, kBaseKs = 8;
+
+constexpr uint32_t inv_mod_c(uint64_t a, uint64_t m) {  // a^-1 mod m (gcd 1)
+  int64_t t = 0, nt = 1, r = static_cast<int64_t>(m), nr = static_cast<int64_t>(a % m);
+  while (nr != 0) {
+    const int64_t qq = r / nr, tt = t - qq * nt, rr = r - qq * nr;
+    t = nt; nt = tt; r = nr; nr = rr;
+  }
+  return static_cast<uint32_t>(t < 0 ? t + static_cast<int64_t>(m) : t);
+}
+constexpr uint32_t kQ1InvQ2 = inv_mod_c(kQ1, kQ2);
+constexpr uint32_t kQ1InvQ2Sh = static_cast<uint32_t>((static_cast<uint64_t>(kQ1InvQ2) << 32) / kQ2);
+constexpr uint64_t kQ = static_cast<uint64_t>(kQ1) * kQ2;
+
+// Garner compose of a canonical residue pair into [0, q1 q2).
+__device__ __forceinline__ uint64_t compose_c(uint32_t r1, uint32_t r2) {
+  const uint32_t r1m = min(r1, r1 - kQ2);                 // q1 < 2 q2
+  const uint32_t diff = r2 - r1m + kQ2;                     // [1, 2 q2)
+  uint32_t k = diff * kQ1InvQ2 - __umulhi(diff, kQ1InvQ2Sh) * kQ2;
+  k = min(k, k - kQ2);
+  return static_cast<uint64_t>(r1) + static_cast<uint64_t>(kQ1) * k;
+}
+// Balanced base-2^B digits, LSB first (gsw.cpp:277-293, bv_keyswitch.cpp:
+// 20-40): v in [0, q) is centred to c in (-q/2, q/2], and c + C with
+// C = 2^(B-1) sum_{i<L} 2^(B i) has plain base-2^B digits u_i = r_i + 2^(B-1)
+// where r_i in [-2^(B-1), 2^(B-1)) are the balanced digits (|c| < 2^(B L)/2,
+// so the balanced expansion ends within L digits).
+template <int L, int B>
+__device__ __forceinline__ uint64_t digit_source(uint64_t v) {
+  uint64_t C = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) C += (1ull << (B - 1)) << (B * i);
+  return v + C - (v > kQ / 2 ? kQ : 0);
+}
+// r_i as a residue mod Q (r_i + Q for negative r_i).
+template <uint32_t Q, int B>
+__device__ __forceinline__ uint32_t digit_res(uint64_t u, int i) {
+  const int o = B * i;  // a constant once the caller's digit loop is unrolled
+  const uint32_t lo = static_cast<uint32_t>(u), hi = static_cast<uint32_t>(u >> 32);
+  uint32_t f;
+  if (o + B <= 32) f = lo >> o;
+  else if (o >= 32) f = hi >> (o - 32);
+  else f = __funnelshift_r(lo, hi, o);
+  const uint32_t t = (f & ((1u << B) - 1)) + (Q - (1u << (B - 1)));
+  return min(t, t - Q);
+}
+
 // --------------------------------------------------------------- forward
 template <uint32_t Q, bool C>
 __device__ __forceinline__ void fbf(uint32_t &X, uint32_t &Y, uint2 w) {
