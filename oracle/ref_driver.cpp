@@ -111,10 +111,12 @@ std::vector<size_t> query_indices(const PirParams &p, size_t pt_idx) {
   return out;
 }
 
-// client.cpp:107-225 (K == 1 branch: every config here is single-limb)
+// client.cpp:107-225 (both branches: K = 1, the logical composite modulus;
+// K = 2, two RNS limbs with the message lifted under Q = q0 q1).
 RlweCt make_query(const PirParams &p, Client &c, size_t pt_idx) {
   constexpr size_t N = DBConsts::PolyDegree;
   const std::vector<uint64_t> qs(p.get_rns_mods().begin(), p.get_rns_mods().end());
+  const size_t K = qs.size();
   const uint64_t t = p.get_plain_mod();
   const std::vector<size_t> qi = query_indices(p, pt_idx);
   const size_t h = p.get_expan_height();
@@ -124,20 +126,34 @@ RlweCt make_query(const PirParams &p, Client &c, size_t pt_idx) {
   const size_t rev = utils::bit_reverse(qi[0], h);
   RlweCt query;
   encrypt_zero_rns(c.sk, N, qs, p.get_noise_std_dev(), c.rng, query, false);
-  const uint64_t Q = qs[0];
-  const uint64_t scaled = utils::round_div_u128((uint128_t)Q * inverse, t) % Q;
-  query.c0[rev] = (query.c0[rev] + scaled) % Q;
+  if (K == 1) {
+    const uint64_t Q = qs[0];
+    const uint64_t scaled = utils::round_div_u128((uint128_t)Q * inverse, t) % Q;
+    query.c0[rev] = (query.c0[rev] + scaled) % Q;
+  } else {
+    const uint128_t Q = (uint128_t)qs[0] * qs[1];
+    const uint128_t Delta = Q / t;
+    const uint64_t r = (uint64_t)(Q - Delta * t);
+    const uint64_t r_inv_round = (uint64_t)(((uint128_t)r * inverse + (t >> 1)) / t);
+    const uint128_t scaled_mp = Delta * inverse + r_inv_round;
+    for (size_t k = 0; k < K; ++k) {
+      const uint64_t sk = (uint64_t)(scaled_mp % qs[k]);
+      query.c0[k * N + rev] = (uint64_t)(((uint128_t)query.c0[k * N + rev] + sk) % qs[k]);
+    }
+  }
   if (qi.size() > 1) {
-    uint64_t inv_cap = 0;
-    utils::try_invert_uint_mod(capacity, Q, inv_cap);
+    std::vector<uint64_t> inv_cap(K);
+    for (size_t k = 0; k < K; ++k) utils::try_invert_uint_mod(capacity, qs[k], inv_cap[k]);
     const auto gadget = utils::gsw_gadget(p.get_l(), p.get_base_log2(), qs);
     for (size_t i = 1; i < qi.size(); i++) {
       if (qi[i] != 1) continue;
       for (size_t k = 0; k < p.get_l(); k++) {
         const size_t pos = p.get_fst_dim_sz() + (i - 1) * p.get_l() + k;
         const size_t ridx = utils::bit_reverse(pos, h);
-        const uint64_t coef = (uint64_t)((uint128_t)gadget[0][k] * inv_cap % Q);
-        query.c0[ridx] = (uint64_t)(((uint128_t)query.c0[ridx] + coef) % Q);
+        for (size_t m = 0; m < K; ++m) {
+          const uint64_t coef = (uint64_t)((uint128_t)gadget[m][k] * inv_cap[m] % qs[m]);
+          query.c0[m * N + ridx] = (uint64_t)(((uint128_t)query.c0[m * N + ridx] + coef) % qs[m]);
+        }
       }
     }
   }
@@ -180,6 +196,7 @@ struct Args {
   size_t queries = 1, warmup = 0, procs = 1;
   std::string out;
   bool dump_inputs = false;
+  std::string stages;  // directory for the public stage outputs (golden mode)
 };
 
 Args parse(int argc, char **argv) {
@@ -202,6 +219,7 @@ Args parse(int argc, char **argv) {
     else if (k == "--procs") a.procs = std::stoull(val());
     else if (k == "--out") a.out = val();
     else if (k == "--dump-inputs") a.dump_inputs = true;
+    else if (k == "--stages") a.stages = val();
     else throw std::invalid_argument("unknown option " + k);
   }
   return a;
@@ -234,6 +252,30 @@ int main(int argc, char **argv) {
       server.set_client_gsw_key(1, c.gsw);
       RlweCt query = make_query(params, c, a.index);
       RlweCt query_copy = query;
+      if (!a.stages.empty()) {
+        // PirServer's public stage methods (server.h:43-99) on a copy of the
+        // query, each written as flat u64 in the reference's own layouts
+        RlweCt q2 = query;
+        std::vector<RlweCt> exp = server.expand_query(1, q2);
+        std::vector<uint64_t> v;
+        for (const auto &ct : exp) { v.insert(v.end(), ct.c0.begin(), ct.c0.end());
+                                     v.insert(v.end(), ct.c1.begin(), ct.c1.end()); }
+        write_u64(a.stages + "/expand.u64", v);
+        std::vector<GSWCt> sel = server.complete_selectors(1, exp);
+        v.clear();
+        for (const auto &g : sel) for (const auto &row : g) v.insert(v.end(), row.begin(), row.end());
+        write_u64(a.stages + "/selectors.u64", v);
+        exp.resize(params.get_fst_dim_sz());
+        std::vector<RlweCt> mid = server.evaluate_first_dim(exp);
+        v.clear();
+        for (const auto &ct : mid) { v.insert(v.end(), ct.c0.begin(), ct.c0.end());
+                                     v.insert(v.end(), ct.c1.begin(), ct.c1.end()); }
+        write_u64(a.stages + "/first_dim.u64", v);
+        RlweCt fin = server.evaluate_other_dim(mid, sel);
+        v.assign(fin.c0.begin(), fin.c0.end());
+        v.insert(v.end(), fin.c1.begin(), fin.c1.end());
+        write_u64(a.stages + "/other_dim.u64", v);
+      }
       RlweCt resp = server.make_query(1, query);
       std::stringstream ss;
       const size_t nbytes = server.save_resp_to_stream(resp, ss);
@@ -263,16 +305,19 @@ int main(int argc, char **argv) {
         }
       }
       const auto &crt = params.get_composite_rns();
+      const auto &qs = params.get_rns_mods();
       std::printf(
           "{\"ok\": %s, \"num_pt\": %zu, \"fst_dim_sz\": %zu, \"num_dims\": %zu, "
-          "\"other_dim_sz\": %zu, \"q\": %llu, \"q1\": %llu, \"q2\": %llu, \"w1\": %llu, "
-          "\"w2\": %llu, \"t\": %llu, \"small_q\": %llu, \"resp_bytes\": %zu, \"load_s\": %.3f}\n",
+          "\"other_dim_sz\": %zu, \"K\": %zu, \"q\": %llu, \"q_limb1\": %llu, \"q1\": %llu, "
+          "\"q2\": %llu, \"w1\": %llu, \"w2\": %llu, \"t\": %llu, \"small_q\": %llu, "
+          "\"base_log2\": %zu, \"base_log2_key\": %zu, \"resp_bytes\": %zu, \"load_s\": %.3f}\n",
           ok ? "true" : "false", params.get_num_pt(), params.get_fst_dim_sz(),
-          params.get_num_dims(), params.get_other_dim_sz(),
-          (unsigned long long)params.get_rns_mods()[0], (unsigned long long)crt.q1,
-          (unsigned long long)crt.q2, (unsigned long long)crt.w1,
+          params.get_num_dims(), params.get_other_dim_sz(), qs.size(),
+          (unsigned long long)qs[0], (unsigned long long)(qs.size() > 1 ? qs[1] : 0),
+          (unsigned long long)crt.q1, (unsigned long long)crt.q2, (unsigned long long)crt.w1,
           (unsigned long long)crt.w2, (unsigned long long)t,
-          (unsigned long long)params.get_small_q(), nbytes, load_s);
+          (unsigned long long)params.get_small_q(), (size_t)params.get_base_log2(),
+          (size_t)params.get_base_log2_key(), nbytes, load_s);
       return ok ? 0 : 3;
     }
 

@@ -8,8 +8,15 @@ digests of the response u64 array and of the client material (query, BV keys,
 RGSW key) so a seeded client can be checked against the reference client
 without committing megabytes of keys.
 
+A second set (golden_c4.json, c4_*.resp.bin) comes from oracle/_ref/opir_ref_c4,
+the same reference built with CONFIG_N4096_K2_MP (N = 4096, two 60-bit RNS
+limbs); those cases also store SHA-256 digests of the outputs of the
+reference's public stage methods (expand_query, complete_selectors,
+evaluate_first_dim, evaluate_other_dim) in the reference's own flat layouts.
+
 Only needed when the fixtures must change; tests never run it.
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # CONFIG_N2048_K1_COMP set
+    python tests/golden/make_golden.py --c4       # CONFIG_N4096_K2_MP set
 """
 from __future__ import annotations
 
@@ -23,6 +30,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "opir_ref")
+REF_BIN_C4 = os.path.join(REPO, "oracle", "_ref", "opir_ref_c4")
 
 # name, target_num_pt, expansion_height, fst_dim_pow2, db_seed, client_seed, index
 CASES = [
@@ -39,21 +47,35 @@ CASES = [
 ]
 
 
+# CONFIG_N4096_K2_MP: same columns
+CASES_C4 = [
+    ("c4_2048_h7", 2048, 7, 1, 3, 4, 777),
+    ("c4_2048_h7_last", 2048, 7, 1, 5, 6, 2047),
+    ("c4_ragged_43_h5", 43, 5, 1, 7, 8, 42),
+    ("c4_tight_100_h6", 100, 6, 0, 9, 10, 57),
+    ("c4_singleton_1_h0", 1, 0, 1, 11, 12, 0),
+    ("c4_16384_h9", 16384, 9, 1, 13, 14, 9999),
+]
+
+
 def sha(path: str) -> str:
     with open(path, "rb") as f:
         return hashlib.sha256(f.read()).hexdigest()
 
 
 def main() -> int:
-    if not os.path.exists(REF_BIN):
+    c4 = "--c4" in sys.argv[1:]
+    ref_bin, cases_ = (REF_BIN_C4, CASES_C4) if c4 else (REF_BIN, CASES)
+    if not os.path.exists(ref_bin):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
     manifest = []
-    for name, target, h, pow2, dbs, cs, idx in CASES:
+    for name, target, h, pow2, dbs, cs, idx in cases_:
         with tempfile.TemporaryDirectory() as tmp:
             out = subprocess.run(
-                [REF_BIN, "--mode", "golden", "--target", str(target), "--height", str(h),
+                [ref_bin, "--mode", "golden", "--target", str(target), "--height", str(h),
                  "--pow2", str(pow2), "--db-seed", str(dbs), "--client-seed", str(cs),
-                 "--index", str(idx), "--out", tmp, "--dump-inputs"],
+                 "--index", str(idx), "--out", tmp, "--dump-inputs"]
+                + (["--stages", tmp] if c4 else []),
                 check=True, capture_output=True, text=True)
             info = json.loads(out.stdout.strip().splitlines()[-1])
             if not info["ok"]:
@@ -77,9 +99,20 @@ def main() -> int:
                 "sha256_bv_keys_u64": sha(os.path.join(tmp, "bv_keys.u64")),
                 "sha256_gsw_key_u64": sha(os.path.join(tmp, "gsw_key.u64")),
             })
+            if c4:
+                manifest[-1].update({
+                    "K": info["K"], "q_limbs": [info["q"], info["q_limb1"]],
+                    "base_log2": info["base_log2"], "base_log2_key": info["base_log2_key"],
+                    "sha256_stage_expand": sha(os.path.join(tmp, "expand.u64")),
+                    "sha256_stage_selectors": sha(os.path.join(tmp, "selectors.u64")),
+                    "sha256_stage_first_dim": sha(os.path.join(tmp, "first_dim.u64")),
+                    "sha256_stage_other_dim": sha(os.path.join(tmp, "other_dim.u64")),
+                })
             print(f"{name}: ok ({info['num_pt']} pts, load {info['load_s']}s)", flush=True)
-    with open(os.path.join(HERE, "golden.json"), "w") as f:
-        json.dump({"generator": "oracle/_ref/opir_ref (reference sources + HEXL stand-in)",
+    with open(os.path.join(HERE, "golden_c4.json" if c4 else "golden.json"), "w") as f:
+        json.dump({"generator": ("oracle/_ref/opir_ref_c4 (reference sources, CONFIG_N4096_K2_MP, "
+                                 "+ HEXL stand-in)") if c4 else
+                   "oracle/_ref/opir_ref (reference sources + HEXL stand-in)",
                    "db_coeff": "mix64(db_seed + (pt*N + c + 1) * 0x9E3779B97F4A7C15) % t",
                    "cases": manifest}, f, indent=1)
     return 0
