@@ -107,6 +107,61 @@ void oracle_bv_apply_galois(const opir_oracle_params *p, uint64_t *ct,
 void oracle_level_mat_mat_32(const uint32_t *A, const uint32_t *B, uint64_t *out,
                              uint64_t m, uint64_t n, uint64_t levels, uint64_t q);
 
+/* ---- CONFIG_N4096_K2_MP (opir_oracle_c4.c): N = 4096, two 60-bit RNS
+ *      limbs, limb-major layouts [limb 0 (N)][limb 1 (N)] per polynomial ---- */
+typedef struct {
+  uint32_t N, K;
+  uint64_t q[2], w[2];          /* limbs and their minimal 2N-th roots   */
+  uint64_t q0_inv_mod_q1, r64_mod_q[2];
+  uint64_t t, small_q;
+  uint32_t small_q_width, ct_mod_width;
+  uint32_t l_ep, l_key, l_ks;
+  uint32_t base_ep, base_key, base_ks;
+  uint64_t target_num_pt, num_pt, fst_dim_sz, other_dim_sz;
+  uint32_t num_dims, expansion_height, fst_dim_pow2;
+} opir_oracle_c4_params;
+
+int oracle_c4_params_init(uint64_t target_num_pt, uint32_t expansion_height,
+                          int fst_dim_pow2, opir_oracle_c4_params *out);
+void oracle_c4_db_plaintext(uint64_t seed, uint64_t pt,
+                            const opir_oracle_c4_params *p, uint64_t *out);
+
+typedef struct oracle_c4_client oracle_c4_client;
+oracle_c4_client *oracle_c4_client_new(const opir_oracle_c4_params *p, uint64_t seed);
+void oracle_c4_client_free(oracle_c4_client *c);
+void oracle_c4_client_bv_keys(const oracle_c4_client *c, uint64_t *out);
+void oracle_c4_client_gsw_key(const oracle_c4_client *c, uint64_t *out);
+int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out);
+void oracle_c4_client_decrypt(const oracle_c4_client *c, const uint64_t *resp,
+                              uint64_t *pt_out);
+
+typedef struct oracle_c4_server oracle_c4_server;
+oracle_c4_server *oracle_c4_server_new(const opir_oracle_c4_params *p);
+void oracle_c4_server_free(oracle_c4_server *s);
+int oracle_c4_server_load_seeded(oracle_c4_server *s, uint64_t logical_num_pt,
+                                 uint64_t seed);
+int oracle_c4_server_set_keys(oracle_c4_server *s, const uint64_t *bv_keys,
+                              const uint64_t *gsw_key);
+int oracle_c4_server_expand(const oracle_c4_server *s, const uint64_t *query,
+                            uint64_t *out);
+int oracle_c4_server_complete_selectors(const oracle_c4_server *s,
+                                        const uint64_t *expanded, uint64_t *out);
+int oracle_c4_server_first_dim(const oracle_c4_server *s,
+                               const uint64_t *fst_query, uint64_t *out);
+int oracle_c4_server_other_dim(const oracle_c4_server *s, uint64_t *mid,
+                               const uint64_t *selectors, uint64_t *out);
+int oracle_c4_server_make_query(const oracle_c4_server *s, const uint64_t *query,
+                                uint64_t *resp);
+void oracle_c4_mod_switch(const opir_oracle_c4_params *p, const uint64_t *ct,
+                          uint64_t *out);
+void oracle_c4_external_product(const opir_oracle_c4_params *p,
+                                const uint64_t *rgsw, uint32_t l, uint32_t base,
+                                const uint64_t *ct, uint64_t *out);
+void oracle_c4_bv_apply_galois(const opir_oracle_c4_params *p, uint64_t *ct,
+                               uint32_t galois_k, const uint64_t *key_rows);
+size_t oracle_c4_serialize(const opir_oracle_c4_params *p, const uint64_t *resp,
+                           uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,7 +2,8 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
 this module, and only as the checker. The library restates the reference
-server path in plain C (oracle/opir_oracle.c); see that file for the
+server path in plain C (oracle/opir_oracle.c for CONFIG_N2048_K1_COMP,
+oracle/opir_oracle_c4.c for CONFIG_N4096_K2_MP); see those files for the
 file:line map into the reference.
 """
 from __future__ import annotations
@@ -36,6 +37,27 @@ class Params(C.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+    @property
+    def useful(self) -> int:
+        return self.fst_dim_sz + self.l_ep * (self.num_dims - 1)
+
+
+class C4Params(C.Structure):
+    """CONFIG_N4096_K2_MP parameters (two 60-bit limbs, N = 4096)."""
+    _fields_ = [
+        ("N", C.c_uint32), ("K", C.c_uint32),
+        ("q", C.c_uint64 * 2), ("w", C.c_uint64 * 2),
+        ("q0_inv_mod_q1", C.c_uint64), ("r64_mod_q", C.c_uint64 * 2),
+        ("t", C.c_uint64), ("small_q", C.c_uint64),
+        ("small_q_width", C.c_uint32), ("ct_mod_width", C.c_uint32),
+        ("l_ep", C.c_uint32), ("l_key", C.c_uint32), ("l_ks", C.c_uint32),
+        ("base_ep", C.c_uint32), ("base_key", C.c_uint32), ("base_ks", C.c_uint32),
+        ("target_num_pt", C.c_uint64), ("num_pt", C.c_uint64),
+        ("fst_dim_sz", C.c_uint64), ("other_dim_sz", C.c_uint64),
+        ("num_dims", C.c_uint32), ("expansion_height", C.c_uint32),
+        ("fst_dim_pow2", C.c_uint32),
+    ]
 
     @property
     def useful(self) -> int:
@@ -102,6 +124,28 @@ def lib():
         L.oracle_external_product.argtypes = [C.POINTER(Params), _u64p, C.c_uint32, C.c_uint32,
                                               _u64p, _u64p]
         L.oracle_bv_apply_galois.argtypes = [C.POINTER(Params), _u64p, C.c_uint32, _u64p]
+        P4 = C.POINTER(C4Params)
+        L.oracle_c4_params_init.argtypes = [C.c_uint64, C.c_uint32, C.c_int, P4]
+        L.oracle_c4_db_plaintext.argtypes = [C.c_uint64, C.c_uint64, P4, _u64p]
+        L.oracle_c4_client_new.argtypes = [P4, C.c_uint64]
+        L.oracle_c4_client_new.restype = C.c_void_p
+        L.oracle_c4_client_free.argtypes = [C.c_void_p]
+        L.oracle_c4_client_bv_keys.argtypes = [C.c_void_p, _u64p]
+        L.oracle_c4_client_gsw_key.argtypes = [C.c_void_p, _u64p]
+        L.oracle_c4_client_query.argtypes = [C.c_void_p, C.c_uint64, _u64p]
+        L.oracle_c4_client_decrypt.argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_c4_server_new.argtypes = [P4]
+        L.oracle_c4_server_new.restype = C.c_void_p
+        L.oracle_c4_server_free.argtypes = [C.c_void_p]
+        L.oracle_c4_server_load_seeded.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
+        L.oracle_c4_server_set_keys.argtypes = [C.c_void_p, _u64p, _u64p]
+        for f in ("oracle_c4_server_expand", "oracle_c4_server_complete_selectors",
+                  "oracle_c4_server_first_dim", "oracle_c4_server_make_query"):
+            getattr(L, f).argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_c4_server_other_dim.argtypes = [C.c_void_p, _u64p, _u64p, _u64p]
+        L.oracle_c4_mod_switch.argtypes = [P4, _u64p, _u64p]
+        L.oracle_c4_serialize.argtypes = [P4, _u64p, C.POINTER(C.c_uint8)]
+        L.oracle_c4_serialize.restype = C.c_size_t
         _lib = L
     return _lib
 
@@ -230,4 +274,129 @@ def serialize(p: Params, resp: np.ndarray) -> bytes:
     r = np.ascontiguousarray(resp, dtype=np.uint64)
     buf = np.zeros(2 * p.N * 8, dtype=np.uint8)
     n = lib().oracle_serialize(C.byref(p), ptr(r), ptr(buf, C.c_uint8))
+    return buf[:n].tobytes()
+
+
+# ---------------------------------------------------------------- CONFIG_N4096_K2_MP
+def c4_params(target: int, height: int, pow2: bool = True) -> C4Params:
+    p = C4Params()
+    if lib().oracle_c4_params_init(target, height, 1 if pow2 else 0, C.byref(p)) != 0:
+        raise ValueError(f"invalid layout target={target} height={height}")
+    return p
+
+
+def c4_db_plaintext(seed: int, pt: int, p: C4Params) -> np.ndarray:
+    out = np.empty(p.N, dtype=np.uint64)
+    lib().oracle_c4_db_plaintext(seed, pt, C.byref(p), ptr(out))
+    return out
+
+
+class C4Client:
+    """Seeded two-limb client: the reference client (K = 2) with seeded generators.
+    Ciphertexts are (2, 2, N): poly x limb x coefficient."""
+
+    def __init__(self, p: C4Params, seed: int):
+        self.p = p
+        self.h = lib().oracle_c4_client_new(C.byref(p), seed)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_c4_client_free(self.h)
+            self.h = None
+
+    def bv_keys(self) -> np.ndarray:
+        p = self.p
+        out = np.zeros((max(p.expansion_height, 0), p.l_ks, 2, 2, p.N), dtype=np.uint64)
+        if p.expansion_height:
+            lib().oracle_c4_client_bv_keys(self.h, ptr(out))
+        return out
+
+    def gsw_key(self) -> np.ndarray:
+        p = self.p
+        out = np.zeros((2 * p.l_key, 2, 2, p.N), dtype=np.uint64)
+        lib().oracle_c4_client_gsw_key(self.h, ptr(out))
+        return out
+
+    def query(self, idx: int) -> np.ndarray:
+        out = np.zeros((2, 2, self.p.N), dtype=np.uint64)
+        if lib().oracle_c4_client_query(self.h, idx, ptr(out)) != 0:
+            raise IndexError("plaintext index outside the layout")
+        return out
+
+    def decrypt(self, resp: np.ndarray) -> np.ndarray:
+        resp = np.ascontiguousarray(resp, dtype=np.uint64)
+        out = np.zeros(self.p.N, dtype=np.uint64)
+        lib().oracle_c4_client_decrypt(self.h, ptr(resp), ptr(out))
+        return out
+
+
+class C4Server:
+    def __init__(self, p: C4Params):
+        self.p = p
+        self.h = lib().oracle_c4_server_new(C.byref(p))
+        if not self.h:
+            raise MemoryError("oracle server allocation failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_c4_server_free(self.h)
+            self.h = None
+
+    def load_seeded(self, logical: int, seed: int):
+        assert lib().oracle_c4_server_load_seeded(self.h, logical, seed) == 0
+
+    def set_keys(self, bv: np.ndarray, gsw: np.ndarray):
+        bv = np.ascontiguousarray(bv, dtype=np.uint64)
+        gsw = np.ascontiguousarray(gsw, dtype=np.uint64)
+        if bv.size == 0:
+            bv = np.zeros(1, dtype=np.uint64)
+        lib().oracle_c4_server_set_keys(self.h, ptr(bv), ptr(gsw))
+
+    def expand(self, query: np.ndarray) -> np.ndarray:
+        out = np.zeros((self.p.useful, 2, 2, self.p.N), dtype=np.uint64)
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        assert lib().oracle_c4_server_expand(self.h, ptr(q), ptr(out)) == 0
+        return out
+
+    def complete_selectors(self, expanded: np.ndarray) -> np.ndarray:
+        p = self.p
+        out = np.zeros((max(p.num_dims - 1, 1), 2 * p.l_ep, 2, 2, p.N), dtype=np.uint64)
+        e = np.ascontiguousarray(expanded, dtype=np.uint64)
+        assert lib().oracle_c4_server_complete_selectors(self.h, ptr(e), ptr(out)) == 0
+        return out[: p.num_dims - 1]
+
+    def first_dim(self, fst_query: np.ndarray) -> np.ndarray:
+        p = self.p
+        out = np.zeros((p.other_dim_sz, 2, 2, p.N), dtype=np.uint64)
+        f = np.ascontiguousarray(fst_query[: p.fst_dim_sz], dtype=np.uint64)
+        assert lib().oracle_c4_server_first_dim(self.h, ptr(f), ptr(out)) == 0
+        return out
+
+    def other_dim(self, mid: np.ndarray, selectors: np.ndarray) -> np.ndarray:
+        out = np.zeros((2, 2, self.p.N), dtype=np.uint64)
+        m = np.array(mid, dtype=np.uint64, copy=True, order="C")
+        s = np.ascontiguousarray(selectors, dtype=np.uint64)
+        if s.size == 0:
+            s = np.zeros(1, dtype=np.uint64)
+        assert lib().oracle_c4_server_other_dim(self.h, ptr(m), ptr(s), ptr(out)) == 0
+        return out
+
+    def make_query(self, query: np.ndarray) -> np.ndarray:
+        out = np.zeros((2, self.p.N), dtype=np.uint64)
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        assert lib().oracle_c4_server_make_query(self.h, ptr(q), ptr(out)) == 0
+        return out
+
+
+def c4_mod_switch(p: C4Params, ct: np.ndarray) -> np.ndarray:
+    out = np.zeros((2, p.N), dtype=np.uint64)
+    c = np.ascontiguousarray(ct, dtype=np.uint64)
+    lib().oracle_c4_mod_switch(C.byref(p), ptr(c), ptr(out))
+    return out
+
+
+def c4_serialize(p: C4Params, resp: np.ndarray) -> bytes:
+    r = np.ascontiguousarray(resp, dtype=np.uint64)
+    buf = np.zeros(2 * p.N * 8, dtype=np.uint8)
+    n = lib().oracle_c4_serialize(C.byref(p), ptr(r), ptr(buf, C.c_uint8))
     return buf[:n].tobytes()

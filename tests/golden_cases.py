@@ -18,6 +18,19 @@ def case(name):
     raise KeyError(name)
 
 
+def cases_c4():
+    """CONFIG_N4096_K2_MP cases (reference built with that configuration)."""
+    with open(os.path.join(GOLDEN_DIR, "golden_c4.json")) as f:
+        return json.load(f)["cases"]
+
+
+def case_c4(name):
+    for c in cases_c4():
+        if c["name"] == name:
+            return c
+    raise KeyError(name)
+
+
 def stream(c):
     with open(os.path.join(GOLDEN_DIR, c["name"] + ".resp.bin"), "rb") as f:
         return f.read()
