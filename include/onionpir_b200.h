@@ -4,10 +4,14 @@
  * (src/server.cpp, src/gsw.cpp, src/bv_keyswitch.cpp, src/matrix.cpp of
  * zcy05331/OnionPIRv2) with hand-written sm_100a CUDA kernels. Every entry
  * point below names the reference interface it replaces (paths relative to
- * the reference's src/). The parameter set is CONFIG_N2048_K1_COMP
- * (includes/database_constants.h:77-94): N = 2048, logical q = q1*q2 with two
- * 29-bit NTT primes, t = 4099, small_q = 4169729, L_EP = 6, L_KEY = 10,
- * L_KS = 8.
+ * the reference's src/). Two parameter sets (includes/database_constants.h):
+ *   CONFIG_N2048_K1_COMP (:77-94): N = 2048, logical q = q1*q2 with two
+ *     29-bit NTT primes, t = 4099, small_q = 4169729, L_EP = 6, L_KEY = 10,
+ *     L_KS = 8 (opir_params_init);
+ *   CONFIG_N4096_K2_MP (:111-125): N = 4096, two 60-bit RNS limbs
+ *     q0 = 1152921504606830593, q1 = 1152921504606748673, t =
+ *     generate_prime(40), 50-bit small_q, L_EP = 5, L_KEY = 8, L_KS = 8
+ *     (opir_params_init_config).
  *
  * Conventions
  *   - Plain pointers and sizes only. Host buffers unless a name ends in
@@ -19,6 +23,11 @@
  *     [0, q) (includes/rlwe.h:17-31, K = 1). Key rows are in the NTT domain of
  *     the reference's NTT (HEXL ordering: forward output bit-reversed,
  *     root = CRT of the minimal primitive 2N-th roots mod q1 and q2).
+ *     Under CONFIG_N4096_K2_MP every polynomial is limb-major,
+ *     [limb 0 (N)][limb 1 (N)], so a ciphertext is 4N u64, each limb
+ *     canonical mod its prime and NTT rows per limb (root = the minimal
+ *     primitive 2N-th root of that limb); the sizes quoted below in N double
+ *     accordingly (2N -> 4N per ciphertext, N -> 2N per key polynomial).
  *   - A server handle owns its device memory (database, client keys, scratch
  *     arena) on the device it was created on. Calls on one handle must not
  *     run concurrently; distinct handles are independent.
@@ -43,6 +52,13 @@ typedef enum {
   OPIR_ERR_OVERFLOW = 6          /* std::overflow_error */
 } opir_status;
 
+/* ACTIVE_CONFIG choices (includes/database_constants.h:31-40) that this
+ * library implements. */
+typedef enum {
+  OPIR_CONFIG_N2048_K1_COMP = 0,
+  OPIR_CONFIG_N4096_K2_MP = 1
+} opir_config;
+
 /* PirLayoutConfig (includes/pir.h:199-203). */
 typedef struct {
   uint64_t target_num_pt;
@@ -54,9 +70,11 @@ typedef struct {
  * getters (includes/pir.h:237-277, src/pir.cpp:14-134). */
 typedef struct {
   uint32_t poly_degree;           /* N */
-  uint32_t num_limbs;             /* K (1: logical single modulus)       */
-  uint64_t q;                     /* logical ciphertext modulus q1*q2    */
-  uint64_t q1, q2;                /* composite first-dim limbs           */
+  uint32_t num_limbs;             /* K (1: logical single modulus, 2: RNS) */
+  uint64_t q;                     /* logical ciphertext modulus q1*q2 (K = 1);
+                                     0 when K = 2 (the product needs 120 bits) */
+  uint64_t q1, q2;                /* composite first-dim limbs (K = 1) or the
+                                     two RNS limbs (K = 2)                */
   uint64_t w1, w2, w_crt;         /* 2N-th roots: q1, q2 and CRT (mod q) */
   uint64_t q1_inv_mod_q2;
   uint64_t plain_mod;             /* t                                   */
@@ -82,6 +100,13 @@ typedef int (*opir_plaintext_source)(void *user, uint64_t logical_index,
 
 /* PirParams().with_layout(layout) (src/pir.cpp:49-134). */
 opir_status opir_params_init(const opir_layout *layout, opir_params *out);
+
+/* PirParams under a chosen ACTIVE_CONFIG: CONFIG_N2048_K1_COMP gives the
+ * same as opir_params_init, CONFIG_N4096_K2_MP the two-limb set
+ * (src/pir.cpp:49-134 with RnsMods {60, 60}, PlainMod 40, SmallQWidth 50;
+ * expansion_height <= 12). Unknown config -> OPIR_ERR_INVALID_ARGUMENT. */
+opir_status opir_params_init_config(opir_config config, const opir_layout *layout,
+                                    opir_params *out);
 
 /* Bytes of the serialized response: ceil(2 N small_q_width / 8). */
 size_t opir_response_bytes(const opir_params *params);

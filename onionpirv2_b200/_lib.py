@@ -49,6 +49,7 @@ SOURCE_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, u64p)
 _SIGS = {
     "opir_version": ([], C.c_char_p),
     "opir_params_init": ([C.POINTER(Layout), C.POINTER(Params)], C.c_int),
+    "opir_params_init_config": ([C.c_int, C.POINTER(Layout), C.POINTER(Params)], C.c_int),
     "opir_response_bytes": ([C.POINTER(Params)], C.c_size_t),
     "opir_server_create": ([C.POINTER(Params), C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "opir_server_destroy": ([C.c_void_p], None),

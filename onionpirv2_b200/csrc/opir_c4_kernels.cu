@@ -1,0 +1,803 @@
+// sm_100a kernels of the server path for CONFIG_N4096_K2_MP (N = 4096, two
+// 60-bit RNS limbs, includes/database_constants.h:111-125). Every polynomial
+// kernel runs 512 threads and one CTA per (item, limb, query); limb-major
+// ciphertexts [c0 l0][c0 l1][c1 l0][c1 l1] u64 stay in the reference's own
+// layout (rlwe.h:17-31), so no split or compose is needed at the boundary.
+#include "opir_c4_kernels.h"
+
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+#include "opir_c4_device.cuh"
+
+namespace opir4 {
+
+namespace {
+
+using u128 = unsigned __int128;
+using i128 = __int128;
+
+constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ull;
+constexpr u128 kQQ = static_cast<u128>(kQ0) * kQ1;
+constexpr int kLKs = 8, kBaseKs = 16, kLKey = 8, kBaseKey = 15, kLEp = 5, kBaseEp = 24;
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+std::atomic<uint64_t> g_launches4{0};
+
+void check_launch(const char *what) {
+  g_launches4.fetch_add(1, std::memory_order_relaxed);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> granted;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_pair(dev, reinterpret_cast<const void *>(kernel));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = granted.find(key);
+  if (it != granted.end() && it->second >= bytes) return;
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(bytes));
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  granted[key] = bytes;
+}
+
+constexpr size_t plane_bytes(int np) { return static_cast<size_t>(np) * kPad * sizeof(uint64_t); }
+
+// 8 consecutive u64 (D-order positions 8t .. 8t+7) as four 16-byte loads
+__device__ __forceinline__ void ld8(const uint64_t *p, uint64_t (&v)[8]) {
+  const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const ulonglong2 x = __ldg(q + i);
+    v[2 * i] = x.x;
+    v[2 * i + 1] = x.y;
+  }
+}
+
+// ------------------------------------------------------------ gadget digits
+// Balanced BV digits (bv_keyswitch.cpp:42-62) lie in (-B/2, B/2]: the
+// centred value plus C = (B/2 - 1) sum_i B^i has plain base-B digits
+// u_i = r_i + B/2 - 1 (|c| < Q/2 < 2^119 < B^L / 2).
+template <int L, int B>
+__device__ __forceinline__ u128 bv_digit_source(u128 x) {
+  u128 C = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) C += static_cast<u128>((1ull << (B - 1)) - 1) << (B * i);
+  return x + C - (x > kQQ / 2 ? kQQ : 0);
+}
+template <int B>
+__device__ __forceinline__ uint64_t field(u128 u, int i) {
+  return static_cast<uint64_t>(u >> (B * i)) & ((1ull << B) - 1);
+}
+
+// ------------------------------------------------------------ DB preprocessing
+constexpr int kDbTile = 4;  // plaintexts per CTA (one padded plane each)
+
+template <int L>
+__device__ __forceinline__ void db_body(const Dev4 &P, const uint64_t *coeffs,
+                                        uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
+                                        uint64_t logical, uint32_t n0, uint32_t other,
+                                        uint64_t pt_begin, uint64_t pt_end, uint64_t *db) {
+  extern __shared__ uint64_t sm4[];
+  const int tid = threadIdx.x;
+  const uint64_t pt0 = pt_begin + static_cast<uint64_t>(blockIdx.x) * kDbTile;
+  for (int e = 0; e < kDbTile; ++e) {
+    const uint64_t pt = pt0 + e;
+    uint64_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int c = posA(tid, k);
+      uint64_t x = 0;
+      if (pt < pt_end && pt < logical)
+        x = coeffs ? coeffs[(pt - coeff_pt_begin) * kN + c] : mix64(seed + (pt * kN + c + 1) * kGolden) % t;
+      v[k] = x;  // x < t < q: canonical (server.cpp:172-180 reduces pt mod q_k)
+    }
+    fA<L>(v);
+    st_plane<0>(sm4 + e * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid<L>(sm4, kDbTile, P.T);
+  ulonglong2 wd[7];
+  fload_d<L>(wd, P.T);
+  for (int e = 0; e < kDbTile; ++e) {
+    const uint64_t pt = pt0 + e;
+    uint64_t v[8];
+    ld_plane<3>(sm4 + e * kPad, v, tid);
+    fD<L>(v, wd);
+    if (pt >= pt_end) continue;
+    const uint64_t row = pt / n0, col = pt % n0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
+      db[(z * other + row) * n0 + col] = canon8<Limb<L>::q>(v[k]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k4_db_preprocess(Dev4 P, const uint64_t *__restrict__ coeffs, uint64_t coeff_pt_begin,
+                 uint64_t seed, uint64_t t, uint64_t logical, uint32_t n0, uint32_t other,
+                 uint64_t pt_begin, uint64_t pt_end, uint64_t *__restrict__ db) {
+  if (blockIdx.y == 0)
+    db_body<0>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, other, pt_begin, pt_end, db);
+  else
+    db_body<1>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, other, pt_begin, pt_end, db);
+}
+
+// ------------------------------------------------------------ expansion level
+// One heap node, one limb per CTA: the K = 2 BV key switch of the node
+// (bv_keyswitch.cpp:373-481) and its two children (server.cpp:794-809).
+// Digits come from the CRT composition of sigma_k(c1) over both limbs.
+constexpr int kExpGroup = 4;  // digit planes per group
+
+template <int L>
+__device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, uint32_t kshift,
+                                            const uint64_t *in, uint64_t in_stride, uint64_t *out,
+                                            uint64_t out_stride, const uint64_t *const *bv_keys,
+                                            uint64_t bv_level_off) {
+  extern __shared__ uint64_t sm4[];
+  constexpr uint64_t Q = Limb<L>::q;
+  const int node = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
+  const uint64_t *ct = in + (static_cast<uint64_t>(b) * in_stride + node) * kCtWords;
+  const uint64_t *key = bv_keys[b] + bv_level_off;  // [row][b (2N)][a (2N)]
+  u128 ab[8], aa[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
+  for (int g = 0; g < kLKs / kExpGroup; ++g) {
+    u128 u[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t j = posA(tid, k);
+      const uint32_t w = (j * galois_inv) & (2 * kN - 1);
+      const bool neg = w >= kN;
+      const uint32_t src = w & (kN - 1);
+      uint64_t a0 = ct[2 * kN + src], a1 = ct[3 * kN + src];
+      if (neg) { a0 = neg_mod<kQ0>(a0); a1 = neg_mod<kQ1>(a1); }
+      u[k] = bv_digit_source<kLKs, kBaseKs>(compose(a0, a1, P.q0inv, P.q0inv_sh));
+    }
+#pragma unroll
+    for (int e = 0; e < kExpGroup; ++e) {
+      uint64_t v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int64_t r = static_cast<int64_t>(field<kBaseKs>(u[k], g * kExpGroup + e)) -
+                          ((1ll << (kBaseKs - 1)) - 1);
+        v[k] = r >= 0 ? static_cast<uint64_t>(r) : static_cast<uint64_t>(r + static_cast<int64_t>(Q));
+      }
+      fA<L>(v);
+      st_plane<0>(sm4 + e * kPad, v, tid);
+    }
+    __syncthreads();
+    fwd_mid<L>(sm4, kExpGroup, P.T);
+    ulonglong2 wd[7];
+    fload_d<L>(wd, P.T);
+    for (int e = 0; e < kExpGroup; ++e) {
+      const int i = g * kExpGroup + e;
+      uint64_t v[8], kb[8], ka[8];
+      ld_plane<3>(sm4 + e * kPad, v, tid);
+      fD<L>(v, wd);  // [0, 6q): 8 rows x 6q x q < 2^126
+      ld8(key + static_cast<uint64_t>(i) * 4 * kN + L * kN + 8 * tid, kb);
+      ld8(key + static_cast<uint64_t>(i) * 4 * kN + 2 * kN + L * kN + 8 * tid, ka);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        ab[k] += static_cast<u128>(v[k]) * kb[k];
+        aa[k] += static_cast<u128>(v[k]) * ka[k];
+      }
+    }
+    __syncthreads();
+  }
+  {
+    ulonglong2 wd[7];
+    iload_d<L>(wd, P.T);
+    uint64_t vb[8], va[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { vb[k] = red128<Q>(ab[k]); va[k] = red128<Q>(aa[k]); }
+    iD<L>(vb, wd);
+    iD<L>(va, wd);
+    st_plane<3>(sm4, vb, tid);
+    st_plane<3>(sm4 + kPad, va, tid);
+  }
+  __syncthreads();
+  inv_mid<L>(sm4, 2, P.T);
+  uint64_t db_[8], da[8];
+  ld_plane<0>(sm4, db_, tid);
+  ld_plane<0>(sm4 + kPad, da, tid);
+  iA<L>(db_);
+  iA<L>(da);
+  uint64_t *outL = out + (static_cast<uint64_t>(b) * out_stride + 2ull * node) * kCtWords;
+  uint64_t *outR = outL + kCtWords;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t j = posA(tid, k);
+    const uint32_t w = (j * galois_inv) & (2 * kN - 1);
+    const uint64_t z = ct[L * kN + (w & (kN - 1))];
+    const uint64_t s0 = w >= kN ? neg_mod<Q>(z) : z;        // sigma_k(c0), own limb
+    const uint64_t n0v = add_mod<Q>(s0, db_[k]), n1v = da[k];
+    const uint64_t o0 = ct[L * kN + j], o1 = ct[2 * kN + L * kN + j];
+    outL[L * kN + j] = add_mod<Q>(o0, n0v);
+    outL[2 * kN + L * kN + j] = add_mod<Q>(o1, n1v);
+    const uint64_t d0 = sub_mod<Q>(o0, n0v), d1 = sub_mod<Q>(o1, n1v);
+    int dst = static_cast<int>(j) - static_cast<int>(kshift);
+    const bool wrap = dst < 0;
+    if (wrap) dst += kN;
+    outR[L * kN + dst] = wrap ? neg_mod<Q>(d0) : d0;
+    outR[2 * kN + L * kN + dst] = wrap ? neg_mod<Q>(d1) : d1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k4_expand_level(Dev4 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *__restrict__ in,
+                uint64_t in_stride, uint64_t *__restrict__ out, uint64_t out_stride,
+                const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  if (blockIdx.y == 0)
+    expand_body<0>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off);
+  else
+    expand_body<1>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off);
+}
+
+// ------------------------------------------------------------ gadget product
+// acc += sum over the 2 l digit rows of NTT(digit) x rgsw[row] for one limb
+// (gsw.cpp:119-182, decomp_rlwe_mp gsw.cpp:184-250): each polynomial of the
+// decomposed ciphertext (both limbs read: y - x, or x when y is null) is
+// CRT-composed and split into l unsigned base-2^B digits; digit d of poly p
+// meets row p l + (l - 1 - d). Uses l planes (G = l when l <= 5, else 4).
+template <int L, int NL, int B, bool CANON>
+__device__ __forceinline__ void gadget_mac(const Dev4 &P, const uint64_t *x, const uint64_t *y,
+                                           const uint64_t *rgsw, uint64_t *sm, u128 (&acc0)[8],
+                                           u128 (&acc1)[8]) {
+  constexpr int G = NL <= 5 ? NL : 4;
+  const int tid = threadIdx.x;
+#pragma unroll 1
+  for (int p = 0; p < 2; ++p) {
+#pragma unroll 1
+    for (int g = 0; g < NL / G; ++g) {
+      u128 u[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int j = posA(tid, k);
+        uint64_t v0 = x[p * 2 * kN + j], v1 = x[p * 2 * kN + kN + j];
+        if (y != nullptr) {
+          v0 = sub_mod<kQ0>(y[p * 2 * kN + j], v0);
+          v1 = sub_mod<kQ1>(y[p * 2 * kN + kN + j], v1);
+        }
+        u[k] = compose(v0, v1, P.q0inv, P.q0inv_sh);
+      }
+#pragma unroll
+      for (int e = 0; e < G; ++e) {
+        uint64_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = field<B>(u[k], g * G + e);  // < 2^B < q
+        fA<L>(v);
+        st_plane<0>(sm + e * kPad, v, tid);
+      }
+      __syncthreads();
+      fwd_mid<L>(sm, G, P.T);
+      ulonglong2 wd[7];
+      fload_d<L>(wd, P.T);
+      for (int e = 0; e < G; ++e) {
+        const int d = g * G + e;
+        const int row = p * NL + (NL - 1 - d);
+        uint64_t v[8], r0[8], r1[8];
+        ld_plane<3>(sm + e * kPad, v, tid);
+        fD<L>(v, wd);
+        if (CANON) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) v[k] = canon8<Limb<L>::q>(v[k]);
+        }
+        const uint64_t *R = rgsw + static_cast<uint64_t>(row) * kCtWords + L * kN + 8 * tid;
+        ld8(R, r0);
+        ld8(R + 2 * kN, r1);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          acc0[k] += static_cast<u128>(v[k]) * r0[k];
+          acc1[k] += static_cast<u128>(v[k]) * r1[k];
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ------------------------------------------------------------ selectors
+template <int L>
+__device__ __forceinline__ void selectors_body(const Dev4 &P, const Shape4 &S,
+                                               const uint64_t *leaves, uint64_t leaf_stride,
+                                               const uint64_t *const *gsw_keys, uint64_t *sel) {
+  extern __shared__ uint64_t sm4[];
+  constexpr uint64_t Q = Limb<L>::q;
+  const int row_id = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
+  const int selno = row_id / S.l_ep, r = row_id % S.l_ep;
+  const uint64_t *ct = leaves + (static_cast<uint64_t>(b) * leaf_stride + S.n0 + row_id) * kCtWords;
+  uint64_t *outs = sel + (static_cast<uint64_t>(b) * (S.num_dims - 1) + selno) * 2 * S.l_ep * kCtWords;
+  u128 acc0[8], acc1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
+  // bottom row: ExtProd(RGSW(s), row) with the key gadget (16 rows: canonical
+  // digit NTTs keep the 128-bit sums below 2^126)
+  gadget_mac<L, kLKey, kBaseKey, true>(P, ct, nullptr, gsw_keys[b], sm4, acc0, acc1);
+  uint64_t *bot = outs + static_cast<uint64_t>(S.l_ep + r) * kCtWords + L * kN + 8 * tid;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    bot[k] = red128<Q>(acc0[k]);
+    bot[2 * kN + k] = red128<Q>(acc1[k]);
+  }
+  // top row: the expanded row itself in NTT form (gsw.cpp:330-338)
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    uint64_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = ct[p * 2 * kN + L * kN + posA(tid, k)];
+    fA<L>(v);
+    st_plane<0>(sm4 + p * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid<L>(sm4, 2, P.T);
+  ulonglong2 wd[7];
+  fload_d<L>(wd, P.T);
+  uint64_t *top = outs + static_cast<uint64_t>(r) * kCtWords + L * kN + 8 * tid;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    uint64_t v[8];
+    ld_plane<3>(sm4 + p * kPad, v, tid);
+    fD<L>(v, wd);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) top[p * 2 * kN + k] = canon8<Q>(v[k]);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k4_selectors(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t leaf_stride,
+             const uint64_t *const *__restrict__ gsw_keys, uint64_t *__restrict__ sel) {
+  if (blockIdx.y == 0)
+    selectors_body<0>(P, S, leaves, leaf_stride, gsw_keys, sel);
+  else
+    selectors_body<1>(P, S, leaves, leaf_stride, gsw_keys, sel);
+}
+
+// ------------------------------------------------------------ first-dim query
+// Forward NTT per limb of the first n0 leaves (server.cpp:205-262) into the
+// scan's query matrix qm[z = limb N + level][k][column], column = 2 b + poly.
+constexpr int kFstTile = 2;  // leaves per CTA (4 planes)
+
+template <int L>
+__device__ __forceinline__ void fst_body(const Dev4 &P, const Shape4 &S, const uint64_t *leaves,
+                                         uint64_t leaf_stride, uint64_t *qm, uint32_t ncols) {
+  extern __shared__ uint64_t sm4[];
+  const int b = blockIdx.z, tid = threadIdx.x;
+  const uint32_t k0 = blockIdx.x * kFstTile;
+  for (int e = 0; e < 2 * kFstTile; ++e) {
+    const uint32_t kk = k0 + (e >> 1);
+    const int p = e & 1;
+    uint64_t v[8];
+    const uint64_t *src =
+        leaves + (static_cast<uint64_t>(b) * leaf_stride + kk) * kCtWords + p * 2 * kN + L * kN;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = kk < S.n0 ? src[posA(tid, k)] : 0;
+    fA<L>(v);
+    st_plane<0>(sm4 + e * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid<L>(sm4, 2 * kFstTile, P.T);
+  ulonglong2 wd[7];
+  fload_d<L>(wd, P.T);
+  for (int e = 0; e < 2 * kFstTile; ++e) {
+    const uint32_t kk = k0 + (e >> 1);
+    if (kk >= S.n0) continue;  // uniform over the CTA
+    const int p = e & 1;
+    uint64_t v[8];
+    ld_plane<3>(sm4 + e * kPad, v, tid);
+    fD<L>(v, wd);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
+      qm[(z * S.n0 + kk) * ncols + 2 * b + p] = canon8<Limb<L>::q>(v[k]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k4_fst_ntt(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t leaf_stride,
+           uint64_t *__restrict__ qm, uint32_t ncols) {
+  if (blockIdx.y == 0)
+    fst_body<0>(P, S, leaves, leaf_stride, qm, ncols);
+  else
+    fst_body<1>(P, S, leaves, leaf_stride, qm, ncols);
+}
+
+// ------------------------------------------------------------ first-dim scan
+// Per limb and NTT level z: C[r][c] = sum_k A[r][k] Q[k][c] mod q_limb
+// (matrix.cpp:36-151). A warp owns a database row, its lanes split k and
+// keep 128-bit sums (folded every 64 terms, each term < 2^120), then a
+// modular shuffle tree. COLS query columns per CTA are staged in shared
+// memory; consecutive CTAs share z, so the column groups' re-reads of a
+// level's rows hit L2. Output cmat[column][row][z] (z contiguous for the
+// INTT that follows).
+constexpr int kScanThreads = 256;
+
+template <int L, int COLS>
+__device__ __forceinline__ void scan_body(const uint64_t *db, const uint64_t *qm, uint32_t n0,
+                                          uint32_t other, uint32_t ncols, uint64_t *cmat) {
+  extern __shared__ uint64_t qs[];  // [COLS][n0]
+  constexpr uint64_t Q = Limb<L>::q;
+  const uint32_t z = blockIdx.y;     // L N + level
+  const uint32_t c0 = blockIdx.x * COLS;
+  for (uint32_t idx = threadIdx.x; idx < n0 * COLS; idx += kScanThreads) {
+    const uint32_t c = idx / n0, k = idx % n0;
+    qs[idx] = c0 + c < ncols ? qm[(static_cast<uint64_t>(z) * n0 + k) * ncols + c0 + c] : 0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t *A = db + static_cast<uint64_t>(z) * other * n0;
+  for (uint32_t r = warp; r < other; r += kScanThreads / 32) {
+    const uint64_t *Ar = A + static_cast<uint64_t>(r) * n0;
+    uint64_t part[COLS];
+    u128 acc[COLS];
+#pragma unroll
+    for (int c = 0; c < COLS; ++c) { part[c] = 0; acc[c] = 0; }
+    int terms = 0;
+    for (uint32_t k = lane; k < n0; k += 32) {
+      const uint64_t a = __ldg(Ar + k);
+#pragma unroll
+      for (int c = 0; c < COLS; ++c) acc[c] += static_cast<u128>(a) * qs[c * n0 + k];
+      if (++terms == 64) {
+#pragma unroll
+        for (int c = 0; c < COLS; ++c) { part[c] = add_mod<Q>(part[c], red128<Q>(acc[c])); acc[c] = 0; }
+        terms = 0;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < COLS; ++c) {
+      uint64_t v = add_mod<Q>(part[c], red128<Q>(acc[c]));
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v = add_mod<Q>(v, __shfl_xor_sync(0xffffffffu, v, off));
+      if (lane == c && c0 + c < ncols)
+        cmat[(static_cast<uint64_t>(c0 + c) * other + r) * (2 * kN) + z] = v;
+    }
+  }
+}
+
+template <int COLS>
+__global__ void __launch_bounds__(kScanThreads)
+k4_scan(const uint64_t *__restrict__ db, const uint64_t *__restrict__ qm, uint32_t n0,
+        uint32_t other, uint32_t ncols, uint64_t *__restrict__ cmat) {
+  if (blockIdx.y < kN)
+    scan_body<0, COLS>(db, qm, n0, other, ncols, cmat);
+  else
+    scan_body<1, COLS>(db, qm, n0, other, ncols, cmat);
+}
+
+// ------------------------------------------------------------ scan epilogue
+// inter_to_cts (server.cpp:405-527): INTT per limb of every candidate. A CTA
+// transforms 4 rows of one column and one limb.
+constexpr int kEpiRows = 4;
+
+template <int L>
+__device__ __forceinline__ void epi_body(const Dev4 &P, const Shape4 &S, const uint64_t *cmat,
+                                         uint64_t *mid, uint64_t mid_stride) {
+  extern __shared__ uint64_t sm4[];
+  const int tid = threadIdx.x;
+  const uint32_t r0 = blockIdx.x * kEpiRows, c = blockIdx.z;
+  {
+    ulonglong2 wd[7];
+    iload_d<L>(wd, P.T);
+    for (int e = 0; e < kEpiRows; ++e) {
+      const uint32_t r = r0 + e;
+      uint64_t v[8];
+      if (r < S.other) {
+        ld8(cmat + (static_cast<uint64_t>(c) * S.other + r) * (2 * kN) + L * kN + 8 * tid, v);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = 0;
+      }
+      iD<L>(v, wd);
+      st_plane<3>(sm4 + e * kPad, v, tid);
+    }
+  }
+  __syncthreads();
+  inv_mid<L>(sm4, kEpiRows, P.T);
+  for (int e = 0; e < kEpiRows; ++e) {
+    const uint32_t r = r0 + e;
+    if (r >= S.other) break;  // uniform over the CTA
+    uint64_t w[8];
+    ld_plane<0>(sm4 + e * kPad, w, tid);
+    iA<L>(w);
+    uint64_t *dst = mid + (static_cast<uint64_t>(c >> 1) * mid_stride + r) * kCtWords +
+                    (c & 1) * 2 * kN + L * kN;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dst[posA(tid, k)] = w[k];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k4_epilogue(Dev4 P, Shape4 S, const uint64_t *__restrict__ cmat, uint64_t *__restrict__ mid,
+            uint64_t mid_stride) {
+  if (blockIdx.y == 0)
+    epi_body<0>(P, S, cmat, mid, mid_stride);
+  else
+    epi_body<1>(P, S, cmat, mid, mid_stride);
+}
+
+// ------------------------------------------------------------ MUX level
+// ext_prod_mux (server.cpp:652-722): out = x + INTT(ExtProd(sel, y - x)).
+template <int L>
+__device__ __forceinline__ void mux_body(const Dev4 &P, const Shape4 &S, uint32_t level,
+                                         uint32_t n_pairs, uint32_t offset, uint32_t half,
+                                         const uint64_t *in, uint64_t *out, uint64_t mid_stride,
+                                         const uint64_t *sel) {
+  extern __shared__ uint64_t sm4[];
+  constexpr uint64_t Q = Limb<L>::q;
+  const int b = blockIdx.z, tid = threadIdx.x;
+  const uint32_t i = blockIdx.x;
+  const uint64_t *base_in = in + static_cast<uint64_t>(b) * mid_stride * kCtWords;
+  uint64_t *base_out = out + static_cast<uint64_t>(b) * mid_stride * kCtWords;
+  if (i >= n_pairs) {  // level 0: carry the unpaired prefix over unchanged
+    const uint64_t c = i - n_pairs;
+    for (int j = tid; j < kN; j += kThreads) {
+      base_out[c * kCtWords + L * kN + j] = base_in[c * kCtWords + L * kN + j];
+      base_out[c * kCtWords + 2 * kN + L * kN + j] = base_in[c * kCtWords + 2 * kN + L * kN + j];
+    }
+    return;
+  }
+  uint32_t xi, yi, oi;
+  if (level == 0) { xi = offset + 2 * i; yi = xi + 1; oi = offset + i; }
+  else { xi = i; yi = i + half; oi = i; }
+  const uint64_t *x = base_in + static_cast<uint64_t>(xi) * kCtWords;
+  const uint64_t *y = base_in + static_cast<uint64_t>(yi) * kCtWords;
+  const uint64_t *rgsw = sel + (static_cast<uint64_t>(b) * (S.num_dims - 1) + level) * 2 * kLEp * kCtWords;
+  u128 acc0[8], acc1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
+  gadget_mac<L, kLEp, kBaseEp, false>(P, x, y, rgsw, sm4, acc0, acc1);
+  {
+    ulonglong2 wd[7];
+    iload_d<L>(wd, P.T);
+    uint64_t v[8], w[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { v[k] = red128<Q>(acc0[k]); w[k] = red128<Q>(acc1[k]); }
+    iD<L>(v, wd);
+    iD<L>(w, wd);
+    st_plane<3>(sm4, v, tid);
+    st_plane<3>(sm4 + kPad, w, tid);
+  }
+  __syncthreads();
+  inv_mid<L>(sm4, 2, P.T);
+  uint64_t *o = base_out + static_cast<uint64_t>(oi) * kCtWords;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    uint64_t v[8];
+    ld_plane<0>(sm4 + p * kPad, v, tid);
+    iA<L>(v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int j = posA(tid, k);
+      o[p * 2 * kN + L * kN + j] = add_mod<Q>(x[p * 2 * kN + L * kN + j], v[k]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k4_mux_level(Dev4 P, Shape4 S, uint32_t level, uint32_t n_pairs, uint32_t offset, uint32_t half,
+             const uint64_t *__restrict__ in, uint64_t *__restrict__ out, uint64_t mid_stride,
+             const uint64_t *__restrict__ sel) {
+  if (blockIdx.y == 0)
+    mux_body<0>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
+  else
+    mux_body<1>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
+}
+
+// ------------------------------------------------------------ modulus switch
+// server.cpp:1044-1075: drop q1 with rounding, then utils::rescale
+// (utils.cpp:445-462) q0 -> small_q; bit packing as save_resp_to_stream
+// (server.cpp:950-1009).
+__device__ __forceinline__ uint64_t rescale_dev(uint64_t a, uint64_t inp, uint64_t outm) {
+  const int64_t inp_i = static_cast<int64_t>(inp);
+  const i128 out_i = static_cast<i128>(outm);
+  int64_t v = static_cast<int64_t>(a % inp);
+  if (v >= inp_i / 2) v -= inp_i;
+  const int64_t sign = v >= 0 ? 1 : -1;
+  const i128 val = static_cast<i128>(v) * static_cast<i128>(outm);
+  i128 r = (val + static_cast<i128>(sign * (inp_i / 2))) / static_cast<i128>(inp);
+  r = (r + static_cast<i128>((inp / outm) * outm) + 2 * out_i) % out_i;
+  return static_cast<uint64_t>((r + out_i) % out_i);
+}
+
+__global__ void __launch_bounds__(256)
+k4_modswitch(Dev4 P, const uint64_t *__restrict__ ct_all, uint64_t ct_stride,
+             uint64_t *__restrict__ resp, uint8_t *__restrict__ bytes, uint32_t resp_bytes) {
+  extern __shared__ uint64_t vals[];  // 2N
+  const int b = blockIdx.x;
+  const uint64_t *ct = ct_all + static_cast<uint64_t>(b) * ct_stride * kCtWords;
+  for (int idx = threadIdx.x; idx < 2 * kN; idx += blockDim.x) {
+    const int p = idx >> 12, j = idx & (kN - 1);
+    const u128 x = compose(ct[p * 2 * kN + j], ct[p * 2 * kN + kN + j], P.q0inv, P.q0inv_sh);
+    uint64_t v = static_cast<uint64_t>((x + (static_cast<u128>(kQ1) >> 1)) / kQ1);
+    if (v >= kQ0) v -= kQ0;
+    const uint64_t r = rescale_dev(v, kQ0, P.small_q);
+    resp[static_cast<uint64_t>(b) * 2 * kN + idx] = r;
+    vals[idx] = r & ((1ull << P.small_q_width) - 1);
+  }
+  if (bytes == nullptr) return;
+  __syncthreads();
+  const uint32_t w = P.small_q_width;
+  for (uint32_t B = threadIdx.x; B < resp_bytes; B += blockDim.x) {
+    const uint64_t bit0 = 8ull * B;
+    const uint32_t i = static_cast<uint32_t>(bit0 / w), o = static_cast<uint32_t>(bit0 % w);
+    uint64_t v = vals[i] >> o;
+    const uint32_t have = w - o;
+    if (have < 8 && i + 1 < 2 * kN) v |= vals[i + 1] << have;
+    bytes[static_cast<uint64_t>(b) * resp_bytes + B] = static_cast<uint8_t>(v & 0xFF);
+  }
+}
+
+}  // namespace
+
+// ============================================================== launchers
+uint64_t launch_count() { return g_launches4.load(std::memory_order_relaxed); }
+
+void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2],
+                      const uint64_t *const iw[2], const uint64_t *const iw_sh[2],
+                      const uint64_t ninv[2][2], const uint64_t w1ninv[2][2]) {
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(dev)) return;
+  ulonglong2 f[2][64], i[2][64], a[2], b[2];
+  for (int r = 0; r < 2; ++r) {
+    for (int k = 0; k < 64; ++k) {
+      f[r][k] = make_ulonglong2(fw[r][k], fw_sh[r][k]);
+      i[r][k] = make_ulonglong2(iw[r][k], iw_sh[r][k]);
+    }
+    a[r] = make_ulonglong2(ninv[r][0], ninv[r][1]);
+    b[r] = make_ulonglong2(w1ninv[r][0], w1ninv[r][1]);
+  }
+  cudaError_t e = cudaMemcpyToSymbol(c4_fwt, f, sizeof(f));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c4_iwt, i, sizeof(i));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c4_ninv, a, sizeof(a));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c4_w1ninv, b, sizeof(b));
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("NTT constants: ") + cudaGetErrorString(e));
+  done.insert(dev);
+}
+
+void launch_db_preprocess(const Dev4 &P, const Shape4 &s, const uint64_t *coeffs,
+                          uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
+                          uint64_t pt_begin, uint64_t pt_end, uint64_t *db, cudaStream_t st) {
+  const size_t smem = plane_bytes(kDbTile);
+  set_smem(k4_db_preprocess, smem);
+  const uint64_t tiles = (pt_end - pt_begin + kDbTile - 1) / kDbTile;
+  dim3 grid(static_cast<unsigned>(tiles), 2);
+  k4_db_preprocess<<<grid, kThreads, smem, st>>>(P, coeffs, coeff_pt_begin, seed, t, logical, s.n0,
+                                                   s.other, pt_begin, pt_end, db);
+  check_launch("k4_db_preprocess");
+}
+
+uint32_t expand_nodes(const Shape4 &s, uint32_t d) {
+  const uint64_t span = 1ull << (s.h - d);  // leaves under one node of level d
+  return static_cast<uint32_t>((s.useful + span - 1) / span);
+}
+
+void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint64_t *in,
+                         uint64_t in_stride, uint64_t *out, uint64_t out_stride,
+                         const uint64_t *const *bv_keys, uint64_t bv_level_stride, uint32_t batch,
+                         cudaStream_t st) {
+  const uint32_t nodes = expand_nodes(s, d);
+  if (nodes == 0) return;
+  const size_t smem = plane_bytes(kExpGroup);
+  set_smem(k4_expand_level, smem);
+  const uint32_t k = 1u << d;
+  const uint32_t galois = kN / k + 1;
+  // sigma_k as a gather: sigma(c)[j] = +-c[j k^-1 mod 2N] (utils.cpp:58-72)
+  uint32_t inv = 1;
+  for (uint32_t e = 0; e < 2 * kN; ++e)
+    if ((static_cast<uint64_t>(galois) * e) % (2 * kN) == 1) { inv = e; break; }
+  dim3 grid(nodes, 2, batch);
+  // nodes of level d are heap slots k .. k + nodes - 1, stored from slot 0;
+  // children of node i go to slots 2 i, 2 i + 1 of the next buffer
+  k4_expand_level<<<grid, kThreads, smem, st>>>(P, inv, k, in, in_stride, out, out_stride, bv_keys,
+                                                 static_cast<uint64_t>(d) * bv_level_stride);
+  check_launch("k4_expand_level");
+}
+
+void launch_selectors(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                      const uint64_t *const *gsw_keys, uint64_t *sel, uint32_t batch,
+                      cudaStream_t st) {
+  if (s.num_dims <= 1) return;
+  const size_t smem = plane_bytes(4);
+  set_smem(k4_selectors, smem);
+  dim3 grid((s.num_dims - 1) * s.l_ep, 2, batch);
+  k4_selectors<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
+  check_launch("k4_selectors");
+}
+
+void launch_fst_ntt(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                    uint64_t *qm, uint32_t batch, cudaStream_t st) {
+  const size_t smem = plane_bytes(2 * kFstTile);
+  set_smem(k4_fst_ntt, smem);
+  dim3 grid((s.n0 + kFstTile - 1) / kFstTile, 2, batch);
+  k4_fst_ntt<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, qm, 2 * batch);
+  check_launch("k4_fst_ntt");
+}
+
+void launch_scan(const Shape4 &s, const uint64_t *db, const uint64_t *qm, uint64_t *cmat,
+                 uint32_t batch, cudaStream_t st) {
+  const uint32_t ncols = 2 * batch;
+  // 8 staged columns up to n0 = 2560 (160 KB), 4 above (n0 < 2^12: 128 KB)
+  if (s.n0 <= 2560) {
+    constexpr int C = 8;
+    const size_t smem = static_cast<size_t>(C) * s.n0 * sizeof(uint64_t);
+    set_smem(k4_scan<C>, smem);
+    dim3 grid((ncols + C - 1) / C, 2 * kN);
+    k4_scan<C><<<grid, kScanThreads, smem, st>>>(db, qm, s.n0, s.other, ncols, cmat);
+  } else {
+    constexpr int C = 4;
+    const size_t smem = static_cast<size_t>(C) * s.n0 * sizeof(uint64_t);
+    set_smem(k4_scan<C>, smem);
+    dim3 grid((ncols + C - 1) / C, 2 * kN);
+    k4_scan<C><<<grid, kScanThreads, smem, st>>>(db, qm, s.n0, s.other, ncols, cmat);
+  }
+  check_launch("k4_scan");
+}
+
+void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint64_t *mid,
+                     uint64_t mid_stride, uint32_t batch, cudaStream_t st) {
+  const size_t smem = plane_bytes(kEpiRows);
+  set_smem(k4_epilogue, smem);
+  dim3 grid((s.other + kEpiRows - 1) / kEpiRows, 2, 2 * batch);
+  k4_epilogue<<<grid, kThreads, smem, st>>>(P, s, cmat, mid, mid_stride);
+  check_launch("k4_epilogue");
+}
+
+void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, const uint64_t *in,
+                      uint64_t *out, uint64_t mid_stride, const uint64_t *sel, uint32_t batch,
+                      cudaStream_t st) {
+  const uint32_t h = s.num_dims - 1;
+  const uint32_t other = s.other;
+  uint32_t n_pairs, offset = 0, half = 0, extra = 0;
+  if (other > (1u << h) || 2ull * other < (1ull << h))
+    throw std::invalid_argument("MUX tree: candidate count outside (2^(d-2), 2^(d-1)]");
+  if (level == 0) {
+    const uint32_t last = 2 * other - (1u << h);
+    offset = other - last;
+    n_pairs = last / 2;
+    extra = offset;  // carried prefix
+  } else {
+    half = ((1u << (h - level)) >> 1);
+    n_pairs = half;
+  }
+  if (n_pairs + extra == 0) return;
+  const size_t smem = plane_bytes(kLEp);
+  set_smem(k4_mux_level, smem);
+  dim3 grid(n_pairs + extra, 2, batch);
+  k4_mux_level<<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,
+                                              mid_stride, sel);
+  check_launch("k4_mux_level");
+}
+
+void launch_modswitch(const Dev4 &P, const uint64_t *ct, uint64_t ct_stride, uint64_t *resp,
+                      uint8_t *bytes, uint32_t resp_bytes, uint32_t batch, cudaStream_t st) {
+  const size_t smem = 2 * kN * sizeof(uint64_t);
+  set_smem(k4_modswitch, smem);
+  k4_modswitch<<<batch, 256, smem, st>>>(P, ct, ct_stride, resp, bytes, resp_bytes);
+  check_launch("k4_modswitch");
+}
+
+}  // namespace opir4

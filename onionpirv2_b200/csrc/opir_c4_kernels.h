@@ -1,0 +1,81 @@
+// Launchers of the CONFIG_N4096_K2_MP kernels (opir_c4_kernels.cu).
+//
+// Device layouts (u64 words, canonical residues):
+//   ciphertext : [c0 limb0 (N)][c0 limb1 (N)][c1 limb0 (N)][c1 limb1 (N)]
+//                (rlwe.h:17-31 with K = 2), kCtWords = 4 N words
+//   database   : db[z][row][col], z = limb N + NTT level, the reference's
+//                db[level * num_pt + pt] with pt = row n0 + col
+//                (server.cpp:172-194)
+//   BV keys    : per client [level < h][row < L_KS][b (2N)][a (2N)], NTT form
+//   RGSW key   : per client [row < 2 L_KEY][c0 (2N)][c1 (2N)], NTT form
+//   selectors  : [query][dim < num_dims-1][row < 2 L_EP][ct], NTT form
+//   query mat  : qm[z][k < n0][col < 2 B], col = 2 query + poly
+//   cmat       : [col][row][z]
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace opir4 {
+
+constexpr int kN = 4096;
+constexpr uint64_t kQ0 = 1152921504606830593ull;  // 2^60 - 2^14 + 1
+constexpr uint64_t kQ1 = 1152921504606748673ull;  // 2^60 - 2^16 - 2^15 + 1
+constexpr int kCtWords = 4 * kN;  // u64 words per ciphertext (2 polys x 2 limbs)
+
+// Full twiddle tables in global memory, (w, floor(w 2^64 / q)) pairs per limb
+struct Tables {
+  const ulonglong2 *fwt[2], *iwt[2];
+};
+
+struct Dev4 {
+  uint64_t q0inv, q0inv_sh;        // q0^-1 mod q1 and its Shoup companion
+  Tables T;
+  uint64_t small_q;
+  uint32_t small_q_width;
+};
+
+struct Shape4 {
+  uint32_t n0, other, num_dims, h, useful, l_ep;
+  uint64_t num_pt;
+};
+
+uint64_t launch_count();
+
+void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2],
+                      const uint64_t *const iw[2], const uint64_t *const iw_sh[2],
+                      const uint64_t ninv[2][2], const uint64_t w1ninv[2][2]);
+
+// Nodes of expansion level d that lead to a useful leaf (server.cpp:794-809).
+uint32_t expand_nodes(const Shape4 &s, uint32_t d);
+
+// server.cpp:80-203: plaintexts [pt_begin, pt_end) -> NTT per limb -> db.
+// coeffs (device, u64 < t) holds plaintexts from coeff_pt_begin on; null
+// generates coefficient(pt, c) = mix64(seed + (pt N + c + 1) golden) % t.
+void launch_db_preprocess(const Dev4 &P, const Shape4 &s, const uint64_t *coeffs,
+                          uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
+                          uint64_t pt_begin, uint64_t pt_end, uint64_t *db, cudaStream_t st);
+// One expansion level for `batch` queries; bv_keys: device array of per-query
+// key pointers.
+void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint64_t *in,
+                         uint64_t in_stride, uint64_t *out, uint64_t out_stride,
+                         const uint64_t *const *bv_keys, uint64_t bv_level_stride, uint32_t batch,
+                         cudaStream_t st);
+void launch_selectors(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                      const uint64_t *const *gsw_keys, uint64_t *sel, uint32_t batch,
+                      cudaStream_t st);
+void launch_fst_ntt(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                    uint64_t *qm, uint32_t batch, cudaStream_t st);
+void launch_scan(const Shape4 &s, const uint64_t *db, const uint64_t *qm, uint64_t *cmat,
+                 uint32_t batch, cudaStream_t st);
+void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint64_t *mid,
+                     uint64_t mid_stride, uint32_t batch, cudaStream_t st);
+void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, const uint64_t *in,
+                      uint64_t *out, uint64_t mid_stride, const uint64_t *sel, uint32_t batch,
+                      cudaStream_t st);
+// Modulus switch + (optional) bit packing of `batch` results; resp: 2N u64 per query.
+void launch_modswitch(const Dev4 &P, const uint64_t *ct, uint64_t ct_stride, uint64_t *resp,
+                      uint8_t *bytes, uint32_t resp_bytes, uint32_t batch, cudaStream_t st);
+
+}  // namespace opir4

@@ -1,0 +1,426 @@
+// Host orchestration of the CONFIG_N4096_K2_MP query path: the two-limb
+// counterpart of the PirServer methods (src/server.cpp) on the kernels of
+// opir_c4_kernels.cu. Every arithmetic step runs on the device; the host only
+// validates inputs, moves buffers and enqueues launches on the handle's
+// stream.
+#include "opir_c4_server.h"
+
+#include <algorithm>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+
+#include "opir_params.h"
+
+namespace opir4 {
+
+using opir::ck;
+
+namespace {
+
+constexpr uint64_t kCt = kCtWords;
+constexpr uint32_t kLKsRows = 8, kLKeyRows = 8;
+
+uint32_t resp_bytes_of(const opir_params &p) {
+  return static_cast<uint32_t>((2ull * p.poly_degree * p.small_q_width + 7) / 8);
+}
+
+Shape4 shape_of(const opir_params &p) {
+  Shape4 s{};
+  s.n0 = static_cast<uint32_t>(p.fst_dim_sz);
+  s.other = static_cast<uint32_t>(p.other_dim_sz);
+  s.num_dims = p.num_dims;
+  s.h = p.expansion_height;
+  s.useful = static_cast<uint32_t>(p.fst_dim_sz + static_cast<uint64_t>(p.l_ep) * (p.num_dims - 1));
+  s.l_ep = p.l_ep;
+  s.num_pt = p.num_pt;
+  return s;
+}
+
+// Ciphertext slots per query of an expansion buffer: the widest tree level,
+// the useful leaves, and the candidate rows (the scan's output matrix reuses
+// the buffer that held the leaves).
+uint64_t lvl_slots_of(const Shape4 &s) {
+  uint64_t slots = std::max<uint64_t>(1, std::max(s.useful, s.other));
+  for (uint32_t d = 0; d < s.h; ++d) slots = std::max<uint64_t>(slots, 2ull * expand_nodes(s, d));
+  return slots;
+}
+
+struct Plan {
+  size_t lvl, sel, mid, resp, keyptrs;
+  uint64_t bytes() const { return (2 * lvl + sel + 2 * mid + resp) * 8 + keyptrs * sizeof(void *); }
+};
+
+Plan plan_for(const Shape4 &s, uint64_t lvl_slots, uint32_t n) {
+  const uint64_t nsel = s.num_dims > 1 ? s.num_dims - 1 : 0;
+  Plan pl{};
+  pl.lvl = static_cast<size_t>(n) * lvl_slots * kCt;
+  pl.sel = std::max<uint64_t>(1, n * nsel * 2 * s.l_ep * kCt);
+  pl.mid = static_cast<size_t>(n) * s.other * kCt;
+  pl.resp = static_cast<size_t>(n) * 2 * kN;
+  pl.keyptrs = 2ull * n;
+  return pl;
+}
+
+}  // namespace
+
+opir_params derive(const opir_layout &layout) { return opir::derive_params_c4(layout); }
+
+Server::Server(const opir_params &p, cudaStream_t stream) : p_(p), st_(stream) {
+  sh_ = shape_of(p_);
+  lvl_slots_ = lvl_slots_of(sh_);
+  const opir::LimbTables64 t[2] = {opir::make_limb_tables64(kN, p_.q1, p_.w1),
+                                   opir::make_limb_tables64(kN, p_.q2, p_.w2)};
+  if (t[0].q != kQ0 || t[1].q != kQ1) throw std::invalid_argument("unexpected RNS limbs");
+  // [limb][forward N][inverse N] (w, Shoup) pairs
+  std::vector<ulonglong2> host(4ull * kN);
+  for (int l = 0; l < 2; ++l)
+    for (int i = 0; i < kN; ++i) {
+      host[l * 2 * kN + i] = make_ulonglong2(t[l].fw[i], t[l].fw_sh[i]);
+      host[l * 2 * kN + kN + i] = make_ulonglong2(t[l].iw[i], t[l].iw_sh[i]);
+    }
+  tables_.alloc(host.size());
+  ck(cudaMemcpy(tables_.p, host.data(), host.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice),
+     "twiddle tables");
+  for (int l = 0; l < 2; ++l) {
+    dp_.T.fwt[l] = tables_.p + l * 2 * kN;
+    dp_.T.iwt[l] = tables_.p + l * 2 * kN + kN;
+  }
+  const uint64_t *fw[2] = {t[0].fw.data(), t[1].fw.data()};
+  const uint64_t *fw_sh[2] = {t[0].fw_sh.data(), t[1].fw_sh.data()};
+  const uint64_t *iw[2] = {t[0].iw.data(), t[1].iw.data()};
+  const uint64_t *iw_sh[2] = {t[0].iw_sh.data(), t[1].iw_sh.data()};
+  const uint64_t ninv[2][2] = {{t[0].n_inv, t[0].n_inv_sh}, {t[1].n_inv, t[1].n_inv_sh}};
+  const uint64_t w1n[2][2] = {{t[0].w1_ninv, t[0].w1_ninv_sh}, {t[1].w1_ninv, t[1].w1_ninv_sh}};
+  upload_constants(fw, fw_sh, iw, iw_sh, ninv, w1n);
+  dp_.q0inv = p_.q1_inv_mod_q2;
+  dp_.q0inv_sh = static_cast<uint64_t>((static_cast<unsigned __int128>(dp_.q0inv) << 64) / kQ1);
+  dp_.small_q = p_.small_q;
+  dp_.small_q_width = p_.small_q_width;
+  const uint64_t words = 2ull * kN * p_.num_pt;
+  db_.alloc(words);
+  ck(cudaMemsetAsync(db_.p, 0, words * 8, st_), "db memset");
+  ck(cudaStreamSynchronize(st_), "create");
+}
+
+Server::~Server() {
+  if (st_) cudaStreamSynchronize(st_);
+  for (PtrSlot &sl : ring_) {
+    if (sl.host) cudaFreeHost(sl.host);
+    if (sl.done) cudaEventDestroy(sl.done);
+  }
+}
+
+// ------------------------------------------------------------------ database
+template <typename Fill>
+void Server::load_tiles(uint64_t logical, Fill &&fill) {
+  if (logical > p_.num_pt)
+    throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
+  const uint64_t tile = 2048;
+  std::vector<uint64_t> host(tile * kN);
+  opir::DevBuf<uint64_t> dev;
+  dev.alloc(tile * kN);
+  db_loaded_ = false;
+  for (uint64_t pb = 0; pb < p_.num_pt; pb += tile) {
+    const uint64_t pe = std::min<uint64_t>(p_.num_pt, pb + tile);
+    const uint64_t real_end = std::min<uint64_t>(pe, logical);
+    if (pb < real_end) {
+      fill(pb, real_end, host.data());
+      ck(cudaMemcpyAsync(dev.p, host.data(), (real_end - pb) * kN * 8, cudaMemcpyHostToDevice, st_),
+         "db upload");
+    }
+    launch_db_preprocess(dp_, sh_, dev.p, pb, 0, p_.plain_mod, logical, pb, pe, db_.p, st_);
+    ck(cudaStreamSynchronize(st_), "db preprocess");
+  }
+  db_loaded_ = true;
+}
+
+void Server::load_db(uint64_t logical, const uint64_t *coeffs) {
+  const uint64_t t = p_.plain_mod;
+  load_tiles(logical, [&](uint64_t b, uint64_t e, uint64_t *dst) {
+    const uint64_t *src = coeffs + b * kN;
+    for (uint64_t i = 0; i < (e - b) * kN; ++i) {
+      if (src[i] >= t)
+        throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
+      dst[i] = src[i];
+    }
+  });
+}
+
+void Server::load_db_u16(uint64_t logical, const uint16_t *coeffs) {
+  load_tiles(logical, [&](uint64_t b, uint64_t e, uint64_t *dst) {
+    const uint16_t *src = coeffs + b * kN;
+    for (uint64_t i = 0; i < (e - b) * kN; ++i) dst[i] = src[i];  // < 2^16 < t
+  });
+}
+
+void Server::load_db_source(uint64_t logical, opir_plaintext_source source, void *user) {
+  const uint64_t t = p_.plain_mod;
+  load_tiles(logical, [&](uint64_t b, uint64_t e, uint64_t *dst) {
+    for (uint64_t idx = b; idx < e; ++idx) {
+      uint64_t *pt = dst + (idx - b) * kN;
+      if (source(user, idx, pt) != 0) throw std::invalid_argument("Plaintext source failed");
+      for (int c = 0; c < kN; ++c)
+        if (pt[c] >= t)
+          throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
+    }
+  });
+}
+
+void Server::load_db_seeded(uint64_t logical, uint64_t seed) {
+  if (logical > p_.num_pt)
+    throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
+  db_loaded_ = false;
+  const uint64_t chunk = 1ull << 18;
+  for (uint64_t pb = 0; pb < p_.num_pt; pb += chunk)
+    launch_db_preprocess(dp_, sh_, nullptr, 0, seed, p_.plain_mod, logical, pb,
+                         std::min<uint64_t>(p_.num_pt, pb + chunk), db_.p, st_);
+  ck(cudaStreamSynchronize(st_), "db preprocess");
+  db_loaded_ = true;
+}
+
+// ------------------------------------------------------------------ clients
+void Server::check_ct_values(const uint64_t *v, size_t cts) const {
+  for (size_t c = 0; c < cts; ++c)
+    for (int part = 0; part < 4; ++part) {
+      const uint64_t q = (part & 1) ? kQ1 : kQ0;
+      const uint64_t *w = v + c * kCt + static_cast<size_t>(part) * kN;
+      for (int j = 0; j < kN; ++j)
+        if (w[j] >= q) throw std::invalid_argument("ciphertext coefficient not reduced mod its limb");
+    }
+}
+
+void Server::set_client_keys(uint64_t id, const uint64_t *bv_keys, const uint32_t *galois_ks,
+                             uint32_t n_keys, const uint64_t *gsw_key) {
+  const uint32_t h = p_.expansion_height;
+  if (!gsw_key) throw std::invalid_argument("PirServer session key bundle cannot be null");
+  if (n_keys < h) throw std::invalid_argument("PirServer session lacks keys for its expansion height");
+  if (n_keys && (!bv_keys || !galois_ks)) throw std::invalid_argument("null BV key arrays");
+  const size_t key_words = static_cast<size_t>(kLKsRows) * kCt;  // one BvKeySwitchKey
+  std::vector<int> order(h);
+  for (uint32_t d = 0; d < h; ++d) {
+    const uint32_t want = kN / (1u << d) + 1;
+    order[d] = -1;
+    for (uint32_t i = 0; i < n_keys; ++i)
+      if (galois_ks[i] == want) { order[d] = static_cast<int>(i); break; }
+    if (order[d] < 0) throw std::out_of_range("BvGaloisKeys::get: galois_k not found");
+    check_ct_values(bv_keys + order[d] * key_words, kLKsRows);
+  }
+  const size_t gsw_rows = 2ull * kLKeyRows;
+  check_ct_values(gsw_key, gsw_rows);
+  Keys k;
+  k.bv.alloc(std::max<size_t>(1, h * key_words));
+  k.gsw.alloc(gsw_rows * kCt);
+  for (uint32_t d = 0; d < h; ++d)
+    ck(cudaMemcpyAsync(k.bv.p + d * key_words, bv_keys + order[d] * key_words, key_words * 8,
+                       cudaMemcpyHostToDevice, st_), "bv upload");
+  ck(cudaMemcpyAsync(k.gsw.p, gsw_key, gsw_rows * kCt * 8, cudaMemcpyHostToDevice, st_),
+     "gsw upload");
+  ck(cudaStreamSynchronize(st_), "key upload");
+  Keys &slot = clients_[id];
+  slot.bv.swap(k.bv);
+  slot.gsw.swap(k.gsw);
+}
+
+void Server::remove_client(uint64_t id) {
+  ck(cudaStreamSynchronize(st_), "remove_client");
+  if (clients_.erase(id) == 0) throw std::out_of_range("unknown client id");
+}
+
+// ------------------------------------------------------------------ scratch
+void Server::ensure_capacity(uint32_t n) {
+  if (n <= cap_) return;
+  const Plan pl = plan_for(sh_, lvl_slots_, n);
+  for (auto &b : lvl_) b.alloc(pl.lvl);
+  sel_.alloc(pl.sel);
+  for (auto &b : mid_) b.alloc(pl.mid);
+  resp_.alloc(pl.resp);
+  keyptrs_.alloc(pl.keyptrs);
+  cap_ = n;
+}
+
+void Server::reserve(uint32_t max_batch) {
+  ensure_capacity(max_batch);
+  grow_ptr_slots(2ull * max_batch);
+}
+
+void Server::plan_memory(const opir_params &p, opir_memory_plan *out) {
+  const Shape4 s = shape_of(p);
+  const uint64_t slots = lvl_slots_of(s);
+  const uint64_t one = plan_for(s, slots, 1).bytes(), two = plan_for(s, slots, 2).bytes();
+  out->database_bytes = 2ull * kN * p.num_pt * 8 + 4ull * kN * sizeof(ulonglong2);
+  out->client_key_bytes =
+      (static_cast<uint64_t>(p.expansion_height) * kLKsRows + 2ull * kLKeyRows) * kCt * 8;
+  out->scratch_bytes_per_query = two - one;
+  out->scratch_bytes_fixed = 2 * one - two;
+}
+
+void Server::grow_ptr_slots(size_t entries) {
+  for (PtrSlot &sl : ring_) {
+    if (!sl.done) ck(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "event");
+    if (sl.cap >= entries) continue;
+    ck(cudaEventSynchronize(sl.done), "key pointer slot");
+    if (sl.host) cudaFreeHost(sl.host);
+    sl.host = nullptr;
+    sl.cap = 0;
+    ck(cudaMallocHost(reinterpret_cast<void **>(&sl.host), entries * sizeof(void *)),
+       "cudaMallocHost");
+    sl.cap = entries;
+  }
+}
+
+// Per-query key pointers (BV then RGSW) from a pinned slot of a small ring,
+// so the upload is asynchronous; a slot is refilled only after the copy that
+// last read it has run.
+void Server::upload_keyptrs(const uint64_t *ids, uint32_t n) {
+  host_ptrs_.resize(2ull * n);
+  for (uint32_t i = 0; i < n; ++i) {
+    auto it = clients_.find(ids[i]);
+    if (it == clients_.end()) throw std::out_of_range("unknown client id " + std::to_string(ids[i]));
+    host_ptrs_[i] = it->second.bv.p;
+    host_ptrs_[n + i] = it->second.gsw.p;
+  }
+  grow_ptr_slots(2ull * n);
+  PtrSlot &sl = ring_[ring_next_++ % kPtrSlots];
+  ck(cudaEventSynchronize(sl.done), "key pointer slot");
+  std::copy(host_ptrs_.begin(), host_ptrs_.end(), sl.host);
+  ck(cudaMemcpyAsync(keyptrs_.p, sl.host, 2ull * n * sizeof(void *), cudaMemcpyHostToDevice, st_),
+     "key pointers");
+  ck(cudaEventRecord(sl.done, st_), "event record");
+}
+
+// ------------------------------------------------------------------ pipeline
+void Server::stage_in(const uint64_t *d_queries, uint32_t n) {
+  ck(cudaMemcpy2DAsync(lvl_[0].p, lvl_slots_ * kCt * 8, d_queries, kCt * 8, kCt * 8, n,
+                       cudaMemcpyDeviceToDevice, st_), "query staging");
+}
+
+const uint64_t *Server::run_expand(uint32_t n) {
+  const uint64_t level_stride = static_cast<uint64_t>(kLKsRows) * kCt;
+  for (uint32_t d = 0; d < sh_.h; ++d)
+    launch_expand_level(dp_, sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p, lvl_slots_,
+                        keyptrs_.p, level_stride, n, st_);
+  return lvl_[sh_.h & 1].p;
+}
+
+// First dimension: NTT of the first n0 leaves into the query matrix (in the
+// expansion buffer that does not hold the leaves), the scan (its output in
+// the leaves' buffer, dead by then), INTT into mid_[0].
+void Server::run_first_dim(const uint64_t *leaves, uint32_t n, const Mark &mark) {
+  const int li = leaves == lvl_[0].p ? 0 : 1;
+  uint64_t *qm = lvl_[li ^ 1].p;
+  uint64_t *cmat = lvl_[li].p;
+  launch_fst_ntt(dp_, sh_, leaves, lvl_slots_, qm, n, st_);
+  if (mark) mark(6);
+  launch_scan(sh_, db_.p, qm, cmat, n, st_);
+  if (mark) mark(7);
+  launch_epilogue(dp_, sh_, cmat, mid_[0].p, sh_.other, n, st_);
+}
+
+const uint64_t *Server::run_other_dims(uint32_t n) {
+  if (sh_.num_dims <= 1) return mid_[0].p;
+  const uint32_t levels = sh_.num_dims - 1;
+  for (uint32_t a = 0; a < levels; ++a)
+    launch_mux_level(dp_, sh_, a, mid_[a & 1].p, mid_[(a + 1) & 1].p, sh_.other, sel_.p, n, st_);
+  return mid_[levels & 1].p;
+}
+
+void Server::run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
+                          uint64_t *d_resp, const Mark &mark) {
+  if (!db_loaded_) throw std::runtime_error("make_query before load_data");
+  if (n == 0) return;
+  ensure_capacity(n);
+  upload_keyptrs(ids, n);
+  if (mark) mark(0);
+  if (d_queries) stage_in(d_queries, n);
+  const uint64_t *leaves = run_expand(n);
+  if (mark) mark(1);
+  launch_selectors(dp_, sh_, leaves, lvl_slots_, keyptrs_.p + n, sel_.p, n, st_);
+  if (mark) mark(2);
+  run_first_dim(leaves, n, mark);
+  if (mark) mark(3);
+  const uint64_t *res = run_other_dims(n);
+  if (mark) mark(4);
+  launch_modswitch(dp_, res, sh_.other, d_resp, nullptr, resp_bytes_of(p_), n, st_);
+  if (mark) mark(5);
+}
+
+void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *queries,
+                              uint64_t *responses, const Mark &mark) {
+  check_ct_values(queries, n);
+  if (!db_loaded_) throw std::runtime_error("make_query before load_data");
+  if (n == 0) return;
+  ensure_capacity(n);
+  ck(cudaMemcpy2DAsync(lvl_[0].p, lvl_slots_ * kCt * 8, queries, kCt * 8, kCt * 8, n,
+                       cudaMemcpyHostToDevice, st_), "query upload");
+  run_pipeline(n, ids, nullptr, resp_.p, mark);
+  ck(cudaMemcpyAsync(responses, resp_.p, static_cast<size_t>(n) * 2 * kN * 8,
+                     cudaMemcpyDeviceToHost, st_), "response download");
+  ck(cudaStreamSynchronize(st_), "make_query");
+}
+
+void Server::make_query_batch_device(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
+                                     uint64_t *d_responses, const Mark &mark) {
+  run_pipeline(n, ids, d_queries, d_responses, mark);
+}
+
+// ------------------------------------------------------------------ stages
+void Server::expand_query(uint64_t id, const uint64_t *query, uint64_t *out) {
+  check_ct_values(query, 1);
+  ensure_capacity(1);
+  upload_keyptrs(&id, 1);
+  ck(cudaMemcpyAsync(lvl_[0].p, query, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  const uint64_t *leaves = run_expand(1);
+  ck(cudaMemcpyAsync(out, leaves, static_cast<size_t>(sh_.useful) * kCt * 8,
+                     cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaStreamSynchronize(st_), "expand_query");
+}
+
+void Server::complete_selectors(uint64_t id, const uint64_t *expanded, uint64_t *out) {
+  check_ct_values(expanded, sh_.useful);
+  ensure_capacity(1);
+  upload_keyptrs(&id, 1);
+  const uint32_t nsel = sh_.num_dims - 1;
+  if (nsel == 0) {
+    ck(cudaStreamSynchronize(st_), "complete_selectors");
+    return;
+  }
+  ck(cudaMemcpyAsync(lvl_[0].p, expanded, static_cast<size_t>(sh_.useful) * kCt * 8,
+                     cudaMemcpyHostToDevice, st_), "upload");
+  launch_selectors(dp_, sh_, lvl_[0].p, lvl_slots_, keyptrs_.p + 1, sel_.p, 1, st_);
+  ck(cudaMemcpyAsync(out, sel_.p, static_cast<size_t>(nsel) * 2 * sh_.l_ep * kCt * 8,
+                     cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaStreamSynchronize(st_), "complete_selectors");
+}
+
+void Server::evaluate_first_dim(const uint64_t *fst_query, uint64_t *out) {
+  if (!db_loaded_) throw std::runtime_error("evaluate_first_dim before load_data");
+  check_ct_values(fst_query, sh_.n0);
+  ensure_capacity(1);
+  ck(cudaMemcpyAsync(lvl_[0].p, fst_query, static_cast<size_t>(sh_.n0) * kCt * 8,
+                     cudaMemcpyHostToDevice, st_), "upload");
+  run_first_dim(lvl_[0].p, 1, Mark());
+  ck(cudaMemcpyAsync(out, mid_[0].p, static_cast<size_t>(sh_.other) * kCt * 8,
+                     cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaStreamSynchronize(st_), "evaluate_first_dim");
+}
+
+void Server::evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, uint64_t *out) {
+  const uint32_t nsel = sh_.num_dims - 1;
+  if (nsel && sh_.other < (1u << (nsel - 1)))
+    throw std::invalid_argument("evaluate_other_dim: layout has fewer candidates than its selector tree");
+  check_ct_values(mid, sh_.other);
+  if (nsel) check_ct_values(selectors, static_cast<size_t>(nsel) * 2 * sh_.l_ep);
+  ensure_capacity(1);
+  ck(cudaMemcpyAsync(mid_[0].p, mid, static_cast<size_t>(sh_.other) * kCt * 8,
+                     cudaMemcpyHostToDevice, st_), "upload");
+  if (nsel)
+    ck(cudaMemcpyAsync(sel_.p, selectors, static_cast<size_t>(nsel) * 2 * sh_.l_ep * kCt * 8,
+                       cudaMemcpyHostToDevice, st_), "upload");
+  const uint64_t *r = run_other_dims(1);
+  ck(cudaMemcpyAsync(out, r, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaStreamSynchronize(st_), "evaluate_other_dim");
+}
+
+}  // namespace opir4

@@ -1,0 +1,101 @@
+// Server state and query pipeline for CONFIG_N4096_K2_MP
+// (includes/database_constants.h:111-125). The C-ABI handle forwards to this
+// class when it was created with two-limb parameters; argument checking that
+// does not depend on the parameter set stays in the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <functional>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/onionpir_b200.h"
+#include "opir_c4_kernels.h"
+#include "opir_host.h"
+
+namespace opir4 {
+
+class Server {
+ public:
+  using Mark = std::function<void(int)>;  // stage-boundary hook (may be empty)
+
+  Server(const opir_params &p, cudaStream_t stream);
+  Server(const Server &) = delete;
+  Server &operator=(const Server &) = delete;
+  ~Server();
+
+  const opir_params &params() const { return p_; }
+  bool db_loaded() const { return db_loaded_; }
+
+  // server.cpp:80-203; coefficients are host arrays (each < t)
+  void load_db(uint64_t logical, const uint64_t *coeffs);
+  void load_db_u16(uint64_t logical, const uint16_t *coeffs);
+  void load_db_source(uint64_t logical, opir_plaintext_source source, void *user);
+  void load_db_seeded(uint64_t logical, uint64_t seed);
+
+  void set_client_keys(uint64_t id, const uint64_t *bv_keys, const uint32_t *galois_ks,
+                       uint32_t n_keys, const uint64_t *gsw_key);
+  void remove_client(uint64_t id);
+
+  // Host buffers: n queries of 4N u64 in, n responses of 2N u64 out.
+  void make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *queries,
+                        uint64_t *responses, const Mark &mark);
+  // Device buffers, enqueued on the handle's stream (no wait).
+  void make_query_batch_device(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
+                               uint64_t *d_responses, const Mark &mark);
+  void reserve(uint32_t max_batch);
+  static void plan_memory(const opir_params &p, opir_memory_plan *out);
+
+  // Public stages of make_query (host buffers, reference layouts).
+  void expand_query(uint64_t id, const uint64_t *query, uint64_t *out);
+  void complete_selectors(uint64_t id, const uint64_t *expanded, uint64_t *out);
+  void evaluate_first_dim(const uint64_t *fst_query, uint64_t *out);
+  void evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, uint64_t *out);
+
+ private:
+  struct Keys {
+    opir::DevBuf<uint64_t> bv, gsw;
+  };
+  struct PtrSlot {
+    const uint64_t **host = nullptr;
+    size_t cap = 0;
+    cudaEvent_t done = nullptr;
+  };
+  static constexpr int kPtrSlots = 4;
+
+  void ensure_capacity(uint32_t n);
+  void upload_keyptrs(const uint64_t *ids, uint32_t n);
+  void grow_ptr_slots(size_t entries);
+  void check_ct_values(const uint64_t *v, size_t cts) const;
+  void stage_in(const uint64_t *d_queries, uint32_t n);
+  const uint64_t *run_expand(uint32_t n);
+  void run_first_dim(const uint64_t *leaves, uint32_t n, const Mark &mark);
+  const uint64_t *run_other_dims(uint32_t n);
+  void run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
+                    uint64_t *d_resp, const Mark &mark);
+  template <typename Fill>
+  void load_tiles(uint64_t logical, Fill &&fill);
+
+  opir_params p_{};
+  Shape4 sh_{};
+  Dev4 dp_{};
+  cudaStream_t st_ = nullptr;
+  opir::DevBuf<ulonglong2> tables_;
+  opir::DevBuf<uint64_t> db_;
+  bool db_loaded_ = false;
+  std::unordered_map<uint64_t, Keys> clients_;
+  uint32_t cap_ = 0;
+  uint64_t lvl_slots_ = 1;
+  opir::DevBuf<uint64_t> q_in_, resp_, lvl_[2], sel_, mid_[2];
+  opir::DevBuf<const uint64_t *> keyptrs_;
+  std::vector<const uint64_t *> host_ptrs_;
+  PtrSlot ring_[kPtrSlots];
+  uint32_t ring_next_ = 0;
+};
+
+// Parameters of the two-limb set for a layout (pir.cpp:49-134).
+opir_params derive(const opir_layout &layout);
+
+}  // namespace opir4

@@ -204,4 +204,79 @@ LimbTables make_limb_tables(uint32_t n, uint32_t q, uint32_t root) {
   return t;
 }
 
+opir_params derive_params_c4(const opir_layout &layout) {
+  // pir.cpp:49-134 with CONFIG_N4096_K2_MP (database_constants.h:111-125):
+  // RnsMods {60, 60}, PlainMod 40, SmallQWidth 50, L_EP 5, L_KEY 8, L_KS 8.
+  constexpr uint32_t N = 4096;
+  opir_params p{};
+  p.poly_degree = N;
+  p.num_limbs = 2;
+  const auto pr = ntt_friendly_primes({60, 60}, N);
+  p.q1 = pr[0];  // the two RNS limbs (q0, q1 in the reference's naming)
+  p.q2 = pr[1];
+  p.q = 0;       // the product exceeds 64 bits
+  p.w1 = min_primitive_root(2ull * N, p.q1);
+  p.w2 = min_primitive_root(2ull * N, p.q2);
+  uint64_t inv = 0;
+  if (!invert_mod(p.q1 % p.q2, p.q2, inv)) throw std::runtime_error("limbs must be coprime");
+  p.q1_inv_mod_q2 = inv;
+  p.w_crt = 0;
+  p.plain_mod = generate_prime(40);
+  p.small_q = ntt_friendly_primes({50}, N)[0];
+  p.small_q_width = 50;
+  p.ct_mod_width = 120;  // pir.cpp:188-194: sum of the configured limb widths
+  p.l_ep = 5;
+  p.l_key = 8;
+  p.l_ks = 8;
+  p.base_log2 = (p.ct_mod_width + p.l_ep - 1) / p.l_ep;
+  p.base_log2_key = (p.ct_mod_width + p.l_key - 1) / p.l_key;
+  p.base_log2_ks = p.ct_mod_width / p.l_ks + 1;
+  if (layout.target_num_pt == 0)
+    throw std::invalid_argument("PirParams: target_num_pt must be positive");
+  if (layout.expansion_height > 12)
+    throw std::invalid_argument("PirParams: expansion_height exceeds the ring automorphism capacity");
+  const auto shape = calc_db_shape(layout.target_num_pt, p.l_ep, layout.expansion_height,
+                                   layout.fst_dim_pow2 != 0);
+  const uint64_t other = (layout.target_num_pt + shape.first - 1) / shape.first;
+  if (other > std::numeric_limits<uint64_t>::max() / shape.first)
+    throw std::overflow_error("PirParams: rounded database shape overflows");
+  p.target_num_pt = layout.target_num_pt;
+  p.expansion_height = layout.expansion_height;
+  p.fst_dim_pow2 = layout.fst_dim_pow2 ? 1 : 0;
+  p.fst_dim_sz = shape.first;
+  p.num_dims = static_cast<uint32_t>(shape.second);
+  p.other_dim_sz = other;
+  p.num_pt = shape.first * other;
+  return p;
+}
+
+LimbTables64 make_limb_tables64(uint32_t n, uint64_t q, uint64_t root) {
+  LimbTables64 t;
+  t.q = q;
+  uint32_t lg = 0;
+  while ((1u << lg) < n) ++lg;
+  uint64_t rinv = 0;
+  invert_mod(root % q, q, rinv);
+  std::vector<uint64_t> pw(n), ipw(n);
+  pw[0] = ipw[0] = 1;
+  for (uint32_t i = 1; i < n; ++i) {
+    pw[i] = static_cast<uint64_t>(static_cast<u128>(pw[i - 1]) * root % q);
+    ipw[i] = static_cast<uint64_t>(static_cast<u128>(ipw[i - 1]) * rinv % q);
+  }
+  auto shoup = [q](uint64_t w) { return static_cast<uint64_t>((static_cast<u128>(w) << 64) / q); };
+  t.fw.resize(n); t.fw_sh.resize(n); t.iw.resize(n); t.iw_sh.resize(n);
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t e = bitrev(k, lg);
+    t.fw[k] = pw[e]; t.fw_sh[k] = shoup(pw[e]);
+    t.iw[k] = ipw[e]; t.iw_sh[k] = shoup(ipw[e]);
+  }
+  uint64_t ninv = 0;
+  invert_mod(n % q, q, ninv);
+  t.n_inv = ninv;
+  t.n_inv_sh = shoup(ninv);
+  t.w1_ninv = static_cast<uint64_t>(static_cast<u128>(t.iw[1]) * ninv % q);
+  t.w1_ninv_sh = shoup(t.w1_ninv);
+  return t;
+}
+
 }  // namespace opir

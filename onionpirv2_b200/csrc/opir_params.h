@@ -1,4 +1,5 @@
-// Host-side parameter derivation for CONFIG_N2048_K1_COMP: primes, roots,
+// Host-side parameter derivation for CONFIG_N2048_K1_COMP (and
+// CONFIG_N4096_K2_MP): primes, roots,
 // gadget bases, database shape, NTT twiddle tables for the two CRT limbs.
 #pragma once
 
@@ -28,5 +29,17 @@ struct LimbTables {
   std::vector<uint32_t> fw, fw_sh, iw, iw_sh;
 };
 LimbTables make_limb_tables(uint32_t n, uint32_t q, uint32_t root);
+
+// CONFIG_N4096_K2_MP: N = 4096, two 60-bit RNS limbs (q1, q2 fields hold the
+// limbs, q = 0), t = generate_prime(40), small_q 50-bit, L_EP 5, L_KEY 8, L_KS 8.
+opir_params derive_params_c4(const opir_layout &layout);
+
+// 64-bit limb tables: bit-reversed powers with Shoup companions
+// floor(w 2^64 / q), N^-1 and iw[1] N^-1 with theirs.
+struct LimbTables64 {
+  uint64_t q = 0, n_inv = 0, n_inv_sh = 0, w1_ninv = 0, w1_ninv_sh = 0;
+  std::vector<uint64_t> fw, fw_sh, iw, iw_sh;
+};
+LimbTables64 make_limb_tables64(uint32_t n, uint64_t q, uint64_t root);
 
 }  // namespace opir

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -15,59 +16,18 @@
 #include <vector>
 
 #include "../../include/onionpir_b200.h"
+#include "opir_c4_server.h"
+#include "opir_host.h"
 #include "opir_kernels.h"
 #include "opir_params.h"
 #include "opir_scan_tc.h"
 
 namespace {
 
-struct CudaError : std::runtime_error {
-  using std::runtime_error::runtime_error;
-};
-
-void ck(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <typename T>
-struct DevBuf {
-  T *p = nullptr;
-  size_t n = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf &) = delete;
-  DevBuf &operator=(const DevBuf &) = delete;
-  ~DevBuf() { reset(); }
-  void reset() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  void alloc(size_t count) {
-    if (count <= n && p) return;
-    reset();
-    if (count == 0) return;
-    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
-      cudaGetLastError();
-      p = nullptr;
-      throw std::bad_alloc();
-    }
-    n = count;
-  }
-};
-
-// Restores the caller's current device on scope exit.
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) ck(cudaSetDevice(dev), "cudaSetDevice");
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
+using opir::CudaError;
+using opir::ck;
+using opir::DevBuf;
+using opir::DeviceGuard;
 
 struct ClientKeys {
   DevBuf<uint32_t> bv;   // h x L_KS x 2 polys x 2 residues x N
@@ -133,6 +93,8 @@ struct opir_server {
   std::vector<std::vector<cudaEvent_t>> ev_pool;
   uint32_t timed_calls = 0;
   cudaEvent_t *cur_ev = nullptr;
+  // CONFIG_N4096_K2_MP handles forward every call to this object
+  std::unique_ptr<opir4::Server> c4;
 };
 
 namespace {
@@ -360,6 +322,15 @@ void mark(opir_server *s, int i) {
   if (s->cur_ev) ck(cudaEventRecord(s->cur_ev[i], s->stream), "cudaEventRecord");
 }
 
+// Stage hook for a two-limb call: one event set per timed call, as above.
+opir4::Server::Mark c4_marks(opir_server *s) {
+  begin_timed_call(s);
+  if (!s->cur_ev) return opir4::Server::Mark();
+  return [s](int i) { mark(s, i); };
+}
+
+bool is_c4(const opir_params &p) { return p.num_limbs == 2 && p.poly_degree == 4096; }
+
 // Expansion (Algorithm 2) over n queries whose residue pairs sit in slot 0 of
 // lvl[0]; returns the buffer holding the leaves.
 uint32_t *run_expand(opir_server *s, uint32_t n) {
@@ -540,6 +511,14 @@ opir_status opir_params_init(const opir_layout *layout, opir_params *out) {
   return guarded(nullptr, [&] { *out = opir::derive_params(*layout); });
 }
 
+opir_status opir_params_init_config(opir_config config, const opir_layout *layout,
+                                    opir_params *out) {
+  if (!layout || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  if (config == OPIR_CONFIG_N2048_K1_COMP) return opir_params_init(layout, out);
+  if (config != OPIR_CONFIG_N4096_K2_MP) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] { *out = opir4::derive(*layout); });
+}
+
 size_t opir_response_bytes(const opir_params *params) {
   return params ? resp_bytes_of(*params) : 0;
 }
@@ -550,8 +529,20 @@ opir_status opir_server_create(const opir_params *params, int device, opir_serve
   opir_server *s = new (std::nothrow) opir_server();
   if (!s) return OPIR_ERR_NO_MEMORY;
   const opir_status st = guarded(s, [&] {
+    if (is_c4(*params)) {
+      opir_layout lay{params->target_num_pt, params->expansion_height, params->fst_dim_pow2};
+      const opir_params check = opir4::derive(lay);
+      if (check.num_pt != params->num_pt || check.q1 != params->q1 || check.q2 != params->q2)
+        throw std::invalid_argument("params do not match their layout");
+      s->params = check;
+      s->device = device;
+      DeviceGuard g(device);
+      ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      s->c4.reset(new opir4::Server(check, s->stream));
+      return;
+    }
     if (params->poly_degree != static_cast<uint32_t>(kN) || params->num_limbs != 1)
-      throw std::invalid_argument("only CONFIG_N2048_K1_COMP parameters are supported");
+      throw std::invalid_argument("unsupported parameter set (CONFIG_N2048_K1_COMP or CONFIG_N4096_K2_MP)");
     opir_layout lay{params->target_num_pt, params->expansion_height, params->fst_dim_pow2};
     const opir_params check = opir::derive_params(lay);
     if (check.num_pt != params->num_pt || check.q != params->q)
@@ -591,6 +582,7 @@ void opir_server_destroy(opir_server *s) {
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    s->c4.reset();
     s->clients.clear();
     s->tables.reset();
     s->db8.reset();
@@ -631,6 +623,7 @@ opir_status opir_server_load_db_u16(opir_server *s, uint64_t logical, const uint
   return guarded(s, [&] {
     if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
+    if (s->c4) return s->c4->load_db_u16(logical, coeffs);
     const uint64_t t = s->params.plain_mod;
     load_tiles(s, logical, [&](uint64_t b, uint64_t e, uint16_t *dst) {
       const uint16_t *src = coeffs + b * kN;
@@ -648,6 +641,7 @@ opir_status opir_server_load_db(opir_server *s, uint64_t logical, const uint64_t
   return guarded(s, [&] {
     if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
+    if (s->c4) return s->c4->load_db(logical, coeffs);
     const uint64_t t = s->params.plain_mod;
     load_tiles(s, logical, [&](uint64_t b, uint64_t e, uint16_t *dst) {
       const uint64_t *src = coeffs + b * kN;
@@ -666,6 +660,7 @@ opir_status opir_server_load_db_source(opir_server *s, uint64_t logical,
   return guarded(s, [&] {
     if (!source) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
+    if (s->c4) return s->c4->load_db_source(logical, source, user);
     const uint64_t t = s->params.plain_mod;
     std::vector<uint64_t> pt(kN);
     load_tiles(s, logical, [&](uint64_t b, uint64_t e, uint16_t *dst) {
@@ -686,6 +681,7 @@ opir_status opir_server_load_db_seeded(opir_server *s, uint64_t logical, uint64_
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     DeviceGuard g(s->device);
+    if (s->c4) return s->c4->load_db_seeded(logical, seed);
     const opir_params &p = s->params;
     if (logical > p.num_pt)
       throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
@@ -704,6 +700,10 @@ opir_status opir_server_set_client_keys(opir_server *s, uint64_t client_id,
                                         uint32_t n_keys, const uint64_t *gsw_key) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
+    if (s->c4) {
+      DeviceGuard g(s->device);
+      return s->c4->set_client_keys(client_id, bv_keys, galois_ks, n_keys, gsw_key);
+    }
     const opir_params &p = s->params;
     const uint32_t h = p.expansion_height;
     if (!gsw_key) throw std::invalid_argument("PirServer session key bundle cannot be null");
@@ -748,6 +748,7 @@ opir_status opir_server_remove_client(opir_server *s, uint64_t client_id) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     DeviceGuard g(s->device);
+    if (s->c4) return s->c4->remove_client(client_id);
     ck(cudaStreamSynchronize(s->stream), "remove_client");
     if (s->clients.erase(client_id) == 0) throw std::out_of_range("unknown client id");
   });
@@ -758,6 +759,10 @@ opir_status opir_server_make_query_batch(opir_server *s, uint32_t n, const uint6
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (n && (!client_ids || !queries || !responses)) throw std::invalid_argument("null argument");
+    if (s->c4) {
+      DeviceGuard g(s->device);
+      return s->c4->make_query_batch(n, client_ids, queries, responses, c4_marks(s));
+    }
     check_query_values(s, queries, static_cast<size_t>(n) * 2 * kN);
     DeviceGuard g(s->device);
     ensure_capacity(s, n);
@@ -791,7 +796,10 @@ opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
       ck(cudaStreamWaitEvent(s->stream, e, 0), "wait");
       cudaEventDestroy(e);
     }
-    run_pipeline(s, client_ids, n, d_queries, d_responses, nullptr);
+    if (s->c4)
+      s->c4->make_query_batch_device(n, client_ids, d_queries, d_responses, c4_marks(s));
+    else
+      run_pipeline(s, client_ids, n, d_queries, d_responses, nullptr);
     if (user) {
       cudaEvent_t e;
       ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -805,8 +813,9 @@ opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
 opir_status opir_plan_memory(const opir_params *params, opir_memory_plan *out) {
   if (!params || !out) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] {
+    if (is_c4(*params)) return opir4::Server::plan_memory(*params, out);
     if (params->poly_degree != static_cast<uint32_t>(kN) || params->num_limbs != 1)
-      throw std::invalid_argument("only CONFIG_N2048_K1_COMP parameters are supported");
+      throw std::invalid_argument("unsupported parameter set (CONFIG_N2048_K1_COMP or CONFIG_N4096_K2_MP)");
     uint64_t slots = 0;
     const opir::Shape sh = make_shape(*params, &slots);
     const uint32_t rb = resp_bytes_of(*params);
@@ -824,6 +833,7 @@ opir_status opir_server_reserve(opir_server *s, uint32_t max_batch) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     DeviceGuard g(s->device);
+    if (s->c4) return s->c4->reserve(max_batch);
     ensure_capacity(s, max_batch);
     grow_keyptr_slots(s, 2ull * max_batch);
   });
@@ -832,8 +842,10 @@ opir_status opir_server_reserve(opir_server *s, uint32_t max_batch) {
 opir_status opir_server_autotune(opir_server *s, uint32_t max_batch) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
-    if (!s->db_loaded) throw std::runtime_error("autotune before load_data");
+    if (!(s->c4 ? s->c4->db_loaded() : s->db_loaded))
+      throw std::runtime_error("autotune before load_data");
     if (max_batch == 0) throw std::invalid_argument("max_batch must be positive");
+    if (s->c4) return;  // the two-limb scan has no tiling to tune
     if (s->shape.n0p > 8192) return;  // the CUDA-core scan has no tiling to tune
     DeviceGuard g(s->device);
     ensure_capacity(s, max_batch);
@@ -877,6 +889,10 @@ opir_status opir_server_autotune(opir_server *s, uint32_t max_batch) {
 opir_status opir_server_scan_tile(const opir_server *s, uint32_t n, uint32_t *ntile, uint32_t *kt,
                                   uint32_t *stages) {
   if (!s || !ntile || !kt || !stages || n == 0) return OPIR_ERR_INVALID_ARGUMENT;
+  if (s->c4) {  // CUDA-core scan: no tensor-core tiling
+    *ntile = *kt = *stages = 0;
+    return OPIR_OK;
+  }
   const ScanTile t = effective_tile(s, n);
   *ntile = t.ntile;
   *kt = t.kt;
@@ -913,15 +929,16 @@ opir_status opir_server_stage_times(opir_server *s, float *ms_out, uint32_t *cal
   });
 }
 
-uint64_t opir_launch_count(void) { return opir::launch_count(); }
+uint64_t opir_launch_count(void) { return opir::launch_count() + opir4::launch_count(); }
 
 opir_status opir_server_expand_query(opir_server *s, uint64_t client_id, const uint64_t *query,
                                      uint64_t *out) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (!query || !out) throw std::invalid_argument("null argument");
-    check_query_values(s, query, 2 * kN);
     DeviceGuard g(s->device);
+    if (s->c4) return s->c4->expand_query(client_id, query, out);
+    check_query_values(s, query, 2 * kN);
     ensure_capacity(s, 1);
     upload_keyptrs(s, &client_id, 1);
     ck(cudaMemcpyAsync(s->q_u64.p, query, 2 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
@@ -940,6 +957,10 @@ opir_status opir_server_complete_selectors(opir_server *s, uint64_t client_id,
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (!expanded || !out) throw std::invalid_argument("null argument");
+    if (s->c4) {
+      DeviceGuard g(s->device);
+      return s->c4->complete_selectors(client_id, expanded, out);
+    }
     const opir::Shape &sh = s->shape;
     check_query_values(s, expanded, static_cast<size_t>(sh.useful) * 2 * kN);
     DeviceGuard g(s->device);
@@ -966,6 +987,10 @@ opir_status opir_server_evaluate_first_dim(opir_server *s, const uint64_t *fst_q
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (!fst_query || !out) throw std::invalid_argument("null argument");
+    if (s->c4) {
+      DeviceGuard g(s->device);
+      return s->c4->evaluate_first_dim(fst_query, out);
+    }
     if (!s->db_loaded) throw std::runtime_error("evaluate_first_dim before load_data");
     const opir::Shape &sh = s->shape;
     check_query_values(s, fst_query, static_cast<size_t>(sh.n0) * 2 * kN);
@@ -988,6 +1013,12 @@ opir_status opir_server_evaluate_other_dim(opir_server *s, const uint64_t *mid,
                                            const uint64_t *selectors, uint64_t *out) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
+    if (s->c4) {
+      const uint32_t nsel = s->params.num_dims - 1;
+      if (!mid || !out || (nsel && !selectors)) throw std::invalid_argument("null argument");
+      DeviceGuard g(s->device);
+      return s->c4->evaluate_other_dim(mid, selectors, out);
+    }
     const opir::Shape &sh = s->shape;
     const uint32_t nsel = sh.num_dims - 1;
     if (!mid || !out || (nsel && !selectors)) throw std::invalid_argument("null argument");

@@ -5,7 +5,9 @@ Names, argument meaning and error behaviour follow the reference
 (src/includes/pir.h, src/includes/server.h): invalid layouts and inputs raise
 ValueError (std::invalid_argument), unknown clients raise KeyError-compatible
 IndexError subclass OutOfRange (std::out_of_range), device failures raise
-RuntimeError. Ciphertexts are numpy uint64 arrays shaped (2, N) = (c0, c1).
+RuntimeError. Ciphertexts are numpy uint64 arrays shaped (2, N) = (c0, c1)
+under CONFIG_N2048_K1_COMP and (2, 2, N) = (poly, RNS limb, coefficient)
+under CONFIG_N4096_K2_MP; responses are (2, N) mod small_q under both.
 """
 from __future__ import annotations
 
@@ -51,20 +53,29 @@ def _ptr(a: np.ndarray, t=C.c_uint64):
     return a.ctypes.data_as(C.POINTER(t))
 
 
+CONFIGS = {"CONFIG_N2048_K1_COMP": 0, "CONFIG_N4096_K2_MP": 1}
+
+
 class PirParams:
-    """PirParams().with_layout({target_num_pt, expansion_height, fst_dim_pow2})."""
+    """PirParams().with_layout({target_num_pt, expansion_height, fst_dim_pow2})
+    under one ACTIVE_CONFIG (includes/database_constants.h:31-40):
+    "CONFIG_N2048_K1_COMP" (default) or "CONFIG_N4096_K2_MP"."""
 
     def __init__(self, target_num_pt: int = 43690, expansion_height: int = 10,
-                 fst_dim_pow2: bool = True):
+                 fst_dim_pow2: bool = True, config: str = "CONFIG_N2048_K1_COMP"):
+        if config not in CONFIGS:
+            raise ValueError(f"unknown parameter set {config!r}")
+        self.config = config
         self._layout = L.Layout(target_num_pt, expansion_height, 1 if fst_dim_pow2 else 0)
         self._p = L.Params()
-        rc = L.load().opir_params_init(C.byref(self._layout), C.byref(self._p))
+        rc = L.load().opir_params_init_config(CONFIGS[config], C.byref(self._layout),
+                                              C.byref(self._p))
         if rc != OPIR_OK:
             _raise(rc, f"invalid layout {target_num_pt}/{expansion_height}/{fst_dim_pow2}")
 
     def with_layout(self, target_num_pt: int, expansion_height: int,
                     fst_dim_pow2: bool = True) -> "PirParams":
-        return PirParams(target_num_pt, expansion_height, fst_dim_pow2)
+        return PirParams(target_num_pt, expansion_height, fst_dim_pow2, self.config)
 
     def __getattr__(self, name):
         p = self.__dict__.get("_p")
@@ -80,7 +91,8 @@ class PirParams:
     def get_expan_height(self): return self._p.expansion_height
     def get_plain_mod(self): return self._p.plain_mod
     def get_small_q(self): return self._p.small_q
-    def get_rns_mods(self): return [self._p.q]
+    def get_rns_mods(self):
+        return [self._p.q] if self._p.num_limbs == 1 else [self._p.q1, self._p.q2]
     def get_poly_degree(self): return self._p.poly_degree
     def get_l(self): return self._p.l_ep
     def get_l_key(self): return self._p.l_key
@@ -89,6 +101,12 @@ class PirParams:
     @property
     def N(self) -> int:
         return self._p.poly_degree
+
+    @property
+    def ct_shape(self) -> tuple:
+        """Shape of one ciphertext: (2, N), or (2, K, N) with RNS limbs."""
+        N = self._p.poly_degree
+        return (2, N) if self._p.num_limbs == 1 else (2, self._p.num_limbs, N)
 
     @property
     def useful(self) -> int:
@@ -199,8 +217,8 @@ class PirServer:
     # ---- query path
     def make_query(self, client_id: int, query: np.ndarray) -> np.ndarray:
         q = np.ascontiguousarray(query, dtype=np.uint64)
-        if q.shape != (2, self.params.N):
-            raise ValueError("query must be (2, N)")
+        if q.shape != self.params.ct_shape:
+            raise ValueError(f"query must be {self.params.ct_shape}")
         out = np.zeros((2, self.params.N), dtype=np.uint64)
         self._check(self._lib.opir_server_make_query(self._h, client_id, _ptr(q), _ptr(out)))
         return out
@@ -212,11 +230,12 @@ class PirServer:
         ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
         q = np.ascontiguousarray(queries, dtype=np.uint64)
         n = ids.size
-        if q.shape != (n, 2, self.params.N):
-            raise ValueError("queries must be (n, 2, N)")
+        if q.shape != (n,) + self.params.ct_shape:
+            raise ValueError(f"queries must be (n,) + {self.params.ct_shape}")
+        shape = (n, 2, self.params.N)
         if out is None:
-            out = np.zeros_like(q)
-        elif out.shape != q.shape or out.dtype != np.uint64 or not out.flags["C_CONTIGUOUS"]:
+            out = np.zeros(shape, dtype=np.uint64)
+        elif out.shape != shape or out.dtype != np.uint64 or not out.flags["C_CONTIGUOUS"]:
             raise ValueError("out must be a contiguous (n, 2, N) uint64 array")
         self._check(self._lib.opir_server_make_query_batch(self._h, n, _ptr(ids), _ptr(q), _ptr(out)))
         return out
@@ -263,30 +282,39 @@ class PirServer:
     # ---- individual stages (public PirServer methods)
     def expand_query(self, client_id: int, query: np.ndarray) -> np.ndarray:
         q = np.ascontiguousarray(query, dtype=np.uint64)
-        out = np.zeros((self.params.useful, 2, self.params.N), dtype=np.uint64)
+        if q.shape != self.params.ct_shape:
+            raise ValueError(f"query must be {self.params.ct_shape}")
+        out = np.zeros((self.params.useful,) + self.params.ct_shape, dtype=np.uint64)
         self._check(self._lib.opir_server_expand_query(self._h, client_id, _ptr(q), _ptr(out)))
         return out
 
     def complete_selectors(self, client_id: int, expanded: np.ndarray) -> np.ndarray:
         p = self.params
         e = np.ascontiguousarray(expanded, dtype=np.uint64)
-        out = np.zeros((max(p.num_dims - 1, 1), 2 * p.l_ep, 2, p.N), dtype=np.uint64)
+        if e.shape != (p.useful,) + p.ct_shape:
+            raise ValueError(f"expanded must be ({p.useful},) + {p.ct_shape}")
+        out = np.zeros((max(p.num_dims - 1, 1), 2 * p.l_ep) + p.ct_shape, dtype=np.uint64)
         self._check(self._lib.opir_server_complete_selectors(self._h, client_id, _ptr(e), _ptr(out)))
         return out[: p.num_dims - 1]
 
     def evaluate_first_dim(self, fst_query: np.ndarray) -> np.ndarray:
         p = self.params
         f = np.ascontiguousarray(fst_query[: p.fst_dim_sz], dtype=np.uint64)
-        out = np.zeros((p.other_dim_sz, 2, p.N), dtype=np.uint64)
+        if f.shape != (p.fst_dim_sz,) + p.ct_shape:
+            raise ValueError(f"fst_query must hold ({p.fst_dim_sz},) + {p.ct_shape}")
+        out = np.zeros((p.other_dim_sz,) + p.ct_shape, dtype=np.uint64)
         self._check(self._lib.opir_server_evaluate_first_dim(self._h, _ptr(f), _ptr(out)))
         return out
 
     def evaluate_other_dim(self, mid: np.ndarray, selectors: np.ndarray) -> np.ndarray:
+        p = self.params
         m = np.ascontiguousarray(mid, dtype=np.uint64)
+        if m.shape != (p.other_dim_sz,) + p.ct_shape:
+            raise ValueError(f"mid must be ({p.other_dim_sz},) + {p.ct_shape}")
         s = np.ascontiguousarray(selectors, dtype=np.uint64)
         if s.size == 0:
             s = np.zeros(1, dtype=np.uint64)
-        out = np.zeros((2, self.params.N), dtype=np.uint64)
+        out = np.zeros(p.ct_shape, dtype=np.uint64)
         self._check(self._lib.opir_server_evaluate_other_dim(self._h, _ptr(m), _ptr(s), _ptr(out)))
         return out
 

@@ -37,4 +37,6 @@ def stream(c):
 
 
 def sha256(arr) -> str:
+    if getattr(arr, "size", 1) == 0:   # memoryview cannot cast empty shapes
+        return hashlib.sha256(b"").hexdigest()
     return hashlib.sha256(memoryview(arr).cast("B")).hexdigest()
