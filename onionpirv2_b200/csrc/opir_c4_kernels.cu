@@ -423,24 +423,30 @@ k4_fst_ntt(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t leaf_
 
 // ------------------------------------------------------------ first-dim scan
 // Per limb and NTT level z: C[r][c] = sum_k A[r][k] Q[k][c] mod q_limb
-// (matrix.cpp:36-151). A warp owns a database row, its lanes split k and
-// keep 128-bit sums (folded every 64 terms, each term < 2^120), then a
-// modular shuffle tree. COLS query columns per CTA are staged in shared
-// memory; consecutive CTAs share z, so the column groups' re-reads of a
-// level's rows hit L2. Output cmat[column][row][z] (z contiguous for the
-// INTT that follows).
+// (matrix.cpp:36-151). A warp owns a database row and its lanes split k.
+// Operands are split into 30-bit halves, a = a1 2^30 + a0, so each term is
+// four 32x32->64 multiply-adds into 64-bit sums lo += a0 b0,
+// mid += a0 b1 + a1 b0, hi += a1 b1 (products < 2^60: eight terms cannot
+// overflow); every 8 terms lo + mid 2^30 + hi 2^60 (< 2^125) is reduced mod
+// q and added to the running residue. A modular shuffle tree ends the row.
+// COLS query columns per CTA sit in shared memory as (b0, b1) pairs;
+// consecutive CTAs share z, so column groups re-read a level's rows from
+// L2. Output cmat[column][row][z] (z contiguous for the INTT that follows).
 constexpr int kScanThreads = 256;
+constexpr int kScanFold = 8;   // terms per 64-bit partial sum
 
 template <int L, int COLS>
 __device__ __forceinline__ void scan_body(const uint64_t *db, const uint64_t *qm, uint32_t n0,
                                           uint32_t other, uint32_t ncols, uint64_t *cmat) {
-  extern __shared__ uint64_t qs[];  // [COLS][n0]
+  extern __shared__ uint2 qh[];  // [COLS][n0] (b0, b1)
   constexpr uint64_t Q = Limb<L>::q;
+  constexpr uint32_t M30 = (1u << 30) - 1;
   const uint32_t z = blockIdx.y;     // L N + level
   const uint32_t c0 = blockIdx.x * COLS;
   for (uint32_t idx = threadIdx.x; idx < n0 * COLS; idx += kScanThreads) {
     const uint32_t c = idx / n0, k = idx % n0;
-    qs[idx] = c0 + c < ncols ? qm[(static_cast<uint64_t>(z) * n0 + k) * ncols + c0 + c] : 0;
+    const uint64_t b = c0 + c < ncols ? qm[(static_cast<uint64_t>(z) * n0 + k) * ncols + c0 + c] : 0;
+    qh[idx] = make_uint2(static_cast<uint32_t>(b) & M30, static_cast<uint32_t>(b >> 30));
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -448,23 +454,43 @@ __device__ __forceinline__ void scan_body(const uint64_t *db, const uint64_t *qm
   for (uint32_t r = warp; r < other; r += kScanThreads / 32) {
     const uint64_t *Ar = A + static_cast<uint64_t>(r) * n0;
     uint64_t part[COLS];
-    u128 acc[COLS];
 #pragma unroll
-    for (int c = 0; c < COLS; ++c) { part[c] = 0; acc[c] = 0; }
-    int terms = 0;
-    for (uint32_t k = lane; k < n0; k += 32) {
-      const uint64_t a = __ldg(Ar + k);
+    for (int c = 0; c < COLS; ++c) part[c] = 0;
+    for (uint32_t k0 = lane; k0 < n0; k0 += 32 * kScanFold) {
+      uint64_t av[kScanFold];
 #pragma unroll
-      for (int c = 0; c < COLS; ++c) acc[c] += static_cast<u128>(a) * qs[c * n0 + k];
-      if (++terms == 64) {
+      for (int i = 0; i < kScanFold; ++i) {
+        const uint32_t k = k0 + 32 * i;
+        av[i] = k < n0 ? __ldg(Ar + k) : 0;
+      }
+      uint64_t lo[COLS], mid[COLS], hi[COLS];
 #pragma unroll
-        for (int c = 0; c < COLS; ++c) { part[c] = add_mod<Q>(part[c], red128<Q>(acc[c])); acc[c] = 0; }
-        terms = 0;
+      for (int c = 0; c < COLS; ++c) lo[c] = mid[c] = hi[c] = 0;
+#pragma unroll
+      for (int i = 0; i < kScanFold; ++i) {
+        const uint32_t k = k0 + 32 * i;
+        if (k >= n0) break;
+        const uint32_t a0 = static_cast<uint32_t>(av[i]) & M30;
+        const uint32_t a1 = static_cast<uint32_t>(av[i] >> 30);
+#pragma unroll
+        for (int c = 0; c < COLS; ++c) {
+          const uint2 b = qh[c * n0 + k];
+          lo[c] += static_cast<uint64_t>(a0) * b.x;
+          mid[c] += static_cast<uint64_t>(a0) * b.y;
+          mid[c] += static_cast<uint64_t>(a1) * b.x;
+          hi[c] += static_cast<uint64_t>(a1) * b.y;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < COLS; ++c) {
+        const u128 t = static_cast<u128>(lo[c]) + (static_cast<u128>(mid[c]) << 30) +
+                       (static_cast<u128>(hi[c]) << 60);
+        part[c] = add_mod<Q>(part[c], red128<Q>(t));
       }
     }
 #pragma unroll
     for (int c = 0; c < COLS; ++c) {
-      uint64_t v = add_mod<Q>(part[c], red128<Q>(acc[c]));
+      uint64_t v = part[c];
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) v = add_mod<Q>(v, __shfl_xor_sync(0xffffffffu, v, off));
       if (lane == c && c0 + c < ncols)
@@ -737,23 +763,26 @@ void launch_fst_ntt(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint
   check_launch("k4_fst_ntt");
 }
 
+template <int C>
+void launch_scan_cols(const Shape4 &s, const uint64_t *db, const uint64_t *qm, uint64_t *cmat,
+                      uint32_t ncols, cudaStream_t st) {
+  const size_t smem = static_cast<size_t>(C) * s.n0 * sizeof(uint2);
+  set_smem(k4_scan<C>, smem);
+  dim3 grid((ncols + C - 1) / C, 2 * kN);
+  k4_scan<C><<<grid, kScanThreads, smem, st>>>(db, qm, s.n0, s.other, ncols, cmat);
+}
+
 void launch_scan(const Shape4 &s, const uint64_t *db, const uint64_t *qm, uint64_t *cmat,
                  uint32_t batch, cudaStream_t st) {
   const uint32_t ncols = 2 * batch;
-  // 8 staged columns up to n0 = 2560 (160 KB), 4 above (n0 < 2^12: 128 KB)
-  if (s.n0 <= 2560) {
-    constexpr int C = 8;
-    const size_t smem = static_cast<size_t>(C) * s.n0 * sizeof(uint64_t);
-    set_smem(k4_scan<C>, smem);
-    dim3 grid((ncols + C - 1) / C, 2 * kN);
-    k4_scan<C><<<grid, kScanThreads, smem, st>>>(db, qm, s.n0, s.other, ncols, cmat);
-  } else {
-    constexpr int C = 4;
-    const size_t smem = static_cast<size_t>(C) * s.n0 * sizeof(uint64_t);
-    set_smem(k4_scan<C>, smem);
-    dim3 grid((ncols + C - 1) / C, 2 * kN);
-    k4_scan<C><<<grid, kScanThreads, smem, st>>>(db, qm, s.n0, s.other, ncols, cmat);
-  }
+  // columns per CTA: the batch's own count up to 8 (n0 < 2^12: at most
+  // 8 x 4096 x 8 B = 256 KB would not fit, so 4 above n0 = 3584)
+  if (ncols <= 2)
+    launch_scan_cols<2>(s, db, qm, cmat, ncols, st);
+  else if (ncols <= 4 || s.n0 > 3584)
+    launch_scan_cols<4>(s, db, qm, cmat, ncols, st);
+  else
+    launch_scan_cols<8>(s, db, qm, cmat, ncols, st);
   check_launch("k4_scan");
 }
 
