@@ -88,13 +88,19 @@ __device__ __forceinline__ uint64_t field(u128 u, int i) {
 }
 
 // ------------------------------------------------------------ DB preprocessing
+// server.cpp:80-203 per limb: pt mod q_k, NTT, transpose into the
+// coefficient-major layout -- here as eight byte planes per NTT level,
+// db8[(z 8 + plane)][row][n0p] (z = limb N + level), the tensor-core scan's
+// A operand. A CTA transforms 4 consecutive plaintexts; when they are 4
+// consecutive columns of one row their bytes go out as one 32-bit store.
 constexpr int kDbTile = 4;  // plaintexts per CTA (one padded plane each)
 
 template <int L>
 __device__ __forceinline__ void db_body(const Dev4 &P, const uint64_t *coeffs,
                                         uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
-                                        uint64_t logical, uint32_t n0, uint32_t other,
-                                        uint64_t pt_begin, uint64_t pt_end, uint64_t *db) {
+                                        uint64_t logical, uint32_t n0, uint32_t n0p,
+                                        uint32_t other, uint64_t pt_begin, uint64_t pt_end,
+                                        uint8_t *db8) {
   extern __shared__ uint64_t sm4[];
   const int tid = threadIdx.x;
   const uint64_t pt0 = pt_begin + static_cast<uint64_t>(blockIdx.x) * kDbTile;
@@ -116,29 +122,57 @@ __device__ __forceinline__ void db_body(const Dev4 &P, const uint64_t *coeffs,
   fwd_mid<L>(sm4, kDbTile, P.T);
   ulonglong2 wd[7];
   fload_d<L>(wd, P.T);
+  uint64_t out[kDbTile][8];
+#pragma unroll
   for (int e = 0; e < kDbTile; ++e) {
-    const uint64_t pt = pt0 + e;
-    uint64_t v[8];
-    ld_plane<3>(sm4 + e * kPad, v, tid);
-    fD<L>(v, wd);
-    if (pt >= pt_end) continue;
-    const uint64_t row = pt / n0, col = pt % n0;
+    ld_plane<3>(sm4 + e * kPad, out[e], tid);
+    fD<L>(out[e], wd);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) out[e][k] = canon8<Limb<L>::q>(out[e][k]);
+  }
+  const uint64_t row = pt0 / n0, col = pt0 % n0;
+  const uint64_t plane_bytes = static_cast<uint64_t>(other) * n0p;
+  // 4 plaintexts in one row from a column that is a multiple of 4: the
+  // address (n0p and every plane size are multiples of 16) is 4-byte aligned
+  if (pt0 + kDbTile <= pt_end && col + kDbTile <= n0 && (col & 3) == 0) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
-      db[(z * other + row) * n0 + col] = canon8<Limb<L>::q>(v[k]);
+      uint8_t *dst = db8 + z * 8 * plane_bytes + row * n0p + col;
+#pragma unroll
+      for (int pl = 0; pl < 8; ++pl) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int e = 0; e < kDbTile; ++e)
+          w |= static_cast<uint32_t>((out[e][k] >> (8 * pl)) & 0xFF) << (8 * e);
+        *reinterpret_cast<uint32_t *>(dst + pl * plane_bytes) = w;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < kDbTile; ++e) {
+      const uint64_t pt = pt0 + e;
+      if (pt >= pt_end) break;
+      const uint64_t r = pt / n0, c = pt % n0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
+        uint8_t *dst = db8 + z * 8 * plane_bytes + r * n0p + c;
+#pragma unroll
+        for (int pl = 0; pl < 8; ++pl) dst[pl * plane_bytes] = static_cast<uint8_t>(out[e][k] >> (8 * pl));
+      }
     }
   }
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
 k4_db_preprocess(Dev4 P, const uint64_t *__restrict__ coeffs, uint64_t coeff_pt_begin,
-                 uint64_t seed, uint64_t t, uint64_t logical, uint32_t n0, uint32_t other,
-                 uint64_t pt_begin, uint64_t pt_end, uint64_t *__restrict__ db) {
+                 uint64_t seed, uint64_t t, uint64_t logical, uint32_t n0, uint32_t n0p,
+                 uint32_t other, uint64_t pt_begin, uint64_t pt_end, uint8_t *__restrict__ db8) {
   if (blockIdx.y == 0)
-    db_body<0>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, other, pt_begin, pt_end, db);
+    db_body<0>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin, pt_end, db8);
   else
-    db_body<1>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, other, pt_begin, pt_end, db);
+    db_body<1>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin, pt_end, db8);
 }
 
 // ------------------------------------------------------------ expansion level
@@ -372,8 +406,9 @@ k4_selectors(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t lea
 }
 
 // ------------------------------------------------------------ first-dim query
-// Forward NTT per limb of the first n0 leaves (server.cpp:205-262) into the
-// scan's query matrix qm[z = limb N + level][k][column], column = 2 b + poly.
+// Forward NTT per limb of the first n0 leaves (server.cpp:205-262) into
+// qm[z][col][k] (col = 2 query + poly, k < n0), then k4_fst_pack splits it
+// into the scan's eight byte planes qb[(z 8 + plane)][col][n0p].
 constexpr int kFstTile = 2;  // leaves per CTA (4 planes)
 
 template <int L>
@@ -407,7 +442,7 @@ __device__ __forceinline__ void fst_body(const Dev4 &P, const Shape4 &S, const u
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
-      qm[(z * S.n0 + kk) * ncols + 2 * b + p] = canon8<Limb<L>::q>(v[k]);
+      qm[(z * ncols + 2 * b + p) * S.n0 + kk] = canon8<Limb<L>::q>(v[k]);
     }
   }
 }
@@ -421,119 +456,66 @@ k4_fst_ntt(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t leaf_
     fst_body<1>(P, S, leaves, leaf_stride, qm, ncols);
 }
 
-// ------------------------------------------------------------ first-dim scan
-// Per limb and NTT level z: C[r][c] = sum_k A[r][k] Q[k][c] mod q_limb
-// (matrix.cpp:36-151). A warp owns a database row and its lanes split k.
-// Operands are split into 30-bit halves, a = a1 2^30 + a0, so each term is
-// four 32x32->64 multiply-adds into 64-bit sums lo += a0 b0,
-// mid += a0 b1 + a1 b0, hi += a1 b1 (products < 2^60: eight terms cannot
-// overflow); every 8 terms lo + mid 2^30 + hi 2^60 (< 2^125) is reduced mod
-// q and added to the running residue. A modular shuffle tree ends the row.
-// COLS query columns per CTA sit in shared memory as (b0, b1) pairs;
-// consecutive CTAs share z, so column groups re-read a level's rows from
-// L2. Output cmat[column][row][z] (z contiguous for the INTT that follows).
-constexpr int kScanThreads = 256;
-constexpr int kScanFold = 8;   // terms per 64-bit partial sum
-
-template <int L, int COLS>
-__device__ __forceinline__ void scan_body(const uint64_t *db, const uint64_t *qm, uint32_t n0,
-                                          uint32_t other, uint32_t ncols, uint64_t *cmat) {
-  extern __shared__ uint2 qh[];  // [COLS][n0] (b0, b1)
-  constexpr uint64_t Q = Limb<L>::q;
-  constexpr uint32_t M30 = (1u << 30) - 1;
-  const uint32_t z = blockIdx.y;     // L N + level
-  const uint32_t c0 = blockIdx.x * COLS;
-  for (uint32_t idx = threadIdx.x; idx < n0 * COLS; idx += kScanThreads) {
-    const uint32_t c = idx / n0, k = idx % n0;
-    const uint64_t b = c0 + c < ncols ? qm[(static_cast<uint64_t>(z) * n0 + k) * ncols + c0 + c] : 0;
-    qh[idx] = make_uint2(static_cast<uint32_t>(b) & M30, static_cast<uint32_t>(b >> 30));
+// One thread per (z, col, 16 consecutive k): 128 contiguous bytes in, one
+// 16-byte store per plane out; k in [n0, n0p) reads as zero.
+__global__ void __launch_bounds__(256)
+k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t ncols,
+            uint8_t *__restrict__ qb) {
+  const uint32_t chunks = n0p / 16;
+  const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t total = static_cast<uint64_t>(2 * kN) * ncols * chunks;
+  if (idx >= total) return;
+  const uint32_t chunk = static_cast<uint32_t>(idx % chunks);
+  const uint64_t zc = idx / chunks;  // z ncols + col
+  const uint64_t z = zc / ncols, col = zc % ncols;
+  const uint64_t *src = qm + zc * n0;
+  uint32_t w[8][4];
+#pragma unroll
+  for (int pl = 0; pl < 8; ++pl)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[pl][j] = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const uint32_t k = chunk * 16 + i;
+    const uint64_t v = k < n0 ? src[k] : 0;
+#pragma unroll
+    for (int pl = 0; pl < 8; ++pl)
+      w[pl][i >> 2] |= static_cast<uint32_t>((v >> (8 * pl)) & 0xFF) << (8 * (i & 3));
   }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint64_t *A = db + static_cast<uint64_t>(z) * other * n0;
-  for (uint32_t r = warp; r < other; r += kScanThreads / 32) {
-    const uint64_t *Ar = A + static_cast<uint64_t>(r) * n0;
-    uint64_t part[COLS];
+  const uint64_t plane_bytes = static_cast<uint64_t>(ncols) * n0p;
+  uint8_t *dst = qb + z * 8 * plane_bytes + col * n0p + chunk * 16;
 #pragma unroll
-    for (int c = 0; c < COLS; ++c) part[c] = 0;
-    for (uint32_t k0 = lane; k0 < n0; k0 += 32 * kScanFold) {
-      uint64_t av[kScanFold];
-#pragma unroll
-      for (int i = 0; i < kScanFold; ++i) {
-        const uint32_t k = k0 + 32 * i;
-        av[i] = k < n0 ? __ldg(Ar + k) : 0;
-      }
-      uint64_t lo[COLS], mid[COLS], hi[COLS];
-#pragma unroll
-      for (int c = 0; c < COLS; ++c) lo[c] = mid[c] = hi[c] = 0;
-#pragma unroll
-      for (int i = 0; i < kScanFold; ++i) {
-        const uint32_t k = k0 + 32 * i;
-        if (k >= n0) break;
-        const uint32_t a0 = static_cast<uint32_t>(av[i]) & M30;
-        const uint32_t a1 = static_cast<uint32_t>(av[i] >> 30);
-#pragma unroll
-        for (int c = 0; c < COLS; ++c) {
-          const uint2 b = qh[c * n0 + k];
-          lo[c] += static_cast<uint64_t>(a0) * b.x;
-          mid[c] += static_cast<uint64_t>(a0) * b.y;
-          mid[c] += static_cast<uint64_t>(a1) * b.x;
-          hi[c] += static_cast<uint64_t>(a1) * b.y;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < COLS; ++c) {
-        const u128 t = static_cast<u128>(lo[c]) + (static_cast<u128>(mid[c]) << 30) +
-                       (static_cast<u128>(hi[c]) << 60);
-        part[c] = add_mod<Q>(part[c], red128<Q>(t));
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < COLS; ++c) {
-      uint64_t v = part[c];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v = add_mod<Q>(v, __shfl_xor_sync(0xffffffffu, v, off));
-      if (lane == c && c0 + c < ncols)
-        cmat[(static_cast<uint64_t>(c0 + c) * other + r) * (2 * kN) + z] = v;
-    }
-  }
-}
-
-template <int COLS>
-__global__ void __launch_bounds__(kScanThreads)
-k4_scan(const uint64_t *__restrict__ db, const uint64_t *__restrict__ qm, uint32_t n0,
-        uint32_t other, uint32_t ncols, uint64_t *__restrict__ cmat) {
-  if (blockIdx.y < kN)
-    scan_body<0, COLS>(db, qm, n0, other, ncols, cmat);
-  else
-    scan_body<1, COLS>(db, qm, n0, other, ncols, cmat);
+  for (int pl = 0; pl < 8; ++pl)
+    *reinterpret_cast<uint4 *>(dst + pl * plane_bytes) = make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
 }
 
 // ------------------------------------------------------------ scan epilogue
 // inter_to_cts (server.cpp:405-527): INTT per limb of every candidate. A CTA
-// transforms 4 rows of one column and one limb.
+// transforms 4 consecutive rows of one column and one limb, reading the
+// scan's cmat[z][col][row] as 32-byte row groups.
 constexpr int kEpiRows = 4;
 
 template <int L>
 __device__ __forceinline__ void epi_body(const Dev4 &P, const Shape4 &S, const uint64_t *cmat,
-                                         uint64_t *mid, uint64_t mid_stride) {
+                                         uint32_t ncols, uint64_t *mid, uint64_t mid_stride) {
   extern __shared__ uint64_t sm4[];
   const int tid = threadIdx.x;
   const uint32_t r0 = blockIdx.x * kEpiRows, c = blockIdx.z;
   {
+    uint64_t v[kEpiRows][8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
+      const uint64_t *src = cmat + (z * ncols + c) * S.other + r0;
+#pragma unroll
+      for (int e = 0; e < kEpiRows; ++e) v[e][k] = r0 + e < S.other ? src[e] : 0;
+    }
     ulonglong2 wd[7];
     iload_d<L>(wd, P.T);
-    for (int e = 0; e < kEpiRows; ++e) {
-      const uint32_t r = r0 + e;
-      uint64_t v[8];
-      if (r < S.other) {
-        ld8(cmat + (static_cast<uint64_t>(c) * S.other + r) * (2 * kN) + L * kN + 8 * tid, v);
-      } else {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = 0;
-      }
-      iD<L>(v, wd);
-      st_plane<3>(sm4 + e * kPad, v, tid);
+    for (int e = 0; e < kEpiRows; ++e) {
+      iD<L>(v[e], wd);
+      st_plane<3>(sm4 + e * kPad, v[e], tid);
     }
   }
   __syncthreads();
@@ -552,12 +534,12 @@ __device__ __forceinline__ void epi_body(const Dev4 &P, const Shape4 &S, const u
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
-k4_epilogue(Dev4 P, Shape4 S, const uint64_t *__restrict__ cmat, uint64_t *__restrict__ mid,
-            uint64_t mid_stride) {
+k4_epilogue(Dev4 P, Shape4 S, const uint64_t *__restrict__ cmat, uint32_t ncols,
+            uint64_t *__restrict__ mid, uint64_t mid_stride) {
   if (blockIdx.y == 0)
-    epi_body<0>(P, S, cmat, mid, mid_stride);
+    epi_body<0>(P, S, cmat, ncols, mid, mid_stride);
   else
-    epi_body<1>(P, S, cmat, mid, mid_stride);
+    epi_body<1>(P, S, cmat, ncols, mid, mid_stride);
 }
 
 // ------------------------------------------------------------ MUX level
@@ -676,6 +658,7 @@ k4_modswitch(Dev4 P, const uint64_t *__restrict__ ct_all, uint64_t ct_stride,
 
 // ============================================================== launchers
 uint64_t launch_count() { return g_launches4.load(std::memory_order_relaxed); }
+void note_launch() { g_launches4.fetch_add(1, std::memory_order_relaxed); }
 
 void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2],
                       const uint64_t *const iw[2], const uint64_t *const iw_sh[2],
@@ -706,13 +689,14 @@ void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2
 
 void launch_db_preprocess(const Dev4 &P, const Shape4 &s, const uint64_t *coeffs,
                           uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
-                          uint64_t pt_begin, uint64_t pt_end, uint64_t *db, cudaStream_t st) {
+                          uint64_t pt_begin, uint64_t pt_end, uint8_t *db8, cudaStream_t st) {
+  if (pt_begin % kDbTile != 0) throw std::invalid_argument("db tiles start at a multiple of 4");
   const size_t smem = plane_bytes(kDbTile);
   set_smem(k4_db_preprocess, smem);
   const uint64_t tiles = (pt_end - pt_begin + kDbTile - 1) / kDbTile;
   dim3 grid(static_cast<unsigned>(tiles), 2);
   k4_db_preprocess<<<grid, kThreads, smem, st>>>(P, coeffs, coeff_pt_begin, seed, t, logical, s.n0,
-                                                   s.other, pt_begin, pt_end, db);
+                                                   s.n0p, s.other, pt_begin, pt_end, db8);
   check_launch("k4_db_preprocess");
 }
 
@@ -763,27 +747,13 @@ void launch_fst_ntt(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint
   check_launch("k4_fst_ntt");
 }
 
-template <int C>
-void launch_scan_cols(const Shape4 &s, const uint64_t *db, const uint64_t *qm, uint64_t *cmat,
-                      uint32_t ncols, cudaStream_t st) {
-  const size_t smem = static_cast<size_t>(C) * s.n0 * sizeof(uint2);
-  set_smem(k4_scan<C>, smem);
-  dim3 grid((ncols + C - 1) / C, 2 * kN);
-  k4_scan<C><<<grid, kScanThreads, smem, st>>>(db, qm, s.n0, s.other, ncols, cmat);
-}
-
-void launch_scan(const Shape4 &s, const uint64_t *db, const uint64_t *qm, uint64_t *cmat,
-                 uint32_t batch, cudaStream_t st) {
+void launch_fst_pack(const Shape4 &s, const uint64_t *qm, uint8_t *qb, uint32_t batch,
+                     cudaStream_t st) {
   const uint32_t ncols = 2 * batch;
-  // columns per CTA: the batch's own count up to 8 (n0 < 2^12: at most
-  // 8 x 4096 x 8 B = 256 KB would not fit, so 4 above n0 = 3584)
-  if (ncols <= 2)
-    launch_scan_cols<2>(s, db, qm, cmat, ncols, st);
-  else if (ncols <= 4 || s.n0 > 3584)
-    launch_scan_cols<4>(s, db, qm, cmat, ncols, st);
-  else
-    launch_scan_cols<8>(s, db, qm, cmat, ncols, st);
-  check_launch("k4_scan");
+  const uint64_t threads = static_cast<uint64_t>(2 * kN) * ncols * (s.n0p / 16);
+  const unsigned blocks = static_cast<unsigned>((threads + 255) / 256);
+  k4_fst_pack<<<blocks, 256, 0, st>>>(qm, s.n0, s.n0p, ncols, qb);
+  check_launch("k4_fst_pack");
 }
 
 void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint64_t *mid,
@@ -791,7 +761,7 @@ void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint6
   const size_t smem = plane_bytes(kEpiRows);
   set_smem(k4_epilogue, smem);
   dim3 grid((s.other + kEpiRows - 1) / kEpiRows, 2, 2 * batch);
-  k4_epilogue<<<grid, kThreads, smem, st>>>(P, s, cmat, mid, mid_stride);
+  k4_epilogue<<<grid, kThreads, smem, st>>>(P, s, cmat, 2 * batch, mid, mid_stride);
   check_launch("k4_epilogue");
 }
 

@@ -3,18 +3,22 @@
 // Device layouts (u64 words, canonical residues):
 //   ciphertext : [c0 limb0 (N)][c0 limb1 (N)][c1 limb0 (N)][c1 limb1 (N)]
 //                (rlwe.h:17-31 with K = 2), kCtWords = 4 N words
-//   database   : db[z][row][col], z = limb N + NTT level, the reference's
-//                db[level * num_pt + pt] with pt = row n0 + col
-//                (server.cpp:172-194)
+//   database   : db8[(z 8 + plane)][row][n0p] bytes, z = limb N + NTT level:
+//                byte `plane` of the reference's db[level * num_pt + pt],
+//                pt = row n0 + col (server.cpp:172-194), rows padded to
+//                n0p = n0 rounded up to 16
 //   BV keys    : per client [level < h][row < L_KS][b (2N)][a (2N)], NTT form
 //   RGSW key   : per client [row < 2 L_KEY][c0 (2N)][c1 (2N)], NTT form
 //   selectors  : [query][dim < num_dims-1][row < 2 L_EP][ct], NTT form
-//   query mat  : qm[z][k < n0][col < 2 B], col = 2 query + poly
-//   cmat       : [col][row][z]
+//   query mat  : qm[z][col < 2 B][k < n0] u64, col = 2 query + poly, then
+//                qb[(z 8 + plane)][col][n0p] bytes
+//   cmat       : [z][col][row] u64
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 namespace opir4 {
@@ -37,11 +41,12 @@ struct Dev4 {
 };
 
 struct Shape4 {
-  uint32_t n0, other, num_dims, h, useful, l_ep;
+  uint32_t n0, n0p, other, num_dims, h, useful, l_ep;
   uint64_t num_pt;
 };
 
 uint64_t launch_count();
+void note_launch();  // counts a launch made outside opir_c4_kernels.cu
 
 void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2],
                       const uint64_t *const iw[2], const uint64_t *const iw_sh[2],
@@ -55,7 +60,7 @@ uint32_t expand_nodes(const Shape4 &s, uint32_t d);
 // generates coefficient(pt, c) = mix64(seed + (pt N + c + 1) golden) % t.
 void launch_db_preprocess(const Dev4 &P, const Shape4 &s, const uint64_t *coeffs,
                           uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
-                          uint64_t pt_begin, uint64_t pt_end, uint64_t *db, cudaStream_t st);
+                          uint64_t pt_begin, uint64_t pt_end, uint8_t *db8, cudaStream_t st);
 // One expansion level for `batch` queries; bv_keys: device array of per-query
 // key pointers.
 void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint64_t *in,
@@ -67,8 +72,8 @@ void launch_selectors(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, ui
                       cudaStream_t st);
 void launch_fst_ntt(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
                     uint64_t *qm, uint32_t batch, cudaStream_t st);
-void launch_scan(const Shape4 &s, const uint64_t *db, const uint64_t *qm, uint64_t *cmat,
-                 uint32_t batch, cudaStream_t st);
+void launch_fst_pack(const Shape4 &s, const uint64_t *qm, uint8_t *qb, uint32_t batch,
+                     cudaStream_t st);
 void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint64_t *mid,
                      uint64_t mid_stride, uint32_t batch, cudaStream_t st);
 void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, const uint64_t *in,
@@ -77,5 +82,23 @@ void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, const uint
 // Modulus switch + (optional) bit packing of `batch` results; resp: 2N u64 per query.
 void launch_modswitch(const Dev4 &P, const uint64_t *ct, uint64_t ct_stride, uint64_t *resp,
                       uint8_t *bytes, uint32_t resp_bytes, uint32_t batch, cudaStream_t st);
+
+// Tensor-core scan (opir_c4_scan_tc.cu): cmat = db8 . qb per z, mod q_limb.
+struct Tc4Args {
+  uint32_t k_tiles;    // ceil(n0p / 64)
+  uint32_t stages;     // pipeline stages (2 .. scan_tc4_max_stages)
+  uint32_t other;      // rows per level
+  uint32_t m_tiles;    // ceil(other / 128)
+  uint32_t ncols;      // output columns (2 x batch)
+  uint32_t ntile;      // columns per tile: 16 or 32
+  uint32_t col_tiles;  // ceil(ncols / ntile)
+  uint32_t zcount;     // 2 N (limbs x levels)
+  uint64_t *cmat;      // [z][col][row]
+  uint32_t *err;       // error bits (0 = ok)
+};
+size_t scan_tc4_smem(uint32_t ntile, uint32_t stages);
+uint32_t scan_tc4_max_stages(uint32_t ntile);
+void launch_scan_tc4(const CUtensorMap &mapA, const CUtensorMap &mapQ, const Tc4Args &args,
+                     int sm_count, cudaStream_t st);
 
 }  // namespace opir4

@@ -12,6 +12,7 @@
 #include <string>
 
 #include "opir_params.h"
+#include "opir_scan_tc.h"
 
 namespace opir4 {
 
@@ -29,6 +30,7 @@ uint32_t resp_bytes_of(const opir_params &p) {
 Shape4 shape_of(const opir_params &p) {
   Shape4 s{};
   s.n0 = static_cast<uint32_t>(p.fst_dim_sz);
+  s.n0p = static_cast<uint32_t>((p.fst_dim_sz + 15) / 16 * 16);
   s.other = static_cast<uint32_t>(p.other_dim_sz);
   s.num_dims = p.num_dims;
   s.h = p.expansion_height;
@@ -39,10 +41,11 @@ Shape4 shape_of(const opir_params &p) {
 }
 
 // Ciphertext slots per query of an expansion buffer: the widest tree level,
-// the useful leaves, and the candidate rows (the scan's output matrix reuses
-// the buffer that held the leaves).
+// the useful leaves, the padded first dimension and the candidate rows (the
+// first dimension's query matrix, its byte planes and the scan's output
+// reuse the two expansion buffers).
 uint64_t lvl_slots_of(const Shape4 &s) {
-  uint64_t slots = std::max<uint64_t>(1, std::max(s.useful, s.other));
+  uint64_t slots = std::max<uint64_t>(1, std::max({s.useful, s.other, s.n0p}));
   for (uint32_t d = 0; d < s.h; ++d) slots = std::max<uint64_t>(slots, 2ull * expand_nodes(s, d));
   return slots;
 }
@@ -98,9 +101,15 @@ Server::Server(const opir_params &p, cudaStream_t stream) : p_(p), st_(stream) {
   dp_.q0inv_sh = static_cast<uint64_t>((static_cast<unsigned __int128>(dp_.q0inv) << 64) / kQ1);
   dp_.small_q = p_.small_q;
   dp_.small_q_width = p_.small_q_width;
-  const uint64_t words = 2ull * kN * p_.num_pt;
-  db_.alloc(words);
-  ck(cudaMemsetAsync(db_.p, 0, words * 8, st_), "db memset");
+  const uint64_t db_bytes = 2ull * kN * 8 * sh_.other * sh_.n0p;
+  db8_.alloc(db_bytes);
+  ck(cudaMemsetAsync(db8_.p, 0, db_bytes, st_), "db memset");
+  opir::make_plane_map(&map_db_, db8_.p, sh_.n0p, sh_.other, 2ull * kN * 8, 128, 64);
+  err_.alloc(1);
+  ck(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), st_), "err memset");
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "device");
+  ck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev), "sm count");
   ck(cudaStreamSynchronize(st_), "create");
 }
 
@@ -130,7 +139,7 @@ void Server::load_tiles(uint64_t logical, Fill &&fill) {
       ck(cudaMemcpyAsync(dev.p, host.data(), (real_end - pb) * kN * 8, cudaMemcpyHostToDevice, st_),
          "db upload");
     }
-    launch_db_preprocess(dp_, sh_, dev.p, pb, 0, p_.plain_mod, logical, pb, pe, db_.p, st_);
+    launch_db_preprocess(dp_, sh_, dev.p, pb, 0, p_.plain_mod, logical, pb, pe, db8_.p, st_);
     ck(cudaStreamSynchronize(st_), "db preprocess");
   }
   db_loaded_ = true;
@@ -175,7 +184,7 @@ void Server::load_db_seeded(uint64_t logical, uint64_t seed) {
   const uint64_t chunk = 1ull << 18;
   for (uint64_t pb = 0; pb < p_.num_pt; pb += chunk)
     launch_db_preprocess(dp_, sh_, nullptr, 0, seed, p_.plain_mod, logical, pb,
-                         std::min<uint64_t>(p_.num_pt, pb + chunk), db_.p, st_);
+                         std::min<uint64_t>(p_.num_pt, pb + chunk), db8_.p, st_);
   ck(cudaStreamSynchronize(st_), "db preprocess");
   db_loaded_ = true;
 }
@@ -249,7 +258,8 @@ void Server::plan_memory(const opir_params &p, opir_memory_plan *out) {
   const Shape4 s = shape_of(p);
   const uint64_t slots = lvl_slots_of(s);
   const uint64_t one = plan_for(s, slots, 1).bytes(), two = plan_for(s, slots, 2).bytes();
-  out->database_bytes = 2ull * kN * p.num_pt * 8 + 4ull * kN * sizeof(ulonglong2);
+  out->database_bytes =
+      2ull * kN * 8 * s.other * s.n0p + 4ull * kN * sizeof(ulonglong2) + sizeof(uint32_t);
   out->client_key_bytes =
       (static_cast<uint64_t>(p.expansion_height) * kLKsRows + 2ull * kLKeyRows) * kCt * 8;
   out->scratch_bytes_per_query = two - one;
@@ -304,16 +314,50 @@ const uint64_t *Server::run_expand(uint32_t n) {
   return lvl_[sh_.h & 1].p;
 }
 
+// Tensor-core scan of n queries: 16 columns per tile up to 8 queries, else
+// 32 (column tiles of one row tile run on neighbouring CTAs, so the
+// database tile is read from HBM once).
+void Server::launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n) {
+  const uint32_t ncols = 2 * n;
+  Tc4Args a{};
+  a.ntile = ncols <= 16 ? 16 : 32;
+  a.stages = scan_tc4_max_stages(a.ntile);
+  a.k_tiles = (sh_.n0p + 63) / 64;
+  a.other = sh_.other;
+  a.m_tiles = (sh_.other + 127) / 128;
+  a.ncols = ncols;
+  a.col_tiles = (ncols + a.ntile - 1) / a.ntile;
+  a.zcount = 2 * kN;
+  a.cmat = cmat;
+  a.err = err_.p;
+  CUtensorMap map_q;
+  opir::make_plane_map(&map_q, qb, sh_.n0p, ncols, 2ull * kN * 8, a.ntile, 64);
+  launch_scan_tc4(map_db_, map_q, a, sm_count_, st_);
+}
+
+// Reads and clears the tensor-core scan's error word (stream must be idle).
+void Server::check_device_error() {
+  uint32_t e = 0;
+  ck(cudaMemcpy(&e, err_.p, sizeof(e), cudaMemcpyDeviceToHost), "error word");
+  if (e != 0) {
+    ck(cudaMemset(err_.p, 0, sizeof(e)), "error word");
+    throw std::runtime_error("tensor-core scan timed out (code " + std::to_string(e) + ")");
+  }
+}
+
 // First dimension: NTT of the first n0 leaves into the query matrix (in the
-// expansion buffer that does not hold the leaves), the scan (its output in
-// the leaves' buffer, dead by then), INTT into mid_[0].
+// expansion buffer that does not hold the leaves), its byte planes (in the
+// leaves' buffer, dead by then), the scan (its output back in the first
+// buffer), INTT into mid_[0].
 void Server::run_first_dim(const uint64_t *leaves, uint32_t n, const Mark &mark) {
   const int li = leaves == lvl_[0].p ? 0 : 1;
   uint64_t *qm = lvl_[li ^ 1].p;
-  uint64_t *cmat = lvl_[li].p;
+  uint8_t *qb = reinterpret_cast<uint8_t *>(lvl_[li].p);
+  uint64_t *cmat = lvl_[li ^ 1].p;
   launch_fst_ntt(dp_, sh_, leaves, lvl_slots_, qm, n, st_);
+  launch_fst_pack(sh_, qm, qb, n, st_);
   if (mark) mark(6);
-  launch_scan(sh_, db_.p, qm, cmat, n, st_);
+  launch_scan(qb, cmat, n);
   if (mark) mark(7);
   launch_epilogue(dp_, sh_, cmat, mid_[0].p, sh_.other, n, st_);
 }
@@ -358,6 +402,7 @@ void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *q
   ck(cudaMemcpyAsync(responses, resp_.p, static_cast<size_t>(n) * 2 * kN * 8,
                      cudaMemcpyDeviceToHost, st_), "response download");
   ck(cudaStreamSynchronize(st_), "make_query");
+  check_device_error();
 }
 
 void Server::make_query_batch_device(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
@@ -404,6 +449,7 @@ void Server::evaluate_first_dim(const uint64_t *fst_query, uint64_t *out) {
   ck(cudaMemcpyAsync(out, mid_[0].p, static_cast<size_t>(sh_.other) * kCt * 8,
                      cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "evaluate_first_dim");
+  check_device_error();
 }
 
 void Server::evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, uint64_t *out) {

@@ -75,6 +75,8 @@ class Server {
   const uint64_t *run_other_dims(uint32_t n);
   void run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
                     uint64_t *d_resp, const Mark &mark);
+  void launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n);
+  void check_device_error();
   template <typename Fill>
   void load_tiles(uint64_t logical, Fill &&fill);
 
@@ -83,7 +85,10 @@ class Server {
   Dev4 dp_{};
   cudaStream_t st_ = nullptr;
   opir::DevBuf<ulonglong2> tables_;
-  opir::DevBuf<uint64_t> db_;
+  opir::DevBuf<uint8_t> db8_;   // byte-plane database (opir_c4_kernels.h)
+  CUtensorMap map_db_{};        // TMA view of db8_ for the tensor-core scan
+  opir::DevBuf<uint32_t> err_;  // error word of the tensor-core scan
+  int sm_count_ = 148;
   bool db_loaded_ = false;
   std::unordered_map<uint64_t, Keys> clients_;
   uint32_t cap_ = 0;
