@@ -1,14 +1,17 @@
 """Benchmark of the B200 OnionPIRv2 server path (PirServer::make_query).
 
-Workload: k1_comp parameters (N = 2048, q = q1 q2 ~ 2^58, t = 4099), a
-2^18-plaintext database (872 MB of 13-bit coefficients; 4 GiB in NTT form on
-the device), first dimension 512 x 9 further binary dimensions. A step is one
+Workload (default, --workload k1): k1_comp parameters (N = 2048,
+q = q1 q2 ~ 2^58, t = 4099), a 2^18-plaintext database (872 MB of 13-bit
+coefficients; 4 GiB in NTT form on the device), first dimension 512 x 9
+further binary dimensions. --workload c4: CONFIG_N4096_K2_MP (N = 4096, two
+60-bit RNS limbs, t = generate_prime(40)), 2^20 plaintexts (64 GiB in NTT
+form), first dimension 1024 x 10 further binary dimensions. A step is one
 batch of B independent queries (each with its own client keys) answered by
 one pass of the path; the first-dimension scan reads the database once per
 batch. The database is larger than L2 (126 MB), so every step streams it from
 HBM; no L2 flush is needed.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--workload c4]
     python bench.py --impl reference ...      # the reference's CPU server
 
 N > 1 runs one rank per GPU (torchrun), each holding a replica of the
@@ -31,6 +34,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "queries/s and DB GB/s at 1 GB DB, batched vs plain GPU (bit-exact); p50/p99 ms"
 TARGET, HEIGHT = 262144, 10
+C4_TARGET, C4_HEIGHT = 1 << 20, 11
+C4_CONFIG = "CONFIG_N4096_K2_MP"
+# two timed layouts of the reference under CONFIG_N4096_K2_MP with the full
+# workload's first dimension (1024) and expansion height (11): 4 and 32
+# candidate rows
+C4_REF_LAYOUTS = (4096, 32768)
 DB_SEED = 20261203
 
 
@@ -43,16 +52,24 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-queries", type=int, default=3)
-    ap.add_argument("--target", type=int, default=TARGET,
+    ap.add_argument("--workload", choices=["k1", "c4"], default="k1",
+                    help="k1: CONFIG_N2048_K1_COMP at 2^18 plaintexts; c4: CONFIG_N4096_K2_MP at 2^20")
+    ap.add_argument("--target", type=int, default=None,
                     help="plaintexts (smaller layouts are for profiling captures)")
-    ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--height", type=int, default=None)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default scan tiling (or OPIR_SCAN_TILE)")
     ap.add_argument("--serve", action="store_true",
                     help="serving loop: Poisson arrivals over three resident databases")
     ap.add_argument("--rates", default="50,500,2000", help="offered queries/s (--serve)")
     ap.add_argument("--duration", type=float, default=3.0, help="seconds per rate (--serve)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    c4 = args.workload == "c4"
+    if args.target is None:
+        args.target = C4_TARGET if c4 else TARGET
+    if args.height is None:
+        args.height = C4_HEIGHT if c4 else HEIGHT
+    return args
 
 
 # ---------------------------------------------------------------- distributed
@@ -151,23 +168,33 @@ def ncu_traffic() -> dict | None:
 
 
 def synthetic_inputs(params, batch: int, seed: int):
-    """Seeded uniform ciphertexts and key material mod q. make_query's work
-    is data-independent, so uniform inputs time the same arithmetic as
-    genuine client queries (parity is proven by tests/)."""
-    N, q = params.N, params.q
+    """Seeded uniform ciphertexts and key material mod q (per RNS limb under
+    CONFIG_N4096_K2_MP). make_query's work is data-independent, so uniform
+    inputs time the same arithmetic as genuine client queries (parity is
+    proven by tests/)."""
+    shape = params.ct_shape
+    mods = np.array(params.get_rns_mods(), dtype=np.uint64)
     rng = np.random.default_rng(seed)
-    queries = rng.integers(0, q, (batch, 2, N), dtype=np.uint64)
+
+    def uniform(lead):
+        if len(mods) == 1:
+            return rng.integers(0, mods[0], tuple(lead) + shape, dtype=np.uint64)
+        a = rng.integers(0, np.iinfo(np.uint64).max, tuple(lead) + shape, dtype=np.uint64,
+                         endpoint=True)
+        return a % mods[:, None]     # limb axis is the second to last
+
+    queries = uniform((batch,))
     keys = []
     for b in range(batch):
-        bv = rng.integers(0, q, (params.expansion_height, params.l_ks, 2, N), dtype=np.uint64)
-        gsw = rng.integers(0, q, (2 * params.l_key, 2, N), dtype=np.uint64)
+        bv = uniform((params.expansion_height, params.l_ks))
+        gsw = uniform((2 * params.l_key,))
         keys.append((bv, gsw))
     return queries, keys
 
 
-def ref_binary() -> str | None:
+def ref_binary(suffix: str = "") -> str | None:
     d = os.path.join(ROOT, "oracle", "_ref")
-    fast, port = os.path.join(d, "opir_ref_avx512"), os.path.join(d, "opir_ref")
+    fast, port = os.path.join(d, f"opir_ref{suffix}_avx512"), os.path.join(d, f"opir_ref{suffix}")
     try:
         with open("/proc/cpuinfo") as f:
             flags = f.read()
@@ -191,6 +218,30 @@ def run_reference(queries: int, warmup: int, procs: int, seed: int) -> dict:
     return res
 
 
+def run_reference_c4(queries: int, procs: int, seed: int) -> dict:
+    """The reference built with CONFIG_N4096_K2_MP, timed at two layouts that
+    share the full workload's first dimension (1024) and expansion height
+    (11). Its make_query cost is affine in the candidate-row count (the scan
+    and the MUX tree grow with it; expansion and selectors barely change), so
+    the per-query time at 1024 rows (2^20 plaintexts, a 64 GiB database the
+    CPU server cannot load within a benchmark) is extrapolated from the two."""
+    exe = ref_binary("_c4")
+    if exe is None:
+        raise FileNotFoundError("oracle/_ref is not built")
+    runs = []
+    for tgt in C4_REF_LAYOUTS:
+        cmd = [exe, "--mode", "time", "--target", str(tgt), "--height", str(C4_HEIGHT),
+               "--db-seed", str(DB_SEED), "--client-seed", str(seed), "--queries", str(queries),
+               "--warmup", "0", "--procs", str(procs)]
+        out = subprocess.run(cmd, check=True, capture_output=True, text=True)
+        runs.append(json.loads(out.stdout.strip().splitlines()[-1]))
+    rows = [(t + 1023) // 1024 for t in C4_REF_LAYOUTS]
+    slope = (runs[1]["mean_ms"] - runs[0]["mean_ms"]) / (rows[1] - rows[0])
+    full_ms = runs[0]["mean_ms"] + slope * (C4_TARGET // 1024 - rows[0])
+    return {"mean_ms": full_ms, "qps": procs * 1000.0 / full_ms, "runs": runs, "rows": rows,
+            "binary": os.path.basename(exe), "queries": queries * procs}
+
+
 def cpu_model() -> str:
     try:
         with open("/proc/cpuinfo") as f:
@@ -207,6 +258,9 @@ def bench_reference(args, world, rank):
     if rank != 0:
         return
     procs = os.cpu_count() or 1
+    if args.workload == "c4":
+        bench_reference_c4(args, procs)
+        return
     # a bounded sample: at most 8 timed queries (and 1 warm-up) per process,
     # ~2 s each on one core, so the run ends within a few minutes
     n_q, n_w = min(args.steps, 8), min(args.warmup, 1)
@@ -233,6 +287,46 @@ def bench_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def c4_workload_name(params) -> str:
+    return (f"CONFIG_N4096_K2_MP N=4096 two 60-bit limbs, {params.num_pt} plaintexts "
+            f"({2 * params.N * params.num_pt * 8} B NTT form), first dim {params.fst_dim_sz} x "
+            f"{params.num_dims - 1} binary dims")
+
+
+def c4_sample(res: dict, cores: int) -> str:
+    a, b = res["runs"]
+    return (f"reference make_query (oracle/_ref/{res['binary']}, HEXL stand-in) under "
+            f"CONFIG_N4096_K2_MP on {cores} host process(es): {a['mean_ms']:.0f} ms/query at "
+            f"{C4_REF_LAYOUTS[0]} plaintexts ({res['rows'][0]} candidate rows) and "
+            f"{b['mean_ms']:.0f} ms at {C4_REF_LAYOUTS[1]} ({res['rows'][1]} rows), first dim 1024, "
+            f"h={C4_HEIGHT}, {res['queries']} queries per layout; per-query time at 1024 rows "
+            f"(2^20 plaintexts) extrapolated along the affine row dependence = "
+            f"{res['mean_ms']:.0f} ms; CPU {cpu_model()}")
+
+
+def bench_reference_c4(args, procs):
+    n_q = max(1, min(args.steps, 2))
+    try:
+        res = run_reference_c4(n_q, procs, 7)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU server: {e}"}))
+        return
+    qps = res["qps"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["mean_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"CONFIG_N4096_K2_MP N=4096, {C4_TARGET} plaintexts, first dim "
+                               f"1024 x 10 binary dims", "batch": 1,
+                   "parallelism": f"{procs} host processes"},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": procs, "kind": "reference",
+                         "sample": c4_sample(res, procs)},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
 # ---------------------------------------------------------------- our arm
 def bench_ours(args, world, rank, local):
     import torch
@@ -246,9 +340,12 @@ def bench_ours(args, world, rank, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=device)
-    params = PirParams(args.target, args.height)
+    c4 = args.workload == "c4"
+    params = (PirParams(args.target, args.height, config=C4_CONFIG) if c4
+              else PirParams(args.target, args.height))
     N = params.N
     B = args.batch
+    ct_words = int(np.prod(params.ct_shape))
     srv = PirServer(params, device=local)
     t0 = time.perf_counter()
     srv.load_data_seeded(args.target, DB_SEED)
@@ -266,7 +363,7 @@ def bench_ours(args, world, rank, local):
     # bracket the whole batch
     stream = torch.cuda.Stream(device)
     d_q = torch.from_numpy(queries.view(np.int64)).to(device)
-    d_r = torch.empty_like(d_q)
+    d_r = torch.empty((B, 2, N), dtype=torch.int64, device=device)
 
     def step(n, qbuf, rbuf):
         srv.make_query_batch_device(ids[:n], qbuf.data_ptr(), rbuf.data_ptr(), stream.cuda_stream)
@@ -315,7 +412,7 @@ def bench_ours(args, world, rank, local):
 
     # end to end through the host-buffer C ABI call (pinned host memory)
     hq = torch.from_numpy(queries.view(np.int64)).pin_memory()
-    hr = torch.empty_like(hq).pin_memory()
+    hr = torch.empty((B, 2, N), dtype=torch.int64).pin_memory()
     hq_np, hr_np = hq.numpy().view(np.uint64), hr.numpy().view(np.uint64)
     for _ in range(args.warmup):
         srv.make_query_batch(ids, hq_np, out=hr_np)
@@ -334,26 +431,32 @@ def bench_ours(args, world, rank, local):
         return
 
     peaks = measured_peaks()
-    db_phys = 2 * N * params.num_pt * 4
-    qmat_bytes = 2 * N * params.fst_dim_sz * 2 * B * 4
-    cmat_bytes = 2 * N * params.other_dim_sz * 2 * B * 4
+    word = 8 if c4 else 4            # bytes per stored residue (u64 limb / u32 half)
+    db_phys = 2 * N * params.num_pt * word
+    qmat_bytes = 2 * N * params.fst_dim_sz * 2 * B * word
+    cmat_bytes = 2 * N * params.other_dim_sz * 2 * B * word
     alg_bytes = db_phys + qmat_bytes + cmat_bytes
     core_ms = stages["Core"]
     achieved = alg_bytes / (core_ms / 1e3) / 1e9
     traffic = ncu_traffic()
-    logical_db = params.num_pt * N * 13 / 8
+    coeff_bits = 40 if c4 else 13    # t = generate_prime(40) / 4099
+    logical_db = params.num_pt * N * coeff_bits / 8
+    workload = (c4_workload_name(params) if c4 else
+                f"k1_comp N=2048, {args.target} plaintexts ({logical_db / 1e6:.1f} MB "
+                f"at 13 bits, {db_phys} B NTT form), first dim {params.fst_dim_sz} x "
+                f"{params.num_dims - 1} binary dims")
     line = {
         "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64" if c4 else "u32",
         "data": "synthetic (seeded DB coefficients < t generated on device; seeded uniform "
                 "ciphertexts and keys mod q -- the path is data-independent)",
-        "config": {"workload": f"k1_comp N=2048, {args.target} plaintexts ({logical_db / 1e6:.1f} MB "
-                               f"at 13 bits, {db_phys} B NTT form), first dim {params.fst_dim_sz} x "
-                               f"{params.num_dims - 1} binary dims",
+        "config": {"workload": workload,
                    "batch": B, "num_pt": params.num_pt, "fst_dim_sz": params.fst_dim_sz,
                    "num_dims": params.num_dims,
-                   "l2": "inputs larger than L2: the 4 GiB database streams from HBM every step",
+                   "l2": (f"inputs larger than L2: the {db_phys / 2**30:.0f} GiB database streams "
+                          "from HBM every step"),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "db_gbs": logical_db * queries_done / (total_max / 1e3) / 1e9,
         "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
@@ -363,20 +466,30 @@ def bench_ours(args, world, rank, local):
                                  "p99": float(np.percentile(plain_per, 99))},
                   "db_gbs": logical_db * world * args.steps / (plain_total / 1e3) / 1e9,
                   "stages_ms": {k: round(v, 4) for k, v in plain_stages.items() if k != "calls"}},
-        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * 2 * N * 8,
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * ct_words * 8,
                 "d2h_bytes_per_step": B * 2 * N * 8},
-        "roofline": {"bound": "hbm", "kernel": "k_scan (first-dimension scan)",
+        "roofline": {"bound": "hbm",
+                     "kernel": ("k4_scan_tc (first-dimension scan, tcgen05)" if c4
+                                else "k_scan (first-dimension scan)"),
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "algorithmic_bytes": alg_bytes,
-                     "traffic": (traffic or {}).get(f"batch_{B}")},
+                     "traffic": (traffic or {}).get(f"{'c4_' if c4 else ''}batch_{B}")},
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "setup": {"db_load_s": round(load_s, 3), "autotune_s": round(tune_s, 3),
                   "scan_tile": srv.scan_tile(B), "scan_tile_plain": srv.scan_tile(1),
                   "gpu": torch.cuda.get_device_name(device)},
     }
-    if world == 1 and not args.no_cpu_baseline and args.target == TARGET:
+    if world == 1 and not args.no_cpu_baseline and c4 and args.target == C4_TARGET:
+        try:
+            res = run_reference_c4(1, 1, 7)
+            line["cpu_baseline"] = {"value": 1000.0 / res["mean_ms"], "unit": "queries/s",
+                                    "cores": 1, "kind": "reference", "sample": c4_sample(res, 1)}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unit": "queries/s", "cores": 0,
+                                    "kind": "reference", "sample": f"unavailable: {e}"}
+    if world == 1 and not args.no_cpu_baseline and not c4 and args.target == TARGET:
         try:
             res = run_reference(args.cpu_queries, 0, 1, 7)
             line["cpu_baseline"] = {
