@@ -509,10 +509,10 @@ def bench_ours(args, world, rank, local):
 
 
 # ---------------------------------------------------------------- serving loop
-SERVE_DBS = [  # name, plaintexts, expansion height, share of arrivals, batch limit
-    ("c1_54MB", 16384, 9, 0.6, 32),
-    ("c2_872MB", 262144, 10, 0.3, 32),
-    ("k1_1M_3.5GB", 1 << 20, 11, 0.1, 16),
+SERVE_DBS = [  # name, plaintexts, expansion height, share of arrivals, batch limit, parameter set
+    ("c1_54MB", 16384, 9, 0.6, 32, "CONFIG_N2048_K1_COMP"),
+    ("c2_872MB", 262144, 10, 0.3, 32, "CONFIG_N2048_K1_COMP"),
+    ("c4_n4096_1M", 1 << 20, 11, 0.1, 16, C4_CONFIG),
 ]
 
 
@@ -533,8 +533,8 @@ def bench_serve(args, world, rank, local):
     n_clients = 16
     inputs = {}
     t0 = time.perf_counter()
-    for k, (name, target, h, _share, mb) in enumerate(SERVE_DBS):
-        params = PirParams(target, h)
+    for k, (name, target, h, _share, mb, cfg) in enumerate(SERVE_DBS):
+        params = PirParams(target, h, config=cfg)
         eng.add_database(name, params, max_batch=mb, seed=DB_SEED + k)
         queries, keys = synthetic_inputs(params, n_clients, 3000 + 100 * k + rank)
         for j, (bv, gsw) in enumerate(keys):
@@ -591,13 +591,14 @@ def bench_serve(args, world, rank, local):
         verified += 1
     line = {
         "metric": "serving: queries/s and p50/p99 ms under Poisson arrivals", "impl": "ours",
-        "unit": "queries/s", "n_gpus": 1, "dtype": "u32",
+        "unit": "queries/s", "n_gpus": 1, "dtype": "u32 (k1_comp) / u64 (two-limb)",
         "data": "synthetic (seeded DBs generated on device; seeded uniform ciphertexts and keys)",
-        "config": {"workload": "three resident k1_comp databases, arrivals mixed "
+        "config": {"workload": "three resident databases (k1_comp 2^14 and 2^18, "
+                               "CONFIG_N4096_K2_MP 2^20), arrivals mixed "
                                + "/".join(f"{int(100 * x)}" for x in shares),
-                   "databases": {nm: {"num_pt": PirParams(t, h).num_pt, "expansion_height": h,
-                                      "max_batch": mb}
-                                 for nm, t, h, _s, mb in SERVE_DBS},
+                   "databases": {nm: {"num_pt": PirParams(t, h, config=cfg).num_pt,
+                                      "expansion_height": h, "max_batch": mb, "params": cfg}
+                                 for nm, t, h, _s, mb, cfg in SERVE_DBS},
                    "depth": eng.depth, "clients_per_db": n_clients,
                    "duration_s_per_rate": args.duration},
         "levels": results,

@@ -60,16 +60,18 @@ class CudaLane:
             self.server.load_data_seeded(params.target_num_pt, 0 if seed is None else seed)
         self.server.reserve(max_batch)
         self.stream = torch.cuda.Stream(dev)
-        shape = (max_batch, 2, params.N)
-        self.d_q = [torch.empty(shape, dtype=torch.int64, device=dev) for _ in range(depth)]
-        self.d_r = [torch.empty(shape, dtype=torch.int64, device=dev) for _ in range(depth)]
-        self.h_q = [torch.empty(shape, dtype=torch.int64).pin_memory() for _ in range(depth)]
-        self.h_r = [torch.empty(shape, dtype=torch.int64).pin_memory() for _ in range(depth)]
+        qshape = (max_batch,) + params.ct_shape      # (2, N) or (2, K, N)
+        rshape = (max_batch, 2, params.N)            # responses mod small_q
+        self.d_q = [torch.empty(qshape, dtype=torch.int64, device=dev) for _ in range(depth)]
+        self.d_r = [torch.empty(rshape, dtype=torch.int64, device=dev) for _ in range(depth)]
+        self.h_q = [torch.empty(qshape, dtype=torch.int64).pin_memory() for _ in range(depth)]
+        self.h_r = [torch.empty(rshape, dtype=torch.int64).pin_memory() for _ in range(depth)]
         self.events = [None] * depth
 
     @staticmethod
     def buffer_bytes(params: PirParams, max_batch: int, depth: int) -> int:
-        return depth * 2 * max_batch * 2 * params.N * 8
+        per_query = (int(np.prod(params.ct_shape)) + 2 * params.N) * 8
+        return depth * max_batch * per_query
 
     def set_client_keys(self, client_id, bv_keys, gsw_key):
         self.server.set_client_keys(client_id, bv_keys, gsw_key)
@@ -213,8 +215,8 @@ class ServingEngine:
             fut.set_exception(IndexError(f"unknown client id {client_id}"))
             return fut
         q = np.ascontiguousarray(query, dtype=np.uint64)
-        if q.shape != (2, db.params.N):
-            fut.set_exception(ValueError("query must be (2, N)"))
+        if q.shape != db.params.ct_shape:
+            fut.set_exception(ValueError(f"query must be {db.params.ct_shape}"))
             return fut
         req = _Request(client_id, q, fut, time.perf_counter())
         with self._cv:

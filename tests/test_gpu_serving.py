@@ -105,3 +105,56 @@ def test_admission_refuses_over_budget_before_allocating():
     assert eng.reserved == 0 and not eng.dbs
     assert torch.cuda.mem_get_info()[0] >= before - (8 << 20)
     eng.close()
+
+
+def test_two_parameter_sets_share_one_engine():
+    """A CONFIG_N2048_K1_COMP and a CONFIG_N4096_K2_MP database served side
+    by side: every response equals the query answered alone and decrypts to
+    the requested plaintext; the two-limb golden query matches the reference."""
+    from onionpirv2_b200 import PirParams
+    from onionpirv2_b200.serving import ServingEngine
+
+    eng = ServingEngine(depth=2)
+    c1 = G.case("c1_16384_h9")
+    op1 = O.params(c1["target_num_pt"], c1["expansion_height"], c1["fst_dim_pow2"])
+    eng.add_database("k1", PirParams(c1["target_num_pt"], c1["expansion_height"]), max_batch=8,
+                     seed=c1["db_seed"], min_fill=2)
+    c4 = G.case_c4("c4_2048_h7")
+    op4 = O.c4_params(c4["target_num_pt"], c4["expansion_height"], c4["fst_dim_pow2"])
+    eng.add_database("c4", PirParams(c4["target_num_pt"], c4["expansion_height"],
+                                     config="CONFIG_N4096_K2_MP"),
+                     max_batch=4, seed=c4["db_seed"], min_fill=2)
+    k1_clients = [O.Client(op1, 700 + j) for j in range(2)]
+    c4_clients = [O.C4Client(op4, c4["client_seed"])] + [O.C4Client(op4, 800 + j) for j in range(2)]
+    for j, cl in enumerate(k1_clients):
+        eng.register_client("k1", j, cl.bv_keys(), cl.gsw_key())
+    for j, cl in enumerate(c4_clients):
+        eng.register_client("c4", j, cl.bv_keys(), cl.gsw_key())
+
+    rng = np.random.default_rng(23)
+    jobs = []   # (db, client index, plaintext index, query)
+    jobs.append(("c4", 0, c4["index"], c4_clients[0].query(c4["index"])))  # the golden query
+    for i in range(24):
+        if i % 2:
+            j, idx = int(rng.integers(0, 2)), int(rng.integers(0, op1.num_pt))
+            jobs.append(("k1", j, idx, k1_clients[j].query(idx)))
+        else:
+            j, idx = int(rng.integers(1, 3)), int(rng.integers(0, op4.num_pt))
+            jobs.append(("c4", j, idx, c4_clients[j].query(idx)))
+    eng.start()
+    futures = [eng.submit(db, j, q) for db, j, _, q in jobs]
+    eng.drain(timeout=300)
+    got = [f.result(timeout=10) for f in futures]
+    eng.stop()
+    assert G.sha256(got[0]) == c4["sha256_response_u64"]
+    for k, (db, j, idx, q) in enumerate(jobs):
+        alone = eng.dbs[db].lane.server.make_query(j, q)
+        assert np.array_equal(got[k], alone), (db, j, idx)
+        if db == "k1":
+            want = O.db_plaintext(c1["db_seed"], idx, op1).astype(np.uint64)
+            assert np.array_equal(k1_clients[j].decrypt(got[k]), want)
+        else:
+            want = O.c4_db_plaintext(c4["db_seed"], idx, op4)
+            assert np.array_equal(c4_clients[j].decrypt(got[k]), want)
+    assert max(n for _, n, _, _ in eng.batch_log) > 1
+    eng.close()
