@@ -260,6 +260,27 @@ __device__ __forceinline__ void iA(uint64_t (&v)[8]) {
   }
 }
 
+// floor(w 2^64 / q) for w < q = 2^60 - c: w 2^64 = w (16 q + 16 c), so the
+// quotient is 16 w + floor(x / q) with x = 16 c w < 2^81, and floor(x / q) is
+// t0 = floor(x / 2^60) or t0 + 1 (x / q - x / 2^60 < 2^-22); the remainder
+// x - t0 q = (x mod 2^60) + t0 c decides.
+template <uint64_t Q>
+__device__ __forceinline__ uint64_t shoup_of(uint64_t w) {
+  constexpr uint64_t c = (1ull << 60) - Q;
+  const unsigned __int128 x = static_cast<unsigned __int128>(w) * (16 * c);
+  const uint64_t hi = static_cast<uint64_t>(x >> 64), lo = static_cast<uint64_t>(x);
+  const uint64_t t0 = (hi << 4) | (lo >> 60);
+  const uint64_t r0 = (lo & ((1ull << 60) - 1)) + t0 * c;
+  return 16 * w + t0 + (r0 >= Q ? 1 : 0);
+}
+// [0, 16q) -> [0, 2q)
+template <uint64_t Q>
+__device__ __forceinline__ uint64_t fold16(uint64_t x) {
+  x = min(x, x - 8 * Q);
+  x = min(x, x - 4 * Q);
+  return min(x, x - 2 * Q);
+}
+
 // ------------------------------------------------------ RNS <-> integer
 // Garner compose of canonical limbs into [0, q0 q1) (gsw.cpp:22-53)
 __device__ __forceinline__ unsigned __int128 compose(uint64_t r0, uint64_t r1, uint64_t q0inv,

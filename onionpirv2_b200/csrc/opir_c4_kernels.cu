@@ -178,7 +178,9 @@ k4_db_preprocess(Dev4 P, const uint64_t *__restrict__ coeffs, uint64_t coeff_pt_
 // ------------------------------------------------------------ expansion level
 // One heap node, one limb per CTA: the K = 2 BV key switch of the node
 // (bv_keyswitch.cpp:373-481) and its two children (server.cpp:794-809).
-// Digits come from the CRT composition of sigma_k(c1) over both limbs.
+// Digits come from the CRT composition of sigma_k(c1) over both limbs. Key
+// products are Shoup products in [0, 2q) with the rows' stored companions,
+// so eight rows sum below 16q in 64 bits.
 constexpr int kExpGroup = 4;  // digit planes per group
 
 template <int L>
@@ -190,8 +192,8 @@ __device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, 
   constexpr uint64_t Q = Limb<L>::q;
   const int node = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
   const uint64_t *ct = in + (static_cast<uint64_t>(b) * in_stride + node) * kCtWords;
-  const uint64_t *key = bv_keys[b] + bv_level_off;  // [row][b (2N)][a (2N)]
-  u128 ab[8], aa[8];
+  const uint64_t *key = bv_keys[b] + bv_level_off;  // [row][b][a][b'][a']
+  uint64_t ab[8], aa[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
   for (int g = 0; g < kLKs / kExpGroup; ++g) {
@@ -220,19 +222,29 @@ __device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, 
     }
     __syncthreads();
     fwd_mid<L>(sm4, kExpGroup, P.T);
-    ulonglong2 wd[7];
-    fload_d<L>(wd, P.T);
     for (int e = 0; e < kExpGroup; ++e) {
       const int i = g * kExpGroup + e;
-      uint64_t v[8], kb[8], ka[8];
-      ld_plane<3>(sm4 + e * kPad, v, tid);
-      fD<L>(v, wd);  // [0, 6q): 8 rows x 6q x q < 2^126
-      ld8(key + static_cast<uint64_t>(i) * 4 * kN + L * kN + 8 * tid, kb);
-      ld8(key + static_cast<uint64_t>(i) * 4 * kN + 2 * kN + L * kN + 8 * tid, ka);
+      uint64_t v[8];
+      {
+        ulonglong2 wd[7];
+        fload_d<L>(wd, P.T);
+        ld_plane<3>(sm4 + e * kPad, v, tid);
+        fD<L>(v, wd);  // [0, 6q)
+      }
+      const uint64_t *R = key + static_cast<uint64_t>(i) * kRowWords + L * kN + 8 * tid;
+      {
+        uint64_t w[8], ws[8];
+        ld8(R, w);
+        ld8(R + 4 * kN, ws);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        ab[k] += static_cast<u128>(v[k]) * kb[k];
-        aa[k] += static_cast<u128>(v[k]) * ka[k];
+        for (int k = 0; k < 8; ++k) ab[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
+      }
+      {
+        uint64_t w[8], ws[8];
+        ld8(R + 2 * kN, w);
+        ld8(R + 6 * kN, ws);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) aa[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
       }
     }
     __syncthreads();
@@ -242,7 +254,7 @@ __device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, 
     iload_d<L>(wd, P.T);
     uint64_t vb[8], va[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { vb[k] = red128<Q>(ab[k]); va[k] = red128<Q>(aa[k]); }
+    for (int k = 0; k < 8; ++k) { vb[k] = fold16<Q>(ab[k]); va[k] = fold16<Q>(aa[k]); }
     iD<L>(vb, wd);
     iD<L>(va, wd);
     st_plane<3>(sm4, vb, tid);
@@ -291,12 +303,15 @@ k4_expand_level(Dev4 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *__
 // (gsw.cpp:119-182, decomp_rlwe_mp gsw.cpp:184-250): each polynomial of the
 // decomposed ciphertext (both limbs read: y - x, or x when y is null) is
 // CRT-composed and split into l unsigned base-2^B digits; digit d of poly p
-// meets row p l + (l - 1 - d). Uses l planes (G = l when l <= 5, else 4).
-template <int L, int NL, int B, bool CANON>
+// meets row p l + (l - 1 - d). Uses G planes (G = l when l <= 5, else 4).
+// Products are Shoup products in [0, 2q) with the rows' companions; the
+// sums are folded below 2q after each group (< 2q + 5 x 2q in between).
+template <int L, int NL, int B>
 __device__ __forceinline__ void gadget_mac(const Dev4 &P, const uint64_t *x, const uint64_t *y,
-                                           const uint64_t *rgsw, uint64_t *sm, u128 (&acc0)[8],
-                                           u128 (&acc1)[8]) {
+                                           const uint64_t *rgsw, uint64_t *sm, uint64_t (&acc0)[8],
+                                           uint64_t (&acc1)[8]) {
   constexpr int G = NL <= 5 ? NL : 4;
+  constexpr uint64_t Q = Limb<L>::q;
   const int tid = threadIdx.x;
 #pragma unroll 1
   for (int p = 0; p < 2; ++p) {
@@ -323,27 +338,34 @@ __device__ __forceinline__ void gadget_mac(const Dev4 &P, const uint64_t *x, con
       }
       __syncthreads();
       fwd_mid<L>(sm, G, P.T);
-      ulonglong2 wd[7];
-      fload_d<L>(wd, P.T);
       for (int e = 0; e < G; ++e) {
         const int d = g * G + e;
         const int row = p * NL + (NL - 1 - d);
-        uint64_t v[8], r0[8], r1[8];
-        ld_plane<3>(sm + e * kPad, v, tid);
-        fD<L>(v, wd);
-        if (CANON) {
-#pragma unroll
-          for (int k = 0; k < 8; ++k) v[k] = canon8<Limb<L>::q>(v[k]);
+        uint64_t v[8];
+        {
+          ulonglong2 wd[7];
+          fload_d<L>(wd, P.T);
+          ld_plane<3>(sm + e * kPad, v, tid);
+          fD<L>(v, wd);
         }
-        const uint64_t *R = rgsw + static_cast<uint64_t>(row) * kCtWords + L * kN + 8 * tid;
-        ld8(R, r0);
-        ld8(R + 2 * kN, r1);
+        const uint64_t *R = rgsw + static_cast<uint64_t>(row) * kRowWords + L * kN + 8 * tid;
+        {
+          uint64_t w[8], ws[8];
+          ld8(R, w);
+          ld8(R + 4 * kN, ws);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          acc0[k] += static_cast<u128>(v[k]) * r0[k];
-          acc1[k] += static_cast<u128>(v[k]) * r1[k];
+          for (int k = 0; k < 8; ++k) acc0[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
+        }
+        {
+          uint64_t w[8], ws[8];
+          ld8(R + 2 * kN, w);
+          ld8(R + 6 * kN, ws);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc1[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
         }
       }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { acc0[k] = fold16<Q>(acc0[k]); acc1[k] = fold16<Q>(acc1[k]); }
       __syncthreads();
     }
   }
@@ -359,18 +381,21 @@ __device__ __forceinline__ void selectors_body(const Dev4 &P, const Shape4 &S,
   const int row_id = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
   const int selno = row_id / S.l_ep, r = row_id % S.l_ep;
   const uint64_t *ct = leaves + (static_cast<uint64_t>(b) * leaf_stride + S.n0 + row_id) * kCtWords;
-  uint64_t *outs = sel + (static_cast<uint64_t>(b) * (S.num_dims - 1) + selno) * 2 * S.l_ep * kCtWords;
-  u128 acc0[8], acc1[8];
+  uint64_t *outs = sel + (static_cast<uint64_t>(b) * (S.num_dims - 1) + selno) * 2 * S.l_ep * kRowWords;
+  uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
-  // bottom row: ExtProd(RGSW(s), row) with the key gadget (16 rows: canonical
-  // digit NTTs keep the 128-bit sums below 2^126)
-  gadget_mac<L, kLKey, kBaseKey, true>(P, ct, nullptr, gsw_keys[b], sm4, acc0, acc1);
-  uint64_t *bot = outs + static_cast<uint64_t>(S.l_ep + r) * kCtWords + L * kN + 8 * tid;
+  // bottom row: ExtProd(RGSW(s), row) with the key gadget; each selector row
+  // is stored with its Shoup companions (the MUX multiplies by it)
+  gadget_mac<L, kLKey, kBaseKey>(P, ct, nullptr, gsw_keys[b], sm4, acc0, acc1);
+  uint64_t *bot = outs + static_cast<uint64_t>(S.l_ep + r) * kRowWords + L * kN + 8 * tid;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    bot[k] = red128<Q>(acc0[k]);
-    bot[2 * kN + k] = red128<Q>(acc1[k]);
+    const uint64_t v0 = min(acc0[k], acc0[k] - Q), v1 = min(acc1[k], acc1[k] - Q);
+    bot[k] = v0;
+    bot[2 * kN + k] = v1;
+    bot[4 * kN + k] = shoup_of<Q>(v0);
+    bot[6 * kN + k] = shoup_of<Q>(v1);
   }
   // top row: the expanded row itself in NTT form (gsw.cpp:330-338)
 #pragma unroll
@@ -385,14 +410,18 @@ __device__ __forceinline__ void selectors_body(const Dev4 &P, const Shape4 &S,
   fwd_mid<L>(sm4, 2, P.T);
   ulonglong2 wd[7];
   fload_d<L>(wd, P.T);
-  uint64_t *top = outs + static_cast<uint64_t>(r) * kCtWords + L * kN + 8 * tid;
+  uint64_t *top = outs + static_cast<uint64_t>(r) * kRowWords + L * kN + 8 * tid;
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
     uint64_t v[8];
     ld_plane<3>(sm4 + p * kPad, v, tid);
     fD<L>(v, wd);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) top[p * 2 * kN + k] = canon8<Q>(v[k]);
+    for (int k = 0; k < 8; ++k) {
+      const uint64_t c = canon8<Q>(v[k]);
+      top[p * 2 * kN + k] = c;
+      top[4 * kN + p * 2 * kN + k] = shoup_of<Q>(c);
+    }
   }
 }
 
@@ -568,17 +597,17 @@ __device__ __forceinline__ void mux_body(const Dev4 &P, const Shape4 &S, uint32_
   else { xi = i; yi = i + half; oi = i; }
   const uint64_t *x = base_in + static_cast<uint64_t>(xi) * kCtWords;
   const uint64_t *y = base_in + static_cast<uint64_t>(yi) * kCtWords;
-  const uint64_t *rgsw = sel + (static_cast<uint64_t>(b) * (S.num_dims - 1) + level) * 2 * kLEp * kCtWords;
-  u128 acc0[8], acc1[8];
+  const uint64_t *rgsw = sel + (static_cast<uint64_t>(b) * (S.num_dims - 1) + level) * 2 * kLEp * kRowWords;
+  uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
-  gadget_mac<L, kLEp, kBaseEp, false>(P, x, y, rgsw, sm4, acc0, acc1);
+  gadget_mac<L, kLEp, kBaseEp>(P, x, y, rgsw, sm4, acc0, acc1);
   {
     ulonglong2 wd[7];
     iload_d<L>(wd, P.T);
     uint64_t v[8], w[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { v[k] = red128<Q>(acc0[k]); w[k] = red128<Q>(acc1[k]); }
+    for (int k = 0; k < 8; ++k) { v[k] = acc0[k]; w[k] = acc1[k]; }  // [0, 2q)
     iD<L>(v, wd);
     iD<L>(w, wd);
     st_plane<3>(sm4, v, tid);

@@ -7,9 +7,11 @@
 //                byte `plane` of the reference's db[level * num_pt + pt],
 //                pt = row n0 + col (server.cpp:172-194), rows padded to
 //                n0p = n0 rounded up to 16
-//   BV keys    : per client [level < h][row < L_KS][b (2N)][a (2N)], NTT form
-//   RGSW key   : per client [row < 2 L_KEY][c0 (2N)][c1 (2N)], NTT form
-//   selectors  : [query][dim < num_dims-1][row < 2 L_EP][ct], NTT form
+//   BV keys    : per client [level < h][row < L_KS][b (2N)][a (2N)]
+//                [b' (2N)][a' (2N)], NTT form, w' = floor(w 2^64 / q_limb)
+//                the Shoup companion of w (kRowWords per row)
+//   RGSW key   : per client [row < 2 L_KEY][c0][c1][c0'][c1'], NTT form
+//   selectors  : [query][dim < num_dims-1][row < 2 L_EP][c0][c1][c0'][c1']
 //   query mat  : qm[z][col < 2 B][k < n0] u64, col = 2 query + poly, then
 //                qb[(z 8 + plane)][col][n0p] bytes
 //   cmat       : [z][col][row] u64
@@ -27,6 +29,7 @@ constexpr int kN = 4096;
 constexpr uint64_t kQ0 = 1152921504606830593ull;  // 2^60 - 2^14 + 1
 constexpr uint64_t kQ1 = 1152921504606748673ull;  // 2^60 - 2^16 - 2^15 + 1
 constexpr int kCtWords = 4 * kN;  // u64 words per ciphertext (2 polys x 2 limbs)
+constexpr int kRowWords = 8 * kN; // a key / RGSW row: ciphertext + Shoup companions
 
 // Full twiddle tables in global memory, (w, floor(w 2^64 / q)) pairs per limb
 struct Tables {

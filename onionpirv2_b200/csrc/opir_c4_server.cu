@@ -23,6 +23,16 @@ namespace {
 constexpr uint64_t kCt = kCtWords;
 constexpr uint32_t kLKsRows = 8, kLKeyRows = 8;
 
+// Appends one ciphertext-shaped row (4N u64, limb-major polynomials) and
+// its Shoup companions floor(w 2^64 / q_limb) in the device row layout.
+void append_row(std::vector<uint64_t> &dst, const uint64_t *row) {
+  dst.insert(dst.end(), row, row + kCt);
+  for (int j = 0; j < kCtWords; ++j) {
+    const uint64_t q = ((j / kN) & 1) ? kQ1 : kQ0;
+    dst.push_back(static_cast<uint64_t>((static_cast<unsigned __int128>(row[j]) << 64) / q));
+  }
+}
+
 uint32_t resp_bytes_of(const opir_params &p) {
   return static_cast<uint32_t>((2ull * p.poly_degree * p.small_q_width + 7) / 8);
 }
@@ -59,7 +69,7 @@ Plan plan_for(const Shape4 &s, uint64_t lvl_slots, uint32_t n) {
   const uint64_t nsel = s.num_dims > 1 ? s.num_dims - 1 : 0;
   Plan pl{};
   pl.lvl = static_cast<size_t>(n) * lvl_slots * kCt;
-  pl.sel = std::max<uint64_t>(1, n * nsel * 2 * s.l_ep * kCt);
+  pl.sel = std::max<uint64_t>(1, n * nsel * 2 * s.l_ep * kRowWords);
   pl.mid = static_cast<size_t>(n) * s.other * kCt;
   pl.resp = static_cast<size_t>(n) * 2 * kN;
   pl.keyptrs = 2ull * n;
@@ -218,14 +228,21 @@ void Server::set_client_keys(uint64_t id, const uint64_t *bv_keys, const uint32_
   }
   const size_t gsw_rows = 2ull * kLKeyRows;
   check_ct_values(gsw_key, gsw_rows);
-  Keys k;
-  k.bv.alloc(std::max<size_t>(1, h * key_words));
-  k.gsw.alloc(gsw_rows * kCt);
+  // device rows carry their Shoup companions (opir_c4_kernels.h)
+  std::vector<uint64_t> bv_rows, gsw_rows_host;
+  bv_rows.reserve(static_cast<size_t>(h) * kLKsRows * kRowWords);
   for (uint32_t d = 0; d < h; ++d)
-    ck(cudaMemcpyAsync(k.bv.p + d * key_words, bv_keys + order[d] * key_words, key_words * 8,
-                       cudaMemcpyHostToDevice, st_), "bv upload");
-  ck(cudaMemcpyAsync(k.gsw.p, gsw_key, gsw_rows * kCt * 8, cudaMemcpyHostToDevice, st_),
-     "gsw upload");
+    for (uint32_t r = 0; r < kLKsRows; ++r)
+      append_row(bv_rows, bv_keys + order[d] * key_words + r * kCt);
+  for (size_t r = 0; r < gsw_rows; ++r) append_row(gsw_rows_host, gsw_key + r * kCt);
+  Keys k;
+  k.bv.alloc(std::max<size_t>(1, bv_rows.size()));
+  k.gsw.alloc(gsw_rows_host.size());
+  if (!bv_rows.empty())
+    ck(cudaMemcpyAsync(k.bv.p, bv_rows.data(), bv_rows.size() * 8, cudaMemcpyHostToDevice, st_),
+       "bv upload");
+  ck(cudaMemcpyAsync(k.gsw.p, gsw_rows_host.data(), gsw_rows_host.size() * 8,
+                     cudaMemcpyHostToDevice, st_), "gsw upload");
   ck(cudaStreamSynchronize(st_), "key upload");
   Keys &slot = clients_[id];
   slot.bv.swap(k.bv);
@@ -261,7 +278,7 @@ void Server::plan_memory(const opir_params &p, opir_memory_plan *out) {
   out->database_bytes =
       2ull * kN * 8 * s.other * s.n0p + 4ull * kN * sizeof(ulonglong2) + sizeof(uint32_t);
   out->client_key_bytes =
-      (static_cast<uint64_t>(p.expansion_height) * kLKsRows + 2ull * kLKeyRows) * kCt * 8;
+      (static_cast<uint64_t>(p.expansion_height) * kLKsRows + 2ull * kLKeyRows) * kRowWords * 8;
   out->scratch_bytes_per_query = two - one;
   out->scratch_bytes_fixed = 2 * one - two;
 }
@@ -307,7 +324,7 @@ void Server::stage_in(const uint64_t *d_queries, uint32_t n) {
 }
 
 const uint64_t *Server::run_expand(uint32_t n) {
-  const uint64_t level_stride = static_cast<uint64_t>(kLKsRows) * kCt;
+  const uint64_t level_stride = static_cast<uint64_t>(kLKsRows) * kRowWords;
   for (uint32_t d = 0; d < sh_.h; ++d)
     launch_expand_level(dp_, sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p, lvl_slots_,
                         keyptrs_.p, level_stride, n, st_);
@@ -434,8 +451,10 @@ void Server::complete_selectors(uint64_t id, const uint64_t *expanded, uint64_t 
   ck(cudaMemcpyAsync(lvl_[0].p, expanded, static_cast<size_t>(sh_.useful) * kCt * 8,
                      cudaMemcpyHostToDevice, st_), "upload");
   launch_selectors(dp_, sh_, lvl_[0].p, lvl_slots_, keyptrs_.p + 1, sel_.p, 1, st_);
-  ck(cudaMemcpyAsync(out, sel_.p, static_cast<size_t>(nsel) * 2 * sh_.l_ep * kCt * 8,
-                     cudaMemcpyDeviceToHost, st_), "download");
+  // the rows without their Shoup companions
+  ck(cudaMemcpy2DAsync(out, kCt * 8, sel_.p, kRowWords * 8, kCt * 8,
+                       static_cast<size_t>(nsel) * 2 * sh_.l_ep, cudaMemcpyDeviceToHost, st_),
+     "download");
   ck(cudaStreamSynchronize(st_), "complete_selectors");
 }
 
@@ -461,9 +480,14 @@ void Server::evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, 
   ensure_capacity(1);
   ck(cudaMemcpyAsync(mid_[0].p, mid, static_cast<size_t>(sh_.other) * kCt * 8,
                      cudaMemcpyHostToDevice, st_), "upload");
-  if (nsel)
-    ck(cudaMemcpyAsync(sel_.p, selectors, static_cast<size_t>(nsel) * 2 * sh_.l_ep * kCt * 8,
-                       cudaMemcpyHostToDevice, st_), "upload");
+  std::vector<uint64_t> rows;
+  if (nsel) {
+    const size_t n_rows = static_cast<size_t>(nsel) * 2 * sh_.l_ep;
+    rows.reserve(n_rows * kRowWords);
+    for (size_t r = 0; r < n_rows; ++r) append_row(rows, selectors + r * kCt);
+    ck(cudaMemcpyAsync(sel_.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st_),
+       "upload");
+  }
   const uint64_t *r = run_other_dims(1);
   ck(cudaMemcpyAsync(out, r, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "evaluate_other_dim");

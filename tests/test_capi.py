@@ -96,6 +96,7 @@ def test_c4_memory_plan_counts_the_two_limb_buffers():
     m = plan_memory(p)
     # NTT-form database: 2 limbs x N levels x 2^20 plaintexts x 8 bytes
     assert m["database_bytes"] >= 2 * 4096 * (1 << 20) * 8
-    # BV keys (11 levels x 8 rows) + RGSW (16 rows), 4N u64 per row
-    assert m["client_key_bytes"] == (11 * 8 + 16) * 4 * 4096 * 8
+    # BV keys (11 levels x 8 rows) + RGSW (16 rows): 4N u64 per row and as
+    # many Shoup companions
+    assert m["client_key_bytes"] == (11 * 8 + 16) * 8 * 4096 * 8
     assert m["scratch_bytes_per_query"] > 2 * 1024 * 4 * 4096 * 8
