@@ -135,3 +135,28 @@ def test_c4_errors_follow_the_reference():
     with pytest.raises(OutOfRange):                          # BvGaloisKeys::get
         srv.set_client_keys(9, bv, gsw, galois_ks=[3] * bv.shape[0])
     assert np.array_equal(srv.make_query(7, q), srv.make_query(7, q))
+
+
+def test_c4_full_size_batch_decrypts():
+    """The benchmark layout itself (2^20 plaintexts, 64 GiB in NTT form, first
+    dimension 1024 x 10 binary dimensions), beyond what the reference can run:
+    genuine clients' queries, batched with repeats, must decrypt to the
+    requested plaintexts, and a batch answer must equal the lone answer."""
+    target, height = 1 << 20, 11
+    op = O.c4_params(target, height)
+    gp = PirParams(target, height, config=C4)
+    assert (gp.fst_dim_sz, gp.num_dims, gp.other_dim_sz) == (1024, 11, 1024)
+    seed = 424242
+    clients = [O.C4Client(op, 9000 + j) for j in range(3)]
+    rng = np.random.default_rng(77)
+    idxs = [0, target - 1] + [int(i) for i in rng.integers(0, target, 2)]
+    with PirServer(gp) as srv:
+        srv.load_data_seeded(target, seed)
+        for j, cl in enumerate(clients):
+            srv.set_client_keys(j, cl.bv_keys(), cl.gsw_key())
+        owner = [0, 1, 2, 0]
+        queries = np.stack([clients[o].query(i) for o, i in zip(owner, idxs)])
+        out = srv.make_query_batch(owner, queries)
+        for k, (o, i) in enumerate(zip(owner, idxs)):
+            assert np.array_equal(clients[o].decrypt(out[k]), O.c4_db_plaintext(seed, i, op)), i
+        assert np.array_equal(out[1], srv.make_query(owner[1], queries[1]))
