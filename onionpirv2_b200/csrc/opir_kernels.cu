@@ -789,6 +789,9 @@ inline unsigned grid1d(uint64_t n) {
 
 // ===================================================================== launchers
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void note_launches(int64_t delta) {
+  g_launches.fetch_add(static_cast<uint64_t>(delta), std::memory_order_relaxed);
+}
 
 void upload_ntt_constants(const uint32_t q[2], const uint32_t *const fw[2],
                           const uint32_t *const fw_sh[2], const uint32_t *const iw[2],

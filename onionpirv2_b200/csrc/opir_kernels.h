@@ -112,5 +112,8 @@ void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride
 
 // Kernel launches issued so far by this library (all launchers count).
 uint64_t launch_count();
+// Adjusts the launch counter (kernels launched outside opir_kernels.cu, or
+// replayed from a CUDA graph).
+void note_launches(int64_t delta);
 
 }  // namespace opir

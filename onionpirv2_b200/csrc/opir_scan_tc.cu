@@ -43,6 +43,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "opir_kernels.h"
 #include "opir_scan_tc.h"
 #include "opir_tc.cuh"
 
@@ -367,6 +368,7 @@ void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcSc
     k_scan_tc<128><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
   else
     k_scan_tc<64><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
+  note_launches(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw std::runtime_error(std::string("k_scan_tc: ") + cudaGetErrorString(e));
 }

@@ -9,8 +9,11 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <map>
 #include <new>
+#include <set>
 #include <stdexcept>
+#include <tuple>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -53,6 +56,17 @@ struct ScanTile {
   uint32_t ntile = 0, kt = 0, stages = 0;  // ntile 0: pick by the default rule
 };
 constexpr int kTileBuckets = 10;
+
+// One captured make_query pipeline: batch size, the scan tiling it was
+// captured with and whether it records the stage events; `kernels` =
+// launches it replays; ev_nodes[i] = the event-record node of stage mark i.
+using GraphKey = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, bool, bool>;
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t kernels = 0;
+  std::vector<cudaGraphNode_t> ev_nodes;
+};
 int tile_bucket(uint32_t n) {
   int b = 0;
   while (b + 1 < kTileBuckets && (1u << b) < n) ++b;
@@ -95,6 +109,10 @@ struct opir_server {
   cudaEvent_t *cur_ev = nullptr;
   // CONFIG_N4096_K2_MP handles forward every call to this object
   std::unique_ptr<opir4::Server> c4;
+  // captured pipelines (see run_pipeline); a key is captured on its second use
+  bool use_graphs = true;
+  std::map<GraphKey, GraphEntry> graphs;
+  std::set<GraphKey> graph_seen;
 };
 
 namespace {
@@ -253,8 +271,19 @@ void setup_device_params(opir_server *s) {
   s->shape = make_shape(p, &s->lvl_slots);
 }
 
+// Drops every captured pipeline (their buffer pointers or tilings changed).
+void clear_graphs(opir_server *s) {
+  for (auto &kv : s->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  s->graphs.clear();
+  s->graph_seen.clear();
+}
+
 void ensure_capacity(opir_server *s, uint32_t n) {
   if (n <= s->cap) return;
+  clear_graphs(s);
   const ScratchPlan pl = plan_scratch(s->shape, s->lvl_slots, resp_bytes_of(s->params), n);
   s->q_u64.alloc(pl.q_u64);
   s->resp_u64.alloc(pl.resp_u64);
@@ -319,7 +348,14 @@ void begin_timed_call(opir_server *s) {
 }
 
 void mark(opir_server *s, int i) {
-  if (s->cur_ev) ck(cudaEventRecord(s->cur_ev[i], s->stream), "cudaEventRecord");
+  if (!s->cur_ev) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ck(cudaStreamIsCapturing(s->stream, &cs), "capture status");
+  if (cs == cudaStreamCaptureStatusActive)  // becomes an event-record node of the graph
+    ck(cudaEventRecordWithFlags(s->cur_ev[i], s->stream, cudaEventRecordExternal),
+       "cudaEventRecord");
+  else
+    ck(cudaEventRecord(s->cur_ev[i], s->stream), "cudaEventRecord");
 }
 
 // Stage hook for a two-limb call: one event set per timed call, as above.
@@ -430,14 +466,12 @@ uint32_t *run_other_dims(opir_server *s, uint32_t n) {
   return s->mid[levels & 1].p;
 }
 
-void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
-                  const uint64_t *d_queries, uint64_t *d_resp, uint8_t *d_bytes) {
-  if (!s->db_loaded) throw std::runtime_error("make_query before load_data");
-  if (n == 0) return;
-  ensure_capacity(s, n);
-  upload_keyptrs(s, client_ids, n);
+// The kernels of one make_query batch, from queries in d_queries to
+// responses in d_resp (key pointers already uploaded). Stage marks are
+// recorded when a timed call is open.
+void enqueue_core(opir_server *s, uint32_t n, const uint64_t *d_queries, uint64_t *d_resp,
+                  uint8_t *d_bytes) {
   const opir::Shape &sh = s->shape;
-  begin_timed_call(s);
   mark(s, 0);
   opir::launch_split_u64(s->dp, d_queries, s->lvl[0].p, n, 2, s->lvl_slots * kCtWords, s->stream);
   const uint32_t *leaves = run_expand(s, n);
@@ -451,6 +485,91 @@ void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
   opir::launch_modswitch(s->dp, res, sh.other, d_resp, d_bytes, resp_bytes_of(s->params), n,
                          s->stream);
   mark(s, 5);
+}
+
+// Replays (capturing on the second use) the pipeline of a batch of n from the
+// handle's staging buffers q_u64 -> resp_u64. The graph holds fixed buffer
+// pointers, so it is dropped whenever the scratch arena grows or the tiling
+// changes; the key-pointer upload stays outside it.
+void launch_graph(opir_server *s, uint32_t n) {
+  const ScanTile t = effective_tile(s, n);
+  const bool tc = s->shape.n0p <= 8192 &&
+                  (s->scan_mode == 1 || (s->scan_mode == 0 && n >= kTcMinBatch));
+  const bool timed = s->cur_ev != nullptr;
+  const GraphKey key{n, t.ntile, t.kt, t.stages, tc, timed};
+  auto it = s->graphs.find(key);
+  if (it == s->graphs.end()) {
+    if (!s->graph_seen.count(key)) {  // first use: run eagerly (warms one-time setup)
+      s->graph_seen.insert(key);
+      enqueue_core(s, n, s->q_u64.p, s->resp_u64.p, nullptr);
+      return;
+    }
+    const uint64_t l0 = opir::launch_count();
+    GraphEntry e;
+    ck(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      enqueue_core(s, n, s->q_u64.p, s->resp_u64.p, nullptr);
+    } catch (...) {
+      cudaGraph_t partial = nullptr;
+      cudaStreamEndCapture(s->stream, &partial);
+      if (partial) cudaGraphDestroy(partial);
+      cudaGetLastError();
+      throw;
+    }
+    ck(cudaStreamEndCapture(s->stream, &e.graph), "end capture");
+    e.kernels = opir::launch_count() - l0;
+    opir::note_launches(-static_cast<int64_t>(e.kernels));  // counted on replay
+    if (timed) {  // find the node of every stage mark, to retarget them per call
+      size_t count = 0;
+      ck(cudaGraphGetNodes(e.graph, nullptr, &count), "graph nodes");
+      std::vector<cudaGraphNode_t> nodes(count);
+      ck(cudaGraphGetNodes(e.graph, nodes.data(), &count), "graph nodes");
+      e.ev_nodes.assign(kEvents, nullptr);
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        ck(cudaGraphNodeGetType(nd, &ty), "node type");
+        if (ty != cudaGraphNodeTypeEventRecord) continue;
+        cudaEvent_t ev = nullptr;
+        ck(cudaGraphEventRecordNodeGetEvent(nd, &ev), "node event");
+        for (int i = 0; i < kEvents; ++i)
+          if (s->cur_ev[i] == ev) e.ev_nodes[i] = nd;
+      }
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&e.exec, e.graph, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(e.graph);
+      ck(ie, "graph instantiate");
+    }
+    it = s->graphs.emplace(key, e).first;
+  }
+  if (timed)  // this call's event slot
+    for (int i = 0; i < kEvents; ++i)
+      if (it->second.ev_nodes[i])
+        ck(cudaGraphExecEventRecordNodeSetEvent(it->second.exec, it->second.ev_nodes[i],
+                                                s->cur_ev[i]), "event node");
+  ck(cudaGraphLaunch(it->second.exec, s->stream), "graph launch");
+  opir::note_launches(static_cast<int64_t>(it->second.kernels));
+}
+
+void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
+                  const uint64_t *d_queries, uint64_t *d_resp, uint8_t *d_bytes) {
+  if (!s->db_loaded) throw std::runtime_error("make_query before load_data");
+  if (n == 0) return;
+  ensure_capacity(s, n);
+  upload_keyptrs(s, client_ids, n);
+  begin_timed_call(s);
+  if (s->use_graphs && d_bytes == nullptr) {
+    const size_t bytes = static_cast<size_t>(n) * 2 * kN * 8;
+    if (d_queries != s->q_u64.p)
+      ck(cudaMemcpyAsync(s->q_u64.p, d_queries, bytes, cudaMemcpyDeviceToDevice, s->stream),
+         "query staging");
+    launch_graph(s, n);
+    if (d_resp != s->resp_u64.p)
+      ck(cudaMemcpyAsync(d_resp, s->resp_u64.p, bytes, cudaMemcpyDeviceToDevice, s->stream),
+         "response copy");
+  } else {
+    enqueue_core(s, n, d_queries, d_resp, d_bytes);
+  }
   s->cur_ev = nullptr;
 }
 
@@ -561,6 +680,7 @@ opir_status opir_server_create(const opir_params *params, int device, opir_serve
     s->err.alloc(1);
     ck(cudaMemsetAsync(s->err.p, 0, sizeof(uint32_t), s->stream), "err memset");
     ck(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
+    if (const char *gph = std::getenv("OPIR_GRAPHS")) s->use_graphs = std::strcmp(gph, "0") != 0;
     if (const char *m = std::getenv("OPIR_SCAN")) {
       if (std::strcmp(m, "tc") == 0) s->scan_mode = 1;
       else if (std::strcmp(m, "cuda") == 0) s->scan_mode = 2;
@@ -582,6 +702,7 @@ void opir_server_destroy(opir_server *s) {
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    clear_graphs(s);
     s->c4.reset();
     s->clients.clear();
     s->tables.reset();
@@ -872,6 +993,7 @@ opir_status opir_server_autotune(opir_server *s, uint32_t max_batch) {
           float ms = 0;
           ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
           if (ms < best) { best = ms; s->tile[b] = c; }
+          clear_graphs(s);
         }
         check_device_error(s);
         if (n == max_batch) break;

@@ -229,3 +229,45 @@ def test_autotune_keeps_results():
         out = s2.make_query_batch([7] * 5, np.stack([q] * 5))
         for i in range(5):
             _check_response(c, cl, op, out[i])
+
+
+def test_graph_replays_match_eager_launches(monkeypatch):
+    """The per-batch-size CUDA graph (eager on first use, captured on the
+    second, replayed afterwards, with and without stage timing) gives the
+    same responses and replays the same kernels as eager launches."""
+    from onionpirv2_b200.server import launch_count
+    name = "c1_16384_h9"
+    c, op, cl, bv, gsw, q, gp, srv = setup(name)
+    rng = np.random.default_rng(9)
+    clients = [O.Client(op, 3000 + i) for i in range(3)]
+    monkeypatch.setenv("OPIR_GRAPHS", "0")
+    eager = PirServer(gp)
+    monkeypatch.delenv("OPIR_GRAPHS")
+    graphed = PirServer(gp)
+    for s2 in (eager, graphed):
+        s2.load_data_seeded(c["target_num_pt"], c["db_seed"])
+        for i, k in enumerate(clients):
+            s2.set_client_keys(i, k.bv_keys(), k.gsw_key())
+    counts = {}
+    for rnd in range(5):
+        if rnd == 3:
+            eager.set_stage_timing(True)
+            graphed.set_stage_timing(True)
+        idx = [int(i) for i in rng.integers(0, op.num_pt, 3)]
+        qs = np.stack([clients[i].query(idx[i]) for i in range(3)])
+        for tag, s2 in (("eager", eager), ("graph", graphed)):
+            l0 = launch_count()
+            out = s2.make_query_batch([0, 1, 2], qs)
+            counts.setdefault(tag, []).append(launch_count() - l0)
+            if tag == "eager":
+                want = out
+            else:
+                assert np.array_equal(out, want), rnd
+        for i in range(3):
+            assert np.array_equal(clients[i].decrypt(want[i]),
+                                  O.db_plaintext(c["db_seed"], idx[i], op).astype(np.uint64))
+    assert counts["graph"] == counts["eager"]
+    st = graphed.stage_times()
+    assert st["calls"] == 2 and st["Core"] > 0 and st["Expand"] > 0
+    eager.close()
+    graphed.close()
