@@ -687,7 +687,9 @@ k4_modswitch(Dev4 P, const uint64_t *__restrict__ ct_all, uint64_t ct_stride,
 
 // ============================================================== launchers
 uint64_t launch_count() { return g_launches4.load(std::memory_order_relaxed); }
-void note_launch() { g_launches4.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(int64_t delta) {
+  g_launches4.fetch_add(static_cast<uint64_t>(delta), std::memory_order_relaxed);
+}
 
 void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2],
                       const uint64_t *const iw[2], const uint64_t *const iw_sh[2],

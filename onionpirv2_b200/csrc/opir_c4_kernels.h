@@ -49,7 +49,9 @@ struct Shape4 {
 };
 
 uint64_t launch_count();
-void note_launch();  // counts a launch made outside opir_c4_kernels.cu
+// Adjusts the launch counter (a launch made outside opir_c4_kernels.cu, or
+// kernels replayed from a CUDA graph).
+void note_launches(int64_t delta);
 
 void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2],
                       const uint64_t *const iw[2], const uint64_t *const iw_sh[2],

@@ -331,7 +331,7 @@ void launch_scan_tc4(const CUtensorMap &mapA, const CUtensorMap &mapQ, const Tc4
   const unsigned grid =
       static_cast<unsigned>(items < static_cast<uint64_t>(sm_count) ? items : sm_count);
   k4_scan_tc<<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
-  note_launch();
+  note_launches(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw std::runtime_error(std::string("k4_scan_tc: ") + cudaGetErrorString(e));
 }

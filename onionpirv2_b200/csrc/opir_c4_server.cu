@@ -6,6 +6,7 @@
 #include "opir_c4_server.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <stdexcept>
@@ -120,11 +121,13 @@ Server::Server(const opir_params &p, cudaStream_t stream) : p_(p), st_(stream) {
   int dev = 0;
   ck(cudaGetDevice(&dev), "device");
   ck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev), "sm count");
+  if (const char *g = std::getenv("OPIR_GRAPHS")) use_graphs_ = std::strcmp(g, "0") != 0;
   ck(cudaStreamSynchronize(st_), "create");
 }
 
 Server::~Server() {
   if (st_) cudaStreamSynchronize(st_);
+  clear_graphs();
   for (PtrSlot &sl : ring_) {
     if (sl.host) cudaFreeHost(sl.host);
     if (sl.done) cudaEventDestroy(sl.done);
@@ -255,13 +258,24 @@ void Server::remove_client(uint64_t id) {
 }
 
 // ------------------------------------------------------------------ scratch
+void Server::clear_graphs() {
+  for (auto &kv : graphs_) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  graphs_.clear();
+  graph_seen_.clear();
+}
+
 void Server::ensure_capacity(uint32_t n) {
   if (n <= cap_) return;
+  clear_graphs();
   const Plan pl = plan_for(sh_, lvl_slots_, n);
   for (auto &b : lvl_) b.alloc(pl.lvl);
   sel_.alloc(pl.sel);
   for (auto &b : mid_) b.alloc(pl.mid);
   resp_.alloc(pl.resp);
+  q_in_.alloc(static_cast<size_t>(n) * kCt);
   keyptrs_.alloc(pl.keyptrs);
   cap_ = n;
 }
@@ -366,16 +380,28 @@ void Server::check_device_error() {
 // expansion buffer that does not hold the leaves), its byte planes (in the
 // leaves' buffer, dead by then), the scan (its output back in the first
 // buffer), INTT into mid_[0].
-void Server::run_first_dim(const uint64_t *leaves, uint32_t n, const Mark &mark) {
+// Records stage mark i of a timed call; inside a capture it becomes an
+// event-record node that later calls retarget to their own events.
+void Server::mark(Events ev, int i) {
+  if (!ev) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ck(cudaStreamIsCapturing(st_, &cs), "capture status");
+  if (cs == cudaStreamCaptureStatusActive)
+    ck(cudaEventRecordWithFlags(ev[i], st_, cudaEventRecordExternal), "event record");
+  else
+    ck(cudaEventRecord(ev[i], st_), "event record");
+}
+
+void Server::run_first_dim(const uint64_t *leaves, uint32_t n, Events ev) {
   const int li = leaves == lvl_[0].p ? 0 : 1;
   uint64_t *qm = lvl_[li ^ 1].p;
   uint8_t *qb = reinterpret_cast<uint8_t *>(lvl_[li].p);
   uint64_t *cmat = lvl_[li ^ 1].p;
   launch_fst_ntt(dp_, sh_, leaves, lvl_slots_, qm, n, st_);
   launch_fst_pack(sh_, qm, qb, n, st_);
-  if (mark) mark(6);
+  mark(ev, 6);
   launch_scan(qb, cmat, n);
-  if (mark) mark(7);
+  mark(ev, 7);
   launch_epilogue(dp_, sh_, cmat, mid_[0].p, sh_.other, n, st_);
 }
 
@@ -387,35 +413,109 @@ const uint64_t *Server::run_other_dims(uint32_t n) {
   return mid_[levels & 1].p;
 }
 
+// The kernels of one batch, queries d_queries -> responses d_resp (key
+// pointers already uploaded).
+void Server::enqueue_core(uint32_t n, const uint64_t *d_queries, uint64_t *d_resp, Events ev) {
+  mark(ev, 0);
+  stage_in(d_queries, n);
+  const uint64_t *leaves = run_expand(n);
+  mark(ev, 1);
+  launch_selectors(dp_, sh_, leaves, lvl_slots_, keyptrs_.p + n, sel_.p, n, st_);
+  mark(ev, 2);
+  run_first_dim(leaves, n, ev);
+  mark(ev, 3);
+  const uint64_t *res = run_other_dims(n);
+  mark(ev, 4);
+  launch_modswitch(dp_, res, sh_.other, d_resp, nullptr, resp_bytes_of(p_), n, st_);
+  mark(ev, 5);
+}
+
+// Replays (capturing on the second use) the pipeline of a batch of n from
+// the staging buffer q_in_ to resp_.
+void Server::launch_graph(uint32_t n, Events ev) {
+  const auto key = std::make_tuple(n, ev != nullptr);
+  auto it = graphs_.find(key);
+  if (it == graphs_.end()) {
+    if (!graph_seen_.count(key)) {  // first use: eager (warms one-time setup)
+      graph_seen_.insert(key);
+      enqueue_core(n, q_in_.p, resp_.p, ev);
+      return;
+    }
+    const uint64_t l0 = launch_count();
+    Graph g;
+    ck(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      enqueue_core(n, q_in_.p, resp_.p, ev);
+    } catch (...) {
+      cudaGraph_t partial = nullptr;
+      cudaStreamEndCapture(st_, &partial);
+      if (partial) cudaGraphDestroy(partial);
+      cudaGetLastError();
+      throw;
+    }
+    ck(cudaStreamEndCapture(st_, &g.graph), "end capture");
+    g.kernels = launch_count() - l0;
+    note_launches(-static_cast<int64_t>(g.kernels));  // counted on replay
+    if (ev) {
+      size_t count = 0;
+      ck(cudaGraphGetNodes(g.graph, nullptr, &count), "graph nodes");
+      std::vector<cudaGraphNode_t> nodes(count);
+      ck(cudaGraphGetNodes(g.graph, nodes.data(), &count), "graph nodes");
+      g.ev_nodes.assign(kMarks, nullptr);
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        ck(cudaGraphNodeGetType(nd, &ty), "node type");
+        if (ty != cudaGraphNodeTypeEventRecord) continue;
+        cudaEvent_t e = nullptr;
+        ck(cudaGraphEventRecordNodeGetEvent(nd, &e), "node event");
+        for (int i = 0; i < kMarks; ++i)
+          if (ev[i] == e) g.ev_nodes[i] = nd;
+      }
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&g.exec, g.graph, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(g.graph);
+      ck(ie, "graph instantiate");
+    }
+    it = graphs_.emplace(key, g).first;
+  }
+  if (ev)
+    for (int i = 0; i < kMarks; ++i)
+      if (it->second.ev_nodes[i])
+        ck(cudaGraphExecEventRecordNodeSetEvent(it->second.exec, it->second.ev_nodes[i], ev[i]),
+           "event node");
+  ck(cudaGraphLaunch(it->second.exec, st_), "graph launch");
+  note_launches(static_cast<int64_t>(it->second.kernels));
+}
+
 void Server::run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
-                          uint64_t *d_resp, const Mark &mark) {
+                          uint64_t *d_resp, Events ev) {
   if (!db_loaded_) throw std::runtime_error("make_query before load_data");
   if (n == 0) return;
   ensure_capacity(n);
   upload_keyptrs(ids, n);
-  if (mark) mark(0);
-  if (d_queries) stage_in(d_queries, n);
-  const uint64_t *leaves = run_expand(n);
-  if (mark) mark(1);
-  launch_selectors(dp_, sh_, leaves, lvl_slots_, keyptrs_.p + n, sel_.p, n, st_);
-  if (mark) mark(2);
-  run_first_dim(leaves, n, mark);
-  if (mark) mark(3);
-  const uint64_t *res = run_other_dims(n);
-  if (mark) mark(4);
-  launch_modswitch(dp_, res, sh_.other, d_resp, nullptr, resp_bytes_of(p_), n, st_);
-  if (mark) mark(5);
+  if (!use_graphs_) {
+    enqueue_core(n, d_queries, d_resp, ev);
+    return;
+  }
+  if (d_queries != q_in_.p)
+    ck(cudaMemcpyAsync(q_in_.p, d_queries, static_cast<size_t>(n) * kCt * 8,
+                       cudaMemcpyDeviceToDevice, st_), "query staging");
+  launch_graph(n, ev);
+  if (d_resp != resp_.p)
+    ck(cudaMemcpyAsync(d_resp, resp_.p, static_cast<size_t>(n) * 2 * kN * 8,
+                       cudaMemcpyDeviceToDevice, st_), "response copy");
 }
 
 void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *queries,
-                              uint64_t *responses, const Mark &mark) {
+                              uint64_t *responses, Events ev) {
   check_ct_values(queries, n);
   if (!db_loaded_) throw std::runtime_error("make_query before load_data");
   if (n == 0) return;
   ensure_capacity(n);
-  ck(cudaMemcpy2DAsync(lvl_[0].p, lvl_slots_ * kCt * 8, queries, kCt * 8, kCt * 8, n,
-                       cudaMemcpyHostToDevice, st_), "query upload");
-  run_pipeline(n, ids, nullptr, resp_.p, mark);
+  ck(cudaMemcpyAsync(q_in_.p, queries, static_cast<size_t>(n) * kCt * 8, cudaMemcpyHostToDevice,
+                     st_), "query upload");
+  run_pipeline(n, ids, q_in_.p, resp_.p, ev);
   ck(cudaMemcpyAsync(responses, resp_.p, static_cast<size_t>(n) * 2 * kN * 8,
                      cudaMemcpyDeviceToHost, st_), "response download");
   ck(cudaStreamSynchronize(st_), "make_query");
@@ -423,8 +523,8 @@ void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *q
 }
 
 void Server::make_query_batch_device(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
-                                     uint64_t *d_responses, const Mark &mark) {
-  run_pipeline(n, ids, d_queries, d_responses, mark);
+                                     uint64_t *d_responses, Events ev) {
+  run_pipeline(n, ids, d_queries, d_responses, ev);
 }
 
 // ------------------------------------------------------------------ stages
@@ -464,7 +564,7 @@ void Server::evaluate_first_dim(const uint64_t *fst_query, uint64_t *out) {
   ensure_capacity(1);
   ck(cudaMemcpyAsync(lvl_[0].p, fst_query, static_cast<size_t>(sh_.n0) * kCt * 8,
                      cudaMemcpyHostToDevice, st_), "upload");
-  run_first_dim(lvl_[0].p, 1, Mark());
+  run_first_dim(lvl_[0].p, 1, nullptr);
   ck(cudaMemcpyAsync(out, mid_[0].p, static_cast<size_t>(sh_.other) * kCt * 8,
                      cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "evaluate_first_dim");

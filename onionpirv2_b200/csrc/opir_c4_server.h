@@ -7,7 +7,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <functional>
+#include <map>
+#include <set>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -19,7 +21,10 @@ namespace opir4 {
 
 class Server {
  public:
-  using Mark = std::function<void(int)>;  // stage-boundary hook (may be empty)
+  // Stage-boundary events of one timed call: kMarks events recorded at the
+  // stage boundaries (0..5) and around the scan (6, 7); null = untimed.
+  using Events = cudaEvent_t *;
+  static constexpr int kMarks = 8;
 
   Server(const opir_params &p, cudaStream_t stream);
   Server(const Server &) = delete;
@@ -41,10 +46,10 @@ class Server {
 
   // Host buffers: n queries of 4N u64 in, n responses of 2N u64 out.
   void make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *queries,
-                        uint64_t *responses, const Mark &mark);
+                        uint64_t *responses, Events ev);
   // Device buffers, enqueued on the handle's stream (no wait).
   void make_query_batch_device(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
-                               uint64_t *d_responses, const Mark &mark);
+                               uint64_t *d_responses, Events ev);
   void reserve(uint32_t max_batch);
   static void plan_memory(const opir_params &p, opir_memory_plan *out);
 
@@ -71,10 +76,14 @@ class Server {
   void check_ct_values(const uint64_t *v, size_t cts) const;
   void stage_in(const uint64_t *d_queries, uint32_t n);
   const uint64_t *run_expand(uint32_t n);
-  void run_first_dim(const uint64_t *leaves, uint32_t n, const Mark &mark);
+  void run_first_dim(const uint64_t *leaves, uint32_t n, Events ev);
   const uint64_t *run_other_dims(uint32_t n);
   void run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
-                    uint64_t *d_resp, const Mark &mark);
+                    uint64_t *d_resp, Events ev);
+  void enqueue_core(uint32_t n, const uint64_t *d_queries, uint64_t *d_resp, Events ev);
+  void launch_graph(uint32_t n, Events ev);
+  void clear_graphs();
+  void mark(Events ev, int i);
   void launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n);
   void check_device_error();
   template <typename Fill>
@@ -98,6 +107,17 @@ class Server {
   std::vector<const uint64_t *> host_ptrs_;
   PtrSlot ring_[kPtrSlots];
   uint32_t ring_next_ = 0;
+  // captured pipelines per (batch size, timed): eager on first use, captured
+  // on the second; ev_nodes[i] = event-record node of stage mark i
+  struct Graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+    std::vector<cudaGraphNode_t> ev_nodes;
+  };
+  bool use_graphs_ = true;
+  std::map<std::tuple<uint32_t, bool>, Graph> graphs_;
+  std::set<std::tuple<uint32_t, bool>> graph_seen_;
 };
 
 // Parameters of the two-limb set for a layout (pir.cpp:49-134).

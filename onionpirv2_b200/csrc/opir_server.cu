@@ -358,11 +358,12 @@ void mark(opir_server *s, int i) {
     ck(cudaEventRecord(s->cur_ev[i], s->stream), "cudaEventRecord");
 }
 
-// Stage hook for a two-limb call: one event set per timed call, as above.
-opir4::Server::Mark c4_marks(opir_server *s) {
+// Event slot of a two-limb call (null when stage timing is off).
+cudaEvent_t *c4_events(opir_server *s) {
   begin_timed_call(s);
-  if (!s->cur_ev) return opir4::Server::Mark();
-  return [s](int i) { mark(s, i); };
+  cudaEvent_t *ev = s->cur_ev;
+  s->cur_ev = nullptr;
+  return ev;
 }
 
 bool is_c4(const opir_params &p) { return p.num_limbs == 2 && p.poly_degree == 4096; }
@@ -882,7 +883,7 @@ opir_status opir_server_make_query_batch(opir_server *s, uint32_t n, const uint6
     if (n && (!client_ids || !queries || !responses)) throw std::invalid_argument("null argument");
     if (s->c4) {
       DeviceGuard g(s->device);
-      return s->c4->make_query_batch(n, client_ids, queries, responses, c4_marks(s));
+      return s->c4->make_query_batch(n, client_ids, queries, responses, c4_events(s));
     }
     check_query_values(s, queries, static_cast<size_t>(n) * 2 * kN);
     DeviceGuard g(s->device);
@@ -918,7 +919,7 @@ opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
       cudaEventDestroy(e);
     }
     if (s->c4)
-      s->c4->make_query_batch_device(n, client_ids, d_queries, d_responses, c4_marks(s));
+      s->c4->make_query_batch_device(n, client_ids, d_queries, d_responses, c4_events(s));
     else
       run_pipeline(s, client_ids, n, d_queries, d_responses, nullptr);
     if (user) {

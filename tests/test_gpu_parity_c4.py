@@ -160,3 +160,43 @@ def test_c4_full_size_batch_decrypts():
         for k, (o, i) in enumerate(zip(owner, idxs)):
             assert np.array_equal(clients[o].decrypt(out[k]), O.c4_db_plaintext(seed, i, op)), i
         assert np.array_equal(out[1], srv.make_query(owner[1], queries[1]))
+
+
+def test_c4_graph_replays_match_eager_launches(monkeypatch):
+    """The two-limb pipeline captured as a CUDA graph (eager on first use,
+    captured on the second, replayed after, also under stage timing) gives
+    the eager responses and replays the same kernels."""
+    from onionpirv2_b200.server import launch_count
+    c, op, cl, bv, gsw, q, gp, srv = setup("c4_2048_h7")
+    monkeypatch.setenv("OPIR_GRAPHS", "0")
+    eager = PirServer(gp)
+    monkeypatch.delenv("OPIR_GRAPHS")
+    graphed = PirServer(gp)
+    clients = [cl, O.C4Client(op, 4242)]
+    for s2 in (eager, graphed):
+        s2.load_data_seeded(c["target_num_pt"], c["db_seed"])
+        for i, k in enumerate(clients):
+            s2.set_client_keys(i, k.bv_keys(), k.gsw_key())
+    rng = np.random.default_rng(3)
+    counts = {"eager": [], "graph": []}
+    for rnd in range(5):
+        if rnd == 3:
+            eager.set_stage_timing(True)
+            graphed.set_stage_timing(True)
+        idx = [int(i) for i in rng.integers(0, op.num_pt, 2)]
+        qs = np.stack([clients[i].query(idx[i]) for i in range(2)])
+        l0 = launch_count()
+        want = eager.make_query_batch([0, 1], qs)
+        counts["eager"].append(launch_count() - l0)
+        l0 = launch_count()
+        got = graphed.make_query_batch([0, 1], qs)
+        counts["graph"].append(launch_count() - l0)
+        assert np.array_equal(got, want), rnd
+        for i in range(2):
+            assert np.array_equal(clients[i].decrypt(got[i]),
+                                  O.c4_db_plaintext(c["db_seed"], idx[i], op))
+    assert counts["graph"] == counts["eager"]
+    st = graphed.stage_times()
+    assert st["calls"] == 2 and st["Core"] > 0 and st["Other dim"] > 0
+    eager.close()
+    graphed.close()
