@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--target", type=int, default=None,
                     help="plaintexts (smaller layouts are for profiling captures)")
     ap.add_argument("--height", type=int, default=None)
+    ap.add_argument("--sweep", default=None,
+                    help="batch sizes timed after the headline (default 1,8,32,128 for k1, "
+                         "1,8,32,64 for c4; 'none' to skip)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default scan tiling (or OPIR_SCAN_TILE)")
     ap.add_argument("--serve", action="store_true",
@@ -69,6 +72,9 @@ def parse():
         args.target = C4_TARGET if c4 else TARGET
     if args.height is None:
         args.height = C4_HEIGHT if c4 else HEIGHT
+    if args.sweep is None:
+        args.sweep = "1,8,32,64" if c4 else "1,8,32,128"
+    args.sweep = [] if args.sweep == "none" else [int(x) for x in args.sweep.split(",")]
     return args
 
 
@@ -350,20 +356,21 @@ def bench_ours(args, world, rank, local):
     t0 = time.perf_counter()
     srv.load_data_seeded(args.target, DB_SEED)
     load_s = time.perf_counter() - t0
-    queries, keys = synthetic_inputs(params, B, 1000 + rank)
+    nq = max([B] + args.sweep)           # queries (and clients) the runs need
+    queries, keys = synthetic_inputs(params, nq, 1000 + rank)
     for b, (bv, gsw) in enumerate(keys):
         srv.set_client_keys(b, bv, gsw)
     t0 = time.perf_counter()
     if not args.no_autotune:
-        srv.autotune(B)                  # scan tiling per batch bucket (setup, untimed)
+        srv.autotune(nq)                 # scan tiling per batch bucket (setup, untimed)
     tune_s = time.perf_counter() - t0
-    ids = list(range(B))
+    ids = list(range(nq))
     # a dedicated (non-default) stream: the library orders its own stream
     # after this one and this one after its work, so events recorded here
     # bracket the whole batch
     stream = torch.cuda.Stream(device)
     d_q = torch.from_numpy(queries.view(np.int64)).to(device)
-    d_r = torch.empty((B, 2, N), dtype=torch.int64, device=device)
+    d_r = torch.empty((nq, 2, N), dtype=torch.int64, device=device)
 
     def step(n, qbuf, rbuf):
         srv.make_query_batch_device(ids[:n], qbuf.data_ptr(), rbuf.data_ptr(), stream.cuda_stream)
@@ -411,17 +418,29 @@ def bench_ours(args, world, rank, local):
     qps = queries_done / (total_max / 1e3)
 
     # end to end through the host-buffer C ABI call (pinned host memory)
-    hq = torch.from_numpy(queries.view(np.int64)).pin_memory()
+    hq = torch.from_numpy(queries[:B].view(np.int64)).pin_memory()
     hr = torch.empty((B, 2, N), dtype=torch.int64).pin_memory()
     hq_np, hr_np = hq.numpy().view(np.uint64), hr.numpy().view(np.uint64)
     for _ in range(args.warmup):
-        srv.make_query_batch(ids, hq_np, out=hr_np)
+        srv.make_query_batch(ids[:B], hq_np, out=hr_np)
     barrier(world, device)
     te = time.perf_counter()
     for _ in range(args.steps):
-        srv.make_query_batch(ids, hq_np, out=hr_np)
+        srv.make_query_batch(ids[:B], hq_np, out=hr_np)
     e2e_s = max_over_ranks(time.perf_counter() - te, world, device)
     e2e_qps = queries_done / e2e_s
+
+    # batch-size sweep (BASELINE's batched configs), fewer steps each
+    sweep = []
+    for sb in args.sweep:
+        k = max(3, min(args.steps, 20))
+        s_total, s_per, s_stages, _ = timed(sb, k, args.warmup)
+        s_total = max_over_ranks(s_total, world, device)
+        sweep.append({"batch": sb, "steps": k,
+                      "queries_per_s": world * sb * k / (s_total / 1e3),
+                      "ms_per_batch": s_total / k,
+                      "p50_ms": float(np.percentile(s_per, 50)),
+                      "scan_ms": round(s_stages["Core"], 4)})
 
     if rank != 0:
         srv.close()
@@ -475,6 +494,7 @@ def bench_ours(args, world, rank, local):
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "algorithmic_bytes": alg_bytes,
                      "traffic": (traffic or {}).get(f"{'c4_' if c4 else ''}batch_{B}")},
+        "batch_sweep": sweep,
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "setup": {"db_load_s": round(load_s, 3), "autotune_s": round(tune_s, 3),

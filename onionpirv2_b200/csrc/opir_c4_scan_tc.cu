@@ -27,6 +27,13 @@
 // columns) or 32 (one set of 480). Every mbarrier wait is bounded; on timeout
 // the kernel records an error bit, drains its own copies and MMAs, frees
 // TMEM and returns.
+//
+// With two column tiles (more than 8 queries) the tiles of one row tile run
+// on CTAs b and b ^ 1 and load the same database tile; their producers
+// publish the item they start and wait up to ~20 us for the partner, so the
+// second load of a tile finds it in L2 instead of drifting apart by more
+// than L2 holds. The wait is soft: past its bound the producer goes on (the
+// partner may not be resident yet when other kernels share the GPU).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -55,6 +62,7 @@ constexpr int kEpilogueThreads = 256;
 constexpr size_t kBarrierBytes = 256;
 constexpr uint32_t kTmemCols = 512;
 constexpr size_t kSmemLimit = 227 * 1024;
+constexpr long long kPairWaitCycles = 40000;  // ~20 us
 
 template <uint64_t Q>
 __device__ __forceinline__ uint64_t red128_tc(u128 x) {  // x < 2^126 -> [0, q)
@@ -128,10 +136,28 @@ k4_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
 
   if (warp == 0) {
     // ---------------------------------------------------------- producer
-    uint32_t stage = 0, phase = 0, total = 0;
+    uint32_t stage = 0, phase = 0, total = 0, started = 0;
     bool ok = true;
+    const uint32_t partner = blockIdx.x ^ 1u;
+    const bool paired = a.progress != nullptr && a.col_tiles == 2 && partner < gridDim.x;
     for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
       const uint32_t ct = it % a.col_tiles, mt = (it / a.col_tiles) % a.m_tiles, z = it / per_z;
+      ++started;
+      if (paired && lane == 0) {
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.progress + blockIdx.x),
+                     "r"(started)
+                     : "memory");
+        const long long t0 = clock64();
+        for (;;) {
+          uint32_t other;
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];"
+                       : "=r"(other)
+                       : "l"(a.progress + partner)
+                       : "memory");
+          if (other >= started || clock64() - t0 > kPairWaitCycles) break;
+        }
+      }
+      __syncwarp();
       for (uint32_t kt = 0; ok && kt < a.k_tiles; ++kt) {
         if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) { ok = false; break; }
         if (lane == 0) {
@@ -330,6 +356,13 @@ void launch_scan_tc4(const CUtensorMap &mapA, const CUtensorMap &mapQ, const Tc4
   const uint64_t items = static_cast<uint64_t>(args.col_tiles) * args.m_tiles * args.zcount;
   const unsigned grid =
       static_cast<unsigned>(items < static_cast<uint64_t>(sm_count) ? items : sm_count);
+  if (args.progress != nullptr && grid > 1024)
+    throw std::invalid_argument("two-limb tensor-core scan: pairing counters hold 1024 CTAs");
+  if (args.progress != nullptr) {
+    const cudaError_t me = cudaMemsetAsync(args.progress, 0, grid * sizeof(uint32_t), st);
+    if (me != cudaSuccess)
+      throw std::runtime_error(std::string("k4_scan_tc progress: ") + cudaGetErrorString(me));
+  }
   k4_scan_tc<<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
   note_launches(1);
   const cudaError_t e = cudaGetLastError();

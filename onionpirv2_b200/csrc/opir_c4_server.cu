@@ -118,6 +118,7 @@ Server::Server(const opir_params &p, cudaStream_t stream) : p_(p), st_(stream) {
   opir::make_plane_map(&map_db_, db8_.p, sh_.n0p, sh_.other, 2ull * kN * 8, 128, 64);
   err_.alloc(1);
   ck(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), st_), "err memset");
+  progress_.alloc(1024);  // one counter per scan CTA (the grid is at most the SM count)
   int dev = 0;
   ck(cudaGetDevice(&dev), "device");
   ck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev), "sm count");
@@ -361,6 +362,7 @@ void Server::launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n) {
   a.zcount = 2 * kN;
   a.cmat = cmat;
   a.err = err_.p;
+  a.progress = progress_.p;
   CUtensorMap map_q;
   opir::make_plane_map(&map_q, qb, sh_.n0p, ncols, 2ull * kN * 8, a.ntile, 64);
   launch_scan_tc4(map_db_, map_q, a, sm_count_, st_);

@@ -97,6 +97,7 @@ class Server {
   opir::DevBuf<uint8_t> db8_;   // byte-plane database (opir_c4_kernels.h)
   CUtensorMap map_db_{};        // TMA view of db8_ for the tensor-core scan
   opir::DevBuf<uint32_t> err_;  // error word of the tensor-core scan
+  opir::DevBuf<uint32_t> progress_;  // scan CTA pairing counters
   int sm_count_ = 148;
   bool db_loaded_ = false;
   std::unordered_map<uint64_t, Keys> clients_;
