@@ -85,8 +85,30 @@ typedef struct {
   uint32_t base_log2, base_log2_key, base_log2_ks;
   uint64_t target_num_pt, num_pt, fst_dim_sz, other_dim_sz;
   uint32_t num_dims, expansion_height, fst_dim_pow2;
-  uint32_t reserved;
+  uint32_t view;                  /* opir_view: what a handle on these
+                                     parameters may do (below)            */
 } opir_params;
+
+/* Views of a parameter set. OPIR_VIEW_LAYOUT: a database layout
+ * (opir_params_init[_config]); every call is available. OPIR_VIEW_QUERY_SHAPE:
+ * PirParams::with_query_shape (includes/pir.h:46-66) -- no database behind
+ * it; a handle only expands queries and completes selectors
+ * (opir_server_expand_query, opir_server_complete_selectors).
+ * OPIR_VIEW_MATRIX: a tree PIR level database (opir_tree_level_create),
+ * answered by opir_tree_select_level. Calls outside a view's scope return
+ * OPIR_ERR_INVALID_ARGUMENT. */
+typedef enum {
+  OPIR_VIEW_LAYOUT = 0,
+  OPIR_VIEW_QUERY_SHAPE = 1,
+  OPIR_VIEW_MATRIX = 2
+} opir_view;
+
+/* PirQueryShapeConfig (includes/pir.h:46-50). */
+typedef struct {
+  uint64_t fst_dim_sz;
+  uint32_t num_selector_bits;
+  uint32_t expansion_height;
+} opir_query_shape;
 
 typedef struct opir_server opir_server;
 
@@ -106,6 +128,14 @@ opir_status opir_params_init(const opir_layout *layout, opir_params *out);
  * (src/pir.cpp:49-134 with RnsMods {60, 60}, PlainMod 40, SmallQWidth 50;
  * expansion_height <= 12). Unknown config -> OPIR_ERR_INVALID_ARGUMENT. */
 opir_status opir_params_init_config(opir_config config, const opir_layout *layout,
+                                    opir_params *out);
+
+/* PirParams::with_query_shape (src/pir.cpp:136-166): the scheme of `scheme`
+ * with first dimension fst_dim_sz, 1 + num_selector_bits dimensions and the
+ * given expansion height, num_pt = fst_dim_sz, view OPIR_VIEW_QUERY_SHAPE.
+ * Shapes that do not fit the expansion capacity or exceed log2 N ->
+ * OPIR_ERR_INVALID_ARGUMENT. */
+opir_status opir_params_query_shape(const opir_params *scheme, const opir_query_shape *shape,
                                     opir_params *out);
 
 /* Bytes of the serialized response: ceil(2 N small_q_width / 8). */
@@ -309,6 +339,74 @@ opir_status opir_ext_prod_mux_noalloc(const opir_params *params, uint32_t n,
                                       const uint64_t *d_x, const uint64_t *d_y,
                                       const uint64_t *d_selectors, uint64_t *d_out,
                                       void *stream);
+
+/* ---- tree PIR level selection ------------------------------------------
+ * The full-binary-tree PIR layer of the reference (src/tree_index.cpp,
+ * src/tree_query.cpp, src/tree_select.cpp): levels 0..L of a tree with
+ * N = 2^L leaves, each level packed into R_l = 2^max(l - r, 0) plaintexts
+ * (r = log2 n), one packed query expanded into an alpha one-hot of N0 = 2^a
+ * ciphertexts plus b + r RGSW selectors. */
+
+/* TreePirParams (includes/tree_index.h:23-55), g = 1. */
+typedef struct {
+  uint64_t N, L, n, g, rho, r, N0, a, P, B, b;
+  uint64_t ell_beta, ell_gamma, w, h_q, W;
+  uint64_t t;
+} opir_tree_params;
+
+typedef enum {
+  OPIR_TREE_SINGLE = 0,          /* R_l = 1 */
+  OPIR_TREE_COARSENED_ALPHA = 1, /* 1 < R_l < N0 */
+  OPIR_TREE_ALPHA_BETA = 2       /* R_l >= N0 */
+} opir_tree_case;
+
+/* LevelPlan (includes/tree_index.h:76-92). */
+typedef struct {
+  uint64_t level, R;
+  uint32_t select_case, reserved;
+  uint64_t coarsen_count, beta_begin, beta_count, gamma_begin, gamma_count,
+      projection_depth;
+} opir_tree_level_plan;
+
+/* make_tree_pir_params (src/tree_index.cpp:47-92) for any ring shape (pure
+ * index math; moduli: n_moduli RNS moduli). Violations of
+ * validate_tree_params (src/tree_index.cpp:93-150) ->
+ * OPIR_ERR_INVALID_ARGUMENT. */
+opir_status opir_tree_params_make(uint64_t L, uint64_t a, uint64_t n, uint64_t ell_beta,
+                                  uint64_t ell_gamma, uint64_t t, const uint64_t *moduli,
+                                  uint32_t n_moduli, opir_tree_params *out);
+/* make_tree_pir_params_for_scheme (src/tree_query.cpp:42-62): n, t, the RNS
+ * moduli and ell_beta = ell_gamma = L_EP from `scheme`, validated as
+ * validate_tree_params (src/tree_index.cpp:93-150); a query expansion height
+ * above the scheme's -> OPIR_ERR_INVALID_ARGUMENT. */
+opir_status opir_tree_params_init(uint64_t L, uint64_t a, const opir_params *scheme,
+                                  opir_tree_params *out);
+/* build_level_plans (src/tree_index.cpp:177-225): L + 1 plans into `out`. */
+opir_status opir_tree_level_plans(const opir_tree_params *tree, opir_tree_level_plan *out);
+/* tree_query_expansion_params (src/tree_query.cpp:64-68): the query-shape
+ * view {N0, b + r, h_q} a server needs for unpack_tree_query, which is
+ * opir_server_expand_query + opir_server_complete_selectors on it. */
+opir_status opir_tree_query_params(const opir_tree_params *tree, const opir_params *scheme,
+                                   opir_params *out);
+/* A device-resident tree level for select_level (src/tree_select.cpp:
+ * 203-238): level `level` of `tree` with its R_l packed plaintexts
+ * (pack_tree_level order, src/tree_select.cpp:55-75: R_l x n coefficients,
+ * each < t). The handle is a server (opir_server_destroy releases it). */
+opir_status opir_tree_level_create(const opir_params *scheme, const opir_tree_params *tree,
+                                   uint64_t level, const uint64_t *plaintexts, int device,
+                                   opir_server **out);
+/* select_level (src/tree_select.cpp:203-238) for one expanded tree query:
+ *   alpha          : N0 ciphertexts (the alpha one-hot A^(0), coefficient form)
+ *   beta_selectors : b RGSW selectors (2 L_EP rows x ciphertext each, NTT
+ *                    form, the complete_selectors layout); may be NULL when
+ *                    the level's plan folds no beta bit
+ *   out            : the selected ciphertext, coefficient form.
+ * Bit for bit the reference's result: the coarsened pyramid and the
+ * alpha-dimension products are one contraction over the N0 alpha
+ * ciphertexts (the level's plaintexts replicated over the columns they
+ * select), followed by the MSB-first beta fold of ext_prod_mux steps. */
+opir_status opir_tree_select_level(opir_server *level, const uint64_t *alpha,
+                                   const uint64_t *beta_selectors, uint64_t *out);
 
 /* Library version string. */
 const char *opir_version(void);

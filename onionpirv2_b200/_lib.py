@@ -35,8 +35,27 @@ class Params(C.Structure):
         ("base_log2", C.c_uint32), ("base_log2_key", C.c_uint32), ("base_log2_ks", C.c_uint32),
         ("target_num_pt", C.c_uint64), ("num_pt", C.c_uint64), ("fst_dim_sz", C.c_uint64),
         ("other_dim_sz", C.c_uint64), ("num_dims", C.c_uint32), ("expansion_height", C.c_uint32),
-        ("fst_dim_pow2", C.c_uint32), ("reserved", C.c_uint32),
+        ("fst_dim_pow2", C.c_uint32), ("view", C.c_uint32),
     ]
+
+
+class QueryShape(C.Structure):
+    _fields_ = [("fst_dim_sz", C.c_uint64), ("num_selector_bits", C.c_uint32),
+                ("expansion_height", C.c_uint32)]
+
+
+class TreeParams(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in
+                ("N", "L", "n", "g", "rho", "r", "N0", "a", "P", "B", "b",
+                 "ell_beta", "ell_gamma", "w", "h_q", "W", "t")]
+
+
+class TreeLevelPlan(C.Structure):
+    _fields_ = [("level", C.c_uint64), ("R", C.c_uint64), ("select_case", C.c_uint32),
+                ("reserved", C.c_uint32), ("coarsen_count", C.c_uint64),
+                ("beta_begin", C.c_uint64), ("beta_count", C.c_uint64),
+                ("gamma_begin", C.c_uint64), ("gamma_count", C.c_uint64),
+                ("projection_depth", C.c_uint64)]
 
 
 class MemoryPlan(C.Structure):
@@ -48,6 +67,18 @@ SOURCE_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, u64p)
 
 _SIGS = {
     "opir_version": ([], C.c_char_p),
+    "opir_params_query_shape": ([C.POINTER(Params), C.POINTER(QueryShape), C.POINTER(Params)],
+                                C.c_int),
+    "opir_tree_params_make": ([C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                               C.c_uint64, u64p, C.c_uint32, C.POINTER(TreeParams)], C.c_int),
+    "opir_tree_params_init": ([C.c_uint64, C.c_uint64, C.POINTER(Params), C.POINTER(TreeParams)],
+                              C.c_int),
+    "opir_tree_level_plans": ([C.POINTER(TreeParams), C.POINTER(TreeLevelPlan)], C.c_int),
+    "opir_tree_query_params": ([C.POINTER(TreeParams), C.POINTER(Params), C.POINTER(Params)],
+                               C.c_int),
+    "opir_tree_level_create": ([C.POINTER(Params), C.POINTER(TreeParams), C.c_uint64, u64p,
+                                C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "opir_tree_select_level": ([C.c_void_p, u64p, u64p, u64p], C.c_int),
     "opir_params_init": ([C.POINTER(Layout), C.POINTER(Params)], C.c_int),
     "opir_params_init_config": ([C.c_int, C.POINTER(Layout), C.POINTER(Params)], C.c_int),
     "opir_response_bytes": ([C.POINTER(Params)], C.c_size_t),

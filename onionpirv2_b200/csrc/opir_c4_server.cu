@@ -595,4 +595,31 @@ void Server::evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, 
   ck(cudaStreamSynchronize(st_), "evaluate_other_dim");
 }
 
+void Server::select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32_t fold,
+                         uint64_t *out) {
+  if (!db_loaded_) throw std::runtime_error("select_level before load_data");
+  check_ct_values(alpha, sh_.n0);
+  if (fold) check_ct_values(fold_sel, static_cast<size_t>(fold) * 2 * sh_.l_ep);
+  ensure_capacity(1);
+  ck(cudaMemcpyAsync(lvl_[0].p, alpha, static_cast<size_t>(sh_.n0) * kCt * 8,
+                     cudaMemcpyHostToDevice, st_), "upload");
+  run_first_dim(lvl_[0].p, 1, nullptr);
+  const uint64_t *res = mid_[0].p;
+  std::vector<uint64_t> rows;
+  if (fold) {
+    const size_t n_rows = static_cast<size_t>(fold) * 2 * sh_.l_ep;
+    rows.reserve(n_rows * kRowWords);
+    for (size_t r = 0; r < n_rows; ++r) append_row(rows, fold_sel + r * kCt);
+    // slot 0 of the selector set is unused: step a takes slot a
+    ck(cudaMemcpyAsync(sel_.p + 2ull * sh_.l_ep * kRowWords, rows.data(), rows.size() * 8,
+                       cudaMemcpyHostToDevice, st_), "upload");
+    for (uint32_t a = 1; a <= fold; ++a)
+      launch_mux_level(dp_, sh_, a, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other, sel_.p, 1, st_);
+    res = mid_[fold & 1].p;
+  }
+  ck(cudaMemcpyAsync(out, res, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaStreamSynchronize(st_), "select_level");
+  check_device_error();
+}
+
 }  // namespace opir4

@@ -58,6 +58,9 @@ class Server {
   void complete_selectors(uint64_t id, const uint64_t *expanded, uint64_t *out);
   void evaluate_first_dim(const uint64_t *fst_query, uint64_t *out);
   void evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, uint64_t *out);
+  // Tree level handles: first dimension over the n0 ciphertexts, then `fold`
+  // MUX steps at levels 1..fold (selector slot a = step a), host buffers.
+  void select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32_t fold, uint64_t *out);
 
  private:
   struct Keys {

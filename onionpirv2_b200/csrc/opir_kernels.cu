@@ -946,6 +946,8 @@ void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, const 
   check_gadgets(s);
   const uint32_t h = s.num_dims - 1;
   uint32_t n_pairs, offset = 0, half = 0, copies = 0;
+  if (level == 0 && (s.other > (1u << h) || 2ull * s.other < (1ull << h)))
+    throw std::invalid_argument("MUX tree: candidate count outside (2^(d-2), 2^(d-1)]");
   if (level == 0) {
     const uint32_t last = 2 * s.other - (1u << h);
     offset = s.other - last;

@@ -24,6 +24,7 @@
 #include "opir_kernels.h"
 #include "opir_params.h"
 #include "opir_scan_tc.h"
+#include "opir_tree.h"
 
 namespace {
 
@@ -109,6 +110,8 @@ struct opir_server {
   cudaEvent_t *cur_ev = nullptr;
   // CONFIG_N4096_K2_MP handles forward every call to this object
   std::unique_ptr<opir4::Server> c4;
+  // tree level handles (view OPIR_VIEW_MATRIX): the plan's beta fold
+  uint64_t tree_b = 0, fold_begin = 0, fold_count = 0;
   // captured pipelines (see run_pipeline); a key is captured on its second use
   bool use_graphs = true;
   std::map<GraphKey, GraphEntry> graphs;
@@ -620,6 +623,113 @@ void load_tiles(opir_server *s, uint64_t logical, Fill &&fill) {
   s->db_loaded = true;
 }
 
+// The parameters a handle is created on, re-derived from their layout (or
+// query shape) so that a caller cannot hand in inconsistent fields.
+opir_params checked_params(const opir_params &p) {
+  const bool c4 = is_c4(p);
+  if (!c4 && (p.poly_degree != static_cast<uint32_t>(kN) || p.num_limbs != 1))
+    throw std::invalid_argument("unsupported parameter set (CONFIG_N2048_K1_COMP or CONFIG_N4096_K2_MP)");
+  auto derive = [&](const opir_layout &lay) { return c4 ? opir4::derive(lay) : opir::derive_params(lay); };
+  if (p.view == OPIR_VIEW_LAYOUT) {
+    const opir_params check = derive(opir_layout{p.target_num_pt, p.expansion_height, p.fst_dim_pow2});
+    if (check.num_pt != p.num_pt || check.q != p.q || check.q1 != p.q1 || check.q2 != p.q2)
+      throw std::invalid_argument("params do not match their layout");
+    return check;
+  }
+  if (p.view == OPIR_VIEW_QUERY_SHAPE) {
+    const opir_params scheme = derive(opir_layout{1, 0, 1});
+    const opir_params check = opir::with_query_shape(
+        scheme, opir_query_shape{p.fst_dim_sz, p.num_dims - 1, p.expansion_height});
+    if (check.num_pt != p.num_pt || check.q != p.q || check.q1 != p.q1 || check.q2 != p.q2 ||
+        check.num_dims != p.num_dims)
+      throw std::invalid_argument("params do not match their query shape");
+    return check;
+  }
+  throw std::invalid_argument("tree level parameters are created by opir_tree_level_create");
+}
+
+// Allocates a handle for already checked parameters (any view).
+opir_status create_handle(const opir_params &checked, int device, opir_server **out) {
+  opir_server *s = new (std::nothrow) opir_server();
+  if (!s) return OPIR_ERR_NO_MEMORY;
+  const opir_status st = guarded(s, [&] {
+    s->params = checked;
+    s->device = device;
+    DeviceGuard g(device);
+    ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (is_c4(checked)) {
+      s->c4.reset(new opir4::Server(checked, s->stream));
+      return;
+    }
+    setup_device_params(s);
+    const opir::Shape &sh = s->shape;
+    const uint64_t db_bytes = 2ull * kN * 4 * sh.other * sh.n0p;
+    s->db8.alloc(db_bytes);
+    ck(cudaMemsetAsync(s->db8.p, 0, db_bytes, s->stream), "db memset");
+    opir::make_plane_map(&s->map_db[0], s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128, 128);
+    opir::make_plane_map(&s->map_db[1], s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128, 64);
+    s->err.alloc(1);
+    ck(cudaMemsetAsync(s->err.p, 0, sizeof(uint32_t), s->stream), "err memset");
+    ck(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
+    if (const char *gph = std::getenv("OPIR_GRAPHS")) s->use_graphs = std::strcmp(gph, "0") != 0;
+    if (const char *m = std::getenv("OPIR_SCAN")) {
+      if (std::strcmp(m, "tc") == 0) s->scan_mode = 1;
+      else if (std::strcmp(m, "cuda") == 0) s->scan_mode = 2;
+    }
+    ck(cudaStreamSynchronize(s->stream), "create");
+  });
+  if (st != OPIR_OK) {
+    opir_server_destroy(s);
+    return st;
+  }
+  *out = s;
+  return OPIR_OK;
+}
+
+void require_view(const opir_server *s, bool ok, const char *what) {
+  if (!ok)
+    throw std::invalid_argument(std::string(what) + " is not available on a handle created with " +
+                                (s->params.view == OPIR_VIEW_QUERY_SHAPE
+                                     ? "a query shape (no database)"
+                                     : "a tree level database"));
+}
+bool is_layout(const opir_server *s) { return s->params.view == OPIR_VIEW_LAYOUT; }
+
+// select_level on a tree level handle (single-modulus set): the alpha
+// ciphertexts through the first dimension into `other` candidates, then
+// fold_count MSB-first MUX steps (levels 1..fold of the handle's MUX shape,
+// selector slot a = the a-th step's beta selector).
+void select_fold_k1(opir_server *s, const uint64_t *alpha, const uint64_t *fold_sel,
+                    uint32_t fold, uint64_t *out) {
+  const opir::Shape &sh = s->shape;
+  ensure_capacity(s, 1);
+  DevBuf<uint64_t> in;
+  const uint64_t rows_per_sel = 2ull * sh.l_ep;
+  in.alloc(std::max<uint64_t>(2ull * sh.n0, fold * rows_per_sel * 2) * kN);
+  ck(cudaMemcpyAsync(in.p, alpha, 2ull * sh.n0 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+  opir::launch_split_u64(s->dp, in.p, s->lvl[0].p, 1, 2ull * sh.n0, 0, s->stream);
+  run_first_dim(s, s->lvl[0].p, 1);
+  const uint32_t *res = s->mid[0].p;
+  if (fold) {
+    ck(cudaStreamSynchronize(s->stream), "upload");  // `in` is reused
+    ck(cudaMemcpyAsync(in.p, fold_sel, fold * rows_per_sel * 2 * kN * 8, cudaMemcpyHostToDevice,
+                       s->stream), "upload");
+    // slot 0 of the handle's selector set is unused: step a takes slot a
+    opir::launch_split_u64(s->dp, in.p, s->sel.p + rows_per_sel * kCtWords, 1,
+                           fold * rows_per_sel * 2, 0, s->stream);
+    for (uint32_t a = 1; a <= fold; ++a)
+      opir::launch_mux_level(s->dp, sh, a, s->mid[(a - 1) & 1].p, s->mid[a & 1].p, sh.other,
+                             s->sel.p, 1, s->stream);
+    res = s->mid[fold & 1].p;
+  }
+  DevBuf<uint64_t> o;
+  o.alloc(2 * kN);
+  opir::launch_compose_u64(s->dp, res, 0, o.p, 1, 2, s->stream);
+  ck(cudaMemcpyAsync(out, o.p, 2 * kN * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+  ck(cudaStreamSynchronize(s->stream), "select_level");
+  check_device_error(s);
+}
+
 }  // namespace
 
 extern "C" {
@@ -646,54 +756,10 @@ size_t opir_response_bytes(const opir_params *params) {
 opir_status opir_server_create(const opir_params *params, int device, opir_server **out) {
   if (!params || !out) return OPIR_ERR_INVALID_ARGUMENT;
   *out = nullptr;
-  opir_server *s = new (std::nothrow) opir_server();
-  if (!s) return OPIR_ERR_NO_MEMORY;
-  const opir_status st = guarded(s, [&] {
-    if (is_c4(*params)) {
-      opir_layout lay{params->target_num_pt, params->expansion_height, params->fst_dim_pow2};
-      const opir_params check = opir4::derive(lay);
-      if (check.num_pt != params->num_pt || check.q1 != params->q1 || check.q2 != params->q2)
-        throw std::invalid_argument("params do not match their layout");
-      s->params = check;
-      s->device = device;
-      DeviceGuard g(device);
-      ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-      s->c4.reset(new opir4::Server(check, s->stream));
-      return;
-    }
-    if (params->poly_degree != static_cast<uint32_t>(kN) || params->num_limbs != 1)
-      throw std::invalid_argument("unsupported parameter set (CONFIG_N2048_K1_COMP or CONFIG_N4096_K2_MP)");
-    opir_layout lay{params->target_num_pt, params->expansion_height, params->fst_dim_pow2};
-    const opir_params check = opir::derive_params(lay);
-    if (check.num_pt != params->num_pt || check.q != params->q)
-      throw std::invalid_argument("params do not match their layout");
-    s->params = check;
-    s->device = device;
-    DeviceGuard g(device);
-    ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    setup_device_params(s);
-    const opir::Shape &sh = s->shape;
-    const uint64_t db_bytes = 2ull * kN * 4 * sh.other * sh.n0p;
-    s->db8.alloc(db_bytes);
-    ck(cudaMemsetAsync(s->db8.p, 0, db_bytes, s->stream), "db memset");
-    opir::make_plane_map(&s->map_db[0], s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128, 128);
-    opir::make_plane_map(&s->map_db[1], s->db8.p, sh.n0p, sh.other, 2ull * kN * 4, 128, 64);
-    s->err.alloc(1);
-    ck(cudaMemsetAsync(s->err.p, 0, sizeof(uint32_t), s->stream), "err memset");
-    ck(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
-    if (const char *gph = std::getenv("OPIR_GRAPHS")) s->use_graphs = std::strcmp(gph, "0") != 0;
-    if (const char *m = std::getenv("OPIR_SCAN")) {
-      if (std::strcmp(m, "tc") == 0) s->scan_mode = 1;
-      else if (std::strcmp(m, "cuda") == 0) s->scan_mode = 2;
-    }
-    ck(cudaStreamSynchronize(s->stream), "create");
-  });
-  if (st != OPIR_OK) {
-    opir_server_destroy(s);
-    return st;
-  }
-  *out = s;
-  return OPIR_OK;
+  opir_params checked{};
+  const opir_status vs = guarded(nullptr, [&] { checked = checked_params(*params); });
+  if (vs != OPIR_OK) return vs;
+  return create_handle(checked, device, out);
 }
 
 void opir_server_destroy(opir_server *s) {
@@ -743,6 +809,7 @@ opir_status opir_server_params(const opir_server *s, opir_params *out) {
 opir_status opir_server_load_db_u16(opir_server *s, uint64_t logical, const uint16_t *coeffs) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
+    require_view(s, is_layout(s), "load_data");
     if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db_u16(logical, coeffs);
@@ -761,6 +828,7 @@ opir_status opir_server_load_db_u16(opir_server *s, uint64_t logical, const uint
 opir_status opir_server_load_db(opir_server *s, uint64_t logical, const uint64_t *coeffs) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
+    require_view(s, is_layout(s), "load_data");
     if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db(logical, coeffs);
@@ -780,6 +848,7 @@ opir_status opir_server_load_db_source(opir_server *s, uint64_t logical,
                                        opir_plaintext_source source, void *user) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
+    require_view(s, is_layout(s), "load_data");
     if (!source) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db_source(logical, source, user);
@@ -802,6 +871,7 @@ opir_status opir_server_load_db_source(opir_server *s, uint64_t logical,
 opir_status opir_server_load_db_seeded(opir_server *s, uint64_t logical, uint64_t seed) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
+    require_view(s, is_layout(s), "load_data");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db_seeded(logical, seed);
     const opir_params &p = s->params;
@@ -881,6 +951,7 @@ opir_status opir_server_make_query_batch(opir_server *s, uint32_t n, const uint6
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (n && (!client_ids || !queries || !responses)) throw std::invalid_argument("null argument");
+    require_view(s, is_layout(s), "make_query");
     if (s->c4) {
       DeviceGuard g(s->device);
       return s->c4->make_query_batch(n, client_ids, queries, responses, c4_events(s));
@@ -909,6 +980,7 @@ opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (n && (!client_ids || !d_queries || !d_responses)) throw std::invalid_argument("null argument");
+    require_view(s, is_layout(s), "make_query");
     DeviceGuard g(s->device);
     cudaStream_t user = static_cast<cudaStream_t>(stream);
     if (user) {  // order after the caller's prior work on its stream
@@ -1059,6 +1131,7 @@ opir_status opir_server_expand_query(opir_server *s, uint64_t client_id, const u
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (!query || !out) throw std::invalid_argument("null argument");
+    require_view(s, s->params.view != OPIR_VIEW_MATRIX, "expand_query");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->expand_query(client_id, query, out);
     check_query_values(s, query, 2 * kN);
@@ -1080,6 +1153,7 @@ opir_status opir_server_complete_selectors(opir_server *s, uint64_t client_id,
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (!expanded || !out) throw std::invalid_argument("null argument");
+    require_view(s, s->params.view != OPIR_VIEW_MATRIX, "complete_selectors");
     if (s->c4) {
       DeviceGuard g(s->device);
       return s->c4->complete_selectors(client_id, expanded, out);
@@ -1110,6 +1184,7 @@ opir_status opir_server_evaluate_first_dim(opir_server *s, const uint64_t *fst_q
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
     if (!fst_query || !out) throw std::invalid_argument("null argument");
+    require_view(s, is_layout(s), "evaluate_first_dim");
     if (s->c4) {
       DeviceGuard g(s->device);
       return s->c4->evaluate_first_dim(fst_query, out);
@@ -1136,6 +1211,7 @@ opir_status opir_server_evaluate_other_dim(opir_server *s, const uint64_t *mid,
                                            const uint64_t *selectors, uint64_t *out) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
+    require_view(s, is_layout(s), "evaluate_other_dim");
     if (s->c4) {
       const uint32_t nsel = s->params.num_dims - 1;
       if (!mid || !out || (nsel && !selectors)) throw std::invalid_argument("null argument");
@@ -1168,6 +1244,134 @@ opir_status opir_server_evaluate_other_dim(opir_server *s, const uint64_t *mid,
     opir::launch_compose_u64(s->dp, r, 0, o.p, 1, 2, s->stream);
     ck(cudaMemcpyAsync(out, o.p, 2 * kN * 8, cudaMemcpyDeviceToHost, s->stream), "download");
     ck(cudaStreamSynchronize(s->stream), "evaluate_other_dim");
+  });
+}
+
+opir_status opir_params_query_shape(const opir_params *scheme, const opir_query_shape *shape,
+                                    opir_params *out) {
+  if (!scheme || !shape || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] { *out = opir::with_query_shape(*scheme, *shape); });
+}
+
+opir_status opir_tree_params_make(uint64_t L, uint64_t a, uint64_t n, uint64_t ell_beta,
+                                  uint64_t ell_gamma, uint64_t t, const uint64_t *moduli,
+                                  uint32_t n_moduli, opir_tree_params *out) {
+  if (!out || (n_moduli && !moduli)) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] {
+    *out = opir::make_tree_params(L, a, n, ell_beta, ell_gamma, t,
+                                  std::vector<uint64_t>(moduli, moduli + n_moduli));
+  });
+}
+
+opir_status opir_tree_params_init(uint64_t L, uint64_t a, const opir_params *scheme,
+                                  opir_tree_params *out) {
+  if (!scheme || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] { *out = opir::tree_params_for_scheme(L, a, *scheme); });
+}
+
+opir_status opir_tree_level_plans(const opir_tree_params *tree, opir_tree_level_plan *out) {
+  if (!tree || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] {
+    const auto plans = opir::level_plans(*tree);
+    std::copy(plans.begin(), plans.end(), out);
+  });
+}
+
+opir_status opir_tree_query_params(const opir_tree_params *tree, const opir_params *scheme,
+                                   opir_params *out) {
+  if (!tree || !scheme || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] {
+    opir::validate_tree_params(*tree, opir::scheme_moduli(*scheme));
+    *out = opir::with_query_shape(
+        *scheme, opir_query_shape{tree->N0, static_cast<uint32_t>(tree->b + tree->r),
+                                  static_cast<uint32_t>(tree->h_q)});
+  });
+}
+
+opir_status opir_tree_level_create(const opir_params *scheme, const opir_tree_params *tree,
+                                   uint64_t level, const uint64_t *plaintexts, int device,
+                                   opir_server **out) {
+  if (!scheme || !tree || !plaintexts || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  opir_params mp{};
+  opir::LevelMatrix m;
+  opir_tree_level_plan plan{};
+  const opir_status vs = guarded(nullptr, [&] {
+    const opir_params sch = checked_params(*scheme);
+    const auto mods = opir::scheme_moduli(sch);
+    opir::validate_tree_params(*tree, mods);
+    if (tree->n != sch.poly_degree || tree->t != sch.plain_mod || tree->ell_beta != sch.l_ep ||
+        tree->ell_gamma != sch.l_ep)
+      throw std::invalid_argument("tree parameters are not bound to this scheme");
+    if (level > tree->L) throw std::invalid_argument("tree_select: level is out of range");
+    plan = opir::level_plans(*tree)[level];
+    for (uint64_t i = 0; i < plan.R * tree->n; ++i)
+      if (plaintexts[i] >= tree->t)
+        throw std::invalid_argument("tree level coefficient exceeds the plaintext modulus");
+    m = opir::arrange_level(*tree, plan, plaintexts);
+    // the level as a rows x N0 first dimension followed by `fold` MUX steps
+    // (levels 1..fold of a tree of height fold + 1), no expansion
+    mp = sch;
+    mp.fst_dim_sz = m.cols;
+    mp.other_dim_sz = m.rows;
+    mp.num_pt = mp.target_num_pt = m.rows * m.cols;
+    mp.num_dims = static_cast<uint32_t>(m.fold + 2);
+    mp.expansion_height = 0;
+    mp.fst_dim_pow2 = 1;
+    mp.view = OPIR_VIEW_MATRIX;
+  });
+  if (vs != OPIR_OK) return vs;
+  opir_server *s = nullptr;
+  const opir_status cs = create_handle(mp, device, &s);
+  if (cs != OPIR_OK) return cs;
+  const opir_status ls = guarded(s, [&] {
+    s->tree_b = tree->b;
+    s->fold_begin = plan.beta_begin;
+    s->fold_count = plan.beta_count;
+    DeviceGuard g(s->device);
+    const uint64_t npt = m.rows * m.cols;
+    if (s->c4) return s->c4->load_db(npt, m.coeffs.data());
+    load_tiles(s, npt, [&](uint64_t b, uint64_t e, uint16_t *dst) {
+      for (uint64_t i = 0; i < (e - b) * kN; ++i) dst[i] = static_cast<uint16_t>(m.coeffs[b * kN + i]);
+    });
+  });
+  if (ls != OPIR_OK) {
+    opir_server_destroy(s);
+    return ls;
+  }
+  *out = s;
+  return OPIR_OK;
+}
+
+opir_status opir_tree_select_level(opir_server *s, const uint64_t *alpha,
+                                   const uint64_t *beta_selectors, uint64_t *out) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (s->params.view != OPIR_VIEW_MATRIX)
+      throw std::invalid_argument("opir_tree_select_level needs a tree level handle");
+    if (!alpha || !out || (s->fold_count && !beta_selectors))
+      throw std::invalid_argument("null argument");
+    const uint32_t fold = static_cast<uint32_t>(s->fold_count);
+    const bool c4 = s->c4 != nullptr;
+    const size_t ct_words = (c4 ? 4ull : 2ull) * s->params.poly_degree;
+    const size_t sel_words = 2ull * s->params.l_ep * ct_words;
+    // fold_beta_dimension (src/tree_select.cpp:175-201): step k consumes beta
+    // bit begin + count - 1 - k (MSB first)
+    std::vector<uint64_t> fold_sel(static_cast<size_t>(fold) * sel_words);
+    for (uint32_t k = 0; k < fold; ++k) {
+      const uint64_t u = s->fold_begin + s->fold_count - 1 - k;
+      if (u >= s->tree_b) throw std::invalid_argument("fold needs a selector for every active beta bit");
+      std::copy(beta_selectors + u * sel_words, beta_selectors + (u + 1) * sel_words,
+                fold_sel.begin() + k * sel_words);
+    }
+    DeviceGuard g(s->device);
+    if (c4) return s->c4->select_fold(alpha, fold_sel.data(), fold, out);
+    const uint64_t q = s->params.q;
+    for (size_t i = 0; i < s->shape.n0 * ct_words; ++i)
+      if (alpha[i] >= q) throw std::invalid_argument("ciphertext coefficient not reduced mod q");
+    for (uint64_t v : fold_sel)
+      if (v >= q) throw std::invalid_argument("selector value not reduced mod q");
+    select_fold_k1(s, alpha, fold_sel.data(), fold, out);
   });
 }
 

@@ -77,6 +77,26 @@ class PirParams:
                     fst_dim_pow2: bool = True) -> "PirParams":
         return PirParams(target_num_pt, expansion_height, fst_dim_pow2, self.config)
 
+    @classmethod
+    def _wrap(cls, raw: "L.Params", config: str) -> "PirParams":
+        p = cls.__new__(cls)
+        p.config = config
+        p._layout = None
+        p._p = raw
+        return p
+
+    def with_query_shape(self, fst_dim_sz: int, num_selector_bits: int,
+                         expansion_height: int) -> "PirParams":
+        """PirParams::with_query_shape (src/pir.cpp:136-166): a view with no
+        database behind it, for servers that only expand queries and complete
+        selectors."""
+        shape = L.QueryShape(fst_dim_sz, num_selector_bits, expansion_height)
+        raw = L.Params()
+        rc = L.load().opir_params_query_shape(C.byref(self._p), C.byref(shape), C.byref(raw))
+        if rc != OPIR_OK:
+            _raise(rc, "query shape does not fit this scheme")
+        return PirParams._wrap(raw, self.config)
+
     def __getattr__(self, name):
         p = self.__dict__.get("_p")
         if p is not None and name in dict(L.Params._fields_):
@@ -116,7 +136,7 @@ class PirParams:
         return int(L.load().opir_response_bytes(C.byref(self._p)))
 
     def as_dict(self) -> dict:
-        return {f: getattr(self._p, f) for f, _ in L.Params._fields_ if f != "reserved"}
+        return {f: getattr(self._p, f) for f, _ in L.Params._fields_ if f != "view"}
 
 
 class PirServer:
