@@ -454,6 +454,49 @@ int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out) {
   }
   return 0;
 }
+/* tree_query.cpp:142-196 (K = 1), make_tree_query: an encryption of zero
+ * from the client's generator, the alpha one-hot as the BFV lift of
+ * W^-1 mod t at BitRev(alpha, h_q) (add_bfv_query_constant, :70-111), and for
+ * every set bit of group g (b beta bits, then r gamma bits) the L_EP data
+ * gadget rows scaled by W^-1 mod q at BitRev(N0 + g L_EP + row, h_q)
+ * (add_rlwe_star_constant, :113-140). */
+int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                             const uint8_t *bits, uint32_t groups, uint64_t *out) {
+  const opir_oracle_params *p = &c->p;
+  const uint64_t q = p->q, t = p->t, W = 1ULL << h_q;
+  if (h_q > 11 || alpha >= N0 || N0 + (uint64_t)groups * p->l_ep > W) return -1;
+  uint64_t w_inv_t = 0, w_inv_q = 0, gd[64];
+  if (!invmod(W % t, t, &w_inv_t) || !invmod(W % q, q, &w_inv_q)) return -1;
+  encrypt_zero(p, c->sk, &c->rng, out);
+  const uint64_t rev = bitrev(alpha, h_q);
+  const uint64_t scaled = (uint64_t)((((u128)q * w_inv_t) + (t >> 1)) / t) % q;
+  out[rev] = (out[rev] + scaled) % q;
+  gadget(p->l_ep, p->base_ep, q, gd);
+  for (uint32_t g = 0; g < groups; ++g) {
+    if (!bits[g]) continue;
+    for (uint32_t row = 0; row < p->l_ep; ++row) {
+      const uint64_t idx = bitrev(N0 + (uint64_t)g * p->l_ep + row, h_q);
+      const uint64_t v = (uint64_t)((u128)gd[row] * w_inv_q % q);
+      out[idx] = (out[idx] + v) % q;
+    }
+  }
+  return 0;
+}
+/* decrypt_rns (rlwe.cpp:310-348, K = 1): phase = c0 + c1 s mod q, then the
+ * centred rescale q -> t per coefficient; ct coefficient form [c0][c1]. */
+void oracle_client_decrypt_q(const oracle_client *c, const uint64_t *ct, uint64_t *pt_out) {
+  const opir_oracle_params *p = &c->p;
+  const uint32_t N = p->N;
+  const uint64_t q = p->q;
+  barrett_t b = barrett_make(q);
+  uint64_t *c1 = malloc(N * 8);
+  memcpy(c1, ct + N, N * 8);
+  ntt_q(p, c1);
+  for (uint32_t i = 0; i < N; ++i) c1[i] = mulmod(&b, c1[i], c->sk[i]);
+  intt_q(p, c1);
+  for (uint32_t i = 0; i < N; ++i) pt_out[i] = oracle_rescale(addmod(c1[i], ct[i], q), q, p->t);
+  free(c1);
+}
 /* client.cpp:364-430 */
 void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp, uint64_t *pt_out) {
   const opir_oracle_params *p = &c->p;

@@ -73,6 +73,12 @@ void oracle_client_free(oracle_client *c);
 void oracle_client_bv_keys(const oracle_client *c, uint64_t *out);
 void oracle_client_gsw_key(const oracle_client *c, uint64_t *out);
 int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out);
+/* tree_query.cpp:142-196 (K = 1): packed tree query; bits = b beta bits
+ * then r gamma bits (little-endian coordinates), groups = b + r. */
+int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                             const uint8_t *bits, uint32_t groups, uint64_t *out);
+/* decrypt_rns (rlwe.cpp:310-348, K = 1) of a coefficient-form ciphertext. */
+void oracle_client_decrypt_q(const oracle_client *c, const uint64_t *ct, uint64_t *pt_out);
 void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp,
                            uint64_t *pt_out);
 

@@ -18,13 +18,22 @@
 //     PirClient::generate_gsw_from_key (client.cpp:25-38) on rng(client_seed);
 //   * query: PirClient::fast_generate_query / add_gsw_to_query
 //     (client.cpp:48-225) restated over the same public helpers on
-//     rng(client_seed), continuing after the RGSW key draws.
+//     rng(client_seed), continuing after the RGSW key draws;
+//   * tree query (mode "tree"): make_tree_query (tree_query.cpp:142-196)
+//     with PirClient::fresh_zero_ct's encryption of zero on the same
+//     generator and the reference's own add_bfv_query_constant /
+//     add_rlwe_star_constant; the server side (unpack_tree_query,
+//     build_alpha_pyramid, preprocess_tree_reference, select_level) is the
+//     reference's code unchanged.
 #include "bv_keyswitch.h"
 #include "client.h"
 #include "gsw.h"
 #include "pir.h"
 #include "rlwe.h"
 #include "server.h"
+#include "tree_index.h"
+#include "tree_query.h"
+#include "tree_select.h"
 #include "utils.h"
 #include "hexl/hexl.hpp"
 
@@ -197,6 +206,7 @@ struct Args {
   std::string out;
   bool dump_inputs = false;
   std::string stages;  // directory for the public stage outputs (golden mode)
+  size_t tree_L = 16, tree_a = 3, leaf = 0;  // mode "tree"
 };
 
 Args parse(int argc, char **argv) {
@@ -220,6 +230,9 @@ Args parse(int argc, char **argv) {
     else if (k == "--out") a.out = val();
     else if (k == "--dump-inputs") a.dump_inputs = true;
     else if (k == "--stages") a.stages = val();
+    else if (k == "--tree-L") a.tree_L = std::stoull(val());
+    else if (k == "--tree-a") a.tree_a = std::stoull(val());
+    else if (k == "--leaf") a.leaf = std::stoull(val());
     else throw std::invalid_argument("unknown option " + k);
   }
   return a;
@@ -227,9 +240,84 @@ Args parse(int argc, char **argv) {
 
 }  // namespace
 
+// Mode "tree": one packed tree query for `leaf` through the reference's tree
+// layer on the default scheme (as src/tests/test_tree_select.cpp does);
+// writes query.u64, alpha.u64, beta.u64 (the beta selectors) and levels.u64
+// (select_level of every level, c0 || c1 each) into --out and prints whether
+// every level decrypts to its packed plaintext D_l[p_l].
+int run_tree(const Args &a) {
+  constexpr size_t N = DBConsts::PolyDegree;
+  PirParams scheme;
+  const TreePirParams tree = make_tree_pir_params_for_scheme(a.tree_L, a.tree_a, scheme);
+  Client c = make_client(scheme, a.client_seed);
+  const std::vector<uint64_t> qs(scheme.get_rns_mods().begin(), scheme.get_rns_mods().end());
+  // make_tree_query (tree_query.cpp:142-196)
+  const ClientCoordinates coords = client_index(a.leaf, tree);
+  RlweCt query;
+  encrypt_zero_rns(c.sk, N, qs, scheme.get_noise_std_dev(), c.rng, query, false);
+  const uint64_t t = scheme.get_plain_mod();
+  uint64_t w_inv_t = 0;
+  utils::try_invert_uint_mod(tree.W, t, w_inv_t);
+  add_bfv_query_constant(query, scheme, coords.alpha, tree.h_q, w_inv_t);
+  const size_t K = qs.size();
+  std::vector<uint64_t> w_inv_q(K);
+  for (size_t k = 0; k < K; ++k) utils::try_invert_uint_mod(tree.W, qs[k], w_inv_q[k]);
+  const size_t ell = scheme.get_l();
+  const auto gadget = utils::gsw_gadget(ell, scheme.get_base_log2(), qs);
+  std::vector<uint64_t> vals(K);
+  auto rows = [&](size_t group) {
+    for (size_t row = 0; row < ell; ++row) {
+      for (size_t k = 0; k < K; ++k)
+        vals[k] = (uint64_t)((uint128_t)gadget[k][row] * w_inv_q[k] % qs[k]);
+      add_rlwe_star_constant(query, scheme, tree.N0 + group * ell + row, tree.h_q, vals);
+    }
+  };
+  for (size_t u = 0; u < tree.b; ++u) if (coords.beta_bits_le[u]) rows(u);
+  for (size_t v = 0; v < tree.r; ++v) if (coords.gamma_bits_le[v]) rows(tree.b + v);
+
+  std::vector<uint64_t> v(query.c0);
+  v.insert(v.end(), query.c1.begin(), query.c1.end());
+  write_u64(a.out + "/query.u64", v);
+  PirServer server(tree_query_expansion_params(tree, scheme));
+  server.set_client_bv_galois_key(1, c.bv);
+  server.set_client_gsw_key(1, c.gsw);
+  ExpandedTreeQuery un = unpack_tree_query(server, scheme, tree, 1, query);
+  v.clear();
+  for (const auto &ct : un.alpha) { v.insert(v.end(), ct.c0.begin(), ct.c0.end());
+                                    v.insert(v.end(), ct.c1.begin(), ct.c1.end()); }
+  write_u64(a.out + "/alpha.u64", v);
+  v.clear();
+  for (const auto &g : un.beta_selectors) for (const auto &row : g) v.insert(v.end(), row.begin(), row.end());
+  write_u64(a.out + "/beta.u64", v);
+  const AlphaPyramid pyramid = build_alpha_pyramid(un.alpha, tree, scheme);
+  const TreeNodeSource source = [&](size_t level, size_t index) {
+    return synthetic_tree_node_value(level, index, t);
+  };
+  const std::vector<TreeLevelDatabase> levels = preprocess_tree_reference(tree, source);
+  const std::vector<LevelPlan> plans = build_level_plans(tree);
+  bool ok = true;
+  v.clear();
+  for (size_t level = 0; level <= tree.L; ++level) {
+    RlweCt sel = select_level(levels[level], plans[level], pyramid,
+                              std::span<GSWCt>(un.beta_selectors), server, tree, scheme);
+    v.insert(v.end(), sel.c0.begin(), sel.c0.end());
+    v.insert(v.end(), sel.c1.begin(), sel.c1.end());
+    RlwePt dec;
+    decrypt_rns(sel, c.sk, N, qs, t, scheme.get_rns_tables(), dec);
+    const LevelOracle oracle = build_level_oracle_for_test(a.leaf, level, tree);
+    ok = ok && dec.data == levels[level].plaintexts[oracle.packed_plaintext_index];
+  }
+  write_u64(a.out + "/levels.u64", v);
+  std::printf("{\"ok\": %s, \"N0\": %zu, \"b\": %zu, \"r\": %zu, \"h_q\": %zu, \"w\": %zu, "
+              "\"alpha\": %zu}\n", ok ? "true" : "false", tree.N0, tree.b, tree.r, tree.h_q,
+              tree.w, coords.alpha);
+  return ok ? 0 : 3;
+}
+
 int main(int argc, char **argv) {
   try {
     const Args a = parse(argc, argv);
+    if (a.mode == "tree") return run_tree(a);
     constexpr size_t N = DBConsts::PolyDegree;
     PirParams params = PirParams().with_layout({a.target, a.height, a.pow2});
     const uint64_t t = params.get_plain_mod();

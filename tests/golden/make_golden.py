@@ -14,9 +14,17 @@ limbs); those cases also store SHA-256 digests of the outputs of the
 reference's public stage methods (expand_query, complete_selectors,
 evaluate_first_dim, evaluate_other_dim) in the reference's own flat layouts.
 
+A third set (golden_tree.json) runs the reference's tree PIR layer
+(src/tree_*.cpp) through the driver's "tree" mode: one packed tree query per
+case on the default scheme, unpacked by unpack_tree_query, and the digests of
+the query, the alpha one-hot, the beta selectors and select_level's output at
+every level (the reference's own Milestone-2 gate, every level decrypting to
+its packed plaintext, must hold).
+
 Only needed when the fixtures must change; tests never run it.
     python tests/golden/make_golden.py            # CONFIG_N2048_K1_COMP set
     python tests/golden/make_golden.py --c4       # CONFIG_N4096_K2_MP set
+    python tests/golden/make_golden.py --tree     # tree PIR select_level set
 """
 from __future__ import annotations
 
@@ -58,12 +66,63 @@ CASES_C4 = [
 ]
 
 
+# (name, L, a, client seed, leaf): the shapes and the boundary, mixed-bit and
+# beta-asymmetric leaves of src/tests/test_tree_select.cpp:103-123
+def tree_cases():
+    out = []
+    for L, a, seed in ((16, 3, 31), (13, 2, 32)):
+        N, r = 1 << L, 11
+        b = L - r - a
+        P, B = N >> r, 1 << b
+        leaves = [0, N - 1, 0x2BADBEEF % N, P + B + (1 if b >= 2 else 0)]
+        for k, leaf in enumerate(leaves):
+            out.append((f"tree_L{L}_a{a}_leaf{leaf}", L, a, seed + 10 * k, leaf))
+    return out
+
+
 def sha(path: str) -> str:
     with open(path, "rb") as f:
         return hashlib.sha256(f.read()).hexdigest()
 
 
+def main_tree() -> int:
+    if not os.path.exists(REF_BIN):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
+    manifest = []
+    for name, L, a, seed, leaf in tree_cases():
+        with tempfile.TemporaryDirectory() as tmp:
+            out = subprocess.run(
+                [REF_BIN, "--mode", "tree", "--tree-L", str(L), "--tree-a", str(a),
+                 "--client-seed", str(seed), "--leaf", str(leaf), "--out", tmp],
+                check=True, capture_output=True, text=True)
+            info = json.loads(out.stdout.strip().splitlines()[-1])
+            if not info["ok"]:
+                raise RuntimeError(f"{name}: reference select_level does not decrypt")
+            import numpy as np
+            levels = np.fromfile(os.path.join(tmp, "levels.u64"), dtype=np.uint64)
+            per = levels.reshape(L + 1, -1)
+            manifest.append({
+                "name": name, "L": L, "a": a, "client_seed": seed, "leaf": leaf,
+                "N0": info["N0"], "b": info["b"], "r": info["r"], "h_q": info["h_q"],
+                "w": info["w"], "alpha": info["alpha"],
+                "sha256_query_u64": sha(os.path.join(tmp, "query.u64")),
+                "sha256_alpha_u64": sha(os.path.join(tmp, "alpha.u64")),
+                "sha256_beta_selectors_u64": sha(os.path.join(tmp, "beta.u64")),
+                "sha256_levels_u64": [hashlib.sha256(per[i].tobytes()).hexdigest()
+                                      for i in range(L + 1)],
+            })
+            print(f"{name}: ok", flush=True)
+    with open(os.path.join(HERE, "golden_tree.json"), "w") as f:
+        json.dump({"generator": "oracle/_ref/opir_ref --mode tree (reference sources incl. "
+                                "src/tree_*.cpp + HEXL stand-in), default PirParams scheme",
+                   "node_source": "synthetic_tree_node_value (src/tree_select.cpp:44-53)",
+                   "cases": manifest}, f, indent=1)
+    return 0
+
+
 def main() -> int:
+    if "--tree" in sys.argv[1:]:
+        return main_tree()
     c4 = "--c4" in sys.argv[1:]
     ref_bin, cases_ = (REF_BIN_C4, CASES_C4) if c4 else (REF_BIN, CASES)
     if not os.path.exists(ref_bin):

@@ -31,6 +31,12 @@ def case_c4(name):
     raise KeyError(name)
 
 
+def cases_tree():
+    """Tree PIR select_level cases (reference tree layer, default scheme)."""
+    with open(os.path.join(GOLDEN_DIR, "golden_tree.json")) as f:
+        return json.load(f)["cases"]
+
+
 def stream(c):
     with open(os.path.join(GOLDEN_DIR, c["name"] + ".resp.bin"), "rb") as f:
         return f.read()
