@@ -52,8 +52,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-queries", type=int, default=3)
-    ap.add_argument("--workload", choices=["k1", "c4"], default="k1",
-                    help="k1: CONFIG_N2048_K1_COMP at 2^18 plaintexts; c4: CONFIG_N4096_K2_MP at 2^20")
+    ap.add_argument("--workload", choices=["k1", "c4", "tree"], default="k1",
+                    help="k1: CONFIG_N2048_K1_COMP at 2^18 plaintexts; c4: CONFIG_N4096_K2_MP at 2^20; "
+                         "tree: tree PIR path selection (L = 16, a = 3)")
     ap.add_argument("--target", type=int, default=None,
                     help="plaintexts (smaller layouts are for profiling captures)")
     ap.add_argument("--height", type=int, default=None)
@@ -266,6 +267,9 @@ def bench_reference(args, world, rank):
     procs = os.cpu_count() or 1
     if args.workload == "c4":
         bench_reference_c4(args, procs)
+        return
+    if args.workload == "tree":
+        bench_reference_tree(args, procs)
         return
     # a bounded sample: at most 8 timed queries (and 1 warm-up) per process,
     # ~2 s each on one core, so the run ends within a few minutes
@@ -630,9 +634,173 @@ def bench_serve(args, world, rank, local):
     eng.close()
 
 
+# ---------------------------------------------------------------- tree PIR
+TREE_L, TREE_A = 16, 3
+
+
+def run_reference_tree(runs: int) -> dict:
+    """The reference's tree layer (driver mode "tree"): server-side time of
+    one tree query (unpack_tree_query + select_level at every level), best of
+    the portable and AVX-512 builds, `runs` queries each."""
+    best = None
+    for exe in (os.path.join(ROOT, "oracle", "_ref", "opir_ref"),
+                os.path.join(ROOT, "oracle", "_ref", "opir_ref_avx512")):
+        if not os.path.exists(exe):
+            continue
+        ms = []
+        for k in range(runs):
+            import tempfile
+            with tempfile.TemporaryDirectory() as tmp:
+                out = subprocess.run([exe, "--mode", "tree", "--tree-L", str(TREE_L), "--tree-a",
+                                      str(TREE_A), "--leaf", str(37 + 1000 * k), "--client-seed",
+                                      str(61 + k), "--out", tmp],
+                                     check=True, capture_output=True, text=True)
+            ms.append(json.loads(out.stdout.strip().splitlines()[-1])["server_ms"])
+        mean = sum(ms) / len(ms)
+        if best is None or mean < best["mean_ms"]:
+            best = {"mean_ms": mean, "binary": os.path.basename(exe), "runs": len(ms)}
+    if best is None:
+        raise FileNotFoundError("oracle/_ref is not built")
+    return best
+
+
+def bench_reference_tree(args, procs):
+    """The reference arm of --workload tree: `procs` concurrent driver
+    processes, each timing min(steps, 3) tree queries server-side."""
+    from concurrent.futures import ThreadPoolExecutor
+    runs = max(1, min(args.steps, 3))
+    try:
+        best = run_reference_tree(1)              # picks the faster build
+        exe = os.path.join(ROOT, "oracle", "_ref", best["binary"])
+
+        def one(k):
+            import tempfile
+            ms = []
+            for j in range(runs):
+                with tempfile.TemporaryDirectory() as tmp:
+                    out = subprocess.run([exe, "--mode", "tree", "--tree-L", str(TREE_L),
+                                          "--tree-a", str(TREE_A), "--leaf", str(37 + 97 * (k * runs + j)),
+                                          "--client-seed", str(100 + k * runs + j), "--out", tmp],
+                                         check=True, capture_output=True, text=True)
+                ms.append(json.loads(out.stdout.strip().splitlines()[-1])["server_ms"])
+            return ms
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(procs) as ex:
+            all_ms = [m for ms in ex.map(one, range(procs)) for m in ms]
+        wall = time.perf_counter() - t0
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference tree layer: {e}"}))
+        return
+    mean = sum(all_ms) / len(all_ms)
+    qps = procs * 1000.0 / mean
+    line = {
+        "impl": "reference", "metric": "tree PIR paths/s (unpack + select_level at every level, bit-exact)",
+        "value": qps, "unit": "tree queries/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mean, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"tree PIR L={TREE_L} a={TREE_A} on CONFIG_N2048_K1_COMP", "batch": 1,
+                   "parallelism": f"{procs} host processes"},
+        "cpu_baseline": {"value": qps, "unit": "tree queries/s", "cores": procs, "kind": "reference",
+                         "sample": (f"reference unpack_tree_query + select_level (oracle/_ref/"
+                                    f"{best['binary']} --mode tree) in {procs} concurrent processes x "
+                                    f"{runs} queries, server-side time per query (wall {wall:.1f} s); "
+                                    f"CPU {cpu_model()}")},
+        "e2e": {"value": qps, "unit": "tree queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def bench_tree(args, world, rank, local):
+    """One tree query = unpack (expansion + selector completion) +
+    select_level at all L + 1 levels through the device-resident tree handle
+    (opir_tree_query: host query in, the L + 1 selected ciphertexts out, one
+    synchronising call), on synthetic uniform ciphertexts and keys (the path
+    is data-independent); replicas at N > 1."""
+    import torch
+    from onionpirv2_b200 import PirParams, PirServer
+    from onionpirv2_b200 import tree as T
+    from onionpirv2_b200.server import launch_count
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
+    scheme = PirParams()
+    tree = T.make_tree_pir_params_for_scheme(TREE_L, TREE_A, scheme)
+    src = lambda level, idx: T.synthetic_tree_node_value(level, idx, scheme.plain_mod)
+    t0 = time.perf_counter()
+    whole = T.Tree(scheme, tree, [T.pack_tree_level(lv, tree, src) for lv in range(tree.L + 1)],
+                   device=local)
+    setup_s = time.perf_counter() - t0
+    qp = T.tree_query_expansion_params(tree, scheme)
+    queries, keys = synthetic_inputs(qp, 1, 4000 + rank)
+    whole.set_client_keys(0, *keys[0])
+    out = np.zeros((tree.L + 1, 2, scheme.N), dtype=np.uint64)
+
+    def step():
+        whole.query(0, queries[0])
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world, device)
+    l0 = launch_count()
+    te = time.perf_counter()
+    per = []
+    for _ in range(args.steps):
+        ts = time.perf_counter()
+        step()
+        per.append((time.perf_counter() - ts) * 1e3)
+    total = max_over_ranks(time.perf_counter() - te, world, device)
+    launches = launch_count() - l0
+    qps = world * args.steps / total
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": "tree PIR paths/s (unpack + select_level at every level, bit-exact)",
+        "value": qps, "unit": "tree queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded uniform query and keys mod q; synthetic_tree_node_value tree)",
+        "config": {"workload": f"tree PIR L={TREE_L} a={TREE_A} on CONFIG_N2048_K1_COMP: N0="
+                               f"{tree.N0}, b={tree.b}, r={tree.r}, h_q={tree.h_q}, "
+                               f"{tree.L + 1} levels", "batch": 1,
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+        "e2e": {"value": qps, "unit": "tree queries/s",
+                "h2d_bytes_per_step": int(queries[0].nbytes), "d2h_bytes_per_step": int(out.nbytes)},
+        "gpu_launches": launches, "setup": {"levels_s": round(setup_s, 3)},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            res = run_reference_tree(3)
+            line["cpu_baseline"] = {
+                "value": 1000.0 / res["mean_ms"], "unit": "tree queries/s", "cores": 1,
+                "kind": "reference",
+                "sample": (f"reference unpack_tree_query + select_level over all {tree.L + 1} levels "
+                           f"(oracle/_ref/{res['binary']} --mode tree, HEXL stand-in), "
+                           f"{res['runs']} seeded tree queries; CPU {cpu_model()}")}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unit": "tree queries/s", "cores": 0,
+                                    "kind": "reference", "sample": f"unavailable: {e}"}
+    print(json.dumps(line))
+    whole.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist_env()
+    if args.workload == "tree" and args.impl == "ours" and not args.serve:
+        bench_tree(args, world, rank, local)
+        return
     if args.serve:
         bench_serve(args, world, rank, local)
         return

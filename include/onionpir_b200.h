@@ -408,6 +408,31 @@ opir_status opir_tree_level_create(const opir_params *scheme, const opir_tree_pa
 opir_status opir_tree_select_level(opir_server *level, const uint64_t *alpha,
                                    const uint64_t *beta_selectors, uint64_t *out);
 
+/* A whole device-resident tree (single-modulus set): the query-shape server
+ * that unpacks tree queries and one level database per level 0..L, all on
+ * one device. A query is answered without host round trips between its
+ * stages: expansion and selector completion on the query handle, then every
+ * level's select_level on its own stream (levels overlap on the GPU), the
+ * alpha ciphertexts and fold selectors passed device to device.
+ *   level_plaintexts : L + 1 pointers, level l = R_l x n coefficients < t
+ *                      (pack_tree_level order) */
+typedef struct opir_tree opir_tree;
+opir_status opir_tree_create(const opir_params *scheme, const opir_tree_params *tree,
+                             const uint64_t *const *level_plaintexts, int device,
+                             opir_tree **out);
+void opir_tree_destroy(opir_tree *tree);
+const char *opir_tree_last_error(const opir_tree *tree);
+/* The client's BV keys (for the tree query's expansion height) and RGSW(s),
+ * as opir_server_set_client_keys. */
+opir_status opir_tree_set_client_keys(opir_tree *tree, uint64_t client_id,
+                                      const uint64_t *bv_keys, const uint32_t *galois_ks,
+                                      uint32_t n_keys, const uint64_t *gsw_key);
+/* unpack_tree_query + select_level at every level for one packed tree query
+ * (host buffers): selected = (L + 1) ciphertexts, level order, coefficient
+ * form -- bit for bit opir_tree_select_level of each level. */
+opir_status opir_tree_query(opir_tree *tree, uint64_t client_id, const uint64_t *query,
+                            uint64_t *selected);
+
 /* Library version string. */
 const char *opir_version(void);
 

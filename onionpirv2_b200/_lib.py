@@ -79,6 +79,12 @@ _SIGS = {
     "opir_tree_level_create": ([C.POINTER(Params), C.POINTER(TreeParams), C.c_uint64, u64p,
                                 C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "opir_tree_select_level": ([C.c_void_p, u64p, u64p, u64p], C.c_int),
+    "opir_tree_create": ([C.POINTER(Params), C.POINTER(TreeParams), C.POINTER(u64p), C.c_int,
+                          C.POINTER(C.c_void_p)], C.c_int),
+    "opir_tree_destroy": ([C.c_void_p], None),
+    "opir_tree_last_error": ([C.c_void_p], C.c_char_p),
+    "opir_tree_set_client_keys": ([C.c_void_p, C.c_uint64, u64p, u32p, C.c_uint32, u64p], C.c_int),
+    "opir_tree_query": ([C.c_void_p, C.c_uint64, u64p, u64p], C.c_int),
     "opir_params_init": ([C.POINTER(Layout), C.POINTER(Params)], C.c_int),
     "opir_params_init_config": ([C.c_int, C.POINTER(Layout), C.POINTER(Params)], C.c_int),
     "opir_response_bytes": ([C.POINTER(Params)], C.c_size_t),

@@ -118,39 +118,60 @@ struct opir_server {
   std::set<GraphKey> graph_seen;
 };
 
+// A whole device-resident tree (see opir_tree_create): the query-shape
+// handle, one level handle per level, a join stream and the output buffer.
+struct opir_tree {
+  opir_tree_params tree{};
+  int device = 0;
+  opir_server *q = nullptr;
+  std::vector<opir_server *> levels;
+  cudaStream_t stream = nullptr;
+  DevBuf<uint64_t> out;            // (L + 1) x 2N u64
+  cudaEvent_t q_done = nullptr;
+  std::vector<cudaEvent_t> done;   // per level
+  std::string last_error;
+};
+
 namespace {
 
 using opir::kCtWords;
 using opir::kN;
 
-opir_status fail(opir_server *s, opir_status code, const std::string &msg) {
-  if (s) s->last_error = msg;
+opir_status fail(std::string *sink, opir_status code, const std::string &msg) {
+  if (sink) *sink = msg;
   return code;
+}
+
+// Runs f, mapping the exception types the reference throws onto status codes
+// and keeping the message in *sink.
+template <typename F>
+opir_status guarded_to(std::string *sink, F &&f) {
+  try {
+    f();
+    if (sink) sink->clear();
+    return OPIR_OK;
+  } catch (const std::invalid_argument &e) {
+    return fail(sink, OPIR_ERR_INVALID_ARGUMENT, e.what());
+  } catch (const std::out_of_range &e) {
+    return fail(sink, OPIR_ERR_OUT_OF_RANGE, e.what());
+  } catch (const std::overflow_error &e) {
+    return fail(sink, OPIR_ERR_OVERFLOW, e.what());
+  } catch (const std::bad_alloc &) {
+    return fail(sink, OPIR_ERR_NO_MEMORY, "device or host allocation failed");
+  } catch (const CudaError &e) {
+    cudaGetLastError();
+    return fail(sink, OPIR_ERR_CUDA, e.what());
+  } catch (const std::runtime_error &e) {
+    cudaGetLastError();
+    return fail(sink, OPIR_ERR_RUNTIME, e.what());
+  } catch (...) {
+    return fail(sink, OPIR_ERR_RUNTIME, "unknown error");
+  }
 }
 
 template <typename F>
 opir_status guarded(opir_server *s, F &&f) {
-  try {
-    f();
-    if (s) s->last_error.clear();
-    return OPIR_OK;
-  } catch (const std::invalid_argument &e) {
-    return fail(s, OPIR_ERR_INVALID_ARGUMENT, e.what());
-  } catch (const std::out_of_range &e) {
-    return fail(s, OPIR_ERR_OUT_OF_RANGE, e.what());
-  } catch (const std::overflow_error &e) {
-    return fail(s, OPIR_ERR_OVERFLOW, e.what());
-  } catch (const std::bad_alloc &) {
-    return fail(s, OPIR_ERR_NO_MEMORY, "device or host allocation failed");
-  } catch (const CudaError &e) {
-    cudaGetLastError();
-    return fail(s, OPIR_ERR_CUDA, e.what());
-  } catch (const std::runtime_error &e) {
-    cudaGetLastError();
-    return fail(s, OPIR_ERR_RUNTIME, e.what());
-  } catch (...) {
-    return fail(s, OPIR_ERR_RUNTIME, "unknown error");
-  }
+  return guarded_to(s ? &s->last_error : nullptr, std::forward<F>(f));
 }
 
 uint32_t resp_bytes_of(const opir_params &p) {
@@ -1372,6 +1393,129 @@ opir_status opir_tree_select_level(opir_server *s, const uint64_t *alpha,
     for (uint64_t v : fold_sel)
       if (v >= q) throw std::invalid_argument("selector value not reduced mod q");
     select_fold_k1(s, alpha, fold_sel.data(), fold, out);
+  });
+}
+
+void opir_tree_destroy(opir_tree *t) {
+  if (!t) return;
+  {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(t->device);
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    for (opir_server *l : t->levels) opir_server_destroy(l);
+    if (t->q) opir_server_destroy(t->q);
+    for (cudaEvent_t e : t->done) cudaEventDestroy(e);
+    if (t->q_done) cudaEventDestroy(t->q_done);
+    t->out.reset();
+    if (t->stream) cudaStreamDestroy(t->stream);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  delete t;
+}
+
+const char *opir_tree_last_error(const opir_tree *t) {
+  return t ? t->last_error.c_str() : "null tree handle";
+}
+
+opir_status opir_tree_create(const opir_params *scheme, const opir_tree_params *tree,
+                             const uint64_t *const *level_plaintexts, int device,
+                             opir_tree **out) {
+  if (!scheme || !tree || !level_plaintexts || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  opir_tree *t = new (std::nothrow) opir_tree();
+  if (!t) return OPIR_ERR_NO_MEMORY;
+  const opir_status st = guarded_to(&t->last_error, [&] {
+    if (is_c4(*scheme))
+      throw std::invalid_argument(
+          "the device-resident tree is built for CONFIG_N2048_K1_COMP; select the two-limb "
+          "levels with opir_tree_level_create / opir_tree_select_level");
+    t->tree = *tree;
+    t->device = device;
+    opir_params qp{};
+    if (opir_tree_query_params(tree, scheme, &qp) != OPIR_OK)
+      throw std::invalid_argument("tree parameters do not fit the scheme");
+    if (create_handle(checked_params(qp), device, &t->q) != OPIR_OK)
+      throw std::runtime_error("tree query handle could not be created");
+    for (uint64_t l = 0; l <= tree->L; ++l) {
+      if (!level_plaintexts[l]) throw std::invalid_argument("null level plaintexts");
+      opir_server *h = nullptr;
+      const opir_status ls = opir_tree_level_create(scheme, tree, l, level_plaintexts[l], device, &h);
+      if (ls != OPIR_OK)
+        throw std::runtime_error("tree level " + std::to_string(l) + " could not be created (status " +
+                                 std::to_string(ls) + ")");
+      t->levels.push_back(h);
+    }
+    DeviceGuard g(device);
+    ck(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreateWithFlags(&t->q_done, cudaEventDisableTiming), "event");
+    t->done.resize(t->levels.size(), nullptr);
+    for (auto &e : t->done) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    t->out.alloc((tree->L + 1) * 2ull * kN);
+    ensure_capacity(t->q, 1);  // no allocation while answering
+    grow_keyptr_slots(t->q, 2);
+    for (opir_server *l : t->levels) ensure_capacity(l, 1);
+  });
+  if (st != OPIR_OK) {
+    opir_tree_destroy(t);
+    return st;
+  }
+  *out = t;
+  return OPIR_OK;
+}
+
+opir_status opir_tree_set_client_keys(opir_tree *t, uint64_t client_id, const uint64_t *bv_keys,
+                                      const uint32_t *galois_ks, uint32_t n_keys,
+                                      const uint64_t *gsw_key) {
+  if (!t) return OPIR_ERR_INVALID_ARGUMENT;
+  const opir_status st = opir_server_set_client_keys(t->q, client_id, bv_keys, galois_ks, n_keys, gsw_key);
+  t->last_error = t->q->last_error;
+  return st;
+}
+
+opir_status opir_tree_query(opir_tree *t, uint64_t client_id, const uint64_t *query,
+                            uint64_t *selected) {
+  if (!t) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded_to(&t->last_error, [&] {
+    if (!query || !selected) throw std::invalid_argument("null argument");
+    opir_server *q = t->q;
+    DeviceGuard g(t->device);
+    check_query_values(q, query, 2 * kN);
+    // unpack_tree_query (src/tree_query.cpp:198-240) on the query handle
+    ensure_capacity(q, 1);
+    upload_keyptrs(q, &client_id, 1);
+    ck(cudaMemcpyAsync(q->q_u64.p, query, 2 * kN * 8, cudaMemcpyHostToDevice, q->stream), "upload");
+    opir::launch_split_u64(q->dp, q->q_u64.p, q->lvl[0].p, 1, 2, q->lvl_slots * kCtWords, q->stream);
+    const uint32_t *leaves = run_expand(q, 1);
+    opir::launch_selectors(q->dp, q->shape, leaves, q->lvl_slots, q->keyptrs.p + 1, q->sel.p, 1,
+                           q->stream);
+    ck(cudaEventRecord(t->q_done, q->stream), "event record");
+    // select_level of every level on its own stream, inputs device to device
+    const uint64_t sel_words = 2ull * q->params.l_ep * kCtWords;  // u32 words per selector
+    for (size_t l = 0; l < t->levels.size(); ++l) {
+      opir_server *ls = t->levels[l];
+      ck(cudaStreamWaitEvent(ls->stream, t->q_done, 0), "wait");
+      ck(cudaMemcpyAsync(ls->lvl[0].p, leaves, ls->shape.n0 * kCtWords * 4,
+                         cudaMemcpyDeviceToDevice, ls->stream), "alpha copy");
+      run_first_dim(ls, ls->lvl[0].p, 1);
+      const uint32_t fold = static_cast<uint32_t>(ls->fold_count);
+      for (uint32_t a = 1; a <= fold; ++a) {  // MSB-first: step a takes beta bit begin+count-a
+        const uint64_t u = ls->fold_begin + ls->fold_count - a;
+        ck(cudaMemcpyAsync(ls->sel.p + a * sel_words, q->sel.p + u * sel_words, sel_words * 4,
+                           cudaMemcpyDeviceToDevice, ls->stream), "selector copy");
+      }
+      for (uint32_t a = 1; a <= fold; ++a)
+        opir::launch_mux_level(ls->dp, ls->shape, a, ls->mid[(a - 1) & 1].p, ls->mid[a & 1].p,
+                               ls->shape.other, ls->sel.p, 1, ls->stream);
+      const uint32_t *res = fold ? ls->mid[fold & 1].p : ls->mid[0].p;
+      opir::launch_compose_u64(ls->dp, res, 0, t->out.p + l * 2ull * kN, 1, 2, ls->stream);
+      ck(cudaEventRecord(t->done[l], ls->stream), "event record");
+      ck(cudaStreamWaitEvent(t->stream, t->done[l], 0), "wait");
+    }
+    ck(cudaMemcpyAsync(selected, t->out.p, t->levels.size() * 2ull * kN * 8, cudaMemcpyDeviceToHost,
+                       t->stream), "download");
+    ck(cudaStreamSynchronize(t->stream), "tree query");
+    for (opir_server *ls : t->levels) check_device_error(ls);
   });
 }
 

@@ -232,3 +232,62 @@ class TreeLevel:
             msg = self._lib.opir_server_last_error(self._h)
             _raise(rc, msg.decode() if msg else f"status {rc}")
         return out
+
+
+class Tree:
+    """A whole device-resident tree (opir_tree_create): unpack + select_level
+    at every level per query with no host round trip between stages, the
+    levels running on their own streams (single-modulus set)."""
+
+    def __init__(self, scheme: PirParams, tree: TreePirParams, level_plaintexts, device: int = 0):
+        self.scheme, self.tree = scheme, tree
+        self._lib = L.load()
+        self._pts = []
+        for level, pts in enumerate(level_plaintexts):
+            a = np.ascontiguousarray(pts, dtype=np.uint64)
+            R = 1 << (level - tree.r) if level >= tree.r else 1
+            if a.shape != (R, tree.n):
+                raise ValueError(f"level {level} needs {R} x {tree.n} plaintext coefficients")
+            self._pts.append(a)
+        if len(self._pts) != tree.L + 1:
+            raise ValueError(f"a tree of height {tree.L} has {tree.L + 1} levels")
+        arr = (L.u64p * len(self._pts))(*[_ptr(a) for a in self._pts])
+        h = C.c_void_p()
+        rc = self._lib.opir_tree_create(C.byref(scheme._p), C.byref(tree._t), arr, device,
+                                        C.byref(h))
+        if rc != OPIR_OK:
+            _raise(rc, f"opir_tree_create failed (status {rc})")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.opir_tree_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != OPIR_OK:
+            msg = self._lib.opir_tree_last_error(self._h)
+            _raise(rc, msg.decode() if msg else f"status {rc}")
+
+    def set_client_keys(self, client_id: int, bv_keys: np.ndarray, gsw_key: np.ndarray):
+        bv = np.ascontiguousarray(bv_keys[: self.tree.h_q], dtype=np.uint64)
+        n_keys = bv.shape[0]
+        gk = np.ascontiguousarray([(self.tree.n >> i) + 1 for i in range(n_keys)], dtype=np.uint32)
+        g = np.ascontiguousarray(gsw_key, dtype=np.uint64)
+        self._check(self._lib.opir_tree_set_client_keys(self._h, client_id, _ptr(bv),
+                                                        _ptr(gk, C.c_uint32), n_keys, _ptr(g)))
+
+    def query(self, client_id: int, query: np.ndarray) -> np.ndarray:
+        """(L + 1) selected ciphertexts, level order."""
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        if q.shape != self.scheme.ct_shape:
+            raise ValueError(f"query must be {self.scheme.ct_shape}")
+        out = np.zeros((self.tree.L + 1,) + self.scheme.ct_shape, dtype=np.uint64)
+        self._check(self._lib.opir_tree_query(self._h, client_id, _ptr(q), _ptr(out)))
+        return out

@@ -281,7 +281,22 @@ int run_tree(const Args &a) {
   PirServer server(tree_query_expansion_params(tree, scheme));
   server.set_client_bv_galois_key(1, c.bv);
   server.set_client_gsw_key(1, c.gsw);
-  ExpandedTreeQuery un = unpack_tree_query(server, scheme, tree, 1, query);
+  const TreeNodeSource source = [&](size_t level, size_t index) {
+    return synthetic_tree_node_value(level, index, t);
+  };
+  const std::vector<TreeLevelDatabase> levels = preprocess_tree_reference(tree, source);
+  const std::vector<LevelPlan> plans = build_level_plans(tree);
+  // server-side time of one tree query: unpack + every level's select_level
+  const auto t0 = std::chrono::steady_clock::now();
+  RlweCt qcopy = query;
+  ExpandedTreeQuery un = unpack_tree_query(server, scheme, tree, 1, qcopy);
+  const AlphaPyramid pyramid = build_alpha_pyramid(un.alpha, tree, scheme);
+  std::vector<RlweCt> selected;
+  for (size_t level = 0; level <= tree.L; ++level)
+    selected.push_back(select_level(levels[level], plans[level], pyramid,
+                                    std::span<GSWCt>(un.beta_selectors), server, tree, scheme));
+  const double server_ms = std::chrono::duration<double, std::milli>(
+      std::chrono::steady_clock::now() - t0).count();
   v.clear();
   for (const auto &ct : un.alpha) { v.insert(v.end(), ct.c0.begin(), ct.c0.end());
                                     v.insert(v.end(), ct.c1.begin(), ct.c1.end()); }
@@ -289,17 +304,10 @@ int run_tree(const Args &a) {
   v.clear();
   for (const auto &g : un.beta_selectors) for (const auto &row : g) v.insert(v.end(), row.begin(), row.end());
   write_u64(a.out + "/beta.u64", v);
-  const AlphaPyramid pyramid = build_alpha_pyramid(un.alpha, tree, scheme);
-  const TreeNodeSource source = [&](size_t level, size_t index) {
-    return synthetic_tree_node_value(level, index, t);
-  };
-  const std::vector<TreeLevelDatabase> levels = preprocess_tree_reference(tree, source);
-  const std::vector<LevelPlan> plans = build_level_plans(tree);
   bool ok = true;
   v.clear();
   for (size_t level = 0; level <= tree.L; ++level) {
-    RlweCt sel = select_level(levels[level], plans[level], pyramid,
-                              std::span<GSWCt>(un.beta_selectors), server, tree, scheme);
+    const RlweCt &sel = selected[level];
     v.insert(v.end(), sel.c0.begin(), sel.c0.end());
     v.insert(v.end(), sel.c1.begin(), sel.c1.end());
     RlwePt dec;
@@ -309,8 +317,8 @@ int run_tree(const Args &a) {
   }
   write_u64(a.out + "/levels.u64", v);
   std::printf("{\"ok\": %s, \"N0\": %zu, \"b\": %zu, \"r\": %zu, \"h_q\": %zu, \"w\": %zu, "
-              "\"alpha\": %zu}\n", ok ? "true" : "false", tree.N0, tree.b, tree.r, tree.h_q,
-              tree.w, coords.alpha);
+              "\"alpha\": %zu, \"server_ms\": %.3f}\n", ok ? "true" : "false", tree.N0, tree.b,
+              tree.r, tree.h_q, tree.w, coords.alpha, server_ms);
   return ok ? 0 : 3;
 }
 

@@ -72,3 +72,26 @@ def test_views_refuse_out_of_scope_calls():
     bad[0, 0, 0] = scheme.q
     with pytest.raises(ValueError):
         lvl.select_level(bad, np.zeros((max(tree.b, 1), 12, 2, scheme.N), np.uint64))
+
+
+@functools.lru_cache(maxsize=None)
+def whole_tree(L, a):
+    scheme, tree, pts, _ = tree_levels(L, a)
+    return T.Tree(scheme, tree, pts)
+
+
+@pytest.mark.parametrize("c", CASES, ids=lambda c: c["name"])
+def test_device_resident_tree_matches_reference(c):
+    """opir_tree_query: the whole path in one call, levels on their own
+    streams, equal to the reference's select_level at every level."""
+    scheme, tree, pts, _ = tree_levels(c["L"], c["a"])
+    t = whole_tree(c["L"], c["a"])
+    cl = O.Client(O.params(scheme.target_num_pt, scheme.expansion_height), c["client_seed"])
+    bv, gsw = cl.bv_keys(), cl.gsw_key()
+    t.set_client_keys(c["client_seed"], bv, gsw)
+    coords = T.client_index(c["leaf"], tree)
+    q = cl.tree_query(tree.N0, tree.h_q, coords.alpha, coords.beta_bits_le, coords.gamma_bits_le)
+    for _ in range(2):     # a repeated query gives the same answer
+        out = t.query(c["client_seed"], q)
+        for level in range(tree.L + 1):
+            assert sha(out[level]) == c["sha256_levels_u64"][level], level
