@@ -95,12 +95,15 @@ typedef struct {
  * it; a handle only expands queries and completes selectors
  * (opir_server_expand_query, opir_server_complete_selectors).
  * OPIR_VIEW_MATRIX: a tree PIR level database (opir_tree_level_create),
- * answered by opir_tree_select_level. Calls outside a view's scope return
+ * answered by opir_tree_select_level. OPIR_VIEW_ROW_SHARD: one GPU's rows
+ * of a layout split across GPUs (opir_server_create_row_shard): loads and
+ * the row-shard query calls. Calls outside a view's scope return
  * OPIR_ERR_INVALID_ARGUMENT. */
 typedef enum {
   OPIR_VIEW_LAYOUT = 0,
   OPIR_VIEW_QUERY_SHAPE = 1,
-  OPIR_VIEW_MATRIX = 2
+  OPIR_VIEW_MATRIX = 2,
+  OPIR_VIEW_ROW_SHARD = 3
 } opir_view;
 
 /* PirQueryShapeConfig (includes/pir.h:46-50). */
@@ -225,6 +228,61 @@ opir_status opir_server_make_query_batch_device(opir_server *server, uint32_t n,
                                                 const uint64_t *d_queries,
                                                 uint64_t *d_responses,
                                                 void *stream);
+
+/* ---- row shards: one database across G GPUs ------------------------------
+ * No counterpart in the reference (one PirServer holds the whole database).
+ * A layout whose database exceeds one GPU is split by candidate rows over
+ * G = 2^k GPUs (1 <= G <= 2^(num_dims-2)). evaluate_other_dim
+ * (src/server.cpp:599-649) first pairs rows (level 0) into 2^(h-1)
+ * positions s (h = num_dims - 1) and then halves along the top bit of s;
+ * shard g holds the rows feeding the positions s with s mod G == g, so its
+ * MUX levels 0 .. h-k-1 stay on the GPU and leave one ciphertext: the full
+ * tree's level-(h-k) position g. The k remaining levels run on one shard
+ * over the G gathered ciphertexts, followed by the modulus switch; the
+ * response is bit for bit PirServer::make_query's.
+ *
+ * Rows of shard g in the order they are stored (database row indices;
+ * rows may be NULL to query only the count) and the MUX levels it answers. */
+opir_status opir_row_shard_rows(const opir_params *params, uint32_t shard,
+                                uint32_t num_shards, uint32_t *rows,
+                                uint64_t *n_rows, uint32_t *tree_h);
+/* A handle holding shard `shard` of `num_shards` of a layout (params of view
+ * OPIR_VIEW_LAYOUT; the handle reports view OPIR_VIEW_ROW_SHARD). Every load
+ * call takes the whole database's arguments (logical count, the full host
+ * array, or a source that is then called for the shard's plaintexts only,
+ * in increasing index order) and keeps the shard's rows. */
+opir_status opir_server_create_row_shard(const opir_params *params,
+                                         uint32_t shard, uint32_t num_shards,
+                                         int device, opir_server **out);
+/* The shard's part of make_query for n queries: expansion and selectors
+ * (replicated on every shard), the first dimension over the shard's rows and
+ * its MUX levels. partials: n ciphertexts in the query layout
+ * ([c0 K*N][c1 K*N] u64, coefficient form mod each limb). The handle keeps
+ * the batch's selectors for opir_server_combine_shards. */
+opir_status opir_server_make_query_shard_batch(opir_server *server, uint32_t n,
+                                               const uint64_t *client_ids,
+                                               const uint64_t *queries,
+                                               uint64_t *partials);
+/* Device-buffer form, enqueued like opir_server_make_query_batch_device. */
+opir_status opir_server_make_query_shard_batch_device(opir_server *server,
+                                                      uint32_t n,
+                                                      const uint64_t *client_ids,
+                                                      const uint64_t *d_queries,
+                                                      uint64_t *d_partials,
+                                                      void *stream);
+/* Finishes n queries on a shard whose last make_query_shard batch had the
+ * same client ids in the same order (else OPIR_ERR_INVALID_ARGUMENT):
+ * partials = G x n ciphertexts, shard-major (shard g's batch output at
+ * g * n), responses = n x 2N u64 mod small_q, as opir_server_make_query. */
+opir_status opir_server_combine_shards(opir_server *server, uint32_t n,
+                                       const uint64_t *client_ids,
+                                       const uint64_t *partials,
+                                       uint64_t *responses);
+opir_status opir_server_combine_shards_device(opir_server *server, uint32_t n,
+                                              const uint64_t *client_ids,
+                                              const uint64_t *d_partials,
+                                              uint64_t *d_responses,
+                                              void *stream);
 
 /* ---- device memory planning ---------------------------------------------
  * No counterpart in the reference (its server grows host vectors as it

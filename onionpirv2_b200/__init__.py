@@ -5,7 +5,7 @@ include/onionpir_b200.h); this package is the host-side mirror of the
 reference's PirParams / PirServer interface over that ABI.
 """
 from .server import (DeviceError, OutOfRange, PirParams, PirServer,  # noqa: F401
-                     plan_memory, save_response)
+                     RowShardServer, plan_memory, row_shard_rows, save_response)
 
-__all__ = ["PirParams", "PirServer", "save_response", "plan_memory", "OutOfRange",
-           "DeviceError"]
+__all__ = ["PirParams", "PirServer", "RowShardServer", "row_shard_rows", "save_response",
+           "plan_memory", "OutOfRange", "DeviceError"]

@@ -102,6 +102,16 @@ _SIGS = {
     "opir_server_make_query_batch": ([C.c_void_p, C.c_uint32, u64p, u64p, u64p], C.c_int),
     "opir_server_make_query_batch_device": ([C.c_void_p, C.c_uint32, u64p, C.c_void_p,
                                              C.c_void_p, C.c_void_p], C.c_int),
+    "opir_row_shard_rows": ([C.POINTER(Params), C.c_uint32, C.c_uint32, u32p, u64p, u32p],
+                            C.c_int),
+    "opir_server_create_row_shard": ([C.POINTER(Params), C.c_uint32, C.c_uint32, C.c_int,
+                                      C.POINTER(C.c_void_p)], C.c_int),
+    "opir_server_make_query_shard_batch": ([C.c_void_p, C.c_uint32, u64p, u64p, u64p], C.c_int),
+    "opir_server_make_query_shard_batch_device": ([C.c_void_p, C.c_uint32, u64p, C.c_void_p,
+                                                   C.c_void_p, C.c_void_p], C.c_int),
+    "opir_server_combine_shards": ([C.c_void_p, C.c_uint32, u64p, u64p, u64p], C.c_int),
+    "opir_server_combine_shards_device": ([C.c_void_p, C.c_uint32, u64p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p], C.c_int),
     "opir_plan_memory": ([C.POINTER(Params), C.POINTER(MemoryPlan)], C.c_int),
     "opir_server_reserve": ([C.c_void_p, C.c_uint32], C.c_int),
     "opir_server_autotune": ([C.c_void_p, C.c_uint32], C.c_int),

@@ -100,19 +100,22 @@ __device__ __forceinline__ void db_body(const Dev4 &P, const uint64_t *coeffs,
                                         uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
                                         uint64_t logical, uint32_t n0, uint32_t n0p,
                                         uint32_t other, uint64_t pt_begin, uint64_t pt_end,
-                                        uint8_t *db8) {
+                                        const uint32_t *row_map, uint8_t *db8) {
   extern __shared__ uint64_t sm4[];
   const int tid = threadIdx.x;
   const uint64_t pt0 = pt_begin + static_cast<uint64_t>(blockIdx.x) * kDbTile;
   for (int e = 0; e < kDbTile; ++e) {
     const uint64_t pt = pt0 + e;
+    // the database plaintext stored at local position pt (a row shard keeps
+    // some of the rows; pt < pt_end keeps pt / n0 below the shard's rows)
+    const uint64_t gpt = (row_map && pt < pt_end) ? static_cast<uint64_t>(row_map[pt / n0]) * n0 + pt % n0 : pt;
     uint64_t v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int c = posA(tid, k);
       uint64_t x = 0;
-      if (pt < pt_end && pt < logical)
-        x = coeffs ? coeffs[(pt - coeff_pt_begin) * kN + c] : mix64(seed + (pt * kN + c + 1) * kGolden) % t;
+      if (pt < pt_end && gpt < logical)
+        x = coeffs ? coeffs[(pt - coeff_pt_begin) * kN + c] : mix64(seed + (gpt * kN + c + 1) * kGolden) % t;
       v[k] = x;  // x < t < q: canonical (server.cpp:172-180 reduces pt mod q_k)
     }
     fA<L>(v);
@@ -168,11 +171,12 @@ __device__ __forceinline__ void db_body(const Dev4 &P, const uint64_t *coeffs,
 __global__ void __launch_bounds__(kThreads, 1)
 k4_db_preprocess(Dev4 P, const uint64_t *__restrict__ coeffs, uint64_t coeff_pt_begin,
                  uint64_t seed, uint64_t t, uint64_t logical, uint32_t n0, uint32_t n0p,
-                 uint32_t other, uint64_t pt_begin, uint64_t pt_end, uint8_t *__restrict__ db8) {
+                 uint32_t other, uint64_t pt_begin, uint64_t pt_end,
+                 const uint32_t *__restrict__ row_map, uint8_t *__restrict__ db8) {
   if (blockIdx.y == 0)
-    db_body<0>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin, pt_end, db8);
+    db_body<0>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin, pt_end, row_map, db8);
   else
-    db_body<1>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin, pt_end, db8);
+    db_body<1>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin, pt_end, row_map, db8);
 }
 
 // ------------------------------------------------------------ expansion level
@@ -720,14 +724,16 @@ void upload_constants(const uint64_t *const fw[2], const uint64_t *const fw_sh[2
 
 void launch_db_preprocess(const Dev4 &P, const Shape4 &s, const uint64_t *coeffs,
                           uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
-                          uint64_t pt_begin, uint64_t pt_end, uint8_t *db8, cudaStream_t st) {
+                          uint64_t pt_begin, uint64_t pt_end, const uint32_t *row_map,
+                          uint8_t *db8, cudaStream_t st) {
   if (pt_begin % kDbTile != 0) throw std::invalid_argument("db tiles start at a multiple of 4");
+  if (pt_end > static_cast<uint64_t>(s.other) * s.n0) throw std::invalid_argument("db tile beyond the layout");
   const size_t smem = plane_bytes(kDbTile);
   set_smem(k4_db_preprocess, smem);
   const uint64_t tiles = (pt_end - pt_begin + kDbTile - 1) / kDbTile;
   dim3 grid(static_cast<unsigned>(tiles), 2);
   k4_db_preprocess<<<grid, kThreads, smem, st>>>(P, coeffs, coeff_pt_begin, seed, t, logical, s.n0,
-                                                   s.n0p, s.other, pt_begin, pt_end, db8);
+                                                   s.n0p, s.other, pt_begin, pt_end, row_map, db8);
   check_launch("k4_db_preprocess");
 }
 
@@ -796,13 +802,15 @@ void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint6
   check_launch("k4_epilogue");
 }
 
-void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, const uint64_t *in,
-                      uint64_t *out, uint64_t mid_stride, const uint64_t *sel, uint32_t batch,
-                      cudaStream_t st) {
-  const uint32_t h = s.num_dims - 1;
+void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, uint32_t tree_h,
+                      const uint64_t *in, uint64_t *out, uint64_t mid_stride, const uint64_t *sel,
+                      uint32_t batch, cudaStream_t st) {
+  const uint32_t h = tree_h;
+  if (h == 0 || h > 31 || level >= h || h > s.num_dims - 1)
+    throw std::invalid_argument("MUX level outside its selector tree");
   const uint32_t other = s.other;
   uint32_t n_pairs, offset = 0, half = 0, extra = 0;
-  if (other > (1u << h) || 2ull * other < (1ull << h))
+  if (level == 0 && (other > (1u << h) || 2ull * other < (1ull << h)))
     throw std::invalid_argument("MUX tree: candidate count outside (2^(d-2), 2^(d-1)]");
   if (level == 0) {
     const uint32_t last = 2 * other - (1u << h);

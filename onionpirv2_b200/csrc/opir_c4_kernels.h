@@ -63,9 +63,13 @@ uint32_t expand_nodes(const Shape4 &s, uint32_t d);
 // server.cpp:80-203: plaintexts [pt_begin, pt_end) -> NTT per limb -> db.
 // coeffs (device, u64 < t) holds plaintexts from coeff_pt_begin on; null
 // generates coefficient(pt, c) = mix64(seed + (pt N + c + 1) golden) % t.
+// row_map (device, one entry per row of s; null = identity) names the
+// database row stored at each row of a row shard: generated coefficients and
+// the logical bound use the database index row_map[pt / n0] n0 + pt % n0.
 void launch_db_preprocess(const Dev4 &P, const Shape4 &s, const uint64_t *coeffs,
                           uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
-                          uint64_t pt_begin, uint64_t pt_end, uint8_t *db8, cudaStream_t st);
+                          uint64_t pt_begin, uint64_t pt_end, const uint32_t *row_map,
+                          uint8_t *db8, cudaStream_t st);
 // One expansion level for `batch` queries; bv_keys: device array of per-query
 // key pointers.
 void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint64_t *in,
@@ -81,9 +85,12 @@ void launch_fst_pack(const Shape4 &s, const uint64_t *qm, uint8_t *qb, uint32_t 
                      cudaStream_t st);
 void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint64_t *mid,
                      uint64_t mid_stride, uint32_t batch, cudaStream_t st);
-void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, const uint64_t *in,
-                      uint64_t *out, uint64_t mid_stride, const uint64_t *sel, uint32_t batch,
-                      cudaStream_t st);
+// One MUX level in a selector tree of height tree_h (num_dims - 1 for a
+// whole layout, less on a row shard); level 0 carries the unpaired prefix
+// 2^tree_h - s.other, level a >= 1 pairs (i, i + 2^(tree_h-a-1)).
+void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, uint32_t tree_h,
+                      const uint64_t *in, uint64_t *out, uint64_t mid_stride, const uint64_t *sel,
+                      uint32_t batch, cudaStream_t st);
 // Modulus switch + (optional) bit packing of `batch` results; resp: 2N u64 per query.
 void launch_modswitch(const Dev4 &P, const uint64_t *ct, uint64_t ct_stride, uint64_t *resp,
                       uint8_t *bytes, uint32_t resp_bytes, uint32_t batch, cudaStream_t st);

@@ -81,8 +81,21 @@ Plan plan_for(const Shape4 &s, uint64_t lvl_slots, uint32_t n) {
 
 opir_params derive(const opir_layout &layout) { return opir::derive_params_c4(layout); }
 
-Server::Server(const opir_params &p, cudaStream_t stream) : p_(p), st_(stream) {
+Server::Server(const opir_params &p, cudaStream_t stream, const opir::RowShard *rs)
+    : p_(p), st_(stream) {
   sh_ = shape_of(p_);
+  tree_h_ = sh_.num_dims > 1 ? sh_.num_dims - 1 : 0;
+  if (rs) {
+    tree_h_ = rs->tree_h;
+    num_shards_ = rs->num_shards;
+    host_rows_ = rs->rows;
+    sh_.other = static_cast<uint32_t>(rs->rows.size());
+    sh_.num_pt = static_cast<uint64_t>(sh_.other) * sh_.n0;
+    out_words_ = kCt;
+    row_map_.alloc(rs->rows.size());
+    ck(cudaMemcpy(row_map_.p, rs->rows.data(), rs->rows.size() * 4, cudaMemcpyHostToDevice),
+       "row map");
+  }
   lvl_slots_ = lvl_slots_of(sh_);
   const opir::LimbTables64 t[2] = {opir::make_limb_tables64(kN, p_.q1, p_.w1),
                                    opir::make_limb_tables64(kN, p_.q2, p_.w2)};
@@ -140,20 +153,19 @@ template <typename Fill>
 void Server::load_tiles(uint64_t logical, Fill &&fill) {
   if (logical > p_.num_pt)
     throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
+  const uint64_t local_pt = static_cast<uint64_t>(sh_.other) * sh_.n0;
   const uint64_t tile = 2048;
   std::vector<uint64_t> host(tile * kN);
   opir::DevBuf<uint64_t> dev;
   dev.alloc(tile * kN);
   db_loaded_ = false;
-  for (uint64_t pb = 0; pb < p_.num_pt; pb += tile) {
-    const uint64_t pe = std::min<uint64_t>(p_.num_pt, pb + tile);
-    const uint64_t real_end = std::min<uint64_t>(pe, logical);
-    if (pb < real_end) {
-      fill(pb, real_end, host.data());
-      ck(cudaMemcpyAsync(dev.p, host.data(), (real_end - pb) * kN * 8, cudaMemcpyHostToDevice, st_),
-         "db upload");
-    }
-    launch_db_preprocess(dp_, sh_, dev.p, pb, 0, p_.plain_mod, logical, pb, pe, db8_.p, st_);
+  for (uint64_t pb = 0; pb < local_pt; pb += tile) {
+    const uint64_t pe = std::min<uint64_t>(local_pt, pb + tile);
+    opir::fill_runs(host_rows_, sh_.n0, logical, pb, pe, host.data(), fill, kN);
+    ck(cudaMemcpyAsync(dev.p, host.data(), (pe - pb) * kN * 8, cudaMemcpyHostToDevice, st_),
+       "db upload");
+    launch_db_preprocess(dp_, sh_, dev.p, pb, 0, p_.plain_mod, logical, pb, pe, row_map_.p, db8_.p,
+                         st_);
     ck(cudaStreamSynchronize(st_), "db preprocess");
   }
   db_loaded_ = true;
@@ -196,9 +208,10 @@ void Server::load_db_seeded(uint64_t logical, uint64_t seed) {
     throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
   db_loaded_ = false;
   const uint64_t chunk = 1ull << 18;
-  for (uint64_t pb = 0; pb < p_.num_pt; pb += chunk)
+  const uint64_t local_pt = static_cast<uint64_t>(sh_.other) * sh_.n0;
+  for (uint64_t pb = 0; pb < local_pt; pb += chunk)
     launch_db_preprocess(dp_, sh_, nullptr, 0, seed, p_.plain_mod, logical, pb,
-                         std::min<uint64_t>(p_.num_pt, pb + chunk), db8_.p, st_);
+                         std::min<uint64_t>(local_pt, pb + chunk), row_map_.p, db8_.p, st_);
   ck(cudaStreamSynchronize(st_), "db preprocess");
   db_loaded_ = true;
 }
@@ -275,7 +288,7 @@ void Server::ensure_capacity(uint32_t n) {
   for (auto &b : lvl_) b.alloc(pl.lvl);
   sel_.alloc(pl.sel);
   for (auto &b : mid_) b.alloc(pl.mid);
-  resp_.alloc(pl.resp);
+  resp_.alloc(static_cast<size_t>(n) * out_words_);
   q_in_.alloc(static_cast<size_t>(n) * kCt);
   keyptrs_.alloc(pl.keyptrs);
   cap_ = n;
@@ -408,10 +421,10 @@ void Server::run_first_dim(const uint64_t *leaves, uint32_t n, Events ev) {
 }
 
 const uint64_t *Server::run_other_dims(uint32_t n) {
-  if (sh_.num_dims <= 1) return mid_[0].p;
-  const uint32_t levels = sh_.num_dims - 1;
+  const uint32_t levels = tree_h_;
   for (uint32_t a = 0; a < levels; ++a)
-    launch_mux_level(dp_, sh_, a, mid_[a & 1].p, mid_[(a + 1) & 1].p, sh_.other, sel_.p, n, st_);
+    launch_mux_level(dp_, sh_, a, levels, mid_[a & 1].p, mid_[(a + 1) & 1].p, sh_.other, sel_.p, n,
+                     st_);
   return mid_[levels & 1].p;
 }
 
@@ -428,7 +441,11 @@ void Server::enqueue_core(uint32_t n, const uint64_t *d_queries, uint64_t *d_res
   mark(ev, 3);
   const uint64_t *res = run_other_dims(n);
   mark(ev, 4);
-  launch_modswitch(dp_, res, sh_.other, d_resp, nullptr, resp_bytes_of(p_), n, st_);
+  if (out_words_ == kCt)  // row shard: the partial ciphertext, before the last levels
+    ck(cudaMemcpy2DAsync(d_resp, kCt * 8, res, static_cast<size_t>(sh_.other) * kCt * 8, kCt * 8, n,
+                         cudaMemcpyDeviceToDevice, st_), "partial copy");
+  else
+    launch_modswitch(dp_, res, sh_.other, d_resp, nullptr, resp_bytes_of(p_), n, st_);
   mark(ev, 5);
 }
 
@@ -505,7 +522,7 @@ void Server::run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_que
                        cudaMemcpyDeviceToDevice, st_), "query staging");
   launch_graph(n, ev);
   if (d_resp != resp_.p)
-    ck(cudaMemcpyAsync(d_resp, resp_.p, static_cast<size_t>(n) * 2 * kN * 8,
+    ck(cudaMemcpyAsync(d_resp, resp_.p, static_cast<size_t>(n) * out_words_ * 8,
                        cudaMemcpyDeviceToDevice, st_), "response copy");
 }
 
@@ -518,9 +535,39 @@ void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *q
   ck(cudaMemcpyAsync(q_in_.p, queries, static_cast<size_t>(n) * kCt * 8, cudaMemcpyHostToDevice,
                      st_), "query upload");
   run_pipeline(n, ids, q_in_.p, resp_.p, ev);
-  ck(cudaMemcpyAsync(responses, resp_.p, static_cast<size_t>(n) * 2 * kN * 8,
+  ck(cudaMemcpyAsync(responses, resp_.p, static_cast<size_t>(n) * out_words_ * 8,
                      cudaMemcpyDeviceToHost, st_), "response download");
   ck(cudaStreamSynchronize(st_), "make_query");
+  check_device_error();
+}
+
+void Server::combine_device(uint32_t n, const uint64_t *d_partials, uint64_t *d_responses) {
+  if (out_words_ != kCt) throw std::invalid_argument("combine_shards needs a row shard");
+  const uint32_t G = num_shards_, h = sh_.num_dims - 1;
+  const uint64_t words = static_cast<uint64_t>(n) * G * kCt;
+  for (auto &b : comb_)
+    if (b.n < words) b.alloc(words);
+  for (uint32_t g = 0; g < G; ++g)  // query i's G ciphertexts side by side
+    ck(cudaMemcpy2DAsync(comb_[0].p + static_cast<uint64_t>(g) * kCt, static_cast<size_t>(G) * kCt * 8,
+                         d_partials + static_cast<uint64_t>(g) * n * kCt, kCt * 8, kCt * 8, n,
+                         cudaMemcpyDeviceToDevice, st_), "partial gather");
+  int cur = 0;
+  for (uint32_t a = tree_h_; a < h; ++a, cur ^= 1)
+    launch_mux_level(dp_, sh_, a, h, comb_[cur].p, comb_[cur ^ 1].p, G, sel_.p, n, st_);
+  launch_modswitch(dp_, comb_[cur].p, G, d_responses, nullptr, resp_bytes_of(p_), n, st_);
+}
+
+void Server::combine_host(uint32_t n, const uint64_t *partials, uint64_t *responses) {
+  const size_t cts = static_cast<size_t>(num_shards_) * n;
+  check_ct_values(partials, cts);
+  opir::DevBuf<uint64_t> d_in, d_out;
+  d_in.alloc(cts * kCt);
+  d_out.alloc(static_cast<size_t>(n) * 2 * kN);
+  ck(cudaMemcpyAsync(d_in.p, partials, cts * kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  combine_device(n, d_in.p, d_out.p);
+  ck(cudaMemcpyAsync(responses, d_out.p, static_cast<size_t>(n) * 2 * kN * 8,
+                     cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaStreamSynchronize(st_), "combine_shards");
   check_device_error();
 }
 
@@ -614,7 +661,8 @@ void Server::select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32
     ck(cudaMemcpyAsync(sel_.p + 2ull * sh_.l_ep * kRowWords, rows.data(), rows.size() * 8,
                        cudaMemcpyHostToDevice, st_), "upload");
     for (uint32_t a = 1; a <= fold; ++a)
-      launch_mux_level(dp_, sh_, a, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other, sel_.p, 1, st_);
+      launch_mux_level(dp_, sh_, a, sh_.num_dims - 1, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other,
+                       sel_.p, 1, st_);
     res = mid_[fold & 1].p;
   }
   ck(cudaMemcpyAsync(out, res, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");

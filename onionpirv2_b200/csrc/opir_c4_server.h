@@ -16,6 +16,7 @@
 #include "../../include/onionpir_b200.h"
 #include "opir_c4_kernels.h"
 #include "opir_host.h"
+#include "opir_shard.h"
 
 namespace opir4 {
 
@@ -26,7 +27,10 @@ class Server {
   using Events = cudaEvent_t *;
   static constexpr int kMarks = 8;
 
-  Server(const opir_params &p, cudaStream_t stream);
+  // rs: a row shard of the layout (opir_shard.h): the database holds the
+  // shard's rows, make_query returns the shard's partial ciphertext (4N u64)
+  // after MUX levels 0 .. rs->tree_h - 1, and combine_* finishes the tree.
+  Server(const opir_params &p, cudaStream_t stream, const opir::RowShard *rs = nullptr);
   Server(const Server &) = delete;
   Server &operator=(const Server &) = delete;
   ~Server();
@@ -44,7 +48,8 @@ class Server {
                        uint32_t n_keys, const uint64_t *gsw_key);
   void remove_client(uint64_t id);
 
-  // Host buffers: n queries of 4N u64 in, n responses of 2N u64 out.
+  // Host buffers: n queries of 4N u64 in, n responses of 2N u64 out (row
+  // shard: n partial ciphertexts of 4N u64).
   void make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *queries,
                         uint64_t *responses, Events ev);
   // Device buffers, enqueued on the handle's stream (no wait).
@@ -58,6 +63,11 @@ class Server {
   void complete_selectors(uint64_t id, const uint64_t *expanded, uint64_t *out);
   void evaluate_first_dim(const uint64_t *fst_query, uint64_t *out);
   void evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, uint64_t *out);
+  // Row shards: the last log2 G MUX levels over each query's G partial
+  // ciphertexts (G x n x 4N u64, shard-major), with the selectors of this
+  // handle's last batch, then the modulus switch (n x 2N u64 out).
+  void combine_host(uint32_t n, const uint64_t *partials, uint64_t *responses);
+  void combine_device(uint32_t n, const uint64_t *d_partials, uint64_t *d_responses);
   // Tree level handles: first dimension over the n0 ciphertexts, then `fold`
   // MUX steps at levels 1..fold (selector slot a = step a), host buffers.
   void select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32_t fold, uint64_t *out);
@@ -103,6 +113,12 @@ class Server {
   opir::DevBuf<uint32_t> progress_;  // scan CTA pairing counters
   int sm_count_ = 148;
   bool db_loaded_ = false;
+  // MUX levels answered here; on a row shard the rows kept (local -> database)
+  uint32_t tree_h_ = 0, num_shards_ = 1;
+  std::vector<uint32_t> host_rows_;
+  opir::DevBuf<uint32_t> row_map_;
+  opir::DevBuf<uint64_t> comb_[2];
+  uint64_t out_words_ = 2ull * kN;  // per query out of make_query: 2N, or 4N on a shard
   std::unordered_map<uint64_t, Keys> clients_;
   uint32_t cap_ = 0;
   uint64_t lvl_slots_ = 1;

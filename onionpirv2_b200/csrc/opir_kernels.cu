@@ -88,23 +88,27 @@ __device__ __forceinline__ void db_preprocess_body(const DevParams &P, const uin
                                                    uint64_t coeff_pt_begin, uint64_t seed,
                                                    uint64_t t, uint64_t logical, uint32_t n0,
                                                    uint32_t n0p, uint32_t other, uint64_t pt_begin,
-                                                   uint64_t pt_end, uint8_t *db8) {
+                                                   uint64_t pt_end, const uint32_t *row_map,
+                                                   uint8_t *db8) {
   extern __shared__ uint32_t sm[];
   const int tid = threadIdx.x;
   const ResidueTables &T = P.r[RES];
   const uint64_t pt0 = pt_begin + (uint64_t)blockIdx.x * kDbTile;
   for (int e = 0; e < kDbTile; ++e) {
     const uint64_t pt = pt0 + e;
+    // the database plaintext stored at local position pt (a row shard keeps
+    // some of the rows; pt < pt_end keeps pt / n0 below the shard's rows)
+    const uint64_t gpt = (row_map && pt < pt_end) ? (uint64_t)row_map[pt / n0] * n0 + pt % n0 : pt;
     uint32_t v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int c = posA(tid, k);
       uint32_t x = 0;
-      if (pt < pt_end && pt < logical) {
+      if (pt < pt_end && gpt < logical) {
         if (coeffs != nullptr)
           x = coeffs[(pt - coeff_pt_begin) * kN + c];
         else
-          x = static_cast<uint32_t>(mix64(seed + (pt * kN + c + 1) * kGolden) % t);
+          x = static_cast<uint32_t>(mix64(seed + (gpt * kN + c + 1) * kGolden) % t);
       }
       v[k] = x;  // x < t < q_res: canonical
     }
@@ -157,13 +161,14 @@ __global__ void __launch_bounds__(kThreads, 2)
 k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
                 uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
                 uint64_t logical, uint32_t n0, uint32_t n0p, uint32_t other,
-                uint64_t pt_begin, uint64_t pt_end, uint8_t *__restrict__ db8) {
+                uint64_t pt_begin, uint64_t pt_end, const uint32_t *__restrict__ row_map,
+                uint8_t *__restrict__ db8) {
   if (blockIdx.y == 0)
     db_preprocess_body<0>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin,
-                          pt_end, db8);
+                          pt_end, row_map, db8);
   else
     db_preprocess_body<1>(P, coeffs, coeff_pt_begin, seed, t, logical, n0, n0p, other, pt_begin,
-                          pt_end, db8);
+                          pt_end, row_map, db8);
 }
 
 // ----------------------------------------------------------- expansion level
@@ -839,14 +844,16 @@ void launch_compose_u64(const DevParams &P, const uint32_t *in, uint64_t in_item
 
 void launch_db_preprocess(const DevParams &P, const Shape &s, const uint16_t *coeffs,
                           uint64_t coeff_pt_begin, uint64_t seed, uint64_t t, uint64_t logical,
-                          uint64_t pt_begin, uint64_t pt_end, uint8_t *db8, cudaStream_t st) {
+                          uint64_t pt_begin, uint64_t pt_end, const uint32_t *row_map,
+                          uint8_t *db8, cudaStream_t st) {
   if (pt_end <= pt_begin) return;
+  if (pt_end > static_cast<uint64_t>(s.other) * s.n0) throw std::invalid_argument("db tile beyond the layout");
   const size_t smem = kDbTile * kPad * sizeof(uint32_t);
   set_smem(k_db_preprocess, smem);
   const uint64_t tiles = (pt_end - pt_begin + kDbTile - 1) / kDbTile;
   dim3 grid(static_cast<unsigned>(tiles), 2);
   k_db_preprocess<<<grid, kThreads, smem, st>>>(P, coeffs, coeff_pt_begin, seed, t, logical, s.n0,
-                                                 s.n0p, s.other, pt_begin, pt_end, db8);
+                                                 s.n0p, s.other, pt_begin, pt_end, row_map, db8);
   check_launch("k_db_preprocess");
 }
 
@@ -940,11 +947,13 @@ void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cm
   check_launch("k_scan_epilogue");
 }
 
-void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, const uint32_t *in,
-                      uint32_t *out, uint64_t mid_stride, const uint32_t *sel, uint32_t batch,
-                      cudaStream_t st) {
+void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32_t tree_h,
+                      const uint32_t *in, uint32_t *out, uint64_t mid_stride, const uint32_t *sel,
+                      uint32_t batch, cudaStream_t st) {
   check_gadgets(s);
-  const uint32_t h = s.num_dims - 1;
+  const uint32_t h = tree_h;
+  if (h == 0 || h > 31 || level >= h || h > s.num_dims - 1)
+    throw std::invalid_argument("MUX level outside its selector tree");
   uint32_t n_pairs, offset = 0, half = 0, copies = 0;
   if (level == 0 && (s.other > (1u << h) || 2ull * s.other < (1ull << h)))
     throw std::invalid_argument("MUX tree: candidate count outside (2^(d-2), 2^(d-1)]");

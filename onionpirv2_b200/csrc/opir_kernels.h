@@ -45,10 +45,13 @@ void launch_compose_u64(const DevParams &P, const uint32_t *in, uint64_t in_item
 // byte planes db8[((res N + level) 4 + plane) other + row][n0p] with
 // pt = row n0 + k. Covers plaintexts [pt_begin, pt_end); rows >= logical are
 // zero. Padding bytes (k >= n0) are never written: the buffer starts zeroed.
+// row_map (device, one entry per row of s; null = identity) names the
+// database row stored at each row of a row shard: generated coefficients and
+// the logical bound use the database index row_map[pt / n0] n0 + pt % n0.
 void launch_db_preprocess(const DevParams &P, const Shape &s, const uint16_t *coeffs,
                           uint64_t coeff_pt_begin, uint64_t seed, uint64_t t,
                           uint64_t logical, uint64_t pt_begin, uint64_t pt_end,
-                          uint8_t *db8, cudaStream_t st);
+                          const uint32_t *row_map, uint8_t *db8, cudaStream_t st);
 
 // One expansion level d over `batch` queries. in: batch x in_stride cts,
 // out: batch x out_stride cts. bv_level[b] points at the (galois level d) key
@@ -95,11 +98,13 @@ void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cm
                           uint32_t *mid, uint64_t mid_stride, uint32_t batch,
                           cudaStream_t st);
 
-// One MUX level of evaluate_other_dim (src/server.cpp:599-722).
+// One MUX level of evaluate_other_dim (src/server.cpp:599-722) in a selector
+// tree of height tree_h (num_dims - 1 for a whole layout, less on a row
+// shard), selector slot `level` of each query's set:
 // level 0: pairs (offset + 2i, offset + 2i + 1) -> out[offset + i], and
-//          out[0, offset) = in[0, offset);
-// level a >= 1: pairs (i, i + half) -> out[i], i < half.
-void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level,
+//          out[0, offset) = in[0, offset), offset = 2^tree_h - s.other;
+// level a >= 1: pairs (i, i + half) -> out[i], i < half = 2^(tree_h-a-1).
+void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32_t tree_h,
                       const uint32_t *in, uint32_t *out, uint64_t mid_stride,
                       const uint32_t *sel, uint32_t batch, cudaStream_t st);
 

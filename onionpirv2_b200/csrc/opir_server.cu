@@ -24,6 +24,7 @@
 #include "opir_kernels.h"
 #include "opir_params.h"
 #include "opir_scan_tc.h"
+#include "opir_shard.h"
 #include "opir_tree.h"
 
 namespace {
@@ -112,6 +113,16 @@ struct opir_server {
   std::unique_ptr<opir4::Server> c4;
   // tree level handles (view OPIR_VIEW_MATRIX): the plan's beta fold
   uint64_t tree_b = 0, fold_begin = 0, fold_count = 0;
+  // MUX levels answered by make_query: num_dims - 1, or h - log2 G on a row
+  // shard (view OPIR_VIEW_ROW_SHARD, opir_shard.h), whose rows are
+  // row_map's database rows and whose last batch's client ids are
+  // shard_ids (their selectors stay in `sel` for opir_server_combine_shards)
+  uint32_t tree_h = 0;
+  uint32_t shard = 0, num_shards = 1;
+  std::vector<uint32_t> host_rows;
+  DevBuf<uint32_t> row_map;
+  std::vector<uint64_t> shard_ids;
+  DevBuf<uint32_t> comb[2];  // combine: n x num_shards ciphertext slots
   // captured pipelines (see run_pipeline); a key is captured on its second use
   bool use_graphs = true;
   std::map<GraphKey, GraphEntry> graphs;
@@ -483,13 +494,14 @@ void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n) {
 // Remaining dimensions: returns the buffer whose slot 0 holds the result.
 uint32_t *run_other_dims(opir_server *s, uint32_t n) {
   const opir::Shape &sh = s->shape;
-  if (sh.num_dims <= 1) return s->mid[0].p;
-  const uint32_t levels = sh.num_dims - 1;
+  const uint32_t levels = s->tree_h;
   for (uint32_t a = 0; a < levels; ++a)
-    opir::launch_mux_level(s->dp, sh, a, s->mid[a & 1].p, s->mid[(a + 1) & 1].p, sh.other,
+    opir::launch_mux_level(s->dp, sh, a, levels, s->mid[a & 1].p, s->mid[(a + 1) & 1].p, sh.other,
                            s->sel.p, n, s->stream);
   return s->mid[levels & 1].p;
 }
+
+bool is_row_shard(const opir_server *s) { return s->params.view == OPIR_VIEW_ROW_SHARD; }
 
 // The kernels of one make_query batch, from queries in d_queries to
 // responses in d_resp (key pointers already uploaded). Stage marks are
@@ -507,8 +519,11 @@ void enqueue_core(opir_server *s, uint32_t n, const uint64_t *d_queries, uint64_
   mark(s, 3);
   const uint32_t *res = run_other_dims(s, n);
   mark(s, 4);
-  opir::launch_modswitch(s->dp, res, sh.other, d_resp, d_bytes, resp_bytes_of(s->params), n,
-                         s->stream);
+  if (is_row_shard(s))  // the shard's partial ciphertext, mod q, before the last levels
+    opir::launch_compose_u64(s->dp, res, sh.other * kCtWords, d_resp, n, 2, s->stream);
+  else
+    opir::launch_modswitch(s->dp, res, sh.other, d_resp, d_bytes, resp_bytes_of(s->params), n,
+                           s->stream);
   mark(s, 5);
 }
 
@@ -618,27 +633,27 @@ void check_query_values(const opir_server *s, const uint64_t *q, size_t count) {
     if (q[i] >= s->params.q) throw std::invalid_argument("query coefficient not reduced mod q");
 }
 
-// Database upload in tiles of plaintexts (u16 coefficients).
+// Database upload in tiles of plaintexts (u16 coefficients). fill(b, e, dst)
+// writes database plaintexts [b, e) to dst; on a row shard it is called for
+// the shard's plaintexts only, in increasing order.
 template <typename Fill>
 void load_tiles(opir_server *s, uint64_t logical, Fill &&fill) {
   const opir_params &p = s->params;
   if (logical > p.num_pt)
     throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
+  const uint64_t local_pt = static_cast<uint64_t>(s->shape.other) * s->shape.n0;
   const uint64_t tile = 16384;
   std::vector<uint16_t> host(tile * kN);
   DevBuf<uint16_t> dev;
   dev.alloc(tile * kN);
   s->db_loaded = false;
-  for (uint64_t pb = 0; pb < p.num_pt; pb += tile) {
-    const uint64_t pe = std::min<uint64_t>(p.num_pt, pb + tile);
-    const uint64_t real_end = std::min<uint64_t>(pe, logical);
-    if (pb < real_end) {
-      fill(pb, real_end, host.data());
-      ck(cudaMemcpyAsync(dev.p, host.data(), (real_end - pb) * kN * 2, cudaMemcpyHostToDevice,
-                         s->stream), "db upload");
-    }
+  for (uint64_t pb = 0; pb < local_pt; pb += tile) {
+    const uint64_t pe = std::min<uint64_t>(local_pt, pb + tile);
+    opir::fill_runs(s->host_rows, s->shape.n0, logical, pb, pe, host.data(), fill, kN);
+    ck(cudaMemcpyAsync(dev.p, host.data(), (pe - pb) * kN * 2, cudaMemcpyHostToDevice, s->stream),
+       "db upload");
     opir::launch_db_preprocess(s->dp, s->shape, dev.p, pb, 0, p.plain_mod, logical, pb, pe,
-                               s->db8.p, s->stream);
+                               s->row_map.p, s->db8.p, s->stream);
     ck(cudaStreamSynchronize(s->stream), "db preprocess");
   }
   s->db_loaded = true;
@@ -669,20 +684,36 @@ opir_params checked_params(const opir_params &p) {
   throw std::invalid_argument("tree level parameters are created by opir_tree_level_create");
 }
 
-// Allocates a handle for already checked parameters (any view).
-opir_status create_handle(const opir_params &checked, int device, opir_server **out) {
+// Allocates a handle for already checked parameters (any view); `rs` makes
+// it a row shard of the layout (view OPIR_VIEW_ROW_SHARD).
+opir_status create_handle(const opir_params &checked, int device, opir_server **out,
+                          const opir::RowShard *rs = nullptr) {
   opir_server *s = new (std::nothrow) opir_server();
   if (!s) return OPIR_ERR_NO_MEMORY;
   const opir_status st = guarded(s, [&] {
     s->params = checked;
     s->device = device;
+    if (rs) {
+      s->shard = rs->shard;
+      s->num_shards = rs->num_shards;
+      s->host_rows = rs->rows;
+    }
     DeviceGuard g(device);
     ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (is_c4(checked)) {
-      s->c4.reset(new opir4::Server(checked, s->stream));
+      s->c4.reset(new opir4::Server(checked, s->stream, rs));
       return;
     }
     setup_device_params(s);
+    s->tree_h = s->shape.num_dims > 1 ? s->shape.num_dims - 1 : 0;
+    if (rs) {  // the shard's rows only; MUX levels 0 .. tree_h - 1 run here
+      s->tree_h = rs->tree_h;
+      s->shape.other = static_cast<uint32_t>(rs->rows.size());
+      s->shape.num_pt = static_cast<uint64_t>(s->shape.other) * s->shape.n0;
+      s->row_map.alloc(rs->rows.size());
+      ck(cudaMemcpy(s->row_map.p, rs->rows.data(), rs->rows.size() * 4, cudaMemcpyHostToDevice),
+         "row map");
+    }
     const opir::Shape &sh = s->shape;
     const uint64_t db_bytes = 2ull * kN * 4 * sh.other * sh.n0p;
     s->db8.alloc(db_bytes);
@@ -710,11 +741,16 @@ opir_status create_handle(const opir_params &checked, int device, opir_server **
 void require_view(const opir_server *s, bool ok, const char *what) {
   if (!ok)
     throw std::invalid_argument(std::string(what) + " is not available on a handle created with " +
-                                (s->params.view == OPIR_VIEW_QUERY_SHAPE
-                                     ? "a query shape (no database)"
-                                     : "a tree level database"));
+                                (s->params.view == OPIR_VIEW_QUERY_SHAPE ? "a query shape (no database)"
+                                 : s->params.view == OPIR_VIEW_ROW_SHARD
+                                     ? "a row shard (opir_server_make_query_shard_batch)"
+                                 : s->params.view == OPIR_VIEW_LAYOUT ? "a whole layout"
+                                                                      : "a tree level database"));
 }
 bool is_layout(const opir_server *s) { return s->params.view == OPIR_VIEW_LAYOUT; }
+bool has_database(const opir_server *s) {
+  return s->params.view == OPIR_VIEW_LAYOUT || s->params.view == OPIR_VIEW_ROW_SHARD;
+}
 
 // select_level on a tree level handle (single-modulus set): the alpha
 // ciphertexts through the first dimension into `other` candidates, then
@@ -739,8 +775,8 @@ void select_fold_k1(opir_server *s, const uint64_t *alpha, const uint64_t *fold_
     opir::launch_split_u64(s->dp, in.p, s->sel.p + rows_per_sel * kCtWords, 1,
                            fold * rows_per_sel * 2, 0, s->stream);
     for (uint32_t a = 1; a <= fold; ++a)
-      opir::launch_mux_level(s->dp, sh, a, s->mid[(a - 1) & 1].p, s->mid[a & 1].p, sh.other,
-                             s->sel.p, 1, s->stream);
+      opir::launch_mux_level(s->dp, sh, a, sh.num_dims - 1, s->mid[(a - 1) & 1].p, s->mid[a & 1].p,
+                             sh.other, s->sel.p, 1, s->stream);
     res = s->mid[fold & 1].p;
   }
   DevBuf<uint64_t> o;
@@ -749,6 +785,52 @@ void select_fold_k1(opir_server *s, const uint64_t *alpha, const uint64_t *fold_
   ck(cudaMemcpyAsync(out, o.p, 2 * kN * 8, cudaMemcpyDeviceToHost, s->stream), "download");
   ck(cudaStreamSynchronize(s->stream), "select_level");
   check_device_error(s);
+}
+
+// The client ids of a shard batch must be those of the handle's last
+// make_query_shard batch: their selectors are still in the handle.
+void check_shard_ids(const std::vector<uint64_t> &last, uint32_t n, const uint64_t *ids) {
+  if (last.size() != n || !std::equal(last.begin(), last.end(), ids))
+    throw std::invalid_argument(
+        "combine_shards: client ids differ from this shard's last make_query_shard batch");
+}
+
+// The last log2 G MUX levels over the G partial ciphertexts of each query
+// (d_partials: G x n x 2N u64, shard-major), then the modulus switch.
+void combine_k1(opir_server *s, uint32_t n, const uint64_t *d_partials, uint64_t *d_resp) {
+  const uint32_t G = s->num_shards, h = s->shape.num_dims - 1;
+  const uint64_t words = static_cast<uint64_t>(n) * G * kCtWords;
+  for (auto &b : s->comb)
+    if (b.n < words) b.alloc(words);
+  for (uint32_t g = 0; g < G; ++g)  // query i's G ciphertexts side by side
+    opir::launch_split_u64(s->dp, d_partials + static_cast<uint64_t>(g) * n * 2 * kN,
+                           s->comb[0].p + static_cast<uint64_t>(g) * kCtWords, n, 2,
+                           static_cast<uint64_t>(G) * kCtWords, s->stream);
+  int cur = 0;
+  for (uint32_t a = s->tree_h; a < h; ++a, cur ^= 1)
+    opir::launch_mux_level(s->dp, s->shape, a, h, s->comb[cur].p, s->comb[cur ^ 1].p, G, s->sel.p,
+                           n, s->stream);
+  opir::launch_modswitch(s->dp, s->comb[cur].p, G, d_resp, nullptr, resp_bytes_of(s->params), n,
+                         s->stream);
+}
+
+// Orders the handle's stream after the caller's work on `user` (if any).
+void wait_user(opir_server *s, cudaStream_t user) {
+  if (!user) return;
+  cudaEvent_t e;
+  ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  ck(cudaEventRecord(e, user), "event record");
+  ck(cudaStreamWaitEvent(s->stream, e, 0), "wait");
+  cudaEventDestroy(e);
+}
+// Orders `user` (if any) after the work enqueued on the handle's stream.
+void signal_user(opir_server *s, cudaStream_t user) {
+  if (!user) return;
+  cudaEvent_t e;
+  ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  ck(cudaEventRecord(e, s->stream), "event record");
+  ck(cudaStreamWaitEvent(user, e, 0), "wait");
+  cudaEventDestroy(e);
 }
 
 }  // namespace
@@ -830,7 +912,7 @@ opir_status opir_server_params(const opir_server *s, opir_params *out) {
 opir_status opir_server_load_db_u16(opir_server *s, uint64_t logical, const uint16_t *coeffs) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
-    require_view(s, is_layout(s), "load_data");
+    require_view(s, has_database(s), "load_data");
     if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db_u16(logical, coeffs);
@@ -849,7 +931,7 @@ opir_status opir_server_load_db_u16(opir_server *s, uint64_t logical, const uint
 opir_status opir_server_load_db(opir_server *s, uint64_t logical, const uint64_t *coeffs) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
-    require_view(s, is_layout(s), "load_data");
+    require_view(s, has_database(s), "load_data");
     if (!coeffs && logical) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db(logical, coeffs);
@@ -869,7 +951,7 @@ opir_status opir_server_load_db_source(opir_server *s, uint64_t logical,
                                        opir_plaintext_source source, void *user) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
-    require_view(s, is_layout(s), "load_data");
+    require_view(s, has_database(s), "load_data");
     if (!source) throw std::invalid_argument("PirServer::load_data requires a source");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db_source(logical, source, user);
@@ -892,7 +974,7 @@ opir_status opir_server_load_db_source(opir_server *s, uint64_t logical,
 opir_status opir_server_load_db_seeded(opir_server *s, uint64_t logical, uint64_t seed) {
   if (!s) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(s, [&] {
-    require_view(s, is_layout(s), "load_data");
+    require_view(s, has_database(s), "load_data");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->load_db_seeded(logical, seed);
     const opir_params &p = s->params;
@@ -900,9 +982,11 @@ opir_status opir_server_load_db_seeded(opir_server *s, uint64_t logical, uint64_
       throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
     s->db_loaded = false;
     const uint64_t chunk = 1ull << 20;
-    for (uint64_t pb = 0; pb < p.num_pt; pb += chunk)
+    const uint64_t local_pt = static_cast<uint64_t>(s->shape.other) * s->shape.n0;
+    for (uint64_t pb = 0; pb < local_pt; pb += chunk)
       opir::launch_db_preprocess(s->dp, s->shape, nullptr, 0, seed, p.plain_mod, logical, pb,
-                                 std::min<uint64_t>(p.num_pt, pb + chunk), s->db8.p, s->stream);
+                                 std::min<uint64_t>(local_pt, pb + chunk), s->row_map.p, s->db8.p,
+                                 s->stream);
     ck(cudaStreamSynchronize(s->stream), "db preprocess");
     s->db_loaded = true;
   });
@@ -1004,24 +1088,136 @@ opir_status opir_server_make_query_batch_device(opir_server *s, uint32_t n,
     require_view(s, is_layout(s), "make_query");
     DeviceGuard g(s->device);
     cudaStream_t user = static_cast<cudaStream_t>(stream);
-    if (user) {  // order after the caller's prior work on its stream
-      cudaEvent_t e;
-      ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-      ck(cudaEventRecord(e, user), "event record");
-      ck(cudaStreamWaitEvent(s->stream, e, 0), "wait");
-      cudaEventDestroy(e);
-    }
+    wait_user(s, user);  // order after the caller's prior work on its stream
     if (s->c4)
       s->c4->make_query_batch_device(n, client_ids, d_queries, d_responses, c4_events(s));
     else
       run_pipeline(s, client_ids, n, d_queries, d_responses, nullptr);
-    if (user) {
-      cudaEvent_t e;
-      ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-      ck(cudaEventRecord(e, s->stream), "event record");
-      ck(cudaStreamWaitEvent(user, e, 0), "wait");
-      cudaEventDestroy(e);
+    signal_user(s, user);
+  });
+}
+
+// ---------------------------------------------------------------- row shards
+
+opir_status opir_row_shard_rows(const opir_params *params, uint32_t shard, uint32_t num_shards,
+                                uint32_t *rows, uint64_t *n_rows, uint32_t *tree_h) {
+  if (!params || !n_rows) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] {
+    const opir_params p = checked_params(*params);
+    if (p.view != OPIR_VIEW_LAYOUT) throw std::invalid_argument("row shards split a database layout");
+    const opir::RowShard rs = opir::row_shard(p.other_dim_sz, p.num_dims, shard, num_shards);
+    if (rows) std::copy(rs.rows.begin(), rs.rows.end(), rows);
+    *n_rows = rs.rows.size();
+    if (tree_h) *tree_h = rs.tree_h;
+  });
+}
+
+opir_status opir_server_create_row_shard(const opir_params *params, uint32_t shard,
+                                         uint32_t num_shards, int device, opir_server **out) {
+  if (!params || !out) return OPIR_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  opir_params checked{};
+  opir::RowShard rs;
+  const opir_status vs = guarded(nullptr, [&] {
+    checked = checked_params(*params);
+    if (checked.view != OPIR_VIEW_LAYOUT)
+      throw std::invalid_argument("row shards split a database layout");
+    rs = opir::row_shard(checked.other_dim_sz, checked.num_dims, shard, num_shards);
+    checked.view = OPIR_VIEW_ROW_SHARD;
+  });
+  if (vs != OPIR_OK) return vs;
+  return create_handle(checked, device, out, &rs);
+}
+
+opir_status opir_server_make_query_shard_batch(opir_server *s, uint32_t n,
+                                               const uint64_t *client_ids,
+                                               const uint64_t *queries, uint64_t *partials) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (n && (!client_ids || !queries || !partials)) throw std::invalid_argument("null argument");
+    require_view(s, is_row_shard(s), "make_query_shard");
+    DeviceGuard g(s->device);
+    if (s->c4) {
+      s->c4->make_query_batch(n, client_ids, queries, partials, c4_events(s));
+    } else {
+      check_query_values(s, queries, static_cast<size_t>(n) * 2 * kN);
+      ensure_capacity(s, n);
+      ck(cudaMemcpyAsync(s->q_u64.p, queries, static_cast<size_t>(n) * 2 * kN * 8,
+                         cudaMemcpyHostToDevice, s->stream), "query upload");
+      run_pipeline(s, client_ids, n, s->q_u64.p, s->resp_u64.p, nullptr);
+      ck(cudaMemcpyAsync(partials, s->resp_u64.p, static_cast<size_t>(n) * 2 * kN * 8,
+                         cudaMemcpyDeviceToHost, s->stream), "partial download");
+      finish(s);
     }
+    s->shard_ids.assign(client_ids, client_ids + n);
+  });
+}
+
+opir_status opir_server_make_query_shard_batch_device(opir_server *s, uint32_t n,
+                                                      const uint64_t *client_ids,
+                                                      const uint64_t *d_queries,
+                                                      uint64_t *d_partials, void *stream) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (n && (!client_ids || !d_queries || !d_partials)) throw std::invalid_argument("null argument");
+    require_view(s, is_row_shard(s), "make_query_shard");
+    DeviceGuard g(s->device);
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    wait_user(s, user);
+    if (s->c4)
+      s->c4->make_query_batch_device(n, client_ids, d_queries, d_partials, c4_events(s));
+    else
+      run_pipeline(s, client_ids, n, d_queries, d_partials, nullptr);
+    s->shard_ids.assign(client_ids, client_ids + n);
+    signal_user(s, user);
+  });
+}
+
+opir_status opir_server_combine_shards(opir_server *s, uint32_t n, const uint64_t *client_ids,
+                                       const uint64_t *partials, uint64_t *responses) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (n && (!client_ids || !partials || !responses)) throw std::invalid_argument("null argument");
+    require_view(s, is_row_shard(s), "combine_shards");
+    check_shard_ids(s->shard_ids, n, client_ids);
+    if (n == 0) return;
+    DeviceGuard g(s->device);
+    const size_t ct = s->c4 ? 4ull * s->params.poly_degree : 2ull * kN;
+    const size_t words = static_cast<size_t>(s->num_shards) * n * ct;
+    if (s->c4) {
+      s->c4->combine_host(n, partials, responses);
+      return;
+    }
+    check_query_values(s, partials, words);
+    DevBuf<uint64_t> d_in, d_out;
+    d_in.alloc(words);
+    d_out.alloc(static_cast<size_t>(n) * 2 * kN);
+    ck(cudaMemcpyAsync(d_in.p, partials, words * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    combine_k1(s, n, d_in.p, d_out.p);
+    ck(cudaMemcpyAsync(responses, d_out.p, static_cast<size_t>(n) * 2 * kN * 8,
+                       cudaMemcpyDeviceToHost, s->stream), "download");
+    finish(s);
+  });
+}
+
+opir_status opir_server_combine_shards_device(opir_server *s, uint32_t n,
+                                              const uint64_t *client_ids,
+                                              const uint64_t *d_partials, uint64_t *d_responses,
+                                              void *stream) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (n && (!client_ids || !d_partials || !d_responses)) throw std::invalid_argument("null argument");
+    require_view(s, is_row_shard(s), "combine_shards");
+    check_shard_ids(s->shard_ids, n, client_ids);
+    if (n == 0) return;
+    DeviceGuard g(s->device);
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    wait_user(s, user);
+    if (s->c4)
+      s->c4->combine_device(n, d_partials, d_responses);
+    else
+      combine_k1(s, n, d_partials, d_responses);
+    signal_user(s, user);
   });
 }
 
@@ -1505,8 +1701,9 @@ opir_status opir_tree_query(opir_tree *t, uint64_t client_id, const uint64_t *qu
                            cudaMemcpyDeviceToDevice, ls->stream), "selector copy");
       }
       for (uint32_t a = 1; a <= fold; ++a)
-        opir::launch_mux_level(ls->dp, ls->shape, a, ls->mid[(a - 1) & 1].p, ls->mid[a & 1].p,
-                               ls->shape.other, ls->sel.p, 1, ls->stream);
+        opir::launch_mux_level(ls->dp, ls->shape, a, ls->shape.num_dims - 1,
+                               ls->mid[(a - 1) & 1].p, ls->mid[a & 1].p, ls->shape.other,
+                               ls->sel.p, 1, ls->stream);
       const uint32_t *res = fold ? ls->mid[fold & 1].p : ls->mid[0].p;
       opir::launch_compose_u64(ls->dp, res, 0, t->out.p + l * 2ull * kN, 1, 2, ls->stream);
       ck(cudaEventRecord(t->done[l], ls->stream), "event record");

@@ -342,6 +342,79 @@ class PirServer:
         return save_response(self.params, response)
 
 
+def row_shard_rows(params: PirParams, shard: int, num_shards: int) -> tuple[np.ndarray, int]:
+    """Database rows of shard `shard` of `num_shards` in storage order, and
+    the MUX levels the shard answers (opir_row_shard_rows)."""
+    lib = L.load()
+    n = C.c_uint64()
+    th = C.c_uint32()
+    rc = lib.opir_row_shard_rows(C.byref(params._p), shard, num_shards, None, C.byref(n), C.byref(th))
+    if rc != OPIR_OK:
+        _raise(rc, f"invalid row shard {shard} of {num_shards} for this layout")
+    rows = np.zeros(max(n.value, 1), dtype=np.uint32)
+    rc = lib.opir_row_shard_rows(C.byref(params._p), shard, num_shards, _ptr(rows, C.c_uint32),
+                                 C.byref(n), C.byref(th))
+    if rc != OPIR_OK:
+        _raise(rc, "opir_row_shard_rows failed")
+    return rows[: n.value], int(th.value)
+
+
+class RowShardServer(PirServer):
+    """One GPU's rows of a database split by candidate rows across
+    `num_shards` GPUs (opir_server_create_row_shard). Loads take the whole
+    database's arguments; make_query_shard_batch returns each query's partial
+    ciphertext (shape params.ct_shape, mod q); combine_shards, on any shard
+    whose last batch had the same client ids, finishes the queries from all
+    shards' partials and returns make_query's responses."""
+
+    def __init__(self, params: PirParams, shard: int, num_shards: int, device: int = 0):
+        self.params = params
+        self.shard, self.num_shards = int(shard), int(num_shards)
+        self._lib = L.load()
+        h = C.c_void_p()
+        rc = self._lib.opir_server_create_row_shard(C.byref(params._p), self.shard,
+                                                    self.num_shards, device, C.byref(h))
+        if rc != OPIR_OK:
+            _raise(rc, f"opir_server_create_row_shard failed (status {rc})")
+        self._h = h
+
+    def make_query_shard_batch(self, client_ids: Sequence[int], queries: np.ndarray) -> np.ndarray:
+        ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
+        q = np.ascontiguousarray(queries, dtype=np.uint64)
+        n = ids.size
+        if q.shape != (n,) + self.params.ct_shape:
+            raise ValueError(f"queries must be (n,) + {self.params.ct_shape}")
+        out = np.zeros((n,) + self.params.ct_shape, dtype=np.uint64)
+        self._check(self._lib.opir_server_make_query_shard_batch(self._h, n, _ptr(ids), _ptr(q),
+                                                                 _ptr(out)))
+        return out
+
+    def make_query_shard_batch_device(self, client_ids: Sequence[int], d_queries: int,
+                                      d_partials: int, stream: int = 0):
+        ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
+        self._check(self._lib.opir_server_make_query_shard_batch_device(
+            self._h, ids.size, _ptr(ids), C.c_void_p(d_queries), C.c_void_p(d_partials),
+            C.c_void_p(stream) if stream else None))
+
+    def combine_shards(self, client_ids: Sequence[int], partials: np.ndarray) -> np.ndarray:
+        """partials: (num_shards, n) + ct_shape, shard g's batch at [g]."""
+        ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
+        n = ids.size
+        pa = np.ascontiguousarray(partials, dtype=np.uint64)
+        if pa.shape != (self.num_shards, n) + self.params.ct_shape:
+            raise ValueError(f"partials must be ({self.num_shards}, {n}) + {self.params.ct_shape}")
+        out = np.zeros((n, 2, self.params.N), dtype=np.uint64)
+        self._check(self._lib.opir_server_combine_shards(self._h, n, _ptr(ids), _ptr(pa), _ptr(out)))
+        return out
+
+    def combine_shards_device(self, client_ids: Sequence[int], d_partials: int,
+                              d_responses: int, stream: int = 0):
+        ids = np.ascontiguousarray(np.asarray(client_ids, dtype=np.uint64))
+        self._check(self._lib.opir_server_combine_shards_device(
+            self._h, ids.size, _ptr(ids), C.c_void_p(d_partials), C.c_void_p(d_responses),
+            C.c_void_p(stream) if stream else None))
+
+
 def plan_memory(params: PirParams) -> dict:
     """Device bytes a server of these parameters requests: database, one
     client's keys, and scratch = fixed + batch * per_query."""

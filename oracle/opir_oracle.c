@@ -766,6 +766,11 @@ static void ext_prod_mux(const opir_oracle_params *p, const uint64_t *x, uint64_
   free(tmp);
 }
 
+void oracle_ext_prod_mux(const opir_oracle_params *p, const uint64_t *x, uint64_t *y,
+                         const uint64_t *sel, uint64_t *res) {
+  ext_prod_mux(p, x, y, sel, res);
+}
+
 /* server.cpp:599-649. mid: other_dim x 2N (consumed). */
 int oracle_server_other_dim(const oracle_server *s, uint64_t *mid, const uint64_t *selectors, uint64_t *out) {
   const opir_oracle_params *p = &s->p;

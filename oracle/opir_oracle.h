@@ -102,6 +102,11 @@ int oracle_server_other_dim(const oracle_server *s, uint64_t *mid,
                             const uint64_t *selectors, uint64_t *out);
 int oracle_server_make_query(const oracle_server *s, const uint64_t *query,
                              uint64_t *resp);
+/* PirServer::ext_prod_mux (server.cpp:652-722): res = x + INTT(ExtProd(sel,
+ * y - x)); x, y coefficient form (2N u64), y is clobbered, res may alias x;
+ * sel = 2 L_EP rows x 2N u64, NTT form. */
+void oracle_ext_prod_mux(const opir_oracle_params *p, const uint64_t *x, uint64_t *y,
+                         const uint64_t *sel, uint64_t *res);
 void oracle_mod_switch(const opir_oracle_params *p, uint64_t *ct);
 size_t oracle_serialize(const opir_oracle_params *p, const uint64_t *resp,
                         uint8_t *out);
@@ -158,6 +163,9 @@ int oracle_c4_server_other_dim(const oracle_c4_server *s, uint64_t *mid,
                                const uint64_t *selectors, uint64_t *out);
 int oracle_c4_server_make_query(const oracle_c4_server *s, const uint64_t *query,
                                 uint64_t *resp);
+/* ext_prod_mux under CONFIG_N4096_K2_MP: 4N u64 ciphertexts (limb-major). */
+void oracle_c4_ext_prod_mux(const opir_oracle_c4_params *p, const uint64_t *x, uint64_t *y,
+                            const uint64_t *sel, uint64_t *res);
 void oracle_c4_mod_switch(const opir_oracle_c4_params *p, const uint64_t *ct,
                           uint64_t *out);
 void oracle_c4_external_product(const opir_oracle_c4_params *p,

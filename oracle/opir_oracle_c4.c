@@ -573,6 +573,11 @@ static void ext_prod_mux_c4(const opir_oracle_c4_params *p, const uint64_t *x, u
   for (size_t j = 0; j < ct; ++j) { const uint64_t q = p->q[(j % KN) / N]; res[j] = addmod(x[j], tmp[j], q); }
   free(tmp);
 }
+void oracle_c4_ext_prod_mux(const opir_oracle_c4_params *p, const uint64_t *x, uint64_t *y,
+                            const uint64_t *sel, uint64_t *res) {
+  ext_prod_mux_c4(p, x, y, sel, res);
+}
+
 /* server.cpp:599-649 */
 int oracle_c4_server_other_dim(const oracle_c4_server *s, uint64_t *mid, const uint64_t *selectors,
                                uint64_t *out) {

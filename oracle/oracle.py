@@ -100,6 +100,7 @@ def lib():
                   "oracle_server_first_dim", "oracle_server_make_query"):
             getattr(L, f).argtypes = [C.c_void_p, _u64p, _u64p]
         L.oracle_server_other_dim.argtypes = [C.c_void_p, _u64p, _u64p, _u64p]
+        L.oracle_ext_prod_mux.argtypes = [C.POINTER(Params), _u64p, _u64p, _u64p, _u64p]
         L.oracle_mod_switch.argtypes = [C.POINTER(Params), _u64p]
         L.oracle_serialize.argtypes = [C.POINTER(Params), _u64p, C.POINTER(C.c_uint8)]
         L.oracle_serialize.restype = C.c_size_t
@@ -146,6 +147,7 @@ def lib():
                   "oracle_c4_server_first_dim", "oracle_c4_server_make_query"):
             getattr(L, f).argtypes = [C.c_void_p, _u64p, _u64p]
         L.oracle_c4_server_other_dim.argtypes = [C.c_void_p, _u64p, _u64p, _u64p]
+        L.oracle_c4_ext_prod_mux.argtypes = [P4, _u64p, _u64p, _u64p, _u64p]
         L.oracle_c4_mod_switch.argtypes = [P4, _u64p, _u64p]
         L.oracle_c4_serialize.argtypes = [P4, _u64p, C.POINTER(C.c_uint8)]
         L.oracle_c4_serialize.restype = C.c_size_t
@@ -421,3 +423,71 @@ def c4_serialize(p: C4Params, resp: np.ndarray) -> bytes:
     buf = np.zeros(2 * p.N * 8, dtype=np.uint8)
     n = lib().oracle_c4_serialize(C.byref(p), ptr(r), ptr(buf, C.c_uint8))
     return buf[:n].tobytes()
+
+
+# ----------------------------------------------------------------------------
+# Row shards: the reference's evaluate_other_dim (server.cpp:599-649) split by
+# MUX level, and the candidate rows that feed each level-1 position.
+
+def ext_prod_mux(p, x: np.ndarray, y: np.ndarray, sel: np.ndarray) -> np.ndarray:
+    """PirServer::ext_prod_mux (server.cpp:652-722): x + INTT(ExtProd(sel, y - x))."""
+    xx = np.ascontiguousarray(x, dtype=np.uint64)
+    yy = np.array(y, dtype=np.uint64, copy=True, order="C")
+    ss = np.ascontiguousarray(sel, dtype=np.uint64)
+    out = np.zeros_like(xx)
+    if isinstance(p, C4Params):
+        lib().oracle_c4_ext_prod_mux(C.byref(p), ptr(xx), ptr(yy), ptr(ss), ptr(out))
+    else:
+        lib().oracle_ext_prod_mux(C.byref(p), ptr(xx), ptr(yy), ptr(ss), ptr(out))
+    return out
+
+
+def mux_levels(p, mid: np.ndarray, selectors: np.ndarray, tree_h: int, begin: int,
+               end: int) -> np.ndarray:
+    """Levels [begin, end) of evaluate_other_dim's MUX tree of height tree_h
+    over the candidates `mid` (level 0: rows offset + 2i and offset + 2i + 1
+    into offset + i, offset = 2^tree_h - len(mid); level a >= 1: i and
+    i + 2^(tree_h-a-1) into i), selector slot a at level a. Returns the
+    positions left after level end - 1."""
+    cur = [np.array(c, dtype=np.uint64) for c in mid]
+    for a in range(begin, end):
+        if a == 0:
+            other = len(cur)
+            last = 2 * other - (1 << tree_h)
+            offset = other - last
+            nxt = cur[:offset]
+            for i in range(0, last, 2):
+                nxt.append(ext_prod_mux(p, cur[offset + i], cur[offset + i + 1], selectors[0]))
+        else:
+            half = (1 << (tree_h - a)) >> 1
+            nxt = [ext_prod_mux(p, cur[i], cur[i + half], selectors[a]) for i in range(half)]
+        cur = nxt
+    return np.stack(cur)
+
+
+def shard_rows(other: int, num_dims: int, shard: int, num_shards: int) -> list[int]:
+    """Candidate rows feeding the level-1 positions s = shard (mod num_shards):
+    row s when s < offset (carried over at level 0), else rows 2s - offset and
+    2s - offset + 1 (server.cpp:626-635), in increasing s."""
+    h = num_dims - 1
+    offset = other - (2 * other - (1 << h))
+    rows = []
+    for s in range(shard, 1 << (h - 1), num_shards):
+        rows += [s] if s < offset else [2 * s - offset, 2 * s - offset + 1]
+    return rows
+
+
+def sharded_other_dim(p, mid: np.ndarray, selectors: np.ndarray, num_shards: int):
+    """evaluate_other_dim computed as num_shards row shards plus a combine:
+    returns (partials, result) with partials[g] = shard g's ciphertext after
+    its levels 0 .. h - log2 G - 1 and result = the full tree's output."""
+    h = p.num_dims - 1
+    k = num_shards.bit_length() - 1
+    partials = []
+    for g in range(num_shards):
+        rows = shard_rows(p.other_dim_sz, p.num_dims, g, num_shards)
+        left = mux_levels(p, mid[rows], selectors, h - k, 0, h - k)
+        assert len(left) == 1
+        partials.append(left[0])
+    result = mux_levels(p, np.stack(partials), selectors, h, h - k, h)
+    return np.stack(partials), result[0]
