@@ -17,6 +17,15 @@ HBM; no L2 flush is needed.
 N > 1 runs one rank per GPU (torchrun), each holding a replica of the
 database and serving its own queries (queries are independent: replicas
 only, no collective on the data path); timing is the max over ranks.
+
+    python bench.py --rows-sharded [--gpus N] ...
+
+instead splits ONE database by candidate rows over the N ranks (strong
+scaling): every step, each rank answers its shard for the same batch, the
+partial ciphertexts are gathered to rank 0 over NCCL and rank 0 finishes
+the last log2 N MUX levels. On one GPU this is the whole database (one
+shard), and the line adds the per-GPU time of one shard of a 2-, 4- and
+8-way split measured on this GPU.
 """
 from __future__ import annotations
 
@@ -63,6 +72,8 @@ def parse():
                          "1,8,32,64 for c4; 'none' to skip)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default scan tiling (or OPIR_SCAN_TILE)")
+    ap.add_argument("--rows-sharded", action="store_true",
+                    help="one database split by candidate rows over the ranks (strong scaling)")
     ap.add_argument("--serve", action="store_true",
                     help="serving loop: Poisson arrivals over three resident databases")
     ap.add_argument("--rates", default="50,500,2000", help="offered queries/s (--serve)")
@@ -795,9 +806,181 @@ def bench_tree(args, world, rank, local):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- row shards
+def bench_rows(args, world, rank, local):
+    """One database split by candidate rows over the job's ranks: per step,
+    every rank answers its shard for the same batch (make_query_shard), the
+    partials are gathered to rank 0 (NCCL) and rank 0 combines them. value =
+    the batch's queries / max-over-ranks step time (strong scaling)."""
+    import torch
+    from onionpirv2_b200 import PirParams, RowShardServer
+    from onionpirv2_b200.server import launch_count
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=device)
+    c4 = args.workload == "c4"
+    params = (PirParams(args.target, args.height, config=C4_CONFIG) if c4
+              else PirParams(args.target, args.height))
+    N, B = params.N, args.batch
+    ids = list(range(B))
+    queries, keys = synthetic_inputs(params, B, 1000)   # the same batch on every rank
+    stream = torch.cuda.Stream(device)
+
+    def make_shard(g, G):
+        srv = RowShardServer(params, g, G, device=local)
+        srv.load_data_seeded(args.target, DB_SEED)
+        for b, (bv, gsw) in enumerate(keys):
+            srv.set_client_keys(b, bv, gsw)
+        if not args.no_autotune:
+            srv.autotune(B)
+        return srv
+
+    d_q = torch.from_numpy(queries.view(np.int64)).to(device)
+    d_part = torch.empty((B,) + params.ct_shape, dtype=torch.int64, device=device)
+    d_resp = torch.empty((B, 2, N), dtype=torch.int64, device=device)
+
+    def timed(srv, G, gather, steps, warm):
+        parts = torch.empty((G, B) + params.ct_shape, dtype=torch.int64, device=device)
+
+        def step():
+            srv.make_query_shard_batch_device(ids, d_q.data_ptr(), d_part.data_ptr(),
+                                              stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                if gather:
+                    import torch.distributed as dist
+                    dist.gather(d_part, [parts[g] for g in range(G)] if rank == 0 else None, dst=0)
+                else:
+                    parts[0].copy_(d_part)
+            if rank == 0:
+                srv.combine_shards_device(ids, parts.data_ptr(), d_resp.data_ptr(),
+                                          stream.cuda_stream)
+
+        if not gather:   # one GPU standing in for shard 0: the other slots hold copies
+            srv.make_query_shard_batch_device(ids, d_q.data_ptr(), d_part.data_ptr(),
+                                              stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                parts.copy_(d_part.expand((G,) + tuple(d_part.shape)))
+        for _ in range(warm):
+            step()
+        torch.cuda.synchronize(device)
+        barrier(world, device)
+        torch.cuda.synchronize(device)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        l0 = launch_count()
+        evs[0].record(stream)
+        for i in range(steps):
+            step()
+            evs[i + 1].record(stream)
+        torch.cuda.synchronize(device)
+        launches = launch_count() - l0
+        barrier(world, device)
+        per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+        return evs[0].elapsed_time(evs[-1]), per, launches
+
+    srv = make_shard(rank, world)
+    with ClockSampler(local) as clk:
+        total, per, launches = timed(srv, world, world > 1, args.steps, args.warmup)
+    total_max = max_over_ranks(total, world, device)
+    qps = B * args.steps / (total_max / 1e3)
+
+    # end to end: host queries in, host responses out on rank 0
+    hq = torch.from_numpy(queries.view(np.int64)).pin_memory()
+    hr = torch.empty((B, 2, N), dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            d_q.copy_(hq, non_blocking=True)
+        srv.make_query_shard_batch_device(ids, d_q.data_ptr(), d_part.data_ptr(), stream.cuda_stream)
+        parts = e2e_parts
+        with torch.cuda.stream(stream):
+            if world > 1:
+                import torch.distributed as dist
+                dist.gather(d_part, [parts[g] for g in range(world)] if rank == 0 else None, dst=0)
+            else:
+                parts[0].copy_(d_part)
+        if rank == 0:
+            srv.combine_shards_device(ids, parts.data_ptr(), d_resp.data_ptr(), stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                hr.copy_(d_resp, non_blocking=True)
+        stream.synchronize()
+
+    e2e_parts = torch.empty((world, B) + params.ct_shape, dtype=torch.int64, device=device)
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier(world, device)
+    te = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = max_over_ranks(time.perf_counter() - te, world, device)
+
+    projection = []
+    if world == 1:   # the per-GPU work of a G-way split, measured on this GPU
+        srv.close()
+        for G in (2, 4, 8):
+            if G > 1 << (params.num_dims - 2):
+                break
+            one = make_shard(0, G)
+            k = max(3, min(args.steps, 20))
+            t, _, _ = timed(one, G, False, k, args.warmup)
+            projection.append({"shards": G, "rows_per_shard": len(one_rows(params, G)),
+                               "per_gpu_ms": t / k,
+                               "per_gpu_queries_per_s": B * k / (t / 1e3)})
+            one.close()
+    if rank != 0:
+        srv.close()
+        import torch.distributed as dist
+        dist.destroy_process_group()
+        return
+    coeff_bits = 40 if c4 else 13
+    logical_db = params.num_pt * N * coeff_bits / 8
+    line = {
+        "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u64" if c4 else "u32",
+        "data": "synthetic (seeded DB coefficients < t generated on device; seeded uniform "
+                "ciphertexts and keys mod q -- the path is data-independent)",
+        "config": {"workload": (c4_workload_name(params) if c4 else
+                                f"k1_comp N=2048, {args.target} plaintexts, first dim "
+                                f"{params.fst_dim_sz} x {params.num_dims - 1} binary dims"),
+                   "batch": B, "parallelism": f"row shards x{world} (gather to rank 0)",
+                   "l2": "inputs larger than L2: every shard streams its rows from HBM every step"},
+        "db_gbs": logical_db * B * args.steps / (total_max / 1e3) / 1e9,
+        "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+        "e2e": {"value": B * args.steps / e2e_s, "unit": "queries/s",
+                "h2d_bytes_per_step": B * int(np.prod(params.ct_shape)) * 8,
+                "d2h_bytes_per_step": B * 2 * N * 8},
+        "clocks": clk.summary(), "gpu_launches": launches,
+    }
+    if projection:
+        line["shard_projection"] = {
+            "note": "one shard of a G-way split on this GPU (expansion and selectors replicated, "
+                    "1/G of the rows scanned and MUXed) plus the root's combine; the gather is "
+                    "not included",
+            "runs": projection}
+    print(json.dumps(line))
+    if world > 1:
+        srv.close()
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def one_rows(params, G):
+    from onionpirv2_b200 import row_shard_rows
+    return row_shard_rows(params, 0, G)[0]
+
+
 def main():
     args = parse()
     world, rank, local = dist_env()
+    if args.rows_sharded and args.impl == "ours":
+        bench_rows(args, world, rank, local)
+        return
     if args.workload == "tree" and args.impl == "ours" and not args.serve:
         bench_tree(args, world, rank, local)
         return
