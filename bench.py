@@ -185,6 +185,41 @@ def ncu_traffic() -> dict | None:
     return None
 
 
+def ntt_butterflies(params) -> dict:
+    """NTT butterflies per query of the two NTT-bound stages, over both RNS
+    residues (limbs): expansion = one BV key switch per heap node
+    (L_KS digit NTTs + 2 INTTs, bv_keyswitch.cpp:296-367 / 373-481; nodes of
+    level d = ceil(useful / 2^(h-d)), server.cpp:786-792); other dimensions =
+    other_dim_sz - 1 external products (2 L_EP digit NTTs + 2 INTTs,
+    gsw.cpp:119-250, server.cpp:652-722). One butterfly = one Shoup product."""
+    N = params.N
+    per_ntt = (N // 2) * (N.bit_length() - 1)
+    h = params.expansion_height
+    useful = params.fst_dim_sz + params.l_ep * (params.num_dims - 1)
+    nodes = sum(-(-useful // (1 << (h - d))) for d in range(h))
+    return {"Expand": nodes * (params.l_ks + 2) * per_ntt * 2,
+            "Other dim": (params.other_dim_sz - 1) * (2 * params.l_ep + 2) * per_ntt * 2}
+
+
+def int_pipe_roofline(params, config: str, stages: dict, batch: int, device: int) -> dict:
+    """Achieved NTT butterflies/s of the NTT-bound stages (live stage times)
+    against the device's measured butterfly rate (register-resident probe)."""
+    from onionpirv2_b200.server import measure_butterfly_rate
+    peak = measure_butterfly_rate(config, device) / 1e9
+    out = {"bound": "integer multiply pipe (NTT butterflies, one Shoup product each)",
+           "unit": "Gbutterflies/s", "peak": peak,
+           "peak_source": "measured (opir_measure_butterfly_rate: the kernels' radix-8 pass on "
+                          "register operands, all SMs)", "stages": {}}
+    for name, per_query in ntt_butterflies(params).items():
+        ms = stages.get(name)
+        if not ms:
+            continue
+        achieved = per_query * batch / (ms / 1e3) / 1e9
+        out["stages"][name] = {"achieved": achieved, "frac": achieved / peak,
+                               "butterflies_per_query": per_query}
+    return out
+
+
 def synthetic_inputs(params, batch: int, seed: int):
     """Seeded uniform ciphertexts and key material mod q (per RNS limb under
     CONFIG_N4096_K2_MP). make_query's work is data-independent, so uniform
@@ -509,6 +544,8 @@ def bench_ours(args, world, rank, local):
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "algorithmic_bytes": alg_bytes,
                      "traffic": (traffic or {}).get(f"{'c4_' if c4 else ''}batch_{B}")},
+        "int_pipe": int_pipe_roofline(params, C4_CONFIG if c4 else "CONFIG_N2048_K1_COMP", stages,
+                                      B, local),
         "batch_sweep": sweep,
         "clocks": clk.summary(),
         "gpu_launches": launches,

@@ -330,6 +330,15 @@ opir_status opir_server_set_stage_timing(opir_server *server, int enabled);
 opir_status opir_server_stage_times(opir_server *server, float *ms_out,
                                     uint32_t *calls);
 
+/* No counterpart in the reference. The rate (butterflies per second) at
+ * which the device retires the NTT's forward radix-2 butterflies of the
+ * parameter set -- the radix-8 register pass of the NTT kernels, with their
+ * lazy-correction pattern, on register-resident values and twiddles, one
+ * modular (Shoup) product each -- over every SM at full occupancy: the
+ * denominator of the NTT-bound stages' roofline. Runs about a millisecond
+ * of probe kernels on `device`. */
+opir_status opir_measure_butterfly_rate(opir_config config, int device, double *per_s);
+
 /* Total kernel launches issued by this library in this process. */
 uint64_t opir_launch_count(void);
 

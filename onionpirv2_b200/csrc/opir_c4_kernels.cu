@@ -838,4 +838,43 @@ void launch_modswitch(const Dev4 &P, const uint64_t *ct, uint64_t ct_stride, uin
   check_launch("k4_modswitch");
 }
 
+// ------------------------------------------------- butterfly-rate probe
+// The two-limb NTT's forward radix-8 pass (fpass, limb 0) on register values
+// and twiddles, three passes per iteration with one pass's corrections per
+// stage pattern of the kernels; see the single-modulus probe.
+__global__ void __launch_bounds__(256)
+k4_bfly_rate(uint64_t *__restrict__ sink, uint32_t iters, ulonglong2 w0) {
+  uint64_t v[8];
+  ulonglong2 w[7];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = (threadIdx.x * 8ull + k + blockIdx.x) % kQ0;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) w[k] = make_ulonglong2(w0.x + 2 * k, w0.y + k);
+  for (uint32_t it = 0; it < iters; ++it) {
+    fpass<kQ0, false, false, false>(v, w);
+    fpass<kQ0, true, false, true>(v, w);
+    fpass<kQ0, false, true, false>(v, w);
+  }
+  uint64_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc ^= v[k];
+  sink[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+uint32_t bfly_rate_blocks(int sms) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k4_bfly_rate, 256, 0) != cudaSuccess || occ < 1)
+    occ = 1;
+  return static_cast<uint32_t>(sms) * static_cast<uint32_t>(occ);
+}
+
+uint64_t launch_bfly_rate(uint64_t *sink, uint32_t blocks, uint32_t iters, cudaStream_t st) {
+  const uint64_t w = 1234567890123456789ull % kQ0;
+  const ulonglong2 w0 = make_ulonglong2(
+      w, static_cast<uint64_t>((static_cast<unsigned __int128>(w) << 64) / kQ0));
+  k4_bfly_rate<<<blocks, 256, 0, st>>>(sink, iters, w0);
+  check_launch("k4_bfly_rate");
+  return static_cast<uint64_t>(blocks) * 256 * iters * 36;
+}
+
 }  // namespace opir4

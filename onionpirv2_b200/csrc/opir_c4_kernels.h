@@ -114,4 +114,10 @@ uint32_t scan_tc4_max_stages(uint32_t ntile);
 void launch_scan_tc4(const CUtensorMap &mapA, const CUtensorMap &mapQ, const Tc4Args &args,
                      int sm_count, cudaStream_t st);
 
+// Butterfly-rate probe of the two-limb NTT (as opir::launch_bfly_rate);
+// sink holds blocks x 256 u64. Returns the butterflies the launch performs.
+// Blocks of 256 threads that fill `sms` SMs with the probe (its occupancy).
+uint32_t bfly_rate_blocks(int sms);
+uint64_t launch_bfly_rate(uint64_t *sink, uint32_t blocks, uint32_t iters, cudaStream_t st);
+
 }  // namespace opir4

@@ -980,4 +980,45 @@ void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride
   check_launch("k_modswitch");
 }
 
+// ------------------------------------------------- butterfly-rate probe
+// The forward radix-8 pass of the NTT kernels (fpass8, the first residue's
+// modulus) on register-resident values and twiddles, three passes per
+// iteration with the kernels' correction pattern (stages 4, 6, 8 of 9
+// corrected): the rate at which an SM retires NTT butterflies when nothing
+// else (shared-memory exchanges, loads, digit work, MACs) is in the way.
+// The values are not meaningful; `sink` keeps the work alive.
+__global__ void __launch_bounds__(256)
+k_bfly_rate(uint32_t *__restrict__ sink, uint32_t iters, uint2 w0) {
+  uint32_t v[8];
+  uint2 w[7];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = (threadIdx.x * 8 + k + blockIdx.x) % kQ1;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) w[k] = make_uint2(w0.x + 2 * k, w0.y + k);
+  for (uint32_t it = 0; it < iters; ++it) {
+    fpass8<kQ1, false, false, false>(v, w);
+    fpass8<kQ1, true, false, true>(v, w);
+    fpass8<kQ1, false, true, false>(v, w);
+  }
+  uint32_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc ^= v[k];
+  sink[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+uint32_t bfly_rate_blocks(int sms) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bfly_rate, 256, 0) != cudaSuccess || occ < 1)
+    occ = 1;
+  return static_cast<uint32_t>(sms) * static_cast<uint32_t>(occ);
+}
+
+uint64_t launch_bfly_rate(uint32_t *sink, uint32_t blocks, uint32_t iters, cudaStream_t st) {
+  const uint32_t w = 123456789u % kQ1;
+  const uint2 w0 = make_uint2(w, static_cast<uint32_t>((static_cast<uint64_t>(w) << 32) / kQ1));
+  k_bfly_rate<<<blocks, 256, 0, st>>>(sink, iters, w0);
+  check_launch("k_bfly_rate");
+  return static_cast<uint64_t>(blocks) * 256 * iters * 36;
+}
+
 }  // namespace opir

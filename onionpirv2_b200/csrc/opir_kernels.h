@@ -121,4 +121,11 @@ uint64_t launch_count();
 // replayed from a CUDA graph).
 void note_launches(int64_t delta);
 
+// Butterfly-rate probe: `blocks` x 256 threads, each running `iters`
+// iterations of three register-resident forward radix-8 passes; sink holds
+// blocks x 256 u32. Returns the butterflies the launch performs.
+// Blocks of 256 threads that fill `sms` SMs with the probe (its occupancy).
+uint32_t bfly_rate_blocks(int sms);
+uint64_t launch_bfly_rate(uint32_t *sink, uint32_t blocks, uint32_t iters, cudaStream_t st);
+
 }  // namespace opir

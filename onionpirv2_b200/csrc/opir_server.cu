@@ -1716,6 +1716,49 @@ opir_status opir_tree_query(opir_tree *t, uint64_t client_id, const uint64_t *qu
   });
 }
 
+opir_status opir_measure_butterfly_rate(opir_config config, int device, double *per_s) {
+  if (!per_s || (config != OPIR_CONFIG_N2048_K1_COMP && config != OPIR_CONFIG_N4096_K2_MP))
+    return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] {
+    DeviceGuard g(device);
+    int sms = 0;
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
+    const bool c4 = config == OPIR_CONFIG_N4096_K2_MP;
+    const uint32_t blocks = c4 ? opir4::bfly_rate_blocks(sms) : opir::bfly_rate_blocks(sms);
+    const uint32_t iters = c4 ? 256 : 1024;
+    DevBuf<uint64_t> sink;
+    sink.alloc(static_cast<size_t>(blocks) * 256);
+    cudaStream_t st = nullptr;
+    ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto launch = [&] {
+      return c4 ? opir4::launch_bfly_rate(sink.p, blocks, iters, st)
+                : opir::launch_bfly_rate(reinterpret_cast<uint32_t *>(sink.p), blocks, iters, st);
+    };
+    try {
+      ck(cudaEventCreate(&e0), "event");
+      ck(cudaEventCreate(&e1), "event");
+      launch();  // warm-up
+      ck(cudaEventRecord(e0, st), "event record");
+      uint64_t bfly = 0;
+      for (int r = 0; r < 3; ++r) bfly += launch();
+      ck(cudaEventRecord(e1, st), "event record");
+      ck(cudaEventSynchronize(e1), "probe");
+      float ms = 0;
+      ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+      *per_s = static_cast<double>(bfly) / (static_cast<double>(ms) / 1e3);
+    } catch (...) {
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+  });
+}
+
 size_t opir_save_response(const opir_params *params, const uint64_t *resp, uint8_t *out,
                           size_t cap) {
   if (!params || !resp || !out) return 0;

@@ -425,6 +425,16 @@ def plan_memory(params: PirParams) -> dict:
     return {f: int(getattr(plan, f)) for f, _ in L.MemoryPlan._fields_}
 
 
+def measure_butterfly_rate(config: str = "CONFIG_N2048_K1_COMP", device: int = 0) -> float:
+    """NTT butterflies per second the device retires with register-resident
+    operands (opir_measure_butterfly_rate): the NTT-bound stages' peak."""
+    out = C.c_double()
+    rc = L.load().opir_measure_butterfly_rate(CONFIGS[config], device, C.byref(out))
+    if rc != OPIR_OK:
+        _raise(rc, "opir_measure_butterfly_rate failed")
+    return float(out.value)
+
+
 def launch_count() -> int:
     """Kernel launches issued by the library in this process."""
     return int(L.load().opir_launch_count())
