@@ -369,6 +369,15 @@ opir_status opir_server_evaluate_other_dim(opir_server *server,
                                            const uint64_t *selectors,
                                            uint64_t *out);
 
+/* PirServer::ext_prod_mux (src/server.cpp:652-722): out = x + b (y - x)
+ * for the RGSW selector bit b. x, y, out: one ciphertext each in the query
+ * layout, coefficient form; selector: 2 L_EP rows in the complete_selectors
+ * layout (NTT form). Unlike the reference, y is not overwritten. Available
+ * on every handle (it does not read the database). */
+opir_status opir_server_ext_prod_mux(opir_server *server, const uint64_t *x,
+                                     const uint64_t *y, const uint64_t *selector,
+                                     uint64_t *out);
+
 /* ---- response codec ------------------------------------------------------- */
 
 /* PirServer::save_resp_to_stream (src/server.cpp:950-1009): c0 then c1,

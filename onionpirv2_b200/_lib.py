@@ -124,6 +124,7 @@ _SIGS = {
     "opir_server_complete_selectors": ([C.c_void_p, C.c_uint64, u64p, u64p], C.c_int),
     "opir_server_evaluate_first_dim": ([C.c_void_p, u64p, u64p], C.c_int),
     "opir_server_evaluate_other_dim": ([C.c_void_p, u64p, u64p, u64p], C.c_int),
+    "opir_server_ext_prod_mux": ([C.c_void_p, u64p, u64p, u64p, u64p], C.c_int),
     "opir_save_response": ([C.POINTER(Params), u64p, u8p, C.c_size_t], C.c_size_t),
     "opir_ext_prod_mux_noalloc": ([C.POINTER(Params), C.c_uint32, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),

@@ -642,6 +642,30 @@ void Server::evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, 
   ck(cudaStreamSynchronize(st_), "evaluate_other_dim");
 }
 
+void Server::ext_prod_mux(const uint64_t *x, const uint64_t *y, const uint64_t *sel,
+                          uint64_t *out) {
+  check_ct_values(x, 1);
+  check_ct_values(y, 1);
+  const size_t n_rows = 2ull * sh_.l_ep;
+  check_ct_values(sel, n_rows);
+  Shape4 sh = sh_;  // one MUX level of a two-candidate tree
+  sh.other = 2;
+  sh.num_dims = 2;
+  std::vector<uint64_t> rows;
+  rows.reserve(n_rows * kRowWords);
+  for (size_t r = 0; r < n_rows; ++r) append_row(rows, sel + r * kCt);
+  opir::DevBuf<uint64_t> xy, res, srows;
+  xy.alloc(2 * kCt);
+  res.alloc(2 * kCt);
+  srows.alloc(rows.size());
+  ck(cudaMemcpyAsync(xy.p, x, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  ck(cudaMemcpyAsync(xy.p + kCt, y, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  ck(cudaMemcpyAsync(srows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st_), "upload");
+  launch_mux_level(dp_, sh, 0, 1, xy.p, res.p, 2, srows.p, 1, st_);
+  ck(cudaMemcpyAsync(out, res.p, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaStreamSynchronize(st_), "ext_prod_mux");
+}
+
 void Server::select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32_t fold,
                          uint64_t *out) {
   if (!db_loaded_) throw std::runtime_error("select_level before load_data");

@@ -63,6 +63,9 @@ class Server {
   void complete_selectors(uint64_t id, const uint64_t *expanded, uint64_t *out);
   void evaluate_first_dim(const uint64_t *fst_query, uint64_t *out);
   void evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, uint64_t *out);
+  // ext_prod_mux (server.cpp:652-722) of one pair, host buffers: x, y and
+  // out 4N u64 coefficient form, sel 2 L_EP rows x 4N u64 NTT form.
+  void ext_prod_mux(const uint64_t *x, const uint64_t *y, const uint64_t *sel, uint64_t *out);
   // Row shards: the last log2 G MUX levels over each query's G partial
   // ciphertexts (G x n x 4N u64, shard-major), with the selectors of this
   // handle's last batch, then the modulus switch (n x 2N u64 out).

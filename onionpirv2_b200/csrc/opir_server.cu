@@ -1464,6 +1464,41 @@ opir_status opir_server_evaluate_other_dim(opir_server *s, const uint64_t *mid,
   });
 }
 
+opir_status opir_server_ext_prod_mux(opir_server *s, const uint64_t *x, const uint64_t *y,
+                                     const uint64_t *selector, uint64_t *out) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    if (!x || !y || !selector || !out) throw std::invalid_argument("null argument");
+    DeviceGuard g(s->device);
+    if (s->c4) return s->c4->ext_prod_mux(x, y, selector, out);
+    // one MUX level of a two-candidate tree: level 0 pairs candidates 0, 1
+    opir::Shape sh = s->shape;
+    sh.other = 2;
+    sh.num_dims = 2;
+    const uint64_t sel_polys = 2ull * 2 * sh.l_ep;
+    check_query_values(s, x, 2 * kN);
+    check_query_values(s, y, 2 * kN);
+    check_query_values(s, selector, sel_polys * kN);
+    DevBuf<uint64_t> in;
+    DevBuf<uint32_t> xy, res, sel;
+    in.alloc(std::max<uint64_t>(4, sel_polys) * kN);
+    xy.alloc(2 * kCtWords);
+    res.alloc(2 * kCtWords);
+    sel.alloc(sel_polys / 2 * kCtWords);
+    ck(cudaMemcpyAsync(in.p, x, 2 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    ck(cudaMemcpyAsync(in.p + 2 * kN, y, 2 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    opir::launch_split_u64(s->dp, in.p, xy.p, 1, 4, 0, s->stream);
+    ck(cudaStreamSynchronize(s->stream), "upload");
+    ck(cudaMemcpyAsync(in.p, selector, sel_polys * kN * 8, cudaMemcpyHostToDevice, s->stream),
+       "upload");
+    opir::launch_split_u64(s->dp, in.p, sel.p, 1, sel_polys, 0, s->stream);
+    opir::launch_mux_level(s->dp, sh, 0, 1, xy.p, res.p, 2, sel.p, 1, s->stream);
+    opir::launch_compose_u64(s->dp, res.p, 0, in.p, 1, 2, s->stream);
+    ck(cudaMemcpyAsync(out, in.p, 2 * kN * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    ck(cudaStreamSynchronize(s->stream), "ext_prod_mux");
+  });
+}
+
 opir_status opir_params_query_shape(const opir_params *scheme, const opir_query_shape *shape,
                                     opir_params *out) {
   if (!scheme || !shape || !out) return OPIR_ERR_INVALID_ARGUMENT;

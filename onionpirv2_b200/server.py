@@ -338,6 +338,22 @@ class PirServer:
         self._check(self._lib.opir_server_evaluate_other_dim(self._h, _ptr(m), _ptr(s), _ptr(out)))
         return out
 
+    def ext_prod_mux(self, x: np.ndarray, y: np.ndarray, selector: np.ndarray) -> np.ndarray:
+        """x + b (y - x) for the RGSW selector bit b (ext_prod_mux); y is
+        left unchanged. selector: (2 L_EP,) + ct_shape rows, NTT form."""
+        p = self.params
+        xx = np.ascontiguousarray(x, dtype=np.uint64)
+        yy = np.ascontiguousarray(y, dtype=np.uint64)
+        ss = np.ascontiguousarray(selector, dtype=np.uint64)
+        if xx.shape != p.ct_shape or yy.shape != p.ct_shape:
+            raise ValueError(f"x and y must be {p.ct_shape}")
+        if ss.shape != (2 * p.l_ep,) + p.ct_shape:
+            raise ValueError(f"selector must be ({2 * p.l_ep},) + {p.ct_shape}")
+        out = np.zeros(p.ct_shape, dtype=np.uint64)
+        self._check(self._lib.opir_server_ext_prod_mux(self._h, _ptr(xx), _ptr(yy), _ptr(ss),
+                                                       _ptr(out)))
+        return out
+
     def save_resp_to_stream(self, response: np.ndarray) -> bytes:
         return save_response(self.params, response)
 

@@ -200,3 +200,13 @@ def test_c4_graph_replays_match_eager_launches(monkeypatch):
     assert st["calls"] == 2 and st["Core"] > 0 and st["Other dim"] > 0
     eager.close()
     graphed.close()
+
+
+def test_c4_ext_prod_mux_matches_oracle():
+    c, op, cl, bv, gsw, q, gp, srv = setup("c4_2048_h7")
+    exp = srv.expand_query(7, q)
+    sel = srv.complete_selectors(7, exp)
+    mid = srv.evaluate_first_dim(exp)
+    for a, b, s in ((0, 1, 0), (3, 2, 1)):
+        got = srv.ext_prod_mux(mid[a], mid[b], sel[s])
+        assert np.array_equal(got, O.ext_prod_mux(op, mid[a], mid[b], sel[s]))
