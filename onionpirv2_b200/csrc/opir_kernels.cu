@@ -6,7 +6,12 @@
 #include "opir_kernels.h"
 #include "opir_ntt.cuh"
 
+#include <cooperative_groups.h>
+
+#include <algorithm>
 #include <atomic>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <set>
@@ -33,6 +38,33 @@ void check_launch(const char *what) {
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// SMs of the current device (cached per device).
+int sm_count() {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    n = 148;
+  }
+  cache[dev] = n;
+  return n;
+}
+
+// Cluster-split MUX levels (k_mux_level_split): on unless OPIR_SPLIT=0.
+bool split_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("OPIR_SPLIT");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
 }
 
 // Raise a kernel's dynamic shared-memory limit once per (device, kernel,
@@ -293,6 +325,156 @@ k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, i
   else
     expand_level_body<1>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
                          bv_keys, bv_level_off);
+}
+
+// Expansion level, cluster split: a level with fewer nodes than the GPU
+// has CTA slots (the top of the heap, and most levels of a single query)
+// runs each node's key switch on a cluster of C CTAs. CTA r NTTs digits
+// [r D, (r + 1) D) (D = L_KS / C) of sigma_k(c1) and multiplies them with
+// their key rows; the partial sums meet in distributed shared memory; CTA 0
+// then finishes the b part (c0 of both children) and CTA 1 the a part (c1 of
+// both children). Every partial and their total are exact 64-bit sums below
+// the single-CTA bound, so the children are the same bit for bit.
+template <int RES, int C>
+__device__ __forceinline__ void expand_split_body(const DevParams &P, uint32_t galois_inv,
+                                                  uint32_t kshift, const uint32_t *in,
+                                                  uint64_t in_stride, uint32_t *out,
+                                                  uint64_t out_stride,
+                                                  const uint32_t *const *bv_keys,
+                                                  uint64_t bv_level_off) {
+  static_assert(kLKs % C == 0, "digits split evenly over the cluster");
+  constexpr int D = kLKs / C;
+  extern __shared__ uint32_t sm[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  constexpr uint32_t q = Res<RES>::q;
+  const int rank = static_cast<int>(cluster.block_rank());
+  const int node = blockIdx.x / C, b = blockIdx.z, tid = threadIdx.x;
+  const ResidueTables &T = P.r[RES];
+  const uint32_t *ct = in + ((uint64_t)b * in_stride + node) * kCtWords;
+  const uint32_t *c0 = ct + RES * kN;
+  const uint32_t *c1 = ct + 2 * kN + RES * kN;
+
+  uint64_t d[8];  // centred sigma_k(c1) + digit offset
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t j = posA(tid, k);
+    const uint32_t u = (j * galois_inv) & (2 * kN - 1);
+    const bool neg = u >= kN;
+    const uint32_t src = u & (kN - 1);
+    const uint32_t a0 = ct[2 * kN + src], a1 = ct[3 * kN + src];
+    d[k] = digit_source<kLKs, kBaseKs>(compose_c(neg ? neg_mod(a0, kQ1) : a0,
+                                                 neg ? neg_mod(a1, kQ2) : a1));
+  }
+  const int i0 = rank * D;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, kBaseKs>(d[k], i0 + i);
+    fA<RES>(v);
+    st_plane<0>(sm + i * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid_r<RES>(sm, D, T.fwt);
+  const uint32_t *key = bv_keys[b] + bv_level_off + RES * kN;
+  uint64_t ab[8], aa[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
+  {
+    uint2 wd[6];
+    fload_d(wd, T.fwt, tid);
+    for (int i = 0; i < D; ++i) {
+      uint32_t v[8];
+      ld_plane<3>(sm + i * kPad, v, tid);
+      fD<RES>(v, wd);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = to4q<RES>(v[k]);
+      const int row = i0 + i;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j0 = 4 * (tid + 256 * h);
+        const uint4 kb = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(row * 4 + 0) * kN + j0));
+        const uint4 ka = __ldg(reinterpret_cast<const uint4 *>(key + (uint64_t)(row * 4 + 2) * kN + j0));
+        ab[4 * h + 0] += (uint64_t)v[4 * h + 0] * kb.x; aa[4 * h + 0] += (uint64_t)v[4 * h + 0] * ka.x;
+        ab[4 * h + 1] += (uint64_t)v[4 * h + 1] * kb.y; aa[4 * h + 1] += (uint64_t)v[4 * h + 1] * ka.y;
+        ab[4 * h + 2] += (uint64_t)v[4 * h + 2] * kb.z; aa[4 * h + 2] += (uint64_t)v[4 * h + 2] * ka.z;
+        ab[4 * h + 3] += (uint64_t)v[4 * h + 3] * kb.w; aa[4 * h + 3] += (uint64_t)v[4 * h + 3] * ka.w;
+      }
+    }
+  }
+  __syncthreads();
+  // partial sums out to shared memory: [b / a][k][tid]
+  uint64_t *ex = reinterpret_cast<uint64_t *>(sm);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    ex[(0 * 8 + k) * kThreads + tid] = ab[k];
+    ex[(1 * 8 + k) * kThreads + tid] = aa[k];
+  }
+  cluster.sync();
+  uint64_t tot[8];
+  if (rank < 2) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tot[k] = rank == 0 ? ab[k] : aa[k];
+    for (int r = 0; r < C; ++r) {
+      if (r == rank) continue;
+      const uint64_t *rex = cluster.map_shared_rank(ex, r);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) tot[k] += rex[(rank * 8 + k) * kThreads + tid];
+    }
+  }
+  cluster.sync();  // every remote read is done before shared memory is reused
+  if (rank >= 2) return;
+  {
+    uint2 wd[6];
+    iload_d(wd, T.iwt, tid);
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = red64<RES>(tot[k]);
+    iD<RES>(v, wd);
+    st_plane<3>(sm, v, tid);
+  }
+  __syncthreads();
+  inv_mid_r<RES>(sm, 1, T.iwt);
+  uint32_t dv[8];
+  ld_plane<0>(sm, dv, tid);
+  iA<RES>(dv);
+  // rank 0: c0 of both children (with sigma_k(c0)); rank 1: c1 of both
+  uint32_t *outL = out + ((uint64_t)b * out_stride + 2 * (uint64_t)node) * kCtWords;
+  uint32_t *outR = outL + kCtWords;
+  const uint32_t *src_poly = rank == 0 ? c0 : c1;
+  const uint64_t off = (uint64_t)rank * 2 * kN + RES * kN;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int j = posA(tid, k);
+    uint32_t nv = dv[k];
+    if (rank == 0) {  // c0' = sigma(c0) + delta_b
+      const uint32_t u = (j * galois_inv) & (2 * kN - 1);
+      const uint32_t z = c0[u & (kN - 1)];
+      nv = add_mod(u >= kN ? neg_mod(z, q) : z, nv, q);
+    }
+    const uint32_t o = src_poly[j];
+    outL[off + j] = add_mod(o, nv, q);
+    const uint32_t dd = sub_mod(o, nv, q);
+    int dst = j - static_cast<int>(kshift);
+    const bool wrap = dst < 0;
+    if (wrap) dst += kN;
+    outR[off + dst] = wrap ? neg_mod(dd, q) : dd;
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(kThreads, 2)
+k_expand_level_split(DevParams P, uint32_t galois_inv, uint32_t kshift,
+                     const uint32_t *__restrict__ in, uint64_t in_stride,
+                     uint32_t *__restrict__ out, uint64_t out_stride,
+                     const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  if (blockIdx.y == 0)
+    expand_split_body<0, C>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                            bv_level_off);
+  else
+    expand_split_body<1, C>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                            bv_level_off);
 }
 
 // Shared gadget product of a coefficient-form ciphertext (both residues read
@@ -745,6 +927,150 @@ k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t off
     mux_level_body<1>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
 }
 
+// ------------------------------------------------- MUX level, cluster split
+// A MUX level with fewer pairs than the GPU has CTA slots (the upper levels
+// of the tree, and most levels of a single query) runs each MUX on a
+// cluster of C CTAs instead of one: CTA r takes D = 2 l / C of the 2 l
+// gadget rows (C = 2: polynomial r; C = 4: half of polynomial r / 2's
+// digits) through their digit NTTs and key products, the partial sums meet
+// in distributed shared memory, and CTAs 0 and 1 finish output polynomials
+// c0 and c1 (sum, reduction, INTT, + x). Every partial and their total are
+// exact 64-bit sums below the single-CTA bound (2 l products < 4q x q each),
+// so the result is the same bit for bit.
+template <int RES, int D>
+__device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32_t *x,
+                                                const uint32_t *y, const uint32_t *rgsw,
+                                                uint32_t *sm, int p, int i0,
+                                                uint64_t (&acc0)[8], uint64_t (&acc1)[8]) {
+  constexpr uint32_t q = Res<RES>::q;
+  constexpr int l = kLEp;
+  constexpr int B = kBaseEp;
+  const ResidueTables &T = P.r[RES];
+  const int tid = threadIdx.x;
+  uint64_t d[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int j = posA(tid, k);
+    const uint32_t v1 = sub_mod(y[(p * 2 + 0) * kN + j], x[(p * 2 + 0) * kN + j], kQ1);
+    const uint32_t v2 = sub_mod(y[(p * 2 + 1) * kN + j], x[(p * 2 + 1) * kN + j], kQ2);
+    d[k] = digit_source<l, B>(compose_c(v1, v2));
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, B>(d[k], i0 + i);
+    fA<RES>(v);
+    st_plane<0>(sm + i * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid_r<RES>(sm, D, T.fwt);
+  uint2 wd[6];
+  fload_d(wd, T.fwt, tid);
+  for (int i = 0; i < D; ++i) {
+    uint32_t v[8];
+    ld_plane<3>(sm + i * kPad, v, tid);
+    fD<RES>(v, wd);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = to4q<RES>(v[k]);
+    const int row = p * l + (l - 1 - (i0 + i));
+    const uint32_t *R0 = rgsw + (uint64_t)row * kCtWords + RES * kN;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j0 = 4 * (tid + 256 * h);
+      const uint4 r0 = __ldg(reinterpret_cast<const uint4 *>(R0 + j0));
+      const uint4 r1 = __ldg(reinterpret_cast<const uint4 *>(R0 + 2 * kN + j0));
+      acc0[4 * h + 0] += (uint64_t)v[4 * h + 0] * r0.x; acc1[4 * h + 0] += (uint64_t)v[4 * h + 0] * r1.x;
+      acc0[4 * h + 1] += (uint64_t)v[4 * h + 1] * r0.y; acc1[4 * h + 1] += (uint64_t)v[4 * h + 1] * r1.y;
+      acc0[4 * h + 2] += (uint64_t)v[4 * h + 2] * r0.z; acc1[4 * h + 2] += (uint64_t)v[4 * h + 2] * r1.z;
+      acc0[4 * h + 3] += (uint64_t)v[4 * h + 3] * r0.w; acc1[4 * h + 3] += (uint64_t)v[4 * h + 3] * r1.w;
+    }
+  }
+  __syncthreads();
+}
+
+// Pair i reads x = in[i xs], y = in[i xs + yoff] and writes out[i]: level 0
+// without a carried prefix has xs = 2, yoff = 1; level a >= 1 has xs = 1,
+// yoff = half.
+template <int RES, int C>
+__device__ __forceinline__ void mux_split_body(const DevParams &P, const Shape &S, uint32_t level,
+                                               uint32_t xs, uint32_t yoff, const uint32_t *in,
+                                               uint32_t *out, uint64_t mid_stride,
+                                               const uint32_t *sel) {
+  static_assert(C == 2 || C == 4, "cluster of 2 or 4 CTAs");
+  constexpr int D = 2 * kLEp / C;  // gadget rows per CTA
+  extern __shared__ uint32_t sm[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  constexpr uint32_t q = Res<RES>::q;
+  const int tid = threadIdx.x, b = blockIdx.z;
+  const int rank = static_cast<int>(cluster.block_rank());
+  const uint32_t i = blockIdx.x / C;
+  const uint32_t *base_in = in + (uint64_t)b * mid_stride * kCtWords;
+  const uint32_t *x = base_in + (uint64_t)i * xs * kCtWords;
+  const uint32_t *y = base_in + ((uint64_t)i * xs + yoff) * kCtWords;
+  const uint32_t *rgsw = sel + ((uint64_t)b * (S.num_dims - 1) + level) * 2 * S.l_ep * kCtWords;
+  uint64_t acc0[8], acc1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
+  const int p = C == 2 ? rank : rank >> 1;
+  const int i0 = C == 2 ? 0 : (rank & 1) * D;
+  gadget_mac_part<RES, D>(P, x, y, rgsw, sm, p, i0, acc0, acc1);
+  // partial sums out to shared memory: [output poly][k][tid]
+  uint64_t *ex = reinterpret_cast<uint64_t *>(sm);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    ex[(0 * 8 + k) * kThreads + tid] = acc0[k];
+    ex[(1 * 8 + k) * kThreads + tid] = acc1[k];
+  }
+  cluster.sync();
+  uint64_t tot[8];
+  if (rank < 2) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tot[k] = rank == 0 ? acc0[k] : acc1[k];
+    for (int r = 0; r < C; ++r) {
+      if (r == rank) continue;
+      const uint64_t *rex = cluster.map_shared_rank(ex, r);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) tot[k] += rex[(rank * 8 + k) * kThreads + tid];
+    }
+  }
+  cluster.sync();  // every remote read is done before shared memory is reused
+  if (rank >= 2) return;
+  const ResidueTables &T = P.r[RES];
+  {
+    uint2 wd[6];
+    iload_d(wd, T.iwt, tid);
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = red64<RES>(tot[k]);
+    iD<RES>(v, wd);
+    st_plane<3>(sm, v, tid);
+  }
+  __syncthreads();
+  inv_mid_r<RES>(sm, 1, T.iwt);
+  uint32_t v[8];
+  ld_plane<0>(sm, v, tid);
+  iA<RES>(v);
+  uint32_t *o = out + (uint64_t)b * mid_stride * kCtWords + (uint64_t)i * kCtWords;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int j = posA(tid, k);
+    o[(rank * 2 + RES) * kN + j] = add_mod(x[(rank * 2 + RES) * kN + j], v[k], q);
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(kThreads, 2)
+k_mux_level_split(DevParams P, Shape S, uint32_t level, uint32_t xs, uint32_t yoff,
+                  const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                  uint64_t mid_stride, const uint32_t *__restrict__ sel) {
+  if (blockIdx.y == 0)
+    mux_split_body<0, C>(P, S, level, xs, yoff, in, out, mid_stride, sel);
+  else
+    mux_split_body<1, C>(P, S, level, xs, yoff, in, out, mid_stride, sel);
+}
+
 // ------------------------------------------------ modulus switch + packing
 // utils.cpp:445-462: centred round(v * out / inp), inp = q, out = small_q.
 __device__ __forceinline__ uint64_t rescale_dev(uint64_t v, uint64_t inp, uint64_t outm) {
@@ -876,11 +1202,52 @@ void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const u
   const uint32_t galois = kN / k + 1;
   uint32_t galois_inv = 1;  // galois^-1 mod 2N (galois is odd)
   while (((galois_inv * galois) & (2 * kN - 1)) != 1) galois_inv += 2;
-  dim3 grid(nodes, 2, batch);
-  k_expand_level<<<grid, kThreads, smem, st>>>(P, galois_inv, k, s.base_ks, s.l_ks, in,
-                                                in_stride, out, out_stride, bv_keys,
-                                                d * bv_level_stride);
-  check_launch("k_expand_level");
+  // levels with fewer nodes than CTA slots (2 per SM) split each key switch
+  // over a cluster of 2, 4 or 8 CTAs (k_expand_level_split)
+  const uint64_t ctas = 2ull * nodes * batch, slots = 2ull * sm_count();
+  const int split = !split_enabled() ? 1
+                    : 8 * ctas <= slots ? 8 : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
+  if (split == 1) {
+    dim3 grid(nodes, 2, batch);
+    k_expand_level<<<grid, kThreads, smem, st>>>(P, galois_inv, k, s.base_ks, s.l_ks, in,
+                                                  in_stride, out, out_stride, bv_keys,
+                                                  d * bv_level_stride);
+    check_launch("k_expand_level");
+    return;
+  }
+  // the exchange area ([2][8][256] u64) reuses the digit planes
+  const size_t smem_split = std::max<size_t>(kLKs / 2 * kPad * sizeof(uint32_t),
+                                             2 * 8 * kThreads * sizeof(uint64_t));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(nodes * split, 2, batch);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem_split;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = split;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const uint64_t koff = d * bv_level_stride;
+  cudaError_t e;
+  if (split == 8) {
+    set_smem(k_expand_level_split<8>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<8>, P, galois_inv, k, in, in_stride, out,
+                           out_stride, bv_keys, koff);
+  } else if (split == 4) {
+    set_smem(k_expand_level_split<4>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<4>, P, galois_inv, k, in, in_stride, out,
+                           out_stride, bv_keys, koff);
+  } else {
+    set_smem(k_expand_level_split<2>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<2>, P, galois_inv, k, in, in_stride, out,
+                           out_stride, bv_keys, koff);
+  }
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("k_expand_level_split: ") + cudaGetErrorString(e));
+  check_launch("k_expand_level_split");
 }
 
 void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves,
@@ -967,11 +1334,48 @@ void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32
     n_pairs = half;
   }
   const size_t smem = s.l_ep * kPad * sizeof(uint32_t);
-  set_smem(k_mux_level, smem);
-  dim3 grid(n_pairs + copies, 2, batch);
-  k_mux_level<<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,
-                                             mid_stride, sel);
-  check_launch("k_mux_level");
+  // levels with fewer MUX steps than CTA slots (2 per SM) split each step
+  // over a cluster of 2 or 4 CTAs (k_mux_level_split)
+  const uint64_t ctas = 2ull * n_pairs * batch, slots = 2ull * sm_count();
+  const int split = (copies != 0 || !split_enabled()) ? 1
+                    : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
+  if (split == 1) {
+    set_smem(k_mux_level, smem);
+    dim3 grid(n_pairs + copies, 2, batch);
+    k_mux_level<<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,
+                                               mid_stride, sel);
+    check_launch("k_mux_level");
+    return;
+  }
+  // the exchange area ([2][8][256] u64) reuses the digit planes
+  const size_t smem_split = std::max<size_t>(smem, 2 * 8 * kThreads * sizeof(uint64_t));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(n_pairs * split, 2, batch);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem_split;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = split;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // offset == copies == 0 here, so level 0 pairs (2i, 2i + 1) into i
+  const uint32_t xs = level == 0 ? 2 : 1, yoff = level == 0 ? 1 : half;
+  cudaError_t e;
+  if (split == 4) {
+    set_smem(k_mux_level_split<4>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_mux_level_split<4>, P, s, level, xs, yoff, in, out, mid_stride,
+                           sel);
+  } else {
+    set_smem(k_mux_level_split<2>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_mux_level_split<2>, P, s, level, xs, yoff, in, out, mid_stride,
+                           sel);
+  }
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("k_mux_level_split: ") + cudaGetErrorString(e));
+  check_launch("k_mux_level_split");
 }
 
 void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride, uint64_t *resp,
