@@ -937,22 +937,27 @@ k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t off
 // c0 and c1 (sum, reduction, INTT, + x). Every partial and their total are
 // exact 64-bit sums below the single-CTA bound (2 l products < 4q x q each),
 // so the result is the same bit for bit.
-template <int RES, int D>
+// gadget_mac restricted to digits [i0, i0 + D) of polynomial p (decomposed
+// value y - x, or x when y is null).
+template <int RES, int L, int B, int D>
 __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32_t *x,
                                                 const uint32_t *y, const uint32_t *rgsw,
                                                 uint32_t *sm, int p, int i0,
                                                 uint64_t (&acc0)[8], uint64_t (&acc1)[8]) {
   constexpr uint32_t q = Res<RES>::q;
-  constexpr int l = kLEp;
-  constexpr int B = kBaseEp;
+  constexpr int l = L;
+  constexpr bool lazy = L <= 8;
   const ResidueTables &T = P.r[RES];
   const int tid = threadIdx.x;
   uint64_t d[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int j = posA(tid, k);
-    const uint32_t v1 = sub_mod(y[(p * 2 + 0) * kN + j], x[(p * 2 + 0) * kN + j], kQ1);
-    const uint32_t v2 = sub_mod(y[(p * 2 + 1) * kN + j], x[(p * 2 + 1) * kN + j], kQ2);
+    uint32_t v1 = x[(p * 2 + 0) * kN + j], v2 = x[(p * 2 + 1) * kN + j];
+    if (y != nullptr) {
+      v1 = sub_mod(y[(p * 2 + 0) * kN + j], v1, kQ1);
+      v2 = sub_mod(y[(p * 2 + 1) * kN + j], v2, kQ2);
+    }
     d[k] = digit_source<l, B>(compose_c(v1, v2));
   }
 #pragma unroll
@@ -972,7 +977,7 @@ __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32
     ld_plane<3>(sm + i * kPad, v, tid);
     fD<RES>(v, wd);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = to4q<RES>(v[k]);
+    for (int k = 0; k < 8; ++k) v[k] = lazy ? to4q<RES>(v[k]) : canon8<RES>(v[k]);
     const int row = p * l + (l - 1 - (i0 + i));
     const uint32_t *R0 = rgsw + (uint64_t)row * kCtWords + RES * kN;
 #pragma unroll
@@ -1015,7 +1020,7 @@ __device__ __forceinline__ void mux_split_body(const DevParams &P, const Shape &
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
   const int p = C == 2 ? rank : rank >> 1;
   const int i0 = C == 2 ? 0 : (rank & 1) * D;
-  gadget_mac_part<RES, D>(P, x, y, rgsw, sm, p, i0, acc0, acc1);
+  gadget_mac_part<RES, kLEp, kBaseEp, D>(P, x, y, rgsw, sm, p, i0, acc0, acc1);
   // partial sums out to shared memory: [output poly][k][tid]
   uint64_t *ex = reinterpret_cast<uint64_t *>(sm);
 #pragma unroll
@@ -1060,6 +1065,85 @@ __device__ __forceinline__ void mux_split_body(const DevParams &P, const Shape &
   }
 }
 
+// Selector completion, cluster split: with fewer rows than CTA slots each
+// row runs on a pair of CTAs, CTA r decomposing polynomial r of the
+// expanded row (l_key digits) against RGSW(s); the two partial sums meet in
+// distributed shared memory and CTA r writes polynomial r of the bottom row
+// (sum, reduction) and of the top row (the row's own NTT). Exact 64-bit
+// partial sums: the same rows bit for bit.
+template <int RES>
+__device__ __forceinline__ void selectors_split_body(const DevParams &P, const Shape &S,
+                                                     const uint32_t *leaves, uint64_t leaf_stride,
+                                                     const uint32_t *const *gsw_keys,
+                                                     uint32_t *sel) {
+  extern __shared__ uint32_t sm[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = static_cast<int>(cluster.block_rank());
+  const int row_id = blockIdx.x / 2, b = blockIdx.z, tid = threadIdx.x;
+  const int selno = row_id / S.l_ep, r = row_id % S.l_ep;
+  const ResidueTables &T = P.r[RES];
+  const uint32_t *ct = leaves + ((uint64_t)b * leaf_stride + S.n0 + row_id) * kCtWords;
+  uint32_t *out = sel + ((uint64_t)b * (S.num_dims - 1) + selno) * 2 * S.l_ep * kCtWords;
+  uint64_t acc0[8], acc1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
+  gadget_mac_part<RES, kLKey, kBaseKey, kLKey>(P, ct, nullptr, gsw_keys[b], sm, rank, 0, acc0,
+                                               acc1);
+  uint64_t *ex = reinterpret_cast<uint64_t *>(sm);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    ex[(0 * 8 + k) * kThreads + tid] = acc0[k];
+    ex[(1 * 8 + k) * kThreads + tid] = acc1[k];
+  }
+  cluster.sync();
+  uint64_t tot[8];
+  {
+    const uint64_t *rex = cluster.map_shared_rank(ex, rank ^ 1);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      tot[k] = (rank == 0 ? acc0[k] : acc1[k]) + rex[(rank * 8 + k) * kThreads + tid];
+  }
+  cluster.sync();  // every remote read is done before shared memory is reused
+  // bottom row, polynomial `rank`: ExtProd(RGSW(s), row) (gsw.cpp:119-182)
+  uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords + RES * kN + rank * 2 * kN;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int j0 = 4 * (tid + 256 * h);
+    *reinterpret_cast<uint4 *>(bot + j0) =
+        make_uint4(red64<RES>(tot[4 * h + 0]), red64<RES>(tot[4 * h + 1]),
+                   red64<RES>(tot[4 * h + 2]), red64<RES>(tot[4 * h + 3]));
+  }
+  // top row, polynomial `rank`: the expanded row in NTT form (gsw.cpp:330-338)
+  uint32_t v[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = ct[(rank * 2 + RES) * kN + posA(tid, k)];
+  fA<RES>(v);
+  st_plane<0>(sm, v, tid);
+  __syncthreads();
+  fwd_mid_r<RES>(sm, 1, T.fwt);
+  uint2 wd[6];
+  fload_d(wd, T.fwt, tid);
+  ld_plane<3>(sm, v, tid);
+  fD<RES>(v, wd);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = canon8<RES>(v[k]);
+  uint32_t *top = out + (uint64_t)r * kCtWords + RES * kN + rank * 2 * kN;
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+    *reinterpret_cast<uint4 *>(top + 4 * (tid + 256 * h)) =
+        make_uint4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_selectors_split(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
+                  const uint32_t *const *__restrict__ gsw_keys, uint32_t *__restrict__ sel) {
+  if (blockIdx.y == 0)
+    selectors_split_body<0>(P, S, leaves, leaf_stride, gsw_keys, sel);
+  else
+    selectors_split_body<1>(P, S, leaves, leaf_stride, gsw_keys, sel);
+}
+
 template <int C>
 __global__ void __launch_bounds__(kThreads, 2)
 k_mux_level_split(DevParams P, Shape S, uint32_t level, uint32_t xs, uint32_t yoff,
@@ -1091,7 +1175,10 @@ k_modswitch(DevParams P, const uint32_t *__restrict__ ct_all, uint64_t ct_stride
   __shared__ uint32_t vals[2 * kN];
   const int b = blockIdx.x;
   const uint32_t *ct = ct_all + (uint64_t)b * ct_stride * kCtWords;
-  for (int idx = threadIdx.x; idx < 2 * kN; idx += kThreads) {
+  // gridDim.y blocks share a query's coefficients (one block when packing)
+  const int per = 2 * kN / gridDim.y;
+  for (int idx = blockIdx.y * per + threadIdx.x; idx < (int)(blockIdx.y + 1) * per;
+       idx += kThreads) {
     const int p = idx >> kLogN, j = idx & (kN - 1);
     const uint64_t v = crt_compose(ct[(p * 2 + 0) * kN + j], ct[(p * 2 + 1) * kN + j], P);
     const uint64_t r = rescale_dev(v, P.q, P.small_q);
@@ -1256,8 +1343,32 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
   check_gadgets(s);
   if (s.num_dims <= 1) return;
   const size_t smem = s.l_key * kPad * sizeof(uint32_t);
+  const uint32_t rows = (s.num_dims - 1) * s.l_ep;
+  // fewer rows than CTA slots (2 per SM): one pair of CTAs per row
+  if (split_enabled() && 2ull * 2 * rows * batch <= 2ull * sm_count()) {
+    const size_t smem_split = std::max<size_t>(smem, 2 * 8 * kThreads * sizeof(uint64_t));
+    set_smem(k_selectors_split, smem_split);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(rows * 2, 2, batch);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem_split;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e =
+        cudaLaunchKernelEx(&cfg, k_selectors_split, P, s, leaves, leaf_stride, gsw_keys, sel);
+    if (e != cudaSuccess)
+      throw std::runtime_error(std::string("k_selectors_split: ") + cudaGetErrorString(e));
+    check_launch("k_selectors_split");
+    return;
+  }
   set_smem(k_selectors, smem);
-  dim3 grid((s.num_dims - 1) * s.l_ep, 2, batch);
+  dim3 grid(rows, 2, batch);
   k_selectors<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
   check_launch("k_selectors");
 }
@@ -1380,7 +1491,10 @@ void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32
 
 void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride, uint64_t *resp,
                       uint8_t *bytes, uint32_t resp_bytes, uint32_t batch, cudaStream_t st) {
-  k_modswitch<<<batch, kThreads, 0, st>>>(P, ct, ct_stride, resp, bytes, resp_bytes);
+  // without packing, 8 blocks per query share the rescale (a 128-bit
+  // division per coefficient); packing needs every value in one block
+  k_modswitch<<<dim3(batch, bytes ? 1 : 8), kThreads, 0, st>>>(P, ct, ct_stride, resp, bytes,
+                                                                resp_bytes);
   check_launch("k_modswitch");
 }
 
