@@ -5,7 +5,10 @@
 // layout (rlwe.h:17-31), so no split or compose is needed at the boundary.
 #include "opir_c4_kernels.h"
 
+#include <algorithm>
 #include <atomic>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <set>
@@ -14,6 +17,8 @@
 #include <utility>
 
 #include "opir_c4_device.cuh"
+
+#include <cooperative_groups.h>
 
 namespace opir4 {
 
@@ -39,6 +44,55 @@ void check_launch(const char *what) {
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// SMs of the current device (cached per device).
+int sm_count() {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    n = 148;
+  }
+  cache[dev] = n;
+  return n;
+}
+
+// Cluster-split levels (k4_expand_level_split, k4_mux_level_split): on
+// unless OPIR_SPLIT=0.
+bool split_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("OPIR_SPLIT");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
+}
+
+// Launch with a 1-D cluster of `c` CTAs along x.
+template <typename Kern, typename... Args>
+void launch_cluster(Kern kernel, int c, dim3 grid, size_t smem, cudaStream_t st, const char *what,
+                    Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = c;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+  check_launch(what);
 }
 
 template <typename K>
@@ -300,6 +354,157 @@ k4_expand_level(Dev4 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *__
     expand_body<0>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off);
   else
     expand_body<1>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off);
+}
+
+// Expansion level, cluster split: with fewer nodes than SMs (the top of the
+// heap, and most levels of a single query) each node's key switch runs on a
+// cluster of C CTAs. CTA r NTTs digits [r D, (r + 1) D) (D = L_KS / C) of
+// sigma_k(c1) and accumulates their Shoup products with the key rows; the
+// partial sums (below 2q D each, their total below 16q as in the single-CTA
+// sum) meet in distributed shared memory; CTA 0 finishes the b part (c0 of
+// both children), CTA 1 the a part (c1 of both children). Same children bit
+// for bit.
+template <int L, int C>
+__device__ __forceinline__ void expand_split_body(const Dev4 &P, uint32_t galois_inv,
+                                                  uint32_t kshift, const uint64_t *in,
+                                                  uint64_t in_stride, uint64_t *out,
+                                                  uint64_t out_stride,
+                                                  const uint64_t *const *bv_keys,
+                                                  uint64_t bv_level_off) {
+  static_assert(kLKs % C == 0 && kLKs / C <= kExpGroup, "digits per CTA fit the planes");
+  constexpr int D = kLKs / C;
+  extern __shared__ uint64_t sm4[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  constexpr uint64_t Q = Limb<L>::q;
+  const int rank = static_cast<int>(cluster.block_rank());
+  const int node = blockIdx.x / C, b = blockIdx.z, tid = threadIdx.x;
+  const uint64_t *ct = in + (static_cast<uint64_t>(b) * in_stride + node) * kCtWords;
+  const uint64_t *key = bv_keys[b] + bv_level_off;
+  uint64_t ab[8], aa[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
+  {
+    u128 u[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t j = posA(tid, k);
+      const uint32_t w = (j * galois_inv) & (2 * kN - 1);
+      const bool neg = w >= kN;
+      const uint32_t src = w & (kN - 1);
+      uint64_t a0 = ct[2 * kN + src], a1 = ct[3 * kN + src];
+      if (neg) { a0 = neg_mod<kQ0>(a0); a1 = neg_mod<kQ1>(a1); }
+      u[k] = bv_digit_source<kLKs, kBaseKs>(compose(a0, a1, P.q0inv, P.q0inv_sh));
+    }
+#pragma unroll
+    for (int e = 0; e < D; ++e) {
+      uint64_t v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int64_t r = static_cast<int64_t>(field<kBaseKs>(u[k], rank * D + e)) -
+                          ((1ll << (kBaseKs - 1)) - 1);
+        v[k] = r >= 0 ? static_cast<uint64_t>(r) : static_cast<uint64_t>(r + static_cast<int64_t>(Q));
+      }
+      fA<L>(v);
+      st_plane<0>(sm4 + e * kPad, v, tid);
+    }
+  }
+  __syncthreads();
+  fwd_mid<L>(sm4, D, P.T);
+  for (int e = 0; e < D; ++e) {
+    const int i = rank * D + e;
+    uint64_t v[8];
+    {
+      ulonglong2 wd[7];
+      fload_d<L>(wd, P.T);
+      ld_plane<3>(sm4 + e * kPad, v, tid);
+      fD<L>(v, wd);  // [0, 6q)
+    }
+    const uint64_t *R = key + static_cast<uint64_t>(i) * kRowWords + L * kN + 8 * tid;
+    {
+      uint64_t w[8], ws[8];
+      ld8(R, w);
+      ld8(R + 4 * kN, ws);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) ab[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
+    }
+    {
+      uint64_t w[8], ws[8];
+      ld8(R + 2 * kN, w);
+      ld8(R + 6 * kN, ws);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) aa[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
+    }
+  }
+  __syncthreads();
+  uint64_t *ex = sm4;  // [b / a][k][tid]
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    ex[(0 * 8 + k) * kThreads + tid] = ab[k];
+    ex[(1 * 8 + k) * kThreads + tid] = aa[k];
+  }
+  cluster.sync();
+  uint64_t tot[8];
+  if (rank < 2) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tot[k] = rank == 0 ? ab[k] : aa[k];
+    for (int r = 0; r < C; ++r) {
+      if (r == rank) continue;
+      const uint64_t *rex = cluster.map_shared_rank(ex, r);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) tot[k] += rex[(rank * 8 + k) * kThreads + tid];
+    }
+  }
+  cluster.sync();  // every remote read is done before shared memory is reused
+  if (rank >= 2) return;
+  {
+    ulonglong2 wd[7];
+    iload_d<L>(wd, P.T);
+    uint64_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = fold16<Q>(tot[k]);
+    iD<L>(v, wd);
+    st_plane<3>(sm4, v, tid);
+  }
+  __syncthreads();
+  inv_mid<L>(sm4, 1, P.T);
+  uint64_t dv[8];
+  ld_plane<0>(sm4, dv, tid);
+  iA<L>(dv);
+  uint64_t *outL = out + (static_cast<uint64_t>(b) * out_stride + 2ull * node) * kCtWords;
+  uint64_t *outR = outL + kCtWords;
+  const uint64_t off = static_cast<uint64_t>(rank) * 2 * kN + L * kN;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t j = posA(tid, k);
+    uint64_t nv = dv[k];
+    if (rank == 0) {  // c0' = sigma_k(c0) + delta_b
+      const uint32_t w = (j * galois_inv) & (2 * kN - 1);
+      const uint64_t z = ct[L * kN + (w & (kN - 1))];
+      nv = add_mod<Q>(w >= kN ? neg_mod<Q>(z) : z, nv);
+    }
+    const uint64_t o = ct[off + j];
+    outL[off + j] = add_mod<Q>(o, nv);
+    const uint64_t dd = sub_mod<Q>(o, nv);
+    int dst = static_cast<int>(j) - static_cast<int>(kshift);
+    const bool wrap = dst < 0;
+    if (wrap) dst += kN;
+    outR[off + dst] = wrap ? neg_mod<Q>(dd) : dd;
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(kThreads, 1)
+k4_expand_level_split(Dev4 P, uint32_t galois_inv, uint32_t kshift,
+                      const uint64_t *__restrict__ in, uint64_t in_stride,
+                      uint64_t *__restrict__ out, uint64_t out_stride,
+                      const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  if (blockIdx.y == 0)
+    expand_split_body<0, C>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                            bv_level_off);
+  else
+    expand_split_body<1, C>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                            bv_level_off);
 }
 
 // ------------------------------------------------------------ gadget product
@@ -643,6 +848,150 @@ k4_mux_level(Dev4 P, Shape4 S, uint32_t level, uint32_t n_pairs, uint32_t offset
     mux_body<1>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
 }
 
+// MUX level, cluster split: with fewer pairs than SMs each MUX runs on a
+// cluster of C CTAs. CTA r takes digits [d0, d0 + dn) of polynomial p of
+// y - x (C = 2: p = r, all l digits; C = 4: p = r / 2, digits 0-2 or 3-4),
+// accumulates their Shoup products with the RGSW rows and folds them below
+// 2q; CTAs 0 and 1 add the partials (below 2q C) through distributed shared
+// memory, fold them below 2q and finish output polynomial c0 / c1 (INTT,
+// + x). The same residues enter the same INTT: bit for bit the single-CTA
+// MUX.
+template <int L>
+__device__ __forceinline__ void gadget_part(const Dev4 &P, const uint64_t *x, const uint64_t *y,
+                                            const uint64_t *rgsw, uint64_t *sm, int p, int d0,
+                                            int dn, uint64_t (&acc0)[8], uint64_t (&acc1)[8]) {
+  constexpr uint64_t Q = Limb<L>::q;
+  const int tid = threadIdx.x;
+  {
+    u128 u[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int j = posA(tid, k);
+      const uint64_t v0 = sub_mod<kQ0>(y[p * 2 * kN + j], x[p * 2 * kN + j]);
+      const uint64_t v1 = sub_mod<kQ1>(y[p * 2 * kN + kN + j], x[p * 2 * kN + kN + j]);
+      u[k] = compose(v0, v1, P.q0inv, P.q0inv_sh);
+    }
+    for (int e = 0; e < dn; ++e) {
+      uint64_t v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = field<kBaseEp>(u[k], d0 + e);  // < 2^B < q
+      fA<L>(v);
+      st_plane<0>(sm + e * kPad, v, tid);
+    }
+  }
+  __syncthreads();
+  fwd_mid<L>(sm, dn, P.T);
+  for (int e = 0; e < dn; ++e) {
+    const int row = p * kLEp + (kLEp - 1 - (d0 + e));
+    uint64_t v[8];
+    {
+      ulonglong2 wd[7];
+      fload_d<L>(wd, P.T);
+      ld_plane<3>(sm + e * kPad, v, tid);
+      fD<L>(v, wd);
+    }
+    const uint64_t *R = rgsw + static_cast<uint64_t>(row) * kRowWords + L * kN + 8 * tid;
+    {
+      uint64_t w[8], ws[8];
+      ld8(R, w);
+      ld8(R + 4 * kN, ws);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc0[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
+    }
+    {
+      uint64_t w[8], ws[8];
+      ld8(R + 2 * kN, w);
+      ld8(R + 6 * kN, ws);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc1[k] += mul_shoup<Q>(v[k], w[k], ws[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) { acc0[k] = fold16<Q>(acc0[k]); acc1[k] = fold16<Q>(acc1[k]); }
+  __syncthreads();
+}
+
+// Pair i reads x = in[i xs], y = in[i xs + yoff] and writes out[i] (level 0
+// without a carried prefix: xs = 2, yoff = 1; level a >= 1: xs = 1,
+// yoff = half).
+template <int L, int C>
+__device__ __forceinline__ void mux_split_body(const Dev4 &P, const Shape4 &S, uint32_t level,
+                                               uint32_t xs, uint32_t yoff, const uint64_t *in,
+                                               uint64_t *out, uint64_t mid_stride,
+                                               const uint64_t *sel) {
+  static_assert(C == 2 || C == 4, "cluster of 2 or 4 CTAs");
+  extern __shared__ uint64_t sm4[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  constexpr uint64_t Q = Limb<L>::q;
+  const int rank = static_cast<int>(cluster.block_rank());
+  const int b = blockIdx.z, tid = threadIdx.x;
+  const uint32_t i = blockIdx.x / C;
+  const uint64_t *base_in = in + static_cast<uint64_t>(b) * mid_stride * kCtWords;
+  const uint64_t *x = base_in + static_cast<uint64_t>(i) * xs * kCtWords;
+  const uint64_t *y = base_in + (static_cast<uint64_t>(i) * xs + yoff) * kCtWords;
+  const uint64_t *rgsw = sel + (static_cast<uint64_t>(b) * (S.num_dims - 1) + level) * 2 * kLEp * kRowWords;
+  uint64_t acc0[8], acc1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
+  constexpr int kHalf = (kLEp + 1) / 2;
+  const int p = C == 2 ? rank : rank >> 1;
+  const int d0 = C == 2 ? 0 : (rank & 1) * kHalf;
+  const int dn = C == 2 ? kLEp : ((rank & 1) ? kLEp - kHalf : kHalf);
+  gadget_part<L>(P, x, y, rgsw, sm4, p, d0, dn, acc0, acc1);
+  uint64_t *ex = sm4;  // [output poly][k][tid]
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    ex[(0 * 8 + k) * kThreads + tid] = acc0[k];
+    ex[(1 * 8 + k) * kThreads + tid] = acc1[k];
+  }
+  cluster.sync();
+  uint64_t tot[8];
+  if (rank < 2) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tot[k] = rank == 0 ? acc0[k] : acc1[k];
+    for (int r = 0; r < C; ++r) {
+      if (r == rank) continue;
+      const uint64_t *rex = cluster.map_shared_rank(ex, r);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) tot[k] += rex[(rank * 8 + k) * kThreads + tid];
+    }
+  }
+  cluster.sync();  // every remote read is done before shared memory is reused
+  if (rank >= 2) return;
+  {
+    ulonglong2 wd[7];
+    iload_d<L>(wd, P.T);
+    uint64_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = fold16<Q>(tot[k]);  // < 2q C <= 8q -> [0, 2q)
+    iD<L>(v, wd);
+    st_plane<3>(sm4, v, tid);
+  }
+  __syncthreads();
+  inv_mid<L>(sm4, 1, P.T);
+  uint64_t v[8];
+  ld_plane<0>(sm4, v, tid);
+  iA<L>(v);
+  uint64_t *o = out + static_cast<uint64_t>(b) * mid_stride * kCtWords + static_cast<uint64_t>(i) * kCtWords;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int j = posA(tid, k);
+    o[rank * 2 * kN + L * kN + j] = add_mod<Q>(x[rank * 2 * kN + L * kN + j], v[k]);
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(kThreads, 1)
+k4_mux_level_split(Dev4 P, Shape4 S, uint32_t level, uint32_t xs, uint32_t yoff,
+                   const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
+                   uint64_t mid_stride, const uint64_t *__restrict__ sel) {
+  if (blockIdx.y == 0)
+    mux_split_body<0, C>(P, S, level, xs, yoff, in, out, mid_stride, sel);
+  else
+    mux_split_body<1, C>(P, S, level, xs, yoff, in, out, mid_stride, sel);
+}
+
 // ------------------------------------------------------------ modulus switch
 // server.cpp:1044-1075: drop q1 with rounding, then utils::rescale
 // (utils.cpp:445-462) q0 -> small_q; bit packing as save_resp_to_stream
@@ -756,12 +1105,34 @@ void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint6
   uint32_t inv = 1;
   for (uint32_t e = 0; e < 2 * kN; ++e)
     if ((static_cast<uint64_t>(galois) * e) % (2 * kN) == 1) { inv = e; break; }
-  dim3 grid(nodes, 2, batch);
   // nodes of level d are heap slots k .. k + nodes - 1, stored from slot 0;
   // children of node i go to slots 2 i, 2 i + 1 of the next buffer
-  k4_expand_level<<<grid, kThreads, smem, st>>>(P, inv, k, in, in_stride, out, out_stride, bv_keys,
-                                                 static_cast<uint64_t>(d) * bv_level_stride);
-  check_launch("k4_expand_level");
+  const uint64_t koff = static_cast<uint64_t>(d) * bv_level_stride;
+  // fewer nodes than SMs (one CTA each): a cluster of 2, 4 or 8 CTAs per node
+  const uint64_t ctas = 2ull * nodes * batch, slots = sm_count();
+  const int split = !split_enabled() ? 1
+                    : 8 * ctas <= slots ? 8 : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
+  if (split == 1) {
+    dim3 grid(nodes, 2, batch);
+    k4_expand_level<<<grid, kThreads, smem, st>>>(P, inv, k, in, in_stride, out, out_stride,
+                                                   bv_keys, koff);
+    check_launch("k4_expand_level");
+    return;
+  }
+  const dim3 grid(nodes * split, 2, batch);
+  if (split == 8) {
+    set_smem(k4_expand_level_split<8>, smem);
+    launch_cluster(k4_expand_level_split<8>, 8, grid, smem, st, "k4_expand_level_split", P, inv, k,
+                   in, in_stride, out, out_stride, bv_keys, koff);
+  } else if (split == 4) {
+    set_smem(k4_expand_level_split<4>, smem);
+    launch_cluster(k4_expand_level_split<4>, 4, grid, smem, st, "k4_expand_level_split", P, inv, k,
+                   in, in_stride, out, out_stride, bv_keys, koff);
+  } else {
+    set_smem(k4_expand_level_split<2>, smem);
+    launch_cluster(k4_expand_level_split<2>, 2, grid, smem, st, "k4_expand_level_split", P, inv, k,
+                   in, in_stride, out, out_stride, bv_keys, koff);
+  }
 }
 
 void launch_selectors(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
@@ -823,6 +1194,25 @@ void launch_mux_level(const Dev4 &P, const Shape4 &s, uint32_t level, uint32_t t
   }
   if (n_pairs + extra == 0) return;
   const size_t smem = plane_bytes(kLEp);
+  // fewer pairs than SMs (one CTA each): a cluster of 2 or 4 CTAs per pair
+  const uint64_t ctas = 2ull * n_pairs * batch, slots = sm_count();
+  const int split = (extra != 0 || !split_enabled()) ? 1
+                    : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
+  if (split != 1) {
+    // offset == extra == 0 here, so level 0 pairs (2i, 2i + 1) into i
+    const uint32_t xs = level == 0 ? 2 : 1, yoff = level == 0 ? 1 : half;
+    const dim3 g(n_pairs * split, 2, batch);
+    if (split == 4) {
+      set_smem(k4_mux_level_split<4>, smem);
+      launch_cluster(k4_mux_level_split<4>, 4, g, smem, st, "k4_mux_level_split", P, s, level, xs,
+                     yoff, in, out, mid_stride, sel);
+    } else {
+      set_smem(k4_mux_level_split<2>, smem);
+      launch_cluster(k4_mux_level_split<2>, 2, g, smem, st, "k4_mux_level_split", P, s, level, xs,
+                     yoff, in, out, mid_stride, sel);
+    }
+    return;
+  }
   set_smem(k4_mux_level, smem);
   dim3 grid(n_pairs + extra, 2, batch);
   k4_mux_level<<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,
