@@ -484,7 +484,7 @@ opir_status opir_tree_level_create(const opir_params *scheme, const opir_tree_pa
 opir_status opir_tree_select_level(opir_server *level, const uint64_t *alpha,
                                    const uint64_t *beta_selectors, uint64_t *out);
 
-/* A whole device-resident tree (single-modulus set): the query-shape server
+/* A whole device-resident tree (either parameter set): the query-shape server
  * that unpacks tree queries and one level database per level 0..L, all on
  * one device. A query is answered without host round trips between its
  * stages: expansion and selector completion on the query handle, then every
@@ -504,8 +504,9 @@ opir_status opir_tree_set_client_keys(opir_tree *tree, uint64_t client_id,
                                       const uint64_t *bv_keys, const uint32_t *galois_ks,
                                       uint32_t n_keys, const uint64_t *gsw_key);
 /* unpack_tree_query + select_level at every level for one packed tree query
- * (host buffers): selected = (L + 1) ciphertexts, level order, coefficient
- * form -- bit for bit opir_tree_select_level of each level. */
+ * (host buffers): selected = (L + 1) ciphertexts (2N u64 each, 4N under
+ * CONFIG_N4096_K2_MP), level order, coefficient form -- bit for bit
+ * opir_tree_select_level of each level. */
 opir_status opir_tree_query(opir_tree *tree, uint64_t client_id, const uint64_t *query,
                             uint64_t *selected);
 

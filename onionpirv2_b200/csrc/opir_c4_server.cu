@@ -666,6 +666,34 @@ void Server::ext_prod_mux(const uint64_t *x, const uint64_t *y, const uint64_t *
   ck(cudaStreamSynchronize(st_), "ext_prod_mux");
 }
 
+void Server::tree_unpack(uint64_t id, const uint64_t *query) {
+  check_ct_values(query, 1);
+  upload_keyptrs(&id, 1);
+  ck(cudaMemcpyAsync(lvl_[0].p, query, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  const uint64_t *leaves = run_expand(1);
+  if (sh_.num_dims > 1)
+    launch_selectors(dp_, sh_, leaves, lvl_slots_, keyptrs_.p + 1, sel_.p, 1, st_);
+}
+
+void Server::tree_select_device(const uint64_t *d_leaves, const uint64_t *d_selectors,
+                                uint64_t fold_begin, uint64_t fold_count, uint64_t *d_out) {
+  if (!db_loaded_) throw std::runtime_error("select_level before load_data");
+  ck(cudaMemcpyAsync(lvl_[0].p, d_leaves, static_cast<size_t>(sh_.n0) * kCt * 8,
+                     cudaMemcpyDeviceToDevice, st_), "alpha copy");
+  run_first_dim(lvl_[0].p, 1, nullptr);
+  const uint32_t fold = static_cast<uint32_t>(fold_count);
+  const size_t sel_words = 2ull * sh_.l_ep * kRowWords;  // one selector with companions
+  for (uint32_t a = 1; a <= fold; ++a) {  // MSB-first: step a takes selector begin+count-a
+    const uint64_t u = fold_begin + fold_count - a;
+    ck(cudaMemcpyAsync(sel_.p + a * sel_words, d_selectors + u * sel_words, sel_words * 8,
+                       cudaMemcpyDeviceToDevice, st_), "selector copy");
+  }
+  for (uint32_t a = 1; a <= fold; ++a)
+    launch_mux_level(dp_, sh_, a, sh_.num_dims - 1, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other,
+                     sel_.p, 1, st_);
+  ck(cudaMemcpyAsync(d_out, mid_[fold & 1].p, kCt * 8, cudaMemcpyDeviceToDevice, st_), "result");
+}
+
 void Server::select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32_t fold,
                          uint64_t *out) {
   if (!db_loaded_) throw std::runtime_error("select_level before load_data");

@@ -75,6 +75,21 @@ class Server {
   // MUX steps at levels 1..fold (selector slot a = step a), host buffers.
   void select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32_t fold, uint64_t *out);
 
+  // Device-resident tree (opir_tree_query), on the handle's stream, after
+  // reserve(1). Query-shape handle: unpack_tree_query of a host query into
+  // the handle's leaves (tree_leaves(), n0 alpha ciphertexts first) and
+  // selector rows (tree_selectors(), 2 L_EP rows of kRowWords per selector).
+  void tree_unpack(uint64_t id, const uint64_t *query);
+  const uint64_t *tree_leaves() const { return lvl_[sh_.h & 1].p; }
+  const uint64_t *tree_selectors() const { return sel_.p; }
+  // Level handle: select_level from the query handle's device leaves and
+  // selectors (fold step a takes selector fold_begin + fold_count - a) into
+  // d_out (one ciphertext, kCt u64).
+  void tree_select_device(const uint64_t *d_leaves, const uint64_t *d_selectors,
+                          uint64_t fold_begin, uint64_t fold_count, uint64_t *d_out);
+  // Reads and clears the tensor-core scan's error word (stream must be idle).
+  void check_device_error();
+
  private:
   struct Keys {
     opir::DevBuf<uint64_t> bv, gsw;
@@ -101,7 +116,6 @@ class Server {
   void clear_graphs();
   void mark(Events ev, int i);
   void launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n);
-  void check_device_error();
   template <typename Fill>
   void load_tiles(uint64_t logical, Fill &&fill);
 

@@ -1657,10 +1657,6 @@ opir_status opir_tree_create(const opir_params *scheme, const opir_tree_params *
   opir_tree *t = new (std::nothrow) opir_tree();
   if (!t) return OPIR_ERR_NO_MEMORY;
   const opir_status st = guarded_to(&t->last_error, [&] {
-    if (is_c4(*scheme))
-      throw std::invalid_argument(
-          "the device-resident tree is built for CONFIG_N2048_K1_COMP; select the two-limb "
-          "levels with opir_tree_level_create / opir_tree_select_level");
     t->tree = *tree;
     t->device = device;
     opir_params qp{};
@@ -1682,10 +1678,17 @@ opir_status opir_tree_create(const opir_params *scheme, const opir_tree_params *
     ck(cudaEventCreateWithFlags(&t->q_done, cudaEventDisableTiming), "event");
     t->done.resize(t->levels.size(), nullptr);
     for (auto &e : t->done) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-    t->out.alloc((tree->L + 1) * 2ull * kN);
-    ensure_capacity(t->q, 1);  // no allocation while answering
-    grow_keyptr_slots(t->q, 2);
-    for (opir_server *l : t->levels) ensure_capacity(l, 1);
+    // no allocation while answering
+    if (t->q->c4) {
+      t->out.alloc((tree->L + 1) * 4ull * scheme->poly_degree);
+      t->q->c4->reserve(1);
+      for (opir_server *l : t->levels) l->c4->reserve(1);
+    } else {
+      t->out.alloc((tree->L + 1) * 2ull * kN);
+      ensure_capacity(t->q, 1);
+      grow_keyptr_slots(t->q, 2);
+      for (opir_server *l : t->levels) ensure_capacity(l, 1);
+    }
   });
   if (st != OPIR_OK) {
     opir_tree_destroy(t);
@@ -1711,6 +1714,24 @@ opir_status opir_tree_query(opir_tree *t, uint64_t client_id, const uint64_t *qu
     if (!query || !selected) throw std::invalid_argument("null argument");
     opir_server *q = t->q;
     DeviceGuard g(t->device);
+    if (q->c4) {  // two-limb set: the same flow through opir4::Server
+      const size_t ct = 4ull * q->params.poly_degree;
+      q->c4->tree_unpack(client_id, query);
+      ck(cudaEventRecord(t->q_done, q->stream), "event record");
+      for (size_t l = 0; l < t->levels.size(); ++l) {
+        opir_server *ls = t->levels[l];
+        ck(cudaStreamWaitEvent(ls->stream, t->q_done, 0), "wait");
+        ls->c4->tree_select_device(q->c4->tree_leaves(), q->c4->tree_selectors(), ls->fold_begin,
+                                   ls->fold_count, t->out.p + l * ct);
+        ck(cudaEventRecord(t->done[l], ls->stream), "event record");
+        ck(cudaStreamWaitEvent(t->stream, t->done[l], 0), "wait");
+      }
+      ck(cudaMemcpyAsync(selected, t->out.p, t->levels.size() * ct * 8, cudaMemcpyDeviceToHost,
+                         t->stream), "download");
+      ck(cudaStreamSynchronize(t->stream), "tree query");
+      for (opir_server *ls : t->levels) ls->c4->check_device_error();
+      return;
+    }
     check_query_values(q, query, 2 * kN);
     // unpack_tree_query (src/tree_query.cpp:198-240) on the query handle
     ensure_capacity(q, 1);

@@ -237,7 +237,7 @@ class TreeLevel:
 class Tree:
     """A whole device-resident tree (opir_tree_create): unpack + select_level
     at every level per query with no host round trip between stages, the
-    levels running on their own streams (single-modulus set)."""
+    levels running on their own streams (either parameter set)."""
 
     def __init__(self, scheme: PirParams, tree: TreePirParams, level_plaintexts, device: int = 0):
         self.scheme, self.tree = scheme, tree

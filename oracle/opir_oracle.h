@@ -143,6 +143,10 @@ void oracle_c4_client_free(oracle_c4_client *c);
 void oracle_c4_client_bv_keys(const oracle_c4_client *c, uint64_t *out);
 void oracle_c4_client_gsw_key(const oracle_c4_client *c, uint64_t *out);
 int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out);
+/* tree_query.cpp:142-196 (K = 2): packed tree query; bits as for
+ * oracle_client_tree_query; out: 4N u64 limb-major. */
+int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                                const uint8_t *bits, uint32_t groups, uint64_t *out);
 void oracle_c4_client_decrypt(const oracle_c4_client *c, const uint64_t *resp,
                               uint64_t *pt_out);
 

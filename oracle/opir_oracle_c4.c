@@ -278,6 +278,51 @@ int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out) 
   }
   return 0;
 }
+/* make_tree_query (tree_query.cpp:142-196) for K = 2: a fresh encryption of
+ * zero from the client's generator, the alpha one-hot as the BFV lift of
+ * W^-1 mod t computed under Q = q0 q1 and reduced per limb
+ * (add_bfv_query_constant, :70-111), and for every set bit of group g
+ * (b beta bits, then r gamma bits) the L_EP data gadget rows scaled by
+ * W^-1 mod q_k, per limb, at BitRev(N0 + g L_EP + row, h_q)
+ * (add_rlwe_star_constant, :113-140). */
+int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                                const uint8_t *bits, uint32_t groups, uint64_t *out) {
+  const opir_oracle_c4_params *p = &c->p;
+  const uint32_t N = p->N;
+  const uint64_t t = p->t, W = 1ULL << h_q;
+  if (h_q > 12 || alpha >= N0 || N0 + (uint64_t)groups * p->l_ep > W) return -1;
+  uint64_t w_inv_t = 0;
+  if (!invmod(W % t, t, &w_inv_t)) return -1;
+  encrypt_zero_c4(p, c->sk, &c->rng, out);
+  const uint64_t rev = bitrev(alpha, h_q);
+  const u128 Q = (u128)p->q[0] * p->q[1];
+  const u128 Delta = Q / t;
+  const uint64_t r = (uint64_t)(Q - Delta * t);
+  const uint64_t r_round = (uint64_t)(((u128)r * w_inv_t + (t >> 1)) / t);
+  const u128 scaled = Delta * w_inv_t + r_round;
+  for (uint32_t k = 0; k < 2; ++k) {
+    const size_t idx = (size_t)k * N + rev;
+    out[idx] = (uint64_t)(((u128)out[idx] + (uint64_t)(scaled % p->q[k])) % p->q[k]);
+  }
+  uint64_t inv[2], gd[2][64];
+  for (uint32_t k = 0; k < 2; ++k) {
+    if (!invmod(W % p->q[k], p->q[k], &inv[k])) return -1;
+    gadget_c4(p->l_ep, p->base_ep, p->q[k], gd[k]);
+  }
+  for (uint32_t g = 0; g < groups; ++g) {
+    if (!bits[g]) continue;
+    for (uint32_t row = 0; row < p->l_ep; ++row) {
+      const uint64_t ridx = bitrev(N0 + (uint64_t)g * p->l_ep + row, h_q);
+      for (uint32_t m = 0; m < 2; ++m) {
+        const uint64_t coef = (uint64_t)((u128)gd[m][row] * inv[m] % p->q[m]);
+        const size_t at = (size_t)m * N + ridx;
+        out[at] = (uint64_t)(((u128)out[at] + coef) % p->q[m]);
+      }
+    }
+  }
+  return 0;
+}
+
 /* client.cpp:364-430 under small_q: s from limb 0, ternary re-mapped */
 void oracle_c4_client_decrypt(const oracle_c4_client *c, const uint64_t *resp, uint64_t *pt_out) {
   const opir_oracle_c4_params *p = &c->p;

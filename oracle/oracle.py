@@ -138,6 +138,9 @@ def lib():
         L.oracle_c4_client_gsw_key.argtypes = [C.c_void_p, _u64p]
         L.oracle_c4_client_query.argtypes = [C.c_void_p, C.c_uint64, _u64p]
         L.oracle_c4_client_decrypt.argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_c4_client_tree_query.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32,
+                                                  C.c_uint64, C.POINTER(C.c_uint8), C.c_uint32,
+                                                  _u64p]
         L.oracle_c4_server_new.argtypes = [P4]
         L.oracle_c4_server_new.restype = C.c_void_p
         L.oracle_c4_server_free.argtypes = [C.c_void_p]
@@ -350,6 +353,17 @@ class C4Client:
         resp = np.ascontiguousarray(resp, dtype=np.uint64)
         out = np.zeros(self.p.N, dtype=np.uint64)
         lib().oracle_c4_client_decrypt(self.h, ptr(resp), ptr(out))
+        return out
+
+    def tree_query(self, N0: int, h_q: int, alpha: int, beta_bits, gamma_bits) -> np.ndarray:
+        """make_tree_query (tree_query.cpp:142-196), K = 2."""
+        bits = np.ascontiguousarray(np.asarray(list(beta_bits) + list(gamma_bits) or [0],
+                                               dtype=np.uint8))
+        groups = len(beta_bits) + len(gamma_bits)
+        out = np.zeros((2, 2, self.p.N), dtype=np.uint64)
+        if lib().oracle_c4_client_tree_query(self.h, N0, h_q, alpha, ptr(bits, C.c_uint8), groups,
+                                             ptr(out)) != 0:
+            raise ValueError("tree query shape does not fit")
         return out
 
 

@@ -25,6 +25,7 @@ Only needed when the fixtures must change; tests never run it.
     python tests/golden/make_golden.py            # CONFIG_N2048_K1_COMP set
     python tests/golden/make_golden.py --c4       # CONFIG_N4096_K2_MP set
     python tests/golden/make_golden.py --tree     # tree PIR select_level set
+    python tests/golden/make_golden.py --tree --c4  # the same under CONFIG_N4096_K2_MP
 """
 from __future__ import annotations
 
@@ -80,19 +81,34 @@ def tree_cases():
     return out
 
 
+# the same shapes under CONFIG_N4096_K2_MP (r = log2 4096 = 12): (17, 3) and
+# (16, 2), b = 2 for both
+def tree_cases_c4():
+    out = []
+    for L, a, seed in ((17, 3, 41), (16, 2, 42)):
+        N, r = 1 << L, 12
+        b = L - r - a
+        P, B = N >> r, 1 << b
+        leaves = [0, N - 1, 0x2BADBEEF % N, P + B + (1 if b >= 2 else 0)]
+        for k, leaf in enumerate(leaves):
+            out.append((f"tree_c4_L{L}_a{a}_leaf{leaf}", L, a, seed + 10 * k, leaf))
+    return out
+
+
 def sha(path: str) -> str:
     with open(path, "rb") as f:
         return hashlib.sha256(f.read()).hexdigest()
 
 
-def main_tree() -> int:
-    if not os.path.exists(REF_BIN):
+def main_tree(c4: bool = False) -> int:
+    ref_bin = REF_BIN_C4 if c4 else REF_BIN
+    if not os.path.exists(ref_bin):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
     manifest = []
-    for name, L, a, seed, leaf in tree_cases():
+    for name, L, a, seed, leaf in (tree_cases_c4() if c4 else tree_cases()):
         with tempfile.TemporaryDirectory() as tmp:
             out = subprocess.run(
-                [REF_BIN, "--mode", "tree", "--tree-L", str(L), "--tree-a", str(a),
+                [ref_bin, "--mode", "tree", "--tree-L", str(L), "--tree-a", str(a),
                  "--client-seed", str(seed), "--leaf", str(leaf), "--out", tmp],
                 check=True, capture_output=True, text=True)
             info = json.loads(out.stdout.strip().splitlines()[-1])
@@ -112,9 +128,10 @@ def main_tree() -> int:
                                       for i in range(L + 1)],
             })
             print(f"{name}: ok", flush=True)
-    with open(os.path.join(HERE, "golden_tree.json"), "w") as f:
-        json.dump({"generator": "oracle/_ref/opir_ref --mode tree (reference sources incl. "
-                                "src/tree_*.cpp + HEXL stand-in), default PirParams scheme",
+    with open(os.path.join(HERE, "golden_tree_c4.json" if c4 else "golden_tree.json"), "w") as f:
+        json.dump({"generator": f"oracle/_ref/{os.path.basename(ref_bin)} --mode tree (reference "
+                                "sources incl. src/tree_*.cpp + HEXL stand-in), default PirParams "
+                                f"scheme{' under CONFIG_N4096_K2_MP' if c4 else ''}",
                    "node_source": "synthetic_tree_node_value (src/tree_select.cpp:44-53)",
                    "cases": manifest}, f, indent=1)
     return 0
@@ -122,7 +139,7 @@ def main_tree() -> int:
 
 def main() -> int:
     if "--tree" in sys.argv[1:]:
-        return main_tree()
+        return main_tree(c4="--c4" in sys.argv[1:])
     c4 = "--c4" in sys.argv[1:]
     ref_bin, cases_ = (REF_BIN_C4, CASES_C4) if c4 else (REF_BIN, CASES)
     if not os.path.exists(ref_bin):

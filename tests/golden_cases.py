@@ -37,6 +37,13 @@ def cases_tree():
         return json.load(f)["cases"]
 
 
+def cases_tree_c4():
+    """Tree PIR select_level cases under CONFIG_N4096_K2_MP (reference tree
+    layer built with that configuration, default scheme)."""
+    with open(os.path.join(GOLDEN_DIR, "golden_tree_c4.json")) as f:
+        return json.load(f)["cases"]
+
+
 def stream(c):
     with open(os.path.join(GOLDEN_DIR, c["name"] + ".resp.bin"), "rb") as f:
         return f.read()

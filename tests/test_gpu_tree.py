@@ -95,3 +95,62 @@ def test_device_resident_tree_matches_reference(c):
         out = t.query(c["client_seed"], q)
         for level in range(tree.L + 1):
             assert sha(out[level]) == c["sha256_levels_u64"][level], level
+
+
+# ---------------------------------------------------------- CONFIG_N4096_K2_MP
+C4 = "CONFIG_N4096_K2_MP"
+C4_CASES = G.cases_tree_c4()
+
+
+@functools.lru_cache(maxsize=None)
+def tree_levels_c4(L, a):
+    scheme = PirParams(config=C4)
+    tree = T.make_tree_pir_params_for_scheme(L, a, scheme)
+    src = lambda level, idx: T.synthetic_tree_node_value(level, idx, scheme.plain_mod)
+    pts = [T.pack_tree_level(level, tree, src) for level in range(L + 1)]
+    levels = [T.TreeLevel(scheme, tree, level, pts[level]) for level in range(L + 1)]
+    return scheme, tree, pts, levels
+
+
+def c4_client_query(c, scheme, tree):
+    cl = O.C4Client(O.c4_params(scheme.target_num_pt, scheme.expansion_height), c["client_seed"])
+    coords = T.client_index(c["leaf"], tree)
+    q = cl.tree_query(tree.N0, tree.h_q, coords.alpha, coords.beta_bits_le, coords.gamma_bits_le)
+    return cl, q
+
+
+@pytest.mark.parametrize("c", C4_CASES, ids=lambda c: c["name"])
+def test_c4_select_level_matches_reference(c):
+    """The two-limb tree layer: unpack on a query-shape server and every
+    level's select_level, bit for bit the reference built under
+    CONFIG_N4096_K2_MP (which checked that every level decrypts)."""
+    scheme, tree, pts, levels = tree_levels_c4(c["L"], c["a"])
+    cl, q = c4_client_query(c, scheme, tree)
+    qparams = T.tree_query_expansion_params(tree, scheme)
+    with PirServer(qparams) as srv:
+        srv.set_client_keys(1, cl.bv_keys()[: qparams.expansion_height], cl.gsw_key())
+        alpha, beta, gamma = T.unpack_tree_query(srv, scheme, tree, 1, q)
+    assert sha(alpha) == c["sha256_alpha_u64"]
+    assert sha(beta) == c["sha256_beta_selectors_u64"]
+    for level in range(tree.L + 1):
+        out = levels[level].select_level(alpha, beta)
+        assert sha(out) == c["sha256_levels_u64"][level], level
+
+
+@functools.lru_cache(maxsize=None)
+def whole_tree_c4(L, a):
+    scheme, tree, pts, _ = tree_levels_c4(L, a)
+    return T.Tree(scheme, tree, pts)
+
+
+@pytest.mark.parametrize("c", C4_CASES, ids=lambda c: c["name"])
+def test_c4_device_resident_tree_matches_reference(c):
+    scheme, tree, pts, _ = tree_levels_c4(c["L"], c["a"])
+    t = whole_tree_c4(c["L"], c["a"])
+    cl, q = c4_client_query(c, scheme, tree)
+    t.set_client_keys(c["client_seed"], cl.bv_keys(), cl.gsw_key())
+    for _ in range(2):
+        out = t.query(c["client_seed"], q)
+        assert out.shape == (tree.L + 1,) + scheme.ct_shape
+        for level in range(tree.L + 1):
+            assert sha(out[level]) == c["sha256_levels_u64"][level], level
