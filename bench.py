@@ -72,6 +72,9 @@ def parse():
                          "1,8,32,64 for c4; 'none' to skip)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default scan tiling (or OPIR_SCAN_TILE)")
+    ap.add_argument("--tree-config", choices=["k1", "c4"], default="k1",
+                    help="--workload tree: CONFIG_N2048_K1_COMP (L=16, a=3) or CONFIG_N4096_K2_MP "
+                         "(L=17, a=3)")
     ap.add_argument("--rows-sharded", action="store_true",
                     help="one database split by candidate rows over the ranks (strong scaling)")
     ap.add_argument("--serve", action="store_true",
@@ -686,21 +689,28 @@ def bench_serve(args, world, rank, local):
 TREE_L, TREE_A = 16, 3
 
 
-def run_reference_tree(runs: int) -> dict:
+def tree_shape(c4: bool):
+    """(parameter set name, L, a) of the tree workload."""
+    return (C4_CONFIG, 17, 3) if c4 else ("CONFIG_N2048_K1_COMP", TREE_L, TREE_A)
+
+
+def run_reference_tree(runs: int, c4: bool = False) -> dict:
     """The reference's tree layer (driver mode "tree"): server-side time of
     one tree query (unpack_tree_query + select_level at every level), best of
     the portable and AVX-512 builds, `runs` queries each."""
     best = None
-    for exe in (os.path.join(ROOT, "oracle", "_ref", "opir_ref"),
-                os.path.join(ROOT, "oracle", "_ref", "opir_ref_avx512")):
+    _, L, a = tree_shape(c4)
+    base = "opir_ref_c4" if c4 else "opir_ref"
+    for exe in (os.path.join(ROOT, "oracle", "_ref", base),
+                os.path.join(ROOT, "oracle", "_ref", base + "_avx512")):
         if not os.path.exists(exe):
             continue
         ms = []
         for k in range(runs):
             import tempfile
             with tempfile.TemporaryDirectory() as tmp:
-                out = subprocess.run([exe, "--mode", "tree", "--tree-L", str(TREE_L), "--tree-a",
-                                      str(TREE_A), "--leaf", str(37 + 1000 * k), "--client-seed",
+                out = subprocess.run([exe, "--mode", "tree", "--tree-L", str(L), "--tree-a",
+                                      str(a), "--leaf", str(37 + 1000 * k), "--client-seed",
                                       str(61 + k), "--out", tmp],
                                      check=True, capture_output=True, text=True)
             ms.append(json.loads(out.stdout.strip().splitlines()[-1])["server_ms"])
@@ -717,8 +727,10 @@ def bench_reference_tree(args, procs):
     processes, each timing min(steps, 3) tree queries server-side."""
     from concurrent.futures import ThreadPoolExecutor
     runs = max(1, min(args.steps, 3))
+    c4 = args.tree_config == "c4"
+    cfg_name, L, A = tree_shape(c4)
     try:
-        best = run_reference_tree(1)              # picks the faster build
+        best = run_reference_tree(1, c4)          # picks the faster build
         exe = os.path.join(ROOT, "oracle", "_ref", best["binary"])
 
         def one(k):
@@ -726,8 +738,8 @@ def bench_reference_tree(args, procs):
             ms = []
             for j in range(runs):
                 with tempfile.TemporaryDirectory() as tmp:
-                    out = subprocess.run([exe, "--mode", "tree", "--tree-L", str(TREE_L),
-                                          "--tree-a", str(TREE_A), "--leaf", str(37 + 97 * (k * runs + j)),
+                    out = subprocess.run([exe, "--mode", "tree", "--tree-L", str(L),
+                                          "--tree-a", str(A), "--leaf", str(37 + 97 * (k * runs + j)),
                                           "--client-seed", str(100 + k * runs + j), "--out", tmp],
                                          check=True, capture_output=True, text=True)
                 ms.append(json.loads(out.stdout.strip().splitlines()[-1])["server_ms"])
@@ -747,7 +759,7 @@ def bench_reference_tree(args, procs):
         "value": qps, "unit": "tree queries/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mean, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"tree PIR L={TREE_L} a={TREE_A} on CONFIG_N2048_K1_COMP", "batch": 1,
+        "config": {"workload": f"tree PIR L={L} a={A} on {cfg_name}", "batch": 1,
                    "parallelism": f"{procs} host processes"},
         "cpu_baseline": {"value": qps, "unit": "tree queries/s", "cores": procs, "kind": "reference",
                          "sample": (f"reference unpack_tree_query + select_level (oracle/_ref/"
@@ -776,8 +788,10 @@ def bench_tree(args, world, rank, local):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
-    scheme = PirParams()
-    tree = T.make_tree_pir_params_for_scheme(TREE_L, TREE_A, scheme)
+    c4 = args.tree_config == "c4"
+    cfg_name, L, A = tree_shape(c4)
+    scheme = PirParams(config=cfg_name)
+    tree = T.make_tree_pir_params_for_scheme(L, A, scheme)
     src = lambda level, idx: T.synthetic_tree_node_value(level, idx, scheme.plain_mod)
     t0 = time.perf_counter()
     whole = T.Tree(scheme, tree, [T.pack_tree_level(lv, tree, src) for lv in range(tree.L + 1)],
@@ -786,7 +800,7 @@ def bench_tree(args, world, rank, local):
     qp = T.tree_query_expansion_params(tree, scheme)
     queries, keys = synthetic_inputs(qp, 1, 4000 + rank)
     whole.set_client_keys(0, *keys[0])
-    out = np.zeros((tree.L + 1, 2, scheme.N), dtype=np.uint64)
+    out = np.zeros((tree.L + 1,) + scheme.ct_shape, dtype=np.uint64)
 
     def step():
         whole.query(0, queries[0])
@@ -813,9 +827,9 @@ def bench_tree(args, world, rank, local):
         "metric": "tree PIR paths/s (unpack + select_level at every level, bit-exact)",
         "value": qps, "unit": "tree queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64" if c4 else "u32",
         "data": "synthetic (seeded uniform query and keys mod q; synthetic_tree_node_value tree)",
-        "config": {"workload": f"tree PIR L={TREE_L} a={TREE_A} on CONFIG_N2048_K1_COMP: N0="
+        "config": {"workload": f"tree PIR L={L} a={A} on {cfg_name}: N0="
                                f"{tree.N0}, b={tree.b}, r={tree.r}, h_q={tree.h_q}, "
                                f"{tree.L + 1} levels", "batch": 1,
                    "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -826,7 +840,7 @@ def bench_tree(args, world, rank, local):
     }
     if world == 1 and not args.no_cpu_baseline:
         try:
-            res = run_reference_tree(3)
+            res = run_reference_tree(3, c4)
             line["cpu_baseline"] = {
                 "value": 1000.0 / res["mean_ms"], "unit": "tree queries/s", "cores": 1,
                 "kind": "reference",
