@@ -645,8 +645,10 @@ k4_selectors(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t lea
 
 // ------------------------------------------------------------ first-dim query
 // Forward NTT per limb of the first n0 leaves (server.cpp:205-262) into
-// qm[z][col][k] (col = 2 query + poly, k < n0), then k4_fst_pack splits it
-// into the scan's eight byte planes qb[(z 8 + plane)][col][n0p].
+// qm[col][k][z] (col = 2 query + poly, k < n0, z = limb N + coefficient:
+// each thread stores its 4-coefficient runs, so the stores are coalesced),
+// then k4_fst_pack transposes it through shared memory into the scan's eight
+// byte planes qb[(z 8 + plane)][col][n0p].
 constexpr int kFstTile = 2;  // leaves per CTA (4 planes)
 
 template <int L>
@@ -677,10 +679,15 @@ __device__ __forceinline__ void fst_body(const Dev4 &P, const Shape4 &S, const u
     uint64_t v[8];
     ld_plane<3>(sm4 + e * kPad, v, tid);
     fD<L>(v, wd);
+    uint64_t *dst = qm + ((static_cast<uint64_t>(2 * b + p)) * S.n0 + kk) * (2 * kN) +
+                    static_cast<uint64_t>(L) * kN;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
-      qm[(z * ncols + 2 * b + p) * S.n0 + kk] = canon8<Limb<L>::q>(v[k]);
+    for (int h = 0; h < 2; ++h) {  // D-order positions 4 (tid + 512 h) .. + 3
+      const int j0 = posD(tid, 4 * h);
+      *reinterpret_cast<ulonglong2 *>(dst + j0) =
+          make_ulonglong2(canon8<Limb<L>::q>(v[4 * h + 0]), canon8<Limb<L>::q>(v[4 * h + 1]));
+      *reinterpret_cast<ulonglong2 *>(dst + j0 + 2) =
+          make_ulonglong2(canon8<Limb<L>::q>(v[4 * h + 2]), canon8<Limb<L>::q>(v[4 * h + 3]));
     }
   }
 }
@@ -694,19 +701,27 @@ k4_fst_ntt(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t leaf_
     fst_body<1>(P, S, leaves, leaf_stride, qm, ncols);
 }
 
-// One thread per (z, col, 16 consecutive k): 128 contiguous bytes in, one
-// 16-byte store per plane out; k in [n0, n0p) reads as zero.
+// A CTA transposes a tile of 32 coefficients z x 128 leaves k of one column
+// through shared memory: 128 rows of 32 consecutive z in (256-byte reads),
+// then one thread per (z, 16 consecutive k) builds that run's eight byte
+// planes and writes 16 bytes per plane (8 threads cover a 128-byte row);
+// k in [n0, n0p) reads as zero.
+constexpr int kPackZ = 32, kPackK = 128;
 __global__ void __launch_bounds__(256)
 k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t ncols,
             uint8_t *__restrict__ qb) {
-  const uint32_t chunks = n0p / 16;
-  const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const uint64_t total = static_cast<uint64_t>(2 * kN) * ncols * chunks;
-  if (idx >= total) return;
-  const uint32_t chunk = static_cast<uint32_t>(idx % chunks);
-  const uint64_t zc = idx / chunks;  // z ncols + col
-  const uint64_t z = zc / ncols, col = zc % ncols;
-  const uint64_t *src = qm + zc * n0;
+  __shared__ uint64_t tile[kPackK][kPackZ + 1];
+  const uint32_t z0 = blockIdx.x * kPackZ, col = blockIdx.y, k0 = blockIdx.z * kPackK;
+  const int t = threadIdx.x;
+  const uint64_t *src = qm + static_cast<uint64_t>(col) * n0 * (2 * kN) + z0;
+#pragma unroll 4
+  for (int i = t; i < kPackK * kPackZ; i += 256) {
+    const int kk = i / kPackZ, zz = i % kPackZ;
+    const uint32_t k = k0 + kk;
+    tile[kk][zz] = k < n0 ? src[static_cast<uint64_t>(k) * (2 * kN) + zz] : 0;
+  }
+  __syncthreads();
+  const int chunk = t % (kPackK / 16), zz = t / (kPackK / 16);
   uint32_t w[8][4];
 #pragma unroll
   for (int pl = 0; pl < 8; ++pl)
@@ -714,14 +729,16 @@ k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t
     for (int j = 0; j < 4; ++j) w[pl][j] = 0;
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
-    const uint32_t k = chunk * 16 + i;
-    const uint64_t v = k < n0 ? src[k] : 0;
+    const uint64_t v = tile[chunk * 16 + i][zz];
 #pragma unroll
     for (int pl = 0; pl < 8; ++pl)
       w[pl][i >> 2] |= static_cast<uint32_t>((v >> (8 * pl)) & 0xFF) << (8 * (i & 3));
   }
   const uint64_t plane_bytes = static_cast<uint64_t>(ncols) * n0p;
-  uint8_t *dst = qb + z * 8 * plane_bytes + col * n0p + chunk * 16;
+  const uint64_t z = z0 + zz;
+  const uint32_t k = k0 + chunk * 16;
+  if (k >= n0p) return;
+  uint8_t *dst = qb + z * 8 * plane_bytes + static_cast<uint64_t>(col) * n0p + k;
 #pragma unroll
   for (int pl = 0; pl < 8; ++pl)
     *reinterpret_cast<uint4 *>(dst + pl * plane_bytes) = make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
@@ -1158,9 +1175,8 @@ void launch_fst_ntt(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint
 void launch_fst_pack(const Shape4 &s, const uint64_t *qm, uint8_t *qb, uint32_t batch,
                      cudaStream_t st) {
   const uint32_t ncols = 2 * batch;
-  const uint64_t threads = static_cast<uint64_t>(2 * kN) * ncols * (s.n0p / 16);
-  const unsigned blocks = static_cast<unsigned>((threads + 255) / 256);
-  k4_fst_pack<<<blocks, 256, 0, st>>>(qm, s.n0, s.n0p, ncols, qb);
+  const dim3 grid(2 * kN / kPackZ, ncols, (s.n0p + kPackK - 1) / kPackK);
+  k4_fst_pack<<<grid, 256, 0, st>>>(qm, s.n0, s.n0p, ncols, qb);
   check_launch("k4_fst_pack");
 }
 
