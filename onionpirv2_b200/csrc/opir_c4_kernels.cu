@@ -747,10 +747,11 @@ k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t
 // ------------------------------------------------------------ scan epilogue
 // inter_to_cts (server.cpp:405-527): INTT per limb of every candidate. A CTA
 // transforms 4 consecutive rows of one column and one limb, reading the
-// scan's cmat[z][col][row] as 32-byte row groups.
+// scan's cmat[z][col][row] as 32-byte row groups (two 16-byte loads each
+// when the row count is even, so that every group is 16-byte aligned).
 constexpr int kEpiRows = 4;
 
-template <int L>
+template <int L, bool VEC>
 __device__ __forceinline__ void epi_body(const Dev4 &P, const Shape4 &S, const uint64_t *cmat,
                                          uint32_t ncols, uint64_t *mid, uint64_t mid_stride) {
   extern __shared__ uint64_t sm4[];
@@ -762,8 +763,14 @@ __device__ __forceinline__ void epi_body(const Dev4 &P, const Shape4 &S, const u
     for (int k = 0; k < 8; ++k) {
       const uint64_t z = static_cast<uint64_t>(L) * kN + posD(tid, k);
       const uint64_t *src = cmat + (z * ncols + c) * S.other + r0;
+      if (VEC && r0 + kEpiRows <= S.other) {
+        const ulonglong2 a = *reinterpret_cast<const ulonglong2 *>(src);
+        const ulonglong2 b = *reinterpret_cast<const ulonglong2 *>(src + 2);
+        v[0][k] = a.x; v[1][k] = a.y; v[2][k] = b.x; v[3][k] = b.y;
+      } else {
 #pragma unroll
-      for (int e = 0; e < kEpiRows; ++e) v[e][k] = r0 + e < S.other ? src[e] : 0;
+        for (int e = 0; e < kEpiRows; ++e) v[e][k] = r0 + e < S.other ? src[e] : 0;
+      }
     }
     ulonglong2 wd[7];
     iload_d<L>(wd, P.T);
@@ -788,13 +795,14 @@ __device__ __forceinline__ void epi_body(const Dev4 &P, const Shape4 &S, const u
   }
 }
 
+template <bool VEC>
 __global__ void __launch_bounds__(kThreads, 1)
 k4_epilogue(Dev4 P, Shape4 S, const uint64_t *__restrict__ cmat, uint32_t ncols,
             uint64_t *__restrict__ mid, uint64_t mid_stride) {
   if (blockIdx.y == 0)
-    epi_body<0>(P, S, cmat, ncols, mid, mid_stride);
+    epi_body<0, VEC>(P, S, cmat, ncols, mid, mid_stride);
   else
-    epi_body<1>(P, S, cmat, ncols, mid, mid_stride);
+    epi_body<1, VEC>(P, S, cmat, ncols, mid, mid_stride);
 }
 
 // ------------------------------------------------------------ MUX level
@@ -1183,9 +1191,15 @@ void launch_fst_pack(const Shape4 &s, const uint64_t *qm, uint8_t *qb, uint32_t 
 void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint64_t *mid,
                      uint64_t mid_stride, uint32_t batch, cudaStream_t st) {
   const size_t smem = plane_bytes(kEpiRows);
-  set_smem(k4_epilogue, smem);
   dim3 grid((s.other + kEpiRows - 1) / kEpiRows, 2, 2 * batch);
-  k4_epilogue<<<grid, kThreads, smem, st>>>(P, s, cmat, 2 * batch, mid, mid_stride);
+  // an even row count keeps every 4-row group (r0 a multiple of 4) 16-byte aligned
+  if (s.other % 2 == 0) {
+    set_smem(k4_epilogue<true>, smem);
+    k4_epilogue<true><<<grid, kThreads, smem, st>>>(P, s, cmat, 2 * batch, mid, mid_stride);
+  } else {
+    set_smem(k4_epilogue<false>, smem);
+    k4_epilogue<false><<<grid, kThreads, smem, st>>>(P, s, cmat, 2 * batch, mid, mid_stride);
+  }
   check_launch("k4_epilogue");
 }
 
