@@ -621,15 +621,22 @@ __device__ __forceinline__ void fst_ntt_body(const DevParams &P, const Shape &S,
   const int b = blockIdx.z, tid = threadIdx.x;
   const uint32_t k0 = blockIdx.x * kFstTile;
   const ResidueTables &T = P.r[RES];
-  for (int e = 0; e < 2 * kFstTile; ++e) {
-    const uint32_t kk = k0 + (e >> 1);
-    const int p = e & 1;
-    uint32_t v[8];
-    const uint32_t *src = leaves + ((uint64_t)b * leaf_stride + kk) * kCtWords + (p * 2 + RES) * kN;
+  {
+    // every plane's loads first (more loads in flight), then the first pass
+    uint32_t v[2 * kFstTile][8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = kk < S.n0 ? src[posA(tid, k)] : 0u;
-    fA<RES>(v);
-    st_plane<0>(sm + e * kPad, v, tid);
+    for (int e = 0; e < 2 * kFstTile; ++e) {
+      const uint32_t kk = k0 + (e >> 1);
+      const int p = e & 1;
+      const uint32_t *src = leaves + ((uint64_t)b * leaf_stride + kk) * kCtWords + (p * 2 + RES) * kN;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[e][k] = kk < S.n0 ? src[posA(tid, k)] : 0u;
+    }
+#pragma unroll
+    for (int e = 0; e < 2 * kFstTile; ++e) {
+      fA<RES>(v[e]);
+      st_plane<0>(sm + e * kPad, v[e], tid);
+    }
   }
   __syncthreads();
   fwd_mid_r<RES>(sm, 2 * kFstTile, T.fwt);
