@@ -584,10 +584,12 @@ def bench_ours(args, world, rank, local):
 
 
 # ---------------------------------------------------------------- serving loop
-SERVE_DBS = [  # name, plaintexts, expansion height, share of arrivals, batch limit, parameter set
-    ("c1_54MB", 16384, 9, 0.6, 32, "CONFIG_N2048_K1_COMP"),
-    ("c2_872MB", 262144, 10, 0.3, 32, "CONFIG_N2048_K1_COMP"),
-    ("c4_n4096_1M", 1 << 20, 11, 0.1, 16, C4_CONFIG),
+SERVE_DBS = [  # name, plaintexts, expansion height, share of arrivals, batch limit, parameter
+    # set, CUDA stream priority (cheapest queries first: the two-limb batches hold the GPU for
+    # tens of ms, so the k1_comp lanes overtake them)
+    ("c1_54MB", 16384, 9, 0.6, 32, "CONFIG_N2048_K1_COMP", -2),
+    ("c2_872MB", 262144, 10, 0.3, 32, "CONFIG_N2048_K1_COMP", -1),
+    ("c4_n4096_1M", 1 << 20, 11, 0.1, 16, C4_CONFIG, 0),
 ]
 
 
@@ -608,9 +610,9 @@ def bench_serve(args, world, rank, local):
     n_clients = 16
     inputs = {}
     t0 = time.perf_counter()
-    for k, (name, target, h, _share, mb, cfg) in enumerate(SERVE_DBS):
+    for k, (name, target, h, _share, mb, cfg, prio) in enumerate(SERVE_DBS):
         params = PirParams(target, h, config=cfg)
-        eng.add_database(name, params, max_batch=mb, seed=DB_SEED + k)
+        eng.add_database(name, params, max_batch=mb, seed=DB_SEED + k, priority=prio)
         queries, keys = synthetic_inputs(params, n_clients, 3000 + 100 * k + rank)
         for j, (bv, gsw) in enumerate(keys):
             eng.register_client(name, j, bv, gsw)
@@ -672,8 +674,9 @@ def bench_serve(args, world, rank, local):
                                "CONFIG_N4096_K2_MP 2^20), arrivals mixed "
                                + "/".join(f"{int(100 * x)}" for x in shares),
                    "databases": {nm: {"num_pt": PirParams(t, h, config=cfg).num_pt,
-                                      "expansion_height": h, "max_batch": mb, "params": cfg}
-                                 for nm, t, h, _s, mb, cfg in SERVE_DBS},
+                                      "expansion_height": h, "max_batch": mb, "params": cfg,
+                                      "stream_priority": prio}
+                                 for nm, t, h, _s, mb, cfg, prio in SERVE_DBS},
                    "depth": eng.depth, "clients_per_db": n_clients,
                    "duration_s_per_rate": args.duration},
         "levels": results,

@@ -319,6 +319,15 @@ opir_status opir_server_scan_tile(const opir_server *server, uint32_t n,
                                   uint32_t *ntile, uint32_t *kt,
                                   uint32_t *stages);
 
+/* No counterpart in the reference. Moves the handle's work to a new CUDA
+ * stream of the given priority (cudaStreamCreateWithPriority: lower numbers
+ * are scheduled first; values outside the device's range are clamped), after
+ * the work already on the old stream has finished. A serving loop gives
+ * databases whose queries are cheap a higher priority than those whose
+ * batches hold the GPU for long, so cheap queries are not queued behind
+ * expensive ones. Results do not depend on the priority. */
+opir_status opir_server_set_priority(opir_server *server, int priority);
+
 /* Per-stage device times (ms), averaged over the make_query / batch calls
  * made since stage timing was (re-)enabled, in the reference's TimerLogger
  * sections (includes/logging.h:34-78): [0] Expand, [1] Convert,

@@ -56,6 +56,9 @@ class Server {
   void make_query_batch_device(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
                                uint64_t *d_responses, Events ev);
   void reserve(uint32_t max_batch);
+  // The stream the handle's work is enqueued on from now on (the caller has
+  // synchronised the previous one).
+  void set_stream(cudaStream_t st) { st_ = st; }
   static void plan_memory(const opir_params &p, opir_memory_plan *out);
 
   // Public stages of make_query (host buffers, reference layouts).

@@ -1221,6 +1221,22 @@ opir_status opir_server_combine_shards_device(opir_server *s, uint32_t n,
   });
 }
 
+opir_status opir_server_set_priority(opir_server *s, int priority) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    DeviceGuard g(s->device);
+    int least = 0, greatest = 0;
+    ck(cudaDeviceGetStreamPriorityRange(&least, &greatest), "priority range");
+    const int p = std::min(std::max(priority, greatest), least);  // greatest < least
+    cudaStream_t ns = nullptr;
+    ck(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, p), "cudaStreamCreateWithPriority");
+    ck(cudaStreamSynchronize(s->stream), "set_priority");
+    if (s->c4) s->c4->set_stream(ns);
+    cudaStreamDestroy(s->stream);
+    s->stream = ns;
+  });
+}
+
 opir_status opir_plan_memory(const opir_params *params, opir_memory_plan *out) {
   if (!params || !out) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] {

@@ -273,6 +273,11 @@ class PirServer:
         that later calls of that size allocate no device memory."""
         self._check(self._lib.opir_server_reserve(self._h, int(max_batch)))
 
+    def set_priority(self, priority: int):
+        """Run the handle's work on a stream of this CUDA priority (lower =
+        scheduled first); results are unchanged."""
+        self._check(self._lib.opir_server_set_priority(self._h, int(priority)))
+
     def autotune(self, max_batch: int):
         """Time the tensor-core scan's tilings on this database for batches
         up to max_batch and keep the fastest per batch-size bucket."""

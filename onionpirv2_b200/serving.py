@@ -76,6 +76,13 @@ class CudaLane:
     def set_client_keys(self, client_id, bv_keys, gsw_key):
         self.server.set_client_keys(client_id, bv_keys, gsw_key)
 
+    def set_priority(self, priority: int):
+        """CUDA stream priority of this database's copies and kernels."""
+        torch = self.torch
+        self.stream.synchronize()
+        self.stream = torch.cuda.Stream(self.stream.device, priority=priority)
+        self.server.set_priority(priority)
+
     def launch(self, slot: int, client_ids, queries: list) -> None:
         torch = self.torch
         n = len(client_ids)
@@ -173,9 +180,12 @@ class ServingEngine:
                 + CudaLane.buffer_bytes(params, max_batch, self.depth))
 
     def add_database(self, name: str, params: PirParams, max_batch: int = 32,
-                     seed: int | None = None, plaintexts=None, min_fill: int | None = None):
+                     seed: int | None = None, plaintexts=None, min_fill: int | None = None,
+                     priority: int | None = None):
         """Admit a database (seeded synthetic or the given plaintexts) that
-        answers batches of up to max_batch queries."""
+        answers batches of up to max_batch queries. `priority` (CUDA stream
+        priority, lower = first) lets a database with cheap queries overtake
+        the long batches of an expensive one on the GPU."""
         if name in self.dbs:
             raise ValueError(f"database {name} exists")
         self._reserve(self.database_bytes(params, max_batch), f"database {name}")
@@ -184,6 +194,8 @@ class ServingEngine:
         except BaseException:
             self.reserved -= self.database_bytes(params, max_batch)
             raise
+        if priority is not None and hasattr(lane, "set_priority"):
+            lane.set_priority(priority)
         mf = max(1, max_batch // 4) if min_fill is None else max(1, min_fill)
         self.dbs[name] = _Database(name, params, lane, max_batch, self.depth, mf)
 

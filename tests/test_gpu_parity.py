@@ -271,3 +271,12 @@ def test_graph_replays_match_eager_launches(monkeypatch):
     assert st["calls"] == 2 and st["Core"] > 0 and st["Expand"] > 0
     eager.close()
     graphed.close()
+
+
+def test_stream_priority_leaves_results_unchanged():
+    """opir_server_set_priority moves the work to another stream; the
+    responses stay the reference's."""
+    c, op, cl, bv, gsw, q, gp, srv = setup("c1_16384_h9")
+    for prio in (-1, 0, -100):
+        srv.set_priority(prio)
+        _check_response(c, cl, op, srv.make_query(7, q))

@@ -210,3 +210,11 @@ def test_c4_ext_prod_mux_matches_oracle():
     for a, b, s in ((0, 1, 0), (3, 2, 1)):
         got = srv.ext_prod_mux(mid[a], mid[b], sel[s])
         assert np.array_equal(got, O.ext_prod_mux(op, mid[a], mid[b], sel[s]))
+
+
+def test_c4_stream_priority_leaves_results_unchanged():
+    c, op, cl, bv, gsw, q, gp, srv = setup("c4_2048_h7")
+    srv.set_priority(-1)
+    resp = srv.make_query(7, q)
+    assert G.sha256(resp) == c["sha256_response_u64"]
+    srv.set_priority(0)
