@@ -705,12 +705,14 @@ k4_fst_ntt(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t leaf_
 // through shared memory: 128 rows of 32 consecutive z in (256-byte reads),
 // then one thread per (z, 16 consecutive k) builds that run's eight byte
 // planes and writes 16 bytes per plane (8 threads cover a 128-byte row);
-// k in [n0, n0p) reads as zero.
-constexpr int kPackZ = 32, kPackK = 128;
+// k in [n0, n0p) reads as zero. The tile is z-major with 16-k runs 18 words
+// apart and rows 145 words apart, so both the fill (32 z of one k) and the
+// run reads (8 runs x 4 z) touch every bank pair at most twice.
+constexpr int kPackZ = 32, kPackK = 128, kRunPitch = 18, kRowPitch = 145;
 __global__ void __launch_bounds__(256)
 k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t ncols,
             uint8_t *__restrict__ qb) {
-  __shared__ uint64_t tile[kPackK][kPackZ + 1];
+  __shared__ uint64_t tile[(kPackZ - 1) * kRowPitch + (kPackK / 16 - 1) * kRunPitch + 16];
   const uint32_t z0 = blockIdx.x * kPackZ, col = blockIdx.y, k0 = blockIdx.z * kPackK;
   const int t = threadIdx.x;
   const uint64_t *src = qm + static_cast<uint64_t>(col) * n0 * (2 * kN) + z0;
@@ -718,10 +720,12 @@ k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t
   for (int i = t; i < kPackK * kPackZ; i += 256) {
     const int kk = i / kPackZ, zz = i % kPackZ;
     const uint32_t k = k0 + kk;
-    tile[kk][zz] = k < n0 ? src[static_cast<uint64_t>(k) * (2 * kN) + zz] : 0;
+    tile[zz * kRowPitch + (kk / 16) * kRunPitch + kk % 16] =
+        k < n0 ? src[static_cast<uint64_t>(k) * (2 * kN) + zz] : 0;
   }
   __syncthreads();
   const int chunk = t % (kPackK / 16), zz = t / (kPackK / 16);
+  const uint64_t *run = tile + zz * kRowPitch + chunk * kRunPitch;
   uint32_t w[8][4];
 #pragma unroll
   for (int pl = 0; pl < 8; ++pl)
@@ -729,7 +733,7 @@ k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t
     for (int j = 0; j < 4; ++j) w[pl][j] = 0;
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
-    const uint64_t v = tile[chunk * 16 + i][zz];
+    const uint64_t v = run[i];
 #pragma unroll
     for (int pl = 0; pl < 8; ++pl)
       w[pl][i >> 2] |= static_cast<uint32_t>((v >> (8 * pl)) & 0xFF) << (8 * (i & 3));
