@@ -396,6 +396,56 @@ opir_status opir_server_ext_prod_mux(opir_server *server, const uint64_t *x,
 size_t opir_save_response(const opir_params *params, const uint64_t *response,
                           uint8_t *out, size_t cap);
 
+/* ---- wire codec: seed-compressed queries and client keys -----------------
+ * No serializer exists in the reference; its communication model
+ * (includes/pir.h:115-139) counts a 32-byte seed in place of every uniformly
+ * random polynomial. This codec is that model as a format. Each uniform
+ * polynomial -- a query's c1, the a of every BV key row, the c1 of every RGSW
+ * row -- is Expand(seed, domain, index): the ChaCha20 block function
+ * (RFC 8439) keyed by the seed, nonce = domain (u32 little-endian) || index
+ * (u64 little-endian), block counter from 0, read as little-endian u64
+ * words; limb k takes, coefficient by coefficient, the next word whose low
+ * bit_length(q_k) bits are below q_k (limb-major; under
+ * CONFIG_N2048_K1_COMP the one limb is the logical q). A client builds its
+ * ciphertexts around these polynomials (opir_prf_expand): for an RGSW row
+ * whose message sits in c1, it takes c1 from the seed and derives its `a`
+ * as c1 - m g. The other polynomial is packed at bit_length(q_k) bits per
+ * coefficient, LSB first, limb by limb.
+ *   query   : "OPQ1" | seed | c0                      (k1_comp: 14,884 bytes)
+ *   keys    : "OPK1" | seed | b of the h x L_KS BV rows (level-major, the
+ *             galois_k of level i is (N >> i) + 1) | c0 of the 2 L_KEY RGSW
+ *             rows                                  (k1_comp, h = 10: 1.49 MB)
+ * Query indices: domain OPIR_PRF_QUERY, index 0; BV row j of level i:
+ * OPIR_PRF_BV_KEY, index i L_KS + j; RGSW row r: OPIR_PRF_GSW_KEY, index r.
+ * Encoders reject a uniform polynomial that is not Expand(seed) and any
+ * unreduced coefficient (OPIR_ERR_INVALID_ARGUMENT); decoders reject a wrong
+ * magic or length. */
+#define OPIR_SEED_BYTES 32
+typedef enum {
+  OPIR_PRF_QUERY = 1,
+  OPIR_PRF_BV_KEY = 2,
+  OPIR_PRF_GSW_KEY = 3
+} opir_prf_domain;
+/* Expand(seed, domain, index): K x N u64. */
+opir_status opir_prf_expand(const opir_params *params, const uint8_t *seed, uint32_t domain,
+                            uint64_t index, uint64_t *out);
+size_t opir_query_wire_bytes(const opir_params *params);
+size_t opir_keys_wire_bytes(const opir_params *params);
+/* query: the [c0][c1] ciphertext (c1 = Expand(seed, OPIR_PRF_QUERY, 0));
+ * out: opir_query_wire_bytes bytes (cap at least that). */
+opir_status opir_query_encode(const opir_params *params, const uint8_t *seed,
+                              const uint64_t *query, uint8_t *out, size_t cap);
+opir_status opir_query_decode(const opir_params *params, const uint8_t *in, size_t len,
+                              uint64_t *query);
+/* bv_keys / gsw_key in the opir_server_set_client_keys layouts, h =
+ * params->expansion_height levels in galois order (N >> i) + 1;
+ * decode also fills galois_ks (h entries). */
+opir_status opir_keys_encode(const opir_params *params, const uint8_t *seed,
+                             const uint64_t *bv_keys, const uint64_t *gsw_key,
+                             uint8_t *out, size_t cap);
+opir_status opir_keys_decode(const opir_params *params, const uint8_t *in, size_t len,
+                             uint64_t *bv_keys, uint32_t *galois_ks, uint64_t *gsw_key);
+
 /* ---- allocation-free MUX ------------------------------------------------- */
 
 /* No counterpart in the reference. For callers that cannot allocate device

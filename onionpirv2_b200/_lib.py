@@ -112,6 +112,13 @@ _SIGS = {
     "opir_server_combine_shards": ([C.c_void_p, C.c_uint32, u64p, u64p, u64p], C.c_int),
     "opir_server_combine_shards_device": ([C.c_void_p, C.c_uint32, u64p, C.c_void_p,
                                            C.c_void_p, C.c_void_p], C.c_int),
+    "opir_prf_expand": ([C.POINTER(Params), u8p, C.c_uint32, C.c_uint64, u64p], C.c_int),
+    "opir_query_wire_bytes": ([C.POINTER(Params)], C.c_size_t),
+    "opir_keys_wire_bytes": ([C.POINTER(Params)], C.c_size_t),
+    "opir_query_encode": ([C.POINTER(Params), u8p, u64p, u8p, C.c_size_t], C.c_int),
+    "opir_query_decode": ([C.POINTER(Params), u8p, C.c_size_t, u64p], C.c_int),
+    "opir_keys_encode": ([C.POINTER(Params), u8p, u64p, u64p, u8p, C.c_size_t], C.c_int),
+    "opir_keys_decode": ([C.POINTER(Params), u8p, C.c_size_t, u64p, u32p, u64p], C.c_int),
     "opir_plan_memory": ([C.POINTER(Params), C.POINTER(MemoryPlan)], C.c_int),
     "opir_server_reserve": ([C.c_void_p, C.c_uint32], C.c_int),
     "opir_server_set_priority": ([C.c_void_p, C.c_int], C.c_int),

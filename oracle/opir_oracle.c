@@ -309,11 +309,15 @@ struct oracle_client {
 };
 
 /* rlwe.cpp:230-276 (K = 1), coefficient-form output */
-static void encrypt_zero(const opir_oracle_params *p, const uint64_t *sk, mt64 *g, uint64_t *ct) {
+/* given_a: the uniform polynomial (c1) supplied by the caller (a seed-
+ * compressed query) instead of drawn from the generator; NULL draws it. */
+static void encrypt_zero_a(const opir_oracle_params *p, const uint64_t *sk, mt64 *g,
+                           const uint64_t *given_a, uint64_t *ct) {
   const uint32_t N = p->N; const uint64_t q = p->q;
   uint64_t *c0 = ct, *c1 = ct + N;
   barrett_t b = barrett_make(q);
-  sample_uniform(c1, N, q, g);
+  if (given_a) memcpy(c1, given_a, N * sizeof *c1);
+  else sample_uniform(c1, N, q, g);
   uint64_t *e = malloc(N * sizeof *e), *a = malloc(N * sizeof *a);
   sample_gaussian(e, N, q, SIGMA, g);
   memcpy(a, c1, N * sizeof *a);
@@ -322,6 +326,9 @@ static void encrypt_zero(const opir_oracle_params *p, const uint64_t *sk, mt64 *
   intt_q(p, c0);
   for (uint32_t i = 0; i < N; ++i) c0[i] = submod(0, addmod(c0[i], e[i], q), q);
   free(e); free(a);
+}
+static void encrypt_zero(const opir_oracle_params *p, const uint64_t *sk, mt64 *g, uint64_t *ct) {
+  encrypt_zero_a(p, sk, g, NULL, ct);
 }
 
 /* bv_keyswitch.cpp:191-259 */
@@ -424,17 +431,18 @@ static uint32_t query_indices(const opir_oracle_params *p, uint64_t idx, uint64_
   return n;
 }
 /* client.cpp:107-225 (K = 1) */
-int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out) {
+static int client_query(oracle_client *c, uint64_t pt_idx, const uint64_t *given_a,
+                        uint64_t *out) {
   const opir_oracle_params *p = &c->p;
   if (pt_idx >= p->num_pt) return -1;
-  const uint32_t N = p->N; const uint64_t q = p->q;
+  const uint64_t q = p->q;
   uint64_t qi[70];
   uint32_t nq = query_indices(p, pt_idx, qi);
   const uint32_t h = p->expansion_height;
   const uint64_t capacity = 1ULL << h;
   uint64_t inverse = 0;
   invmod(capacity % p->t, p->t, &inverse);
-  encrypt_zero(p, c->sk, &c->rng, out);
+  encrypt_zero_a(p, c->sk, &c->rng, given_a, out);
   uint64_t rev = bitrev(qi[0], h);
   uint64_t scaled = (uint64_t)((((u128)q * inverse) + (p->t >> 1)) / p->t) % q;
   out[rev] = (out[rev] + scaled) % q;
@@ -453,6 +461,13 @@ int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out) {
     }
   }
   return 0;
+}
+int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out) {
+  return client_query(c, pt_idx, NULL, out);
+}
+int oracle_client_query_with_a(oracle_client *c, uint64_t pt_idx, const uint64_t *a,
+                               uint64_t *out) {
+  return client_query(c, pt_idx, a, out);
 }
 /* tree_query.cpp:142-196 (K = 1), make_tree_query: an encryption of zero
  * from the client's generator, the alpha one-hot as the BFV lift of

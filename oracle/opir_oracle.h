@@ -73,6 +73,11 @@ void oracle_client_free(oracle_client *c);
 void oracle_client_bv_keys(const oracle_client *c, uint64_t *out);
 void oracle_client_gsw_key(const oracle_client *c, uint64_t *out);
 int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out);
+/* The same query with its uniform polynomial c1 = a given by the caller
+ * (a seed-compressed query: a = Expand(seed)); the error still comes from
+ * the client's generator. */
+int oracle_client_query_with_a(oracle_client *c, uint64_t pt_idx, const uint64_t *a,
+                               uint64_t *out);
 /* tree_query.cpp:142-196 (K = 1): packed tree query; bits = b beta bits
  * then r gamma bits (little-endian coordinates), groups = b + r. */
 int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,

@@ -86,6 +86,7 @@ def lib():
         L.oracle_client_bv_keys.argtypes = [C.c_void_p, _u64p]
         L.oracle_client_gsw_key.argtypes = [C.c_void_p, _u64p]
         L.oracle_client_query.argtypes = [C.c_void_p, C.c_uint64, _u64p]
+        L.oracle_client_query_with_a.argtypes = [C.c_void_p, C.c_uint64, _u64p, _u64p]
         L.oracle_client_decrypt.argtypes = [C.c_void_p, _u64p, _u64p]
         L.oracle_client_tree_query.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,
                                                C.POINTER(C.c_uint8), C.c_uint32, _u64p]
@@ -205,6 +206,14 @@ class Client:
     def query(self, idx: int) -> np.ndarray:
         out = np.zeros((2, self.p.N), dtype=np.uint64)
         if lib().oracle_client_query(self.h, idx, ptr(out)) != 0:
+            raise IndexError("plaintext index outside the layout")
+        return out
+
+    def query_with_a(self, idx: int, a: np.ndarray) -> np.ndarray:
+        """The query for idx with c1 = a (a seed-compressed query)."""
+        out = np.zeros((2, self.p.N), dtype=np.uint64)
+        aa = np.ascontiguousarray(a, dtype=np.uint64)
+        if lib().oracle_client_query_with_a(self.h, idx, ptr(aa), ptr(out)) != 0:
             raise IndexError("plaintext index outside the layout")
         return out
 
