@@ -77,6 +77,11 @@ def parse():
                          "(L=17, a=3)")
     ap.add_argument("--rows-sharded", action="store_true",
                     help="one database split by candidate rows over the ranks (strong scaling)")
+    ap.add_argument("--client", action="store_true",
+                    help="client-side batch operations: response decryption and query packing")
+    ap.add_argument("--client-config", choices=["k1", "c4"], default="k1")
+    ap.add_argument("--client-batch", type=int, default=1024,
+                    help="responses (and queries) per step (--client)")
     ap.add_argument("--serve", action="store_true",
                     help="serving loop: Poisson arrivals over three resident databases")
     ap.add_argument("--rates", default="50,500,2000", help="offered queries/s (--serve)")
@@ -860,6 +865,139 @@ def bench_tree(args, world, rank, local):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- client side
+def bench_client(args, world, rank, local):
+    """Client-side batch operations of one client (one ternary secret):
+    decrypt_mod_q over --client-batch responses per step (the headline value)
+    and fast_generate_query over as many queries (reported beside it), on
+    seeded synthetic responses, uniform c1 and rounded-Gaussian errors; the
+    work is data-independent. Replicas at N > 1."""
+    import torch
+    from onionpirv2_b200 import PirParams
+    from onionpirv2_b200.client import PirClient
+    from onionpirv2_b200.server import launch_count
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
+    c4 = args.client_config == "c4"
+    gp = PirParams(config="CONFIG_N4096_K2_MP") if c4 else PirParams()
+    N, n = gp.N, args.client_batch
+    rng = np.random.default_rng(1234 + rank)
+    secret = rng.integers(-1, 2, N).astype(np.int8)
+    nz = int(np.count_nonzero(secret))
+    gc = PirClient(gp, secret, device=local)
+    sq = int(gp.small_q)
+    resp = rng.integers(0, sq, (n, 2, N), dtype=np.uint64)
+    mods = gp.get_rns_mods()
+    a = np.stack([np.stack([rng.integers(0, int(q), N, dtype=np.uint64) for q in mods])
+                  for _ in range(n)])
+    e = np.rint(rng.normal(0.0, 3.2, (n, N))).astype(np.int64)
+    idx = rng.integers(0, gp.num_pt, n)
+    d_resp = torch.from_numpy(resp.view(np.int64)).to(device)
+    d_pt = torch.empty((n, N), dtype=torch.int64, device=device)
+    d_a = torch.from_numpy(a.view(np.int64)).to(device)
+    d_e = torch.from_numpy(e).to(device)
+    d_q = torch.empty((n, 2) + a.shape[1:], dtype=torch.int64, device=device)
+    h_resp = torch.from_numpy(resp.view(np.int64)).pin_memory()
+    h_pt = torch.empty((n, N), dtype=torch.int64).pin_memory()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device)
+    sp = stream.cuda_stream
+
+    def dec():
+        gc.decrypt_device(n, d_resp.data_ptr(), d_pt.data_ptr(), 0, sp)
+
+    def pack():
+        gc.generate_queries_device(idx, d_a.data_ptr(), d_e.data_ptr(), d_q.data_ptr(), sp)
+
+    def timed(fn, steps):
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            fn()
+            s1.record(stream)
+            s1.synchronize()
+            total += s0.elapsed_time(s1) / 1e3
+        return total
+
+    for _ in range(args.warmup):
+        dec()
+        pack()
+    torch.cuda.synchronize(device)
+    barrier(world, device)
+    l0 = launch_count()
+    with ClockSampler(local) as clk:
+        t_dec = max_over_ranks(timed(dec, args.steps), world, device)
+        t_pack = max_over_ranks(timed(pack, args.steps), world, device)
+
+        def e2e_step():
+            d_resp.copy_(h_resp, non_blocking=True)
+            dec()
+            h_pt.copy_(d_pt, non_blocking=True)
+
+        t_e2e = max_over_ranks(timed(e2e_step, args.steps), world, device)
+    launches = launch_count() - l0
+    torch.cuda.synchronize(device)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    clocks = clk.summary()
+    parts = 1 if sq < (1 << 31) else 2
+    smem_bytes = n * N * nz * parts * 4          # shared words read by the ternary product
+    ms_dec = t_dec * 1e3 / args.steps
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clocks.get("sm_mhz") or 1965.0
+    peak = sms * 128 * mhz * 1e6 / 1e9         # GB/s: 128 B/clk/SM shared-memory bandwidth
+    achieved = smem_bytes / (ms_dec / 1e3) / 1e9
+    line = {
+        "metric": "client responses decrypted/s (decrypt_mod_q, bit-exact)",
+        "value": world * n * args.steps / t_dec, "unit": "responses/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dec,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded ternary secret, uniform responses mod small_q, uniform c1, "
+                "rounded Gaussian errors)",
+        "config": {"workload": f"client batch of {n} on {gp.config}: N={N}, small_q={sq}, "
+                               f"{nz} nonzero secret coefficients",
+                   "batch": n, "l2": "flushed (256 MiB write) between timed steps",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "pack": {"value": world * n * args.steps / t_pack, "unit": "queries/s",
+                 "ms_per_step": t_pack * 1e3 / args.steps},
+        "e2e": {"value": world * n * args.steps / t_e2e, "unit": "responses/s",
+                "h2d_bytes_per_step": int(resp.nbytes), "d2h_bytes_per_step": int(n * N * 8)},
+        "roofline": {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_kind": f"nominal: {sms} SMs x 128 B/clk x sampled {mhz:.0f} MHz"},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as O
+        op = O.c4_params(gp.target_num_pt, gp.expansion_height) if c4 else \
+            O.params(gp.target_num_pt, gp.expansion_height)
+        cl = (O.C4Client if c4 else O.Client)(op, 99)
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 10.0 and done < n:
+            cl.decrypt(resp[done])
+            done += 1
+        el = time.perf_counter() - t0
+        line["cpu_baseline"] = {
+            "value": done / el, "unit": "responses/s", "cores": 1, "kind": "port",
+            "sample": f"oracle decrypt_mod_q (NTT mod small_q, one core) of {done} of the "
+                      f"step's responses; CPU {cpu_model()}"}
+    print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 # ---------------------------------------------------------------- row shards
 def bench_rows(args, world, rank, local):
     """One database split by candidate rows over the job's ranks: per step,
@@ -1034,6 +1172,9 @@ def main():
     world, rank, local = dist_env()
     if args.rows_sharded and args.impl == "ours":
         bench_rows(args, world, rank, local)
+        return
+    if args.client and args.impl == "ours":
+        bench_client(args, world, rank, local)
         return
     if args.workload == "tree" and args.impl == "ours" and not args.serve:
         bench_tree(args, world, rank, local)

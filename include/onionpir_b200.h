@@ -475,6 +475,49 @@ opir_status opir_ext_prod_mux_noalloc(const opir_params *params, uint32_t n,
                                       const uint64_t *d_selectors, uint64_t *d_out,
                                       void *stream);
 
+/* ---- client-side batch operations ---------------------------------------
+ * The two client steps of the protocol that scale with the number of queries
+ * or responses, for one client (one ternary secret) at a time: query packing
+ * (PirClient::fast_generate_query, src/client.cpp:107-225) and response
+ * decryption (PirClient::decrypt_mod_q, src/client.cpp:364-410). Key
+ * generation stays with the caller. A client handle holds the secret on one
+ * device; calls on one handle must not run concurrently. */
+typedef struct opir_client opir_client;
+
+/* secret: N int8 coefficients in {-1, 0, 1} (the coefficient form of the
+ * client's RlweSk, includes/rlwe.h:33-44). params: a database layout
+ * (opir_params_init[_config]); the queries address that layout. */
+opir_status opir_client_create(const opir_params *params, const int8_t *secret, int device,
+                               opir_client **out);
+void opir_client_destroy(opir_client *client);
+const char *opir_client_last_error(const opir_client *client);
+
+/* fast_generate_query for n plaintext indices (host array pt_idx, each below
+ * num_pt, else OPIR_ERR_OUT_OF_RANGE) with the randomness given:
+ *   d_a       : n x K N u64 device array, the uniform c1 of each query, limb
+ *               k below q_k (the logical q when K = 1)
+ *   d_e       : n x N int64 device array, the error of each query (shared by
+ *               the limbs when K = 2)
+ *   d_queries : n x 2 K N u64 device array, each [c0 (K N)][c1 (K N)] with
+ *               c1 = a and c0 = -(a s + e) plus the packed plaintext (the
+ *               one-hot's BFV lift and the selector gadget rows)
+ * stream: cudaStream_t (NULL = legacy default stream). Equal, for equal
+ * (secret, a, e), to the reference's query coefficient for coefficient. */
+opir_status opir_client_generate_queries_device(opir_client *client, uint32_t n,
+                                                const uint64_t *pt_idx, const uint64_t *d_a,
+                                                const int64_t *d_e, uint64_t *d_queries,
+                                                void *stream);
+
+/* decrypt_mod_q for n responses:
+ *   d_responses  : n x 2N u64 device array, coefficient form mod small_q as
+ *                  PirClient::load_resp_from_stream yields (client.cpp:315-361)
+ *   d_plaintexts : n x N u64 device array, each coefficient below t
+ *   d_max_noise  : n u64 device array or NULL: the response's max noise
+ *                  |phase - round(small_q m / t)| (client.cpp:389-407) */
+opir_status opir_client_decrypt_device(opir_client *client, uint32_t n,
+                                       const uint64_t *d_responses, uint64_t *d_plaintexts,
+                                       uint64_t *d_max_noise, void *stream);
+
 /* ---- tree PIR level selection ------------------------------------------
  * The full-binary-tree PIR layer of the reference (src/tree_index.cpp,
  * src/tree_query.cpp, src/tree_select.cpp): levels 0..L of a tree with

@@ -134,6 +134,14 @@ _SIGS = {
     "opir_server_evaluate_other_dim": ([C.c_void_p, u64p, u64p, u64p], C.c_int),
     "opir_server_ext_prod_mux": ([C.c_void_p, u64p, u64p, u64p, u64p], C.c_int),
     "opir_save_response": ([C.POINTER(Params), u64p, u8p, C.c_size_t], C.c_size_t),
+    "opir_client_create": ([C.POINTER(Params), C.POINTER(C.c_int8), C.c_int,
+                            C.POINTER(C.c_void_p)], C.c_int),
+    "opir_client_destroy": ([C.c_void_p], None),
+    "opir_client_last_error": ([C.c_void_p], C.c_char_p),
+    "opir_client_generate_queries_device": ([C.c_void_p, C.c_uint32, u64p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "opir_client_decrypt_device": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p], C.c_int),
     "opir_ext_prod_mux_noalloc": ([C.POINTER(Params), C.c_uint32, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
 }

@@ -17,7 +17,7 @@ BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libonionpir_b200.so")
 SOURCES = ["opir_kernels.cu", "opir_server.cu", "opir_params.cpp", "opir_noalloc.cu",
            "opir_scan_tc.cu", "opir_c4_kernels.cu", "opir_c4_server.cu", "opir_c4_scan_tc.cu", "opir_tree.cpp",
-           "opir_shard.cpp", "opir_codec.cpp", "opir_codec_abi.cpp"]
+           "opir_shard.cpp", "opir_codec.cpp", "opir_codec_abi.cpp", "opir_client.cu"]
 HEADERS = ["opir_device.cuh", "opir_kernels.h", "opir_params.h", "opir_scan_tc.h", "opir_ntt.cuh",
            "opir_host.h", "opir_c4_device.cuh", "opir_c4_kernels.h", "opir_c4_server.h", "opir_tc.cuh", "opir_tree.h",
            "opir_shard.h", "opir_codec.h"]

@@ -1,0 +1,113 @@
+"""GPU batch operations of the reference's PirClient (src/client.cpp) for
+one client's secret: query packing (fast_generate_query, :107-225) and
+response decryption (decrypt_mod_q, :364-410), over the C ABI's
+opir_client_* calls (include/onionpir_b200.h).
+
+The randomness of a query (the uniform c1 `a` and the error `e`) is an input:
+the reference draws it from its own generators, the codec expands `a` from a
+seed (codec.prf_expand), and a caller may sample `e` however it likes. Key
+generation stays on the host.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib as L
+from .server import OPIR_OK, PirParams, _ptr, _raise
+
+
+class PirClient:
+    """One client's ternary secret, resident on one GPU."""
+
+    def __init__(self, params: PirParams, secret: np.ndarray, device: int = 0):
+        s = np.ascontiguousarray(secret, dtype=np.int8)
+        if s.shape != (params.N,):
+            raise ValueError(f"secret must be ({params.N},) int8 in {{-1, 0, 1}}")
+        self.params = params
+        self.device = device
+        self._lib = L.load()
+        h = C.c_void_p()
+        rc = self._lib.opir_client_create(C.byref(params._p), _ptr(s, C.c_int8), device,
+                                          C.byref(h))
+        if rc != OPIR_OK:
+            _raise(rc, "client creation failed")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.opir_client_destroy(h)
+            self._h = None
+
+    def _check(self, rc: int):
+        if rc != OPIR_OK:
+            _raise(rc, self._lib.opir_client_last_error(self._h).decode())
+
+    @property
+    def query_shape(self) -> tuple:
+        return self.params.ct_shape
+
+    # ---- device-pointer form ------------------------------------------------
+    def generate_queries_device(self, pt_idx: Sequence[int], d_a: int, d_e: int, d_queries: int,
+                                stream: int = 0):
+        """Enqueue on device pointers (ints), e.g. torch tensors' data_ptr()."""
+        idx = np.ascontiguousarray(np.asarray(pt_idx, dtype=np.uint64))
+        self._check(self._lib.opir_client_generate_queries_device(
+            self._h, idx.size, _ptr(idx), C.c_void_p(d_a), C.c_void_p(d_e),
+            C.c_void_p(d_queries), C.c_void_p(stream) if stream else None))
+
+    def decrypt_device(self, n: int, d_responses: int, d_plaintexts: int, d_max_noise: int = 0,
+                       stream: int = 0):
+        self._check(self._lib.opir_client_decrypt_device(
+            self._h, int(n), C.c_void_p(d_responses), C.c_void_p(d_plaintexts),
+            C.c_void_p(d_max_noise) if d_max_noise else None,
+            C.c_void_p(stream) if stream else None))
+
+    # ---- host form (torch moves the buffers) -------------------------------
+    def fast_generate_query_batch(self, pt_idx: Sequence[int], a: np.ndarray,
+                                  e: np.ndarray) -> np.ndarray:
+        """Queries for pt_idx with c1 = a[i] and error e[i]: (n,) + ct_shape."""
+        import torch
+        idx = np.asarray(pt_idx, dtype=np.uint64).reshape(-1)
+        n = idx.size
+        cs = self.params.ct_shape
+        a = np.ascontiguousarray(a, dtype=np.uint64).reshape((n,) + cs[1:])
+        e = np.ascontiguousarray(e, dtype=np.int64).reshape(n, self.params.N)
+        dev = torch.device("cuda", self.device)
+        da = torch.from_numpy(a.view(np.int64)).to(dev)
+        de = torch.from_numpy(e).to(dev)
+        dq = torch.empty((n,) + cs, dtype=torch.int64, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        self.generate_queries_device(idx, da.data_ptr(), de.data_ptr(), dq.data_ptr(),
+                                     stream.cuda_stream)
+        return dq.cpu().numpy().view(np.uint64)
+
+    def fast_generate_query(self, pt_idx: int, a: np.ndarray, e: np.ndarray) -> np.ndarray:
+        return self.fast_generate_query_batch([pt_idx], a[None], e[None])[0]
+
+    def decrypt_mod_q_batch(self, responses: np.ndarray,
+                            with_noise: bool = False):
+        """Plaintexts (n, N) of responses (n, 2, N); with_noise adds each
+        response's max noise."""
+        import torch
+        r = np.ascontiguousarray(responses, dtype=np.uint64)
+        n = r.shape[0]
+        N = self.params.N
+        r = r.reshape(n, 2, N)
+        dev = torch.device("cuda", self.device)
+        dr = torch.from_numpy(r.view(np.int64)).to(dev)
+        dp = torch.empty((n, N), dtype=torch.int64, device=dev)
+        dn = torch.empty(n, dtype=torch.int64, device=dev) if with_noise else None
+        stream = torch.cuda.current_stream(dev)
+        self.decrypt_device(n, dr.data_ptr(), dp.data_ptr(), dn.data_ptr() if with_noise else 0,
+                            stream.cuda_stream)
+        pt = dp.cpu().numpy().view(np.uint64)
+        if with_noise:
+            return pt, dn.cpu().numpy().view(np.uint64)
+        return pt
+
+    def decrypt_mod_q(self, response: np.ndarray) -> np.ndarray:
+        return self.decrypt_mod_q_batch(np.asarray(response)[None])[0]

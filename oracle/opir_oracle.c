@@ -312,7 +312,7 @@ struct oracle_client {
 /* given_a: the uniform polynomial (c1) supplied by the caller (a seed-
  * compressed query) instead of drawn from the generator; NULL draws it. */
 static void encrypt_zero_a(const opir_oracle_params *p, const uint64_t *sk, mt64 *g,
-                           const uint64_t *given_a, uint64_t *ct) {
+                           const uint64_t *given_a, uint64_t *ct, int64_t *e_out) {
   const uint32_t N = p->N; const uint64_t q = p->q;
   uint64_t *c0 = ct, *c1 = ct + N;
   barrett_t b = barrett_make(q);
@@ -320,6 +320,8 @@ static void encrypt_zero_a(const opir_oracle_params *p, const uint64_t *sk, mt64
   else sample_uniform(c1, N, q, g);
   uint64_t *e = malloc(N * sizeof *e), *a = malloc(N * sizeof *a);
   sample_gaussian(e, N, q, SIGMA, g);
+  if (e_out)
+    for (uint32_t i = 0; i < N; ++i) e_out[i] = e[i] > q / 2 ? -(int64_t)(q - e[i]) : (int64_t)e[i];
   memcpy(a, c1, N * sizeof *a);
   ntt_q(p, a);
   for (uint32_t i = 0; i < N; ++i) c0[i] = mulmod(&b, a[i], sk[i]);
@@ -328,7 +330,7 @@ static void encrypt_zero_a(const opir_oracle_params *p, const uint64_t *sk, mt64
   free(e); free(a);
 }
 static void encrypt_zero(const opir_oracle_params *p, const uint64_t *sk, mt64 *g, uint64_t *ct) {
-  encrypt_zero_a(p, sk, g, NULL, ct);
+  encrypt_zero_a(p, sk, g, NULL, ct, NULL);
 }
 
 /* bv_keyswitch.cpp:191-259 */
@@ -432,7 +434,7 @@ static uint32_t query_indices(const opir_oracle_params *p, uint64_t idx, uint64_
 }
 /* client.cpp:107-225 (K = 1) */
 static int client_query(oracle_client *c, uint64_t pt_idx, const uint64_t *given_a,
-                        uint64_t *out) {
+                        uint64_t *out, int64_t *e_out) {
   const opir_oracle_params *p = &c->p;
   if (pt_idx >= p->num_pt) return -1;
   const uint64_t q = p->q;
@@ -442,7 +444,7 @@ static int client_query(oracle_client *c, uint64_t pt_idx, const uint64_t *given
   const uint64_t capacity = 1ULL << h;
   uint64_t inverse = 0;
   invmod(capacity % p->t, p->t, &inverse);
-  encrypt_zero_a(p, c->sk, &c->rng, given_a, out);
+  encrypt_zero_a(p, c->sk, &c->rng, given_a, out, e_out);
   uint64_t rev = bitrev(qi[0], h);
   uint64_t scaled = (uint64_t)((((u128)q * inverse) + (p->t >> 1)) / p->t) % q;
   out[rev] = (out[rev] + scaled) % q;
@@ -463,11 +465,23 @@ static int client_query(oracle_client *c, uint64_t pt_idx, const uint64_t *given
   return 0;
 }
 int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out) {
-  return client_query(c, pt_idx, NULL, out);
+  return client_query(c, pt_idx, NULL, out, NULL);
 }
 int oracle_client_query_with_a(oracle_client *c, uint64_t pt_idx, const uint64_t *a,
                                uint64_t *out) {
-  return client_query(c, pt_idx, a, out);
+  return client_query(c, pt_idx, a, out, NULL);
+}
+int oracle_client_query_parts(oracle_client *c, uint64_t pt_idx, const uint64_t *a,
+                              uint64_t *out, int64_t *e_out) {
+  return client_query(c, pt_idx, a, out, e_out);
+}
+void oracle_client_secret(const oracle_client *c, int8_t *out) {
+  const opir_oracle_params *p = &c->p;
+  uint64_t *s = malloc(p->N * sizeof *s);
+  memcpy(s, c->sk, p->N * sizeof *s);
+  intt_q(p, s);
+  for (uint32_t i = 0; i < p->N; ++i) out[i] = s[i] == 0 ? 0 : s[i] == 1 ? 1 : -1;
+  free(s);
 }
 /* tree_query.cpp:142-196 (K = 1), make_tree_query: an encryption of zero
  * from the client's generator, the alpha one-hot as the BFV lift of
@@ -512,8 +526,16 @@ void oracle_client_decrypt_q(const oracle_client *c, const uint64_t *ct, uint64_
   for (uint32_t i = 0; i < N; ++i) pt_out[i] = oracle_rescale(addmod(c1[i], ct[i], q), q, p->t);
   free(c1);
 }
+/* The noise figure decrypt_mod_q reports (client.cpp:389-407): max over
+ * the coefficients of |phase - round(sq m / t)| mod sq, centred. */
+static uint64_t noise_of(uint64_t phase, uint64_t m, uint64_t sq, uint64_t t) {
+  const uint64_t approx = (uint64_t)((((u128)sq * m) + (t >> 1)) / t) % sq;
+  const uint64_t pos = phase >= approx ? phase - approx : sq - approx + phase;
+  return pos > sq / 2 ? sq - pos : pos;
+}
 /* client.cpp:364-430 */
-void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp, uint64_t *pt_out) {
+void oracle_client_decrypt_noise(const oracle_client *c, const uint64_t *resp, uint64_t *pt_out,
+                                 uint64_t *max_noise) {
   const opir_oracle_params *p = &c->p;
   const uint32_t N = p->N; const uint64_t sq = p->small_q, t = p->t;
   const uint64_t root = small_root(p);
@@ -527,11 +549,18 @@ void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp, uint64_
   oracle_ntt_fwd(c1, N, sq, root);
   for (uint32_t i = 0; i < N; ++i) ph[i] = mulmod(&b, c1[i], sks[i]);
   oracle_ntt_inv(ph, N, sq, root);
+  uint64_t worst = 0;
   for (uint32_t i = 0; i < N; ++i) {
     uint64_t v = addmod(ph[i], c0[i], sq);
     pt_out[i] = (uint64_t)((((u128)v * t) + (sq >> 1)) / sq) % t;
+    const uint64_t nz = noise_of(v, pt_out[i], sq, t);
+    if (nz > worst) worst = nz;
   }
+  if (max_noise) *max_noise = worst;
   free(skc); free(sks); free(c0); free(c1); free(ph);
+}
+void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp, uint64_t *pt_out) {
+  oracle_client_decrypt_noise(c, resp, pt_out, NULL);
 }
 
 /* ======================================================================

@@ -78,6 +78,11 @@ int oracle_client_query(oracle_client *c, uint64_t pt_idx, uint64_t *out);
  * the client's generator. */
 int oracle_client_query_with_a(oracle_client *c, uint64_t pt_idx, const uint64_t *a,
                                uint64_t *out);
+/* The same, also returning the error e (N signed values) it drew. */
+int oracle_client_query_parts(oracle_client *c, uint64_t pt_idx, const uint64_t *a,
+                              uint64_t *out, int64_t *e_out);
+/* The secret key in coefficient form, N values in {-1, 0, 1}. */
+void oracle_client_secret(const oracle_client *c, int8_t *out);
 /* tree_query.cpp:142-196 (K = 1): packed tree query; bits = b beta bits
  * then r gamma bits (little-endian coordinates), groups = b + r. */
 int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
@@ -86,6 +91,9 @@ int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64
 void oracle_client_decrypt_q(const oracle_client *c, const uint64_t *ct, uint64_t *pt_out);
 void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp,
                            uint64_t *pt_out);
+/* The same, also returning the response's max noise (client.cpp:389-407). */
+void oracle_client_decrypt_noise(const oracle_client *c, const uint64_t *resp, uint64_t *pt_out,
+                                 uint64_t *max_noise);
 
 /* ---- server (server.cpp, gsw.cpp, bv_keyswitch.cpp, matrix.cpp) ---- */
 typedef struct oracle_server oracle_server;
@@ -152,8 +160,15 @@ int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out);
  * oracle_client_tree_query; out: 4N u64 limb-major. */
 int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
                                 const uint8_t *bits, uint32_t groups, uint64_t *out);
+/* Query with a given uniform c1 (2N, limb-major), returning the shared
+ * error (N signed values); the secret in coefficient form (N in {-1,0,1}). */
+int oracle_c4_client_query_parts(oracle_c4_client *c, uint64_t pt_idx, const uint64_t *a,
+                                 uint64_t *out, int64_t *e_out);
+void oracle_c4_client_secret(const oracle_c4_client *c, int8_t *out);
 void oracle_c4_client_decrypt(const oracle_c4_client *c, const uint64_t *resp,
                               uint64_t *pt_out);
+void oracle_c4_client_decrypt_noise(const oracle_c4_client *c, const uint64_t *resp,
+                                    uint64_t *pt_out, uint64_t *max_noise);
 
 typedef struct oracle_c4_server oracle_c4_server;
 oracle_c4_server *oracle_c4_server_new(const opir_oracle_c4_params *p);

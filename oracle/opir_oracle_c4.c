@@ -79,13 +79,18 @@ struct oracle_c4_client {
 
 /* rlwe.cpp:230-276: per-limb uniform c1, one shared Gaussian e reduced per
  * limb (rlwe.cpp:196-215), c0_k = -(a_k s_k + e_k); coefficient form. */
-static void encrypt_zero_c4(const opir_oracle_c4_params *p, const uint64_t *sk, mt64 *g, uint64_t *ct) {
+/* given_a (2N, limb-major): the uniform c1 supplied by the caller instead of
+ * drawn from the generator (NULL draws it); e_out receives the shared error. */
+static void encrypt_zero_c4_a(const opir_oracle_c4_params *p, const uint64_t *sk, mt64 *g,
+                              const uint64_t *given_a, uint64_t *ct, int64_t *e_out) {
   const uint32_t N = p->N;
   uint64_t *c0 = ct, *c1 = ct + 2 * (size_t)N;
-  for (uint32_t k = 0; k < 2; ++k) sample_uniform(c1 + (size_t)k * N, N, p->q[k], g);
+  if (given_a) memcpy(c1, given_a, 2 * (size_t)N * sizeof *c1);
+  else for (uint32_t k = 0; k < 2; ++k) sample_uniform(c1 + (size_t)k * N, N, p->q[k], g);
   int64_t *e = malloc(N * sizeof *e);
   normal_t nd = {0.0, 0, SIGMA_C4};
   for (uint32_t i = 0; i < N; ++i) e[i] = llround(normal_next(&nd, g));
+  if (e_out) memcpy(e_out, e, N * sizeof *e);
   uint64_t *a = malloc(N * sizeof *a);
   for (uint32_t k = 0; k < 2; ++k) {
     const uint64_t q = p->q[k];
@@ -98,6 +103,9 @@ static void encrypt_zero_c4(const opir_oracle_c4_params *p, const uint64_t *sk, 
     for (uint32_t i = 0; i < N; ++i) c0k[i] = submod(0, addmod(c0k[i], sreduce(e[i], q), q), q);
   }
   free(e); free(a);
+}
+static void encrypt_zero_c4(const opir_oracle_c4_params *p, const uint64_t *sk, mt64 *g, uint64_t *ct) {
+  encrypt_zero_c4_a(p, sk, g, NULL, ct, NULL);
 }
 
 /* bv_keyswitch.cpp:191-259 (K = 2): sigma_k(s) per limb (utils.cpp:74-82),
@@ -235,7 +243,8 @@ static uint32_t query_indices_c4(const opir_oracle_c4_params *p, uint64_t idx, u
 }
 /* client.cpp:107-225 (K = 2): the message Delta (2^h)^-1 lifted under Q,
  * then reduced per limb; gadget rows written under every limb. */
-int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out) {
+static int c4_client_query(oracle_c4_client *c, uint64_t pt_idx, const uint64_t *given_a,
+                           uint64_t *out, int64_t *e_out) {
   const opir_oracle_c4_params *p = &c->p;
   if (pt_idx >= p->num_pt) return -1;
   const uint32_t N = p->N;
@@ -245,7 +254,7 @@ int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out) 
   const uint64_t capacity = 1ULL << h, t = p->t;
   uint64_t inverse = 0;
   invmod(capacity % t, t, &inverse);
-  encrypt_zero_c4(p, c->sk, &c->rng, out);
+  encrypt_zero_c4_a(p, c->sk, &c->rng, given_a, out, e_out);
   const uint64_t rev = bitrev(qi[0], h);
   const u128 Q = (u128)p->q[0] * p->q[1];
   const u128 Delta = Q / t;
@@ -277,6 +286,21 @@ int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out) 
     }
   }
   return 0;
+}
+int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out) {
+  return c4_client_query(c, pt_idx, NULL, out, NULL);
+}
+int oracle_c4_client_query_parts(oracle_c4_client *c, uint64_t pt_idx, const uint64_t *a,
+                                 uint64_t *out, int64_t *e_out) {
+  return c4_client_query(c, pt_idx, a, out, e_out);
+}
+void oracle_c4_client_secret(const oracle_c4_client *c, int8_t *out) {
+  const opir_oracle_c4_params *p = &c->p;
+  uint64_t *s = malloc(p->N * sizeof *s);
+  memcpy(s, c->sk, p->N * sizeof *s);
+  intt_k(p, 0, s);
+  for (uint32_t i = 0; i < p->N; ++i) out[i] = s[i] == 0 ? 0 : s[i] == 1 ? 1 : -1;
+  free(s);
 }
 /* make_tree_query (tree_query.cpp:142-196) for K = 2: a fresh encryption of
  * zero from the client's generator, the alpha one-hot as the BFV lift of
@@ -323,8 +347,10 @@ int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, 
   return 0;
 }
 
-/* client.cpp:364-430 under small_q: s from limb 0, ternary re-mapped */
-void oracle_c4_client_decrypt(const oracle_c4_client *c, const uint64_t *resp, uint64_t *pt_out) {
+/* client.cpp:364-430 under small_q: s from limb 0, ternary re-mapped;
+ * max_noise (may be NULL) as in the reference's noise report (:389-407). */
+void oracle_c4_client_decrypt_noise(const oracle_c4_client *c, const uint64_t *resp,
+                                    uint64_t *pt_out, uint64_t *max_noise) {
   const opir_oracle_c4_params *p = &c->p;
   const uint32_t N = p->N;
   const uint64_t sq = p->small_q, t = p->t;
@@ -339,11 +365,21 @@ void oracle_c4_client_decrypt(const oracle_c4_client *c, const uint64_t *resp, u
   oracle_ntt_fwd(c1, N, sq, root);
   for (uint32_t i = 0; i < N; ++i) ph[i] = mulmod(&b, c1[i], sks[i]);
   oracle_ntt_inv(ph, N, sq, root);
+  uint64_t worst = 0;
   for (uint32_t i = 0; i < N; ++i) {
     const uint64_t v = addmod(ph[i], c0[i], sq);
-    pt_out[i] = (uint64_t)((((u128)v * t) + (sq >> 1)) / sq) % t;
+    const uint64_t m = (uint64_t)((((u128)v * t) + (sq >> 1)) / sq) % t;
+    pt_out[i] = m;
+    const uint64_t approx = (uint64_t)((((u128)sq * m) + (t >> 1)) / t) % sq;
+    const uint64_t pos = v >= approx ? v - approx : sq - approx + v;
+    const uint64_t nz = pos > sq / 2 ? sq - pos : pos;
+    if (nz > worst) worst = nz;
   }
+  if (max_noise) *max_noise = worst;
   free(skc); free(sks); free(c0); free(c1); free(ph);
+}
+void oracle_c4_client_decrypt(const oracle_c4_client *c, const uint64_t *resp, uint64_t *pt_out) {
+  oracle_c4_client_decrypt_noise(c, resp, pt_out, NULL);
 }
 void oracle_c4_db_plaintext(uint64_t seed, uint64_t pt, const opir_oracle_c4_params *p, uint64_t *out) {
   for (uint32_t c = 0; c < p->N; ++c) out[c] = oracle_db_coeff(seed, pt, c, p->N, p->t);

@@ -88,6 +88,10 @@ def lib():
         L.oracle_client_query.argtypes = [C.c_void_p, C.c_uint64, _u64p]
         L.oracle_client_query_with_a.argtypes = [C.c_void_p, C.c_uint64, _u64p, _u64p]
         L.oracle_client_decrypt.argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_client_decrypt_noise.argtypes = [C.c_void_p, _u64p, _u64p, _u64p]
+        L.oracle_client_query_parts.argtypes = [C.c_void_p, C.c_uint64, _u64p, _u64p,
+                                                C.POINTER(C.c_int64)]
+        L.oracle_client_secret.argtypes = [C.c_void_p, C.POINTER(C.c_int8)]
         L.oracle_client_tree_query.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,
                                                C.POINTER(C.c_uint8), C.c_uint32, _u64p]
         L.oracle_client_decrypt_q.argtypes = [C.c_void_p, _u64p, _u64p]
@@ -139,6 +143,10 @@ def lib():
         L.oracle_c4_client_gsw_key.argtypes = [C.c_void_p, _u64p]
         L.oracle_c4_client_query.argtypes = [C.c_void_p, C.c_uint64, _u64p]
         L.oracle_c4_client_decrypt.argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_c4_client_decrypt_noise.argtypes = [C.c_void_p, _u64p, _u64p, _u64p]
+        L.oracle_c4_client_query_parts.argtypes = [C.c_void_p, C.c_uint64, _u64p, _u64p,
+                                                   C.POINTER(C.c_int64)]
+        L.oracle_c4_client_secret.argtypes = [C.c_void_p, C.POINTER(C.c_int8)]
         L.oracle_c4_client_tree_query.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32,
                                                   C.c_uint64, C.POINTER(C.c_uint8), C.c_uint32,
                                                   _u64p]
@@ -222,6 +230,29 @@ class Client:
         out = np.zeros(self.p.N, dtype=np.uint64)
         lib().oracle_client_decrypt(self.h, ptr(resp), ptr(out))
         return out
+
+    def decrypt_noise(self, resp: np.ndarray) -> tuple[np.ndarray, int]:
+        """decrypt_mod_q (client.cpp:364-410) and the max noise it reports."""
+        resp = np.ascontiguousarray(resp, dtype=np.uint64)
+        out = np.zeros(self.p.N, dtype=np.uint64)
+        noise = np.zeros(1, dtype=np.uint64)
+        lib().oracle_client_decrypt_noise(self.h, ptr(resp), ptr(out), ptr(noise))
+        return out, int(noise[0])
+
+    def secret(self) -> np.ndarray:
+        """The ternary secret in coefficient form (N int8 in {-1, 0, 1})."""
+        out = np.zeros(self.p.N, dtype=np.int8)
+        lib().oracle_client_secret(self.h, ptr(out, C.c_int8))
+        return out
+
+    def query_parts(self, idx: int, a: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """The query for idx with c1 = a, and the error e (N int64) it drew."""
+        out = np.zeros((2, self.p.N), dtype=np.uint64)
+        e = np.zeros(self.p.N, dtype=np.int64)
+        aa = np.ascontiguousarray(a, dtype=np.uint64)
+        if lib().oracle_client_query_parts(self.h, idx, ptr(aa), ptr(out), ptr(e, C.c_int64)) != 0:
+            raise IndexError("plaintext index outside the layout")
+        return out, e
 
     def tree_query(self, N0: int, h_q: int, alpha: int, beta_bits, gamma_bits) -> np.ndarray:
         """make_tree_query (tree_query.cpp:142-196) for client coordinates."""
@@ -363,6 +394,28 @@ class C4Client:
         out = np.zeros(self.p.N, dtype=np.uint64)
         lib().oracle_c4_client_decrypt(self.h, ptr(resp), ptr(out))
         return out
+
+    def decrypt_noise(self, resp: np.ndarray) -> tuple[np.ndarray, int]:
+        resp = np.ascontiguousarray(resp, dtype=np.uint64)
+        out = np.zeros(self.p.N, dtype=np.uint64)
+        noise = np.zeros(1, dtype=np.uint64)
+        lib().oracle_c4_client_decrypt_noise(self.h, ptr(resp), ptr(out), ptr(noise))
+        return out, int(noise[0])
+
+    def secret(self) -> np.ndarray:
+        out = np.zeros(self.p.N, dtype=np.int8)
+        lib().oracle_c4_client_secret(self.h, ptr(out, C.c_int8))
+        return out
+
+    def query_parts(self, idx: int, a: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """The query for idx with c1 = a (2, N limb-major), and the shared error e."""
+        out = np.zeros((2, 2, self.p.N), dtype=np.uint64)
+        e = np.zeros(self.p.N, dtype=np.int64)
+        aa = np.ascontiguousarray(a, dtype=np.uint64)
+        if lib().oracle_c4_client_query_parts(self.h, idx, ptr(aa), ptr(out),
+                                              ptr(e, C.c_int64)) != 0:
+            raise IndexError("plaintext index outside the layout")
+        return out, e
 
     def tree_query(self, N0: int, h_q: int, alpha: int, beta_bits, gamma_bits) -> np.ndarray:
         """make_tree_query (tree_query.cpp:142-196), K = 2."""

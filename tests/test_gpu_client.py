@@ -1,0 +1,140 @@
+"""GPU client batch operations (opir_client_*, the reference's
+PirClient::fast_generate_query, client.cpp:107-225, and decrypt_mod_q,
+client.cpp:364-410) against the oracle client, bit for bit: queries packed on
+the GPU from the oracle's own uniform c1 and error equal the oracle's queries;
+responses decrypted on the GPU equal the oracle's plaintexts and max noise;
+and a GPU-packed query answered by the GPU server decrypts on the GPU to the
+database plaintext. Batch sizes cover every outputs-per-thread width the
+launcher picks (1, 2, 4, 8)."""
+import numpy as np
+import pytest
+
+from onionpirv2_b200 import OutOfRange, PirParams, PirServer
+from onionpirv2_b200.client import PirClient
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+C4 = "CONFIG_N4096_K2_MP"
+
+
+def _indices(num_pt, rng, n):
+    fixed = [0, num_pt - 1, num_pt // 2]
+    return (fixed + [int(x) for x in rng.integers(0, num_pt, max(n - 3, 0))])[:n]
+
+
+def _uniform(rng, mods, n, N):
+    return np.stack([np.stack([rng.integers(0, int(q), N, dtype=np.uint64) for q in mods])
+                     for _ in range(n)])
+
+
+@pytest.mark.parametrize("n", [1, 80, 150, 300])
+def test_k1_queries_match_oracle(n):
+    target, h = 43690, 10
+    gp, op = PirParams(target, h), O.params(target, h)
+    rng = np.random.default_rng(1000 + n)
+    idx = _indices(op.num_pt, rng, n)
+    a = _uniform(rng, [op.q], n, op.N)[:, 0]
+    cl = O.Client(op, 91)
+    parts = [cl.query_parts(x, a[i]) for i, x in enumerate(idx)]
+    gc = PirClient(gp, cl.secret())
+    got = gc.fast_generate_query_batch(idx, a, np.stack([e for _, e in parts]))
+    assert got.shape == (n, 2, op.N)
+    assert np.array_equal(got, np.stack([q for q, _ in parts]))
+
+
+@pytest.mark.parametrize("n", [1, 40, 75, 200])
+def test_c4_queries_match_oracle(n):
+    target, h = 16384, 9
+    gp, op = PirParams(target, h, config=C4), O.c4_params(target, h)
+    rng = np.random.default_rng(2000 + n)
+    idx = _indices(op.num_pt, rng, n)
+    a = _uniform(rng, op.q[:2], n, op.N)
+    cl = O.C4Client(op, 93)
+    parts = [cl.query_parts(x, a[i]) for i, x in enumerate(idx)]
+    gc = PirClient(gp, cl.secret())
+    got = gc.fast_generate_query_batch(idx, a, np.stack([e for _, e in parts]))
+    assert got.shape == (n, 2, 2, op.N)
+    assert np.array_equal(got, np.stack([q for q, _ in parts]))
+
+
+def test_k1_error_of_any_size_enters_linearly():
+    """c0 is -(a s + e) mod q for any int64 error, not only Gaussian ones:
+    the difference of two packings is -(e' - e) mod q everywhere."""
+    target, h = 16384, 9
+    gp, op = PirParams(target, h), O.params(target, h)
+    rng = np.random.default_rng(7)
+    a = _uniform(rng, [op.q], 2, op.N)[:, 0]
+    cl = O.Client(op, 5)
+    gc = PirClient(gp, cl.secret())
+    e = np.stack([cl.query_parts(3, a[i])[1] for i in range(2)])
+    big = rng.integers(-(1 << 62), 1 << 62, size=(2, op.N), dtype=np.int64)
+    big[0, :4] = [np.iinfo(np.int64).min, np.iinfo(np.int64).max, -1, 0]
+    q1 = gc.fast_generate_query_batch([3, 3], a, e)
+    q2 = gc.fast_generate_query_batch([3, 3], a, big)
+    q = int(op.q)
+    for i in range(2):
+        for j in range(op.N):
+            assert (int(q2[i, 0, j]) - int(q1[i, 0, j])) % q == (-(int(big[i, j]) - int(e[i, j]))) % q
+    assert np.array_equal(q1[:, 1], q2[:, 1])
+
+
+@pytest.mark.parametrize("config,n", [("k1", 1), ("k1", 80), ("k1", 150), ("k1", 300),
+                                      ("c4", 1), ("c4", 40), ("c4", 75), ("c4", 200)])
+def test_decrypt_matches_oracle(config, n):
+    if config == "k1":
+        gp, op = PirParams(16384, 9), O.params(16384, 9)
+        cl = O.Client(op, 17)
+    else:
+        gp, op = PirParams(16384, 9, config=C4), O.c4_params(16384, 9)
+        cl = O.C4Client(op, 19)
+    rng = np.random.default_rng(n)
+    resp = rng.integers(0, int(op.small_q), size=(n, 2, op.N), dtype=np.uint64)
+    resp[0, :, :3] = int(op.small_q) - 1
+    gc = PirClient(gp, cl.secret())
+    pt, noise = gc.decrypt_mod_q_batch(resp, with_noise=True)
+    for i in range(n):
+        want, want_noise = cl.decrypt_noise(resp[i])
+        assert np.array_equal(pt[i], want)
+        assert int(noise[i]) == want_noise
+
+
+@pytest.mark.parametrize("config", ["k1", "c4"])
+def test_gpu_query_answer_decrypt_round_trip(config):
+    target, h, db_seed = 16384, 9, 23
+    if config == "k1":
+        gp, op = PirParams(target, h), O.params(target, h)
+        cl = O.Client(op, 29)
+        mods = [op.q]
+        plain = lambda i: O.db_plaintext(db_seed, i, op).astype(np.uint64)  # noqa: E731
+    else:
+        gp, op = PirParams(target, h, config=C4), O.c4_params(target, h)
+        cl = O.C4Client(op, 31)
+        mods = op.q[:2]
+        plain = lambda i: O.c4_db_plaintext(db_seed, i, op)  # noqa: E731
+    rng = np.random.default_rng(5)
+    idx = [0, 77, target - 1, 9000]
+    a = _uniform(rng, mods, len(idx), op.N).reshape((len(idx),) + gp.ct_shape[1:])
+    e = np.stack([cl.query_parts(i, a[k])[1] for k, i in enumerate(idx)])
+    gc = PirClient(gp, cl.secret())
+    queries = gc.fast_generate_query_batch(idx, a, e)
+    srv = PirServer(gp)
+    srv.load_data_seeded(target, db_seed)
+    srv.set_client_keys(3, cl.bv_keys(), cl.gsw_key())
+    resp = srv.make_query_batch([3] * len(idx), queries)
+    pt, noise = gc.decrypt_mod_q_batch(resp, with_noise=True)
+    for k, i in enumerate(idx):
+        assert np.array_equal(pt[k], plain(i))
+        assert np.array_equal(pt[k], cl.decrypt(resp[k]))
+    assert int(noise.max()) < int(op.small_q) // (2 * int(op.t))
+
+
+def test_out_of_range_index():
+    gp, op = PirParams(16384, 9), O.params(16384, 9)
+    gc = PirClient(gp, O.Client(op, 1).secret())
+    a = np.zeros((1, op.N), np.uint64)
+    e = np.zeros((1, op.N), np.int64)
+    with pytest.raises(OutOfRange):
+        gc.fast_generate_query_batch([op.num_pt], a, e)
+    # the handle stays usable
+    assert gc.fast_generate_query_batch([0], a, e).shape == (1, 2, op.N)
