@@ -9,14 +9,18 @@
 //     (x*s)_i = sum_{j in P} xe[N+i-j] - sum_{j in M} xe[N+i-j]
 // over the sign-extended copy xe[N+m] = x[m], xe[m] = -x[m] (m < N) staged in
 // shared memory; only the epilogue reduces, so the result equals the NTT
-// product mod the same modulus exactly. x is split into 31-bit parts so each
-// shared word is an int32 and each partial sum fits an int64 (N 2^31 < 2^43).
-// Cost: |P|+|M| (about 2N/3) shared loads per output coefficient and part --
-// shared-memory bandwidth bound, one CTA per (item, output slice).
+// product mod the same modulus exactly. x is split into parts of at most 31
+// bits so each shared word is an int32 and each partial sum fits an int64.
+// Two forms of the product: the index-list form (list_product: one shared
+// load per nonzero secret coefficient, output and part) for any batch, and
+// for decryption batches that fill the GPU the window form (window_product:
+// register windows reused across secret coefficients one block apart, int32
+// partial sums). One CTA of kBlock threads per (item, output slice).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -44,117 +48,226 @@ struct ConstEntry {
   uint64_t val[2];
 };
 
-// xe for one polynomial, PARTS 31-bit parts, part p at ext + p 2n.
-template <int PARTS>
+// xe for one polynomial in NP parts of PB bits, part p at ext + p 2n.
+template <int NP, int PB>
 __device__ __forceinline__ void stage_ext(const uint64_t *__restrict__ x, uint64_t mod, uint32_t n,
                                           int32_t *ext) {
+  constexpr uint64_t kMask = (1ull << PB) - 1;
   for (uint32_t m = threadIdx.x; m < n; m += blockDim.x) {
     const uint64_t v = x[m] % mod;
-    const int32_t lo = static_cast<int32_t>(v & 0x7FFFFFFFull);
-    ext[n + m] = lo;
-    ext[m] = -lo;
-    if (PARTS == 2) {
-      const int32_t hi = static_cast<int32_t>(v >> 31);
-      ext[3 * n + m] = hi;
-      ext[2 * n + m] = -hi;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int32_t part = static_cast<int32_t>(p + 1 < NP ? (v >> (PB * p)) & kMask : v >> (PB * p));
+      ext[2 * n * p + n + m] = part;
+      ext[2 * n * p + m] = -part;
     }
   }
 }
 
-// acc[p][r] = part p of (x*s)_i for i = i0 + kBlock r.
-template <int PARTS, int R>
-__device__ __forceinline__ void ternary_product(const int32_t *ext, const uint16_t *sl,
-                                                uint32_t npos, uint32_t nneg, uint32_t n,
-                                                uint32_t i0, int64_t (&acc)[PARTS][R]) {
+// Index-list product: acc[p][r] = part p of (x*s)_i for i = i0 + kBlock r,
+// one shared load per nonzero secret coefficient, output and part.
+template <int NP, int R>
+__device__ __forceinline__ void list_product(const int32_t *ext, const uint16_t *sl,
+                                             uint32_t npos, uint32_t nneg, uint32_t n,
+                                             uint32_t i0, int64_t (&acc)[NP][R]) {
 #pragma unroll
-  for (int p = 0; p < PARTS; ++p)
+  for (int p = 0; p < NP; ++p)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[p][r] = 0;
   const int32_t *e0 = ext + n + i0;
-  const int32_t *e1 = ext + 3 * n + i0;
 #pragma unroll 4
   for (uint32_t u = 0; u < npos; ++u) {
     const int j = sl[u];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      acc[0][r] += e0[kBlock * r - j];
-      if (PARTS == 2) acc[PARTS - 1][r] += e1[kBlock * r - j];
-    }
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < NP; ++p) acc[p][r] += e0[2 * n * p + kBlock * r - j];
   }
 #pragma unroll 4
   for (uint32_t u = npos; u < npos + nneg; ++u) {
     const int j = sl[u];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      acc[0][r] -= e0[kBlock * r - j];
-      if (PARTS == 2) acc[PARTS - 1][r] -= e1[kBlock * r - j];
-    }
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < NP; ++p) acc[p][r] -= e0[2 * n * p + kBlock * r - j];
   }
 }
 
-template <int PARTS, int R>
-__device__ __forceinline__ uint64_t reduce_part_sums(const int64_t (&acc)[PARTS][R], int r,
-                                                     uint64_t mod) {
-  if (PARTS == 1) {
-    int64_t v = acc[0][r] % static_cast<int64_t>(mod);
-    return static_cast<uint64_t>(v < 0 ? v + static_cast<int64_t>(mod) : v);
+// Window product for n = kBlock J: with j = jl + kBlock jh, the term of output
+// i_r = i0 + kBlock r is xe[n + i0 - jl + kBlock (r - jh)], so for one jl the
+// thread loads the R + J - 1 window values once into registers and applies
+// all J secret coefficients s[jl + kBlock jh] (packed 2 bits each in cs[jl]:
+// 1 = +1, 2 = -1, 0 = 0; the same word for every thread, so the branches are
+// uniform) to all R outputs. Partial sums run in int32 for F = 2^(31 - PB -
+// log2 J) values of jl (each adds at most J terms below 2^PB per output) and
+// are then folded into the int64 totals.
+template <int NP, int PB, int R, int J>
+__device__ __forceinline__ void window_product(const int32_t *ext, const uint32_t *cs, uint32_t n,
+                                               uint32_t i0, int64_t (&acc)[NP][R]) {
+  constexpr int W = R + J - 1;
+  constexpr int kLogJ = J == 16 ? 4 : J == 8 ? 3 : J == 4 ? 2 : J == 2 ? 1 : 0;
+  constexpr int F = 1 << (31 - PB - kLogJ);
+  static_assert(31 - PB - kLogJ >= 0, "partial sums must fit an int32");
+  static_assert((1 << kLogJ) == J, "J is a power of two up to 16");
+  int32_t a32[NP][R];
+#pragma unroll
+  for (int p = 0; p < NP; ++p)
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[p][r] = 0, a32[p][r] = 0;
+  const int32_t *base = ext + n + i0 - kBlock * (J - 1);
+  for (int jl0 = 0; jl0 < kBlock; jl0 += F) {
+    const int jend = jl0 + F < kBlock ? jl0 + F : kBlock;
+#pragma unroll 1
+    for (int jl = jl0; jl < jend; ++jl) {
+      const uint32_t c = cs[jl];
+      if (c == 0) continue;
+      int32_t w[NP][W];
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+#pragma unroll
+        for (int d = 0; d < W; ++d) w[p][d] = base[2 * n * p - jl + kBlock * d];
+#pragma unroll
+      for (int jh = 0; jh < J; ++jh) {
+        const uint32_t cc = (c >> (2 * jh)) & 3u;
+        if (cc == 1u) {
+#pragma unroll
+          for (int p = 0; p < NP; ++p)
+#pragma unroll
+            for (int r = 0; r < R; ++r) a32[p][r] += w[p][r - jh + J - 1];
+        } else if (cc == 2u) {
+#pragma unroll
+          for (int p = 0; p < NP; ++p)
+#pragma unroll
+            for (int r = 0; r < R; ++r) a32[p][r] -= w[p][r - jh + J - 1];
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[p][r] += a32[p][r], a32[p][r] = 0;
   }
-  const __int128 v = (static_cast<__int128>(acc[PARTS - 1][r]) << 31) + acc[0][r];
-  __int128 m = v % static_cast<__int128>(mod);
-  if (m < 0) m += mod;
-  return static_cast<uint64_t>(m);
+}
+
+// sum_p acc[p] 2^(PB p) mod m, canonical.
+template <int NP, int PB, int R>
+__device__ __forceinline__ uint64_t reduce_parts(const int64_t (&acc)[NP][R], int r, uint64_t m) {
+  __int128 v = acc[NP - 1][r];
+#pragma unroll
+  for (int p = NP - 2; p >= 0; --p) v = v * (static_cast<__int128>(1) << PB) + acc[p][r];
+  __int128 x = v % static_cast<__int128>(m);
+  if (x < 0) x += m;
+  return static_cast<uint64_t>(x);
 }
 
 __device__ __forceinline__ uint64_t round_div(unsigned __int128 a, uint64_t b) {
   return static_cast<uint64_t>((a + (b >> 1)) / b);
 }
 
-// decrypt_mod_q: pt = round((c0 + c1 s mod sq) t / sq) mod t per coefficient;
-// max_noise (may be null, zeroed by the host) receives max |phase - round(sq m
-// / t)| over the response, the figure the reference reports as its noise
-// budget (client.cpp:389-407).
-template <int PARTS, int R>
+// decrypt_mod_q of one coefficient from prod = (c1 s mod sq): pt =
+// round((c0 + prod mod sq) t / sq) mod t; *worst tracks the max noise
+// |phase - round(sq m / t)| the reference reports as its noise budget
+// (client.cpp:389-407).
+__device__ __forceinline__ uint64_t decrypt_coeff(uint64_t prod, uint64_t c0, uint64_t sq,
+                                                  uint64_t t, uint64_t &worst) {
+  uint64_t phase = prod + c0 % sq;
+  if (phase >= sq) phase -= sq;
+  const uint64_t m = round_div(static_cast<unsigned __int128>(phase) * t, sq) % t;
+  const uint64_t approx = round_div(static_cast<unsigned __int128>(sq) * m, t) % sq;
+  const uint64_t pos = phase >= approx ? phase - approx : sq - approx + phase;
+  const uint64_t nabs = pos > (sq >> 1) ? sq - pos : pos;
+  worst = nabs > worst ? nabs : worst;
+  return m;
+}
+
+__device__ __forceinline__ void publish_noise(uint64_t worst, unsigned long long *max_noise) {
+  if (!max_noise) return;
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t w = __shfl_xor_sync(0xFFFFFFFFu, worst, o);
+    worst = w > worst ? w : worst;
+  }
+  if ((threadIdx.x & 31) == 0)
+    atomicMax(max_noise + blockIdx.x, static_cast<unsigned long long>(worst));
+}
+
+// c0 of one coefficient: -(prod + e) mod q (prod = a s mod q, e any int64).
+__device__ __forceinline__ uint64_t pack_coeff(uint64_t prod, int64_t ei, uint64_t q) {
+  const uint64_t em = ei >= 0 ? static_cast<uint64_t>(ei) % q
+                              : (q - static_cast<uint64_t>(-(ei + 1)) % q - 1);
+  uint64_t v = prod + em;
+  if (v >= q) v -= q;
+  return v ? q - v : 0;
+}
+
+// The query's plaintext constants that fall in this CTA's output slice
+// [o0, o0 + span), after every thread's c0 store (caller synchronises).
+__device__ __forceinline__ void add_constants(const ConstEntry *ce, uint32_t nconst, uint32_t limb,
+                                              uint32_t o0, uint32_t span, uint64_t q,
+                                              uint64_t *c0) {
+  for (uint32_t u = threadIdx.x; u < nconst; u += blockDim.x) {
+    const uint32_t pos = ce[u].pos;
+    if (pos == kNoPos || pos < o0 || pos >= o0 + span) continue;
+    const uint64_t v = c0[pos] + ce[u].val[limb];
+    c0[pos] = v >= q ? v - q : v;
+  }
+}
+
+// decrypt_mod_q for response blockIdx.x, output slice blockIdx.y: index-list
+// product (any batch) with 31-bit parts.
+template <int NP, int R>
 __global__ void __launch_bounds__(kBlock) k_client_decrypt(
     const uint64_t *__restrict__ resp, const uint16_t *__restrict__ sidx, uint32_t npos,
     uint32_t nneg, uint32_t n, uint64_t sq, uint64_t t, uint64_t *__restrict__ pt,
     unsigned long long *__restrict__ max_noise) {
   extern __shared__ __align__(16) int32_t smem[];
   int32_t *ext = smem;
-  uint16_t *sl = reinterpret_cast<uint16_t *>(smem + PARTS * 2 * n);
+  uint16_t *sl = reinterpret_cast<uint16_t *>(smem + NP * 2 * n);
   const uint64_t b = blockIdx.x;
   const uint64_t *c0 = resp + b * 2 * n, *c1 = c0 + n;
-  stage_ext<PARTS>(c1, sq, n, ext);
+  stage_ext<NP, 31>(c1, sq, n, ext);
   for (uint32_t u = threadIdx.x; u < npos + nneg; u += blockDim.x) sl[u] = sidx[u];
   __syncthreads();
   const uint32_t i0 = blockIdx.y * (n / gridDim.y) + threadIdx.x;
-  int64_t acc[PARTS][R];
-  ternary_product<PARTS, R>(ext, sl, npos, nneg, n, i0, acc);
+  int64_t acc[NP][R];
+  list_product<NP, R>(ext, sl, npos, nneg, n, i0, acc);
   uint64_t worst = 0;
-  const uint64_t half = sq >> 1;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const uint32_t i = i0 + kBlock * r;
-    uint64_t phase = reduce_part_sums<PARTS, R>(acc, r, sq) + c0[i] % sq;
-    if (phase >= sq) phase -= sq;
-    const uint64_t m = round_div(static_cast<unsigned __int128>(phase) * t, sq) % t;
-    pt[b * n + i] = m;
-    const uint64_t approx = round_div(static_cast<unsigned __int128>(sq) * m, t) % sq;
-    const uint64_t npos_ = phase >= approx ? phase - approx : sq - approx + phase;
-    const uint64_t nabs = npos_ > half ? sq - npos_ : npos_;
-    worst = nabs > worst ? nabs : worst;
+    pt[b * n + i] = decrypt_coeff(reduce_parts<NP, 31, R>(acc, r, sq), c0[i], sq, t, worst);
   }
-  if (max_noise) {
-    for (int o = 16; o > 0; o >>= 1) {
-      const uint64_t w = __shfl_xor_sync(0xFFFFFFFFu, worst, o);
-      worst = w > worst ? w : worst;
-    }
-    if ((threadIdx.x & 31) == 0) atomicMax(max_noise + b, static_cast<unsigned long long>(worst));
-  }
+  publish_noise(worst, max_noise);
 }
 
-// fast_generate_query for item = (query, limb): c0 = -(a s + e) mod q_k plus
-// the query's plaintext constants, c1 = a as given. a and the output are
-// limb-major per query: a [K n], out [c0 (K n)][c1 (K n)].
+// The same with the window product (n = kBlock J, PB-bit parts).
+template <int NP, int PB, int R, int J>
+__global__ void __launch_bounds__(kBlock) k_client_decrypt_w(
+    const uint64_t *__restrict__ resp, const uint32_t *__restrict__ code, uint32_t n, uint64_t sq,
+    uint64_t t, uint64_t *__restrict__ pt, unsigned long long *__restrict__ max_noise) {
+  extern __shared__ __align__(16) int32_t smem[];
+  int32_t *ext = smem;
+  uint32_t *cs = reinterpret_cast<uint32_t *>(smem + NP * 2 * n);
+  const uint64_t b = blockIdx.x;
+  const uint64_t *c0 = resp + b * 2 * n, *c1 = c0 + n;
+  stage_ext<NP, PB>(c1, sq, n, ext);
+  for (uint32_t u = threadIdx.x; u < kBlock; u += blockDim.x) cs[u] = code[u];
+  __syncthreads();
+  const uint32_t i0 = blockIdx.y * (n / gridDim.y) + threadIdx.x;
+  int64_t acc[NP][R];
+  window_product<NP, PB, R, J>(ext, cs, n, i0, acc);
+  uint64_t worst = 0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const uint32_t i = i0 + kBlock * r;
+    pt[b * n + i] = decrypt_coeff(reduce_parts<NP, PB, R>(acc, r, sq), c0[i], sq, t, worst);
+  }
+  publish_noise(worst, max_noise);
+}
+
+// fast_generate_query for item = (query, limb) = blockIdx.x, output slice
+// blockIdx.y: c0 = -(a s + e) mod q_k plus the query's plaintext constants,
+// c1 = a as given. a and the output are limb-major per query: a [K n], out
+// [c0 (K n)][c1 (K n)]. Index-list product with 31-bit parts.
 template <int R>
 __global__ void __launch_bounds__(kBlock) k_client_pack(
     const uint64_t *__restrict__ a, const int64_t *__restrict__ e,
@@ -169,35 +282,24 @@ __global__ void __launch_bounds__(kBlock) k_client_pack(
   const uint64_t q = limb ? q1 : q0;
   const uint64_t kn = static_cast<uint64_t>(limbs) * n;
   const uint64_t *x = a + query * kn + static_cast<uint64_t>(limb) * n;
-  stage_ext<2>(x, q, n, ext);
+  stage_ext<2, 31>(x, q, n, ext);
   for (uint32_t u = threadIdx.x; u < npos + nneg; u += blockDim.x) sl[u] = sidx[u];
   __syncthreads();
   const uint32_t span = n / gridDim.y, o0 = blockIdx.y * span;
   const uint32_t i0 = o0 + threadIdx.x;
   int64_t acc[2][R];
-  ternary_product<2, R>(ext, sl, npos, nneg, n, i0, acc);
+  list_product<2, R>(ext, sl, npos, nneg, n, i0, acc);
   uint64_t *c0 = out + query * 2 * kn + static_cast<uint64_t>(limb) * n;
   uint64_t *c1 = c0 + kn;
   const int64_t *eq = e + query * n;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const uint32_t i = i0 + kBlock * r;
-    const int64_t ei = eq[i];
-    const uint64_t em = ei >= 0 ? static_cast<uint64_t>(ei) % q
-                                : (q - static_cast<uint64_t>(-(ei + 1)) % q - 1);
-    uint64_t v = reduce_part_sums<2, R>(acc, r, q) + em;
-    if (v >= q) v -= q;
-    c0[i] = v ? q - v : 0;
+    c0[i] = pack_coeff(reduce_parts<2, 31, R>(acc, r, q), eq[i], q);
     c1[i] = x[i];
   }
   __syncthreads();
-  const ConstEntry *ce = consts + query * nconst;
-  for (uint32_t u = threadIdx.x; u < nconst; u += blockDim.x) {
-    const uint32_t pos = ce[u].pos;
-    if (pos == kNoPos || pos < o0 || pos >= o0 + span) continue;
-    const uint64_t v = c0[pos] + ce[u].val[limb];
-    c0[pos] = v >= q ? v - q : v;
-  }
+  add_constants(consts + query * nconst, nconst, limb, o0, span, q, c0);
 }
 
 uint64_t bitrev(uint64_t x, uint32_t bits) {
@@ -220,6 +322,7 @@ struct opir_client {
   uint64_t mods[2]{};        // ciphertext moduli: the logical q (K = 1) or the two limbs
   DevBuf<uint16_t> sidx;     // [P | M] secret index lists
   uint32_t npos = 0, nneg = 0;
+  DevBuf<uint32_t> code;     // [kBlock]: s[jl + kBlock jh] 2 bits each (window product)
   uint32_t nconst = 1;       // constant slots per query
   uint64_t one_val[2]{};     // the one-hot's value per limb
   std::vector<uint64_t> gadget_val;  // [k][limb]: B^(L_EP-1-k) (2^h)^-1 mod q_limb
@@ -353,9 +456,8 @@ void query_constants(const opir_client &c, uint64_t idx, ConstEntry *out) {
   }
 }
 
-// Output slices per item so that a batch fills the GPU; R = n / (s kBlock)
-// outputs per thread, at most kMaxR (registers: 2 kMaxR int64 accumulators,
-// so that two or more CTAs stay resident per SM).
+// Output slices per item so that a batch fills the GPU (index-list
+// product); R = n / (s kBlock) outputs per thread, at most kMaxR.
 constexpr uint32_t kMaxR = 8;
 uint32_t slices_for(uint64_t items, uint32_t n, int sms) {
   uint32_t s = 1;
@@ -364,50 +466,95 @@ uint32_t slices_for(uint64_t items, uint32_t n, int sms) {
   return s;
 }
 
-template <int PARTS>
-void launch_decrypt(uint32_t R, dim3 grid, size_t smem, cudaStream_t st, const uint64_t *resp,
-                    const opir_client &c, uint64_t *pt, unsigned long long *noise) {
-  const uint16_t *s = c.sidx.p;
-  const uint32_t n = c.n;
-  const uint64_t sq = c.params.small_q, t = c.params.plain_mod;
-  switch (R) {
-#define OPIR_DEC(RR)                                                                          \
-  case RR:                                                                                    \
-    ck(cudaFuncSetAttribute(k_client_decrypt<PARTS, RR>,                                      \
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),          \
-       "client decrypt smem");                                                                \
-    k_client_decrypt<PARTS, RR><<<grid, kBlock, smem, st>>>(resp, s, c.npos, c.nneg, n, sq, t, \
-                                                            pt, noise);                       \
-    break;
-    OPIR_DEC(1) OPIR_DEC(2) OPIR_DEC(4) OPIR_DEC(8)
-#undef OPIR_DEC
-    default:
-      throw std::runtime_error("client decrypt: unsupported slice width");
-  }
-  ck(cudaGetLastError(), "client decrypt launch");
+// The window product pays when each thread keeps R >= 4 outputs (R + J - 1
+// loads serve R J terms); decryption uses it when those slices still give
+// every SM a CTA. Query packing keeps the index-list product: its moduli need
+// three 20-bit parts in the window form, which issued as many instructions
+// per term as the list form at half the occupancy. OPIR_CLIENT_WINDOW=0 keeps
+// the index-list product everywhere.
+bool window_enabled() {
+  const char *v = std::getenv("OPIR_CLIENT_WINDOW");
+  return !(v && v[0] == '0');
+}
+uint32_t window_r(uint64_t items, uint32_t n, int sms) {
+  if (!window_enabled() || (n != 2048 && n != 4096)) return 0;
+  for (uint32_t R : {8u, 4u})
+    if (items * (n / (kBlock * R)) >= static_cast<uint64_t>(sms)) return R;
+  return 0;
+}
+
+template <typename K>
+void set_smem(K kernel, size_t smem, const char *what) {
+  ck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          static_cast<int>(smem)),
+     what);
+}
+
+void launched(const char *what) {
+  ck(cudaGetLastError(), what);
   opir::note_launches(1);
 }
 
-void launch_pack(uint32_t R, dim3 grid, size_t smem, cudaStream_t st, const uint64_t *a,
-                 const int64_t *e, const opir_client &c, uint64_t *out) {
-  const uint16_t *s = c.sidx.p;
-  switch (R) {
-#define OPIR_PACK(RR)                                                                          \
-  case RR:                                                                                     \
-    ck(cudaFuncSetAttribute(k_client_pack<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                            (int)smem),                                                        \
-       "client pack smem");                                                                    \
-    k_client_pack<RR><<<grid, kBlock, smem, st>>>(a, e, c.consts.p, c.nconst, s, c.npos,       \
-                                                  c.nneg, c.n, c.limbs, c.mods[0], c.mods[1],  \
-                                                  out);                                        \
-    break;
-    OPIR_PACK(1) OPIR_PACK(2) OPIR_PACK(4) OPIR_PACK(8)
-#undef OPIR_PACK
-    default:
-      throw std::runtime_error("client pack: unsupported slice width");
+void launch_decrypt(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, const opir_client &c,
+                    uint64_t *pt, unsigned long long *noise) {
+  const uint32_t n = c.n;
+  const uint64_t sq = c.params.small_q, t = c.params.plain_mod;
+  const uint32_t nb = static_cast<uint32_t>(n_resp);
+  const uint32_t R = sq < (1ull << 50) ? window_r(n_resp, n, c.sms) : 0;
+  if (R) {
+    const int np = sq < (1ull << 25) ? 1 : 2;
+    const dim3 grid(nb, n / (kBlock * R));
+    const size_t smem = np * 2 * n * sizeof(int32_t) + kBlock * sizeof(uint32_t);
+#define OPIR_DECW(NP, RR, JJ)                                                                  \
+  if (np == NP && R == RR && n == kBlock * JJ) {                                              \
+    set_smem(k_client_decrypt_w<NP, 25, RR, JJ>, smem, "client decrypt smem");               \
+    k_client_decrypt_w<NP, 25, RR, JJ><<<grid, kBlock, smem, st>>>(resp, c.code.p, n, sq, t,  \
+                                                                   pt, noise);                \
+    return launched("client decrypt launch");                                                 \
   }
-  ck(cudaGetLastError(), "client pack launch");
-  opir::note_launches(1);
+    OPIR_DECW(1, 8, 8) OPIR_DECW(1, 4, 8) OPIR_DECW(1, 8, 16) OPIR_DECW(1, 4, 16)
+    OPIR_DECW(2, 8, 8) OPIR_DECW(2, 4, 8) OPIR_DECW(2, 8, 16) OPIR_DECW(2, 4, 16)
+#undef OPIR_DECW
+    throw std::runtime_error("client decrypt: no window kernel for this shape");
+  }
+  const uint32_t s = slices_for(n_resp, n, c.sms);
+  const uint32_t Rl = n / (s * kBlock);
+  const dim3 grid(nb, s);
+  const size_t lists = (c.npos + c.nneg + 8) * sizeof(uint16_t);
+  const int np = sq < (1ull << 31) ? 1 : 2;
+  const size_t smem = np * 2 * n * sizeof(int32_t) + lists;
+#define OPIR_DEC(NP, RR)                                                                      \
+  if (np == NP && Rl == RR) {                                                                 \
+    set_smem(k_client_decrypt<NP, RR>, smem, "client decrypt smem");                          \
+    k_client_decrypt<NP, RR><<<grid, kBlock, smem, st>>>(resp, c.sidx.p, c.npos, c.nneg, n,   \
+                                                         sq, t, pt, noise);                   \
+    return launched("client decrypt launch");                                                 \
+  }
+  OPIR_DEC(1, 1) OPIR_DEC(1, 2) OPIR_DEC(1, 4) OPIR_DEC(1, 8)
+  OPIR_DEC(2, 1) OPIR_DEC(2, 2) OPIR_DEC(2, 4) OPIR_DEC(2, 8)
+#undef OPIR_DEC
+  throw std::runtime_error("client decrypt: unsupported slice width");
+}
+
+void launch_pack(uint64_t items, cudaStream_t st, const uint64_t *a, const int64_t *e,
+                 const opir_client &c, uint64_t *out) {
+  const uint32_t n = c.n;
+  const uint32_t ni = static_cast<uint32_t>(items);
+  const uint32_t s = slices_for(items, n, c.sms);
+  const uint32_t Rl = n / (s * kBlock);
+  const dim3 grid(ni, s);
+  const size_t smem = 2 * 2 * n * sizeof(int32_t) + (c.npos + c.nneg + 8) * sizeof(uint16_t);
+#define OPIR_PACK(RR)                                                                         \
+  if (Rl == RR) {                                                                             \
+    set_smem(k_client_pack<RR>, smem, "client pack smem");                                    \
+    k_client_pack<RR><<<grid, kBlock, smem, st>>>(a, e, c.consts.p, c.nconst, c.sidx.p,       \
+                                                  c.npos, c.nneg, n, c.limbs, c.mods[0],      \
+                                                  c.mods[1], out);                            \
+    return launched("client pack launch");                                                    \
+  }
+  OPIR_PACK(1) OPIR_PACK(2) OPIR_PACK(4) OPIR_PACK(8)
+#undef OPIR_PACK
+  throw std::runtime_error("client pack: unsupported slice width");
 }
 
 }  // namespace
@@ -442,6 +589,11 @@ opir_status opir_client_create(const opir_params *params, const int8_t *secret, 
     for (uint32_t j = 0; j < c->n; ++j)
       if (secret[j] == -1) lists.push_back(static_cast<uint16_t>(j));
     c->nneg = static_cast<uint32_t>(lists.size()) - c->npos;
+    std::vector<uint32_t> code(kBlock, 0);
+    if (c->n % kBlock == 0 && c->n / kBlock <= 16)
+      for (uint32_t j = 0; j < c->n; ++j)
+        if (secret[j] != 0)
+          code[j % kBlock] |= (secret[j] == 1 ? 1u : 2u) << (2 * (j / kBlock));
     c->nconst = 1 + (c->params.num_dims - 1) * c->params.l_ep;
     prepare_constants(*c);
     DeviceGuard g(device);
@@ -452,6 +604,9 @@ opir_status opir_client_create(const opir_params *params, const int8_t *secret, 
       ck(cudaMemcpy(c->sidx.p, lists.data(), lists.size() * sizeof(uint16_t),
                     cudaMemcpyHostToDevice),
          "secret upload");
+    c->code.alloc(kBlock);
+    ck(cudaMemcpy(c->code.p, code.data(), kBlock * sizeof(uint32_t), cudaMemcpyHostToDevice),
+       "secret code upload");
   });
   if (st != OPIR_OK) {
     delete c;
@@ -469,6 +624,7 @@ void opir_client_destroy(opir_client *c) {
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
     c->sidx.reset();
+    c->code.reset();
     c->consts.reset();
     if (c->staging) cudaFreeHost(c->staging);
     if (c->staged) cudaEventDestroy(c->staged);
@@ -514,11 +670,7 @@ opir_status opir_client_generate_queries_device(opir_client *c, uint32_t n,
                        cudaMemcpyHostToDevice, st),
        "client constants upload");
     ck(cudaEventRecord(c->staged, st), "client staging record");
-    const uint64_t items = static_cast<uint64_t>(n) * c->limbs;
-    const uint32_t s = slices_for(items, c->n, c->sms);
-    const size_t smem = 2 * 2 * c->n * sizeof(int32_t) + (c->npos + c->nneg + 8) * sizeof(uint16_t);
-    launch_pack(c->n / (s * kBlock), dim3(static_cast<uint32_t>(items), s), smem, st, d_a, d_e, *c,
-                d_queries);
+    launch_pack(static_cast<uint64_t>(n) * c->limbs, st, d_a, d_e, *c, d_queries);
   });
 }
 
@@ -534,17 +686,8 @@ opir_status opir_client_decrypt_device(opir_client *c, uint32_t n, const uint64_
     if (d_max_noise)
       ck(cudaMemsetAsync(d_max_noise, 0, static_cast<size_t>(n) * sizeof(uint64_t), st),
          "noise reset");
-    const uint32_t s = slices_for(n, c->n, c->sms);
-    const uint32_t R = c->n / (s * kBlock);
-    const dim3 grid(n, s);
-    auto *noise = reinterpret_cast<unsigned long long *>(d_max_noise);
-    const size_t lists = (c->npos + c->nneg + 8) * sizeof(uint16_t);
-    if (c->params.small_q < (1ull << 31))
-      launch_decrypt<1>(R, grid, 2 * c->n * sizeof(int32_t) + lists, st, d_responses, *c,
-                        d_plaintexts, noise);
-    else
-      launch_decrypt<2>(R, grid, 4 * c->n * sizeof(int32_t) + lists, st, d_responses, *c,
-                        d_plaintexts, noise);
+    launch_decrypt(n, st, d_responses, *c, d_plaintexts,
+                   reinterpret_cast<unsigned long long *>(d_max_noise));
   });
 }
 

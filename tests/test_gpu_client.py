@@ -4,8 +4,10 @@ client.cpp:364-410) against the oracle client, bit for bit: queries packed on
 the GPU from the oracle's own uniform c1 and error equal the oracle's queries;
 responses decrypted on the GPU equal the oracle's plaintexts and max noise;
 and a GPU-packed query answered by the GPU server decrypts on the GPU to the
-database plaintext. Batch sizes cover every outputs-per-thread width the
-launcher picks (1, 2, 4, 8)."""
+database plaintext. Every case runs twice: as the launcher picks (auto: the
+window kernel for decryption batches that fill the GPU) and with the
+index-list kernel forced (OPIR_CLIENT_WINDOW=0); batch sizes cover every
+outputs-per-thread width each kernel uses (list: 1, 2, 4, 8; window: 4, 8)."""
 import numpy as np
 import pytest
 
@@ -14,6 +16,15 @@ from onionpirv2_b200.client import PirClient
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=["auto", "list"])
+def kernel(request, monkeypatch):
+    if request.param == "list":
+        monkeypatch.setenv("OPIR_CLIENT_WINDOW", "0")
+    else:
+        monkeypatch.delenv("OPIR_CLIENT_WINDOW", raising=False)
+    return request.param
 
 C4 = "CONFIG_N4096_K2_MP"
 
@@ -29,7 +40,7 @@ def _uniform(rng, mods, n, N):
 
 
 @pytest.mark.parametrize("n", [1, 80, 150, 300])
-def test_k1_queries_match_oracle(n):
+def test_k1_queries_match_oracle(n, kernel):
     target, h = 43690, 10
     gp, op = PirParams(target, h), O.params(target, h)
     rng = np.random.default_rng(1000 + n)
@@ -44,7 +55,7 @@ def test_k1_queries_match_oracle(n):
 
 
 @pytest.mark.parametrize("n", [1, 40, 75, 200])
-def test_c4_queries_match_oracle(n):
+def test_c4_queries_match_oracle(n, kernel):
     target, h = 16384, 9
     gp, op = PirParams(target, h, config=C4), O.c4_params(target, h)
     rng = np.random.default_rng(2000 + n)
@@ -58,22 +69,23 @@ def test_c4_queries_match_oracle(n):
     assert np.array_equal(got, np.stack([q for q, _ in parts]))
 
 
-def test_k1_error_of_any_size_enters_linearly():
+def test_k1_error_of_any_size_enters_linearly(kernel):
     """c0 is -(a s + e) mod q for any int64 error, not only Gaussian ones:
     the difference of two packings is -(e' - e) mod q everywhere."""
     target, h = 16384, 9
     gp, op = PirParams(target, h), O.params(target, h)
     rng = np.random.default_rng(7)
-    a = _uniform(rng, [op.q], 2, op.N)[:, 0]
+    n = 160  # wide enough for the window kernel
+    a = _uniform(rng, [op.q], n, op.N)[:, 0]
     cl = O.Client(op, 5)
     gc = PirClient(gp, cl.secret())
-    e = np.stack([cl.query_parts(3, a[i])[1] for i in range(2)])
-    big = rng.integers(-(1 << 62), 1 << 62, size=(2, op.N), dtype=np.int64)
+    e = np.stack([cl.query_parts(3, a[i])[1] for i in range(n)])
+    big = rng.integers(-(1 << 62), 1 << 62, size=(n, op.N), dtype=np.int64)
     big[0, :4] = [np.iinfo(np.int64).min, np.iinfo(np.int64).max, -1, 0]
-    q1 = gc.fast_generate_query_batch([3, 3], a, e)
-    q2 = gc.fast_generate_query_batch([3, 3], a, big)
+    q1 = gc.fast_generate_query_batch([3] * n, a, e)
+    q2 = gc.fast_generate_query_batch([3] * n, a, big)
     q = int(op.q)
-    for i in range(2):
+    for i in (0, n - 1):
         for j in range(op.N):
             assert (int(q2[i, 0, j]) - int(q1[i, 0, j])) % q == (-(int(big[i, j]) - int(e[i, j]))) % q
     assert np.array_equal(q1[:, 1], q2[:, 1])
@@ -81,7 +93,7 @@ def test_k1_error_of_any_size_enters_linearly():
 
 @pytest.mark.parametrize("config,n", [("k1", 1), ("k1", 80), ("k1", 150), ("k1", 300),
                                       ("c4", 1), ("c4", 40), ("c4", 75), ("c4", 200)])
-def test_decrypt_matches_oracle(config, n):
+def test_decrypt_matches_oracle(config, n, kernel):
     if config == "k1":
         gp, op = PirParams(16384, 9), O.params(16384, 9)
         cl = O.Client(op, 17)
@@ -100,7 +112,7 @@ def test_decrypt_matches_oracle(config, n):
 
 
 @pytest.mark.parametrize("config", ["k1", "c4"])
-def test_gpu_query_answer_decrypt_round_trip(config):
+def test_gpu_query_answer_decrypt_round_trip(config, kernel):
     target, h, db_seed = 16384, 9, 23
     if config == "k1":
         gp, op = PirParams(target, h), O.params(target, h)
