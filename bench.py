@@ -914,6 +914,24 @@ def bench_client(args, world, rank, local):
     def pack():
         gc.generate_queries_device(idx, d_a.data_ptr(), d_e.data_ptr(), d_q.data_ptr(), sp)
 
+    # one client's session keys per keygen step
+    h, lks, lkey = gp.expansion_height, gp.l_ks, gp.l_key
+    kshape = a.shape[1:]
+    d_bva = torch.from_numpy(np.stack([np.stack([rng.integers(0, int(q), N, dtype=np.uint64)
+                                                 for q in mods]) for _ in range(h * lks)])
+                             .view(np.int64)).to(device)
+    d_bve = torch.from_numpy(np.rint(rng.normal(0.0, 3.2, (h * lks, N))).astype(np.int64)).to(device)
+    d_ga = torch.from_numpy(np.stack([np.stack([rng.integers(0, int(q), N, dtype=np.uint64)
+                                                for q in mods]) for _ in range(2 * lkey)])
+                            .view(np.int64)).to(device)
+    d_ge = torch.from_numpy(np.rint(rng.normal(0.0, 3.2, (2 * lkey, N))).astype(np.int64)).to(device)
+    d_bvk = torch.empty((h * lks, 2) + kshape, dtype=torch.int64, device=device)
+    d_gk = torch.empty((2 * lkey, 2) + kshape, dtype=torch.int64, device=device)
+
+    def keygen():
+        gc.keygen_device(d_bva.data_ptr(), d_bve.data_ptr(), d_ga.data_ptr(), d_ge.data_ptr(),
+                         d_bvk.data_ptr(), d_gk.data_ptr(), sp)
+
     def timed(fn, steps):
         total = 0.0
         for _ in range(steps):
@@ -929,12 +947,14 @@ def bench_client(args, world, rank, local):
     for _ in range(args.warmup):
         dec()
         pack()
+        keygen()
     torch.cuda.synchronize(device)
     barrier(world, device)
     l0 = launch_count()
     with ClockSampler(local) as clk:
         t_dec = max_over_ranks(timed(dec, args.steps), world, device)
         t_pack = max_over_ranks(timed(pack, args.steps), world, device)
+        t_key = max_over_ranks(timed(keygen, args.steps), world, device)
 
         def e2e_step():
             d_resp.copy_(h_resp, non_blocking=True)
@@ -970,6 +990,9 @@ def bench_client(args, world, rank, local):
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "pack": {"value": world * n * args.steps / t_pack, "unit": "queries/s",
                  "ms_per_step": t_pack * 1e3 / args.steps},
+        "keygen": {"value": world * args.steps / t_key, "unit": "session key sets/s",
+                   "ms_per_step": t_key * 1e3 / args.steps,
+                   "rows": h * lks + 2 * lkey},
         "e2e": {"value": world * n * args.steps / t_e2e, "unit": "responses/s",
                 "h2d_bytes_per_step": int(resp.nbytes), "d2h_bytes_per_step": int(n * N * 8)},
         "roofline": {"bound": "issue", "achieved": achieved, "peak": peak,
@@ -993,6 +1016,14 @@ def bench_client(args, world, rank, local):
             "value": done / el, "unit": "responses/s", "cores": 1, "kind": "port",
             "sample": f"oracle decrypt_mod_q (NTT mod small_q, one core) of {done} of the "
                       f"step's responses; CPU {cpu_model()}"}
+        t0 = time.perf_counter()
+        made = 0
+        while time.perf_counter() - t0 < 5.0 and made < 20:
+            (O.C4Client if c4 else O.Client)(op, 100 + made)
+            made += 1
+        line["keygen"]["cpu_port"] = {
+            "value": made / (time.perf_counter() - t0), "unit": "session key sets/s", "cores": 1,
+            "sample": f"oracle client construction (secret + BV keys + RGSW key), {made} clients"}
     print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

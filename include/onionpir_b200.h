@@ -479,9 +479,10 @@ opir_status opir_ext_prod_mux_noalloc(const opir_params *params, uint32_t n,
  * The two client steps of the protocol that scale with the number of queries
  * or responses, for one client (one ternary secret) at a time: query packing
  * (PirClient::fast_generate_query, src/client.cpp:107-225) and response
- * decryption (PirClient::decrypt_mod_q, src/client.cpp:364-410). Key
- * generation stays with the caller. A client handle holds the secret on one
- * device; calls on one handle must not run concurrently. */
+ * decryption (PirClient::decrypt_mod_q, src/client.cpp:364-410), plus the
+ * client's session keys. The random samples stay with the caller. A client
+ * handle holds the secret on one device; calls on one handle must not run
+ * concurrently. */
 typedef struct opir_client opir_client;
 
 /* secret: N int8 coefficients in {-1, 0, 1} (the coefficient form of the
@@ -517,6 +518,25 @@ opir_status opir_client_generate_queries_device(opir_client *client, uint32_t n,
 opir_status opir_client_decrypt_device(opir_client *client, uint32_t n,
                                        const uint64_t *d_responses, uint64_t *d_plaintexts,
                                        uint64_t *d_max_noise, void *stream);
+
+/* create_session_keys (client.cpp:40-45) with the randomness given: the BV
+ * key-switching keys for galois_k = N/2^i + 1, i < h (gen_bv_ks_key,
+ * bv_keyswitch.cpp:191-276: row r = (B^r sigma_k(s) - a s + e, a) with
+ * B = 2^base_log2_ks) and the RGSW encryption of s (generate_gsw_from_key,
+ * client.cpp:25-38, gsw.cpp:359-422: row (half, r) = an encryption of zero
+ * (-(a s + e), a) plus s B_key^(L_KEY-1-r) in polynomial `half`), every
+ * polynomial then in the NTT domain -- the layouts opir_server_set_client_keys
+ * takes.
+ *   d_bv_a / d_bv_e   : h x L_KS x K N u64 (uniform, coefficient form) and
+ *                       h x L_KS x N int64 (error) device arrays; NULL when h = 0
+ *   d_gsw_a / d_gsw_e : 2 L_KEY x K N u64 and 2 L_KEY x N int64
+ *   d_bv_keys         : h x L_KS x 2 x K N u64, each row [b][a]
+ *   d_gsw_key         : 2 L_KEY x 2 x K N u64, each row [c0][c1]
+ * Equal, for equal (secret, a, e), to the reference's keys. */
+opir_status opir_client_keygen_device(opir_client *client, const uint64_t *d_bv_a,
+                                      const int64_t *d_bv_e, const uint64_t *d_gsw_a,
+                                      const int64_t *d_gsw_e, uint64_t *d_bv_keys,
+                                      uint64_t *d_gsw_key, void *stream);
 
 /* ---- tree PIR level selection ------------------------------------------
  * The full-binary-tree PIR layer of the reference (src/tree_index.cpp,

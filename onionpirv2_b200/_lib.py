@@ -142,6 +142,7 @@ _SIGS = {
                                              C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "opir_client_decrypt_device": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p], C.c_int),
+    "opir_client_keygen_device": ([C.c_void_p] + [C.c_void_p] * 6 + [C.c_void_p], C.c_int),
     "opir_ext_prod_mux_noalloc": ([C.POINTER(Params), C.c_uint32, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
 }

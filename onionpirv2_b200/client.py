@@ -1,12 +1,13 @@
 """GPU batch operations of the reference's PirClient (src/client.cpp) for
-one client's secret: query packing (fast_generate_query, :107-225) and
-response decryption (decrypt_mod_q, :364-410), over the C ABI's
-opir_client_* calls (include/onionpir_b200.h).
+one client's secret: query packing (fast_generate_query, :107-225),
+response decryption (decrypt_mod_q, :364-410) and the session keys
+(create_session_keys, :40-45), over the C ABI's opir_client_* calls
+(include/onionpir_b200.h).
 
 The randomness of a query (the uniform c1 `a` and the error `e`) is an input:
 the reference draws it from its own generators, the codec expands `a` from a
-seed (codec.prf_expand), and a caller may sample `e` however it likes. Key
-generation stays on the host.
+seed (codec.prf_expand), and a caller may sample `e` however it likes; the
+same holds for the uniform parts and errors of the session keys.
 """
 from __future__ import annotations
 
@@ -66,7 +67,43 @@ class PirClient:
             C.c_void_p(d_max_noise) if d_max_noise else None,
             C.c_void_p(stream) if stream else None))
 
+    def keygen_device(self, d_bv_a: int, d_bv_e: int, d_gsw_a: int, d_gsw_e: int,
+                      d_bv_keys: int, d_gsw_key: int, stream: int = 0):
+        p = lambda v: C.c_void_p(v) if v else None  # noqa: E731
+        self._check(self._lib.opir_client_keygen_device(
+            self._h, p(d_bv_a), p(d_bv_e), p(d_gsw_a), p(d_gsw_e), p(d_bv_keys), p(d_gsw_key),
+            p(stream)))
+
     # ---- host form (torch moves the buffers) -------------------------------
+    def create_session_keys(self, bv_a: np.ndarray, bv_e: np.ndarray, gsw_a: np.ndarray,
+                            gsw_e: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """The BV keys (h, L_KS) + ct_shape and the RGSW key (2 L_KEY,) +
+        ct_shape from the uniform parts (coefficient form, limb-major per
+        row) and errors the reference's generators would draw."""
+        import torch
+        P = self.params
+        h, lks, lkey, N = P.expansion_height, P.l_ks, P.l_key, P.N
+        cs = P.ct_shape
+        dev = torch.device("cuda", self.device)
+
+        def up(x, dt, shape):
+            x = np.ascontiguousarray(x, dtype=dt).reshape(shape)
+            t = torch.from_numpy(x.view(np.int64) if dt == np.uint64 else x)
+            return t.to(dev)
+
+        da_bv = up(bv_a, np.uint64, (h, lks) + cs[1:]) if h else None
+        de_bv = up(bv_e, np.int64, (h, lks, N)) if h else None
+        da_g = up(gsw_a, np.uint64, (2 * lkey,) + cs[1:])
+        de_g = up(gsw_e, np.int64, (2 * lkey, N))
+        bv = torch.empty((h, lks) + cs, dtype=torch.int64, device=dev) if h else None
+        gsw = torch.empty((2 * lkey,) + cs, dtype=torch.int64, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        ptr = lambda t: t.data_ptr() if t is not None else 0  # noqa: E731
+        self.keygen_device(ptr(da_bv), ptr(de_bv), da_g.data_ptr(), de_g.data_ptr(), ptr(bv),
+                           gsw.data_ptr(), stream.cuda_stream)
+        bv_h = bv.cpu().numpy().view(np.uint64) if h else np.zeros((0, lks) + cs, np.uint64)
+        return bv_h, gsw.cpu().numpy().view(np.uint64)
+
     def fast_generate_query_batch(self, pt_idx: Sequence[int], a: np.ndarray,
                                   e: np.ndarray) -> np.ndarray:
         """Queries for pt_idx with c1 = a[i] and error e[i]: (n,) + ct_shape."""

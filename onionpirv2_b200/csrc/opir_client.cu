@@ -1,6 +1,7 @@
 // Client-side batch operations: query packing (PirClient::fast_generate_query,
-// src/client.cpp:107-225) and response decryption (PirClient::decrypt_mod_q,
-// src/client.cpp:364-410) for many queries or responses of one client.
+// src/client.cpp:107-225), response decryption (PirClient::decrypt_mod_q,
+// src/client.cpp:364-410) for many queries or responses of one client, and
+// its session keys (create_session_keys, src/client.cpp:40-45).
 //
 // Both are dominated by one negacyclic product x * s with the client's ternary
 // secret s. The reference multiplies in the NTT domain mod the target modulus;
@@ -25,6 +26,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/onionpir_b200.h"
@@ -302,6 +304,105 @@ __global__ void __launch_bounds__(kBlock) k_client_pack(
   add_constants(consts + query * nconst, nconst, limb, o0, span, q, c0);
 }
 
+// One ciphertext row of the client's session keys (create_session_keys,
+// client.cpp:40-45), before the NTT: c0 = -(a s) + esign e + [half = 0] msg,
+// c1 = a + [half = 1] msg, msg = scale_k * m for a ternary polynomial m (s for
+// the RGSW rows, sigma_k(s) for the BV rows).
+struct KeyRow {
+  const uint64_t *a;  // K n, coefficient form, limb k below q_k
+  const int64_t *e;   // n
+  uint64_t *out;      // [c0 (K n)][c1 (K n)]
+  uint32_t msg;       // ternary message polynomial: 0 = s, 1 + i = sigma_{N/2^i + 1}(s)
+  uint32_t half;      // message in c0 (0) or c1 (1)
+  int32_t esign;      // +1: BV row (b = msg - a s + e), -1: encryption of zero
+  uint32_t pad;
+  uint64_t scale[2];  // message scale per limb, below q_k
+};
+
+__device__ __forceinline__ uint64_t signed_mod(int64_t v, uint64_t q) {
+  return v >= 0 ? static_cast<uint64_t>(v) % q : (q - static_cast<uint64_t>(-(v + 1)) % q - 1);
+}
+
+// Coefficient-form key rows, item = (row, limb) = blockIdx.x, output slice
+// blockIdx.y; index-list product with 31-bit parts.
+template <int R>
+__global__ void __launch_bounds__(kBlock) k_client_keyrows(
+    const KeyRow *__restrict__ rows, const int8_t *__restrict__ msgs,
+    const uint16_t *__restrict__ sidx, uint32_t npos, uint32_t nneg, uint32_t n, uint32_t limbs,
+    uint64_t q0, uint64_t q1) {
+  extern __shared__ __align__(16) int32_t smem[];
+  int32_t *ext = smem;
+  uint16_t *sl = reinterpret_cast<uint16_t *>(smem + 2 * 2 * n);
+  const KeyRow row = rows[blockIdx.x / limbs];
+  const uint32_t limb = blockIdx.x % limbs;
+  const uint64_t q = limb ? q1 : q0;
+  const uint64_t kn = static_cast<uint64_t>(limbs) * n;
+  const uint64_t *x = row.a + static_cast<uint64_t>(limb) * n;
+  stage_ext<2, 31>(x, q, n, ext);
+  for (uint32_t u = threadIdx.x; u < npos + nneg; u += blockDim.x) sl[u] = sidx[u];
+  __syncthreads();
+  const uint32_t i0 = blockIdx.y * (n / gridDim.y) + threadIdx.x;
+  int64_t acc[2][R];
+  list_product<2, R>(ext, sl, npos, nneg, n, i0, acc);
+  uint64_t *c0 = row.out + static_cast<uint64_t>(limb) * n;
+  uint64_t *c1 = c0 + kn;
+  const int8_t *m = msgs + static_cast<uint64_t>(row.msg) * n;
+  const uint64_t sc = row.scale[limb];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const uint32_t i = i0 + kBlock * r;
+    const uint64_t prod = reduce_parts<2, 31, R>(acc, r, q);
+    const uint64_t em = signed_mod(row.e[i], q);
+    const uint64_t term = m[i] == 1 ? sc : (m[i] == -1 && sc ? q - sc : 0);
+    uint64_t v = prod ? q - prod : 0;                        // -(a s)
+    if (row.esign > 0) {
+      v += em;
+      if (v >= q) v -= q;
+    } else {
+      v = v >= em ? v - em : v + (q - em);
+    }
+    uint64_t w = x[i] % q;
+    if (row.half == 0) {
+      v += term;
+      if (v >= q) v -= q;
+    } else {
+      w += term;
+      if (w >= q) w -= q;
+    }
+    c0[i] = v;
+    c1[i] = w;
+  }
+}
+
+// In-place forward negacyclic NTT of polynomial blockIdx.x (limb = index % K)
+// in the reference's convention: Cooley-Tukey from natural order, output in
+// bit-reversed order, twiddle at butterfly group m + i = root^BitRev(m + i)
+// (fw, per limb), every value canonical in [0, q).
+__global__ void __launch_bounds__(kBlock) k_client_ntt(uint64_t *__restrict__ polys, uint32_t n,
+                                                       uint32_t limbs, const uint64_t *__restrict__ fw,
+                                                       uint64_t q0, uint64_t q1) {
+  extern __shared__ __align__(16) uint64_t sp[];
+  const uint32_t limb = blockIdx.x % limbs;
+  const uint64_t q = limb ? q1 : q0;
+  const uint64_t *w = fw + static_cast<uint64_t>(limb) * n;
+  uint64_t *a = polys + static_cast<uint64_t>(blockIdx.x) * n;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sp[i] = a[i];
+  __syncthreads();
+  for (uint32_t m = 1, t = n >> 1; m < n; m <<= 1, t >>= 1) {
+    for (uint32_t b = threadIdx.x; b < n / 2; b += blockDim.x) {
+      const uint32_t g = b / t, j = b % t;
+      const uint32_t xi = 2 * g * t + j, yi = xi + t;
+      const uint64_t u = sp[xi];
+      const uint64_t v = static_cast<uint64_t>(static_cast<unsigned __int128>(sp[yi]) * w[m + g] % q);
+      const uint64_t s = u + v;
+      sp[xi] = s >= q ? s - q : s;
+      sp[yi] = u >= v ? u - v : u + (q - v);
+    }
+    __syncthreads();
+  }
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) a[i] = sp[i];
+}
+
 uint64_t bitrev(uint64_t x, uint32_t bits) {
   uint64_t r = 0;
   for (uint32_t i = 0; i < bits; ++i) r |= ((x >> i) & 1ull) << (bits - 1 - i);
@@ -323,6 +424,9 @@ struct opir_client {
   DevBuf<uint16_t> sidx;     // [P | M] secret index lists
   uint32_t npos = 0, nneg = 0;
   DevBuf<uint32_t> code;     // [kBlock]: s[jl + kBlock jh] 2 bits each (window product)
+  DevBuf<int8_t> msgs;       // [1 + h][n]: s, then sigma_{N/2^i + 1}(s) for i < h
+  DevBuf<uint64_t> fw;       // [K][n]: forward NTT twiddles per limb
+  DevBuf<KeyRow> keyrows;
   uint32_t nconst = 1;       // constant slots per query
   uint64_t one_val[2]{};     // the one-hot's value per limb
   std::vector<uint64_t> gadget_val;  // [k][limb]: B^(L_EP-1-k) (2^h)^-1 mod q_limb
@@ -557,6 +661,35 @@ void launch_pack(uint64_t items, cudaStream_t st, const uint64_t *a, const int64
   throw std::runtime_error("client pack: unsupported slice width");
 }
 
+void launch_keygen(const opir_client &c, const std::vector<KeyRow> &rows, uint64_t *bv,
+                   uint64_t bv_polys, uint64_t *gsw, uint64_t gsw_polys, cudaStream_t st) {
+  const uint32_t n = c.n;
+  const uint64_t items = rows.size() * c.limbs;
+  const uint32_t s = slices_for(items, n, c.sms);
+  const uint32_t Rl = n / (s * kBlock);
+  const dim3 grid(static_cast<uint32_t>(items), s);
+  const size_t smem = 2 * 2 * n * sizeof(int32_t) + (c.npos + c.nneg + 8) * sizeof(uint16_t);
+  bool done = false;
+#define OPIR_KEYROWS(RR)                                                                      \
+  if (!done && Rl == RR) {                                                                    \
+    set_smem(k_client_keyrows<RR>, smem, "client keygen smem");                               \
+    k_client_keyrows<RR><<<grid, kBlock, smem, st>>>(c.keyrows.p, c.msgs.p, c.sidx.p, c.npos, \
+                                                     c.nneg, n, c.limbs, c.mods[0],          \
+                                                     c.mods[1]);                              \
+    launched("client keygen launch");                                                         \
+    done = true;                                                                              \
+  }
+  OPIR_KEYROWS(1) OPIR_KEYROWS(2) OPIR_KEYROWS(4) OPIR_KEYROWS(8)
+#undef OPIR_KEYROWS
+  if (!done) throw std::runtime_error("client keygen: unsupported slice width");
+  for (const auto &part : {std::make_pair(bv, bv_polys), std::make_pair(gsw, gsw_polys)}) {
+    if (part.second == 0) continue;
+    k_client_ntt<<<static_cast<uint32_t>(part.second), kBlock, n * sizeof(uint64_t), st>>>(
+        part.first, n, c.limbs, c.fw.p, c.mods[0], c.mods[1]);
+    launched("client keygen NTT launch");
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -607,6 +740,37 @@ opir_status opir_client_create(const opir_params *params, const int8_t *secret, 
     c->code.alloc(kBlock);
     ck(cudaMemcpy(c->code.p, code.data(), kBlock * sizeof(uint32_t), cudaMemcpyHostToDevice),
        "secret code upload");
+    // key generation: s and its automorphisms sigma_k(s), k = N/2^i + 1
+    // (utils.cpp:58-72: coefficient j moves to j k mod 2N, negated past N)
+    const uint32_t h = c->params.expansion_height;
+    std::vector<int8_t> msgs(static_cast<size_t>(1 + h) * c->n, 0);
+    std::copy(secret, secret + c->n, msgs.begin());
+    for (uint32_t i = 0; i < h; ++i) {
+      const uint64_t k = (c->n >> i) + 1, two_n = 2ull * c->n;
+      int8_t *o = msgs.data() + static_cast<size_t>(1 + i) * c->n;
+      for (uint64_t j = 0; j < c->n; ++j) {
+        const uint64_t dest = j * k % two_n;
+        if (dest < c->n) o[dest] = secret[j];
+        else o[dest - c->n] = static_cast<int8_t>(-secret[j]);
+      }
+    }
+    c->msgs.alloc(msgs.size());
+    ck(cudaMemcpy(c->msgs.p, msgs.data(), msgs.size(), cudaMemcpyHostToDevice), "message upload");
+    // forward twiddles root^BitRev(k) per limb (the logical q's CRT root when K = 1)
+    uint32_t lg = 0;
+    while ((1u << lg) < c->n) ++lg;
+    std::vector<uint64_t> fw(static_cast<size_t>(c->limbs) * c->n);
+    for (uint32_t m = 0; m < c->limbs; ++m) {
+      const uint64_t q = c->mods[m];
+      const uint64_t root = c->limbs == 1 ? c->params.w_crt % q : (m == 0 ? c->params.w1 : c->params.w2);
+      std::vector<uint64_t> pw(c->n);
+      pw[0] = 1 % q;
+      for (uint32_t e = 1; e < c->n; ++e) pw[e] = mulmod(pw[e - 1], root, q);
+      for (uint32_t k = 0; k < c->n; ++k) fw[static_cast<size_t>(m) * c->n + k] = pw[bitrev(k, lg)];
+    }
+    c->fw.alloc(fw.size());
+    ck(cudaMemcpy(c->fw.p, fw.data(), fw.size() * sizeof(uint64_t), cudaMemcpyHostToDevice),
+       "twiddle upload");
   });
   if (st != OPIR_OK) {
     delete c;
@@ -625,6 +789,9 @@ void opir_client_destroy(opir_client *c) {
     cudaDeviceSynchronize();
     c->sidx.reset();
     c->code.reset();
+    c->msgs.reset();
+    c->fw.reset();
+    c->keyrows.reset();
     c->consts.reset();
     if (c->staging) cudaFreeHost(c->staging);
     if (c->staged) cudaEventDestroy(c->staged);
@@ -688,6 +855,51 @@ opir_status opir_client_decrypt_device(opir_client *c, uint32_t n, const uint64_
          "noise reset");
     launch_decrypt(n, st, d_responses, *c, d_plaintexts,
                    reinterpret_cast<unsigned long long *>(d_max_noise));
+  });
+}
+
+opir_status opir_client_keygen_device(opir_client *c, const uint64_t *d_bv_a,
+                                      const int64_t *d_bv_e, const uint64_t *d_gsw_a,
+                                      const int64_t *d_gsw_e, uint64_t *d_bv_keys,
+                                      uint64_t *d_gsw_key, void *stream) {
+  if (!c) return OPIR_ERR_INVALID_ARGUMENT;
+  return client_guarded(c, [&] {
+    const opir_params &p = c->params;
+    const uint32_t h = p.expansion_height, K = c->limbs, n = c->n;
+    if (h && (!d_bv_a || !d_bv_e || !d_bv_keys)) throw std::invalid_argument("null BV buffer");
+    if (!d_gsw_a || !d_gsw_e || !d_gsw_key) throw std::invalid_argument("null RGSW buffer");
+    const uint64_t kn = static_cast<uint64_t>(K) * n;
+    auto power = [&](uint32_t bits, uint32_t m) {  // 2^bits mod q_m
+      uint64_t v = 1 % c->mods[m];
+      for (uint32_t b = 0; b < bits; ++b) v = mulmod(v, 2, c->mods[m]);
+      return v;
+    };
+    std::vector<KeyRow> rows;
+    for (uint32_t i = 0; i < h; ++i)
+      for (uint32_t r = 0; r < p.l_ks; ++r) {
+        const uint64_t at = static_cast<uint64_t>(i) * p.l_ks + r;
+        KeyRow kr{d_bv_a + at * kn, d_bv_e + at * n, d_bv_keys + at * 2 * kn, 1 + i, 0, 1, 0, {0, 0}};
+        for (uint32_t m = 0; m < K; ++m) kr.scale[m] = power(r * p.base_log2_ks, m);
+        rows.push_back(kr);
+      }
+    for (uint32_t half = 0; half < 2; ++half)
+      for (uint32_t r = 0; r < p.l_key; ++r) {
+        const uint64_t at = static_cast<uint64_t>(half) * p.l_key + r;
+        KeyRow kr{d_gsw_a + at * kn, d_gsw_e + at * n, d_gsw_key + at * 2 * kn, 0, half, -1, 0, {0, 0}};
+        for (uint32_t m = 0; m < K; ++m) kr.scale[m] = power(p.base_log2_key * (p.l_key - 1 - r), m);
+        rows.push_back(kr);
+      }
+    DeviceGuard g(c->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (c->keyrows.n < rows.size()) {
+      ck(cudaStreamSynchronize(st), "client sync");
+      c->keyrows.alloc(rows.size());
+    }
+    ck(cudaMemcpyAsync(c->keyrows.p, rows.data(), rows.size() * sizeof(KeyRow),
+                       cudaMemcpyHostToDevice, st),
+       "key row upload");
+    launch_keygen(*c, rows, d_bv_keys, static_cast<uint64_t>(h) * p.l_ks * 2 * K, d_gsw_key,
+                  2ull * p.l_key * 2 * K, st);
   });
 }
 

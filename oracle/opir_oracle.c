@@ -334,8 +334,10 @@ static void encrypt_zero(const opir_oracle_params *p, const uint64_t *sk, mt64 *
 }
 
 /* bv_keyswitch.cpp:191-259 */
+/* cap_a / cap_e (may be NULL): each row's uniform a (coefficient form, N)
+ * and signed Gaussian e (N), in generation order. */
 static void gen_bv_key(const opir_oracle_params *p, const uint64_t *sk, uint32_t galois_k,
-                       mt64 *g, uint64_t *rows) {
+                       mt64 *g, uint64_t *rows, uint64_t *cap_a, int64_t *cap_e) {
   const uint32_t N = p->N; const uint64_t q = p->q;
   barrett_t b = barrett_make(q);
   uint64_t *sig = malloc(N * sizeof *sig), *tmp = malloc(N * sizeof *tmp);
@@ -351,6 +353,10 @@ static void gen_bv_key(const opir_oracle_params *p, const uint64_t *sk, uint32_t
     uint64_t *rb = rows + (size_t)i * 2 * N, *ra = rb + N;
     sample_uniform(ra, N, q, g);
     sample_gaussian(e, N, q, SIGMA, g);
+    if (cap_a) memcpy(cap_a + (size_t)i * N, ra, N * sizeof *ra);
+    if (cap_e)
+      for (uint32_t j = 0; j < N; ++j)
+        cap_e[(size_t)i * N + j] = e[j] > q / 2 ? -(int64_t)(q - e[j]) : (int64_t)e[j];
     ntt_q(p, ra);
     ntt_q(p, e);
     for (uint32_t j = 0; j < N; ++j)
@@ -367,14 +373,17 @@ static void gadget(uint32_t l, uint32_t base, uint64_t q, uint64_t *out) {
 
 /* gsw.cpp:359-422 (K = 1) */
 static void plain_to_gsw(const opir_oracle_params *p, const uint64_t *pt, const uint64_t *sk,
-                         uint32_t l, uint32_t base, mt64 *g, uint64_t *out) {
+                         uint32_t l, uint32_t base, mt64 *g, uint64_t *out, uint64_t *cap_a,
+                         int64_t *cap_e) {
   const uint32_t N = p->N; const uint64_t q = p->q;
   uint64_t gd[64];
   gadget(l, base, q, gd);
   for (uint32_t half = 0; half < 2; ++half)
     for (uint32_t r = 0; r < l; ++r) {
       uint64_t *row = out + (size_t)(half * l + r) * 2 * N;
-      encrypt_zero(p, sk, g, row);
+      const size_t at = (size_t)(half * l + r) * N;
+      encrypt_zero_a(p, sk, g, NULL, row, cap_e ? cap_e + at : NULL);
+      if (cap_a) memcpy(cap_a + at, row + N, N * sizeof *row);
       uint64_t *tgt = row + (size_t)half * N;
       for (uint32_t c = 0; c < N; ++c) {
         uint64_t val = (uint64_t)((u128)(pt[c] % q) * gd[r] % q);
@@ -385,7 +394,8 @@ static void plain_to_gsw(const opir_oracle_params *p, const uint64_t *pt, const 
     }
 }
 
-oracle_client *oracle_client_new(const opir_oracle_params *p, uint64_t seed) {
+static oracle_client *client_new(const opir_oracle_params *p, uint64_t seed, uint64_t *bv_a,
+                                 int64_t *bv_e, uint64_t *gsw_a, int64_t *gsw_e) {
   const uint32_t N = p->N; const uint64_t q = p->q;
   oracle_client *c = calloc(1, sizeof *c);
   c->p = *p;
@@ -397,14 +407,24 @@ oracle_client *oracle_client_new(const opir_oracle_params *p, uint64_t seed) {
   const uint32_t h = p->expansion_height;
   c->bv = malloc((size_t)(h ? h : 1) * p->l_ks * 2 * N * sizeof *c->bv);
   for (uint32_t i = 0; i < h; ++i)              /* bv_keyswitch.cpp:270-274 */
-    gen_bv_key(p, c->sk, (N >> i) + 1, &gbv, c->bv + (size_t)i * p->l_ks * 2 * N);
+    gen_bv_key(p, c->sk, (N >> i) + 1, &gbv, c->bv + (size_t)i * p->l_ks * 2 * N,
+               bv_a ? bv_a + (size_t)i * p->l_ks * N : NULL,
+               bv_e ? bv_e + (size_t)i * p->l_ks * N : NULL);
   uint64_t *skc = malloc(N * sizeof *skc);
   memcpy(skc, c->sk, N * sizeof *skc);
   intt_q(p, skc);                               /* client.cpp:25-38 */
   c->gsw = malloc((size_t)2 * p->l_key * 2 * N * sizeof *c->gsw);
-  plain_to_gsw(p, skc, c->sk, p->l_key, p->base_key, &c->rng, c->gsw);
+  plain_to_gsw(p, skc, c->sk, p->l_key, p->base_key, &c->rng, c->gsw, gsw_a, gsw_e);
   free(skc);
   return c;
+}
+oracle_client *oracle_client_new(const opir_oracle_params *p, uint64_t seed) {
+  return client_new(p, seed, NULL, NULL, NULL, NULL);
+}
+oracle_client *oracle_client_new_keygen_parts(const opir_oracle_params *p, uint64_t seed,
+                                              uint64_t *bv_a, int64_t *bv_e, uint64_t *gsw_a,
+                                              int64_t *gsw_e) {
+  return client_new(p, seed, bv_a, bv_e, gsw_a, gsw_e);
 }
 void oracle_client_free(oracle_client *c) {
   if (!c) return;

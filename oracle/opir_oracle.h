@@ -69,6 +69,13 @@ void oracle_db_plaintext(uint64_t seed, uint64_t pt, const opir_oracle_params *p
 
 typedef struct oracle_client oracle_client;
 oracle_client *oracle_client_new(const opir_oracle_params *p, uint64_t seed);
+/* The same client, also returning the randomness its key generation drew,
+ * in generation order: bv_a (h x L_KS x N, coefficient form) and bv_e
+ * (h x L_KS x N, signed) for the BV keys, gsw_a / gsw_e (2 L_KEY x N) for
+ * the RGSW rows (create_session_keys, client.cpp:40-45). */
+oracle_client *oracle_client_new_keygen_parts(const opir_oracle_params *p, uint64_t seed,
+                                              uint64_t *bv_a, int64_t *bv_e, uint64_t *gsw_a,
+                                              int64_t *gsw_e);
 void oracle_client_free(oracle_client *c);
 void oracle_client_bv_keys(const oracle_client *c, uint64_t *out);
 void oracle_client_gsw_key(const oracle_client *c, uint64_t *out);
@@ -152,6 +159,11 @@ void oracle_c4_db_plaintext(uint64_t seed, uint64_t pt,
 
 typedef struct oracle_c4_client oracle_c4_client;
 oracle_c4_client *oracle_c4_client_new(const opir_oracle_c4_params *p, uint64_t seed);
+/* Two-limb form: bv_a h x L_KS x 2N, gsw_a 2 L_KEY x 2N (limb-major), the
+ * errors N each (shared by the limbs). */
+oracle_c4_client *oracle_c4_client_new_keygen_parts(const opir_oracle_c4_params *p, uint64_t seed,
+                                                    uint64_t *bv_a, int64_t *bv_e,
+                                                    uint64_t *gsw_a, int64_t *gsw_e);
 void oracle_c4_client_free(oracle_c4_client *c);
 void oracle_c4_client_bv_keys(const oracle_c4_client *c, uint64_t *out);
 void oracle_c4_client_gsw_key(const oracle_c4_client *c, uint64_t *out);

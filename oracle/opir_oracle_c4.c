@@ -112,7 +112,7 @@ static void encrypt_zero_c4(const opir_oracle_c4_params *p, const uint64_t *sk, 
  * row i encrypts sigma_k(s) 2^(i base) under both limbs with per-limb
  * uniform a and one shared Gaussian e (bv_keyswitch.cpp:166-186). */
 static void gen_bv_key_c4(const opir_oracle_c4_params *p, const uint64_t *sk, uint32_t galois_k,
-                          mt64 *g, uint64_t *rows) {
+                          mt64 *g, uint64_t *rows, uint64_t *cap_a, int64_t *cap_e) {
   const uint32_t N = p->N;
   const size_t KN = 2 * (size_t)N;
   uint64_t *sig = malloc(KN * 8), *tmp = malloc(N * 8), *msg = malloc(KN * 8);
@@ -135,6 +135,8 @@ static void gen_bv_key_c4(const opir_oracle_c4_params *p, const uint64_t *sk, ui
     for (uint32_t k = 0; k < 2; ++k) sample_uniform(ra + (size_t)k * N, N, p->q[k], g);
     normal_t nd = {0.0, 0, SIGMA_C4};
     for (uint32_t j = 0; j < N; ++j) e[j] = llround(normal_next(&nd, g));
+    if (cap_a) memcpy(cap_a + (size_t)i * KN, ra, KN * sizeof *ra);
+    if (cap_e) memcpy(cap_e + (size_t)i * N, e, N * sizeof *e);
     for (uint32_t k = 0; k < 2; ++k) {
       const uint64_t q = p->q[k];
       barrett_t b = barrett_make(q);
@@ -158,7 +160,8 @@ static void gadget_c4(uint32_t l, uint32_t base, uint64_t q, uint64_t *out) {
 /* gsw.cpp:359-422 (K = 2): the plaintext arrives mod q0 and is
  * re-canonicalised per limb (a value above q0/2 is negative). */
 static void plain_to_gsw_c4(const opir_oracle_c4_params *p, const uint64_t *pt, const uint64_t *sk,
-                            uint32_t l, uint32_t base, mt64 *g, uint64_t *out) {
+                            uint32_t l, uint32_t base, mt64 *g, uint64_t *out, uint64_t *cap_a,
+                            int64_t *cap_e) {
   const uint32_t N = p->N;
   const size_t KN = 2 * (size_t)N;
   uint64_t gd[2][64];
@@ -167,7 +170,8 @@ static void plain_to_gsw_c4(const opir_oracle_c4_params *p, const uint64_t *pt, 
   for (uint32_t half = 0; half < 2; ++half)
     for (uint32_t r = 0; r < l; ++r) {
       uint64_t *row = out + (size_t)(half * l + r) * 2 * KN;
-      encrypt_zero_c4(p, sk, g, row);
+      encrypt_zero_c4_a(p, sk, g, NULL, row, cap_e ? cap_e + (size_t)(half * l + r) * N : NULL);
+      if (cap_a) memcpy(cap_a + (size_t)(half * l + r) * KN, row + KN, KN * sizeof *row);
       for (uint32_t k = 0; k < 2; ++k) {
         const uint64_t qk = p->q[k];
         uint64_t *tgt = row + (size_t)half * KN + (size_t)k * N;
@@ -189,7 +193,9 @@ static void plain_to_gsw_c4(const opir_oracle_c4_params *p, const uint64_t *pt, 
 /* client.cpp:20-38 with the driver's seeding: rng(seed) for s (rlwe.cpp:
  * 177-228, one ternary draw shared by both limbs), RGSW(s) and queries;
  * rng(seed ^ salt) for the BV keys. */
-oracle_c4_client *oracle_c4_client_new(const opir_oracle_c4_params *p, uint64_t seed) {
+static oracle_c4_client *c4_client_new(const opir_oracle_c4_params *p, uint64_t seed,
+                                       uint64_t *bv_a, int64_t *bv_e, uint64_t *gsw_a,
+                                       int64_t *gsw_e) {
   const uint32_t N = p->N;
   oracle_c4_client *c = calloc(1, sizeof *c);
   c->p = *p;
@@ -206,14 +212,24 @@ oracle_c4_client *oracle_c4_client_new(const opir_oracle_c4_params *p, uint64_t 
   const size_t key_words = (size_t)p->l_ks * 2 * 2 * N;
   c->bv = malloc((h ? h : 1) * key_words * sizeof *c->bv);
   for (uint32_t i = 0; i < h; ++i)
-    gen_bv_key_c4(p, c->sk, (N >> i) + 1, &gbv, c->bv + (size_t)i * key_words);
+    gen_bv_key_c4(p, c->sk, (N >> i) + 1, &gbv, c->bv + (size_t)i * key_words,
+                  bv_a ? bv_a + (size_t)i * p->l_ks * 2 * N : NULL,
+                  bv_e ? bv_e + (size_t)i * p->l_ks * N : NULL);
   uint64_t *skc = malloc(N * sizeof *skc);
   memcpy(skc, c->sk, N * sizeof *skc);
   intt_k(p, 0, skc);
   c->gsw = malloc((size_t)2 * p->l_key * 2 * 2 * N * sizeof *c->gsw);
-  plain_to_gsw_c4(p, skc, c->sk, p->l_key, p->base_key, &c->rng, c->gsw);
+  plain_to_gsw_c4(p, skc, c->sk, p->l_key, p->base_key, &c->rng, c->gsw, gsw_a, gsw_e);
   free(skc);
   return c;
+}
+oracle_c4_client *oracle_c4_client_new(const opir_oracle_c4_params *p, uint64_t seed) {
+  return c4_client_new(p, seed, NULL, NULL, NULL, NULL);
+}
+oracle_c4_client *oracle_c4_client_new_keygen_parts(const opir_oracle_c4_params *p, uint64_t seed,
+                                                    uint64_t *bv_a, int64_t *bv_e,
+                                                    uint64_t *gsw_a, int64_t *gsw_e) {
+  return c4_client_new(p, seed, bv_a, bv_e, gsw_a, gsw_e);
 }
 void oracle_c4_client_free(oracle_c4_client *c) {
   if (!c) return;

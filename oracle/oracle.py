@@ -82,6 +82,10 @@ def lib():
         L.oracle_params_init.argtypes = [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(Params)]
         L.oracle_client_new.argtypes = [C.POINTER(Params), C.c_uint64]
         L.oracle_client_new.restype = C.c_void_p
+        L.oracle_client_new_keygen_parts.argtypes = [C.POINTER(Params), C.c_uint64, _u64p,
+                                                     C.POINTER(C.c_int64), _u64p,
+                                                     C.POINTER(C.c_int64)]
+        L.oracle_client_new_keygen_parts.restype = C.c_void_p
         L.oracle_client_free.argtypes = [C.c_void_p]
         L.oracle_client_bv_keys.argtypes = [C.c_void_p, _u64p]
         L.oracle_client_gsw_key.argtypes = [C.c_void_p, _u64p]
@@ -138,6 +142,10 @@ def lib():
         L.oracle_c4_db_plaintext.argtypes = [C.c_uint64, C.c_uint64, P4, _u64p]
         L.oracle_c4_client_new.argtypes = [P4, C.c_uint64]
         L.oracle_c4_client_new.restype = C.c_void_p
+        L.oracle_c4_client_new_keygen_parts.argtypes = [C.POINTER(C4Params), C.c_uint64, _u64p,
+                                                        C.POINTER(C.c_int64), _u64p,
+                                                        C.POINTER(C.c_int64)]
+        L.oracle_c4_client_new_keygen_parts.restype = C.c_void_p
         L.oracle_c4_client_free.argtypes = [C.c_void_p]
         L.oracle_c4_client_bv_keys.argtypes = [C.c_void_p, _u64p]
         L.oracle_c4_client_gsw_key.argtypes = [C.c_void_p, _u64p]
@@ -189,9 +197,24 @@ def db_plaintext(seed: int, pt: int, p: Params) -> np.ndarray:
 class Client:
     """Seeded client: the reference client with seeded generators."""
 
-    def __init__(self, p: Params, seed: int):
+    def __init__(self, p: Params, seed: int, keygen_parts: bool = False):
+        """keygen_parts keeps the randomness key generation drew in
+        self.keygen: bv_a / bv_e (h, L_KS, N), gsw_a / gsw_e (2 L_KEY, N)."""
         self.p = p
-        self.h = lib().oracle_client_new(C.byref(p), seed)
+        if keygen_parts:
+            h = max(p.expansion_height, 0)
+            k = {"bv_a": np.zeros((h, p.l_ks, p.N), np.uint64),
+                 "bv_e": np.zeros((h, p.l_ks, p.N), np.int64),
+                 "gsw_a": np.zeros((2 * p.l_key, p.N), np.uint64),
+                 "gsw_e": np.zeros((2 * p.l_key, p.N), np.int64)}
+            bv_a = k["bv_a"] if h else np.zeros(1, np.uint64)
+            bv_e = k["bv_e"] if h else np.zeros(1, np.int64)
+            self.h = lib().oracle_client_new_keygen_parts(
+                C.byref(p), seed, ptr(bv_a), ptr(bv_e, C.c_int64), ptr(k["gsw_a"]),
+                ptr(k["gsw_e"], C.c_int64))
+            self.keygen = k
+        else:
+            self.h = lib().oracle_client_new(C.byref(p), seed)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -361,9 +384,25 @@ class C4Client:
     """Seeded two-limb client: the reference client (K = 2) with seeded generators.
     Ciphertexts are (2, 2, N): poly x limb x coefficient."""
 
-    def __init__(self, p: C4Params, seed: int):
+    def __init__(self, p: C4Params, seed: int, keygen_parts: bool = False):
+        """keygen_parts keeps the key-generation randomness in self.keygen:
+        bv_a (h, L_KS, 2, N), bv_e (h, L_KS, N), gsw_a (2 L_KEY, 2, N),
+        gsw_e (2 L_KEY, N)."""
         self.p = p
-        self.h = lib().oracle_c4_client_new(C.byref(p), seed)
+        if keygen_parts:
+            h = max(p.expansion_height, 0)
+            k = {"bv_a": np.zeros((h, p.l_ks, 2, p.N), np.uint64),
+                 "bv_e": np.zeros((h, p.l_ks, p.N), np.int64),
+                 "gsw_a": np.zeros((2 * p.l_key, 2, p.N), np.uint64),
+                 "gsw_e": np.zeros((2 * p.l_key, p.N), np.int64)}
+            bv_a = k["bv_a"] if h else np.zeros(1, np.uint64)
+            bv_e = k["bv_e"] if h else np.zeros(1, np.int64)
+            self.h = lib().oracle_c4_client_new_keygen_parts(
+                C.byref(p), seed, ptr(bv_a), ptr(bv_e, C.c_int64), ptr(k["gsw_a"]),
+                ptr(k["gsw_e"], C.c_int64))
+            self.keygen = k
+        else:
+            self.h = lib().oracle_c4_client_new(C.byref(p), seed)
 
     def __del__(self):
         if getattr(self, "h", None):

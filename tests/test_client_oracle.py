@@ -80,3 +80,71 @@ def test_create_rejects_bad_arguments_before_any_device_call():
     shaped = PirParams().with_query_shape(8, 2, 7)
     with pytest.raises(ValueError):
         PirClient(shaped, np.zeros(p.N, np.int8))
+
+
+def _ntt(poly, q, root):
+    a = np.ascontiguousarray(np.array([int(v) % q for v in poly], dtype=np.uint64))
+    O.lib().oracle_ntt_fwd(O.ptr(a), a.size, q, root)
+    return a
+
+
+def _sigma(s, k):
+    N = s.size
+    out = np.zeros(N, np.int8)
+    for j in range(N):
+        d = (j * k) % (2 * N)
+        if d < N:
+            out[d] = s[j]
+        else:
+            out[d - N] = -s[j]
+    return out
+
+
+def _row(a, e, s, msg, scale, half, esign, q):
+    """(c0, c1) coefficient form: c0 = -(a s) + esign e + [half=0] scale msg,
+    c1 = a + [half=1] scale msg (mod q)."""
+    prod = negacyclic_ternary(a, s, q)
+    m = [scale * int(x) for x in msg]
+    c0 = [(-int(prod[i]) + esign * int(e[i]) + (m[i] if half == 0 else 0)) % q
+          for i in range(a.size)]
+    c1 = [(int(a[i]) + (m[i] if half == 1 else 0)) % q for i in range(a.size)]
+    return c0, c1
+
+
+@pytest.mark.parametrize("config", ["k1", "c4"])
+def test_keygen_randomness_reproduces_the_keys(config):
+    """The session keys are, row by row, coefficient-form ciphertexts built
+    from the captured (a, e) and then NTT'd per limb -- the computation the
+    GPU key generation performs (sampled rows)."""
+    if config == "k1":
+        p = O.params(16384, 9)
+        cl = O.Client(p, 12, keygen_parts=True)
+        mods, roots = [int(p.q)], [int(p.w_crt)]
+        base_ks, base_key = p.base_ks, p.base_key
+    else:
+        p = O.c4_params(16384, 9)
+        cl = O.C4Client(p, 12, keygen_parts=True)
+        mods, roots = [int(x) for x in p.q[:2]], [int(x) for x in p.w[:2]]
+        base_ks, base_key = p.base_ks, p.base_key
+    s = cl.secret()
+    kg = cl.keygen
+    bv, gsw = cl.bv_keys(), cl.gsw_key()
+    h, N = p.expansion_height, p.N
+    for i in (0, h - 1):
+        sig = _sigma(s, (N >> i) + 1)
+        for r in (0, p.l_ks - 1):
+            for k, (q, root) in enumerate(zip(mods, roots)):
+                a = kg["bv_a"][i, r] if config == "k1" else kg["bv_a"][i, r, k]
+                c0, c1 = _row(a, kg["bv_e"][i, r], s, sig, pow(2, r * base_ks, q), 0, 1, q)
+                got = bv[i, r] if config == "k1" else bv[i, r, :, k]
+                assert np.array_equal(_ntt(c0, q, root), got[0])
+                assert np.array_equal(_ntt(c1, q, root), got[1])
+    for row in (0, p.l_key - 1, p.l_key, 2 * p.l_key - 1):
+        half, r = divmod(row, p.l_key)
+        for k, (q, root) in enumerate(zip(mods, roots)):
+            a = kg["gsw_a"][row] if config == "k1" else kg["gsw_a"][row, k]
+            scale = pow(2, base_key * (p.l_key - 1 - r), q)
+            c0, c1 = _row(a, kg["gsw_e"][row], s, s, scale, half, -1, q)
+            got = gsw[row] if config == "k1" else gsw[row, :, k]
+            assert np.array_equal(_ntt(c0, q, root), got[0])
+            assert np.array_equal(_ntt(c1, q, root), got[1])

@@ -150,3 +150,30 @@ def test_out_of_range_index():
         gc.fast_generate_query_batch([op.num_pt], a, e)
     # the handle stays usable
     assert gc.fast_generate_query_batch([0], a, e).shape == (1, 2, op.N)
+
+
+@pytest.mark.parametrize("config,target,h", [("k1", 16384, 9), ("k1", 43690, 10),
+                                             ("c4", 16384, 9)])
+def test_session_keys_match_oracle(config, target, h):
+    """create_session_keys on the GPU from the randomness the oracle client's
+    key generation drew equals its BV and RGSW keys bit for bit, and the
+    GPU server answers with them like with the oracle's keys."""
+    if config == "k1":
+        gp, op = PirParams(target, h), O.params(target, h)
+        cl = O.Client(op, 61, keygen_parts=True)
+    else:
+        gp, op = PirParams(target, h, config=C4), O.c4_params(target, h)
+        cl = O.C4Client(op, 61, keygen_parts=True)
+    kg = cl.keygen
+    gc = PirClient(gp, cl.secret())
+    bv, gsw = gc.create_session_keys(kg["bv_a"], kg["bv_e"], kg["gsw_a"], kg["gsw_e"])
+    assert np.array_equal(bv, cl.bv_keys())
+    assert np.array_equal(gsw, cl.gsw_key())
+    idx = 1234
+    srv = PirServer(gp)
+    srv.load_data_seeded(target, 3)
+    srv.set_client_keys(1, bv, gsw)
+    resp = srv.make_query(1, cl.query(idx))
+    want = (O.db_plaintext(3, idx, op).astype(np.uint64) if config == "k1"
+            else O.c4_db_plaintext(3, idx, op))
+    assert np.array_equal(gc.decrypt_mod_q(resp), want)
