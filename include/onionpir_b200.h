@@ -196,6 +196,24 @@ opir_status opir_server_set_client_keys(opir_server *server, uint64_t client_id,
                                         const uint32_t *galois_ks,
                                         uint32_t n_keys,
                                         const uint64_t *gsw_key);
+/* Representation of the key rows handed to opir_server_set_client_keys_ex. */
+typedef enum {
+  OPIR_KEYS_NTT = 0,   /* this library's NTT domain (the Conventions above) */
+  OPIR_KEYS_COEFF = 1  /* coefficient form */
+} opir_key_form;
+
+/* opir_server_set_client_keys with the rows' representation named. Key rows
+ * made by a producer with another NTT convention (a client built on Intel
+ * HEXL, whose NTT-domain order is its own) are handed over in coefficient
+ * form -- the producer's own inverse NTT of each row, which no convention
+ * affects -- as OPIR_KEYS_COEFF; the server takes every polynomial into its
+ * NTT domain on the GPU and installs the keys as opir_server_set_client_keys
+ * does. Same layouts, limbs and errors; a coefficient at or above its
+ * limb's modulus is OPIR_ERR_INVALID_ARGUMENT. */
+opir_status opir_server_set_client_keys_ex(opir_server *server, uint64_t client_id,
+                                           const uint64_t *bv_keys,
+                                           const uint32_t *galois_ks, uint32_t n_keys,
+                                           const uint64_t *gsw_key, uint32_t key_form);
 opir_status opir_server_remove_client(opir_server *server, uint64_t client_id);
 
 /* ---- query processing ----------------------------------------------------- */

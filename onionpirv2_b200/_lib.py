@@ -97,6 +97,8 @@ _SIGS = {
     "opir_server_load_db_source": ([C.c_void_p, C.c_uint64, SOURCE_CB, C.c_void_p], C.c_int),
     "opir_server_load_db_seeded": ([C.c_void_p, C.c_uint64, C.c_uint64], C.c_int),
     "opir_server_set_client_keys": ([C.c_void_p, C.c_uint64, u64p, u32p, C.c_uint32, u64p], C.c_int),
+    "opir_server_set_client_keys_ex": ([C.c_void_p, C.c_uint64, u64p, u32p, C.c_uint32, u64p,
+                                        C.c_uint32], C.c_int),
     "opir_server_remove_client": ([C.c_void_p, C.c_uint64], C.c_int),
     "opir_server_make_query": ([C.c_void_p, C.c_uint64, u64p, u64p], C.c_int),
     "opir_server_make_query_batch": ([C.c_void_p, C.c_uint32, u64p, u64p, u64p], C.c_int),

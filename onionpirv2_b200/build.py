@@ -20,7 +20,7 @@ SOURCES = ["opir_kernels.cu", "opir_server.cu", "opir_params.cpp", "opir_noalloc
            "opir_shard.cpp", "opir_codec.cpp", "opir_codec_abi.cpp", "opir_client.cu"]
 HEADERS = ["opir_device.cuh", "opir_kernels.h", "opir_params.h", "opir_scan_tc.h", "opir_ntt.cuh",
            "opir_host.h", "opir_c4_device.cuh", "opir_c4_kernels.h", "opir_c4_server.h", "opir_tc.cuh", "opir_tree.h",
-           "opir_shard.h", "opir_codec.h"]
+           "opir_shard.h", "opir_codec.h", "opir_client.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
                      "--expt-relaxed-constexpr"]

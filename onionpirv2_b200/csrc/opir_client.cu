@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "../../include/onionpir_b200.h"
+#include "opir_client.h"
 #include "opir_host.h"
 #include "opir_kernels.h"
 #include "opir_params.h"
@@ -692,6 +693,41 @@ void launch_keygen(const opir_client &c, const std::vector<KeyRow> &rows, uint64
 
 }  // namespace
 
+namespace opir {
+
+std::vector<uint64_t> forward_twiddles(const opir_params &p) {
+  const uint32_t n = p.poly_degree, limbs = p.num_limbs;
+  uint32_t lg = 0;
+  while ((1u << lg) < n) ++lg;
+  std::vector<uint64_t> fw(static_cast<size_t>(limbs) * n);
+  for (uint32_t m = 0; m < limbs; ++m) {
+    const uint64_t q = limbs == 1 ? p.q : (m == 0 ? p.q1 : p.q2);
+    const uint64_t root = limbs == 1 ? p.w_crt % q : (m == 0 ? p.w1 : p.w2);
+    std::vector<uint64_t> pw(n);
+    pw[0] = 1 % q;
+    for (uint32_t e = 1; e < n; ++e) pw[e] = mulmod(pw[e - 1], root, q);
+    for (uint32_t k = 0; k < n; ++k) fw[static_cast<size_t>(m) * n + k] = pw[bitrev(k, lg)];
+  }
+  return fw;
+}
+
+void forward_ntt_polys(uint64_t *d_polys, uint64_t count, const opir_params &p,
+                       const uint64_t *d_fw, cudaStream_t st) {
+  if (count == 0) return;
+  const uint32_t n = p.poly_degree, limbs = p.num_limbs;
+  const uint64_t q0 = limbs == 1 ? p.q : p.q1, q1 = limbs == 1 ? 0 : p.q2;
+  for (uint64_t done = 0; done < count;) {
+    const uint32_t chunk = static_cast<uint32_t>(std::min<uint64_t>(count - done, 1u << 30));
+    // chunks keep the limb of polynomial i at i % limbs (chunk sizes are multiples of limbs)
+    k_client_ntt<<<chunk, kBlock, n * sizeof(uint64_t), st>>>(d_polys + done * n, n, limbs, d_fw,
+                                                            q0, q1);
+    launched("NTT launch");
+    done += chunk;
+  }
+}
+
+}  // namespace opir
+
 extern "C" {
 
 opir_status opir_client_create(const opir_params *params, const int8_t *secret, int device,
@@ -756,18 +792,7 @@ opir_status opir_client_create(const opir_params *params, const int8_t *secret, 
     }
     c->msgs.alloc(msgs.size());
     ck(cudaMemcpy(c->msgs.p, msgs.data(), msgs.size(), cudaMemcpyHostToDevice), "message upload");
-    // forward twiddles root^BitRev(k) per limb (the logical q's CRT root when K = 1)
-    uint32_t lg = 0;
-    while ((1u << lg) < c->n) ++lg;
-    std::vector<uint64_t> fw(static_cast<size_t>(c->limbs) * c->n);
-    for (uint32_t m = 0; m < c->limbs; ++m) {
-      const uint64_t q = c->mods[m];
-      const uint64_t root = c->limbs == 1 ? c->params.w_crt % q : (m == 0 ? c->params.w1 : c->params.w2);
-      std::vector<uint64_t> pw(c->n);
-      pw[0] = 1 % q;
-      for (uint32_t e = 1; e < c->n; ++e) pw[e] = mulmod(pw[e - 1], root, q);
-      for (uint32_t k = 0; k < c->n; ++k) fw[static_cast<size_t>(m) * c->n + k] = pw[bitrev(k, lg)];
-    }
+    const std::vector<uint64_t> fw = opir::forward_twiddles(c->params);
     c->fw.alloc(fw.size());
     ck(cudaMemcpy(c->fw.p, fw.data(), fw.size() * sizeof(uint64_t), cudaMemcpyHostToDevice),
        "twiddle upload");

@@ -20,6 +20,7 @@
 
 #include "../../include/onionpir_b200.h"
 #include "opir_c4_server.h"
+#include "opir_client.h"
 #include "opir_host.h"
 #include "opir_kernels.h"
 #include "opir_params.h"
@@ -1039,6 +1040,51 @@ opir_status opir_server_set_client_keys(opir_server *s, uint64_t client_id,
     std::swap(slot.bv.p, k.bv.p); std::swap(slot.bv.n, k.bv.n);
     std::swap(slot.gsw.p, k.gsw.p); std::swap(slot.gsw.n, k.gsw.n);
   });
+}
+
+opir_status opir_server_set_client_keys_ex(opir_server *s, uint64_t client_id,
+                                           const uint64_t *bv_keys, const uint32_t *galois_ks,
+                                           uint32_t n_keys, const uint64_t *gsw_key,
+                                           uint32_t key_form) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  if (key_form == OPIR_KEYS_NTT)
+    return opir_server_set_client_keys(s, client_id, bv_keys, galois_ks, n_keys, gsw_key);
+  std::vector<uint64_t> bv, gsw;
+  const opir_status st = guarded(s, [&] {
+    if (key_form != OPIR_KEYS_COEFF) throw std::invalid_argument("unknown key form");
+    if (!gsw_key) throw std::invalid_argument("PirServer session key bundle cannot be null");
+    if (n_keys && (!bv_keys || !galois_ks)) throw std::invalid_argument("null BV key arrays");
+    const opir_params &p = s->params;
+    const uint32_t n = p.poly_degree, K = p.num_limbs;
+    const uint64_t mods[2] = {K == 1 ? p.q : p.q1, K == 1 ? 0 : p.q2};
+    const size_t key_words = static_cast<size_t>(p.l_ks) * 2 * K * n;
+    const size_t gsw_words = static_cast<size_t>(2) * p.l_key * 2 * K * n;
+    bv.assign(bv_keys, bv_keys + n_keys * key_words);
+    gsw.assign(gsw_key, gsw_key + gsw_words);
+    for (const std::vector<uint64_t> *v : {&bv, &gsw})
+      for (size_t i = 0; i < v->size(); ++i)
+        if ((*v)[i] >= mods[(i / n) % K]) throw std::invalid_argument("key value not reduced mod its limb");
+    // coefficient form -> this library's NTT domain, on the device
+    DeviceGuard g(s->device);
+    const std::vector<uint64_t> fw = opir::forward_twiddles(p);
+    DevBuf<uint64_t> d_fw, d;
+    d_fw.alloc(fw.size());
+    d.alloc(bv.size() + gsw.size());
+    ck(cudaMemcpyAsync(d_fw.p, fw.data(), fw.size() * 8, cudaMemcpyHostToDevice, s->stream), "twiddle upload");
+    if (!bv.empty())
+      ck(cudaMemcpyAsync(d.p, bv.data(), bv.size() * 8, cudaMemcpyHostToDevice, s->stream), "bv upload");
+    ck(cudaMemcpyAsync(d.p + bv.size(), gsw.data(), gsw.size() * 8, cudaMemcpyHostToDevice, s->stream),
+       "gsw upload");
+    opir::forward_ntt_polys(d.p, (bv.size() + gsw.size()) / n, p, d_fw.p, s->stream);
+    if (!bv.empty())
+      ck(cudaMemcpyAsync(bv.data(), d.p, bv.size() * 8, cudaMemcpyDeviceToHost, s->stream), "bv download");
+    ck(cudaMemcpyAsync(gsw.data(), d.p + bv.size(), gsw.size() * 8, cudaMemcpyDeviceToHost, s->stream),
+       "gsw download");
+    ck(cudaStreamSynchronize(s->stream), "key NTT");
+  });
+  if (st != OPIR_OK) return st;
+  return opir_server_set_client_keys(s, client_id, bv.empty() ? nullptr : bv.data(), galois_ks,
+                                     n_keys, gsw.data());
 }
 
 opir_status opir_server_remove_client(opir_server *s, uint64_t client_id) {

@@ -214,9 +214,13 @@ class PirServer:
 
     # ---- keys
     def set_client_keys(self, client_id: int, bv_keys: np.ndarray, gsw_key: np.ndarray,
-                        galois_ks: Iterable[int] | None = None):
+                        galois_ks: Iterable[int] | None = None, key_form: str = "ntt"):
         """set_client_bv_galois_key + set_client_gsw_key. bv_keys: (n_keys, L_KS,
-        2, N) NTT form [b, a]; galois_ks defaults to (N >> i) + 1."""
+        2, N) NTT form [b, a]; galois_ks defaults to (N >> i) + 1. key_form
+        "coeff": every row polynomial in coefficient form instead (keys from a
+        producer with another NTT convention); the server NTTs them itself."""
+        if key_form not in ("ntt", "coeff"):
+            raise ValueError("key_form is 'ntt' or 'coeff'")
         N = self.params.N
         bv = np.ascontiguousarray(bv_keys, dtype=np.uint64)
         n_keys = bv.shape[0] if bv.size else 0
@@ -228,8 +232,9 @@ class PirServer:
         if bv.size == 0:
             bv = np.zeros(1, dtype=np.uint64)
         g = np.ascontiguousarray(gsw_key, dtype=np.uint64)
-        self._check(self._lib.opir_server_set_client_keys(
-            self._h, client_id, _ptr(bv), _ptr(gk, C.c_uint32), n_keys, _ptr(g)))
+        self._check(self._lib.opir_server_set_client_keys_ex(
+            self._h, client_id, _ptr(bv), _ptr(gk, C.c_uint32), n_keys, _ptr(g),
+            0 if key_form == "ntt" else 1))
 
     def remove_client(self, client_id: int):
         self._check(self._lib.opir_server_remove_client(self._h, client_id))
