@@ -181,8 +181,8 @@ def measured_peaks() -> dict:
     if os.path.exists(path):
         with open(path) as f:
             d = json.load(f)
-        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
-    return {"hbm_gbs": 6650.0, "source": "fallback"}
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d.get("bf16_tflops"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": None, "source": "fallback"}
 
 
 def ncu_traffic() -> dict | None:
@@ -975,8 +975,28 @@ def bench_client(args, world, rank, local):
     ms_dec = t_dec * 1e3 / args.steps
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     mhz = clocks.get("sm_mhz") or 1965.0
-    peak = sms * 128 * mhz * 1e6 / 1e9         # G lane-ops/s: 4 x 32 lanes issued per clk per SM
-    achieved = adds / (ms_dec / 1e3) / 1e9
+    tensor_path = (not c4 and n >= 32 and os.environ.get("OPIR_CLIENT_TC", "1") != "0"
+                   and os.environ.get("OPIR_CLIENT_WINDOW", "1") != "0")
+    if tensor_path:
+        # tcgen05 byte-plane scan: 4 A planes x 4 x planes of N x N per response
+        ops = n * 2 * N * N * 16
+        peaks = measured_peaks()
+        bf16 = peaks.get("bf16_tflops")
+        peak = 2 * bf16 if bf16 else 2 * 1590.0   # int8 dense = 2 x bf16 dense
+        achieved = ops / (ms_dec / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
+                "frac": achieved / peak, "traffic": None,
+                "work": "2 N^2 x 16 byte-plane products per response (3 of them nonzero: "
+                        "one secret plane x three planes of a 22-bit c1)",
+                "peak_kind": ("2 x measured" if bf16 else "2 x fallback")
+                             + " dense bf16 (int8 dense is twice bf16 on B200)"}
+    else:
+        peak = sms * 128 * mhz * 1e6 / 1e9     # G lane-ops/s: 4 x 32 lanes issued per clk per SM
+        achieved = adds / (ms_dec / 1e3) / 1e9
+        roof = {"bound": "issue", "achieved": achieved, "peak": peak,
+                "unit": "G int32 ops/s", "frac": achieved / peak, "traffic": None,
+                "work": "N x nonzero secret coefficients x parts additions per response",
+                "peak_kind": f"nominal: {sms} SMs x 128 lanes x sampled {mhz:.0f} MHz"}
     line = {
         "metric": "client responses decrypted/s (decrypt_mod_q, bit-exact)",
         "value": world * n * args.steps / t_dec, "unit": "responses/s", "n_gpus": world,
@@ -995,10 +1015,7 @@ def bench_client(args, world, rank, local):
                    "rows": h * lks + 2 * lkey},
         "e2e": {"value": world * n * args.steps / t_e2e, "unit": "responses/s",
                 "h2d_bytes_per_step": int(resp.nbytes), "d2h_bytes_per_step": int(n * N * 8)},
-        "roofline": {"bound": "issue", "achieved": achieved, "peak": peak,
-                     "unit": "G int32 ops/s", "frac": achieved / peak, "traffic": None,
-                     "work": "N x nonzero secret coefficients x parts additions per response",
-                     "peak_kind": f"nominal: {sms} SMs x 128 lanes x sampled {mhz:.0f} MHz"},
+        "roofline": roof,
         "gpu_launches": launches, "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:

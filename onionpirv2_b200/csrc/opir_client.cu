@@ -34,6 +34,7 @@
 #include "opir_host.h"
 #include "opir_kernels.h"
 #include "opir_params.h"
+#include "opir_scan_tc.h"
 
 namespace {
 
@@ -167,16 +168,42 @@ __device__ __forceinline__ uint64_t round_div(unsigned __int128 a, uint64_t b) {
   return static_cast<uint64_t>((a + (b >> 1)) / b);
 }
 
+// Constants of the decryption epilogue. When sq t < 2^63 every product fits
+// 64 bits and the divisions use Barrett reciprocals mu = floor(2^64 / d):
+// mulhi(x, mu) is floor(x / d) or one less (x mu / 2^64 lies in (x/d - 1,
+// x/d]), so one correction makes it exact; otherwise (wide) 128-bit division.
+struct DecConst {
+  uint64_t sq, t, mu_sq, mu_t;
+  uint32_t wide, pad;
+};
+
+__device__ __forceinline__ uint64_t div_barrett(uint64_t x, uint64_t d, uint64_t mu) {
+  uint64_t q = __umul64hi(x, mu);
+  if (x - q * d >= d) ++q;
+  return q;
+}
+
 // decrypt_mod_q of one coefficient from prod = (c1 s mod sq): pt =
 // round((c0 + prod mod sq) t / sq) mod t; *worst tracks the max noise
 // |phase - round(sq m / t)| the reference reports as its noise budget
 // (client.cpp:389-407).
-__device__ __forceinline__ uint64_t decrypt_coeff(uint64_t prod, uint64_t c0, uint64_t sq,
-                                                  uint64_t t, uint64_t &worst) {
-  uint64_t phase = prod + c0 % sq;
-  if (phase >= sq) phase -= sq;
-  const uint64_t m = round_div(static_cast<unsigned __int128>(phase) * t, sq) % t;
-  const uint64_t approx = round_div(static_cast<unsigned __int128>(sq) * m, t) % sq;
+__device__ __forceinline__ uint64_t decrypt_coeff(uint64_t prod, uint64_t c0, const DecConst &dc,
+                                                  uint64_t &worst) {
+  const uint64_t sq = dc.sq, t = dc.t;
+  uint64_t m, approx, phase;
+  if (!dc.wide) {
+    phase = prod + (c0 - div_barrett(c0, sq, dc.mu_sq) * sq);
+    if (phase >= sq) phase -= sq;
+    m = div_barrett(phase * t + (sq >> 1), sq, dc.mu_sq);
+    if (m >= t) m -= t;
+    approx = div_barrett(sq * m + (t >> 1), t, dc.mu_t);
+    if (approx >= sq) approx -= sq;
+  } else {
+    phase = prod + c0 % sq;
+    if (phase >= sq) phase -= sq;
+    m = round_div(static_cast<unsigned __int128>(phase) * t, sq) % t;
+    approx = round_div(static_cast<unsigned __int128>(sq) * m, t) % sq;
+  }
   const uint64_t pos = phase >= approx ? phase - approx : sq - approx + phase;
   const uint64_t nabs = pos > (sq >> 1) ? sq - pos : pos;
   worst = nabs > worst ? nabs : worst;
@@ -220,8 +247,9 @@ __device__ __forceinline__ void add_constants(const ConstEntry *ce, uint32_t nco
 template <int NP, int R>
 __global__ void __launch_bounds__(kBlock) k_client_decrypt(
     const uint64_t *__restrict__ resp, const uint16_t *__restrict__ sidx, uint32_t npos,
-    uint32_t nneg, uint32_t n, uint64_t sq, uint64_t t, uint64_t *__restrict__ pt,
+    uint32_t nneg, uint32_t n, DecConst dc, uint64_t *__restrict__ pt,
     unsigned long long *__restrict__ max_noise) {
+  const uint64_t sq = dc.sq;
   extern __shared__ __align__(16) int32_t smem[];
   int32_t *ext = smem;
   uint16_t *sl = reinterpret_cast<uint16_t *>(smem + NP * 2 * n);
@@ -237,7 +265,7 @@ __global__ void __launch_bounds__(kBlock) k_client_decrypt(
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const uint32_t i = i0 + kBlock * r;
-    pt[b * n + i] = decrypt_coeff(reduce_parts<NP, 31, R>(acc, r, sq), c0[i], sq, t, worst);
+    pt[b * n + i] = decrypt_coeff(reduce_parts<NP, 31, R>(acc, r, sq), c0[i], dc, worst);
   }
   publish_noise(worst, max_noise);
 }
@@ -245,8 +273,9 @@ __global__ void __launch_bounds__(kBlock) k_client_decrypt(
 // The same with the window product (n = kBlock J, PB-bit parts).
 template <int NP, int PB, int R, int J>
 __global__ void __launch_bounds__(kBlock) k_client_decrypt_w(
-    const uint64_t *__restrict__ resp, const uint32_t *__restrict__ code, uint32_t n, uint64_t sq,
-    uint64_t t, uint64_t *__restrict__ pt, unsigned long long *__restrict__ max_noise) {
+    const uint64_t *__restrict__ resp, const uint32_t *__restrict__ code, uint32_t n, DecConst dc,
+    uint64_t *__restrict__ pt, unsigned long long *__restrict__ max_noise) {
+  const uint64_t sq = dc.sq;
   extern __shared__ __align__(16) int32_t smem[];
   int32_t *ext = smem;
   uint32_t *cs = reinterpret_cast<uint32_t *>(smem + NP * 2 * n);
@@ -262,7 +291,7 @@ __global__ void __launch_bounds__(kBlock) k_client_decrypt_w(
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const uint32_t i = i0 + kBlock * r;
-    pt[b * n + i] = decrypt_coeff(reduce_parts<NP, PB, R>(acc, r, sq), c0[i], sq, t, worst);
+    pt[b * n + i] = decrypt_coeff(reduce_parts<NP, PB, R>(acc, r, sq), c0[i], dc, worst);
   }
   publish_noise(worst, max_noise);
 }
@@ -404,6 +433,66 @@ __global__ void __launch_bounds__(kBlock) k_client_ntt(uint64_t *__restrict__ po
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) a[i] = sp[i];
 }
 
+// Tensor-core decryption (single-modulus set, small_q < 2^29): (c1 s)_i =
+// sum_j S[i][j] x_j with S[i][j] = s[i - j] (i >= j) or -s[N + i - j], so with
+// A = S + 1 (entries 0, 1, 2: one unsigned byte plane) y = A x - sum_j x_j.
+// A x mod small_q is the tensor-core scan (opir_scan_tc.h) with one residue
+// and one level: A [4 planes (1..3 zero)][N rows][N bytes], x as the four byte
+// planes of each response's c1 mod small_q, Q [4][n][N].
+__global__ void __launch_bounds__(kBlock) k_client_secret_matrix(const int8_t *__restrict__ s,
+                                                                 uint32_t n,
+                                                                 uint8_t *__restrict__ a) {
+  const uint32_t i = blockIdx.x;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const int v = i >= j ? s[i - j] : -s[n + i - j];
+    a[static_cast<uint64_t>(i) * n + j] = static_cast<uint8_t>(v + 1);
+  }
+}
+
+// Q planes and sum_j x_j mod small_q of response blockIdx.x.
+__global__ void __launch_bounds__(kBlock) k_client_tc_prep(const uint64_t *__restrict__ resp,
+                                                           uint32_t n, uint32_t nresp, uint64_t sq,
+                                                           uint8_t *__restrict__ qpl,
+                                                           uint64_t *__restrict__ colsum) {
+  __shared__ uint64_t part[kBlock / 32];
+  const uint64_t b = blockIdx.x;
+  const uint64_t *c1 = resp + b * 2 * n + n;
+  uint64_t sum = 0;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const uint64_t x = c1[j] % sq;
+    sum += x;
+#pragma unroll
+    for (int pl = 0; pl < 4; ++pl)
+      qpl[(static_cast<uint64_t>(pl) * nresp + b) * n + j] = static_cast<uint8_t>(x >> (8 * pl));
+  }
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t t = 0;
+    for (int w = 0; w < kBlock / 32; ++w) t += part[w];
+    colsum[b] = t % sq;
+  }
+}
+
+// pt from the scan's (A x mod small_q), laid out [response][i].
+__global__ void __launch_bounds__(kBlock) k_client_tc_finish(
+    const uint64_t *__restrict__ resp, const uint32_t *__restrict__ ax,
+    const uint64_t *__restrict__ colsum, uint32_t n, DecConst dc,
+    uint64_t *__restrict__ pt, unsigned long long *__restrict__ max_noise) {
+  const uint64_t sq = dc.sq;
+  const uint64_t b = blockIdx.x;
+  const uint64_t *c0 = resp + b * 2 * n;
+  const uint64_t cs = colsum[b];
+  uint64_t worst = 0;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint64_t v = ax[b * n + i];
+    const uint64_t prod = v >= cs ? v - cs : v + (sq - cs);
+    pt[b * n + i] = decrypt_coeff(prod, c0[i], dc, worst);
+  }
+  publish_noise(worst, max_noise);
+}
+
 uint64_t bitrev(uint64_t x, uint32_t bits) {
   uint64_t r = 0;
   for (uint32_t i = 0; i < bits; ++i) r |= ((x >> i) & 1ull) << (bits - 1 - i);
@@ -428,6 +517,10 @@ struct opir_client {
   DevBuf<int8_t> msgs;       // [1 + h][n]: s, then sigma_{N/2^i + 1}(s) for i < h
   DevBuf<uint64_t> fw;       // [K][n]: forward NTT twiddles per limb
   DevBuf<KeyRow> keyrows;
+  // tensor-core decryption: A = S + 1 (built on first use), per-call scratch
+  DevBuf<uint8_t> tc_a, tc_q;
+  DevBuf<uint64_t> tc_colsum;
+  DevBuf<uint32_t> tc_ax, tc_err;
   uint32_t nconst = 1;       // constant slots per query
   uint64_t one_val[2]{};     // the one-hot's value per limb
   std::vector<uint64_t> gadget_val;  // [k][limb]: B^(L_EP-1-k) (2^h)^-1 mod q_limb
@@ -600,10 +693,86 @@ void launched(const char *what) {
   opir::note_launches(1);
 }
 
+DecConst dec_const(const opir_params &p) {
+  DecConst dc{};
+  dc.sq = p.small_q;
+  dc.t = p.plain_mod;
+  dc.mu_sq = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / dc.sq);
+  dc.mu_t = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / dc.t);
+  dc.wide = static_cast<unsigned __int128>(dc.sq) * dc.t + dc.sq >= (static_cast<unsigned __int128>(1) << 63);
+  return dc;
+}
+
+// The tensor-core form serves single-modulus decryption batches of at least
+// kTcMinResponses (OPIR_CLIENT_TC=0 turns it off).
+constexpr uint64_t kTcMinResponses = 32;
+bool tc_enabled(const opir_client &c, uint64_t n_resp) {
+  const char *v = std::getenv("OPIR_CLIENT_TC");
+  if ((v && v[0] == '0') || !window_enabled()) return false;
+  return c.limbs == 1 && c.n % 128 == 0 && c.n <= 8192 && c.params.small_q < (1ull << 29) &&
+         n_resp >= kTcMinResponses;
+}
+
+void launch_decrypt_tc(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, opir_client &c,
+                       uint64_t *pt, unsigned long long *noise) {
+  const uint32_t n = c.n, nr = static_cast<uint32_t>(n_resp);
+  const uint64_t sq = c.params.small_q;
+  if (!c.tc_a.p) {
+    c.tc_a.alloc(4ull * n * n);
+    ck(cudaMemsetAsync(c.tc_a.p, 0, 4ull * n * n, st), "secret matrix clear");
+    k_client_secret_matrix<<<n, kBlock, 0, st>>>(c.msgs.p, n, c.tc_a.p);
+    launched("secret matrix launch");
+    c.tc_err.alloc(1);
+  }
+  if (c.tc_colsum.n < n_resp) {
+    ck(cudaStreamSynchronize(st), "client sync");
+    c.tc_q.alloc(4ull * n_resp * n);
+    c.tc_colsum.alloc(n_resp);
+    c.tc_ax.alloc(n_resp * n);
+  }
+  ck(cudaMemsetAsync(c.tc_err.p, 0, sizeof(uint32_t), st), "scan error reset");
+  k_client_tc_prep<<<nr, kBlock, 0, st>>>(resp, n, nr, sq, c.tc_q.p, c.tc_colsum.p);
+  launched("client prep launch");
+  opir::TcScanArgs a{};
+  a.ntile = nr <= 16 ? 16 : nr <= 32 ? 32 : 64;
+  a.kt = 128;
+  a.stages = opir::scan_tc_max_stages(a.ntile, a.kt);
+  a.col_tiles = (nr + a.ntile - 1) / a.ntile;
+  a.k_tiles = n / a.kt;
+  a.other = n;
+  a.m_tiles = n / 128;
+  a.ncols = nr;
+  a.zcount = 1;
+  a.levels_per_res = 1;
+  a.q[0] = a.q[1] = static_cast<uint32_t>(sq);
+  a.mu[0] = a.mu[1] = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / sq);
+  uint64_t w = 1;
+  for (int sft = 0; sft < 7; ++sft) {
+    a.w[0][sft] = a.w[1][sft] = static_cast<uint32_t>(w);
+    w = (w << 8) % sq;
+  }
+  a.cmat = c.tc_ax.p;
+  a.err = c.tc_err.p;
+  CUtensorMap map_a, map_q;
+  opir::make_plane_map(&map_a, c.tc_a.p, n, n, 4, 128, 128);
+  opir::make_plane_map(&map_q, c.tc_q.p, n, nr, 4, a.ntile, 128);
+  opir::launch_scan_tc(map_a, map_q, a, c.sms, st);
+  k_client_tc_finish<<<nr, kBlock, 0, st>>>(resp, c.tc_ax.p, c.tc_colsum.p, n,
+                                            dec_const(c.params), pt, noise);
+  launched("client finish launch");
+  // the scan's bounded waits report through its error word
+  uint32_t err = 0;
+  ck(cudaMemcpyAsync(&err, c.tc_err.p, sizeof(err), cudaMemcpyDeviceToHost, st), "scan error read");
+  ck(cudaStreamSynchronize(st), "client decrypt");
+  if (err) throw std::runtime_error("client decrypt: tensor-core scan gave up (error bits " +
+                                    std::to_string(err) + ")");
+}
+
 void launch_decrypt(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, const opir_client &c,
                     uint64_t *pt, unsigned long long *noise) {
   const uint32_t n = c.n;
-  const uint64_t sq = c.params.small_q, t = c.params.plain_mod;
+  const uint64_t sq = c.params.small_q;
+  const DecConst dc = dec_const(c.params);
   const uint32_t nb = static_cast<uint32_t>(n_resp);
   const uint32_t R = sq < (1ull << 50) ? window_r(n_resp, n, c.sms) : 0;
   if (R) {
@@ -613,8 +782,8 @@ void launch_decrypt(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, cons
 #define OPIR_DECW(NP, RR, JJ)                                                                  \
   if (np == NP && R == RR && n == kBlock * JJ) {                                              \
     set_smem(k_client_decrypt_w<NP, 25, RR, JJ>, smem, "client decrypt smem");               \
-    k_client_decrypt_w<NP, 25, RR, JJ><<<grid, kBlock, smem, st>>>(resp, c.code.p, n, sq, t,  \
-                                                                   pt, noise);                \
+    k_client_decrypt_w<NP, 25, RR, JJ><<<grid, kBlock, smem, st>>>(resp, c.code.p, n, dc, pt, \
+                                                                   noise);                    \
     return launched("client decrypt launch");                                                 \
   }
     OPIR_DECW(1, 8, 8) OPIR_DECW(1, 4, 8) OPIR_DECW(1, 8, 16) OPIR_DECW(1, 4, 16)
@@ -632,7 +801,7 @@ void launch_decrypt(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, cons
   if (np == NP && Rl == RR) {                                                                 \
     set_smem(k_client_decrypt<NP, RR>, smem, "client decrypt smem");                          \
     k_client_decrypt<NP, RR><<<grid, kBlock, smem, st>>>(resp, c.sidx.p, c.npos, c.nneg, n,   \
-                                                         sq, t, pt, noise);                   \
+                                                         dc, pt, noise);                      \
     return launched("client decrypt launch");                                                 \
   }
   OPIR_DEC(1, 1) OPIR_DEC(1, 2) OPIR_DEC(1, 4) OPIR_DEC(1, 8)
@@ -817,6 +986,11 @@ void opir_client_destroy(opir_client *c) {
     c->msgs.reset();
     c->fw.reset();
     c->keyrows.reset();
+    c->tc_a.reset();
+    c->tc_q.reset();
+    c->tc_colsum.reset();
+    c->tc_ax.reset();
+    c->tc_err.reset();
     c->consts.reset();
     if (c->staging) cudaFreeHost(c->staging);
     if (c->staged) cudaEventDestroy(c->staged);
@@ -878,8 +1052,11 @@ opir_status opir_client_decrypt_device(opir_client *c, uint32_t n, const uint64_
     if (d_max_noise)
       ck(cudaMemsetAsync(d_max_noise, 0, static_cast<size_t>(n) * sizeof(uint64_t), st),
          "noise reset");
-    launch_decrypt(n, st, d_responses, *c, d_plaintexts,
-                   reinterpret_cast<unsigned long long *>(d_max_noise));
+    auto *noise = reinterpret_cast<unsigned long long *>(d_max_noise);
+    if (tc_enabled(*c, n))
+      launch_decrypt_tc(n, st, d_responses, *c, d_plaintexts, noise);
+    else
+      launch_decrypt(n, st, d_responses, *c, d_plaintexts, noise);
   });
 }
 

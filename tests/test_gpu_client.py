@@ -4,10 +4,13 @@ client.cpp:364-410) against the oracle client, bit for bit: queries packed on
 the GPU from the oracle's own uniform c1 and error equal the oracle's queries;
 responses decrypted on the GPU equal the oracle's plaintexts and max noise;
 and a GPU-packed query answered by the GPU server decrypts on the GPU to the
-database plaintext. Every case runs twice: as the launcher picks (auto: the
-window kernel for decryption batches that fill the GPU) and with the
-index-list kernel forced (OPIR_CLIENT_WINDOW=0); batch sizes cover every
-outputs-per-thread width each kernel uses (list: 1, 2, 4, 8; window: 4, 8)."""
+database plaintext. Every case runs three times: as the launcher picks
+(auto: tensor-core decryption for single-modulus batches of 32 or more, the
+window kernel for other batches that fill the GPU), with the tensor-core form
+off (OPIR_CLIENT_TC=0) and with the index-list kernel forced
+(OPIR_CLIENT_WINDOW=0); batch sizes cover every outputs-per-thread width each
+CUDA-core kernel uses (list: 1, 2, 4, 8; window: 4, 8) and full and partial
+column tiles of the tensor-core scan (33, 80, 150, 300)."""
 import numpy as np
 import pytest
 
@@ -18,12 +21,14 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=["auto", "list"])
+@pytest.fixture(params=["auto", "window", "list"])
 def kernel(request, monkeypatch):
-    if request.param == "list":
+    monkeypatch.delenv("OPIR_CLIENT_WINDOW", raising=False)
+    monkeypatch.delenv("OPIR_CLIENT_TC", raising=False)
+    if request.param == "window":
+        monkeypatch.setenv("OPIR_CLIENT_TC", "0")
+    elif request.param == "list":
         monkeypatch.setenv("OPIR_CLIENT_WINDOW", "0")
-    else:
-        monkeypatch.delenv("OPIR_CLIENT_WINDOW", raising=False)
     return request.param
 
 C4 = "CONFIG_N4096_K2_MP"
@@ -91,7 +96,7 @@ def test_k1_error_of_any_size_enters_linearly(kernel):
     assert np.array_equal(q1[:, 1], q2[:, 1])
 
 
-@pytest.mark.parametrize("config,n", [("k1", 1), ("k1", 80), ("k1", 150), ("k1", 300),
+@pytest.mark.parametrize("config,n", [("k1", 1), ("k1", 33), ("k1", 80), ("k1", 150), ("k1", 300),
                                       ("c4", 1), ("c4", 40), ("c4", 75), ("c4", 200)])
 def test_decrypt_matches_oracle(config, n, kernel):
     if config == "k1":
