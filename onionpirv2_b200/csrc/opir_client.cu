@@ -493,6 +493,120 @@ __global__ void __launch_bounds__(kBlock) k_client_tc_finish(
   publish_noise(worst, max_noise);
 }
 
+// Tensor-core packing (single-modulus set, q = q1 q2): a s mod q is the CRT
+// of a s mod q1 and mod q2, each the scan of the same A = S + 1 against the
+// byte planes of a mod q_r. Planes [r][4][nq][n], sums [r][nq].
+__global__ void __launch_bounds__(kBlock) k_client_tc_pack_prep(const uint64_t *__restrict__ a,
+                                                                uint32_t n, uint32_t nq,
+                                                                uint64_t q1, uint64_t q2,
+                                                                uint8_t *__restrict__ qpl,
+                                                                uint64_t *__restrict__ colsum) {
+  __shared__ uint64_t part[2][kBlock / 32];
+  const uint64_t b = blockIdx.x;
+  const uint64_t *x = a + b * n;
+  uint64_t sum[2] = {0, 0};
+  const uint64_t plane = static_cast<uint64_t>(nq) * n;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const uint64_t r[2] = {x[j] % q1, x[j] % q2};
+#pragma unroll
+    for (int res = 0; res < 2; ++res) {
+      sum[res] += r[res];
+#pragma unroll
+      for (int pl = 0; pl < 4; ++pl)
+        qpl[(4ull * res + pl) * plane + b * n + j] = static_cast<uint8_t>(r[res] >> (8 * pl));
+    }
+  }
+#pragma unroll
+  for (int res = 0; res < 2; ++res) {
+    for (int o = 16; o > 0; o >>= 1) sum[res] += __shfl_xor_sync(0xFFFFFFFFu, sum[res], o);
+    if ((threadIdx.x & 31) == 0) part[res][threadIdx.x >> 5] = sum[res];
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    uint64_t tot = 0;
+    for (int w = 0; w < kBlock / 32; ++w) tot += part[threadIdx.x][w];
+    colsum[static_cast<uint64_t>(threadIdx.x) * nq + b] = tot % (threadIdx.x ? q2 : q1);
+  }
+}
+
+// What the device needs to place a query's plaintext constants itself.
+struct PackLayout {
+  uint64_t n0, other;      // first-dimension size, rows
+  uint32_t num_dims, h;    // dimensions, expansion height
+  uint32_t l_ep, pad;
+  uint64_t one;            // the one-hot's value (single modulus)
+  uint64_t gadget[16];     // B^(L_EP-1-k) (2^h)^-1 mod q
+};
+
+__device__ __forceinline__ uint32_t bitrev_dev(uint64_t x, uint32_t bits) {
+  return bits ? static_cast<uint32_t>(__brevll(x) >> (64 - bits)) : 0u;
+}
+
+// get_query_indices (src/client.cpp:48-98) for selector bit i >= 1 of index
+// idx: the leaf's parity on the incomplete last level, then the perfect-tree
+// path MSB first.
+__device__ __forceinline__ uint32_t selector_bit(const PackLayout &L, uint64_t idx, uint32_t i) {
+  const uint64_t row = idx / L.n0;
+  const uint64_t hd = L.num_dims - 1;
+  const uint64_t r = 2 * L.other - (1ull << hd), sl = L.other - r;
+  uint64_t perfect, first;
+  if (row < sl) {
+    first = 0;
+    perfect = row;
+  } else {
+    first = (row - sl) % 2;
+    perfect = sl + (row - sl) / 2;
+  }
+  return static_cast<uint32_t>(i == 1 ? first : (perfect >> (hd - i)) & 1ull);
+}
+
+// c0 = -(a s + e) mod q plus the query's constants, c1 = a, from the two
+// scans' (A x_r mod q_r) [r][nq][n]: y_r = A x_r - sum_j x_r,j mod q_r, then
+// Garner: a s mod q = y_1 + q1 ((y_2 - y_1) q1^-1 mod q2). The constants
+// (client.cpp:128-225) are placed from the index: the one-hot at
+// BitRev(col, h), and for each set selector bit i the L_EP gadget rows at
+// BitRev(N0 + (i-1) L_EP + k, h).
+__global__ void __launch_bounds__(kBlock) k_client_tc_pack_finish(
+    const uint64_t *__restrict__ a, const int64_t *__restrict__ e,
+    const uint64_t *__restrict__ pt_idx, PackLayout L, const uint32_t *__restrict__ ax,
+    const uint64_t *__restrict__ colsum, uint32_t n, uint32_t nq, uint64_t q1, uint64_t q2,
+    uint64_t q1_inv_mod_q2, uint64_t *__restrict__ out) {
+  const uint64_t b = blockIdx.x, q = q1 * q2;
+  const uint64_t cs1 = colsum[b], cs2 = colsum[static_cast<uint64_t>(nq) + b];
+  const uint32_t *ax1 = ax + b * n, *ax2 = ax + (static_cast<uint64_t>(nq) + b) * n;
+  uint64_t *c0 = out + b * 2 * n, *c1 = c0 + n;
+  const uint64_t *x = a + b * n;
+  const int64_t *eq = e + b * n;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint64_t v1 = ax1[i], v2 = ax2[i];
+    const uint64_t y1 = v1 >= cs1 ? v1 - cs1 : v1 + (q1 - cs1);
+    const uint64_t y2 = v2 >= cs2 ? v2 - cs2 : v2 + (q2 - cs2);
+    const uint64_t y1m = y1 >= q2 ? y1 - q2 : y1;  // q1 < 2 q2
+    const uint64_t d = y2 >= y1m ? y2 - y1m : y2 + (q2 - y1m);
+    const uint64_t k = d * q1_inv_mod_q2 % q2;
+    c0[i] = pack_coeff(y1 + q1 * k, eq[i], q);
+    c1[i] = x[i];
+  }
+  __syncthreads();
+  const uint64_t idx = pt_idx[b];
+  const uint32_t nconst = 1 + (L.num_dims - 1) * L.l_ep;
+  for (uint32_t u = threadIdx.x; u < nconst; u += blockDim.x) {
+    uint32_t pos;
+    uint64_t val;
+    if (u == 0) {
+      pos = bitrev_dev(idx % L.n0, L.h);
+      val = L.one;
+    } else {
+      const uint32_t i = 1 + (u - 1) / L.l_ep, k = (u - 1) % L.l_ep;
+      if (!selector_bit(L, idx, i)) continue;
+      pos = bitrev_dev(L.n0 + static_cast<uint64_t>(i - 1) * L.l_ep + k, L.h);
+      val = L.gadget[k];
+    }
+    const uint64_t v = c0[pos] + val;
+    c0[pos] = v >= q ? v - q : v;
+  }
+}
+
 uint64_t bitrev(uint64_t x, uint32_t bits) {
   uint64_t r = 0;
   for (uint32_t i = 0; i < bits; ++i) r |= ((x >> i) & 1ull) << (bits - 1 - i);
@@ -519,8 +633,12 @@ struct opir_client {
   DevBuf<KeyRow> keyrows;
   // tensor-core decryption: A = S + 1 (built on first use), per-call scratch
   DevBuf<uint8_t> tc_a, tc_q;
-  DevBuf<uint64_t> tc_colsum;
-  DevBuf<uint32_t> tc_ax, tc_err;
+  DevBuf<uint64_t> tc_colsum, pk_colsum;
+  DevBuf<uint32_t> tc_ax, tc_err, pk_ax;
+  DevBuf<uint8_t> pk_q;
+  DevBuf<uint64_t> pk_idx;
+  uint64_t *idx_staging = nullptr;   // pinned copy of the last call's indices
+  size_t idx_staging_cap = 0;
   uint32_t nconst = 1;       // constant slots per query
   uint64_t one_val[2]{};     // the one-hot's value per limb
   std::vector<uint64_t> gadget_val;  // [k][limb]: B^(L_EP-1-k) (2^h)^-1 mod q_limb
@@ -706,33 +824,28 @@ DecConst dec_const(const opir_params &p) {
 // The tensor-core form serves single-modulus decryption batches of at least
 // kTcMinResponses (OPIR_CLIENT_TC=0 turns it off).
 constexpr uint64_t kTcMinResponses = 32;
-bool tc_enabled(const opir_client &c, uint64_t n_resp) {
+bool tc_enabled(const opir_client &c, uint64_t items, uint64_t modulus_bound) {
   const char *v = std::getenv("OPIR_CLIENT_TC");
   if ((v && v[0] == '0') || !window_enabled()) return false;
-  return c.limbs == 1 && c.n % 128 == 0 && c.n <= 8192 && c.params.small_q < (1ull << 29) &&
-         n_resp >= kTcMinResponses;
+  return c.limbs == 1 && c.n % 128 == 0 && c.n <= 8192 && modulus_bound < (1ull << 29) &&
+         items >= kTcMinResponses;
 }
 
-void launch_decrypt_tc(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, opir_client &c,
-                       uint64_t *pt, unsigned long long *noise) {
-  const uint32_t n = c.n, nr = static_cast<uint32_t>(n_resp);
-  const uint64_t sq = c.params.small_q;
-  if (!c.tc_a.p) {
-    c.tc_a.alloc(4ull * n * n);
-    ck(cudaMemsetAsync(c.tc_a.p, 0, 4ull * n * n, st), "secret matrix clear");
-    k_client_secret_matrix<<<n, kBlock, 0, st>>>(c.msgs.p, n, c.tc_a.p);
-    launched("secret matrix launch");
-    c.tc_err.alloc(1);
-  }
-  if (c.tc_colsum.n < n_resp) {
-    ck(cudaStreamSynchronize(st), "client sync");
-    c.tc_q.alloc(4ull * n_resp * n);
-    c.tc_colsum.alloc(n_resp);
-    c.tc_ax.alloc(n_resp * n);
-  }
-  ck(cudaMemsetAsync(c.tc_err.p, 0, sizeof(uint32_t), st), "scan error reset");
-  k_client_tc_prep<<<nr, kBlock, 0, st>>>(resp, n, nr, sq, c.tc_q.p, c.tc_colsum.p);
-  launched("client prep launch");
+void ensure_secret_matrix(opir_client &c, cudaStream_t st) {
+  if (c.tc_a.p) return;
+  const uint32_t n = c.n;
+  c.tc_a.alloc(4ull * n * n);
+  ck(cudaMemsetAsync(c.tc_a.p, 0, 4ull * n * n, st), "secret matrix clear");
+  k_client_secret_matrix<<<n, kBlock, 0, st>>>(c.msgs.p, n, c.tc_a.p);
+  launched("secret matrix launch");
+  c.tc_err.alloc(1);
+}
+
+// One scan C = A x mod q (< 2^29) over nr columns of byte planes `planes`
+// ([4][nr][n]) into cmat [nr][n].
+void scan_secret_matrix(const opir_client &c, uint32_t nr, uint64_t q, const uint8_t *planes,
+                        uint32_t *cmat, cudaStream_t st) {
+  const uint32_t n = c.n;
   opir::TcScanArgs a{};
   a.ntile = nr <= 16 ? 16 : nr <= 32 ? 32 : 64;
   a.kt = 128;
@@ -744,28 +857,97 @@ void launch_decrypt_tc(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, o
   a.ncols = nr;
   a.zcount = 1;
   a.levels_per_res = 1;
-  a.q[0] = a.q[1] = static_cast<uint32_t>(sq);
-  a.mu[0] = a.mu[1] = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / sq);
+  a.q[0] = a.q[1] = static_cast<uint32_t>(q);
+  a.mu[0] = a.mu[1] = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / q);
   uint64_t w = 1;
   for (int sft = 0; sft < 7; ++sft) {
     a.w[0][sft] = a.w[1][sft] = static_cast<uint32_t>(w);
-    w = (w << 8) % sq;
+    w = (w << 8) % q;
   }
-  a.cmat = c.tc_ax.p;
+  a.cmat = cmat;
   a.err = c.tc_err.p;
   CUtensorMap map_a, map_q;
   opir::make_plane_map(&map_a, c.tc_a.p, n, n, 4, 128, 128);
-  opir::make_plane_map(&map_q, c.tc_q.p, n, nr, 4, a.ntile, 128);
+  opir::make_plane_map(&map_q, planes, n, nr, 4, a.ntile, 128);
   opir::launch_scan_tc(map_a, map_q, a, c.sms, st);
+}
+
+// Reads the scans' error word (synchronises the stream).
+void check_scan_error(const opir_client &c, cudaStream_t st, const char *what) {
+  uint32_t err = 0;
+  ck(cudaMemcpyAsync(&err, c.tc_err.p, sizeof(err), cudaMemcpyDeviceToHost, st), "scan error read");
+  ck(cudaStreamSynchronize(st), what);
+  if (err) throw std::runtime_error(std::string(what) + ": tensor-core scan gave up (error bits " +
+                                    std::to_string(err) + ")");
+}
+
+void launch_pack_tc(uint64_t n_q, const uint64_t *pt_idx, cudaStream_t st, const uint64_t *a,
+                    const int64_t *e, opir_client &c, uint64_t *out) {
+  const uint32_t n = c.n, nq = static_cast<uint32_t>(n_q);
+  const opir_params &p = c.params;
+  if (p.l_ep > 16) throw std::runtime_error("client pack: L_EP above 16");
+  ensure_secret_matrix(c, st);
+  if (c.pk_colsum.n < 2 * n_q) {
+    ck(cudaStreamSynchronize(st), "client sync");
+    c.pk_q.alloc(8ull * n_q * n);
+    c.pk_colsum.alloc(2 * n_q);
+    c.pk_ax.alloc(2 * n_q * n);
+    c.pk_idx.alloc(n_q);
+  }
+  // the previous call's index upload must have left the staging buffer
+  ck(cudaEventSynchronize(c.staged), "client staging wait");
+  if (c.idx_staging_cap < n_q) {
+    if (c.idx_staging) cudaFreeHost(c.idx_staging);
+    c.idx_staging = nullptr;
+    c.idx_staging_cap = 0;
+    ck(cudaMallocHost(&c.idx_staging, n_q * sizeof(uint64_t)), "client index staging");
+    c.idx_staging_cap = n_q;
+  }
+  std::memcpy(c.idx_staging, pt_idx, n_q * sizeof(uint64_t));
+  ck(cudaMemcpyAsync(c.pk_idx.p, c.idx_staging, n_q * sizeof(uint64_t), cudaMemcpyHostToDevice, st),
+     "client index upload");
+  ck(cudaEventRecord(c.staged, st), "client staging record");
+  PackLayout L{};
+  L.n0 = p.fst_dim_sz;
+  L.other = p.other_dim_sz;
+  L.num_dims = p.num_dims;
+  L.h = p.expansion_height;
+  L.l_ep = p.l_ep;
+  L.one = c.one_val[0];
+  for (uint32_t k = 0; k < p.l_ep; ++k) L.gadget[k] = c.gadget_val[2 * k];
+  ck(cudaMemsetAsync(c.tc_err.p, 0, sizeof(uint32_t), st), "scan error reset");
+  k_client_tc_pack_prep<<<nq, kBlock, 0, st>>>(a, n, nq, p.q1, p.q2, c.pk_q.p, c.pk_colsum.p);
+  launched("client pack prep launch");
+  const uint64_t plane_set = 4ull * n_q * n;
+  scan_secret_matrix(c, nq, p.q1, c.pk_q.p, c.pk_ax.p, st);
+  scan_secret_matrix(c, nq, p.q2, c.pk_q.p + plane_set, c.pk_ax.p + n_q * n, st);
+  k_client_tc_pack_finish<<<nq, kBlock, 0, st>>>(a, e, c.pk_idx.p, L, c.pk_ax.p,
+                                                 c.pk_colsum.p, n, nq, p.q1, p.q2,
+                                                 p.q1_inv_mod_q2, out);
+  launched("client pack finish launch");
+  check_scan_error(c, st, "client pack");
+}
+
+void launch_decrypt_tc(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, opir_client &c,
+                       uint64_t *pt, unsigned long long *noise) {
+  const uint32_t n = c.n, nr = static_cast<uint32_t>(n_resp);
+  const uint64_t sq = c.params.small_q;
+  ensure_secret_matrix(c, st);
+  if (c.tc_colsum.n < n_resp) {
+    ck(cudaStreamSynchronize(st), "client sync");
+    c.tc_q.alloc(4ull * n_resp * n);
+    c.tc_colsum.alloc(n_resp);
+    c.tc_ax.alloc(n_resp * n);
+  }
+  ck(cudaMemsetAsync(c.tc_err.p, 0, sizeof(uint32_t), st), "scan error reset");
+  k_client_tc_prep<<<nr, kBlock, 0, st>>>(resp, n, nr, sq, c.tc_q.p, c.tc_colsum.p);
+  launched("client prep launch");
+  scan_secret_matrix(c, nr, sq, c.tc_q.p, c.tc_ax.p, st);
   k_client_tc_finish<<<nr, kBlock, 0, st>>>(resp, c.tc_ax.p, c.tc_colsum.p, n,
                                             dec_const(c.params), pt, noise);
   launched("client finish launch");
   // the scan's bounded waits report through its error word
-  uint32_t err = 0;
-  ck(cudaMemcpyAsync(&err, c.tc_err.p, sizeof(err), cudaMemcpyDeviceToHost, st), "scan error read");
-  ck(cudaStreamSynchronize(st), "client decrypt");
-  if (err) throw std::runtime_error("client decrypt: tensor-core scan gave up (error bits " +
-                                    std::to_string(err) + ")");
+  check_scan_error(c, st, "client decrypt");
 }
 
 void launch_decrypt(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, const opir_client &c,
@@ -991,6 +1173,11 @@ void opir_client_destroy(opir_client *c) {
     c->tc_colsum.reset();
     c->tc_ax.reset();
     c->tc_err.reset();
+    c->pk_q.reset();
+    c->pk_idx.reset();
+    if (c->idx_staging) cudaFreeHost(c->idx_staging);
+    c->pk_colsum.reset();
+    c->pk_ax.reset();
     c->consts.reset();
     if (c->staging) cudaFreeHost(c->staging);
     if (c->staged) cudaEventDestroy(c->staged);
@@ -1014,9 +1201,13 @@ opir_status opir_client_generate_queries_device(opir_client *c, uint32_t n,
     for (uint32_t i = 0; i < n; ++i)
       if (pt_idx[i] >= c->params.num_pt)
         throw std::out_of_range("PIR plaintext index exceeds the runtime layout");
-    const size_t count = static_cast<size_t>(n) * c->nconst;
     DeviceGuard g(c->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (tc_enabled(*c, n, std::max(c->params.q1, c->params.q2))) {
+      launch_pack_tc(n, pt_idx, st, d_a, d_e, *c, d_queries);
+      return;
+    }
+    const size_t count = static_cast<size_t>(n) * c->nconst;
     // the previous call's upload must have left the staging buffer
     ck(cudaEventSynchronize(c->staged), "client staging wait");
     if (c->staging_cap < count) {
@@ -1053,7 +1244,7 @@ opir_status opir_client_decrypt_device(opir_client *c, uint32_t n, const uint64_
       ck(cudaMemsetAsync(d_max_noise, 0, static_cast<size_t>(n) * sizeof(uint64_t), st),
          "noise reset");
     auto *noise = reinterpret_cast<unsigned long long *>(d_max_noise);
-    if (tc_enabled(*c, n))
+    if (tc_enabled(*c, n, c->params.small_q))
       launch_decrypt_tc(n, st, d_responses, *c, d_plaintexts, noise);
     else
       launch_decrypt(n, st, d_responses, *c, d_plaintexts, noise);
