@@ -182,3 +182,33 @@ def test_session_keys_match_oracle(config, target, h):
     want = (O.db_plaintext(3, idx, op).astype(np.uint64) if config == "k1"
             else O.c4_db_plaintext(3, idx, op))
     assert np.array_equal(gc.decrypt_mod_q(resp), want)
+
+
+@pytest.mark.parametrize("config,n", [("k1", 64), ("c4", 40)])
+def test_whole_client_pipeline_on_the_gpu(config, n):
+    """Session keys, queries and decryption all on the GPU around the GPU
+    server: every plaintext comes back."""
+    target, h, db_seed = 16384, 9, 41
+    if config == "k1":
+        gp, op = PirParams(target, h), O.params(target, h)
+        cl = O.Client(op, 71, keygen_parts=True)
+        mods = [op.q]
+        plain = lambda i: O.db_plaintext(db_seed, i, op).astype(np.uint64)  # noqa: E731
+    else:
+        gp, op = PirParams(target, h, config=C4), O.c4_params(target, h)
+        cl = O.C4Client(op, 71, keygen_parts=True)
+        mods = op.q[:2]
+        plain = lambda i: O.c4_db_plaintext(db_seed, i, op)  # noqa: E731
+    gc = PirClient(gp, cl.secret())
+    bv, gsw = gc.create_session_keys(**cl.keygen)
+    srv = PirServer(gp)
+    srv.load_data_seeded(target, db_seed)
+    srv.set_client_keys(9, bv, gsw)
+    rng = np.random.default_rng(13)
+    idx = [int(x) for x in rng.integers(0, target, n)]
+    a = _uniform(rng, mods, n, op.N).reshape((n,) + gp.ct_shape[1:])
+    e = np.rint(rng.normal(0.0, 3.2, (n, op.N))).astype(np.int64)
+    resp = srv.make_query_batch([9] * n, gc.fast_generate_query_batch(idx, a, e))
+    pt = gc.decrypt_mod_q_batch(resp)
+    for k, i in enumerate(idx):
+        assert np.array_equal(pt[k], plain(i))
