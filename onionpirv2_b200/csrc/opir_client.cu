@@ -1149,7 +1149,9 @@ opir_status opir_client_create(const opir_params *params, const int8_t *secret, 
        "twiddle upload");
   });
   if (st != OPIR_OK) {
-    delete c;
+    // device resources exist once the event does; release them on their device
+    if (c->staged) opir_client_destroy(c);
+    else delete c;
     return st;
   }
   *out = c;
