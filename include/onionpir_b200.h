@@ -556,6 +556,18 @@ opir_status opir_client_keygen_device(opir_client *client, const uint64_t *d_bv_
                                       const int64_t *d_gsw_e, uint64_t *d_bv_keys,
                                       uint64_t *d_gsw_key, void *stream);
 
+/* The same three calls on host arrays (same layouts and meaning, without the
+ * d_ prefix), run on the handle's own stream; each returns once its results
+ * are in host memory. max_noise may be NULL. */
+opir_status opir_client_generate_queries(opir_client *client, uint32_t n, const uint64_t *pt_idx,
+                                         const uint64_t *a, const int64_t *e,
+                                         uint64_t *queries);
+opir_status opir_client_decrypt(opir_client *client, uint32_t n, const uint64_t *responses,
+                                uint64_t *plaintexts, uint64_t *max_noise);
+opir_status opir_client_keygen(opir_client *client, const uint64_t *bv_a, const int64_t *bv_e,
+                               const uint64_t *gsw_a, const int64_t *gsw_e, uint64_t *bv_keys,
+                               uint64_t *gsw_key);
+
 /* ---- tree PIR level selection ------------------------------------------
  * The full-binary-tree PIR layer of the reference (src/tree_index.cpp,
  * src/tree_query.cpp, src/tree_select.cpp): levels 0..L of a tree with

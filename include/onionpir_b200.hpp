@@ -14,6 +14,7 @@
 // OPIR_ERR_NO_MEMORY -> std::bad_alloc, anything else -> std::runtime_error.
 #pragma once
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <exception>
@@ -473,6 +474,124 @@ class PirServer {
   std::map<size_t, GSWCt> pending_gsw_;
   std::map<size_t, SharedPirSessionKeys> sessions_;
   std::unordered_map<size_t, RlwePt> recorded_pts_;
+};
+
+// ------------------------------------------------------------- client
+// The GPU forms of PirClient's steps that scale with queries, responses and
+// sessions (client.cpp:25-225, 364-410) for one client's secret. The
+// randomness the reference client draws from its own generators (each
+// query's uniform c1 and error, each key row's uniform part and error) is
+// passed in, so results equal the reference client's for the same draws.
+class GpuPirClient {
+ public:
+  // secret: the coefficient form of the client's RlweSk, N values in {-1, 0, 1}.
+  GpuPirClient(const PirParams &pir_params, const std::vector<int8_t> &secret, int device = 0)
+      : params_(pir_params) {
+    if (secret.size() != pir_params.get_poly_degree())
+      throw std::invalid_argument("GpuPirClient: the secret holds N coefficients");
+    opir_client *h = nullptr;
+    detail::check(opir_client_create(&pir_params.raw(), secret.data(), device, &h),
+                  "GpuPirClient::GpuPirClient");
+    h_.reset(h);
+  }
+
+  // fast_generate_query (client.cpp:107-225): c1 = a (K*N, limb-major),
+  // c0 = -(a s + e) plus the packed plaintext.
+  RlweCt fast_generate_query(size_t pt_idx, const std::vector<uint64_t> &a,
+                             const std::vector<int64_t> &e) {
+    return std::move(fast_generate_queries({pt_idx}, a, e).front());
+  }
+  // n queries at once: a is n x K*N, e is n x N.
+  std::vector<RlweCt> fast_generate_queries(const std::vector<size_t> &pt_idx,
+                                            const std::vector<uint64_t> &a,
+                                            const std::vector<int64_t> &e) {
+    const size_t n = pt_idx.size(), kn = params_.get_coeff_val_cnt();
+    if (a.size() != n * kn || e.size() != n * params_.get_poly_degree())
+      throw std::invalid_argument("GpuPirClient: a holds n x K*N and e n x N values");
+    const std::vector<uint64_t> idx(pt_idx.begin(), pt_idx.end());
+    std::vector<uint64_t> q(std::max<size_t>(1, n * 2 * kn));
+    status(opir_client_generate_queries(h_.get(), static_cast<uint32_t>(n), idx.data(), a.data(),
+                                        e.data(), q.data()),
+           "GpuPirClient::fast_generate_query");
+    std::vector<RlweCt> out(n);
+    for (size_t i = 0; i < n; ++i) {
+      out[i].c0.assign(q.begin() + i * 2 * kn, q.begin() + i * 2 * kn + kn);
+      out[i].c1.assign(q.begin() + i * 2 * kn + kn, q.begin() + (i + 1) * 2 * kn);
+    }
+    return out;
+  }
+
+  // decrypt_mod_q (client.cpp:364-410) of a response as
+  // load_resp_from_stream yields it (2 x N values below small_q).
+  RlwePt decrypt_mod_q(const RlweCt &ct) { return std::move(decrypt_mod_q_batch({ct}).front()); }
+  // n responses; *max_noise (optional) receives each one's max noise, the
+  // figure the reference prints as its noise budget (client.cpp:389-407).
+  std::vector<RlwePt> decrypt_mod_q_batch(const std::vector<RlweCt> &cts,
+                                          std::vector<uint64_t> *max_noise = nullptr) {
+    const size_t n = cts.size(), N = params_.get_poly_degree();
+    std::vector<uint64_t> in(std::max<size_t>(1, n * 2 * N)), pt(std::max<size_t>(1, n * N));
+    for (size_t i = 0; i < n; ++i) {
+      if (cts[i].c0.size() != N || cts[i].c1.size() != N)
+        throw std::invalid_argument("GpuPirClient: a response holds 2 x N values");
+      std::copy(cts[i].c0.begin(), cts[i].c0.end(), in.begin() + i * 2 * N);
+      std::copy(cts[i].c1.begin(), cts[i].c1.end(), in.begin() + i * 2 * N + N);
+    }
+    if (max_noise) max_noise->assign(std::max<size_t>(1, n), 0);
+    status(opir_client_decrypt(h_.get(), static_cast<uint32_t>(n), in.data(), pt.data(),
+                               max_noise ? max_noise->data() : nullptr),
+           "GpuPirClient::decrypt_mod_q");
+    if (max_noise) max_noise->resize(n);
+    std::vector<RlwePt> out(n);
+    for (size_t i = 0; i < n; ++i) out[i].data.assign(pt.begin() + i * N, pt.begin() + (i + 1) * N);
+    return out;
+  }
+
+  // create_session_keys (client.cpp:40-45): the BV keys for galois_k =
+  // N/2^i + 1, i < h (bv_a h*L_KS x K*N, bv_e h*L_KS x N) and RGSW(s)
+  // (gsw_a 2 L_KEY x K*N, gsw_e 2 L_KEY x N), NTT form.
+  PirSessionKeys create_session_keys(const std::vector<uint64_t> &bv_a,
+                                     const std::vector<int64_t> &bv_e,
+                                     const std::vector<uint64_t> &gsw_a,
+                                     const std::vector<int64_t> &gsw_e) {
+    const opir_params &p = params_.raw();
+    const size_t kn = params_.get_coeff_val_cnt(), N = params_.get_poly_degree();
+    const size_t bv_rows = static_cast<size_t>(p.expansion_height) * p.l_ks;
+    const size_t gsw_rows = 2ull * p.l_key;
+    if (bv_a.size() != bv_rows * kn || bv_e.size() != bv_rows * N ||
+        gsw_a.size() != gsw_rows * kn || gsw_e.size() != gsw_rows * N)
+      throw std::invalid_argument("GpuPirClient: key randomness of the wrong size");
+    std::vector<uint64_t> bv(std::max<size_t>(1, bv_rows * 2 * kn)), g(gsw_rows * 2 * kn);
+    status(opir_client_keygen(h_.get(), bv_rows ? bv_a.data() : nullptr,
+                              bv_rows ? bv_e.data() : nullptr, gsw_a.data(), gsw_e.data(),
+                              bv_rows ? bv.data() : nullptr, g.data()),
+           "GpuPirClient::create_session_keys");
+    PirSessionKeys keys;
+    for (uint32_t i = 0; i < p.expansion_height; ++i) {
+      bvks::BvKeySwitchKey key;
+      key.galois_k = (p.poly_degree >> i) + 1;
+      for (uint32_t r = 0; r < p.l_ks; ++r) {
+        const auto row = bv.begin() + (static_cast<size_t>(i) * p.l_ks + r) * 2 * kn;
+        key.cts.push_back(bvks::BvRlweCt{std::vector<uint64_t>(row + kn, row + 2 * kn),
+                                         std::vector<uint64_t>(row, row + kn)});
+      }
+      keys.bv_galois_keys.keys.push_back(std::move(key));
+    }
+    for (size_t r = 0; r < gsw_rows; ++r)
+      keys.gsw_key.emplace_back(g.begin() + r * 2 * kn, g.begin() + (r + 1) * 2 * kn);
+    return keys;
+  }
+
+ private:
+  struct Deleter {
+    void operator()(opir_client *h) const { opir_client_destroy(h); }
+  };
+  void status(opir_status st, const char *what) const {
+    if (st != OPIR_OK)
+      detail::raise(st, std::string(what) + ": " + opir_client_last_error(h_.get()));
+  }
+
+  PirParams params_;
+  std::unique_ptr<opir_client, Deleter> h_;
 };
 
 }  // namespace onionpir_b200

@@ -74,77 +74,54 @@ class PirClient:
             self._h, p(d_bv_a), p(d_bv_e), p(d_gsw_a), p(d_gsw_e), p(d_bv_keys), p(d_gsw_key),
             p(stream)))
 
-    # ---- host form (torch moves the buffers) -------------------------------
+    # ---- host form (the C ABI's host-buffer calls) ---------------------------
     def create_session_keys(self, bv_a: np.ndarray, bv_e: np.ndarray, gsw_a: np.ndarray,
                             gsw_e: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
         """The BV keys (h, L_KS) + ct_shape and the RGSW key (2 L_KEY,) +
         ct_shape from the uniform parts (coefficient form, limb-major per
         row) and errors the reference's generators would draw."""
-        import torch
         P = self.params
         h, lks, lkey, N = P.expansion_height, P.l_ks, P.l_key, P.N
         cs = P.ct_shape
-        dev = torch.device("cuda", self.device)
-
-        def up(x, dt, shape):
-            x = np.ascontiguousarray(x, dtype=dt).reshape(shape)
-            t = torch.from_numpy(x.view(np.int64) if dt == np.uint64 else x)
-            return t.to(dev)
-
-        da_bv = up(bv_a, np.uint64, (h, lks) + cs[1:]) if h else None
-        de_bv = up(bv_e, np.int64, (h, lks, N)) if h else None
-        da_g = up(gsw_a, np.uint64, (2 * lkey,) + cs[1:])
-        de_g = up(gsw_e, np.int64, (2 * lkey, N))
-        bv = torch.empty((h, lks) + cs, dtype=torch.int64, device=dev) if h else None
-        gsw = torch.empty((2 * lkey,) + cs, dtype=torch.int64, device=dev)
-        stream = torch.cuda.current_stream(dev)
-        ptr = lambda t: t.data_ptr() if t is not None else 0  # noqa: E731
-        self.keygen_device(ptr(da_bv), ptr(de_bv), da_g.data_ptr(), de_g.data_ptr(), ptr(bv),
-                           gsw.data_ptr(), stream.cuda_stream)
-        bv_h = bv.cpu().numpy().view(np.uint64) if h else np.zeros((0, lks) + cs, np.uint64)
-        return bv_h, gsw.cpu().numpy().view(np.uint64)
+        ba = np.ascontiguousarray(bv_a, dtype=np.uint64).reshape((h * lks,) + cs[1:]) if h else None
+        be = np.ascontiguousarray(bv_e, dtype=np.int64).reshape(h * lks, N) if h else None
+        ga = np.ascontiguousarray(gsw_a, dtype=np.uint64).reshape((2 * lkey,) + cs[1:])
+        ge = np.ascontiguousarray(gsw_e, dtype=np.int64).reshape(2 * lkey, N)
+        bv = np.zeros((h, lks) + cs, np.uint64)
+        gsw = np.zeros((2 * lkey,) + cs, np.uint64)
+        self._check(self._lib.opir_client_keygen(
+            self._h, _ptr(ba) if h else None, _ptr(be, C.c_int64) if h else None, _ptr(ga),
+            _ptr(ge, C.c_int64), _ptr(bv) if h else None, _ptr(gsw)))
+        return bv, gsw
 
     def fast_generate_query_batch(self, pt_idx: Sequence[int], a: np.ndarray,
                                   e: np.ndarray) -> np.ndarray:
         """Queries for pt_idx with c1 = a[i] and error e[i]: (n,) + ct_shape."""
-        import torch
-        idx = np.asarray(pt_idx, dtype=np.uint64).reshape(-1)
+        idx = np.ascontiguousarray(np.asarray(pt_idx, dtype=np.uint64).reshape(-1))
         n = idx.size
         cs = self.params.ct_shape
         a = np.ascontiguousarray(a, dtype=np.uint64).reshape((n,) + cs[1:])
         e = np.ascontiguousarray(e, dtype=np.int64).reshape(n, self.params.N)
-        dev = torch.device("cuda", self.device)
-        da = torch.from_numpy(a.view(np.int64)).to(dev)
-        de = torch.from_numpy(e).to(dev)
-        dq = torch.empty((n,) + cs, dtype=torch.int64, device=dev)
-        stream = torch.cuda.current_stream(dev)
-        self.generate_queries_device(idx, da.data_ptr(), de.data_ptr(), dq.data_ptr(),
-                                     stream.cuda_stream)
-        return dq.cpu().numpy().view(np.uint64)
+        out = np.zeros((n,) + cs, np.uint64)
+        self._check(self._lib.opir_client_generate_queries(
+            self._h, n, _ptr(idx), _ptr(a), _ptr(e, C.c_int64), _ptr(out)))
+        return out
 
     def fast_generate_query(self, pt_idx: int, a: np.ndarray, e: np.ndarray) -> np.ndarray:
         return self.fast_generate_query_batch([pt_idx], a[None], e[None])[0]
 
-    def decrypt_mod_q_batch(self, responses: np.ndarray,
-                            with_noise: bool = False):
+    def decrypt_mod_q_batch(self, responses: np.ndarray, with_noise: bool = False):
         """Plaintexts (n, N) of responses (n, 2, N); with_noise adds each
         response's max noise."""
-        import torch
+        N = self.params.N
         r = np.ascontiguousarray(responses, dtype=np.uint64)
         n = r.shape[0]
-        N = self.params.N
         r = r.reshape(n, 2, N)
-        dev = torch.device("cuda", self.device)
-        dr = torch.from_numpy(r.view(np.int64)).to(dev)
-        dp = torch.empty((n, N), dtype=torch.int64, device=dev)
-        dn = torch.empty(n, dtype=torch.int64, device=dev) if with_noise else None
-        stream = torch.cuda.current_stream(dev)
-        self.decrypt_device(n, dr.data_ptr(), dp.data_ptr(), dn.data_ptr() if with_noise else 0,
-                            stream.cuda_stream)
-        pt = dp.cpu().numpy().view(np.uint64)
-        if with_noise:
-            return pt, dn.cpu().numpy().view(np.uint64)
-        return pt
+        pt = np.zeros((n, N), np.uint64)
+        noise = np.zeros(n, np.uint64) if with_noise else None
+        self._check(self._lib.opir_client_decrypt(
+            self._h, n, _ptr(r), _ptr(pt), _ptr(noise) if with_noise else None))
+        return (pt, noise) if with_noise else pt
 
     def decrypt_mod_q(self, response: np.ndarray) -> np.ndarray:
         return self.decrypt_mod_q_batch(np.asarray(response)[None])[0]

@@ -639,6 +639,10 @@ struct opir_client {
   DevBuf<uint64_t> pk_idx;
   uint64_t *idx_staging = nullptr;   // pinned copy of the last call's indices
   size_t idx_staging_cap = 0;
+  // host-buffer calls: the handle's stream and device copies of their buffers
+  cudaStream_t io_stream = nullptr;
+  DevBuf<uint64_t> io_u0, io_u1, io_out, io_noise;
+  DevBuf<int64_t> io_e0, io_e1;
   uint32_t nconst = 1;       // constant slots per query
   uint64_t one_val[2]{};     // the one-hot's value per limb
   std::vector<uint64_t> gadget_val;  // [k][limb]: B^(L_EP-1-k) (2^h)^-1 mod q_limb
@@ -1079,6 +1083,28 @@ void forward_ntt_polys(uint64_t *d_polys, uint64_t count, const opir_params &p,
 
 }  // namespace opir
 
+// Helpers of the host-buffer calls.
+namespace {
+
+template <typename T>
+T *upload(DevBuf<T> &buf, const T *host, size_t count, cudaStream_t st) {
+  buf.alloc(std::max<size_t>(count, 1));
+  if (count)
+    ck(cudaMemcpyAsync(buf.p, host, count * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
+  return buf.p;
+}
+
+void ensure_io_stream(opir_client &c) {
+  if (!c.io_stream) ck(cudaStreamCreateWithFlags(&c.io_stream, cudaStreamNonBlocking), "client stream");
+}
+
+void download(void *host, const void *dev, size_t bytes, cudaStream_t st) {
+  ck(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st), "download");
+  ck(cudaStreamSynchronize(st), "client call");
+}
+
+}  // namespace
+
 extern "C" {
 
 opir_status opir_client_create(const opir_params *params, const int8_t *secret, int device,
@@ -1183,6 +1209,13 @@ void opir_client_destroy(opir_client *c) {
     c->consts.reset();
     if (c->staging) cudaFreeHost(c->staging);
     if (c->staged) cudaEventDestroy(c->staged);
+    c->io_u0.reset();
+    c->io_u1.reset();
+    c->io_out.reset();
+    c->io_noise.reset();
+    c->io_e0.reset();
+    c->io_e1.reset();
+    if (c->io_stream) cudaStreamDestroy(c->io_stream);
     if (prev >= 0) cudaSetDevice(prev);
   }
   delete c;
@@ -1295,6 +1328,95 @@ opir_status opir_client_keygen_device(opir_client *c, const uint64_t *d_bv_a,
        "key row upload");
     launch_keygen(*c, rows, d_bv_keys, static_cast<uint64_t>(h) * p.l_ks * 2 * K, d_gsw_key,
                   2ull * p.l_key * 2 * K, st);
+  });
+}
+
+// ---- host-buffer forms: the same calls on host arrays (same layouts), on
+// the handle's own stream; each returns when its results are in host memory.
+
+opir_status opir_client_generate_queries(opir_client *c, uint32_t n, const uint64_t *pt_idx,
+                                         const uint64_t *a, const int64_t *e,
+                                         uint64_t *queries) {
+  if (!c) return OPIR_ERR_INVALID_ARGUMENT;
+  if (n == 0) return OPIR_OK;
+  const size_t kn = static_cast<size_t>(c->limbs) * c->n;
+  opir_status st = client_guarded(c, [&] {
+    if (!pt_idx || !a || !e || !queries) throw std::invalid_argument("null buffer");
+    DeviceGuard g(c->device);
+    ensure_io_stream(*c);
+    upload(c->io_u0, a, n * kn, c->io_stream);
+    upload(c->io_e0, e, static_cast<size_t>(n) * c->n, c->io_stream);
+    c->io_out.alloc(n * 2 * kn);
+  });
+  if (st != OPIR_OK) return st;
+  st = opir_client_generate_queries_device(c, n, pt_idx, c->io_u0.p, c->io_e0.p, c->io_out.p,
+                                           c->io_stream);
+  if (st != OPIR_OK) return st;
+  return client_guarded(c, [&] {
+    DeviceGuard g(c->device);
+    download(queries, c->io_out.p, n * 2 * kn * sizeof(uint64_t), c->io_stream);
+  });
+}
+
+opir_status opir_client_decrypt(opir_client *c, uint32_t n, const uint64_t *responses,
+                                uint64_t *plaintexts, uint64_t *max_noise) {
+  if (!c) return OPIR_ERR_INVALID_ARGUMENT;
+  if (n == 0) return OPIR_OK;
+  opir_status st = client_guarded(c, [&] {
+    if (!responses || !plaintexts) throw std::invalid_argument("null buffer");
+    DeviceGuard g(c->device);
+    ensure_io_stream(*c);
+    upload(c->io_u0, responses, static_cast<size_t>(n) * 2 * c->n, c->io_stream);
+    c->io_out.alloc(static_cast<size_t>(n) * c->n);
+    if (max_noise) c->io_noise.alloc(n);
+  });
+  if (st != OPIR_OK) return st;
+  st = opir_client_decrypt_device(c, n, c->io_u0.p, c->io_out.p, max_noise ? c->io_noise.p : nullptr,
+                                  c->io_stream);
+  if (st != OPIR_OK) return st;
+  return client_guarded(c, [&] {
+    DeviceGuard g(c->device);
+    if (max_noise)
+      ck(cudaMemcpyAsync(max_noise, c->io_noise.p, n * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                         c->io_stream),
+         "download");
+    download(plaintexts, c->io_out.p, static_cast<size_t>(n) * c->n * sizeof(uint64_t),
+             c->io_stream);
+  });
+}
+
+opir_status opir_client_keygen(opir_client *c, const uint64_t *bv_a, const int64_t *bv_e,
+                               const uint64_t *gsw_a, const int64_t *gsw_e, uint64_t *bv_keys,
+                               uint64_t *gsw_key) {
+  if (!c) return OPIR_ERR_INVALID_ARGUMENT;
+  const opir_params &p = c->params;
+  const size_t kn = static_cast<size_t>(c->limbs) * c->n;
+  const size_t bv_rows = static_cast<size_t>(p.expansion_height) * p.l_ks;
+  const size_t gsw_rows = 2ull * p.l_key;
+  opir_status st = client_guarded(c, [&] {
+    if (bv_rows && (!bv_a || !bv_e || !bv_keys)) throw std::invalid_argument("null BV buffer");
+    if (!gsw_a || !gsw_e || !gsw_key) throw std::invalid_argument("null RGSW buffer");
+    DeviceGuard g(c->device);
+    ensure_io_stream(*c);
+    upload(c->io_u0, bv_a, bv_rows * kn, c->io_stream);
+    upload(c->io_e0, bv_e, bv_rows * c->n, c->io_stream);
+    upload(c->io_u1, gsw_a, gsw_rows * kn, c->io_stream);
+    upload(c->io_e1, gsw_e, gsw_rows * c->n, c->io_stream);
+    c->io_out.alloc((bv_rows + gsw_rows) * 2 * kn);
+  });
+  if (st != OPIR_OK) return st;
+  st = opir_client_keygen_device(c, bv_rows ? c->io_u0.p : nullptr, bv_rows ? c->io_e0.p : nullptr,
+                                 c->io_u1.p, c->io_e1.p, bv_rows ? c->io_out.p : nullptr,
+                                 c->io_out.p + bv_rows * 2 * kn, c->io_stream);
+  if (st != OPIR_OK) return st;
+  return client_guarded(c, [&] {
+    DeviceGuard g(c->device);
+    if (bv_rows)
+      ck(cudaMemcpyAsync(bv_keys, c->io_out.p, bv_rows * 2 * kn * sizeof(uint64_t),
+                         cudaMemcpyDeviceToHost, c->io_stream),
+         "download");
+    download(gsw_key, c->io_out.p + bv_rows * 2 * kn, gsw_rows * 2 * kn * sizeof(uint64_t),
+             c->io_stream);
   });
 }
 

@@ -1,7 +1,8 @@
 """The C++ facade (include/onionpir_b200.hpp): it compiles self-contained
-with warnings as errors, and its parity program (tests/cpp/
-test_server_facade.cpp, written like the reference's test_pir.cpp) builds
-against the library and the oracle on CPU and passes on a GPU."""
+with warnings as errors, and its parity programs (tests/cpp/
+test_server_facade.cpp and test_client_facade.cpp, written like the
+reference's test_pir.cpp) build against the library and the oracle on CPU and
+pass on a GPU."""
 import os
 import shutil
 import subprocess
@@ -18,12 +19,12 @@ CXX = shutil.which("g++")
 pytestmark = pytest.mark.skipif(CXX is None, reason="no C++ compiler")
 
 
-def build(tmp_path) -> str:
+def build(tmp_path, name: str = "test_server_facade") -> str:
     O.build()
-    exe = str(tmp_path / "test_server_facade")
+    exe = str(tmp_path / name)
     subprocess.run([CXX, "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror",
                     "-I", os.path.join(ROOT, "include"), "-I", ORACLE,
-                    os.path.join(ROOT, "tests", "cpp", "test_server_facade.cpp"),
+                    os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
                     "-L", PKG, "-lonionpir_b200", "-L", ORACLE, "-lopir_oracle",
                     f"-Wl,-rpath,{PKG}:{ORACLE}", "-o", exe], check=True)
     return exe
@@ -45,6 +46,18 @@ def test_parity_program_builds(tmp_path):
 @pytest.mark.gpu
 def test_parity_program_passes(tmp_path):
     exe = build(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-4000:]
+    assert r.stdout.strip().endswith("ok")
+
+
+def test_client_parity_program_builds(tmp_path):
+    assert os.path.exists(build(tmp_path, "test_client_facade"))
+
+
+@pytest.mark.gpu
+def test_client_parity_program_passes(tmp_path):
+    exe = build(tmp_path, "test_client_facade")
     r = subprocess.run([exe], capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stderr[-4000:]
     assert r.stdout.strip().endswith("ok")
