@@ -662,6 +662,18 @@ opir_status opir_tree_set_client_keys(opir_tree *tree, uint64_t client_id,
 opir_status opir_tree_query(opir_tree *tree, uint64_t client_id, const uint64_t *query,
                             uint64_t *selected);
 
+/* make_tree_query (src/tree_query.cpp:142-196) for n client coordinates on
+ * the GPU, with a client handle (opir_client_create, any layout of the same
+ * parameter set) and the randomness given: per query alpha (< N0), `groups`
+ * selector bits (b beta bits, then r gamma bits, one byte each, n x groups),
+ * the uniform c1 a (K N) and the error e (N); queries: n ciphertexts in the
+ * opir_tree_query layout. Host arrays; returns when the queries are written. */
+opir_status opir_client_generate_tree_queries(opir_client *client, const opir_tree_params *tree,
+                                              uint32_t n, const uint64_t *alpha,
+                                              const uint8_t *bits, uint32_t groups,
+                                              const uint64_t *a, const int64_t *e,
+                                              uint64_t *queries);
+
 /* Library version string. */
 const char *opir_version(void);
 

@@ -148,6 +148,9 @@ _SIGS = {
     "opir_client_generate_queries": ([C.c_void_p, C.c_uint32, u64p, u64p,
                                       C.POINTER(C.c_int64), u64p], C.c_int),
     "opir_client_decrypt": ([C.c_void_p, C.c_uint32, u64p, u64p, u64p], C.c_int),
+    "opir_client_generate_tree_queries": ([C.c_void_p, C.POINTER(TreeParams), C.c_uint32, u64p,
+                                           u8p, C.c_uint32, u64p, C.POINTER(C.c_int64), u64p],
+                                          C.c_int),
     "opir_client_keygen": ([C.c_void_p, u64p, C.POINTER(C.c_int64), u64p,
                             C.POINTER(C.c_int64), u64p, u64p], C.c_int),
     "opir_ext_prod_mux_noalloc": ([C.POINTER(Params), C.c_uint32, C.c_void_p, C.c_void_p,

@@ -125,3 +125,23 @@ class PirClient:
 
     def decrypt_mod_q(self, response: np.ndarray) -> np.ndarray:
         return self.decrypt_mod_q_batch(np.asarray(response)[None])[0]
+
+    def make_tree_queries(self, tree, alpha: Sequence[int], bits: np.ndarray, a: np.ndarray,
+                          e: np.ndarray) -> np.ndarray:
+        """make_tree_query (tree_query.cpp:142-196) for n client coordinates:
+        alpha (n,), bits (n, b + r) beta then gamma bits, a (n,) + ct_shape[1:]
+        uniform c1, e (n, N) errors; returns (n,) + ct_shape."""
+        al = np.ascontiguousarray(np.asarray(alpha, dtype=np.uint64).reshape(-1))
+        n = al.size
+        bt = np.ascontiguousarray(np.asarray(bits, dtype=np.uint8).reshape(n, -1))
+        groups = bt.shape[1]
+        if groups == 0:
+            bt = np.zeros((n, 1), np.uint8)
+        cs = self.params.ct_shape
+        aa = np.ascontiguousarray(a, dtype=np.uint64).reshape((n,) + cs[1:])
+        ee = np.ascontiguousarray(e, dtype=np.int64).reshape(n, self.params.N)
+        out = np.zeros((n,) + cs, np.uint64)
+        self._check(self._lib.opir_client_generate_tree_queries(
+            self._h, C.byref(tree._t), n, _ptr(al), _ptr(bt, C.c_uint8), groups, _ptr(aa),
+            _ptr(ee, C.c_int64), _ptr(out)))
+        return out

@@ -776,6 +776,53 @@ void query_constants(const opir_client &c, uint64_t idx, ConstEntry *out) {
   }
 }
 
+// make_tree_query's plaintext constants (tree_query.cpp:70-140) for one
+// query, W = 2^h_q: the alpha one-hot as the BFV lift of W^-1 mod t at
+// BitRev(alpha, h_q) (add_bfv_query_constant), and for every set bit of group
+// g (b beta bits, then r gamma bits) the L_EP gadget rows times W^-1 mod q_k
+// at BitRev(N0 + g L_EP + row, h_q) (add_rlwe_star_constant).
+void tree_query_constants(const opir_client &c, uint64_t n0, uint32_t h_q, uint64_t alpha,
+                          const uint8_t *bits, uint32_t groups, ConstEntry *out) {
+  const opir_params &p = c.params;
+  const uint32_t nconst = 1 + groups * p.l_ep;
+  for (uint32_t u = 0; u < nconst; ++u) out[u] = ConstEntry{kNoPos, 0, {0, 0}};
+  const uint64_t t = p.plain_mod, W = 1ull << h_q;
+  uint64_t w_inv_t = 0;
+  if (!opir::invert_mod(W % t, t, w_inv_t)) throw std::invalid_argument("W is not invertible mod t");
+  out[0].pos = static_cast<uint32_t>(bitrev(alpha, h_q));
+  if (c.limbs == 1) {
+    const uint64_t q = c.mods[0];
+    out[0].val[0] = static_cast<uint64_t>(
+        ((static_cast<unsigned __int128>(q) * w_inv_t + (t >> 1)) / t) % q);
+  } else {
+    const unsigned __int128 Q = static_cast<unsigned __int128>(c.mods[0]) * c.mods[1];
+    const unsigned __int128 delta = Q / t;
+    const uint64_t rem = static_cast<uint64_t>(Q - delta * t);
+    const uint64_t rem_round =
+        static_cast<uint64_t>((static_cast<unsigned __int128>(rem) * w_inv_t + (t >> 1)) / t);
+    const unsigned __int128 scaled = delta * w_inv_t + rem_round;
+    for (uint32_t k = 0; k < 2; ++k) out[0].val[k] = static_cast<uint64_t>(scaled % c.mods[k]);
+  }
+  uint64_t w_inv_q[2] = {0, 0};
+  for (uint32_t m = 0; m < c.limbs; ++m)
+    if (!opir::invert_mod(W % c.mods[m], c.mods[m], w_inv_q[m]))
+      throw std::invalid_argument("W is not invertible mod q");
+  uint32_t at = 1;
+  for (uint32_t g = 0; g < groups; ++g) {
+    if (!bits[g]) continue;
+    for (uint32_t row = 0; row < p.l_ep; ++row) {
+      ConstEntry &ce = out[at++];
+      ce.pos = static_cast<uint32_t>(bitrev(n0 + static_cast<uint64_t>(g) * p.l_ep + row, h_q));
+      for (uint32_t m = 0; m < c.limbs; ++m) {
+        uint64_t gd = 1;  // B^(L_EP-1-row) mod q_m
+        for (uint32_t s2 = 0; s2 + 1 + row < p.l_ep; ++s2)
+          gd = static_cast<uint64_t>((static_cast<unsigned __int128>(gd) << p.base_log2) % c.mods[m]);
+        ce.val[m] = mulmod(gd, w_inv_q[m], c.mods[m]);
+      }
+    }
+  }
+}
+
 // Output slices per item so that a batch fills the GPU (index-list
 // product); R = n / (s kBlock) outputs per thread, at most kMaxR.
 constexpr uint32_t kMaxR = 8;
@@ -997,7 +1044,7 @@ void launch_decrypt(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, cons
 }
 
 void launch_pack(uint64_t items, cudaStream_t st, const uint64_t *a, const int64_t *e,
-                 const opir_client &c, uint64_t *out) {
+                 const opir_client &c, const ConstEntry *consts, uint32_t nconst, uint64_t *out) {
   const uint32_t n = c.n;
   const uint32_t ni = static_cast<uint32_t>(items);
   const uint32_t s = slices_for(items, n, c.sms);
@@ -1007,7 +1054,7 @@ void launch_pack(uint64_t items, cudaStream_t st, const uint64_t *a, const int64
 #define OPIR_PACK(RR)                                                                         \
   if (Rl == RR) {                                                                             \
     set_smem(k_client_pack<RR>, smem, "client pack smem");                                    \
-    k_client_pack<RR><<<grid, kBlock, smem, st>>>(a, e, c.consts.p, c.nconst, c.sidx.p,       \
+    k_client_pack<RR><<<grid, kBlock, smem, st>>>(a, e, consts, nconst, c.sidx.p,             \
                                                   c.npos, c.nneg, n, c.limbs, c.mods[0],      \
                                                   c.mods[1], out);                            \
     return launched("client pack launch");                                                    \
@@ -1262,7 +1309,8 @@ opir_status opir_client_generate_queries_device(opir_client *c, uint32_t n,
                        cudaMemcpyHostToDevice, st),
        "client constants upload");
     ck(cudaEventRecord(c->staged, st), "client staging record");
-    launch_pack(static_cast<uint64_t>(n) * c->limbs, st, d_a, d_e, *c, d_queries);
+    launch_pack(static_cast<uint64_t>(n) * c->limbs, st, d_a, d_e, *c, c->consts.p, c->nconst,
+                d_queries);
   });
 }
 
@@ -1417,6 +1465,57 @@ opir_status opir_client_keygen(opir_client *c, const uint64_t *bv_a, const int64
          "download");
     download(gsw_key, c->io_out.p + bv_rows * 2 * kn, gsw_rows * 2 * kn * sizeof(uint64_t),
              c->io_stream);
+  });
+}
+
+opir_status opir_client_generate_tree_queries(opir_client *c, const opir_tree_params *tree,
+                                              uint32_t n, const uint64_t *alpha,
+                                              const uint8_t *bits, uint32_t groups,
+                                              const uint64_t *a, const int64_t *e,
+                                              uint64_t *queries) {
+  if (!c) return OPIR_ERR_INVALID_ARGUMENT;
+  return client_guarded(c, [&] {
+    if (n == 0) return;
+    if (!tree || !alpha || (groups && !bits) || !a || !e || !queries)
+      throw std::invalid_argument("null buffer");
+    const opir_params &p = c->params;
+    const uint64_t n0 = tree->N0;
+    const uint32_t h_q = static_cast<uint32_t>(tree->h_q);
+    if ((1ull << h_q) > c->n || n0 + static_cast<uint64_t>(groups) * p.l_ep > (1ull << h_q))
+      throw std::invalid_argument("tree query shape does not fit the polynomial");
+    for (uint32_t i = 0; i < n; ++i)
+      if (alpha[i] >= n0) throw std::out_of_range("tree query alpha exceeds N0");
+    const uint32_t nconst = 1 + groups * p.l_ep;
+    const size_t count = static_cast<size_t>(n) * nconst;
+    const size_t kn = static_cast<size_t>(c->limbs) * c->n;
+    DeviceGuard g(c->device);
+    ensure_io_stream(*c);
+    cudaStream_t st = c->io_stream;
+    ck(cudaEventSynchronize(c->staged), "client staging wait");
+    if (c->staging_cap < count) {
+      if (c->staging) cudaFreeHost(c->staging);
+      c->staging = nullptr;
+      c->staging_cap = 0;
+      ck(cudaMallocHost(&c->staging, count * sizeof(ConstEntry)), "client staging");
+      c->staging_cap = count;
+    }
+    for (uint32_t i = 0; i < n; ++i)
+      tree_query_constants(*c, n0, h_q, alpha[i], bits + static_cast<size_t>(i) * groups, groups,
+                           c->staging + static_cast<size_t>(i) * nconst);
+    if (c->consts.n < count) {
+      ck(cudaStreamSynchronize(st), "client sync");
+      c->consts.alloc(count);
+    }
+    ck(cudaMemcpyAsync(c->consts.p, c->staging, count * sizeof(ConstEntry),
+                       cudaMemcpyHostToDevice, st),
+       "client constants upload");
+    ck(cudaEventRecord(c->staged, st), "client staging record");
+    upload(c->io_u0, a, n * kn, st);
+    upload(c->io_e0, e, static_cast<size_t>(n) * c->n, st);
+    c->io_out.alloc(n * 2 * kn);
+    launch_pack(static_cast<uint64_t>(n) * c->limbs, st, c->io_u0.p, c->io_e0.p, *c, c->consts.p,
+                nconst, c->io_out.p);
+    download(queries, c->io_out.p, n * 2 * kn * sizeof(uint64_t), st);
   });
 }
 

@@ -329,9 +329,6 @@ static void encrypt_zero_a(const opir_oracle_params *p, const uint64_t *sk, mt64
   for (uint32_t i = 0; i < N; ++i) c0[i] = submod(0, addmod(c0[i], e[i], q), q);
   free(e); free(a);
 }
-static void encrypt_zero(const opir_oracle_params *p, const uint64_t *sk, mt64 *g, uint64_t *ct) {
-  encrypt_zero_a(p, sk, g, NULL, ct, NULL);
-}
 
 /* bv_keyswitch.cpp:191-259 */
 /* cap_a / cap_e (may be NULL): each row's uniform a (coefficient form, N)
@@ -509,14 +506,15 @@ void oracle_client_secret(const oracle_client *c, int8_t *out) {
  * every set bit of group g (b beta bits, then r gamma bits) the L_EP data
  * gadget rows scaled by W^-1 mod q at BitRev(N0 + g L_EP + row, h_q)
  * (add_rlwe_star_constant, :113-140). */
-int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
-                             const uint8_t *bits, uint32_t groups, uint64_t *out) {
+static int client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                             const uint8_t *bits, uint32_t groups, const uint64_t *given_a,
+                             uint64_t *out, int64_t *e_out) {
   const opir_oracle_params *p = &c->p;
   const uint64_t q = p->q, t = p->t, W = 1ULL << h_q;
   if (h_q > 11 || alpha >= N0 || N0 + (uint64_t)groups * p->l_ep > W) return -1;
   uint64_t w_inv_t = 0, w_inv_q = 0, gd[64];
   if (!invmod(W % t, t, &w_inv_t) || !invmod(W % q, q, &w_inv_q)) return -1;
-  encrypt_zero(p, c->sk, &c->rng, out);
+  encrypt_zero_a(p, c->sk, &c->rng, given_a, out, e_out);
   const uint64_t rev = bitrev(alpha, h_q);
   const uint64_t scaled = (uint64_t)((((u128)q * w_inv_t) + (t >> 1)) / t) % q;
   out[rev] = (out[rev] + scaled) % q;
@@ -530,6 +528,15 @@ int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64
     }
   }
   return 0;
+}
+int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                             const uint8_t *bits, uint32_t groups, uint64_t *out) {
+  return client_tree_query(c, N0, h_q, alpha, bits, groups, NULL, out, NULL);
+}
+int oracle_client_tree_query_parts(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                                   const uint8_t *bits, uint32_t groups, const uint64_t *a,
+                                   uint64_t *out, int64_t *e_out) {
+  return client_tree_query(c, N0, h_q, alpha, bits, groups, a, out, e_out);
 }
 /* decrypt_rns (rlwe.cpp:310-348, K = 1): phase = c0 + c1 s mod q, then the
  * centred rescale q -> t per coefficient; ct coefficient form [c0][c1]. */

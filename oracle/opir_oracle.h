@@ -94,6 +94,10 @@ void oracle_client_secret(const oracle_client *c, int8_t *out);
  * then r gamma bits (little-endian coordinates), groups = b + r. */
 int oracle_client_tree_query(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
                              const uint8_t *bits, uint32_t groups, uint64_t *out);
+/* The same with c1 = a given (N), also returning the error drawn (N). */
+int oracle_client_tree_query_parts(oracle_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                                   const uint8_t *bits, uint32_t groups, const uint64_t *a,
+                                   uint64_t *out, int64_t *e_out);
 /* decrypt_rns (rlwe.cpp:310-348, K = 1) of a coefficient-form ciphertext. */
 void oracle_client_decrypt_q(const oracle_client *c, const uint64_t *ct, uint64_t *pt_out);
 void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp,
@@ -172,6 +176,9 @@ int oracle_c4_client_query(oracle_c4_client *c, uint64_t pt_idx, uint64_t *out);
  * oracle_client_tree_query; out: 4N u64 limb-major. */
 int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
                                 const uint8_t *bits, uint32_t groups, uint64_t *out);
+int oracle_c4_client_tree_query_parts(oracle_c4_client *c, uint64_t N0, uint32_t h_q,
+                                      uint64_t alpha, const uint8_t *bits, uint32_t groups,
+                                      const uint64_t *a, uint64_t *out, int64_t *e_out);
 /* Query with a given uniform c1 (2N, limb-major), returning the shared
  * error (N signed values); the secret in coefficient form (N in {-1,0,1}). */
 int oracle_c4_client_query_parts(oracle_c4_client *c, uint64_t pt_idx, const uint64_t *a,

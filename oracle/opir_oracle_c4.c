@@ -104,9 +104,6 @@ static void encrypt_zero_c4_a(const opir_oracle_c4_params *p, const uint64_t *sk
   }
   free(e); free(a);
 }
-static void encrypt_zero_c4(const opir_oracle_c4_params *p, const uint64_t *sk, mt64 *g, uint64_t *ct) {
-  encrypt_zero_c4_a(p, sk, g, NULL, ct, NULL);
-}
 
 /* bv_keyswitch.cpp:191-259 (K = 2): sigma_k(s) per limb (utils.cpp:74-82),
  * row i encrypts sigma_k(s) 2^(i base) under both limbs with per-limb
@@ -325,15 +322,16 @@ void oracle_c4_client_secret(const oracle_c4_client *c, int8_t *out) {
  * (b beta bits, then r gamma bits) the L_EP data gadget rows scaled by
  * W^-1 mod q_k, per limb, at BitRev(N0 + g L_EP + row, h_q)
  * (add_rlwe_star_constant, :113-140). */
-int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
-                                const uint8_t *bits, uint32_t groups, uint64_t *out) {
+static int c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                                const uint8_t *bits, uint32_t groups, const uint64_t *given_a,
+                                uint64_t *out, int64_t *e_out) {
   const opir_oracle_c4_params *p = &c->p;
   const uint32_t N = p->N;
   const uint64_t t = p->t, W = 1ULL << h_q;
   if (h_q > 12 || alpha >= N0 || N0 + (uint64_t)groups * p->l_ep > W) return -1;
   uint64_t w_inv_t = 0;
   if (!invmod(W % t, t, &w_inv_t)) return -1;
-  encrypt_zero_c4(p, c->sk, &c->rng, out);
+  encrypt_zero_c4_a(p, c->sk, &c->rng, given_a, out, e_out);
   const uint64_t rev = bitrev(alpha, h_q);
   const u128 Q = (u128)p->q[0] * p->q[1];
   const u128 Delta = Q / t;
@@ -361,6 +359,15 @@ int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, 
     }
   }
   return 0;
+}
+int oracle_c4_client_tree_query(oracle_c4_client *c, uint64_t N0, uint32_t h_q, uint64_t alpha,
+                                const uint8_t *bits, uint32_t groups, uint64_t *out) {
+  return c4_client_tree_query(c, N0, h_q, alpha, bits, groups, NULL, out, NULL);
+}
+int oracle_c4_client_tree_query_parts(oracle_c4_client *c, uint64_t N0, uint32_t h_q,
+                                      uint64_t alpha, const uint8_t *bits, uint32_t groups,
+                                      const uint64_t *a, uint64_t *out, int64_t *e_out) {
+  return c4_client_tree_query(c, N0, h_q, alpha, bits, groups, a, out, e_out);
 }
 
 /* client.cpp:364-430 under small_q: s from limb 0, ternary re-mapped;

@@ -99,6 +99,10 @@ def lib():
         L.oracle_client_tree_query.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,
                                                C.POINTER(C.c_uint8), C.c_uint32, _u64p]
         L.oracle_client_decrypt_q.argtypes = [C.c_void_p, _u64p, _u64p]
+        L.oracle_client_tree_query_parts.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32,
+                                                     C.c_uint64, C.POINTER(C.c_uint8),
+                                                     C.c_uint32, _u64p, _u64p,
+                                                     C.POINTER(C.c_int64)]
         L.oracle_server_new.argtypes = [C.POINTER(Params)]
         L.oracle_server_new.restype = C.c_void_p
         L.oracle_server_free.argtypes = [C.c_void_p]
@@ -158,6 +162,10 @@ def lib():
         L.oracle_c4_client_tree_query.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32,
                                                   C.c_uint64, C.POINTER(C.c_uint8), C.c_uint32,
                                                   _u64p]
+        L.oracle_c4_client_tree_query_parts.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32,
+                                                        C.c_uint64, C.POINTER(C.c_uint8),
+                                                        C.c_uint32, _u64p, _u64p,
+                                                        C.POINTER(C.c_int64)]
         L.oracle_c4_server_new.argtypes = [P4]
         L.oracle_c4_server_new.restype = C.c_void_p
         L.oracle_c4_server_free.argtypes = [C.c_void_p]
@@ -287,6 +295,21 @@ class Client:
                                           ptr(out)) != 0:
             raise ValueError("tree query shape does not fit")
         return out
+
+    def tree_query_parts(self, N0: int, h_q: int, alpha: int, beta_bits, gamma_bits,
+                         a: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """tree_query with c1 = a, and the error it drew."""
+        bits = np.ascontiguousarray(np.asarray(list(beta_bits) + list(gamma_bits) or [0],
+                                               dtype=np.uint8))
+        groups = len(beta_bits) + len(gamma_bits)
+        out = np.zeros((2, self.p.N), dtype=np.uint64)
+        e = np.zeros(self.p.N, dtype=np.int64)
+        aa = np.ascontiguousarray(a, dtype=np.uint64)
+        if lib().oracle_client_tree_query_parts(self.h, N0, h_q, alpha, ptr(bits, C.c_uint8),
+                                                groups, ptr(aa), ptr(out),
+                                                ptr(e, C.c_int64)) != 0:
+            raise ValueError("tree query shape does not fit")
+        return out, e
 
     def decrypt_q(self, ct: np.ndarray) -> np.ndarray:
         """decrypt_rns (rlwe.cpp:310-348) of a coefficient-form ciphertext mod q."""
@@ -454,6 +477,20 @@ class C4Client:
         if lib().oracle_c4_client_query_parts(self.h, idx, ptr(aa), ptr(out),
                                               ptr(e, C.c_int64)) != 0:
             raise IndexError("plaintext index outside the layout")
+        return out, e
+
+    def tree_query_parts(self, N0: int, h_q: int, alpha: int, beta_bits, gamma_bits,
+                         a: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        bits = np.ascontiguousarray(np.asarray(list(beta_bits) + list(gamma_bits) or [0],
+                                               dtype=np.uint8))
+        groups = len(beta_bits) + len(gamma_bits)
+        out = np.zeros((2, 2, self.p.N), dtype=np.uint64)
+        e = np.zeros(self.p.N, dtype=np.int64)
+        aa = np.ascontiguousarray(a, dtype=np.uint64)
+        if lib().oracle_c4_client_tree_query_parts(self.h, N0, h_q, alpha, ptr(bits, C.c_uint8),
+                                                   groups, ptr(aa), ptr(out),
+                                                   ptr(e, C.c_int64)) != 0:
+            raise ValueError("tree query shape does not fit")
         return out, e
 
     def tree_query(self, N0: int, h_q: int, alpha: int, beta_bits, gamma_bits) -> np.ndarray:

@@ -212,3 +212,35 @@ def test_whole_client_pipeline_on_the_gpu(config, n):
     pt = gc.decrypt_mod_q_batch(resp)
     for k, i in enumerate(idx):
         assert np.array_equal(pt[k], plain(i))
+
+
+@pytest.mark.parametrize("config", ["k1", "c4"])
+def test_tree_queries_match_oracle(config):
+    """make_tree_query on the GPU equals the oracle client's for the same c1
+    and error, over the golden tree cases' coordinates and random leaves."""
+    from onionpirv2_b200 import tree as T
+    from tests import golden_cases as G
+    if config == "k1":
+        scheme, cases = PirParams(), G.cases_tree()
+        op = O.params(scheme.target_num_pt, scheme.expansion_height)
+        cl = O.Client(op, 55)
+        mods = [op.q]
+    else:
+        scheme, cases = PirParams(config=C4), G.cases_tree_c4()
+        op = O.c4_params(scheme.target_num_pt, scheme.expansion_height)
+        cl = O.C4Client(op, 55)
+        mods = op.q[:2]
+    gc = PirClient(scheme, cl.secret())
+    rng = np.random.default_rng(3)
+    for c in cases[:4]:
+        tree = T.make_tree_pir_params_for_scheme(c["L"], c["a"], scheme)
+        leaves = [c["leaf"]] + [int(x) for x in rng.integers(0, 1 << c["L"], 5)]
+        coords = [T.client_index(leaf, tree) for leaf in leaves]
+        bits = np.array([list(k.beta_bits_le) + list(k.gamma_bits_le) for k in coords],
+                        dtype=np.uint8)
+        a = _uniform(rng, mods, len(leaves), op.N).reshape((len(leaves),) + scheme.ct_shape[1:])
+        parts = [cl.tree_query_parts(tree.N0, tree.h_q, k.alpha, k.beta_bits_le,
+                                     k.gamma_bits_le, a[i]) for i, k in enumerate(coords)]
+        got = gc.make_tree_queries(tree, [k.alpha for k in coords], bits, a,
+                                   np.stack([e for _, e in parts]))
+        assert np.array_equal(got, np.stack([q for q, _ in parts])), c["name"]
