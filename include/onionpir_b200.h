@@ -532,7 +532,11 @@ opir_status opir_client_generate_queries_device(opir_client *client, uint32_t n,
  *                  PirClient::load_resp_from_stream yields (client.cpp:315-361)
  *   d_plaintexts : n x N u64 device array, each coefficient below t
  *   d_max_noise  : n u64 device array or NULL: the response's max noise
- *                  |phase - round(small_q m / t)| (client.cpp:389-407) */
+ *                  |phase - round(small_q m / t)| (client.cpp:389-407)
+ * Under CONFIG_N2048_K1_COMP batches of 32 or more run on the tensor cores
+ * (as do query batches of 32 or more in opir_client_generate_queries_device);
+ * those calls synchronise `stream` before returning, to read the bounded
+ * waits' error word of the tensor-core kernel. */
 opir_status opir_client_decrypt_device(opir_client *client, uint32_t n,
                                        const uint64_t *d_responses, uint64_t *d_plaintexts,
                                        uint64_t *d_max_noise, void *stream);
