@@ -975,19 +975,22 @@ def bench_client(args, world, rank, local):
     ms_dec = t_dec * 1e3 / args.steps
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     mhz = clocks.get("sm_mhz") or 1965.0
-    tensor_path = (not c4 and n >= 32 and os.environ.get("OPIR_CLIENT_TC", "1") != "0"
+    tensor_path = (n >= 32 and os.environ.get("OPIR_CLIENT_TC", "1") != "0"
                    and os.environ.get("OPIR_CLIENT_WINDOW", "1") != "0")
     if tensor_path:
-        # tcgen05 byte-plane scan: 4 A planes x 4 x planes of N x N per response
-        ops = n * 2 * N * N * 16
+        # tcgen05 byte-plane scans: 4 A planes x 4 x planes of N x N per response
+        # and scan (one scan mod small_q < 2^29; else two 25-bit halves of c1,
+        # each mod two primes: four scans)
+        scans = 1 if sq < (1 << 29) else 4
+        ops = n * scans * 2 * N * N * 16
         peaks = measured_peaks()
         bf16 = peaks.get("bf16_tflops")
         peak = 2 * bf16 if bf16 else 2 * 1590.0   # int8 dense = 2 x bf16 dense
         achieved = ops / (ms_dec / 1e3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
                 "frac": achieved / peak, "traffic": None,
-                "work": "2 N^2 x 16 byte-plane products per response (3 of them nonzero: "
-                        "one secret plane x three planes of a 22-bit c1)",
+                "work": f"{scans} scan(s) x 2 N^2 x 16 byte-plane products per response "
+                        "(one secret plane is nonzero)",
                 "peak_kind": ("2 x measured" if bf16 else "2 x fallback")
                              + " dense bf16 (int8 dense is twice bf16 on B200)"}
     else:

@@ -475,6 +475,74 @@ __global__ void __launch_bounds__(kBlock) k_client_tc_prep(const uint64_t *__res
   }
 }
 
+// Two-limb decryption (small_q < 2^50): x = c1 mod small_q splits into 25-bit
+// halves; A x_half < 2 N 2^25 <= 2^38 is exact from its residues mod two
+// primes P1 P2 > 2^38 (four scans). Planes [half][4][nr][n], sums [half][nr].
+__global__ void __launch_bounds__(kBlock) k_client_tc_prep_split(const uint64_t *__restrict__ resp,
+                                                                 uint32_t n, uint32_t nr,
+                                                                 uint64_t sq,
+                                                                 uint8_t *__restrict__ qpl,
+                                                                 uint64_t *__restrict__ colsum) {
+  __shared__ uint64_t part[2][kBlock / 32];
+  const uint64_t b = blockIdx.x;
+  const uint64_t *c1 = resp + b * 2 * n + n;
+  const uint64_t plane = static_cast<uint64_t>(nr) * n;
+  uint64_t sum[2] = {0, 0};
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const uint64_t x = c1[j] % sq;
+    const uint64_t h[2] = {x & ((1ull << 25) - 1), x >> 25};
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf) {
+      sum[hf] += h[hf];
+#pragma unroll
+      for (int pl = 0; pl < 4; ++pl)
+        qpl[(4ull * hf + pl) * plane + b * n + j] = static_cast<uint8_t>(h[hf] >> (8 * pl));
+    }
+  }
+#pragma unroll
+  for (int hf = 0; hf < 2; ++hf) {
+    for (int o = 16; o > 0; o >>= 1) sum[hf] += __shfl_xor_sync(0xFFFFFFFFu, sum[hf], o);
+    if ((threadIdx.x & 31) == 0) part[hf][threadIdx.x >> 5] = sum[hf];
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    uint64_t tot = 0;
+    for (int w = 0; w < kBlock / 32; ++w) tot += part[threadIdx.x][w];
+    colsum[static_cast<uint64_t>(threadIdx.x) * nr + b] = tot;
+  }
+}
+
+// pt from the four scans ax [half][prime][nr][n]: u_half = CRT(mod P1, mod
+// P2) = A x_half exactly, y = (u_lo - sum_lo) + 2^25 (u_hi - sum_hi) = c1 s
+// (|y| < 2^62), then the decryption epilogue on y mod small_q.
+__global__ void __launch_bounds__(kBlock) k_client_tc_finish_split(
+    const uint64_t *__restrict__ resp, const uint32_t *__restrict__ ax,
+    const uint64_t *__restrict__ colsum, uint32_t n, uint32_t nr, uint64_t p1, uint64_t p2,
+    uint64_t p1_inv_mod_p2, DecConst dc, uint64_t *__restrict__ pt,
+    unsigned long long *__restrict__ max_noise) {
+  const uint64_t b = blockIdx.x;
+  const uint64_t *c0 = resp + b * 2 * n;
+  const uint64_t plane = static_cast<uint64_t>(nr) * n;
+  uint64_t worst = 0;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    int64_t y[2];
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf) {
+      const uint64_t v1 = ax[(2ull * hf) * plane + b * n + i];
+      const uint64_t v2 = ax[(2ull * hf + 1) * plane + b * n + i];
+      const uint64_t v1m = v1 >= p2 ? v1 - p2 : v1;  // p1 < 2 p2
+      const uint64_t d = v2 >= v1m ? v2 - v1m : v2 + (p2 - v1m);
+      const uint64_t u = v1 + p1 * (d * p1_inv_mod_p2 % p2);
+      y[hf] = static_cast<int64_t>(u) - static_cast<int64_t>(colsum[static_cast<uint64_t>(hf) * nr + b]);
+    }
+    const int64_t v = y[0] + y[1] * (int64_t{1} << 25);
+    const int64_t r = v % static_cast<int64_t>(dc.sq);
+    const uint64_t prod = static_cast<uint64_t>(r < 0 ? r + static_cast<int64_t>(dc.sq) : r);
+    pt[b * n + i] = decrypt_coeff(prod, c0[i], dc, worst);
+  }
+  publish_noise(worst, max_noise);
+}
+
 // pt from the scan's (A x mod small_q), laid out [response][i].
 __global__ void __launch_bounds__(kBlock) k_client_tc_finish(
     const uint64_t *__restrict__ resp, const uint32_t *__restrict__ ax,
@@ -875,11 +943,13 @@ DecConst dec_const(const opir_params &p) {
 // The tensor-core form serves single-modulus decryption batches of at least
 // kTcMinResponses (OPIR_CLIENT_TC=0 turns it off).
 constexpr uint64_t kTcMinResponses = 32;
-bool tc_enabled(const opir_client &c, uint64_t items, uint64_t modulus_bound) {
+// any_limbs: decryption, whose modulus (small_q) is one prime for both sets.
+bool tc_enabled(const opir_client &c, uint64_t items, uint64_t modulus_bound,
+                bool any_limbs = false) {
   const char *v = std::getenv("OPIR_CLIENT_TC");
   if ((v && v[0] == '0') || !window_enabled()) return false;
-  return c.limbs == 1 && c.n % 128 == 0 && c.n <= 8192 && modulus_bound < (1ull << 29) &&
-         items >= kTcMinResponses;
+  return (any_limbs || c.limbs == 1) && c.n % 128 == 0 && c.n <= 8192 &&
+         modulus_bound < (1ull << 29) && items >= kTcMinResponses;
 }
 
 void ensure_secret_matrix(opir_client &c, cudaStream_t st) {
@@ -979,8 +1049,40 @@ void launch_pack_tc(uint64_t n_q, const uint64_t *pt_idx, cudaStream_t st, const
   check_scan_error(c, st, "client pack");
 }
 
+// The two primes of the split decryption (29-bit, product above 2^57).
+constexpr uint64_t kSplitP1 = 536813569, kSplitP2 = 536752129;
+
+void launch_decrypt_tc_split(uint64_t n_resp, cudaStream_t st, const uint64_t *resp,
+                             opir_client &c, uint64_t *pt, unsigned long long *noise) {
+  const uint32_t n = c.n, nr = static_cast<uint32_t>(n_resp);
+  ensure_secret_matrix(c, st);
+  if (c.tc_colsum.n < 2 * n_resp) {
+    ck(cudaStreamSynchronize(st), "client sync");
+    c.tc_q.alloc(8ull * n_resp * n);
+    c.tc_colsum.alloc(2 * n_resp);
+    c.tc_ax.alloc(4 * n_resp * n);
+  }
+  uint64_t inv = 0;
+  if (!opir::invert_mod(kSplitP1 % kSplitP2, kSplitP2, inv)) throw std::runtime_error("split primes");
+  ck(cudaMemsetAsync(c.tc_err.p, 0, sizeof(uint32_t), st), "scan error reset");
+  k_client_tc_prep_split<<<nr, kBlock, 0, st>>>(resp, n, nr, c.params.small_q, c.tc_q.p,
+                                                c.tc_colsum.p);
+  launched("client prep launch");
+  const uint64_t plane_set = 4ull * n_resp * n, out = n_resp * n;
+  for (int hf = 0; hf < 2; ++hf)
+    for (int pr = 0; pr < 2; ++pr)
+      scan_secret_matrix(c, nr, pr ? kSplitP2 : kSplitP1, c.tc_q.p + hf * plane_set,
+                         c.tc_ax.p + (2 * hf + pr) * out, st);
+  k_client_tc_finish_split<<<nr, kBlock, 0, st>>>(resp, c.tc_ax.p, c.tc_colsum.p, n, nr, kSplitP1,
+                                                  kSplitP2, inv, dec_const(c.params), pt, noise);
+  launched("client finish launch");
+  check_scan_error(c, st, "client decrypt");
+}
+
 void launch_decrypt_tc(uint64_t n_resp, cudaStream_t st, const uint64_t *resp, opir_client &c,
                        uint64_t *pt, unsigned long long *noise) {
+  if (c.params.small_q >= (1ull << 29))
+    return launch_decrypt_tc_split(n_resp, st, resp, c, pt, noise);
   const uint32_t n = c.n, nr = static_cast<uint32_t>(n_resp);
   const uint64_t sq = c.params.small_q;
   ensure_secret_matrix(c, st);
@@ -1327,7 +1429,8 @@ opir_status opir_client_decrypt_device(opir_client *c, uint32_t n, const uint64_
       ck(cudaMemsetAsync(d_max_noise, 0, static_cast<size_t>(n) * sizeof(uint64_t), st),
          "noise reset");
     auto *noise = reinterpret_cast<unsigned long long *>(d_max_noise);
-    if (tc_enabled(*c, n, c->params.small_q))
+    const uint64_t sq = c->params.small_q;
+    if (tc_enabled(*c, n, sq < (1ull << 29) ? sq : 0, true) && sq < (1ull << 50))
       launch_decrypt_tc(n, st, d_responses, *c, d_plaintexts, noise);
     else
       launch_decrypt(n, st, d_responses, *c, d_plaintexts, noise);
