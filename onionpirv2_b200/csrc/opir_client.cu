@@ -602,8 +602,8 @@ struct PackLayout {
   uint64_t n0, other;      // first-dimension size, rows
   uint32_t num_dims, h;    // dimensions, expansion height
   uint32_t l_ep, pad;
-  uint64_t one;            // the one-hot's value (single modulus)
-  uint64_t gadget[16];     // B^(L_EP-1-k) (2^h)^-1 mod q
+  uint64_t one[2];         // the one-hot's value per limb
+  uint64_t gadget[16][2];  // B^(L_EP-1-k) (2^h)^-1 mod q_limb
 };
 
 __device__ __forceinline__ uint32_t bitrev_dev(uint64_t x, uint32_t bits) {
@@ -663,17 +663,108 @@ __global__ void __launch_bounds__(kBlock) k_client_tc_pack_finish(
     uint64_t val;
     if (u == 0) {
       pos = bitrev_dev(idx % L.n0, L.h);
-      val = L.one;
+      val = L.one[0];
     } else {
       const uint32_t i = 1 + (u - 1) / L.l_ep, k = (u - 1) % L.l_ep;
       if (!selector_bit(L, idx, i)) continue;
       pos = bitrev_dev(L.n0 + static_cast<uint64_t>(i - 1) * L.l_ep + k, L.h);
-      val = L.gadget[k];
+      val = L.gadget[k][0];
     }
     const uint64_t v = c0[pos] + val;
     c0[pos] = v >= q ? v - q : v;
   }
 }
+
+// Two-limb packing: every (query, limb) is one column x = a_limb mod q_limb
+// (< 2^60), split into 30-bit halves; A x_half < 2 N 2^30 <= 2^43 comes back
+// exactly from its residues mod P1 and P2. Planes [half][4][cols][n], sums
+// [half][cols], cols = queries x 2.
+__global__ void __launch_bounds__(kBlock) k_client_tc_pack_prep_split(
+    const uint64_t *__restrict__ a, uint32_t n, uint32_t cols, uint64_t q0, uint64_t q1,
+    uint8_t *__restrict__ qpl, uint64_t *__restrict__ colsum) {
+  __shared__ uint64_t part[2][kBlock / 32];
+  const uint64_t col = blockIdx.x;
+  const uint64_t q = (col & 1) ? q1 : q0;
+  const uint64_t *x = a + col * n;
+  const uint64_t plane = static_cast<uint64_t>(cols) * n;
+  uint64_t sum[2] = {0, 0};
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const uint64_t v = x[j] % q;
+    const uint64_t h[2] = {v & ((1ull << 30) - 1), v >> 30};
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf) {
+      sum[hf] += h[hf];
+#pragma unroll
+      for (int pl = 0; pl < 4; ++pl)
+        qpl[(4ull * hf + pl) * plane + col * n + j] = static_cast<uint8_t>(h[hf] >> (8 * pl));
+    }
+  }
+#pragma unroll
+  for (int hf = 0; hf < 2; ++hf) {
+    for (int o = 16; o > 0; o >>= 1) sum[hf] += __shfl_xor_sync(0xFFFFFFFFu, sum[hf], o);
+    if ((threadIdx.x & 31) == 0) part[hf][threadIdx.x >> 5] = sum[hf];
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    uint64_t tot = 0;
+    for (int w = 0; w < kBlock / 32; ++w) tot += part[threadIdx.x][w];
+    colsum[static_cast<uint64_t>(threadIdx.x) * cols + col] = tot;
+  }
+}
+
+// Query blockIdx.x: per limb k, a_k s = (A x_lo - sum_lo) + 2^30 (A x_hi -
+// sum_hi) (|.| < 2^73, 128-bit) mod q_k, c0 = -(a_k s + e) plus the constants
+// placed from the index, c1 = a.
+__global__ void __launch_bounds__(kBlock) k_client_tc_pack_finish_split(
+    const uint64_t *__restrict__ a, const int64_t *__restrict__ e,
+    const uint64_t *__restrict__ pt_idx, PackLayout L, const uint32_t *__restrict__ ax,
+    const uint64_t *__restrict__ colsum, uint32_t n, uint32_t cols, uint64_t p1, uint64_t p2,
+    uint64_t p1_inv_mod_p2, uint64_t q0, uint64_t q1, uint64_t *__restrict__ out) {
+  const uint64_t b = blockIdx.x;
+  const uint64_t plane = static_cast<uint64_t>(cols) * n;
+  uint64_t *c0 = out + b * 4 * n, *c1 = c0 + 2 * n;
+  const int64_t *eq = e + b * n;
+  for (uint32_t w = threadIdx.x; w < 2 * n; w += blockDim.x) {
+    const uint32_t k = w / n, i = w % n;
+    const uint64_t col = 2 * b + k, q = k ? q1 : q0;
+    __int128 y[2];
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf) {
+      const uint64_t v1 = ax[(2ull * hf) * plane + col * n + i];
+      const uint64_t v2 = ax[(2ull * hf + 1) * plane + col * n + i];
+      const uint64_t v1m = v1 >= p2 ? v1 - p2 : v1;
+      const uint64_t d = v2 >= v1m ? v2 - v1m : v2 + (p2 - v1m);
+      const uint64_t u = v1 + p1 * (d * p1_inv_mod_p2 % p2);
+      y[hf] = static_cast<__int128>(u) - static_cast<__int128>(colsum[static_cast<uint64_t>(hf) * cols + col]);
+    }
+    __int128 v = (y[0] + y[1] * (static_cast<__int128>(1) << 30)) % static_cast<__int128>(q);
+    if (v < 0) v += q;
+    c0[w] = pack_coeff(static_cast<uint64_t>(v), eq[i], q);
+    c1[w] = a[col * n + i];
+  }
+  __syncthreads();
+  const uint64_t idx = pt_idx[b];
+  const uint32_t nconst = 1 + (L.num_dims - 1) * L.l_ep;
+  for (uint32_t u = threadIdx.x; u < 2 * nconst; u += blockDim.x) {
+    const uint32_t k = u / nconst, cu = u % nconst;
+    const uint64_t q = k ? q1 : q0;
+    uint32_t pos;
+    uint64_t val;
+    if (cu == 0) {
+      pos = bitrev_dev(idx % L.n0, L.h);
+      val = L.one[k];
+    } else {
+      const uint32_t i = 1 + (cu - 1) / L.l_ep, r = (cu - 1) % L.l_ep;
+      if (!selector_bit(L, idx, i)) continue;
+      pos = bitrev_dev(L.n0 + static_cast<uint64_t>(i - 1) * L.l_ep + r, L.h);
+      val = L.gadget[r][k];
+    }
+    uint64_t *cell = c0 + static_cast<uint64_t>(k) * n + pos;
+    const uint64_t s2 = *cell + val;
+    *cell = s2 >= q ? s2 - q : s2;
+  }
+}
+
 
 uint64_t bitrev(uint64_t x, uint32_t bits) {
   uint64_t r = 0;
@@ -1002,17 +1093,24 @@ void check_scan_error(const opir_client &c, cudaStream_t st, const char *what) {
                                     std::to_string(err) + ")");
 }
 
+// The two primes of the split forms (29-bit, product above 2^57).
+constexpr uint64_t kSplitP1 = 536813569, kSplitP2 = 536752129;
+
 void launch_pack_tc(uint64_t n_q, const uint64_t *pt_idx, cudaStream_t st, const uint64_t *a,
                     const int64_t *e, opir_client &c, uint64_t *out) {
   const uint32_t n = c.n, nq = static_cast<uint32_t>(n_q);
   const opir_params &p = c.params;
   if (p.l_ep > 16) throw std::runtime_error("client pack: L_EP above 16");
   ensure_secret_matrix(c, st);
-  if (c.pk_colsum.n < 2 * n_q) {
+  // columns: one per query (single modulus: two residue sets) or one per
+  // (query, limb) (two limbs: two 30-bit halves); both need 8 plane sets'
+  // worth of room per column pair
+  const uint64_t cols = n_q * c.limbs;
+  if (c.pk_colsum.n < 2 * cols) {
     ck(cudaStreamSynchronize(st), "client sync");
-    c.pk_q.alloc(8ull * n_q * n);
-    c.pk_colsum.alloc(2 * n_q);
-    c.pk_ax.alloc(2 * n_q * n);
+    c.pk_q.alloc(8ull * cols * n);
+    c.pk_colsum.alloc(2 * cols);
+    c.pk_ax.alloc((c.limbs == 2 ? 4 : 2) * cols * n);
     c.pk_idx.alloc(n_q);
   }
   // the previous call's index upload must have left the staging buffer
@@ -1034,9 +1132,32 @@ void launch_pack_tc(uint64_t n_q, const uint64_t *pt_idx, cudaStream_t st, const
   L.num_dims = p.num_dims;
   L.h = p.expansion_height;
   L.l_ep = p.l_ep;
-  L.one = c.one_val[0];
-  for (uint32_t k = 0; k < p.l_ep; ++k) L.gadget[k] = c.gadget_val[2 * k];
+  L.one[0] = c.one_val[0];
+  L.one[1] = c.one_val[1];
+  for (uint32_t k = 0; k < p.l_ep; ++k) {
+    L.gadget[k][0] = c.gadget_val[2 * k];
+    L.gadget[k][1] = c.gadget_val[2 * k + 1];
+  }
   ck(cudaMemsetAsync(c.tc_err.p, 0, sizeof(uint32_t), st), "scan error reset");
+  if (c.limbs == 2) {
+    const uint32_t nc = static_cast<uint32_t>(cols);
+    uint64_t inv = 0;
+    if (!opir::invert_mod(kSplitP1 % kSplitP2, kSplitP2, inv)) throw std::runtime_error("split primes");
+    k_client_tc_pack_prep_split<<<nc, kBlock, 0, st>>>(a, n, nc, p.q1, p.q2, c.pk_q.p,
+                                                       c.pk_colsum.p);
+    launched("client pack prep launch");
+    const uint64_t set = 4ull * cols * n, outw = cols * n;
+    for (int hf = 0; hf < 2; ++hf)
+      for (int pr = 0; pr < 2; ++pr)
+        scan_secret_matrix(c, nc, pr ? kSplitP2 : kSplitP1, c.pk_q.p + hf * set,
+                           c.pk_ax.p + (2 * hf + pr) * outw, st);
+    k_client_tc_pack_finish_split<<<nq, kBlock, 0, st>>>(a, e, c.pk_idx.p, L, c.pk_ax.p,
+                                                         c.pk_colsum.p, n, nc, kSplitP1, kSplitP2,
+                                                         inv, p.q1, p.q2, out);
+    launched("client pack finish launch");
+    check_scan_error(c, st, "client pack");
+    return;
+  }
   k_client_tc_pack_prep<<<nq, kBlock, 0, st>>>(a, n, nq, p.q1, p.q2, c.pk_q.p, c.pk_colsum.p);
   launched("client pack prep launch");
   const uint64_t plane_set = 4ull * n_q * n;
@@ -1048,9 +1169,6 @@ void launch_pack_tc(uint64_t n_q, const uint64_t *pt_idx, cudaStream_t st, const
   launched("client pack finish launch");
   check_scan_error(c, st, "client pack");
 }
-
-// The two primes of the split decryption (29-bit, product above 2^57).
-constexpr uint64_t kSplitP1 = 536813569, kSplitP2 = 536752129;
 
 void launch_decrypt_tc_split(uint64_t n_resp, cudaStream_t st, const uint64_t *resp,
                              opir_client &c, uint64_t *pt, unsigned long long *noise) {
@@ -1387,7 +1505,10 @@ opir_status opir_client_generate_queries_device(opir_client *c, uint32_t n,
         throw std::out_of_range("PIR plaintext index exceeds the runtime layout");
     DeviceGuard g(c->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (tc_enabled(*c, n, std::max(c->params.q1, c->params.q2))) {
+    const uint64_t qmax = std::max(c->params.q1, c->params.q2);
+    const bool tc = c->limbs == 1 ? tc_enabled(*c, n, qmax)
+                                  : tc_enabled(*c, n, 0, true) && qmax < (1ull << 60);
+    if (tc) {
       launch_pack_tc(n, pt_idx, st, d_a, d_e, *c, d_queries);
       return;
     }
