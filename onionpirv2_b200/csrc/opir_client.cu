@@ -164,18 +164,38 @@ __device__ __forceinline__ uint64_t reduce_parts(const int64_t (&acc)[NP][R], in
   return static_cast<uint64_t>(x);
 }
 
-__device__ __forceinline__ uint64_t round_div(unsigned __int128 a, uint64_t b) {
-  return static_cast<uint64_t>((a + (b >> 1)) / b);
-}
-
 // Constants of the decryption epilogue. When sq t < 2^63 every product fits
 // 64 bits and the divisions use Barrett reciprocals mu = floor(2^64 / d):
 // mulhi(x, mu) is floor(x / d) or one less (x mu / 2^64 lies in (x/d - 1,
 // x/d]), so one correction makes it exact; otherwise (wide) 128-bit division.
 struct DecConst {
   uint64_t sq, t, mu_sq, mu_t;
+  double inv_sq, inv_t;  // 1/sq, 1/t (wide form)
   uint32_t wide, pad;
 };
+
+// floor(x / d) for x < 2^104 whose quotient is below 2^52: the double
+// estimate x (1/d) carries a relative error of a few 2^-53, so it is off by
+// at most a small integer, which the exact remainder x - q d corrects
+// (long division by an estimated reciprocal with integer correction).
+__device__ __forceinline__ uint64_t div_est(unsigned __int128 x, uint64_t d, double inv_d) {
+  const double xd = static_cast<double>(static_cast<uint64_t>(x >> 64)) * 18446744073709551616.0 +
+                    static_cast<double>(static_cast<uint64_t>(x));
+  double qd = xd * inv_d;
+  uint64_t q = qd <= 0.0 ? 0 : static_cast<uint64_t>(qd);
+  __int128 r = static_cast<__int128>(x) - static_cast<__int128>(static_cast<unsigned __int128>(q) * d);
+  for (int it = 0; it < 4 && r < 0; ++it) { --q; r += d; }
+  for (int it = 0; it < 4 && r >= static_cast<__int128>(d); ++it) { ++q; r -= d; }
+  return q;
+}
+
+// v mod q (canonical) for |v| < 2^104 with |v| / q below 2^52.
+__device__ __forceinline__ uint64_t mod_est(__int128 v, uint64_t q, double inv_q) {
+  const bool neg = v < 0;
+  const unsigned __int128 a = static_cast<unsigned __int128>(neg ? -v : v);
+  const uint64_t r = static_cast<uint64_t>(a - static_cast<unsigned __int128>(div_est(a, q, inv_q)) * q);
+  return neg && r ? q - r : r;
+}
 
 __device__ __forceinline__ uint64_t div_barrett(uint64_t x, uint64_t d, uint64_t mu) {
   uint64_t q = __umul64hi(x, mu);
@@ -201,8 +221,10 @@ __device__ __forceinline__ uint64_t decrypt_coeff(uint64_t prod, uint64_t c0, co
   } else {
     phase = prod + c0 % sq;
     if (phase >= sq) phase -= sq;
-    m = round_div(static_cast<unsigned __int128>(phase) * t, sq) % t;
-    approx = round_div(static_cast<unsigned __int128>(sq) * m, t) % sq;
+    m = div_est(static_cast<unsigned __int128>(phase) * t + (sq >> 1), sq, dc.inv_sq);
+    if (m >= t) m -= t;
+    approx = div_est(static_cast<unsigned __int128>(sq) * m + (t >> 1), t, dc.inv_t);
+    if (approx >= sq) approx -= sq;
   }
   const uint64_t pos = phase >= approx ? phase - approx : sq - approx + phase;
   const uint64_t nabs = pos > (sq >> 1) ? sq - pos : pos;
@@ -719,7 +741,8 @@ __global__ void __launch_bounds__(kBlock) k_client_tc_pack_finish_split(
     const uint64_t *__restrict__ a, const int64_t *__restrict__ e,
     const uint64_t *__restrict__ pt_idx, PackLayout L, const uint32_t *__restrict__ ax,
     const uint64_t *__restrict__ colsum, uint32_t n, uint32_t cols, uint64_t p1, uint64_t p2,
-    uint64_t p1_inv_mod_p2, uint64_t q0, uint64_t q1, uint64_t *__restrict__ out) {
+    uint64_t p1_inv_mod_p2, uint64_t q0, uint64_t q1, double inv_q0, double inv_q1,
+    uint64_t *__restrict__ out) {
   const uint64_t b = blockIdx.x;
   const uint64_t plane = static_cast<uint64_t>(cols) * n;
   uint64_t *c0 = out + b * 4 * n, *c1 = c0 + 2 * n;
@@ -737,9 +760,9 @@ __global__ void __launch_bounds__(kBlock) k_client_tc_pack_finish_split(
       const uint64_t u = v1 + p1 * (d * p1_inv_mod_p2 % p2);
       y[hf] = static_cast<__int128>(u) - static_cast<__int128>(colsum[static_cast<uint64_t>(hf) * cols + col]);
     }
-    __int128 v = (y[0] + y[1] * (static_cast<__int128>(1) << 30)) % static_cast<__int128>(q);
-    if (v < 0) v += q;
-    c0[w] = pack_coeff(static_cast<uint64_t>(v), eq[i], q);
+    const uint64_t v = mod_est(y[0] + y[1] * (static_cast<__int128>(1) << 30), q,
+                               k ? inv_q1 : inv_q0);
+    c0[w] = pack_coeff(v, eq[i], q);
     c1[w] = a[col * n + i];
   }
   __syncthreads();
@@ -1028,6 +1051,8 @@ DecConst dec_const(const opir_params &p) {
   dc.mu_sq = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / dc.sq);
   dc.mu_t = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) / dc.t);
   dc.wide = static_cast<unsigned __int128>(dc.sq) * dc.t + dc.sq >= (static_cast<unsigned __int128>(1) << 63);
+  dc.inv_sq = 1.0 / static_cast<double>(dc.sq);
+  dc.inv_t = 1.0 / static_cast<double>(dc.t);
   return dc;
 }
 
@@ -1153,7 +1178,8 @@ void launch_pack_tc(uint64_t n_q, const uint64_t *pt_idx, cudaStream_t st, const
                            c.pk_ax.p + (2 * hf + pr) * outw, st);
     k_client_tc_pack_finish_split<<<nq, kBlock, 0, st>>>(a, e, c.pk_idx.p, L, c.pk_ax.p,
                                                          c.pk_colsum.p, n, nc, kSplitP1, kSplitP2,
-                                                         inv, p.q1, p.q2, out);
+                                                         inv, p.q1, p.q2, 1.0 / static_cast<double>(p.q1),
+                                                         1.0 / static_cast<double>(p.q2), out);
     launched("client pack finish launch");
     check_scan_error(c, st, "client pack");
     return;
