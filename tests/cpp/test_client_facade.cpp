@@ -145,7 +145,7 @@ void test_client_k1() {
 
 // ---------------------------------------------------------- CONFIG_N4096_K2_MP
 void test_client_c4() {
-  const size_t target = 16384, height = 9, n = 8;
+  const size_t target = 16384, height = 9, n = 40;  // the tensor-core forms
   const uint64_t seed_db = 6;
   PirParams pir_params = PirParams(OPIR_CONFIG_N4096_K2_MP).with_layout({target, height, true});
   opir_oracle_c4_params op;
