@@ -124,6 +124,7 @@ _SIGS = {
     "opir_plan_memory": ([C.POINTER(Params), C.POINTER(MemoryPlan)], C.c_int),
     "opir_server_reserve": ([C.c_void_p, C.c_uint32], C.c_int),
     "opir_server_set_priority": ([C.c_void_p, C.c_int], C.c_int),
+    "opir_server_set_scan_wait_limit": ([C.c_void_p, C.c_uint64], C.c_int),
     "opir_server_autotune": ([C.c_void_p, C.c_uint32], C.c_int),
     "opir_server_scan_tile": ([C.c_void_p, C.c_uint32, u32p, u32p, u32p], C.c_int),
     "opir_server_set_stage_timing": ([C.c_void_p, C.c_int], C.c_int),

@@ -108,6 +108,7 @@ struct Tc4Args {
   uint64_t *cmat;      // [z][col][row]
   uint32_t *err;       // error bits (0 = ok)
   uint32_t *progress;  // per-CTA item counters (>= grid entries) or null
+  long long wait_cycles;  // limit of each pipeline wait (clock cycles)
 };
 size_t scan_tc4_smem(uint32_t ntile, uint32_t stages);
 uint32_t scan_tc4_max_stages(uint32_t ntile);

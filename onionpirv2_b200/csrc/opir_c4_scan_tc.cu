@@ -159,7 +159,7 @@ k4_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
       }
       __syncwarp();
       for (uint32_t kt = 0; ok && kt < a.k_tiles; ++kt) {
-        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) { ok = false; break; }
+        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
         if (lane == 0) {
           uint8_t *st = sm + stage * stage_bytes;
           mbar_expect_tx(&full[stage], stage_bytes);
@@ -196,11 +196,11 @@ k4_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
     uint32_t stage = 0, phase = 0, acc_phases = 0, buf = 0;
     bool ok = true;
     for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
-      if (!mbar_wait(&acc_empty[buf], ((acc_phases >> buf) & 1) ^ 1, abort_flag)) { ok = false; break; }
+      if (!mbar_wait(&acc_empty[buf], ((acc_phases >> buf) & 1) ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
       fence_after();
       const uint32_t acc = tmem + buf * 256;  // S_s at columns acc + s nt
       for (uint32_t kt = 0; kt < a.k_tiles; ++kt) {
-        if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
+        if (!mbar_wait(&full[stage], phase, abort_flag, a.wait_cycles)) { ok = false; break; }
         fence_after();
         if (lane == 0) {
           const uint32_t base = sa(sm + stage * stage_bytes);
@@ -248,7 +248,7 @@ k4_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
     const int row = quad * 32 + lane;
     uint32_t acc_phases = 0, buf = 0;
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-      if (!mbar_wait(&acc_full[buf], (acc_phases >> buf) & 1, abort_flag)) {
+      if (!mbar_wait(&acc_full[buf], (acc_phases >> buf) & 1, abort_flag, a.wait_cycles)) {
         if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 4u); }
         break;
       }
@@ -363,7 +363,9 @@ void launch_scan_tc4(const CUtensorMap &mapA, const CUtensorMap &mapQ, const Tc4
     if (me != cudaSuccess)
       throw std::runtime_error(std::string("k4_scan_tc progress: ") + cudaGetErrorString(me));
   }
-  k4_scan_tc<<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
+  Tc4Args a = args;  // 0: the default limit (~1 s)
+  if (a.wait_cycles <= 0) a.wait_cycles = opir::tc::kWaitCycles;
+  k4_scan_tc<<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
   note_launches(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw std::runtime_error(std::string("k4_scan_tc: ") + cudaGetErrorString(e));

@@ -376,6 +376,7 @@ void Server::launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n) {
   a.cmat = cmat;
   a.err = err_.p;
   a.progress = progress_.p;
+  a.wait_cycles = scan_wait_;
   CUtensorMap map_q;
   opir::make_plane_map(&map_q, qb, sh_.n0p, ncols, 2ull * kN * 8, a.ntile, 64);
   launch_scan_tc4(map_db_, map_q, a, sm_count_, st_);

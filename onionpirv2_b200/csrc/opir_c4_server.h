@@ -59,6 +59,13 @@ class Server {
   // The stream the handle's work is enqueued on from now on (the caller has
   // synchronised the previous one).
   void set_stream(cudaStream_t st) { st_ = st; }
+  // Limit of each tensor-core scan pipeline wait in clock cycles (0: the
+  // default, about one second); drops the captured pipelines that hold the
+  // old limit.
+  void set_scan_wait_limit(long long cycles) {
+    if (cycles != scan_wait_) clear_graphs();
+    scan_wait_ = cycles;
+  }
   static void plan_memory(const opir_params &p, opir_memory_plan *out);
 
   // Public stages of make_query (host buffers, reference layouts).
@@ -132,6 +139,7 @@ class Server {
   opir::DevBuf<uint32_t> err_;  // error word of the tensor-core scan
   opir::DevBuf<uint32_t> progress_;  // scan CTA pairing counters
   int sm_count_ = 148;
+  long long scan_wait_ = 0;     // scan pipeline wait limit (0: default)
   bool db_loaded_ = false;
   // MUX levels answered here; on a row shard the rows kept (local -> database)
   uint32_t tree_h_ = 0, num_shards_ = 1;

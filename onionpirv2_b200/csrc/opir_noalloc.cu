@@ -1,4 +1,6 @@
-// Allocation-free entry point: opir_ext_prod_mux_noalloc.
+// Allocation-free entry point: opir_ext_prod_mux_noalloc. Each of its MUX
+// steps computes what PirServer::ext_prod_mux (src/server.cpp:652-722)
+// computes, x + INTT(ExtProd(sel, y - x)).
 //
 // Why it exists: some callers cannot call cudaMalloc at the point where they
 // need a MUX step -- for example code running inside a host that owns and

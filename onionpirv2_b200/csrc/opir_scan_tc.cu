@@ -122,7 +122,7 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
       const uint32_t ct = it % a.col_tiles, mt = (it / a.col_tiles) % a.m_tiles, z = it / per_z;
       for (uint32_t kt = 0; ok && kt < a.k_tiles; ++kt) {
-        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag)) { ok = false; break; }
+        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
         if (lane == 0) {
           uint8_t *st = sm + stage * stage_bytes;
           mbar_expect_tx(&full[stage], stage_bytes);
@@ -161,11 +161,11 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     uint32_t stage = 0, phase = 0, acc_phases = 0, buf = 0;  // bit b: phase of set b
     bool ok = true;
     for (uint32_t it = blockIdx.x; ok && it < n_items; it += gridDim.x) {
-      if (!mbar_wait(&acc_empty[buf], ((acc_phases >> buf) & 1) ^ 1, abort_flag)) { ok = false; break; }
+      if (!mbar_wait(&acc_empty[buf], ((acc_phases >> buf) & 1) ^ 1, abort_flag, a.wait_cycles)) { ok = false; break; }
       fence_after();
       const uint32_t acc = tmem + buf * 256;  // S_s at columns acc + s nt
       for (uint32_t kt = 0; kt < a.k_tiles; ++kt) {
-        if (!mbar_wait(&full[stage], phase, abort_flag)) { ok = false; break; }
+        if (!mbar_wait(&full[stage], phase, abort_flag, a.wait_cycles)) { ok = false; break; }
         fence_after();
         if (lane == 0) {
           const uint32_t base = sa(sm + stage * stage_bytes);
@@ -213,7 +213,7 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     const int row = quad * 32 + lane;
     uint32_t acc_phases = 0, buf = 0;  // bit b: phase of set b
     for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
-      if (!mbar_wait(&acc_full[buf], (acc_phases >> buf) & 1, abort_flag)) {
+      if (!mbar_wait(&acc_full[buf], (acc_phases >> buf) & 1, abort_flag, a.wait_cycles)) {
         if (lane == 0) { *abort_flag = 1; atomicOr(a.err, 4u); }
         break;
       }
@@ -364,10 +364,12 @@ void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcSc
   configure_scan_tc();
   const uint64_t items = static_cast<uint64_t>(args.col_tiles) * args.m_tiles * args.zcount;
   const unsigned grid = static_cast<unsigned>(items < static_cast<uint64_t>(sm_count) ? items : sm_count);
-  if (args.kt == 128)
-    k_scan_tc<128><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
+  TcScanArgs a = args;  // 0: the default limit (~1 s)
+  if (a.wait_cycles <= 0) a.wait_cycles = tc::kWaitCycles;
+  if (a.kt == 128)
+    k_scan_tc<128><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
   else
-    k_scan_tc<64><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, args);
+    k_scan_tc<64><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
   note_launches(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw std::runtime_error(std::string("k_scan_tc: ") + cudaGetErrorString(e));

@@ -25,6 +25,7 @@ struct TcScanArgs {
   uint32_t w[2][7];         // 2^(8 s) mod q
   uint32_t *cmat;           // [z][column][row] u32
   uint32_t *err;            // error bits (0 = ok)
+  long long wait_cycles;    // limit of each pipeline wait (clock cycles)
 };
 
 // 3-D byte tensor [planes][rows][k_bytes] for TMA (box_k-byte swizzle, boxes

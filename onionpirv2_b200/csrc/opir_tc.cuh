@@ -30,14 +30,23 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: false on timeout or when another role aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag) {
+// Bounded wait, called by all 32 lanes of a warp together: false on timeout
+// (`limit` cycles) or when another role aborted. The answer is the same on
+// every lane (a lane whose phase completed still reports false when another
+// lane gave up), so the caller's branches and the .sync.aligned tcgen05
+// instructions after it never diverge. A completed phase stays complete
+// until this warp acts on it, and the abort flag and the clock only move one
+// way, so each lane's stop condition never reverts.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag,
+                                          long long limit = kWaitCycles) {
   const long long t0 = clock64();
-  while (!mbar_try(b, parity)) {
-    if (*abort_flag) return false;
-    if (clock64() - t0 > kWaitCycles) return false;
+  bool done = false;
+  for (;;) {
+    done = done || mbar_try(b, parity);
+    const bool stop = done || *abort_flag != 0 || clock64() - t0 > limit;
+    if (__all_sync(0xffffffffu, stop)) break;
   }
-  return true;
+  return __all_sync(0xffffffffu, done);
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(b)) : "memory");
