@@ -56,7 +56,8 @@ typedef enum {
  * library implements. */
 typedef enum {
   OPIR_CONFIG_N2048_K1_COMP = 0,
-  OPIR_CONFIG_N4096_K2_MP = 1
+  OPIR_CONFIG_N4096_K2_MP = 1,
+  OPIR_CONFIG_N2048_K2_MP = 2
 } opir_config;
 
 /* PirLayoutConfig (includes/pir.h:199-203). */
@@ -71,8 +72,9 @@ typedef struct {
 typedef struct {
   uint32_t poly_degree;           /* N */
   uint32_t num_limbs;             /* K (1: logical single modulus, 2: RNS) */
-  uint64_t q;                     /* logical ciphertext modulus q1*q2 (K = 1);
-                                     0 when K = 2 (the product needs 120 bits) */
+  uint64_t q;                     /* logical ciphertext modulus q1*q2 (K = 1,
+                                     and K = 2 at N = 2048); 0 at N = 4096
+                                     (the product needs 120 bits)          */
   uint64_t q1, q2;                /* composite first-dim limbs (K = 1) or the
                                      two RNS limbs (K = 2)                */
   uint64_t w1, w2, w_crt;         /* 2N-th roots: q1, q2 and CRT (mod q) */
@@ -129,7 +131,14 @@ opir_status opir_params_init(const opir_layout *layout, opir_params *out);
 /* PirParams under a chosen ACTIVE_CONFIG: CONFIG_N2048_K1_COMP gives the
  * same as opir_params_init, CONFIG_N4096_K2_MP the two-limb set
  * (src/pir.cpp:49-134 with RnsMods {60, 60}, PlainMod 40, SmallQWidth 50;
- * expansion_height <= 12). Unknown config -> OPIR_ERR_INVALID_ARGUMENT. */
+ * expansion_height <= 12), CONFIG_N2048_K2_MP the two-limb set at N = 2048
+ * (RnsMods {29, 29} as real RNS limbs, PlainMod 10, SmallQWidth 22, L_EP 5,
+ * L_KEY 8, L_KS 8, the MP gadgets; includes/database_constants.h:96-110;
+ * expansion_height <= 11). Handles on CONFIG_N2048_K2_MP take ciphertexts,
+ * keys and stage arrays limb-major (K = 2) like CONFIG_N4096_K2_MP and
+ * answer make_query, its batch forms and the stage methods; row shards and
+ * tree PIR are built for the other two sets. Unknown config ->
+ * OPIR_ERR_INVALID_ARGUMENT. */
 opir_status opir_params_init_config(opir_config config, const opir_layout *layout,
                                     opir_params *out);
 
@@ -346,6 +355,19 @@ opir_status opir_server_scan_tile(const opir_server *server, uint32_t n,
  * expensive ones. Results do not depend on the priority. */
 opir_status opir_server_set_priority(opir_server *server, int priority);
 
+/* No counterpart in the reference. Every wait inside the tensor-core
+ * first-dimension scan (a pipeline stage filled by TMA, the MMAs of a tile,
+ * the epilogue handing back its accumulators) gives up after a limit; the
+ * kernel then records an error code, lets its own copies and MMAs finish,
+ * frees its tensor memory and returns, and the call fails with
+ * OPIR_ERR_RUNTIME ("tensor-core scan timed out"). The default limit, about
+ * one second of clock cycles, is far above any legitimate wait. This call
+ * sets the limit in SM clock cycles (0 restores the default; at most 2^40),
+ * so a test can make a wait run out and check that the handle reports it
+ * and answers correctly afterwards. Waits while the kernel drains are not
+ * affected. Synchronises the handle's stream. */
+opir_status opir_server_set_scan_wait_limit(opir_server *server, uint64_t cycles);
+
 /* Per-stage device times (ms), averaged over the make_query / batch calls
  * made since stage timing was (re-)enabled, in the reference's TimerLogger
  * sections (includes/logging.h:34-78): [0] Expand, [1] Convert,
@@ -470,8 +492,10 @@ opir_status opir_keys_decode(const opir_params *params, const uint8_t *in, size_
  * memory when they run a MUX step (a host that pre-budgets and owns all
  * device memory, or a request loop that must not touch the CUDA allocator
  * because an allocation can synchronise the device): n independent MUX
- * steps out_i = x_i + b_i * (y_i - x_i), exactly PirServer::ext_prod_mux
- * (src/server.cpp:652-722), with no server handle and no allocation.
+ * steps out_i = x_i + INTT(ExtProd(sel_i, y_i - x_i)) (the gadget
+ * decomposition of y_i - x_i times the RGSW selector sel_i, in the NTT
+ * domain, back to coefficient form), with no server handle and no
+ * allocation.
  *   d_x, d_y      : n x 2N u64 device arrays, coefficient form mod q
  *   d_selectors   : n x 2 L_EP rows x 2N u64 device array, RGSW selector in
  *                   NTT form (the complete_selectors layout)

@@ -44,7 +44,10 @@ struct DevParams {
   uint32_t q1_inv, q1_inv_sh;   // q1^-1 mod q2 and its Shoup companion
   uint64_t small_q;
   uint32_t small_q_width;
-  uint32_t pad;
+  // ciphertext limbs at the boundary: 0 or 1 = one u64 per coefficient mod
+  // q1 q2 (CONFIG_N2048_K1_COMP); 2 = two RNS limbs q1, q2, limb-major, one
+  // u64 per limb (CONFIG_N2048_K2_MP, the same residue pair on the device)
+  uint32_t limbs;
 };
 
 // ---------------------------------------------------------------- modular ops

@@ -87,6 +87,8 @@ void set_smem(K kernel, size_t bytes) {
 }
 
 // ------------------------------------------------------------ split/compose
+// Boundary polynomials -> residue pairs. One boundary polynomial is N u64
+// mod q1 q2 (limbs <= 1) or 2N u64, limb q1 then limb q2 (limbs == 2).
 __global__ void k_split_u64(DevParams P, const uint64_t *__restrict__ in,
                             uint32_t *__restrict__ out, uint64_t n, uint64_t per_item,
                             uint64_t stride) {
@@ -94,13 +96,20 @@ __global__ void k_split_u64(DevParams P, const uint64_t *__restrict__ in,
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t p = i >> kLogN, j = i & (kN - 1);
     const uint64_t item = p / per_item, pp = p % per_item;
-    const uint64_t v = in[i];
     uint32_t *o = out + item * stride + pp * 2 * kN + j;
-    o[0] = reduce64(v, P.q1, P.r[0].mu);
-    o[kN] = reduce64(v, P.q2, P.r[1].mu);
+    if (P.limbs == 2) {
+      const uint64_t *src = in + p * 2 * kN + j;
+      o[0] = reduce64(src[0], P.q1, P.r[0].mu);
+      o[kN] = reduce64(src[kN], P.q2, P.r[1].mu);
+    } else {
+      const uint64_t v = in[i];
+      o[0] = reduce64(v, P.q1, P.r[0].mu);
+      o[kN] = reduce64(v, P.q2, P.r[1].mu);
+    }
   }
 }
 
+// Residue pairs -> boundary polynomials (the inverse of k_split_u64).
 __global__ void k_compose_u64(DevParams P, const uint32_t *__restrict__ in, uint64_t stride,
                               uint64_t *__restrict__ out, uint64_t n, uint64_t per_item) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
@@ -108,7 +117,12 @@ __global__ void k_compose_u64(DevParams P, const uint32_t *__restrict__ in, uint
     const uint64_t p = i >> kLogN, j = i & (kN - 1);
     const uint64_t item = p / per_item, pp = p % per_item;
     const uint32_t *s = in + item * stride + pp * 2 * kN + j;
-    out[i] = crt_compose(s[0], s[kN], P);
+    if (P.limbs == 2) {
+      out[p * 2 * kN + j] = s[0];
+      out[p * 2 * kN + kN + j] = s[kN];
+    } else {
+      out[i] = crt_compose(s[0], s[kN], P);
+    }
   }
 }
 
@@ -208,7 +222,7 @@ k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
 // ciphertext (bv_keyswitch.cpp:296-367) then the two children
 // (server.cpp:794-809): left = c + c', right = (c - c') X^-k.
 // sigma_k is applied as a gather: sigma(c)[j] = +-c[j k^-1 mod 2N].
-template <int RES>
+template <int RES, class G>
 __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t galois_inv,
                                                   uint32_t kshift, int base_ks, int l_ks,
                                                   const uint32_t *in, uint64_t in_stride,
@@ -234,31 +248,31 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
     const uint32_t src = u & (kN - 1);
     const uint32_t z = c0[src], a0 = ct[2 * kN + src], a1 = ct[3 * kN + src];
     s0[k] = neg ? neg_mod(z, q) : z;
-    d[k] = digit_source<kLKs, kBaseKs>(compose_c(neg ? neg_mod(a0, kQ1) : a0,
-                                                 neg ? neg_mod(a1, kQ2) : a1));
+    d[k] = digit_source<G::lks, G::bks, G::kks>(compose_c(neg ? neg_mod(a0, kQ1) : a0,
+                                                          neg ? neg_mod(a1, kQ2) : a1));
   }
   // digit planes: decompose, pass A in registers
 #pragma unroll
-  for (int i = 0; i < kLKs; ++i) {
+  for (int i = 0; i < G::lks; ++i) {
     uint32_t v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, kBaseKs>(d[k], i);
+    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, G::bks, G::kks>(d[k], i);
     fA<RES>(v);
     st_plane<0>(sm + i * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid_r<RES>(sm, kLKs, T.fwt);
+  fwd_mid_r<RES>(sm, G::lks, T.fwt);
   // inner product with the key rows (row t encrypts sigma(s) B^t), D-order;
   // digit NTT values stay in [0, 4q) when l_ks <= 8 (sum < 2^64), else canonical
   const uint32_t *key = bv_keys[b] + bv_level_off + RES * kN;
-  constexpr bool lazy = kLKs <= 8;
+  constexpr bool lazy = G::lks <= 8;
   uint64_t ab[8], aa[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
   {
     uint2 wd[6];
     fload_d(wd, T.fwt, tid);
-    for (int i = 0; i < kLKs; ++i) {
+    for (int i = 0; i < G::lks; ++i) {
       uint32_t v[8];
       ld_plane<3>(sm + i * kPad, v, tid);
       fD<RES>(v, wd);
@@ -314,17 +328,18 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
   }
 }
 
+template <class G>
 __global__ void __launch_bounds__(kThreads, 2)
 k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, int l_ks,
                const uint32_t *__restrict__ in, uint64_t in_stride,
                uint32_t *__restrict__ out, uint64_t out_stride,
                const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
   if (blockIdx.y == 0)
-    expand_level_body<0>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
-                         bv_keys, bv_level_off);
+    expand_level_body<0, G>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
+                            bv_keys, bv_level_off);
   else
-    expand_level_body<1>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
-                         bv_keys, bv_level_off);
+    expand_level_body<1, G>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
+                            bv_keys, bv_level_off);
 }
 
 // Expansion level, cluster split: a level with fewer nodes than the GPU
@@ -335,15 +350,15 @@ k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, i
 // then finishes the b part (c0 of both children) and CTA 1 the a part (c1 of
 // both children). Every partial and their total are exact 64-bit sums below
 // the single-CTA bound, so the children are the same bit for bit.
-template <int RES, int C>
+template <int RES, int C, class G>
 __device__ __forceinline__ void expand_split_body(const DevParams &P, uint32_t galois_inv,
                                                   uint32_t kshift, const uint32_t *in,
                                                   uint64_t in_stride, uint32_t *out,
                                                   uint64_t out_stride,
                                                   const uint32_t *const *bv_keys,
                                                   uint64_t bv_level_off) {
-  static_assert(kLKs % C == 0, "digits split evenly over the cluster");
-  constexpr int D = kLKs / C;
+  static_assert(G::lks % C == 0, "digits split evenly over the cluster");
+  constexpr int D = G::lks / C;
   extern __shared__ uint32_t sm[];
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
@@ -363,15 +378,15 @@ __device__ __forceinline__ void expand_split_body(const DevParams &P, uint32_t g
     const bool neg = u >= kN;
     const uint32_t src = u & (kN - 1);
     const uint32_t a0 = ct[2 * kN + src], a1 = ct[3 * kN + src];
-    d[k] = digit_source<kLKs, kBaseKs>(compose_c(neg ? neg_mod(a0, kQ1) : a0,
-                                                 neg ? neg_mod(a1, kQ2) : a1));
+    d[k] = digit_source<G::lks, G::bks, G::kks>(compose_c(neg ? neg_mod(a0, kQ1) : a0,
+                                                          neg ? neg_mod(a1, kQ2) : a1));
   }
   const int i0 = rank * D;
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     uint32_t v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, kBaseKs>(d[k], i0 + i);
+    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, G::bks, G::kks>(d[k], i0 + i);
     fA<RES>(v);
     st_plane<0>(sm + i * kPad, v, tid);
   }
@@ -463,18 +478,18 @@ __device__ __forceinline__ void expand_split_body(const DevParams &P, uint32_t g
   }
 }
 
-template <int C>
+template <int C, class G>
 __global__ void __launch_bounds__(kThreads, 2)
 k_expand_level_split(DevParams P, uint32_t galois_inv, uint32_t kshift,
                      const uint32_t *__restrict__ in, uint64_t in_stride,
                      uint32_t *__restrict__ out, uint64_t out_stride,
                      const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
   if (blockIdx.y == 0)
-    expand_split_body<0, C>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
-                            bv_level_off);
+    expand_split_body<0, C, G>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                               bv_level_off);
   else
-    expand_split_body<1, C>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
-                            bv_level_off);
+    expand_split_body<1, C, G>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                               bv_level_off);
 }
 
 // Shared gadget product of a coefficient-form ciphertext (both residues read
@@ -484,7 +499,7 @@ k_expand_level_split(DevParams P, uint32_t galois_inv, uint32_t kshift,
 // poly p meets row p*l + (l - 1 - i) (gsw.cpp:283-293). Uses l padded planes.
 // Digit NTT values enter the MAC in [0, 4q) when 2 l <= 16 (a sum of 2 l
 // products below 4q x q < 2^60 stays below 2^64), else canonical.
-template <int RES, int L, int B>
+template <int RES, int L, int B, int KIND>
 __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x,
                                            const uint32_t *y, const uint32_t *rgsw,
                                            uint32_t *sm, uint64_t (&acc0)[8],
@@ -505,13 +520,13 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x
         v1 = sub_mod(y[(p * 2 + 0) * kN + j], v1, kQ1);
         v2 = sub_mod(y[(p * 2 + 1) * kN + j], v2, kQ2);
       }
-      d[k] = digit_source<L, B>(compose_c(v1, v2));
+      d[k] = digit_source<L, B, KIND>(compose_c(v1, v2));
     }
 #pragma unroll
     for (int i = 0; i < l; ++i) {
       uint32_t v[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = digit_res<q, B>(d[k], i);
+      for (int k = 0; k < 8; ++k) v[k] = digit_res<q, B, KIND>(d[k], i);
       fA<RES>(v);
       st_plane<0>(sm + i * kPad, v, tid);
     }
@@ -543,7 +558,7 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x
 }
 
 // -------------------------------------------------------- selector completion
-template <int RES>
+template <int RES, class G>
 __device__ __forceinline__ void selectors_body(const DevParams &P, const Shape &S,
                                                const uint32_t *leaves, uint64_t leaf_stride,
                                                const uint32_t *const *gsw_keys, uint32_t *sel) {
@@ -557,7 +572,7 @@ __device__ __forceinline__ void selectors_body(const DevParams &P, const Shape &
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
   // bottom row: ExtProd(RGSW(s), row) with the key gadget (gsw.cpp:119-182)
-  gadget_mac<RES, kLKey, kBaseKey>(P, ct, nullptr, gsw_keys[b], sm, acc0, acc1);
+  gadget_mac<RES, G::lkey, G::bkey, G::kkey>(P, ct, nullptr, gsw_keys[b], sm, acc0, acc1);
   uint32_t *bot = out + (uint64_t)(S.l_ep + r) * kCtWords + RES * kN;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -598,13 +613,14 @@ __device__ __forceinline__ void selectors_body(const DevParams &P, const Shape &
   }
 }
 
+template <class G>
 __global__ void __launch_bounds__(kThreads, 2)
 k_selectors(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
             const uint32_t *const *__restrict__ gsw_keys, uint32_t *__restrict__ sel) {
   if (blockIdx.y == 0)
-    selectors_body<0>(P, S, leaves, leaf_stride, gsw_keys, sel);
+    selectors_body<0, G>(P, S, leaves, leaf_stride, gsw_keys, sel);
   else
-    selectors_body<1>(P, S, leaves, leaf_stride, gsw_keys, sel);
+    selectors_body<1, G>(P, S, leaves, leaf_stride, gsw_keys, sel);
 }
 
 // ------------------------------------------------------- first-dim query prep
@@ -866,7 +882,7 @@ k_scan_epilogue(DevParams P, Shape S, const uint32_t *__restrict__ cmat, uint32_
 
 // --------------------------------------------------------------- MUX level
 // ext_prod_mux (server.cpp:652-722): out = x + INTT(ExtProd(sel, y - x)).
-template <int RES>
+template <int RES, class G>
 __device__ __forceinline__ void mux_level_body(const DevParams &P, const Shape &S, uint32_t level,
                                                uint32_t n_pairs, uint32_t offset, uint32_t half,
                                                const uint32_t *in, uint32_t *out,
@@ -896,7 +912,7 @@ __device__ __forceinline__ void mux_level_body(const DevParams &P, const Shape &
   uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
-  gadget_mac<RES, kLEp, kBaseEp>(P, x, y, rgsw, sm, acc0, acc1);
+  gadget_mac<RES, G::lep, G::bep, G::kep>(P, x, y, rgsw, sm, acc0, acc1);
   {
     uint2 wd[6];
     iload_d(wd, T.iwt, tid);
@@ -924,14 +940,15 @@ __device__ __forceinline__ void mux_level_body(const DevParams &P, const Shape &
   }
 }
 
+template <class G>
 __global__ void __launch_bounds__(kThreads, 2)
 k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t offset,
             uint32_t half, const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
             uint64_t mid_stride, const uint32_t *__restrict__ sel) {
   if (blockIdx.y == 0)
-    mux_level_body<0>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
+    mux_level_body<0, G>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
   else
-    mux_level_body<1>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
+    mux_level_body<1, G>(P, S, level, n_pairs, offset, half, in, out, mid_stride, sel);
 }
 
 // ------------------------------------------------- MUX level, cluster split
@@ -946,7 +963,7 @@ k_mux_level(DevParams P, Shape S, uint32_t level, uint32_t n_pairs, uint32_t off
 // so the result is the same bit for bit.
 // gadget_mac restricted to digits [i0, i0 + D) of polynomial p (decomposed
 // value y - x, or x when y is null).
-template <int RES, int L, int B, int D>
+template <int RES, int L, int B, int KIND, int D>
 __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32_t *x,
                                                 const uint32_t *y, const uint32_t *rgsw,
                                                 uint32_t *sm, int p, int i0,
@@ -965,13 +982,13 @@ __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32
       v1 = sub_mod(y[(p * 2 + 0) * kN + j], v1, kQ1);
       v2 = sub_mod(y[(p * 2 + 1) * kN + j], v2, kQ2);
     }
-    d[k] = digit_source<l, B>(compose_c(v1, v2));
+    d[k] = digit_source<l, B, KIND>(compose_c(v1, v2));
   }
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     uint32_t v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, B>(d[k], i0 + i);
+    for (int k = 0; k < 8; ++k) v[k] = digit_res<q, B, KIND>(d[k], i0 + i);
     fA<RES>(v);
     st_plane<0>(sm + i * kPad, v, tid);
   }
@@ -1004,13 +1021,15 @@ __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32
 // Pair i reads x = in[i xs], y = in[i xs + yoff] and writes out[i]: level 0
 // without a carried prefix has xs = 2, yoff = 1; level a >= 1 has xs = 1,
 // yoff = half.
-template <int RES, int C>
+template <int RES, int C, class G>
 __device__ __forceinline__ void mux_split_body(const DevParams &P, const Shape &S, uint32_t level,
                                                uint32_t xs, uint32_t yoff, const uint32_t *in,
                                                uint32_t *out, uint64_t mid_stride,
                                                const uint32_t *sel) {
   static_assert(C == 2 || C == 4, "cluster of 2 or 4 CTAs");
-  constexpr int D = 2 * kLEp / C;  // gadget rows per CTA
+  static_assert((2 * G::lep) % C == 0 && (C == 2 || G::lep % 2 == 0),
+                "gadget rows split evenly, within one polynomial per CTA");
+  constexpr int D = 2 * G::lep / C;  // gadget rows per CTA
   extern __shared__ uint32_t sm[];
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
@@ -1027,7 +1046,7 @@ __device__ __forceinline__ void mux_split_body(const DevParams &P, const Shape &
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
   const int p = C == 2 ? rank : rank >> 1;
   const int i0 = C == 2 ? 0 : (rank & 1) * D;
-  gadget_mac_part<RES, kLEp, kBaseEp, D>(P, x, y, rgsw, sm, p, i0, acc0, acc1);
+  gadget_mac_part<RES, G::lep, G::bep, G::kep, D>(P, x, y, rgsw, sm, p, i0, acc0, acc1);
   // partial sums out to shared memory: [output poly][k][tid]
   uint64_t *ex = reinterpret_cast<uint64_t *>(sm);
 #pragma unroll
@@ -1078,7 +1097,7 @@ __device__ __forceinline__ void mux_split_body(const DevParams &P, const Shape &
 // distributed shared memory and CTA r writes polynomial r of the bottom row
 // (sum, reduction) and of the top row (the row's own NTT). Exact 64-bit
 // partial sums: the same rows bit for bit.
-template <int RES>
+template <int RES, class G>
 __device__ __forceinline__ void selectors_split_body(const DevParams &P, const Shape &S,
                                                      const uint32_t *leaves, uint64_t leaf_stride,
                                                      const uint32_t *const *gsw_keys,
@@ -1095,8 +1114,8 @@ __device__ __forceinline__ void selectors_split_body(const DevParams &P, const S
   uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
-  gadget_mac_part<RES, kLKey, kBaseKey, kLKey>(P, ct, nullptr, gsw_keys[b], sm, rank, 0, acc0,
-                                               acc1);
+  gadget_mac_part<RES, G::lkey, G::bkey, G::kkey, G::lkey>(P, ct, nullptr, gsw_keys[b], sm, rank,
+                                                            0, acc0, acc1);
   uint64_t *ex = reinterpret_cast<uint64_t *>(sm);
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -1142,28 +1161,30 @@ __device__ __forceinline__ void selectors_split_body(const DevParams &P, const S
         make_uint4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
 }
 
+template <class G>
 __global__ void __launch_bounds__(kThreads, 2)
 k_selectors_split(DevParams P, Shape S, const uint32_t *__restrict__ leaves, uint64_t leaf_stride,
                   const uint32_t *const *__restrict__ gsw_keys, uint32_t *__restrict__ sel) {
   if (blockIdx.y == 0)
-    selectors_split_body<0>(P, S, leaves, leaf_stride, gsw_keys, sel);
+    selectors_split_body<0, G>(P, S, leaves, leaf_stride, gsw_keys, sel);
   else
-    selectors_split_body<1>(P, S, leaves, leaf_stride, gsw_keys, sel);
+    selectors_split_body<1, G>(P, S, leaves, leaf_stride, gsw_keys, sel);
 }
 
-template <int C>
+template <int C, class G>
 __global__ void __launch_bounds__(kThreads, 2)
 k_mux_level_split(DevParams P, Shape S, uint32_t level, uint32_t xs, uint32_t yoff,
                   const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
                   uint64_t mid_stride, const uint32_t *__restrict__ sel) {
   if (blockIdx.y == 0)
-    mux_split_body<0, C>(P, S, level, xs, yoff, in, out, mid_stride, sel);
+    mux_split_body<0, C, G>(P, S, level, xs, yoff, in, out, mid_stride, sel);
   else
-    mux_split_body<1, C>(P, S, level, xs, yoff, in, out, mid_stride, sel);
+    mux_split_body<1, C, G>(P, S, level, xs, yoff, in, out, mid_stride, sel);
 }
 
 // ------------------------------------------------ modulus switch + packing
-// utils.cpp:445-462: centred round(v * out / inp), inp = q, out = small_q.
+// utils.cpp:445-462: centred round(v * out / inp), inp = q (or q1 after the
+// high limb is dropped), out = small_q.
 __device__ __forceinline__ uint64_t rescale_dev(uint64_t v, uint64_t inp, uint64_t outm) {
   const int64_t inp_i = static_cast<int64_t>(inp);
   int64_t c = static_cast<int64_t>(v);
@@ -1188,7 +1209,16 @@ k_modswitch(DevParams P, const uint32_t *__restrict__ ct_all, uint64_t ct_stride
        idx += kThreads) {
     const int p = idx >> kLogN, j = idx & (kN - 1);
     const uint64_t v = crt_compose(ct[(p * 2 + 0) * kN + j], ct[(p * 2 + 1) * kN + j], P);
-    const uint64_t r = rescale_dev(v, P.q, P.small_q);
+    uint64_t r;
+    if (P.limbs == 2) {
+      // two RNS limbs (server.cpp:1044-1075): round the composed value's
+      // high limb q2 away (mod q1), then rescale q1 -> small_q
+      uint64_t d = (v + (P.q2 >> 1)) / P.q2;
+      if (d >= P.q1) d -= P.q1;
+      r = rescale_dev(d, P.q1, P.small_q);
+    } else {
+      r = rescale_dev(v, P.q, P.small_q);
+    }
     resp[(uint64_t)b * 2 * kN + idx] = r;
     vals[idx] = static_cast<uint32_t>(r & ((1ull << P.small_q_width) - 1));
   }
@@ -1277,21 +1307,29 @@ void launch_db_preprocess(const DevParams &P, const Shape &s, const uint16_t *co
   check_launch("k_db_preprocess");
 }
 
-// The kernels are compiled for the CONFIG_N2048_K1_COMP gadget shapes.
+// The kernels are compiled for the gadget shapes of CONFIG_N2048_K1_COMP
+// (s.gadget 0) and CONFIG_N2048_K2_MP (s.gadget 1).
+template <class G>
+static bool gadgets_match(const Shape &s) {
+  return s.l_ep == static_cast<uint32_t>(G::lep) && s.base_ep == static_cast<uint32_t>(G::bep) &&
+         s.l_key == static_cast<uint32_t>(G::lkey) && s.base_key == static_cast<uint32_t>(G::bkey) &&
+         s.l_ks == static_cast<uint32_t>(G::lks) && s.base_ks == static_cast<uint32_t>(G::bks);
+}
 static void check_gadgets(const Shape &s) {
-  if (s.l_ep != kLEp || s.base_ep != kBaseEp || s.l_key != kLKey || s.base_key != kBaseKey ||
-      s.l_ks != kLKs || s.base_ks != kBaseKs)
-    throw std::invalid_argument("the kernels are compiled for the CONFIG_N2048_K1_COMP gadgets");
+  if (s.gadget == 0 ? !gadgets_match<GadgetsK1Comp>(s)
+                    : s.gadget != 1 || !gadgets_match<GadgetsK2Mp>(s))
+    throw std::invalid_argument(
+        "the kernels are compiled for the CONFIG_N2048_K1_COMP and CONFIG_N2048_K2_MP gadgets");
 }
 
-void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const uint32_t *in,
-                         uint64_t in_stride, uint32_t *out, uint64_t out_stride,
-                         const uint32_t *const *bv_keys, uint64_t bv_level_stride,
-                         uint32_t batch, cudaStream_t st) {
-  check_gadgets(s);
+template <class G>
+static void expand_level_impl(const DevParams &P, const Shape &s, uint32_t d, const uint32_t *in,
+                              uint64_t in_stride, uint32_t *out, uint64_t out_stride,
+                              const uint32_t *const *bv_keys, uint64_t bv_level_stride,
+                              uint32_t batch, cudaStream_t st) {
   const uint32_t nodes = expand_nodes(s, d);
   const size_t smem = s.l_ks * kPad * sizeof(uint32_t);
-  set_smem(k_expand_level, smem);
+  set_smem(k_expand_level<G>, smem);
   const uint32_t k = 1u << d;
   const uint32_t galois = kN / k + 1;
   uint32_t galois_inv = 1;  // galois^-1 mod 2N (galois is odd)
@@ -1303,14 +1341,14 @@ void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const u
                     : 8 * ctas <= slots ? 8 : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
   if (split == 1) {
     dim3 grid(nodes, 2, batch);
-    k_expand_level<<<grid, kThreads, smem, st>>>(P, galois_inv, k, s.base_ks, s.l_ks, in,
-                                                  in_stride, out, out_stride, bv_keys,
-                                                  d * bv_level_stride);
+    k_expand_level<G><<<grid, kThreads, smem, st>>>(P, galois_inv, k, s.base_ks, s.l_ks, in,
+                                                     in_stride, out, out_stride, bv_keys,
+                                                     d * bv_level_stride);
     check_launch("k_expand_level");
     return;
   }
   // the exchange area ([2][8][256] u64) reuses the digit planes
-  const size_t smem_split = std::max<size_t>(kLKs / 2 * kPad * sizeof(uint32_t),
+  const size_t smem_split = std::max<size_t>(G::lks / 2 * kPad * sizeof(uint32_t),
                                              2 * 8 * kThreads * sizeof(uint64_t));
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(nodes * split, 2, batch);
@@ -1327,16 +1365,16 @@ void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const u
   const uint64_t koff = d * bv_level_stride;
   cudaError_t e;
   if (split == 8) {
-    set_smem(k_expand_level_split<8>, smem_split);
-    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<8>, P, galois_inv, k, in, in_stride, out,
+    set_smem(k_expand_level_split<8, G>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<8, G>, P, galois_inv, k, in, in_stride, out,
                            out_stride, bv_keys, koff);
   } else if (split == 4) {
-    set_smem(k_expand_level_split<4>, smem_split);
-    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<4>, P, galois_inv, k, in, in_stride, out,
+    set_smem(k_expand_level_split<4, G>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<4, G>, P, galois_inv, k, in, in_stride, out,
                            out_stride, bv_keys, koff);
   } else {
-    set_smem(k_expand_level_split<2>, smem_split);
-    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<2>, P, galois_inv, k, in, in_stride, out,
+    set_smem(k_expand_level_split<2, G>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_expand_level_split<2, G>, P, galois_inv, k, in, in_stride, out,
                            out_stride, bv_keys, koff);
   }
   if (e != cudaSuccess)
@@ -1344,17 +1382,29 @@ void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const u
   check_launch("k_expand_level_split");
 }
 
-void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves,
-                      uint64_t leaf_stride, const uint32_t *const *gsw_keys, uint32_t *sel,
-                      uint32_t batch, cudaStream_t st) {
+void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const uint32_t *in,
+                         uint64_t in_stride, uint32_t *out, uint64_t out_stride,
+                         const uint32_t *const *bv_keys, uint64_t bv_level_stride,
+                         uint32_t batch, cudaStream_t st) {
   check_gadgets(s);
-  if (s.num_dims <= 1) return;
+  if (s.gadget == 1)
+    expand_level_impl<GadgetsK2Mp>(P, s, d, in, in_stride, out, out_stride, bv_keys,
+                                   bv_level_stride, batch, st);
+  else
+    expand_level_impl<GadgetsK1Comp>(P, s, d, in, in_stride, out, out_stride, bv_keys,
+                                     bv_level_stride, batch, st);
+}
+
+template <class G>
+static void selectors_impl(const DevParams &P, const Shape &s, const uint32_t *leaves,
+                           uint64_t leaf_stride, const uint32_t *const *gsw_keys, uint32_t *sel,
+                           uint32_t batch, cudaStream_t st) {
   const size_t smem = s.l_key * kPad * sizeof(uint32_t);
   const uint32_t rows = (s.num_dims - 1) * s.l_ep;
   // fewer rows than CTA slots (2 per SM): one pair of CTAs per row
   if (split_enabled() && 2ull * 2 * rows * batch <= 2ull * sm_count()) {
     const size_t smem_split = std::max<size_t>(smem, 2 * 8 * kThreads * sizeof(uint64_t));
-    set_smem(k_selectors_split, smem_split);
+    set_smem(k_selectors_split<G>, smem_split);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(rows * 2, 2, batch);
     cfg.blockDim = dim3(kThreads);
@@ -1368,16 +1418,27 @@ void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const cudaError_t e =
-        cudaLaunchKernelEx(&cfg, k_selectors_split, P, s, leaves, leaf_stride, gsw_keys, sel);
+        cudaLaunchKernelEx(&cfg, k_selectors_split<G>, P, s, leaves, leaf_stride, gsw_keys, sel);
     if (e != cudaSuccess)
       throw std::runtime_error(std::string("k_selectors_split: ") + cudaGetErrorString(e));
     check_launch("k_selectors_split");
     return;
   }
-  set_smem(k_selectors, smem);
+  set_smem(k_selectors<G>, smem);
   dim3 grid(rows, 2, batch);
-  k_selectors<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
+  k_selectors<G><<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
   check_launch("k_selectors");
+}
+
+void launch_selectors(const DevParams &P, const Shape &s, const uint32_t *leaves,
+                      uint64_t leaf_stride, const uint32_t *const *gsw_keys, uint32_t *sel,
+                      uint32_t batch, cudaStream_t st) {
+  check_gadgets(s);
+  if (s.num_dims <= 1) return;
+  if (s.gadget == 1)
+    selectors_impl<GadgetsK2Mp>(P, s, leaves, leaf_stride, gsw_keys, sel, batch, st);
+  else
+    selectors_impl<GadgetsK1Comp>(P, s, leaves, leaf_stride, gsw_keys, sel, batch, st);
 }
 
 void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
@@ -1432,10 +1493,10 @@ void launch_scan_epilogue(const DevParams &P, const Shape &s, const uint32_t *cm
   check_launch("k_scan_epilogue");
 }
 
-void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32_t tree_h,
-                      const uint32_t *in, uint32_t *out, uint64_t mid_stride, const uint32_t *sel,
-                      uint32_t batch, cudaStream_t st) {
-  check_gadgets(s);
+template <class G>
+static void mux_level_impl(const DevParams &P, const Shape &s, uint32_t level, uint32_t tree_h,
+                           const uint32_t *in, uint32_t *out, uint64_t mid_stride,
+                           const uint32_t *sel, uint32_t batch, cudaStream_t st) {
   const uint32_t h = tree_h;
   if (h == 0 || h > 31 || level >= h || h > s.num_dims - 1)
     throw std::invalid_argument("MUX level outside its selector tree");
@@ -1453,15 +1514,17 @@ void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32
   }
   const size_t smem = s.l_ep * kPad * sizeof(uint32_t);
   // levels with fewer MUX steps than CTA slots (2 per SM) split each step
-  // over a cluster of 2 or 4 CTAs (k_mux_level_split)
+  // over a cluster of 2 or 4 CTAs (k_mux_level_split); 4 only when each
+  // polynomial's digits halve evenly
+  constexpr bool four = G::lep % 2 == 0;
   const uint64_t ctas = 2ull * n_pairs * batch, slots = 2ull * sm_count();
   const int split = (copies != 0 || !split_enabled()) ? 1
-                    : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
+                    : (four && 4 * ctas <= slots) ? 4 : 2 * ctas <= slots ? 2 : 1;
   if (split == 1) {
-    set_smem(k_mux_level, smem);
+    set_smem(k_mux_level<G>, smem);
     dim3 grid(n_pairs + copies, 2, batch);
-    k_mux_level<<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,
-                                               mid_stride, sel);
+    k_mux_level<G><<<grid, kThreads, smem, st>>>(P, s, level, n_pairs, offset, half, in, out,
+                                                  mid_stride, sel);
     check_launch("k_mux_level");
     return;
   }
@@ -1481,19 +1544,32 @@ void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32
   cfg.numAttrs = 1;
   // offset == copies == 0 here, so level 0 pairs (2i, 2i + 1) into i
   const uint32_t xs = level == 0 ? 2 : 1, yoff = level == 0 ? 1 : half;
-  cudaError_t e;
-  if (split == 4) {
-    set_smem(k_mux_level_split<4>, smem_split);
-    e = cudaLaunchKernelEx(&cfg, k_mux_level_split<4>, P, s, level, xs, yoff, in, out, mid_stride,
-                           sel);
-  } else {
-    set_smem(k_mux_level_split<2>, smem_split);
-    e = cudaLaunchKernelEx(&cfg, k_mux_level_split<2>, P, s, level, xs, yoff, in, out, mid_stride,
-                           sel);
+  cudaError_t e = cudaSuccess;
+  if constexpr (four) {
+    if (split == 4) {
+      set_smem(k_mux_level_split<4, G>, smem_split);
+      e = cudaLaunchKernelEx(&cfg, k_mux_level_split<4, G>, P, s, level, xs, yoff, in, out,
+                             mid_stride, sel);
+    }
+  }
+  if (split == 2) {
+    set_smem(k_mux_level_split<2, G>, smem_split);
+    e = cudaLaunchKernelEx(&cfg, k_mux_level_split<2, G>, P, s, level, xs, yoff, in, out,
+                           mid_stride, sel);
   }
   if (e != cudaSuccess)
     throw std::runtime_error(std::string("k_mux_level_split: ") + cudaGetErrorString(e));
   check_launch("k_mux_level_split");
+}
+
+void launch_mux_level(const DevParams &P, const Shape &s, uint32_t level, uint32_t tree_h,
+                      const uint32_t *in, uint32_t *out, uint64_t mid_stride, const uint32_t *sel,
+                      uint32_t batch, cudaStream_t st) {
+  check_gadgets(s);
+  if (s.gadget == 1)
+    mux_level_impl<GadgetsK2Mp>(P, s, level, tree_h, in, out, mid_stride, sel, batch, st);
+  else
+    mux_level_impl<GadgetsK1Comp>(P, s, level, tree_h, in, out, mid_stride, sel, batch, st);
 }
 
 void launch_modswitch(const DevParams &P, const uint32_t *ct, uint64_t ct_stride, uint64_t *resp,

@@ -19,6 +19,7 @@ struct Shape {
   uint32_t l_ep, l_key, l_ks;
   uint32_t base_ep, base_key, base_ks;
   uint32_t n0p;         // n0 rounded up to 16 (byte-plane row length)
+  uint32_t gadget;      // 0: CONFIG_N2048_K1_COMP gadgets, 1: CONFIG_N2048_K2_MP gadgets
   uint64_t num_pt;
 };
 

@@ -58,9 +58,27 @@ __device__ __forceinline__ uint32_t to4q(uint32_t x) {  // [0, 8q) -> [0, 4q)
 }
 
 // ------------------------------------------------------ gadget digits
-// Gadget shapes of CONFIG_N2048_K1_COMP (digits x log2 base): data RGSW
-// (L_EP), key RGSW (L_KEY), BV key switching (L_KS).
-constexpr int kLEp = 6, kBaseEp = 10, kLKey = 10, kBaseKey = 6, kLKs = 8, kBaseKs = 8;
+// Gadget shapes (digits x log2 base) and digit kinds of the two parameter
+// sets whose ring is the residue pair (q1, q2):
+//   CONFIG_N2048_K1_COMP: data RGSW (L_EP 6 x 10), key RGSW (L_KEY 10 x 6)
+//     and BV key switching (L_KS 8 x 8), all balanced digits of the centred
+//     value mod q1 q2 in [-B/2, B/2) (gsw.cpp:252-295, bv_keyswitch.cpp:20-40);
+//   CONFIG_N2048_K2_MP: data RGSW (5 x 12) and key RGSW (8 x 8) as unsigned
+//     digits of the composed value in [0, q1 q2) (gsw.cpp:184-250), BV key
+//     switching (8 x 8) as balanced digits in (-B/2, B/2] of the centred
+//     composed value (bv_keyswitch.cpp:42-62, 373-481).
+enum DigitKind { kDigitsLow = 0, kDigitsHigh = 1, kDigitsUnsigned = 2 };
+template <int LEp, int BEp, int KEp, int LKey, int BKey, int KKey, int LKs, int BKs, int KKs>
+struct Gadgets {
+  static constexpr int lep = LEp, bep = BEp, kep = KEp;
+  static constexpr int lkey = LKey, bkey = BKey, kkey = KKey;
+  static constexpr int lks = LKs, bks = BKs, kks = KKs;
+};
+using GadgetsK1Comp = Gadgets<6, 10, kDigitsLow, 10, 6, kDigitsLow, 8, 8, kDigitsLow>;
+using GadgetsK2Mp = Gadgets<5, 12, kDigitsUnsigned, 8, 8, kDigitsUnsigned, 8, 8, kDigitsHigh>;
+constexpr int kLEp = GadgetsK1Comp::lep, kBaseEp = GadgetsK1Comp::bep;
+constexpr int kLKey = GadgetsK1Comp::lkey, kBaseKey = GadgetsK1Comp::bkey;
+constexpr int kLKs = GadgetsK1Comp::lks, kBaseKs = GadgetsK1Comp::bks;
 
 constexpr uint32_t inv_mod_c(uint64_t a, uint64_t m) {  // a^-1 mod m (gcd 1)
   int64_t t = 0, nt = 1, r = static_cast<int64_t>(m), nr = static_cast<int64_t>(a % m);
@@ -82,20 +100,28 @@ __device__ __forceinline__ uint64_t compose_c(uint32_t r1, uint32_t r2) {
   k = min(k, k - kQ2);
   return static_cast<uint64_t>(r1) + static_cast<uint64_t>(kQ1) * k;
 }
-// Balanced base-2^B digits, LSB first (gsw.cpp:277-293, bv_keyswitch.cpp:
-// 20-40): v in [0, q) is centred to c in (-q/2, q/2], and c + C with
-// C = 2^(B-1) sum_{i<L} 2^(B i) has plain base-2^B digits u_i = r_i + 2^(B-1)
-// where r_i in [-2^(B-1), 2^(B-1)) are the balanced digits (|c| < 2^(B L)/2,
-// so the balanced expansion ends within L digits).
-template <int L, int B>
+// Per-digit offset of a digit kind: balanced digits r_i in [-o, B - o).
+template <int B, int KIND>
+__host__ __device__ constexpr uint32_t digit_offset() {
+  return KIND == kDigitsLow ? (1u << (B - 1)) : KIND == kDigitsHigh ? (1u << (B - 1)) - 1u : 0u;
+}
+// Base-2^B digits, LSB first, as the plain base-2^B digits u_i of one 64-bit
+// word. Balanced kinds: v in [0, q) is centred to c in (-q/2, q/2], and
+// c + C with C = o sum_{i<L} 2^(B i) (o the kind's offset) has plain digits
+// u_i = r_i + o, where r_i in [-o, B - o) are the balanced digits (the
+// balanced expansion of |c| < 2^(B L) / 2 ends within L digits, and the
+// base-2^B expansion of c + C is unique). Unsigned kind: u_i are the digits
+// of v itself.
+template <int L, int B, int KIND = kDigitsLow>
 __device__ __forceinline__ uint64_t digit_source(uint64_t v) {
+  if (KIND == kDigitsUnsigned) return v;
   uint64_t C = 0;
 #pragma unroll
-  for (int i = 0; i < L; ++i) C += (1ull << (B - 1)) << (B * i);
+  for (int i = 0; i < L; ++i) C += static_cast<uint64_t>(digit_offset<B, KIND>()) << (B * i);
   return v + C - (v > kQ / 2 ? kQ : 0);
 }
 // r_i as a residue mod Q (r_i + Q for negative r_i).
-template <uint32_t Q, int B>
+template <uint32_t Q, int B, int KIND = kDigitsLow>
 __device__ __forceinline__ uint32_t digit_res(uint64_t u, int i) {
   const int o = B * i;  // a constant once the caller's digit loop is unrolled
   const uint32_t lo = static_cast<uint32_t>(u), hi = static_cast<uint32_t>(u >> 32);
@@ -103,7 +129,9 @@ __device__ __forceinline__ uint32_t digit_res(uint64_t u, int i) {
   if (o + B <= 32) f = lo >> o;
   else if (o >= 32) f = hi >> (o - 32);
   else f = __funnelshift_r(lo, hi, o);
-  const uint32_t t = (f & ((1u << B) - 1)) + (Q - (1u << (B - 1)));
+  f &= (1u << B) - 1;
+  if (KIND == kDigitsUnsigned) return f;  // f < 2^B < Q
+  const uint32_t t = f + (Q - digit_offset<B, KIND>());
   return min(t, t - Q);
 }
 

@@ -33,6 +33,8 @@ LimbTables make_limb_tables(uint32_t n, uint32_t q, uint32_t root);
 // CONFIG_N4096_K2_MP: N = 4096, two 60-bit RNS limbs (q1, q2 fields hold the
 // limbs, q = 0), t = generate_prime(40), small_q 50-bit, L_EP 5, L_KEY 8, L_KS 8.
 opir_params derive_params_c4(const opir_layout &layout);
+// PirParams under CONFIG_N2048_K2_MP (two 29-bit RNS limbs at N = 2048).
+opir_params derive_params_k2mp(const opir_layout &layout);
 
 // 64-bit limb tables: bit-reversed powers with Shoup companions
 // floor(w 2^64 / q), N^-1 and iw[1] N^-1 with theirs.

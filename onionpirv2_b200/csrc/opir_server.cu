@@ -92,6 +92,7 @@ struct opir_server {
   int sm_count = 148;
   int scan_mode = 0;         // 0 auto, 1 tensor cores, 2 CUDA cores
   DevBuf<uint32_t> err;      // device error word of the tensor-core scan
+  long long scan_wait = 0;   // scan pipeline wait limit in cycles (0: default)
   std::unordered_map<uint64_t, ClientKeys> clients;
   std::string last_error;
   // scratch arena (sized for `cap` queries)
@@ -190,6 +191,16 @@ uint32_t resp_bytes_of(const opir_params &p) {
   return static_cast<uint32_t>((2ull * p.poly_degree * p.small_q_width + 7) / 8);
 }
 
+// CONFIG_N2048_K2_MP: two 29-bit RNS limbs at N = 2048, the residue pair of
+// CONFIG_N2048_K1_COMP with the MP gadgets; runs on the same kernels.
+bool is_k2mp(const opir_params &p) { return p.num_limbs == 2 && p.poly_degree == 2048; }
+
+// u64 words of one polynomial at the boundary (queries, keys, stage
+// outputs): N values mod q1 q2, or N per RNS limb (limb-major).
+uint64_t poly_words(const opir_params &p) {
+  return static_cast<uint64_t>(opir::kN) * (is_k2mp(p) ? 2 : 1);
+}
+
 // Kernel-facing shape of a layout; *lvl_slots receives the ciphertext slots
 // per query that an expansion buffer needs (the widest tree level, at least
 // the useful leaves).
@@ -208,6 +219,7 @@ opir::Shape make_shape(const opir_params &p, uint64_t *lvl_slots) {
   sh.base_ks = p.base_log2_ks;
   sh.num_pt = p.num_pt;
   sh.n0p = static_cast<uint32_t>((p.fst_dim_sz + 15) / 16 * 16);
+  sh.gadget = is_k2mp(p) ? 1 : 0;
   uint64_t slots = 1;
   for (uint32_t d2 = 0; d2 < sh.h; ++d2) slots = std::max<uint64_t>(slots, 2ull * opir::expand_nodes(sh, d2));
   *lvl_slots = std::max<uint64_t>(slots, sh.useful);
@@ -224,12 +236,13 @@ struct ScratchPlan {
   }
 };
 
-ScratchPlan plan_scratch(const opir::Shape &sh, uint64_t lvl_slots, uint32_t resp_bytes, uint32_t n) {
+ScratchPlan plan_scratch(const opir::Shape &sh, uint64_t lvl_slots, uint32_t resp_bytes, uint32_t n,
+                         uint64_t pw = opir::kN) {
   const uint64_t ct = kCtWords;
   const uint64_t nsel = sh.num_dims > 1 ? sh.num_dims - 1 : 0;
   ScratchPlan pl{};
-  pl.q_u64 = static_cast<size_t>(n) * 2 * kN;
-  pl.resp_u64 = pl.q_u64;
+  pl.q_u64 = static_cast<size_t>(n) * 2 * pw;  // queries at the boundary
+  pl.resp_u64 = static_cast<size_t>(n) * 2 * kN;
   pl.resp_bytes = static_cast<size_t>(n) * resp_bytes;
   pl.lvl = n * lvl_slots * ct;
   pl.sel = std::max<uint64_t>(1, n * nsel * 2 * sh.l_ep * ct);
@@ -303,6 +316,7 @@ void setup_device_params(opir_server *s) {
   d.q1_inv_sh = static_cast<uint32_t>((static_cast<uint64_t>(d.q1_inv) << 32) / d.q2);
   d.small_q = p.small_q;
   d.small_q_width = p.small_q_width;
+  d.limbs = is_k2mp(p) ? 2 : 1;
 
   s->shape = make_shape(p, &s->lvl_slots);
 }
@@ -320,7 +334,8 @@ void clear_graphs(opir_server *s) {
 void ensure_capacity(opir_server *s, uint32_t n) {
   if (n <= s->cap) return;
   clear_graphs(s);
-  const ScratchPlan pl = plan_scratch(s->shape, s->lvl_slots, resp_bytes_of(s->params), n);
+  const ScratchPlan pl =
+      plan_scratch(s->shape, s->lvl_slots, resp_bytes_of(s->params), n, poly_words(s->params));
   s->q_u64.alloc(pl.q_u64);
   s->resp_u64.alloc(pl.resp_u64);
   s->resp_bytes.alloc(pl.resp_bytes);
@@ -444,6 +459,7 @@ void launch_scan_tc_tile(opir_server *s, uint32_t n, const ScanTile &t) {
   }
   a.cmat = s->cmat.p;
   a.err = s->err.p;
+  a.wait_cycles = s->scan_wait;
   CUtensorMap map_q;
   opir::make_plane_map(&map_q, s->qb.p, sh.n0p, ncols, 2ull * kN * 4, a.ntile, a.kt);
   opir::launch_scan_tc(s->map_db[a.kt == 128 ? 0 : 1], map_q, a, s->sm_count, s->stream);
@@ -600,13 +616,14 @@ void run_pipeline(opir_server *s, const uint64_t *client_ids, uint32_t n,
   upload_keyptrs(s, client_ids, n);
   begin_timed_call(s);
   if (s->use_graphs && d_bytes == nullptr) {
-    const size_t bytes = static_cast<size_t>(n) * 2 * kN * 8;
+    const size_t qbytes = static_cast<size_t>(n) * 2 * poly_words(s->params) * 8;
+    const size_t rbytes = static_cast<size_t>(n) * 2 * kN * 8;
     if (d_queries != s->q_u64.p)
-      ck(cudaMemcpyAsync(s->q_u64.p, d_queries, bytes, cudaMemcpyDeviceToDevice, s->stream),
+      ck(cudaMemcpyAsync(s->q_u64.p, d_queries, qbytes, cudaMemcpyDeviceToDevice, s->stream),
          "query staging");
     launch_graph(s, n);
     if (d_resp != s->resp_u64.p)
-      ck(cudaMemcpyAsync(d_resp, s->resp_u64.p, bytes, cudaMemcpyDeviceToDevice, s->stream),
+      ck(cudaMemcpyAsync(d_resp, s->resp_u64.p, rbytes, cudaMemcpyDeviceToDevice, s->stream),
          "response copy");
   } else {
     enqueue_core(s, n, d_queries, d_resp, d_bytes);
@@ -629,7 +646,14 @@ void finish(opir_server *s) {
   check_device_error(s);
 }
 
+// count: u64 words at the boundary (whole polynomials of poly_words each).
 void check_query_values(const opir_server *s, const uint64_t *q, size_t count) {
+  if (is_k2mp(s->params)) {  // limb-major: limb (i / N) % 2
+    const uint64_t m[2] = {s->params.q1, s->params.q2};
+    for (size_t i = 0; i < count; ++i)
+      if (q[i] >= m[(i / kN) & 1]) throw std::invalid_argument("query coefficient not reduced mod its limb");
+    return;
+  }
   for (size_t i = 0; i < count; ++i)
     if (q[i] >= s->params.q) throw std::invalid_argument("query coefficient not reduced mod q");
 }
@@ -663,10 +687,13 @@ void load_tiles(opir_server *s, uint64_t logical, Fill &&fill) {
 // The parameters a handle is created on, re-derived from their layout (or
 // query shape) so that a caller cannot hand in inconsistent fields.
 opir_params checked_params(const opir_params &p) {
-  const bool c4 = is_c4(p);
-  if (!c4 && (p.poly_degree != static_cast<uint32_t>(kN) || p.num_limbs != 1))
-    throw std::invalid_argument("unsupported parameter set (CONFIG_N2048_K1_COMP or CONFIG_N4096_K2_MP)");
-  auto derive = [&](const opir_layout &lay) { return c4 ? opir4::derive(lay) : opir::derive_params(lay); };
+  const bool c4 = is_c4(p), k2 = is_k2mp(p);
+  if (!c4 && !k2 && (p.poly_degree != static_cast<uint32_t>(kN) || p.num_limbs != 1))
+    throw std::invalid_argument(
+        "unsupported parameter set (CONFIG_N2048_K1_COMP, CONFIG_N2048_K2_MP or CONFIG_N4096_K2_MP)");
+  auto derive = [&](const opir_layout &lay) {
+    return c4 ? opir4::derive(lay) : k2 ? opir::derive_params_k2mp(lay) : opir::derive_params(lay);
+  };
   if (p.view == OPIR_VIEW_LAYOUT) {
     const opir_params check = derive(opir_layout{p.target_num_pt, p.expansion_height, p.fst_dim_pow2});
     if (check.num_pt != p.num_pt || check.q != p.q || check.q1 != p.q1 || check.q2 != p.q2)
@@ -849,6 +876,8 @@ opir_status opir_params_init_config(opir_config config, const opir_layout *layou
                                     opir_params *out) {
   if (!layout || !out) return OPIR_ERR_INVALID_ARGUMENT;
   if (config == OPIR_CONFIG_N2048_K1_COMP) return opir_params_init(layout, out);
+  if (config == OPIR_CONFIG_N2048_K2_MP)
+    return guarded(nullptr, [&] { *out = opir::derive_params_k2mp(*layout); });
   if (config != OPIR_CONFIG_N4096_K2_MP) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] { *out = opir4::derive(*layout); });
 }
@@ -1007,7 +1036,8 @@ opir_status opir_server_set_client_keys(opir_server *s, uint64_t client_id,
     if (!gsw_key) throw std::invalid_argument("PirServer session key bundle cannot be null");
     if (n_keys < h) throw std::invalid_argument("PirServer session lacks keys for its expansion height");
     if (n_keys && (!bv_keys || !galois_ks)) throw std::invalid_argument("null BV key arrays");
-    const size_t key_words = static_cast<size_t>(p.l_ks) * 2 * kN;  // one BvKeySwitchKey, u64
+    const uint64_t pw = poly_words(p);
+    const size_t key_words = static_cast<size_t>(p.l_ks) * 2 * pw;  // one BvKeySwitchKey, u64
     std::vector<uint64_t> ordered(static_cast<size_t>(h) * key_words);
     for (uint32_t d = 0; d < h; ++d) {
       const uint32_t want = kN / (1u << d) + 1;
@@ -1017,24 +1047,32 @@ opir_status opir_server_set_client_keys(opir_server *s, uint64_t client_id,
       if (found < 0) throw std::out_of_range("BvGaloisKeys::get: galois_k not found");
       std::memcpy(ordered.data() + d * key_words, bv_keys + found * key_words, key_words * 8);
     }
-    const size_t gsw_words = static_cast<size_t>(2) * p.l_key * 2 * kN;
-    for (uint64_t v : ordered)
-      if (v >= p.q) throw std::invalid_argument("BV key value not reduced mod q");
-    for (size_t i = 0; i < gsw_words; ++i)
-      if (gsw_key[i] >= p.q) throw std::invalid_argument("RGSW key value not reduced mod q");
+    const size_t gsw_words = static_cast<size_t>(2) * p.l_key * 2 * pw;
+    if (is_k2mp(p)) {  // limb-major rows: limb (i / N) % 2
+      const uint64_t m[2] = {p.q1, p.q2};
+      for (size_t i = 0; i < ordered.size(); ++i)
+        if (ordered[i] >= m[(i / kN) & 1]) throw std::invalid_argument("BV key value not reduced mod its limb");
+      for (size_t i = 0; i < gsw_words; ++i)
+        if (gsw_key[i] >= m[(i / kN) & 1]) throw std::invalid_argument("RGSW key value not reduced mod its limb");
+    } else {
+      for (uint64_t v : ordered)
+        if (v >= p.q) throw std::invalid_argument("BV key value not reduced mod q");
+      for (size_t i = 0; i < gsw_words; ++i)
+        if (gsw_key[i] >= p.q) throw std::invalid_argument("RGSW key value not reduced mod q");
+    }
     DeviceGuard g(s->device);
     ClientKeys k;
     DevBuf<uint64_t> tmp;
     tmp.alloc(std::max(ordered.size(), gsw_words));
-    k.bv.alloc(std::max<size_t>(1, ordered.size() * 2));
-    k.gsw.alloc(gsw_words * 2);
+    k.bv.alloc(std::max<size_t>(1, ordered.size() / pw * 2 * kN));
+    k.gsw.alloc(gsw_words / pw * 2 * kN);
     if (!ordered.empty()) {
       ck(cudaMemcpyAsync(tmp.p, ordered.data(), ordered.size() * 8, cudaMemcpyHostToDevice, s->stream), "bv upload");
-      opir::launch_split_u64(s->dp, tmp.p, k.bv.p, 1, ordered.size() / kN, 0, s->stream);
+      opir::launch_split_u64(s->dp, tmp.p, k.bv.p, 1, ordered.size() / pw, 0, s->stream);
       ck(cudaStreamSynchronize(s->stream), "bv split");
     }
     ck(cudaMemcpyAsync(tmp.p, gsw_key, gsw_words * 8, cudaMemcpyHostToDevice, s->stream), "gsw upload");
-    opir::launch_split_u64(s->dp, tmp.p, k.gsw.p, 1, gsw_words / kN, 0, s->stream);
+    opir::launch_split_u64(s->dp, tmp.p, k.gsw.p, 1, gsw_words / pw, 0, s->stream);
     ck(cudaStreamSynchronize(s->stream), "gsw split");
     ClientKeys &slot = s->clients[client_id];
     std::swap(slot.bv.p, k.bv.p); std::swap(slot.bv.n, k.bv.n);
@@ -1107,10 +1145,11 @@ opir_status opir_server_make_query_batch(opir_server *s, uint32_t n, const uint6
       DeviceGuard g(s->device);
       return s->c4->make_query_batch(n, client_ids, queries, responses, c4_events(s));
     }
-    check_query_values(s, queries, static_cast<size_t>(n) * 2 * kN);
+    const uint64_t pw = poly_words(s->params);
+    check_query_values(s, queries, static_cast<size_t>(n) * 2 * pw);
     DeviceGuard g(s->device);
     ensure_capacity(s, n);
-    ck(cudaMemcpyAsync(s->q_u64.p, queries, static_cast<size_t>(n) * 2 * kN * 8,
+    ck(cudaMemcpyAsync(s->q_u64.p, queries, static_cast<size_t>(n) * 2 * pw * 8,
                        cudaMemcpyHostToDevice, s->stream), "query upload");
     run_pipeline(s, client_ids, n, s->q_u64.p, s->resp_u64.p, nullptr);
     ck(cudaMemcpyAsync(responses, s->resp_u64.p, static_cast<size_t>(n) * 2 * kN * 8,
@@ -1168,6 +1207,9 @@ opir_status opir_server_create_row_shard(const opir_params *params, uint32_t sha
     checked = checked_params(*params);
     if (checked.view != OPIR_VIEW_LAYOUT)
       throw std::invalid_argument("row shards split a database layout");
+    if (is_k2mp(checked))
+      throw std::invalid_argument(
+          "row shards are built for CONFIG_N2048_K1_COMP and CONFIG_N4096_K2_MP");
     rs = opir::row_shard(checked.other_dim_sz, checked.num_dims, shard, num_shards);
     checked.view = OPIR_VIEW_ROW_SHARD;
   });
@@ -1283,17 +1325,33 @@ opir_status opir_server_set_priority(opir_server *s, int priority) {
   });
 }
 
+opir_status opir_server_set_scan_wait_limit(opir_server *s, uint64_t cycles) {
+  if (!s) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(s, [&] {
+    DeviceGuard g(s->device);
+    if (cycles > (1ull << 40)) throw std::invalid_argument("wait limit above 2^40 cycles");
+    const long long c = static_cast<long long>(cycles);
+    ck(cudaStreamSynchronize(s->stream), "set_scan_wait_limit");
+    if (s->c4) return s->c4->set_scan_wait_limit(c);
+    if (c != s->scan_wait) clear_graphs(s);  // captured scans hold the old limit
+    s->scan_wait = c;
+  });
+}
+
 opir_status opir_plan_memory(const opir_params *params, opir_memory_plan *out) {
   if (!params || !out) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] {
     if (is_c4(*params)) return opir4::Server::plan_memory(*params, out);
-    if (params->poly_degree != static_cast<uint32_t>(kN) || params->num_limbs != 1)
-      throw std::invalid_argument("unsupported parameter set (CONFIG_N2048_K1_COMP or CONFIG_N4096_K2_MP)");
+    if (!is_k2mp(*params) &&
+        (params->poly_degree != static_cast<uint32_t>(kN) || params->num_limbs != 1))
+      throw std::invalid_argument(
+          "unsupported parameter set (CONFIG_N2048_K1_COMP, CONFIG_N2048_K2_MP or CONFIG_N4096_K2_MP)");
     uint64_t slots = 0;
     const opir::Shape sh = make_shape(*params, &slots);
     const uint32_t rb = resp_bytes_of(*params);
-    const uint64_t one = plan_scratch(sh, slots, rb, 1).bytes();
-    const uint64_t two = plan_scratch(sh, slots, rb, 2).bytes();
+    const uint64_t pw = poly_words(*params);
+    const uint64_t one = plan_scratch(sh, slots, rb, 1, pw).bytes();
+    const uint64_t two = plan_scratch(sh, slots, rb, 2, pw).bytes();
     out->database_bytes = 2ull * kN * 4 * sh.other * sh.n0p + 16ull * kN * 4 + sizeof(uint32_t);
     out->client_key_bytes =
         (static_cast<uint64_t>(sh.h) * sh.l_ks * 2 * kN + 2ull * sh.l_key * 2 * kN) * 2 * 4;
@@ -1413,14 +1471,15 @@ opir_status opir_server_expand_query(opir_server *s, uint64_t client_id, const u
     require_view(s, s->params.view != OPIR_VIEW_MATRIX, "expand_query");
     DeviceGuard g(s->device);
     if (s->c4) return s->c4->expand_query(client_id, query, out);
-    check_query_values(s, query, 2 * kN);
+    const uint64_t pw = poly_words(s->params);
+    check_query_values(s, query, 2 * pw);
     ensure_capacity(s, 1);
     upload_keyptrs(s, &client_id, 1);
-    ck(cudaMemcpyAsync(s->q_u64.p, query, 2 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    ck(cudaMemcpyAsync(s->q_u64.p, query, 2 * pw * 8, cudaMemcpyHostToDevice, s->stream), "upload");
     opir::launch_split_u64(s->dp, s->q_u64.p, s->lvl[0].p, 1, 2, 0, s->stream);
     const uint32_t *leaves = run_expand(s, 1);
     DevBuf<uint64_t> o;
-    o.alloc(static_cast<size_t>(s->shape.useful) * 2 * kN);
+    o.alloc(static_cast<size_t>(s->shape.useful) * 2 * pw);
     opir::launch_compose_u64(s->dp, leaves, 0, o.p, 1, 2ull * s->shape.useful, s->stream);
     ck(cudaMemcpyAsync(out, o.p, o.n * 8, cudaMemcpyDeviceToHost, s->stream), "download");
     ck(cudaStreamSynchronize(s->stream), "expand_query");
@@ -1438,21 +1497,22 @@ opir_status opir_server_complete_selectors(opir_server *s, uint64_t client_id,
       return s->c4->complete_selectors(client_id, expanded, out);
     }
     const opir::Shape &sh = s->shape;
-    check_query_values(s, expanded, static_cast<size_t>(sh.useful) * 2 * kN);
+    const uint64_t pw = poly_words(s->params);
+    check_query_values(s, expanded, static_cast<size_t>(sh.useful) * 2 * pw);
     DeviceGuard g(s->device);
     ensure_capacity(s, 1);
     upload_keyptrs(s, &client_id, 1);
     const uint32_t nsel = sh.num_dims - 1;
     if (nsel == 0) return;
     DevBuf<uint64_t> in;
-    in.alloc(static_cast<size_t>(sh.useful) * 2 * kN);
+    in.alloc(static_cast<size_t>(sh.useful) * 2 * pw);
     ck(cudaMemcpyAsync(in.p, expanded, in.n * 8, cudaMemcpyHostToDevice, s->stream), "upload");
     opir::launch_split_u64(s->dp, in.p, s->lvl[0].p, 1, 2ull * sh.useful, 0, s->stream);
     opir::launch_selectors(s->dp, sh, s->lvl[0].p, s->lvl_slots, s->keyptrs.p + 1, s->sel.p, 1,
                            s->stream);
     const uint64_t polys = 2ull * nsel * 2 * sh.l_ep;
     DevBuf<uint64_t> o;
-    o.alloc(polys * kN);
+    o.alloc(polys * pw);
     opir::launch_compose_u64(s->dp, s->sel.p, 0, o.p, 1, polys, s->stream);
     ck(cudaMemcpyAsync(out, o.p, o.n * 8, cudaMemcpyDeviceToHost, s->stream), "download");
     ck(cudaStreamSynchronize(s->stream), "complete_selectors");
@@ -1470,16 +1530,17 @@ opir_status opir_server_evaluate_first_dim(opir_server *s, const uint64_t *fst_q
     }
     if (!s->db_loaded) throw std::runtime_error("evaluate_first_dim before load_data");
     const opir::Shape &sh = s->shape;
-    check_query_values(s, fst_query, static_cast<size_t>(sh.n0) * 2 * kN);
+    const uint64_t pw = poly_words(s->params);
+    check_query_values(s, fst_query, static_cast<size_t>(sh.n0) * 2 * pw);
     DeviceGuard g(s->device);
     ensure_capacity(s, 1);
     DevBuf<uint64_t> in;
-    in.alloc(static_cast<size_t>(sh.n0) * 2 * kN);
+    in.alloc(static_cast<size_t>(sh.n0) * 2 * pw);
     ck(cudaMemcpyAsync(in.p, fst_query, in.n * 8, cudaMemcpyHostToDevice, s->stream), "upload");
     opir::launch_split_u64(s->dp, in.p, s->lvl[0].p, 1, 2ull * sh.n0, 0, s->stream);
     run_first_dim(s, s->lvl[0].p, 1);
     DevBuf<uint64_t> o;
-    o.alloc(static_cast<size_t>(sh.other) * 2 * kN);
+    o.alloc(static_cast<size_t>(sh.other) * 2 * pw);
     opir::launch_compose_u64(s->dp, s->mid[0].p, 0, o.p, 1, 2ull * sh.other, s->stream);
     ck(cudaMemcpyAsync(out, o.p, o.n * 8, cudaMemcpyDeviceToHost, s->stream), "download");
     ck(cudaStreamSynchronize(s->stream), "evaluate_first_dim");
@@ -1502,26 +1563,27 @@ opir_status opir_server_evaluate_other_dim(opir_server *s, const uint64_t *mid,
     if (!mid || !out || (nsel && !selectors)) throw std::invalid_argument("null argument");
     if (nsel && sh.other < (1u << (nsel - 1)))
       throw std::invalid_argument("evaluate_other_dim: layout has fewer candidates than its selector tree");
-    check_query_values(s, mid, static_cast<size_t>(sh.other) * 2 * kN);
+    const uint64_t pw = poly_words(s->params);
+    check_query_values(s, mid, static_cast<size_t>(sh.other) * 2 * pw);
     DeviceGuard g(s->device);
     ensure_capacity(s, 1);
     DevBuf<uint64_t> in;
     const uint64_t sel_polys = 2ull * nsel * 2 * sh.l_ep;
-    in.alloc(std::max<uint64_t>(static_cast<uint64_t>(sh.other) * 2, sel_polys) * kN);
-    ck(cudaMemcpyAsync(in.p, mid, static_cast<size_t>(sh.other) * 2 * kN * 8,
+    in.alloc(std::max<uint64_t>(static_cast<uint64_t>(sh.other) * 2, sel_polys) * pw);
+    ck(cudaMemcpyAsync(in.p, mid, static_cast<size_t>(sh.other) * 2 * pw * 8,
                        cudaMemcpyHostToDevice, s->stream), "upload");
     opir::launch_split_u64(s->dp, in.p, s->mid[0].p, 1, 2ull * sh.other, 0, s->stream);
     if (nsel) {
       ck(cudaStreamSynchronize(s->stream), "upload");
-      ck(cudaMemcpyAsync(in.p, selectors, sel_polys * kN * 8, cudaMemcpyHostToDevice, s->stream),
+      ck(cudaMemcpyAsync(in.p, selectors, sel_polys * pw * 8, cudaMemcpyHostToDevice, s->stream),
          "upload");
       opir::launch_split_u64(s->dp, in.p, s->sel.p, 1, sel_polys, 0, s->stream);
     }
     const uint32_t *r = run_other_dims(s, 1);
     DevBuf<uint64_t> o;
-    o.alloc(2 * kN);
+    o.alloc(2 * pw);
     opir::launch_compose_u64(s->dp, r, 0, o.p, 1, 2, s->stream);
-    ck(cudaMemcpyAsync(out, o.p, 2 * kN * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    ck(cudaMemcpyAsync(out, o.p, 2 * pw * 8, cudaMemcpyDeviceToHost, s->stream), "download");
     ck(cudaStreamSynchronize(s->stream), "evaluate_other_dim");
   });
 }
@@ -1538,25 +1600,26 @@ opir_status opir_server_ext_prod_mux(opir_server *s, const uint64_t *x, const ui
     sh.other = 2;
     sh.num_dims = 2;
     const uint64_t sel_polys = 2ull * 2 * sh.l_ep;
-    check_query_values(s, x, 2 * kN);
-    check_query_values(s, y, 2 * kN);
-    check_query_values(s, selector, sel_polys * kN);
+    const uint64_t pw = poly_words(s->params);
+    check_query_values(s, x, 2 * pw);
+    check_query_values(s, y, 2 * pw);
+    check_query_values(s, selector, sel_polys * pw);
     DevBuf<uint64_t> in;
     DevBuf<uint32_t> xy, res, sel;
-    in.alloc(std::max<uint64_t>(4, sel_polys) * kN);
+    in.alloc(std::max<uint64_t>(4, sel_polys) * pw);
     xy.alloc(2 * kCtWords);
     res.alloc(2 * kCtWords);
     sel.alloc(sel_polys / 2 * kCtWords);
-    ck(cudaMemcpyAsync(in.p, x, 2 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
-    ck(cudaMemcpyAsync(in.p + 2 * kN, y, 2 * kN * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    ck(cudaMemcpyAsync(in.p, x, 2 * pw * 8, cudaMemcpyHostToDevice, s->stream), "upload");
+    ck(cudaMemcpyAsync(in.p + 2 * pw, y, 2 * pw * 8, cudaMemcpyHostToDevice, s->stream), "upload");
     opir::launch_split_u64(s->dp, in.p, xy.p, 1, 4, 0, s->stream);
     ck(cudaStreamSynchronize(s->stream), "upload");
-    ck(cudaMemcpyAsync(in.p, selector, sel_polys * kN * 8, cudaMemcpyHostToDevice, s->stream),
+    ck(cudaMemcpyAsync(in.p, selector, sel_polys * pw * 8, cudaMemcpyHostToDevice, s->stream),
        "upload");
     opir::launch_split_u64(s->dp, in.p, sel.p, 1, sel_polys, 0, s->stream);
     opir::launch_mux_level(s->dp, sh, 0, 1, xy.p, res.p, 2, sel.p, 1, s->stream);
     opir::launch_compose_u64(s->dp, res.p, 0, in.p, 1, 2, s->stream);
-    ck(cudaMemcpyAsync(out, in.p, 2 * kN * 8, cudaMemcpyDeviceToHost, s->stream), "download");
+    ck(cudaMemcpyAsync(out, in.p, 2 * pw * 8, cudaMemcpyDeviceToHost, s->stream), "download");
     ck(cudaStreamSynchronize(s->stream), "ext_prod_mux");
   });
 }
@@ -1612,6 +1675,8 @@ opir_status opir_tree_level_create(const opir_params *scheme, const opir_tree_pa
   opir_tree_level_plan plan{};
   const opir_status vs = guarded(nullptr, [&] {
     const opir_params sch = checked_params(*scheme);
+    if (is_k2mp(sch))
+      throw std::invalid_argument("tree PIR is built for CONFIG_N2048_K1_COMP and CONFIG_N4096_K2_MP");
     const auto mods = opir::scheme_moduli(sch);
     opir::validate_tree_params(*tree, mods);
     if (tree->n != sch.poly_degree || tree->t != sch.plain_mod || tree->ell_beta != sch.l_ep ||

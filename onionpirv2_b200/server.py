@@ -7,7 +7,8 @@ ValueError (std::invalid_argument), unknown clients raise KeyError-compatible
 IndexError subclass OutOfRange (std::out_of_range), device failures raise
 RuntimeError. Ciphertexts are numpy uint64 arrays shaped (2, N) = (c0, c1)
 under CONFIG_N2048_K1_COMP and (2, 2, N) = (poly, RNS limb, coefficient)
-under CONFIG_N4096_K2_MP; responses are (2, N) mod small_q under both.
+under CONFIG_N2048_K2_MP and CONFIG_N4096_K2_MP; responses are (2, N) mod
+small_q under all three.
 """
 from __future__ import annotations
 
@@ -53,13 +54,14 @@ def _ptr(a: np.ndarray, t=C.c_uint64):
     return a.ctypes.data_as(C.POINTER(t))
 
 
-CONFIGS = {"CONFIG_N2048_K1_COMP": 0, "CONFIG_N4096_K2_MP": 1}
+CONFIGS = {"CONFIG_N2048_K1_COMP": 0, "CONFIG_N4096_K2_MP": 1, "CONFIG_N2048_K2_MP": 2}
 
 
 class PirParams:
     """PirParams().with_layout({target_num_pt, expansion_height, fst_dim_pow2})
     under one ACTIVE_CONFIG (includes/database_constants.h:31-40):
-    "CONFIG_N2048_K1_COMP" (default) or "CONFIG_N4096_K2_MP"."""
+    "CONFIG_N2048_K1_COMP" (default), "CONFIG_N2048_K2_MP" or
+    "CONFIG_N4096_K2_MP"."""
 
     def __init__(self, target_num_pt: int = 43690, expansion_height: int = 10,
                  fst_dim_pow2: bool = True, config: str = "CONFIG_N2048_K1_COMP"):
@@ -282,6 +284,12 @@ class PirServer:
         """Run the handle's work on a stream of this CUDA priority (lower =
         scheduled first); results are unchanged."""
         self._check(self._lib.opir_server_set_priority(self._h, int(priority)))
+
+    def set_scan_wait_limit(self, cycles: int):
+        """Limit (SM clock cycles) of each wait inside the tensor-core scan;
+        0 restores the default of about one second. A wait that runs out
+        makes the call raise RuntimeError, and the handle stays usable."""
+        self._check(self._lib.opir_server_set_scan_wait_limit(self._h, int(cycles)))
 
     def autotune(self, max_batch: int):
         """Time the tensor-core scan's tilings on this database for batches

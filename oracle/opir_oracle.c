@@ -128,6 +128,38 @@ int oracle_params_init(uint64_t target, uint32_t h, int pow2, opir_oracle_params
   return 0;
 }
 
+/* pir.cpp:14-98 with CONFIG_N2048_K1 (database_constants.h:61-76): one real
+ * NTT prime q of 60 bits (RnsMods {60}, no composite split: q1 = q2 = 0
+ * marks the single-prime set below), w_crt = its minimal 2N-th root,
+ * PlainMod 14, SmallQWidth 22, L_EP 5, L_KEY 8, L_KS 8; ct_mod_width 60. */
+int oracle_k1p_params_init(uint64_t target, uint32_t h, int pow2, opir_oracle_params *p) {
+  memset(p, 0, sizeof *p);
+  p->N = 2048;
+  if (target == 0 || h > log2u(p->N)) return -1;
+  const uint32_t bits = 60;
+  uint64_t q = 0;
+  if (oracle_ntt_primes(&bits, 1, p->N, &q)) return -1;
+  p->q = q;
+  p->q1 = p->q2 = 0;
+  p->w_crt = oracle_min_primitive_root(2ULL * p->N, q);
+  p->t = oracle_generate_prime(14);
+  const uint32_t sbits = 22;
+  if (oracle_ntt_primes(&sbits, 1, p->N, &p->small_q)) return -1;
+  p->small_q_width = (uint32_t)ceil(log2((double)p->small_q));
+  p->ct_mod_width = 60;
+  p->l_ep = 5; p->l_key = 8; p->l_ks = 8;
+  p->base_ep = (p->ct_mod_width + p->l_ep - 1) / p->l_ep;
+  p->base_key = (p->ct_mod_width + p->l_key - 1) / p->l_key;
+  p->base_ks = p->ct_mod_width / p->l_ks + 1;
+  uint64_t fst, dims;
+  if (oracle_calc_db_shape(target, p->l_ep, h, pow2, &fst, &dims)) return -1;
+  p->target_num_pt = target; p->expansion_height = h; p->fst_dim_pow2 = pow2 ? 1 : 0;
+  p->fst_dim_sz = fst; p->num_dims = (uint32_t)dims;
+  p->other_dim_sz = (target + fst - 1) / fst;
+  p->num_pt = fst * p->other_dim_sz;
+  return 0;
+}
+
 /* ======================================================================
  * negacyclic NTT (HEXL NTT semantics as restated in oracle/hexl_standin)
  * ====================================================================== */
@@ -596,14 +628,22 @@ void oracle_client_decrypt(const oracle_client *c, const uint64_t *resp, uint64_
 struct oracle_server {
   opir_oracle_params p;
   uint32_t *db_lo, *db_hi;  /* [coeff][pt] residues mod q1 / q2 (server.h:117-118) */
+  uint64_t *db64;           /* [coeff][pt] mod q, single-prime set (server.h:110-116) */
   uint64_t *bv, *gsw;
   int has_keys;
 };
+
+static int single_prime(const opir_oracle_params *p) { return p->q1 == 0; }
 
 oracle_server *oracle_server_new(const opir_oracle_params *p) {
   oracle_server *s = calloc(1, sizeof *s);
   s->p = *p;
   size_t n = (size_t)p->num_pt * p->N;
+  if (single_prime(p)) {
+    s->db64 = calloc(n, sizeof *s->db64);
+    if (!s->db64) { oracle_server_free(s); return NULL; }
+    return s;
+  }
   s->db_lo = calloc(n, sizeof *s->db_lo);
   s->db_hi = calloc(n, sizeof *s->db_hi);
   if (!s->db_lo || !s->db_hi) { oracle_server_free(s); return NULL; }
@@ -611,7 +651,7 @@ oracle_server *oracle_server_new(const opir_oracle_params *p) {
 }
 void oracle_server_free(oracle_server *s) {
   if (!s) return;
-  free(s->db_lo); free(s->db_hi); free(s->bv); free(s->gsw); free(s);
+  free(s->db_lo); free(s->db_hi); free(s->db64); free(s->bv); free(s->gsw); free(s);
 }
 
 /* server.cpp:80-171 (composite path) */
@@ -633,6 +673,10 @@ static int load_impl(oracle_server *s, uint64_t logical, const uint16_t *coeffs,
         else buf[c] = coeffs[(size_t)pt * N + c];
       }
       ntt_q(p, buf);
+      if (single_prime(p)) {
+        for (uint32_t c = 0; c < N; ++c) s->db64[(size_t)c * p->num_pt + pt] = buf[c];
+        continue;
+      }
       for (uint32_t c = 0; c < N; ++c) {
         s->db_lo[(size_t)c * p->num_pt + pt] = (uint32_t)(buf[c] % p->q1);
         s->db_hi[(size_t)c * p->num_pt + pt] = (uint32_t)(buf[c] % p->q2);
@@ -787,10 +831,60 @@ void oracle_level_mat_mat_32(const uint32_t *A, const uint32_t *B, uint64_t *out
   }
 }
 
+/* matrix.cpp:36-151 (level_mat_mat, u64 x u64 -> u128 chunks): per NTT
+ * level, C = A B mod q with A [m x n], B [n x 2], values < q < 2^60; at most
+ * 255 products (< 2^120 each) are summed before a reduction. */
+static void level_mat_mat_64(const uint64_t *A, const uint64_t *B, uint64_t *out, uint64_t m,
+                             uint64_t n, uint64_t levels, uint64_t q) {
+  long long L = (long long)levels;
+#pragma omp parallel for schedule(static)
+  for (long long lvl = 0; lvl < L; ++lvl) {
+    const uint64_t *Ap = A + (size_t)lvl * m * n, *Bp = B + (size_t)lvl * n * 2;
+    uint64_t *Cp = out + (size_t)lvl * m * 2;
+    for (uint64_t i = 0; i < m; ++i) {
+      u128 t0 = 0, t1 = 0;
+      const uint64_t *Ar = Ap + i * n;
+      for (uint64_t k = 0; k < n; ++k) {
+        t0 += (u128)Ar[k] * Bp[2 * k];
+        t1 += (u128)Ar[k] * Bp[2 * k + 1];
+        if ((k & 127) == 127) { t0 %= q; t1 %= q; }
+      }
+      Cp[2 * i] = (uint64_t)(t0 % q); Cp[2 * i + 1] = (uint64_t)(t1 % q);
+    }
+  }
+}
+
+/* server.cpp:313-405 for the single-prime set: query NTT, level_mat_mat mod
+ * q, inter_to_cts (server.cpp:408-527) with an INTT per candidate. */
+static int first_dim_single(const oracle_server *s, const uint64_t *fst_query, uint64_t *out) {
+  const opir_oracle_params *p = &s->p;
+  const uint32_t N = p->N;
+  const uint64_t n0 = p->fst_dim_sz, m = p->other_dim_sz;
+  const size_t ct = 2 * (size_t)N;
+  uint64_t *qm = malloc((size_t)N * n0 * 2 * 8), *tmp = malloc(ct * 8);
+  for (uint64_t i = 0; i < n0; ++i) {
+    memcpy(tmp, fst_query + i * ct, ct * 8);
+    ntt_q(p, tmp); ntt_q(p, tmp + N);
+    for (uint32_t lv = 0; lv < N; ++lv)
+      for (uint32_t c = 0; c < 2; ++c) qm[(size_t)lv * n0 * 2 + i * 2 + c] = tmp[(size_t)c * N + lv];
+  }
+  uint64_t *inter = malloc((size_t)N * m * 2 * 8);
+  level_mat_mat_64(s->db64, qm, inter, m, n0, N, p->q);
+  for (uint64_t j = 0; j < m; ++j) {
+    uint64_t *o = out + j * ct;
+    for (uint32_t lv = 0; lv < N; ++lv)
+      for (uint32_t c = 0; c < 2; ++c) o[(size_t)c * N + lv] = inter[(size_t)lv * m * 2 + j * 2 + c];
+    intt_q(p, o); intt_q(p, o + N);
+  }
+  free(qm); free(tmp); free(inter);
+  return 0;
+}
+
 /* server.cpp:313-361 + 264-304 + 529-597. fst_query: N0 x 2N coeff form;
  * out: other_dim x 2N coeff form. */
 int oracle_server_first_dim(const oracle_server *s, const uint64_t *fst_query, uint64_t *out) {
   const opir_oracle_params *p = &s->p;
+  if (single_prime(p)) return first_dim_single(s, fst_query, out);
   const uint32_t N = p->N;
   const uint64_t n0 = p->fst_dim_sz, m = p->other_dim_sz;
   const size_t ct = 2 * (size_t)N;

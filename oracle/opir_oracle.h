@@ -48,6 +48,9 @@ int oracle_calc_db_shape(uint64_t target, uint64_t l, uint32_t h, int pow2,
                          uint64_t *fst_dim_sz, uint64_t *num_dims);
 int oracle_params_init(uint64_t target_num_pt, uint32_t expansion_height,
                        int fst_dim_pow2, opir_oracle_params *out);
+/* CONFIG_N2048_K1 (the reference's default): one 60-bit prime q, q1 = q2 = 0 */
+int oracle_k1p_params_init(uint64_t target_num_pt, uint32_t expansion_height,
+                           int fst_dim_pow2, opir_oracle_params *out);
 
 /* ---- ring primitives ---- */
 void oracle_ntt_fwd(uint64_t *a, uint32_t N, uint64_t q, uint64_t root);
@@ -158,6 +161,9 @@ typedef struct {
 
 int oracle_c4_params_init(uint64_t target_num_pt, uint32_t expansion_height,
                           int fst_dim_pow2, opir_oracle_c4_params *out);
+/* CONFIG_N2048_K2_MP: the same two-limb routines at N = 2048, limbs of 29 bits */
+int oracle_k2mp_params_init(uint64_t target_num_pt, uint32_t expansion_height,
+                            int fst_dim_pow2, opir_oracle_c4_params *out);
 void oracle_c4_db_plaintext(uint64_t seed, uint64_t pt,
                             const opir_oracle_c4_params *p, uint64_t *out);
 

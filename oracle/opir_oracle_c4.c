@@ -53,6 +53,43 @@ int oracle_c4_params_init(uint64_t target, uint32_t h, int pow2, opir_oracle_c4_
   return 0;
 }
 
+/* ---- CONFIG_N2048_K2_MP (database_constants.h:96-110): the same K = 2 MP
+ *      pipeline at N = 2048 with RnsMods = {29, 29}, PlainMod 10,
+ *      SmallQWidth 22; ct_mod_width = 58, data/key gadget bases ceil(58 / l)
+ *      (pir.cpp:101-103), BV base 58 / L_KS + 1 (bv_keyswitch.cpp:73-76).
+ *      Every routine below is written for any N and limb width below 2^62, so
+ *      both two-limb sets share them. */
+int oracle_k2mp_params_init(uint64_t target, uint32_t h, int pow2, opir_oracle_c4_params *p) {
+  memset(p, 0, sizeof *p);
+  p->N = 2048u;
+  p->K = C4_K;
+  const uint32_t widths[2] = {29, 29};
+  if (oracle_ntt_primes(widths, 2, p->N, p->q) != 0) return -1;
+  for (int k = 0; k < 2; ++k) p->w[k] = oracle_min_primitive_root(2ULL * p->N, p->q[k]);
+  if (!invmod(p->q[0] % p->q[1], p->q[1], &p->q0_inv_mod_q1)) return -1;
+  for (int k = 0; k < 2; ++k) p->r64_mod_q[k] = (uint64_t)(((u128)1 << 64) % p->q[k]);
+  p->t = oracle_generate_prime(10);
+  const uint32_t sw = 22;
+  if (oracle_ntt_primes(&sw, 1, p->N, &p->small_q) != 0) return -1;
+  p->small_q_width = 22;
+  p->ct_mod_width = 58;
+  p->l_ep = 5; p->l_key = 8; p->l_ks = 8;
+  p->base_ep = (58 + 5 - 1) / 5;
+  p->base_key = (58 + 8 - 1) / 8;
+  p->base_ks = 58 / 8 + 1;
+  if (target == 0 || h > 11) return -1;
+  uint64_t fst = 0, nd = 0;
+  if (oracle_calc_db_shape(target, p->l_ep, h, pow2, &fst, &nd) != 0) return -1;
+  p->target_num_pt = target;
+  p->expansion_height = h;
+  p->fst_dim_pow2 = pow2 ? 1 : 0;
+  p->fst_dim_sz = fst;
+  p->num_dims = (uint32_t)nd;
+  p->other_dim_sz = (target + fst - 1) / fst;
+  p->num_pt = fst * p->other_dim_sz;
+  return 0;
+}
+
 static void ntt_k(const opir_oracle_c4_params *p, uint32_t k, uint64_t *a) {
   oracle_ntt_fwd(a, p->N, p->q[k], p->w[k]);
 }

@@ -80,6 +80,7 @@ def lib():
     if _lib is None:
         L = C.CDLL(build())
         L.oracle_params_init.argtypes = [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(Params)]
+        L.oracle_k1p_params_init.argtypes = [C.c_uint64, C.c_uint32, C.c_int, C.POINTER(Params)]
         L.oracle_client_new.argtypes = [C.POINTER(Params), C.c_uint64]
         L.oracle_client_new.restype = C.c_void_p
         L.oracle_client_new_keygen_parts.argtypes = [C.POINTER(Params), C.c_uint64, _u64p,
@@ -143,6 +144,7 @@ def lib():
         L.oracle_bv_apply_galois.argtypes = [C.POINTER(Params), _u64p, C.c_uint32, _u64p]
         P4 = C.POINTER(C4Params)
         L.oracle_c4_params_init.argtypes = [C.c_uint64, C.c_uint32, C.c_int, P4]
+        L.oracle_k2mp_params_init.argtypes = [C.c_uint64, C.c_uint32, C.c_int, P4]
         L.oracle_c4_db_plaintext.argtypes = [C.c_uint64, C.c_uint64, P4, _u64p]
         L.oracle_c4_client_new.argtypes = [P4, C.c_uint64]
         L.oracle_c4_client_new.restype = C.c_void_p
@@ -191,6 +193,17 @@ def ptr(a: np.ndarray, ctype=C.c_uint64):
 def params(target: int, height: int, pow2: bool = True) -> Params:
     p = Params()
     rc = lib().oracle_params_init(target, height, 1 if pow2 else 0, C.byref(p))
+    if rc != 0:
+        raise ValueError(f"invalid layout target={target} height={height}")
+    return p
+
+
+def k1p_params(target: int, height: int, pow2: bool = True) -> Params:
+    """CONFIG_N2048_K1 (the reference's default): one 60-bit NTT prime
+    (q1 = q2 = 0 in the struct); the Client/Server classes and functions take
+    these parameters too."""
+    p = Params()
+    rc = lib().oracle_k1p_params_init(target, height, 1 if pow2 else 0, C.byref(p))
     if rc != 0:
         raise ValueError(f"invalid layout target={target} height={height}")
     return p
@@ -393,6 +406,15 @@ def serialize(p: Params, resp: np.ndarray) -> bytes:
 def c4_params(target: int, height: int, pow2: bool = True) -> C4Params:
     p = C4Params()
     if lib().oracle_c4_params_init(target, height, 1 if pow2 else 0, C.byref(p)) != 0:
+        raise ValueError(f"invalid layout target={target} height={height}")
+    return p
+
+
+def k2mp_params(target: int, height: int, pow2: bool = True) -> C4Params:
+    """CONFIG_N2048_K2_MP: the two-limb routines at N = 2048 with 29-bit limbs
+    (the C4* classes and functions take these parameters too)."""
+    p = C4Params()
+    if lib().oracle_k2mp_params_init(target, height, 1 if pow2 else 0, C.byref(p)) != 0:
         raise ValueError(f"invalid layout target={target} height={height}")
     return p
 

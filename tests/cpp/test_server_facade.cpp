@@ -237,18 +237,22 @@ void test_pir_k1() {
   oracle_server_free(ref);
 }
 
-// ---------------------------------------------------------- CONFIG_N4096_K2_MP
-void test_pir_c4() {
+// ------------------------------- CONFIG_N4096_K2_MP and CONFIG_N2048_K2_MP
+// The two-limb sets: the oracle's two-limb routines take either set's
+// parameters (init picks the set).
+void test_pir_two_limb(opir_config config,
+                       int (*init)(uint64_t, uint32_t, int, opir_oracle_c4_params *),
+                       size_t target, size_t height, size_t idx, size_t resp_bytes,
+                       const std::string &label) {
   const uint64_t seed_db = 5;
-  const size_t target = 2048, height = 7;
-  PirParams pir_params = PirParams(OPIR_CONFIG_N4096_K2_MP).with_layout({target, height, true});
+  PirParams pir_params = PirParams(config).with_layout({target, height, true});
   opir_oracle_c4_params op;
-  oracle_c4_params_init(target, height, 1, &op);
+  init(target, static_cast<uint32_t>(height), 1, &op);
   const size_t N = pir_params.get_poly_degree(), kn = pir_params.get_coeff_val_cnt();
-  require_test(pir_params.K() == 2 && kn == 2 * N && pir_params.get_num_pt() == op.num_pt,
-               "c4 layout");
+  require_test(pir_params.K() == 2 && kn == 2 * N && N == op.N &&
+                   pir_params.get_num_pt() == op.num_pt,
+               label + " layout");
   PirServer server(pir_params);
-  const size_t idx = 777;
   server.load_data(target, [&](size_t i, RlwePt &pt) {
     pt.data.resize(N);
     oracle_c4_db_plaintext(seed_db, i, &op, pt.data.data());
@@ -270,19 +274,20 @@ void test_pir_c4() {
   RlweCt response = server.make_query(3, query);
   std::vector<uint64_t> want(2 * N);
   oracle_c4_server_make_query(ref, q.data(), want.data());
-  require_test(flat(response) == want, "c4 response bit-exact");
+  require_test(flat(response) == want, label + " response bit-exact");
   std::stringstream resp_stream;
-  require_test(server.save_resp_to_stream(response, resp_stream) == 51200, "c4 response bytes");
+  require_test(server.save_resp_to_stream(response, resp_stream) == resp_bytes,
+               label + " response bytes");
   std::vector<uint64_t> decrypted(N), r = flat(response);
   oracle_c4_client_decrypt(client, r.data(), decrypted.data());
   require_test(decrypted == server.direct_get_original_plaintext(idx).data,
-               "c4 decrypts to the recorded plaintext");
+               label + " decrypts to the recorded plaintext");
 
   // batched form (no counterpart in the reference) equals the single calls
   std::vector<RlweCt> qs = {query, query};
   std::vector<RlweCt> batch = server.make_query_batch({3, 3}, qs);
   require_test(batch.size() == 2 && flat(batch[0]) == want && flat(batch[1]) == want,
-               "c4 batch equals make_query");
+               label + " batch equals make_query");
   oracle_c4_client_free(client);
   oracle_c4_server_free(ref);
 }
@@ -291,7 +296,10 @@ void test_pir_c4() {
 
 int main() {
   test_pir_k1();
-  test_pir_c4();
+  test_pir_two_limb(OPIR_CONFIG_N4096_K2_MP, oracle_c4_params_init, 2048, 7, 777, 51200,
+                    "CONFIG_N4096_K2_MP");
+  test_pir_two_limb(OPIR_CONFIG_N2048_K2_MP, oracle_k2mp_params_init, 1000, 7, 777, 11264,
+                    "CONFIG_N2048_K2_MP");
   if (failures) {
     std::fprintf(stderr, "%d check(s) failed\n", failures);
     return 1;

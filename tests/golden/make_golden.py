@@ -14,6 +14,13 @@ limbs); those cases also store SHA-256 digests of the outputs of the
 reference's public stage methods (expand_query, complete_selectors,
 evaluate_first_dim, evaluate_other_dim) in the reference's own flat layouts.
 
+Two more sets come from the reference built with the other two parameter
+sets it ships: golden_k2mp.json / k2mp_*.resp.bin from oracle/_ref/opir_ref_k2mp
+(CONFIG_N2048_K2_MP: N = 2048, two 29-bit RNS limbs, the MP gadget) and
+golden_k1p.json / k1p_*.resp.bin from oracle/_ref/opir_ref_k1
+(CONFIG_N2048_K1, the reference's default: N = 2048, one 60-bit prime), with
+the same stage digests as the CONFIG_N4096_K2_MP set.
+
 A third set (golden_tree.json) runs the reference's tree PIR layer
 (src/tree_*.cpp) through the driver's "tree" mode: one packed tree query per
 case on the default scheme, unpacked by unpack_tree_query, and the digests of
@@ -24,6 +31,8 @@ its packed plaintext, must hold).
 Only needed when the fixtures must change; tests never run it.
     python tests/golden/make_golden.py            # CONFIG_N2048_K1_COMP set
     python tests/golden/make_golden.py --c4       # CONFIG_N4096_K2_MP set
+    python tests/golden/make_golden.py --k2mp     # CONFIG_N2048_K2_MP set
+    python tests/golden/make_golden.py --k1p      # CONFIG_N2048_K1 set
     python tests/golden/make_golden.py --tree     # tree PIR select_level set
     python tests/golden/make_golden.py --tree --c4  # the same under CONFIG_N4096_K2_MP
 """
@@ -40,6 +49,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "opir_ref")
 REF_BIN_C4 = os.path.join(REPO, "oracle", "_ref", "opir_ref_c4")
+REF_BIN_K2 = os.path.join(REPO, "oracle", "_ref", "opir_ref_k2mp")
+REF_BIN_K1 = os.path.join(REPO, "oracle", "_ref", "opir_ref_k1")
 
 # name, target_num_pt, expansion_height, fst_dim_pow2, db_seed, client_seed, index
 CASES = [
@@ -65,6 +76,31 @@ CASES_C4 = [
     ("c4_singleton_1_h0", 1, 0, 1, 11, 12, 0),
     ("c4_16384_h9", 16384, 9, 1, 13, 14, 9999),
 ]
+
+
+# CONFIG_N2048_K2_MP and CONFIG_N2048_K1: same columns
+CASES_K2 = [
+    ("k2mp_1000_h7", 1000, 7, 1, 3, 4, 777),
+    ("k2mp_1000_h7_last", 1000, 7, 1, 5, 6, 999),
+    ("k2mp_ragged_43_h5", 43, 5, 1, 7, 8, 42),
+    ("k2mp_tight_100_h6", 100, 6, 0, 9, 10, 57),
+    ("k2mp_singleton_1_h0", 1, 0, 1, 11, 12, 0),
+    ("k2mp_16384_h9", 16384, 9, 1, 13, 14, 9999),
+]
+CASES_K1 = [(n.replace("k2mp_", "k1p_"), t, h, pw, d + 100, c + 100, i)
+            for n, t, h, pw, d, c, i in CASES_K2]
+
+# per set: reference binary, cases, manifest, whether stage digests are kept
+SETS = {
+    "k1": (REF_BIN, CASES, "golden.json", False,
+           "oracle/_ref/opir_ref (reference sources + HEXL stand-in)"),
+    "c4": (REF_BIN_C4, CASES_C4, "golden_c4.json", True,
+           "oracle/_ref/opir_ref_c4 (reference sources, CONFIG_N4096_K2_MP, + HEXL stand-in)"),
+    "k2mp": (REF_BIN_K2, CASES_K2, "golden_k2mp.json", True,
+             "oracle/_ref/opir_ref_k2mp (reference sources, CONFIG_N2048_K2_MP, + HEXL stand-in)"),
+    "k1p": (REF_BIN_K1, CASES_K1, "golden_k1p.json", True,
+            "oracle/_ref/opir_ref_k1 (reference sources, CONFIG_N2048_K1, + HEXL stand-in)"),
+}
 
 
 # (name, L, a, client seed, leaf): the shapes and the boundary, mixed-bit and
@@ -140,8 +176,8 @@ def main_tree(c4: bool = False) -> int:
 def main() -> int:
     if "--tree" in sys.argv[1:]:
         return main_tree(c4="--c4" in sys.argv[1:])
-    c4 = "--c4" in sys.argv[1:]
-    ref_bin, cases_ = (REF_BIN_C4, CASES_C4) if c4 else (REF_BIN, CASES)
+    which = next((k for k in ("c4", "k2mp", "k1p") if "--" + k in sys.argv[1:]), "k1")
+    ref_bin, cases_, manifest_name, c4, generator = SETS[which]
     if not os.path.exists(ref_bin):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
     manifest = []
@@ -185,10 +221,8 @@ def main() -> int:
                     "sha256_stage_other_dim": sha(os.path.join(tmp, "other_dim.u64")),
                 })
             print(f"{name}: ok ({info['num_pt']} pts, load {info['load_s']}s)", flush=True)
-    with open(os.path.join(HERE, "golden_c4.json" if c4 else "golden.json"), "w") as f:
-        json.dump({"generator": ("oracle/_ref/opir_ref_c4 (reference sources, CONFIG_N4096_K2_MP, "
-                                 "+ HEXL stand-in)") if c4 else
-                   "oracle/_ref/opir_ref (reference sources + HEXL stand-in)",
+    with open(os.path.join(HERE, manifest_name), "w") as f:
+        json.dump({"generator": generator,
                    "db_coeff": "mix64(db_seed + (pt*N + c + 1) * 0x9E3779B97F4A7C15) % t",
                    "cases": manifest}, f, indent=1)
     return 0

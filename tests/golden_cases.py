@@ -31,6 +31,20 @@ def case_c4(name):
     raise KeyError(name)
 
 
+def cases_set(which):
+    """The cases of another parameter set: "k2mp" (CONFIG_N2048_K2_MP) or
+    "k1p" (CONFIG_N2048_K1), each made by the reference built with it."""
+    with open(os.path.join(GOLDEN_DIR, f"golden_{which}.json")) as f:
+        return json.load(f)["cases"]
+
+
+def case_set(which, name):
+    for c in cases_set(which):
+        if c["name"] == name:
+            return c
+    raise KeyError(name)
+
+
 def cases_tree():
     """Tree PIR select_level cases (reference tree layer, default scheme)."""
     with open(os.path.join(GOLDEN_DIR, "golden_tree.json")) as f:

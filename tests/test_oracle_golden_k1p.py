@@ -1,0 +1,52 @@
+"""The CONFIG_N2048_K1 oracle (oracle/opir_oracle.c with one 60-bit prime,
+the reference's default ACTIVE_CONFIG) against the reference itself:
+golden_k1p.json was produced by the unmodified reference sources built with
+CONFIG_N2048_K1 (tests/golden/make_golden.py --k1p). The seeded client must
+reproduce the reference client's keys and query, and the server restatement
+every public stage, the response and its 22-bit serialization; the client
+must decrypt the requested plaintext."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import golden_cases as G
+
+CASES = [c["name"] for c in G.cases_set("k1p")]
+
+
+def sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_k1p_oracle_matches_reference(name):
+    c = G.case_set("k1p", name)
+    p = O.k1p_params(c["target_num_pt"], c["expansion_height"], c["fst_dim_pow2"])
+    assert p.q == c["q"] and c["K"] == 1
+    assert (p.t, p.small_q, p.fst_dim_sz, p.num_dims, p.other_dim_sz) == (
+        c["t"], c["small_q"], c["fst_dim_sz"], c["num_dims"], c["other_dim_sz"])
+    assert (p.base_ep, p.base_key) == (c["base_log2"], c["base_log2_key"])
+    cl = O.Client(p, c["client_seed"])
+    bv, gsw = cl.bv_keys(), cl.gsw_key()
+    q = cl.query(c["index"])
+    assert sha(bv) == c["sha256_bv_keys_u64"]
+    assert sha(gsw) == c["sha256_gsw_key_u64"]
+    assert sha(q) == c["sha256_query_u64"]
+    s = O.Server(p)
+    s.load_seeded(c["target_num_pt"], c["db_seed"])
+    s.set_keys(bv, gsw)
+    exp = s.expand(q)
+    assert sha(exp) == c["sha256_stage_expand"]
+    sel = s.complete_selectors(exp)
+    assert sha(sel) == c["sha256_stage_selectors"]
+    mid = s.first_dim(exp)
+    assert sha(mid) == c["sha256_stage_first_dim"]
+    assert sha(s.other_dim(mid, sel)) == c["sha256_stage_other_dim"]
+    resp = s.make_query(q)
+    assert sha(resp) == c["sha256_response_u64"]
+    assert O.serialize(p, resp) == G.stream(c)
+    want = (O.db_plaintext(c["db_seed"], c["index"], p).astype(np.uint64)
+            if c["index"] < c["target_num_pt"] else np.zeros(p.N, np.uint64))
+    assert np.array_equal(cl.decrypt(resp), want)
