@@ -45,6 +45,9 @@ METRIC = "queries/s and DB GB/s at 1 GB DB, batched vs plain GPU (bit-exact); p5
 TARGET, HEIGHT = 262144, 10
 C4_TARGET, C4_HEIGHT = 1 << 20, 11
 C4_CONFIG = "CONFIG_N4096_K2_MP"
+K2_CONFIG = "CONFIG_N2048_K2_MP"
+# the parameter set of each workload (tree: its own scheme)
+CONFIGS = {"k1": "CONFIG_N2048_K1_COMP", "c4": C4_CONFIG, "k2mp": K2_CONFIG}
 # two timed layouts of the reference under CONFIG_N4096_K2_MP with the full
 # workload's first dimension (1024) and expansion height (11): 4 and 32
 # candidate rows
@@ -61,8 +64,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-queries", type=int, default=3)
-    ap.add_argument("--workload", choices=["k1", "c4", "tree"], default="k1",
+    ap.add_argument("--workload", choices=["k1", "c4", "k2mp", "tree"], default="k1",
                     help="k1: CONFIG_N2048_K1_COMP at 2^18 plaintexts; c4: CONFIG_N4096_K2_MP at 2^20; "
+                         "k2mp: CONFIG_N2048_K2_MP at 2^18; "
                          "tree: tree PIR path selection (L = 16, a = 3)")
     ap.add_argument("--target", type=int, default=None,
                     help="plaintexts (smaller layouts are for profiling captures)")
@@ -266,8 +270,8 @@ def ref_binary(suffix: str = "") -> str | None:
     return port if os.path.exists(port) else None
 
 
-def run_reference(queries: int, warmup: int, procs: int, seed: int) -> dict:
-    exe = ref_binary()
+def run_reference(queries: int, warmup: int, procs: int, seed: int, suffix: str = "") -> dict:
+    exe = ref_binary(suffix)
     if exe is None:
         raise FileNotFoundError("oracle/_ref is not built")
     cmd = [exe, "--mode", "time", "--target", str(TARGET), "--height", str(HEIGHT),
@@ -328,8 +332,9 @@ def bench_reference(args, world, rank):
     # a bounded sample: at most 8 timed queries (and 1 warm-up) per process,
     # ~2 s each on one core, so the run ends within a few minutes
     n_q, n_w = min(args.steps, 8), min(args.warmup, 1)
+    k2 = args.workload == "k2mp"
     try:
-        res = run_reference(n_q, n_w, procs, 7)
+        res = run_reference(n_q, n_w, procs, 7, "_k2mp" if k2 else "")
     except Exception as e:  # reference binary missing or failed
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU server: {e}"}))
         return
@@ -339,16 +344,25 @@ def bench_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": res["mean_ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"k1_comp N=2048, {TARGET} plaintexts, first dim 512 x 9 binary dims",
+        "config": {"workload": (f"{'CONFIG_N2048_K2_MP' if k2 else 'k1_comp'} N=2048, {TARGET} "
+                                f"plaintexts, first dim 512 x 9 binary dims"),
                    "batch": 1, "parallelism": f"{procs} host processes"},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": procs, "kind": "reference",
                          "sample": (f"reference make_query (oracle/_ref/{res['binary']}, HEXL stand-in) "
                                     f"on {procs} forked processes x {n_q} queries ({n_w} warm-up) after one "
                                     f"load_data; "
-                                    f"CPU {cpu_model()}")},
+                                    f"CPU {cpu_model()}; " + HEXL_CAVEAT)},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+# the CPU baseline runs the reference's sources against this repository's
+# HEXL stand-in (Intel HEXL cannot be installed here)
+HEXL_CAVEAT = ("the HEXL stand-in is written from the mathematics, not Intel HEXL's AVX-512 "
+               "kernels: the paper's single-thread HEXL figure (1031 MB/s over the 805 MB "
+               "logical database at 12 bits per coefficient, docs/2025-1142.pdf Table 2) is "
+               "about 1.28 queries/s per core at this layout, about 2.3x this stand-in's rate")
 
 
 def c4_workload_name(params) -> str:
@@ -405,8 +419,9 @@ def bench_ours(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=device)
     c4 = args.workload == "c4"
-    params = (PirParams(args.target, args.height, config=C4_CONFIG) if c4
-              else PirParams(args.target, args.height))
+    k2 = args.workload == "k2mp"
+    config = CONFIGS[args.workload]
+    params = PirParams(args.target, args.height, config=config)
     N = params.N
     B = args.batch
     ct_words = int(np.prod(params.ct_shape))
@@ -516,12 +531,19 @@ def bench_ours(args, world, rank, local):
     core_ms = stages["Core"]
     achieved = alg_bytes / (core_ms / 1e3) / 1e9
     traffic = ncu_traffic()
-    coeff_bits = 40 if c4 else 13    # t = generate_prime(40) / 4099
-    logical_db = params.num_pt * N * coeff_bits / 8
-    workload = (c4_workload_name(params) if c4 else
-                f"k1_comp N=2048, {args.target} plaintexts ({logical_db / 1e6:.1f} MB "
-                f"at 13 bits, {db_phys} B NTT form), first dim {params.fst_dim_sz} x "
-                f"{params.num_dims - 1} binary dims")
+    # logical database bytes: BASELINE's sizing is 13 bits per coefficient
+    # for every config; the parameter set's own t gives the second figure
+    # (t = 4099: 13 bits; generate_prime(40): 40; generate_prime(10) = 521: 10)
+    t_bits = int(params._p.plain_mod - 1).bit_length()
+    logical_db = params.num_pt * N * 13 / 8
+    logical_db_t = params.num_pt * N * t_bits / 8
+    if c4:
+        workload = c4_workload_name(params)
+    else:
+        workload = (f"{'CONFIG_N2048_K2_MP N=2048 two 29-bit limbs' if k2 else 'k1_comp N=2048'}, "
+                    f"{args.target} plaintexts ({logical_db / 1e6:.1f} MB at 13 bits, "
+                    f"{db_phys} B NTT form), first dim {params.fst_dim_sz} x "
+                    f"{params.num_dims - 1} binary dims")
     line = {
         "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,
@@ -536,6 +558,8 @@ def bench_ours(args, world, rank, local):
                           "from HBM every step"),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "db_gbs": logical_db * queries_done / (total_max / 1e3) / 1e9,
+        "db_gbs_at_log_t": {"bits": t_bits,
+                            "value": logical_db_t * queries_done / (total_max / 1e3) / 1e9},
         "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
         "stages_ms": {k: round(v, 4) for k, v in stages.items() if k != "calls"},
         "plain": {"batch": 1, "value": world * args.steps / (plain_total / 1e3), "unit": "queries/s",
@@ -552,8 +576,7 @@ def bench_ours(args, world, rank, local):
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "algorithmic_bytes": alg_bytes,
                      "traffic": (traffic or {}).get(f"{'c4_' if c4 else ''}batch_{B}")},
-        "int_pipe": int_pipe_roofline(params, C4_CONFIG if c4 else "CONFIG_N2048_K1_COMP", stages,
-                                      B, local),
+        "int_pipe": int_pipe_roofline(params, config, stages, B, local),
         "batch_sweep": sweep,
         "clocks": clk.summary(),
         "gpu_launches": launches,
@@ -571,13 +594,14 @@ def bench_ours(args, world, rank, local):
                                     "kind": "reference", "sample": f"unavailable: {e}"}
     if world == 1 and not args.no_cpu_baseline and not c4 and args.target == TARGET:
         try:
-            res = run_reference(args.cpu_queries, 0, 1, 7)
+            res = run_reference(args.cpu_queries, 0, 1, 7, "_k2mp" if k2 else "")
             line["cpu_baseline"] = {
                 "value": 1000.0 / res["mean_ms"], "unit": "queries/s", "cores": 1,
                 "kind": "reference",
                 "sample": (f"reference make_query (oracle/_ref/{res['binary']}, HEXL stand-in), "
                            f"{res['queries']} queries on the same layout after one untimed "
-                           f"load_data ({res['load_s']:.1f} s); CPU {cpu_model()}")}
+                           f"load_data ({res['load_s']:.1f} s); CPU {cpu_model()}; "
+                           + HEXL_CAVEAT)}
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unit": "queries/s", "cores": 0,
                                     "kind": "reference", "sample": f"unavailable: {e}"}
@@ -1180,8 +1204,7 @@ def bench_rows(args, world, rank, local):
         import torch.distributed as dist
         dist.destroy_process_group()
         return
-    coeff_bits = 40 if c4 else 13
-    logical_db = params.num_pt * N * coeff_bits / 8
+    logical_db = params.num_pt * N * 13 / 8   # BASELINE's 13 bits per coefficient
     line = {
         "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,

@@ -1900,7 +1900,9 @@ opir_status opir_tree_query(opir_tree *t, uint64_t client_id, const uint64_t *qu
 }
 
 opir_status opir_measure_butterfly_rate(opir_config config, int device, double *per_s) {
-  if (!per_s || (config != OPIR_CONFIG_N2048_K1_COMP && config != OPIR_CONFIG_N4096_K2_MP))
+  // CONFIG_N2048_K2_MP runs on the residue-pair NTT of CONFIG_N2048_K1_COMP
+  if (!per_s || (config != OPIR_CONFIG_N2048_K1_COMP && config != OPIR_CONFIG_N4096_K2_MP &&
+                 config != OPIR_CONFIG_N2048_K2_MP))
     return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] {
     DeviceGuard g(device);
