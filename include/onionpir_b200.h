@@ -57,7 +57,8 @@ typedef enum {
 typedef enum {
   OPIR_CONFIG_N2048_K1_COMP = 0,
   OPIR_CONFIG_N4096_K2_MP = 1,
-  OPIR_CONFIG_N2048_K2_MP = 2
+  OPIR_CONFIG_N2048_K2_MP = 2,
+  OPIR_CONFIG_N2048_K1 = 3
 } opir_config;
 
 /* PirLayoutConfig (includes/pir.h:199-203). */
@@ -75,8 +76,9 @@ typedef struct {
   uint64_t q;                     /* logical ciphertext modulus q1*q2 (K = 1,
                                      and K = 2 at N = 2048); 0 at N = 4096
                                      (the product needs 120 bits)          */
-  uint64_t q1, q2;                /* composite first-dim limbs (K = 1) or the
-                                     two RNS limbs (K = 2)                */
+  uint64_t q1, q2;                /* composite first-dim limbs (K = 1), or the
+                                     two RNS limbs (K = 2); 0 under
+                                     CONFIG_N2048_K1 (q itself is prime)   */
   uint64_t w1, w2, w_crt;         /* 2N-th roots: q1, q2 and CRT (mod q) */
   uint64_t q1_inv_mod_q2;
   uint64_t plain_mod;             /* t                                   */
@@ -136,8 +138,13 @@ opir_status opir_params_init(const opir_layout *layout, opir_params *out);
  * L_KEY 8, L_KS 8, the MP gadgets; includes/database_constants.h:96-110;
  * expansion_height <= 11). Handles on CONFIG_N2048_K2_MP take ciphertexts,
  * keys and stage arrays limb-major (K = 2) like CONFIG_N4096_K2_MP and
- * answer make_query, its batch forms and the stage methods; row shards and
- * tree PIR are built for the other two sets. Unknown config ->
+ * answer make_query, its batch forms and the stage methods;
+ * CONFIG_N2048_K1, the reference's default (includes/database_constants.h:
+ * 61-76), one real 60-bit NTT prime at N = 2048 (num_limbs 1, q the prime,
+ * q1 = q2 = 0), PlainMod 14, SmallQWidth 22, L_EP 5, L_KEY 8, L_KS 8 with
+ * signed single-modulus digits (expansion_height <= 11), ciphertexts
+ * [c0 (N)][c1 (N)] u64 mod q. Row shards and tree PIR are built for
+ * CONFIG_N2048_K1_COMP and CONFIG_N4096_K2_MP. Unknown config ->
  * OPIR_ERR_INVALID_ARGUMENT. */
 opir_status opir_params_init_config(opir_config config, const opir_layout *layout,
                                     opir_params *out);

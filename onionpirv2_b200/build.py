@@ -16,10 +16,10 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libonionpir_b200.so")
 SOURCES = ["opir_kernels.cu", "opir_server.cu", "opir_params.cpp", "opir_noalloc.cu",
-           "opir_scan_tc.cu", "opir_c4_kernels.cu", "opir_c4_server.cu", "opir_c4_scan_tc.cu", "opir_tree.cpp",
+           "opir_scan_tc.cu", "opir_c4_kernels.cu", "opir_c4_server.cu", "opir_c4_scan_tc.cu", "opir_k1p_kernels.cu", "opir_tree.cpp",
            "opir_shard.cpp", "opir_codec.cpp", "opir_codec_abi.cpp", "opir_client.cu"]
 HEADERS = ["opir_device.cuh", "opir_kernels.h", "opir_params.h", "opir_scan_tc.h", "opir_ntt.cuh",
-           "opir_host.h", "opir_c4_device.cuh", "opir_c4_kernels.h", "opir_c4_server.h", "opir_tc.cuh", "opir_tree.h",
+           "opir_host.h", "opir_c4_device.cuh", "opir_c4_kernels.h", "opir_c4_server.h", "opir_k1p_kernels.h", "opir_tc.cuh", "opir_tree.h",
            "opir_shard.h", "opir_codec.h", "opir_client.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",

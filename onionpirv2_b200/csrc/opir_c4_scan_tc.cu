@@ -348,9 +348,11 @@ uint32_t scan_tc4_max_stages(uint32_t ntile) {
 
 void launch_scan_tc4(const CUtensorMap &mapA, const CUtensorMap &mapQ, const Tc4Args &args,
                      int sm_count, cudaStream_t st) {
+  // zcount: 2 x 4096 levels of CONFIG_N4096_K2_MP, or the 2048 levels of the
+  // one-limb CONFIG_N2048_K1 (whose prime is limb 0's, kQ0)
   if ((args.ntile != 16 && args.ntile != 32) || args.stages < 2 ||
-      args.stages > scan_tc4_max_stages(args.ntile) || args.zcount != 2u * kN)
-    throw std::invalid_argument("two-limb tensor-core scan: unsupported tile configuration");
+      args.stages > scan_tc4_max_stages(args.ntile) || (args.zcount != 2u * kN && args.zcount != 2048u))
+    throw std::invalid_argument("tensor-core scan of 64-bit limbs: unsupported tile configuration");
   const size_t smem = scan_tc4_smem(args.ntile, args.stages);
   configure();
   const uint64_t items = static_cast<uint64_t>(args.col_tiles) * args.m_tiles * args.zcount;

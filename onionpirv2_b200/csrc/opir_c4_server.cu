@@ -1,8 +1,10 @@
-// Host orchestration of the CONFIG_N4096_K2_MP query path: the two-limb
-// counterpart of the PirServer methods (src/server.cpp) on the kernels of
-// opir_c4_kernels.cu. Every arithmetic step runs on the device; the host only
-// validates inputs, moves buffers and enqueues launches on the handle's
-// stream.
+// Host orchestration of the query paths whose limbs are 64-bit words: the
+// PirServer methods (src/server.cpp) under CONFIG_N4096_K2_MP (two 60-bit
+// limbs at N = 4096, the kernels of opir_c4_kernels.cu) and under
+// CONFIG_N2048_K1 (one 60-bit prime at N = 2048, opir_k1p_kernels.cu); both
+// share the 64-bit-limb tensor-core scan (opir_c4_scan_tc.cu). Every
+// arithmetic step runs on the device; the host only validates inputs, moves
+// buffers and enqueues launches on the handle's stream.
 #include "opir_c4_server.h"
 
 #include <algorithm>
@@ -12,6 +14,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "opir_k1p_kernels.h"
 #include "opir_params.h"
 #include "opir_scan_tc.h"
 
@@ -21,15 +24,15 @@ using opir::ck;
 
 namespace {
 
-constexpr uint64_t kCt = kCtWords;
-constexpr uint32_t kLKsRows = 8, kLKeyRows = 8;
+constexpr uint32_t kLKsRows = 8, kLKeyRows = 8;  // L_KS, L_KEY of both sets
 
-// Appends one ciphertext-shaped row (4N u64, limb-major polynomials) and
-// its Shoup companions floor(w 2^64 / q_limb) in the device row layout.
-void append_row(std::vector<uint64_t> &dst, const uint64_t *row) {
-  dst.insert(dst.end(), row, row + kCt);
-  for (int j = 0; j < kCtWords; ++j) {
-    const uint64_t q = ((j / kN) & 1) ? kQ1 : kQ0;
+// Appends one ciphertext-shaped row (2 N limbs u64, limb-major polynomials)
+// and its Shoup companions floor(w 2^64 / q_limb) in the device row layout.
+void append_row(std::vector<uint64_t> &dst, const uint64_t *row, uint32_t n, uint32_t limbs) {
+  const uint64_t ct = 2ull * n * limbs;
+  dst.insert(dst.end(), row, row + ct);
+  for (uint64_t j = 0; j < ct; ++j) {
+    const uint64_t q = (limbs == 2 && ((j / n) & 1)) ? kQ1 : kQ0;
     dst.push_back(static_cast<uint64_t>((static_cast<unsigned __int128>(row[j]) << 64) / q));
   }
 }
@@ -66,13 +69,14 @@ struct Plan {
   uint64_t bytes() const { return (2 * lvl + sel + 2 * mid + resp) * 8 + keyptrs * sizeof(void *); }
 };
 
-Plan plan_for(const Shape4 &s, uint64_t lvl_slots, uint32_t n) {
+// ct: u64 words per ciphertext (2 N limbs); row = 2 ct (with companions)
+Plan plan_for(const Shape4 &s, uint64_t lvl_slots, uint32_t n, uint32_t N, uint64_t ct) {
   const uint64_t nsel = s.num_dims > 1 ? s.num_dims - 1 : 0;
   Plan pl{};
-  pl.lvl = static_cast<size_t>(n) * lvl_slots * kCt;
-  pl.sel = std::max<uint64_t>(1, n * nsel * 2 * s.l_ep * kRowWords);
-  pl.mid = static_cast<size_t>(n) * s.other * kCt;
-  pl.resp = static_cast<size_t>(n) * 2 * kN;
+  pl.lvl = static_cast<size_t>(n) * lvl_slots * ct;
+  pl.sel = std::max<uint64_t>(1, n * nsel * 2 * s.l_ep * 2 * ct);
+  pl.mid = static_cast<size_t>(n) * s.other * ct;
+  pl.resp = static_cast<size_t>(n) * 2 * N;
   pl.keyptrs = 2ull * n;
   return pl;
 }
@@ -83,6 +87,14 @@ opir_params derive(const opir_layout &layout) { return opir::derive_params_c4(la
 
 Server::Server(const opir_params &p, cudaStream_t stream, const opir::RowShard *rs)
     : p_(p), st_(stream) {
+  k1_ = p_.num_limbs == 1;
+  if (k1_ && (p_.poly_degree != static_cast<uint32_t>(opir1::kN) || p_.q != opir1::kQ))
+    throw std::invalid_argument("unexpected CONFIG_N2048_K1 modulus");
+  n_ = p_.poly_degree;
+  limbs_ = p_.num_limbs;
+  ct_ = 2ull * n_ * limbs_;
+  row_ = 2 * ct_;
+  out_words_ = 2ull * n_;
   sh_ = shape_of(p_);
   tree_h_ = sh_.num_dims > 1 ? sh_.num_dims - 1 : 0;
   if (rs) {
@@ -91,12 +103,58 @@ Server::Server(const opir_params &p, cudaStream_t stream, const opir::RowShard *
     host_rows_ = rs->rows;
     sh_.other = static_cast<uint32_t>(rs->rows.size());
     sh_.num_pt = static_cast<uint64_t>(sh_.other) * sh_.n0;
-    out_words_ = kCt;
+    out_words_ = ct_;
     row_map_.alloc(rs->rows.size());
     ck(cudaMemcpy(row_map_.p, rs->rows.data(), rs->rows.size() * 4, cudaMemcpyHostToDevice),
        "row map");
   }
   lvl_slots_ = lvl_slots_of(sh_);
+  if (k1_) {
+    setup_k1_tables();
+  } else {
+    setup_c4_tables();
+  }
+  dp_.small_q = p_.small_q;
+  dp_.small_q_width = p_.small_q_width;
+  const uint64_t planes = static_cast<uint64_t>(n_) * limbs_ * 8;  // byte planes of the database
+  const uint64_t db_bytes = planes * sh_.other * sh_.n0p;
+  db8_.alloc(db_bytes);
+  ck(cudaMemsetAsync(db8_.p, 0, db_bytes, st_), "db memset");
+  opir::make_plane_map(&map_db_, db8_.p, sh_.n0p, sh_.other, planes, 128, 64);
+  err_.alloc(1);
+  ck(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), st_), "err memset");
+  progress_.alloc(1024);  // one counter per scan CTA (the grid is at most the SM count)
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "device");
+  ck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev), "sm count");
+  if (const char *g = std::getenv("OPIR_GRAPHS")) use_graphs_ = std::strcmp(g, "0") != 0;
+  ck(cudaStreamSynchronize(st_), "create");
+}
+
+// Twiddle tables of CONFIG_N2048_K1: [forward N][inverse N] (w, Shoup) of
+// the one limb, the first 64 of each to constant memory.
+void Server::setup_k1_tables() {
+  const opir::LimbTables64 t = opir::make_limb_tables64(n_, p_.q, p_.w1);
+  std::vector<ulonglong2> host(2ull * n_);
+  for (uint32_t i = 0; i < n_; ++i) {
+    host[i] = make_ulonglong2(t.fw[i], t.fw_sh[i]);
+    host[n_ + i] = make_ulonglong2(t.iw[i], t.iw_sh[i]);
+  }
+  tables_.alloc(host.size());
+  ck(cudaMemcpy(tables_.p, host.data(), host.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice),
+     "twiddle tables");
+  dp_.T.fwt[0] = dp_.T.fwt[1] = tables_.p;
+  dp_.T.iwt[0] = dp_.T.iwt[1] = tables_.p + n_;
+  const uint64_t ninv[2] = {t.n_inv, t.n_inv_sh}, w1n[2] = {t.w1_ninv, t.w1_ninv_sh};
+  opir1::upload_constants(t.fw.data(), t.fw_sh.data(), t.iw.data(), t.iw_sh.data(), ninv, w1n);
+}
+
+opir1::Dev1 Server::d1() const {
+  return opir1::Dev1{dp_.T.fwt[0], dp_.T.iwt[0], dp_.small_q, dp_.small_q_width};
+}
+
+// Twiddle tables of CONFIG_N4096_K2_MP: [limb][forward N][inverse N].
+void Server::setup_c4_tables() {
   const opir::LimbTables64 t[2] = {opir::make_limb_tables64(kN, p_.q1, p_.w1),
                                    opir::make_limb_tables64(kN, p_.q2, p_.w2)};
   if (t[0].q != kQ0 || t[1].q != kQ1) throw std::invalid_argument("unexpected RNS limbs");
@@ -123,20 +181,31 @@ Server::Server(const opir_params &p, cudaStream_t stream, const opir::RowShard *
   upload_constants(fw, fw_sh, iw, iw_sh, ninv, w1n);
   dp_.q0inv = p_.q1_inv_mod_q2;
   dp_.q0inv_sh = static_cast<uint64_t>((static_cast<unsigned __int128>(dp_.q0inv) << 64) / kQ1);
-  dp_.small_q = p_.small_q;
-  dp_.small_q_width = p_.small_q_width;
-  const uint64_t db_bytes = 2ull * kN * 8 * sh_.other * sh_.n0p;
-  db8_.alloc(db_bytes);
-  ck(cudaMemsetAsync(db8_.p, 0, db_bytes, st_), "db memset");
-  opir::make_plane_map(&map_db_, db8_.p, sh_.n0p, sh_.other, 2ull * kN * 8, 128, 64);
-  err_.alloc(1);
-  ck(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), st_), "err memset");
-  progress_.alloc(1024);  // one counter per scan CTA (the grid is at most the SM count)
-  int dev = 0;
-  ck(cudaGetDevice(&dev), "device");
-  ck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, dev), "sm count");
-  if (const char *g = std::getenv("OPIR_GRAPHS")) use_graphs_ = std::strcmp(g, "0") != 0;
-  ck(cudaStreamSynchronize(st_), "create");
+}
+
+// ------------------------------------------------------------------ launches
+// The kernels of this handle's parameter set.
+void Server::run_db_preprocess(const uint64_t *coeffs, uint64_t coeff_pt_begin, uint64_t seed,
+                               uint64_t logical, uint64_t pb, uint64_t pe) {
+  if (k1_)
+    opir1::launch_db_preprocess(d1(), sh_, coeffs, coeff_pt_begin, seed, p_.plain_mod, logical, pb,
+                                pe, db8_.p, st_);
+  else
+    launch_db_preprocess(dp_, sh_, coeffs, coeff_pt_begin, seed, p_.plain_mod, logical, pb, pe,
+                         row_map_.p, db8_.p, st_);
+}
+void Server::run_selectors(const uint64_t *leaves, const uint64_t *const *gsw, uint32_t n) {
+  if (k1_) opir1::launch_selectors(d1(), sh_, leaves, lvl_slots_, gsw, sel_.p, n, st_);
+  else launch_selectors(dp_, sh_, leaves, lvl_slots_, gsw, sel_.p, n, st_);
+}
+void Server::run_mux(const Shape4 &sh, uint32_t level, uint32_t tree_h, const uint64_t *in,
+                     uint64_t *out, uint64_t mid_stride, const uint64_t *sel, uint32_t n) {
+  if (k1_) opir1::launch_mux_level(d1(), sh, level, tree_h, in, out, mid_stride, sel, n, st_);
+  else launch_mux_level(dp_, sh, level, tree_h, in, out, mid_stride, sel, n, st_);
+}
+void Server::run_modswitch(const uint64_t *ct, uint64_t ct_stride, uint64_t *resp, uint32_t n) {
+  if (k1_) opir1::launch_modswitch(d1(), ct, ct_stride, resp, nullptr, resp_bytes_of(p_), n, st_);
+  else launch_modswitch(dp_, ct, ct_stride, resp, nullptr, resp_bytes_of(p_), n, st_);
 }
 
 Server::~Server() {
@@ -155,17 +224,16 @@ void Server::load_tiles(uint64_t logical, Fill &&fill) {
     throw std::invalid_argument("PirServer::load_data logical plaintext count exceeds its layout");
   const uint64_t local_pt = static_cast<uint64_t>(sh_.other) * sh_.n0;
   const uint64_t tile = 2048;
-  std::vector<uint64_t> host(tile * kN);
+  std::vector<uint64_t> host(tile * n_);
   opir::DevBuf<uint64_t> dev;
-  dev.alloc(tile * kN);
+  dev.alloc(tile * n_);
   db_loaded_ = false;
   for (uint64_t pb = 0; pb < local_pt; pb += tile) {
     const uint64_t pe = std::min<uint64_t>(local_pt, pb + tile);
-    opir::fill_runs(host_rows_, sh_.n0, logical, pb, pe, host.data(), fill, kN);
-    ck(cudaMemcpyAsync(dev.p, host.data(), (pe - pb) * kN * 8, cudaMemcpyHostToDevice, st_),
+    opir::fill_runs(host_rows_, sh_.n0, logical, pb, pe, host.data(), fill, n_);
+    ck(cudaMemcpyAsync(dev.p, host.data(), (pe - pb) * n_ * 8, cudaMemcpyHostToDevice, st_),
        "db upload");
-    launch_db_preprocess(dp_, sh_, dev.p, pb, 0, p_.plain_mod, logical, pb, pe, row_map_.p, db8_.p,
-                         st_);
+    run_db_preprocess(dev.p, pb, 0, logical, pb, pe);
     ck(cudaStreamSynchronize(st_), "db preprocess");
   }
   db_loaded_ = true;
@@ -174,8 +242,8 @@ void Server::load_tiles(uint64_t logical, Fill &&fill) {
 void Server::load_db(uint64_t logical, const uint64_t *coeffs) {
   const uint64_t t = p_.plain_mod;
   load_tiles(logical, [&](uint64_t b, uint64_t e, uint64_t *dst) {
-    const uint64_t *src = coeffs + b * kN;
-    for (uint64_t i = 0; i < (e - b) * kN; ++i) {
+    const uint64_t *src = coeffs + b * n_;
+    for (uint64_t i = 0; i < (e - b) * n_; ++i) {
       if (src[i] >= t)
         throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
       dst[i] = src[i];
@@ -184,9 +252,14 @@ void Server::load_db(uint64_t logical, const uint64_t *coeffs) {
 }
 
 void Server::load_db_u16(uint64_t logical, const uint16_t *coeffs) {
+  const uint64_t t = p_.plain_mod;
   load_tiles(logical, [&](uint64_t b, uint64_t e, uint64_t *dst) {
-    const uint16_t *src = coeffs + b * kN;
-    for (uint64_t i = 0; i < (e - b) * kN; ++i) dst[i] = src[i];  // < 2^16 < t
+    const uint16_t *src = coeffs + b * n_;
+    for (uint64_t i = 0; i < (e - b) * n_; ++i) {
+      if (src[i] >= t)
+        throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
+      dst[i] = src[i];
+    }
   });
 }
 
@@ -194,9 +267,9 @@ void Server::load_db_source(uint64_t logical, opir_plaintext_source source, void
   const uint64_t t = p_.plain_mod;
   load_tiles(logical, [&](uint64_t b, uint64_t e, uint64_t *dst) {
     for (uint64_t idx = b; idx < e; ++idx) {
-      uint64_t *pt = dst + (idx - b) * kN;
+      uint64_t *pt = dst + (idx - b) * n_;
       if (source(user, idx, pt) != 0) throw std::invalid_argument("Plaintext source failed");
-      for (int c = 0; c < kN; ++c)
+      for (uint32_t c = 0; c < n_; ++c)
         if (pt[c] >= t)
           throw std::invalid_argument("Plaintext source coefficient exceeds the plaintext modulus");
     }
@@ -210,19 +283,19 @@ void Server::load_db_seeded(uint64_t logical, uint64_t seed) {
   const uint64_t chunk = 1ull << 18;
   const uint64_t local_pt = static_cast<uint64_t>(sh_.other) * sh_.n0;
   for (uint64_t pb = 0; pb < local_pt; pb += chunk)
-    launch_db_preprocess(dp_, sh_, nullptr, 0, seed, p_.plain_mod, logical, pb,
-                         std::min<uint64_t>(local_pt, pb + chunk), row_map_.p, db8_.p, st_);
+    run_db_preprocess(nullptr, 0, seed, logical, pb, std::min<uint64_t>(local_pt, pb + chunk));
   ck(cudaStreamSynchronize(st_), "db preprocess");
   db_loaded_ = true;
 }
 
 // ------------------------------------------------------------------ clients
 void Server::check_ct_values(const uint64_t *v, size_t cts) const {
+  const uint32_t parts = 2 * limbs_;  // polynomial limbs of a ciphertext, limb-major
   for (size_t c = 0; c < cts; ++c)
-    for (int part = 0; part < 4; ++part) {
-      const uint64_t q = (part & 1) ? kQ1 : kQ0;
-      const uint64_t *w = v + c * kCt + static_cast<size_t>(part) * kN;
-      for (int j = 0; j < kN; ++j)
+    for (uint32_t part = 0; part < parts; ++part) {
+      const uint64_t q = (limbs_ == 2 && (part & 1)) ? kQ1 : kQ0;
+      const uint64_t *w = v + c * ct_ + static_cast<size_t>(part) * n_;
+      for (uint32_t j = 0; j < n_; ++j)
         if (w[j] >= q) throw std::invalid_argument("ciphertext coefficient not reduced mod its limb");
     }
 }
@@ -233,10 +306,10 @@ void Server::set_client_keys(uint64_t id, const uint64_t *bv_keys, const uint32_
   if (!gsw_key) throw std::invalid_argument("PirServer session key bundle cannot be null");
   if (n_keys < h) throw std::invalid_argument("PirServer session lacks keys for its expansion height");
   if (n_keys && (!bv_keys || !galois_ks)) throw std::invalid_argument("null BV key arrays");
-  const size_t key_words = static_cast<size_t>(kLKsRows) * kCt;  // one BvKeySwitchKey
+  const size_t key_words = static_cast<size_t>(kLKsRows) * ct_;  // one BvKeySwitchKey
   std::vector<int> order(h);
   for (uint32_t d = 0; d < h; ++d) {
-    const uint32_t want = kN / (1u << d) + 1;
+    const uint32_t want = n_ / (1u << d) + 1;
     order[d] = -1;
     for (uint32_t i = 0; i < n_keys; ++i)
       if (galois_ks[i] == want) { order[d] = static_cast<int>(i); break; }
@@ -247,11 +320,11 @@ void Server::set_client_keys(uint64_t id, const uint64_t *bv_keys, const uint32_
   check_ct_values(gsw_key, gsw_rows);
   // device rows carry their Shoup companions (opir_c4_kernels.h)
   std::vector<uint64_t> bv_rows, gsw_rows_host;
-  bv_rows.reserve(static_cast<size_t>(h) * kLKsRows * kRowWords);
+  bv_rows.reserve(static_cast<size_t>(h) * kLKsRows * row_);
   for (uint32_t d = 0; d < h; ++d)
     for (uint32_t r = 0; r < kLKsRows; ++r)
-      append_row(bv_rows, bv_keys + order[d] * key_words + r * kCt);
-  for (size_t r = 0; r < gsw_rows; ++r) append_row(gsw_rows_host, gsw_key + r * kCt);
+      append_row(bv_rows, bv_keys + order[d] * key_words + r * ct_, n_, limbs_);
+  for (size_t r = 0; r < gsw_rows; ++r) append_row(gsw_rows_host, gsw_key + r * ct_, n_, limbs_);
   Keys k;
   k.bv.alloc(std::max<size_t>(1, bv_rows.size()));
   k.gsw.alloc(gsw_rows_host.size());
@@ -284,12 +357,12 @@ void Server::clear_graphs() {
 void Server::ensure_capacity(uint32_t n) {
   if (n <= cap_) return;
   clear_graphs();
-  const Plan pl = plan_for(sh_, lvl_slots_, n);
+  const Plan pl = plan_for(sh_, lvl_slots_, n, n_, ct_);
   for (auto &b : lvl_) b.alloc(pl.lvl);
   sel_.alloc(pl.sel);
   for (auto &b : mid_) b.alloc(pl.mid);
   resp_.alloc(static_cast<size_t>(n) * out_words_);
-  q_in_.alloc(static_cast<size_t>(n) * kCt);
+  q_in_.alloc(static_cast<size_t>(n) * ct_);
   keyptrs_.alloc(pl.keyptrs);
   cap_ = n;
 }
@@ -302,11 +375,13 @@ void Server::reserve(uint32_t max_batch) {
 void Server::plan_memory(const opir_params &p, opir_memory_plan *out) {
   const Shape4 s = shape_of(p);
   const uint64_t slots = lvl_slots_of(s);
-  const uint64_t one = plan_for(s, slots, 1).bytes(), two = plan_for(s, slots, 2).bytes();
-  out->database_bytes =
-      2ull * kN * 8 * s.other * s.n0p + 4ull * kN * sizeof(ulonglong2) + sizeof(uint32_t);
+  const uint32_t N = p.poly_degree;
+  const uint64_t ct = 2ull * N * p.num_limbs;
+  const uint64_t one = plan_for(s, slots, 1, N, ct).bytes(), two = plan_for(s, slots, 2, N, ct).bytes();
+  out->database_bytes = static_cast<uint64_t>(N) * p.num_limbs * 8 * s.other * s.n0p +
+                        2ull * N * p.num_limbs * sizeof(ulonglong2) + sizeof(uint32_t);
   out->client_key_bytes =
-      (static_cast<uint64_t>(p.expansion_height) * kLKsRows + 2ull * kLKeyRows) * kRowWords * 8;
+      (static_cast<uint64_t>(p.expansion_height) * kLKsRows + 2ull * kLKeyRows) * 2 * ct * 8;
   out->scratch_bytes_per_query = two - one;
   out->scratch_bytes_fixed = 2 * one - two;
 }
@@ -347,15 +422,19 @@ void Server::upload_keyptrs(const uint64_t *ids, uint32_t n) {
 
 // ------------------------------------------------------------------ pipeline
 void Server::stage_in(const uint64_t *d_queries, uint32_t n) {
-  ck(cudaMemcpy2DAsync(lvl_[0].p, lvl_slots_ * kCt * 8, d_queries, kCt * 8, kCt * 8, n,
+  ck(cudaMemcpy2DAsync(lvl_[0].p, lvl_slots_ * ct_ * 8, d_queries, ct_ * 8, ct_ * 8, n,
                        cudaMemcpyDeviceToDevice, st_), "query staging");
 }
 
 const uint64_t *Server::run_expand(uint32_t n) {
-  const uint64_t level_stride = static_cast<uint64_t>(kLKsRows) * kRowWords;
+  const uint64_t level_stride = static_cast<uint64_t>(kLKsRows) * row_;
   for (uint32_t d = 0; d < sh_.h; ++d)
-    launch_expand_level(dp_, sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p, lvl_slots_,
-                        keyptrs_.p, level_stride, n, st_);
+    if (k1_)
+      opir1::launch_expand_level(d1(), sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p,
+                                 lvl_slots_, keyptrs_.p, level_stride, n, st_);
+    else
+      launch_expand_level(dp_, sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p, lvl_slots_,
+                          keyptrs_.p, level_stride, n, st_);
   return lvl_[sh_.h & 1].p;
 }
 
@@ -372,13 +451,14 @@ void Server::launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n) {
   a.m_tiles = (sh_.other + 127) / 128;
   a.ncols = ncols;
   a.col_tiles = (ncols + a.ntile - 1) / a.ntile;
-  a.zcount = 2 * kN;
+  a.zcount = n_ * limbs_;
   a.cmat = cmat;
   a.err = err_.p;
   a.progress = progress_.p;
   a.wait_cycles = scan_wait_;
   CUtensorMap map_q;
-  opir::make_plane_map(&map_q, qb, sh_.n0p, ncols, 2ull * kN * 8, a.ntile, 64);
+  opir::make_plane_map(&map_q, qb, sh_.n0p, ncols, static_cast<uint64_t>(n_) * limbs_ * 8, a.ntile,
+                       64);
   launch_scan_tc4(map_db_, map_q, a, sm_count_, st_);
 }
 
@@ -413,19 +493,24 @@ void Server::run_first_dim(const uint64_t *leaves, uint32_t n, Events ev) {
   uint64_t *qm = lvl_[li ^ 1].p;
   uint8_t *qb = reinterpret_cast<uint8_t *>(lvl_[li].p);
   uint64_t *cmat = lvl_[li ^ 1].p;
-  launch_fst_ntt(dp_, sh_, leaves, lvl_slots_, qm, n, st_);
-  launch_fst_pack(sh_, qm, qb, n, st_);
+  if (k1_) {
+    opir1::launch_fst_ntt(d1(), sh_, leaves, lvl_slots_, qm, n, st_);
+    opir1::launch_fst_pack(sh_, qm, qb, n, st_);
+  } else {
+    launch_fst_ntt(dp_, sh_, leaves, lvl_slots_, qm, n, st_);
+    launch_fst_pack(sh_, qm, qb, n, st_);
+  }
   mark(ev, 6);
   launch_scan(qb, cmat, n);
   mark(ev, 7);
-  launch_epilogue(dp_, sh_, cmat, mid_[0].p, sh_.other, n, st_);
+  if (k1_) opir1::launch_epilogue(d1(), sh_, cmat, mid_[0].p, sh_.other, n, st_);
+  else launch_epilogue(dp_, sh_, cmat, mid_[0].p, sh_.other, n, st_);
 }
 
 const uint64_t *Server::run_other_dims(uint32_t n) {
   const uint32_t levels = tree_h_;
   for (uint32_t a = 0; a < levels; ++a)
-    launch_mux_level(dp_, sh_, a, levels, mid_[a & 1].p, mid_[(a + 1) & 1].p, sh_.other, sel_.p, n,
-                     st_);
+    run_mux(sh_, a, levels, mid_[a & 1].p, mid_[(a + 1) & 1].p, sh_.other, sel_.p, n);
   return mid_[levels & 1].p;
 }
 
@@ -436,17 +521,17 @@ void Server::enqueue_core(uint32_t n, const uint64_t *d_queries, uint64_t *d_res
   stage_in(d_queries, n);
   const uint64_t *leaves = run_expand(n);
   mark(ev, 1);
-  launch_selectors(dp_, sh_, leaves, lvl_slots_, keyptrs_.p + n, sel_.p, n, st_);
+  run_selectors(leaves, keyptrs_.p + n, n);
   mark(ev, 2);
   run_first_dim(leaves, n, ev);
   mark(ev, 3);
   const uint64_t *res = run_other_dims(n);
   mark(ev, 4);
-  if (out_words_ == kCt)  // row shard: the partial ciphertext, before the last levels
-    ck(cudaMemcpy2DAsync(d_resp, kCt * 8, res, static_cast<size_t>(sh_.other) * kCt * 8, kCt * 8, n,
+  if (out_words_ == ct_)  // row shard: the partial ciphertext, before the last levels
+    ck(cudaMemcpy2DAsync(d_resp, ct_ * 8, res, static_cast<size_t>(sh_.other) * ct_ * 8, ct_ * 8, n,
                          cudaMemcpyDeviceToDevice, st_), "partial copy");
   else
-    launch_modswitch(dp_, res, sh_.other, d_resp, nullptr, resp_bytes_of(p_), n, st_);
+    run_modswitch(res, sh_.other, d_resp, n);
   mark(ev, 5);
 }
 
@@ -519,7 +604,7 @@ void Server::run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_que
     return;
   }
   if (d_queries != q_in_.p)
-    ck(cudaMemcpyAsync(q_in_.p, d_queries, static_cast<size_t>(n) * kCt * 8,
+    ck(cudaMemcpyAsync(q_in_.p, d_queries, static_cast<size_t>(n) * ct_ * 8,
                        cudaMemcpyDeviceToDevice, st_), "query staging");
   launch_graph(n, ev);
   if (d_resp != resp_.p)
@@ -533,7 +618,7 @@ void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *q
   if (!db_loaded_) throw std::runtime_error("make_query before load_data");
   if (n == 0) return;
   ensure_capacity(n);
-  ck(cudaMemcpyAsync(q_in_.p, queries, static_cast<size_t>(n) * kCt * 8, cudaMemcpyHostToDevice,
+  ck(cudaMemcpyAsync(q_in_.p, queries, static_cast<size_t>(n) * ct_ * 8, cudaMemcpyHostToDevice,
                      st_), "query upload");
   run_pipeline(n, ids, q_in_.p, resp_.p, ev);
   ck(cudaMemcpyAsync(responses, resp_.p, static_cast<size_t>(n) * out_words_ * 8,
@@ -543,28 +628,28 @@ void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *q
 }
 
 void Server::combine_device(uint32_t n, const uint64_t *d_partials, uint64_t *d_responses) {
-  if (out_words_ != kCt) throw std::invalid_argument("combine_shards needs a row shard");
+  if (out_words_ != ct_) throw std::invalid_argument("combine_shards needs a row shard");
   const uint32_t G = num_shards_, h = sh_.num_dims - 1;
-  const uint64_t words = static_cast<uint64_t>(n) * G * kCt;
+  const uint64_t words = static_cast<uint64_t>(n) * G * ct_;
   for (auto &b : comb_)
     if (b.n < words) b.alloc(words);
   for (uint32_t g = 0; g < G; ++g)  // query i's G ciphertexts side by side
-    ck(cudaMemcpy2DAsync(comb_[0].p + static_cast<uint64_t>(g) * kCt, static_cast<size_t>(G) * kCt * 8,
-                         d_partials + static_cast<uint64_t>(g) * n * kCt, kCt * 8, kCt * 8, n,
+    ck(cudaMemcpy2DAsync(comb_[0].p + static_cast<uint64_t>(g) * ct_, static_cast<size_t>(G) * ct_ * 8,
+                         d_partials + static_cast<uint64_t>(g) * n * ct_, ct_ * 8, ct_ * 8, n,
                          cudaMemcpyDeviceToDevice, st_), "partial gather");
   int cur = 0;
   for (uint32_t a = tree_h_; a < h; ++a, cur ^= 1)
-    launch_mux_level(dp_, sh_, a, h, comb_[cur].p, comb_[cur ^ 1].p, G, sel_.p, n, st_);
-  launch_modswitch(dp_, comb_[cur].p, G, d_responses, nullptr, resp_bytes_of(p_), n, st_);
+    run_mux(sh_, a, h, comb_[cur].p, comb_[cur ^ 1].p, G, sel_.p, n);
+  run_modswitch(comb_[cur].p, G, d_responses, n);
 }
 
 void Server::combine_host(uint32_t n, const uint64_t *partials, uint64_t *responses) {
   const size_t cts = static_cast<size_t>(num_shards_) * n;
   check_ct_values(partials, cts);
   opir::DevBuf<uint64_t> d_in, d_out;
-  d_in.alloc(cts * kCt);
+  d_in.alloc(cts * ct_);
   d_out.alloc(static_cast<size_t>(n) * 2 * kN);
-  ck(cudaMemcpyAsync(d_in.p, partials, cts * kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  ck(cudaMemcpyAsync(d_in.p, partials, cts * ct_ * 8, cudaMemcpyHostToDevice, st_), "upload");
   combine_device(n, d_in.p, d_out.p);
   ck(cudaMemcpyAsync(responses, d_out.p, static_cast<size_t>(n) * 2 * kN * 8,
                      cudaMemcpyDeviceToHost, st_), "download");
@@ -582,9 +667,9 @@ void Server::expand_query(uint64_t id, const uint64_t *query, uint64_t *out) {
   check_ct_values(query, 1);
   ensure_capacity(1);
   upload_keyptrs(&id, 1);
-  ck(cudaMemcpyAsync(lvl_[0].p, query, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  ck(cudaMemcpyAsync(lvl_[0].p, query, ct_ * 8, cudaMemcpyHostToDevice, st_), "upload");
   const uint64_t *leaves = run_expand(1);
-  ck(cudaMemcpyAsync(out, leaves, static_cast<size_t>(sh_.useful) * kCt * 8,
+  ck(cudaMemcpyAsync(out, leaves, static_cast<size_t>(sh_.useful) * ct_ * 8,
                      cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "expand_query");
 }
@@ -598,11 +683,11 @@ void Server::complete_selectors(uint64_t id, const uint64_t *expanded, uint64_t 
     ck(cudaStreamSynchronize(st_), "complete_selectors");
     return;
   }
-  ck(cudaMemcpyAsync(lvl_[0].p, expanded, static_cast<size_t>(sh_.useful) * kCt * 8,
+  ck(cudaMemcpyAsync(lvl_[0].p, expanded, static_cast<size_t>(sh_.useful) * ct_ * 8,
                      cudaMemcpyHostToDevice, st_), "upload");
-  launch_selectors(dp_, sh_, lvl_[0].p, lvl_slots_, keyptrs_.p + 1, sel_.p, 1, st_);
+  run_selectors(lvl_[0].p, keyptrs_.p + 1, 1);
   // the rows without their Shoup companions
-  ck(cudaMemcpy2DAsync(out, kCt * 8, sel_.p, kRowWords * 8, kCt * 8,
+  ck(cudaMemcpy2DAsync(out, ct_ * 8, sel_.p, row_ * 8, ct_ * 8,
                        static_cast<size_t>(nsel) * 2 * sh_.l_ep, cudaMemcpyDeviceToHost, st_),
      "download");
   ck(cudaStreamSynchronize(st_), "complete_selectors");
@@ -612,10 +697,10 @@ void Server::evaluate_first_dim(const uint64_t *fst_query, uint64_t *out) {
   if (!db_loaded_) throw std::runtime_error("evaluate_first_dim before load_data");
   check_ct_values(fst_query, sh_.n0);
   ensure_capacity(1);
-  ck(cudaMemcpyAsync(lvl_[0].p, fst_query, static_cast<size_t>(sh_.n0) * kCt * 8,
+  ck(cudaMemcpyAsync(lvl_[0].p, fst_query, static_cast<size_t>(sh_.n0) * ct_ * 8,
                      cudaMemcpyHostToDevice, st_), "upload");
   run_first_dim(lvl_[0].p, 1, nullptr);
-  ck(cudaMemcpyAsync(out, mid_[0].p, static_cast<size_t>(sh_.other) * kCt * 8,
+  ck(cudaMemcpyAsync(out, mid_[0].p, static_cast<size_t>(sh_.other) * ct_ * 8,
                      cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "evaluate_first_dim");
   check_device_error();
@@ -628,18 +713,18 @@ void Server::evaluate_other_dim(const uint64_t *mid, const uint64_t *selectors, 
   check_ct_values(mid, sh_.other);
   if (nsel) check_ct_values(selectors, static_cast<size_t>(nsel) * 2 * sh_.l_ep);
   ensure_capacity(1);
-  ck(cudaMemcpyAsync(mid_[0].p, mid, static_cast<size_t>(sh_.other) * kCt * 8,
+  ck(cudaMemcpyAsync(mid_[0].p, mid, static_cast<size_t>(sh_.other) * ct_ * 8,
                      cudaMemcpyHostToDevice, st_), "upload");
   std::vector<uint64_t> rows;
   if (nsel) {
     const size_t n_rows = static_cast<size_t>(nsel) * 2 * sh_.l_ep;
-    rows.reserve(n_rows * kRowWords);
-    for (size_t r = 0; r < n_rows; ++r) append_row(rows, selectors + r * kCt);
+    rows.reserve(n_rows * row_);
+    for (size_t r = 0; r < n_rows; ++r) append_row(rows, selectors + r * ct_, n_, limbs_);
     ck(cudaMemcpyAsync(sel_.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st_),
        "upload");
   }
   const uint64_t *r = run_other_dims(1);
-  ck(cudaMemcpyAsync(out, r, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaMemcpyAsync(out, r, ct_ * 8, cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "evaluate_other_dim");
 }
 
@@ -653,46 +738,45 @@ void Server::ext_prod_mux(const uint64_t *x, const uint64_t *y, const uint64_t *
   sh.other = 2;
   sh.num_dims = 2;
   std::vector<uint64_t> rows;
-  rows.reserve(n_rows * kRowWords);
-  for (size_t r = 0; r < n_rows; ++r) append_row(rows, sel + r * kCt);
+  rows.reserve(n_rows * row_);
+  for (size_t r = 0; r < n_rows; ++r) append_row(rows, sel + r * ct_, n_, limbs_);
   opir::DevBuf<uint64_t> xy, res, srows;
-  xy.alloc(2 * kCt);
-  res.alloc(2 * kCt);
+  xy.alloc(2 * ct_);
+  res.alloc(2 * ct_);
   srows.alloc(rows.size());
-  ck(cudaMemcpyAsync(xy.p, x, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
-  ck(cudaMemcpyAsync(xy.p + kCt, y, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  ck(cudaMemcpyAsync(xy.p, x, ct_ * 8, cudaMemcpyHostToDevice, st_), "upload");
+  ck(cudaMemcpyAsync(xy.p + ct_, y, ct_ * 8, cudaMemcpyHostToDevice, st_), "upload");
   ck(cudaMemcpyAsync(srows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st_), "upload");
-  launch_mux_level(dp_, sh, 0, 1, xy.p, res.p, 2, srows.p, 1, st_);
-  ck(cudaMemcpyAsync(out, res.p, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");
+  run_mux(sh, 0, 1, xy.p, res.p, 2, srows.p, 1);
+  ck(cudaMemcpyAsync(out, res.p, ct_ * 8, cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "ext_prod_mux");
 }
 
 void Server::tree_unpack(uint64_t id, const uint64_t *query) {
   check_ct_values(query, 1);
   upload_keyptrs(&id, 1);
-  ck(cudaMemcpyAsync(lvl_[0].p, query, kCt * 8, cudaMemcpyHostToDevice, st_), "upload");
+  ck(cudaMemcpyAsync(lvl_[0].p, query, ct_ * 8, cudaMemcpyHostToDevice, st_), "upload");
   const uint64_t *leaves = run_expand(1);
   if (sh_.num_dims > 1)
-    launch_selectors(dp_, sh_, leaves, lvl_slots_, keyptrs_.p + 1, sel_.p, 1, st_);
+    run_selectors(leaves, keyptrs_.p + 1, 1);
 }
 
 void Server::tree_select_device(const uint64_t *d_leaves, const uint64_t *d_selectors,
                                 uint64_t fold_begin, uint64_t fold_count, uint64_t *d_out) {
   if (!db_loaded_) throw std::runtime_error("select_level before load_data");
-  ck(cudaMemcpyAsync(lvl_[0].p, d_leaves, static_cast<size_t>(sh_.n0) * kCt * 8,
+  ck(cudaMemcpyAsync(lvl_[0].p, d_leaves, static_cast<size_t>(sh_.n0) * ct_ * 8,
                      cudaMemcpyDeviceToDevice, st_), "alpha copy");
   run_first_dim(lvl_[0].p, 1, nullptr);
   const uint32_t fold = static_cast<uint32_t>(fold_count);
-  const size_t sel_words = 2ull * sh_.l_ep * kRowWords;  // one selector with companions
+  const size_t sel_words = 2ull * sh_.l_ep * row_;  // one selector with companions
   for (uint32_t a = 1; a <= fold; ++a) {  // MSB-first: step a takes selector begin+count-a
     const uint64_t u = fold_begin + fold_count - a;
     ck(cudaMemcpyAsync(sel_.p + a * sel_words, d_selectors + u * sel_words, sel_words * 8,
                        cudaMemcpyDeviceToDevice, st_), "selector copy");
   }
   for (uint32_t a = 1; a <= fold; ++a)
-    launch_mux_level(dp_, sh_, a, sh_.num_dims - 1, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other,
-                     sel_.p, 1, st_);
-  ck(cudaMemcpyAsync(d_out, mid_[fold & 1].p, kCt * 8, cudaMemcpyDeviceToDevice, st_), "result");
+    run_mux(sh_, a, sh_.num_dims - 1, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other, sel_.p, 1);
+  ck(cudaMemcpyAsync(d_out, mid_[fold & 1].p, ct_ * 8, cudaMemcpyDeviceToDevice, st_), "result");
 }
 
 void Server::select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32_t fold,
@@ -701,24 +785,23 @@ void Server::select_fold(const uint64_t *alpha, const uint64_t *fold_sel, uint32
   check_ct_values(alpha, sh_.n0);
   if (fold) check_ct_values(fold_sel, static_cast<size_t>(fold) * 2 * sh_.l_ep);
   ensure_capacity(1);
-  ck(cudaMemcpyAsync(lvl_[0].p, alpha, static_cast<size_t>(sh_.n0) * kCt * 8,
+  ck(cudaMemcpyAsync(lvl_[0].p, alpha, static_cast<size_t>(sh_.n0) * ct_ * 8,
                      cudaMemcpyHostToDevice, st_), "upload");
   run_first_dim(lvl_[0].p, 1, nullptr);
   const uint64_t *res = mid_[0].p;
   std::vector<uint64_t> rows;
   if (fold) {
     const size_t n_rows = static_cast<size_t>(fold) * 2 * sh_.l_ep;
-    rows.reserve(n_rows * kRowWords);
-    for (size_t r = 0; r < n_rows; ++r) append_row(rows, fold_sel + r * kCt);
+    rows.reserve(n_rows * row_);
+    for (size_t r = 0; r < n_rows; ++r) append_row(rows, fold_sel + r * ct_, n_, limbs_);
     // slot 0 of the selector set is unused: step a takes slot a
-    ck(cudaMemcpyAsync(sel_.p + 2ull * sh_.l_ep * kRowWords, rows.data(), rows.size() * 8,
+    ck(cudaMemcpyAsync(sel_.p + 2ull * sh_.l_ep * row_, rows.data(), rows.size() * 8,
                        cudaMemcpyHostToDevice, st_), "upload");
     for (uint32_t a = 1; a <= fold; ++a)
-      launch_mux_level(dp_, sh_, a, sh_.num_dims - 1, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other,
-                       sel_.p, 1, st_);
+      run_mux(sh_, a, sh_.num_dims - 1, mid_[(a - 1) & 1].p, mid_[a & 1].p, sh_.other, sel_.p, 1);
     res = mid_[fold & 1].p;
   }
-  ck(cudaMemcpyAsync(out, res, kCt * 8, cudaMemcpyDeviceToHost, st_), "download");
+  ck(cudaMemcpyAsync(out, res, ct_ * 8, cudaMemcpyDeviceToHost, st_), "download");
   ck(cudaStreamSynchronize(st_), "select_level");
   check_device_error();
 }

@@ -1,7 +1,11 @@
-// Server state and query pipeline for CONFIG_N4096_K2_MP
-// (includes/database_constants.h:111-125). The C-ABI handle forwards to this
-// class when it was created with two-limb parameters; argument checking that
-// does not depend on the parameter set stays in the C-ABI layer.
+// Server state and query pipeline for the parameter sets whose limbs are
+// 64-bit words: CONFIG_N4096_K2_MP (includes/database_constants.h:111-125,
+// two 60-bit limbs at N = 4096) and CONFIG_N2048_K1 (:61-76, one 60-bit
+// prime at N = 2048; no row shards or tree levels). The C-ABI handle
+// forwards to this class when it was created with either set; argument
+// checking that does not depend on the parameter set stays in the C-ABI
+// layer. Ciphertexts are [c0][c1] with each polynomial limb-major (2 N K
+// u64).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,6 +20,7 @@
 #include "../../include/onionpir_b200.h"
 #include "opir_c4_kernels.h"
 #include "opir_host.h"
+#include "opir_k1p_kernels.h"
 #include "opir_shard.h"
 
 namespace opir4 {
@@ -126,10 +131,24 @@ class Server {
   void clear_graphs();
   void mark(Events ev, int i);
   void launch_scan(const uint8_t *qb, uint64_t *cmat, uint32_t n);
+  void setup_k1_tables();
+  void setup_c4_tables();
+  opir1::Dev1 d1() const;
+  void run_db_preprocess(const uint64_t *coeffs, uint64_t coeff_pt_begin, uint64_t seed,
+                         uint64_t logical, uint64_t pb, uint64_t pe);
+  void run_selectors(const uint64_t *leaves, const uint64_t *const *gsw, uint32_t n);
+  void run_mux(const Shape4 &sh, uint32_t level, uint32_t tree_h, const uint64_t *in, uint64_t *out,
+               uint64_t mid_stride, const uint64_t *sel, uint32_t n);
+  void run_modswitch(const uint64_t *ct, uint64_t ct_stride, uint64_t *resp, uint32_t n);
   template <typename Fill>
   void load_tiles(uint64_t logical, Fill &&fill);
 
   opir_params p_{};
+  bool k1_ = false;          // CONFIG_N2048_K1 (opir_k1p_kernels.h) instead of CONFIG_N4096_K2_MP
+  uint32_t n_ = kN;          // ring degree N
+  uint32_t limbs_ = 2;       // RNS limbs K
+  uint64_t ct_ = kCtWords;   // u64 words per ciphertext: 2 N K
+  uint64_t row_ = kRowWords; // u64 words per key / selector row: ciphertext + companions
   Shape4 sh_{};
   Dev4 dp_{};
   cudaStream_t st_ = nullptr;

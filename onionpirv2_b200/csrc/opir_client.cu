@@ -865,7 +865,7 @@ opir_status client_guarded(opir_client *c, F &&f) {
 // The layout must be one opir_params_init[_config] produces.
 opir_params checked_layout(const opir_params &p) {
   const bool c4 = p.num_limbs == 2 && p.poly_degree == 4096;
-  if (!c4 && !(p.num_limbs == 1 && p.poly_degree == 2048))
+  if (!c4 && !(p.num_limbs == 1 && p.poly_degree == 2048 && p.q1 != 0))
     throw std::invalid_argument("unsupported parameter set (CONFIG_N2048_K1_COMP or CONFIG_N4096_K2_MP)");
   if (p.view != OPIR_VIEW_LAYOUT)
     throw std::invalid_argument("a client needs a database layout (opir_params_init[_config])");

@@ -216,6 +216,49 @@ opir_params derive_params_k2mp(const opir_layout &layout) {
   return p;
 }
 
+opir_params derive_params_k1p(const opir_layout &layout) {
+  // pir.cpp:49-134 with CONFIG_N2048_K1 (database_constants.h:61-76), the
+  // reference's default ACTIVE_CONFIG: RnsMods {60} (one real NTT prime, no
+  // composite split), PlainMod 14, SmallQWidth 22, L_EP 5, L_KEY 8, L_KS 8.
+  constexpr uint32_t N = 2048;
+  opir_params p{};
+  p.poly_degree = N;
+  p.num_limbs = 1;
+  p.q = ntt_friendly_primes({60}, N)[0];
+  p.q1 = p.q2 = 0;  // no composite first-dimension split
+  p.w1 = min_primitive_root(2ull * N, p.q);
+  p.w2 = 0;
+  p.w_crt = p.w1;
+  p.q1_inv_mod_q2 = 0;
+  p.plain_mod = generate_prime(14);
+  p.small_q = ntt_friendly_primes({22}, N)[0];
+  p.small_q_width = static_cast<uint32_t>(std::ceil(std::log2(static_cast<double>(p.small_q))));
+  p.ct_mod_width = 60;
+  p.l_ep = 5;
+  p.l_key = 8;
+  p.l_ks = 8;
+  p.base_log2 = (p.ct_mod_width + p.l_ep - 1) / p.l_ep;
+  p.base_log2_key = (p.ct_mod_width + p.l_key - 1) / p.l_key;
+  p.base_log2_ks = p.ct_mod_width / p.l_ks + 1;
+  if (layout.target_num_pt == 0)
+    throw std::invalid_argument("PirParams: target_num_pt must be positive");
+  if (layout.expansion_height > 11)
+    throw std::invalid_argument("PirParams: expansion_height exceeds the ring automorphism capacity");
+  const auto shape = calc_db_shape(layout.target_num_pt, p.l_ep, layout.expansion_height,
+                                   layout.fst_dim_pow2 != 0);
+  const uint64_t other = (layout.target_num_pt + shape.first - 1) / shape.first;
+  if (other > std::numeric_limits<uint64_t>::max() / shape.first)
+    throw std::overflow_error("PirParams: rounded database shape overflows");
+  p.target_num_pt = layout.target_num_pt;
+  p.expansion_height = layout.expansion_height;
+  p.fst_dim_pow2 = layout.fst_dim_pow2 ? 1 : 0;
+  p.fst_dim_sz = shape.first;
+  p.num_dims = static_cast<uint32_t>(shape.second);
+  p.other_dim_sz = other;
+  p.num_pt = shape.first * other;
+  return p;
+}
+
 static uint32_t bitrev(uint32_t x, uint32_t bits) {
   uint32_t y = 0;
   for (uint32_t i = 0; i < bits; ++i) { y = (y << 1) | (x & 1); x >>= 1; }

@@ -35,6 +35,8 @@ LimbTables make_limb_tables(uint32_t n, uint32_t q, uint32_t root);
 opir_params derive_params_c4(const opir_layout &layout);
 // PirParams under CONFIG_N2048_K2_MP (two 29-bit RNS limbs at N = 2048).
 opir_params derive_params_k2mp(const opir_layout &layout);
+// PirParams under CONFIG_N2048_K1 (one 60-bit prime at N = 2048; q1 = q2 = 0).
+opir_params derive_params_k1p(const opir_layout &layout);
 
 // 64-bit limb tables: bit-reversed powers with Shoup companions
 // floor(w 2^64 / q), N^-1 and iw[1] N^-1 with theirs.

@@ -417,7 +417,15 @@ cudaEvent_t *c4_events(opir_server *s) {
   return ev;
 }
 
-bool is_c4(const opir_params &p) { return p.num_limbs == 2 && p.poly_degree == 4096; }
+// CONFIG_N2048_K1: one 60-bit prime at N = 2048 (no composite split).
+bool is_k1p(const opir_params &p) {
+  return p.num_limbs == 1 && p.poly_degree == 2048 && p.q1 == 0;
+}
+// Handles whose limbs are 64-bit words forward to opir4::Server:
+// CONFIG_N4096_K2_MP and CONFIG_N2048_K1.
+bool is_c4(const opir_params &p) {
+  return (p.num_limbs == 2 && p.poly_degree == 4096) || is_k1p(p);
+}
 
 // Expansion (Algorithm 2) over n queries whose residue pairs sit in slot 0 of
 // lvl[0]; returns the buffer holding the leaves.
@@ -692,7 +700,10 @@ opir_params checked_params(const opir_params &p) {
     throw std::invalid_argument(
         "unsupported parameter set (CONFIG_N2048_K1_COMP, CONFIG_N2048_K2_MP or CONFIG_N4096_K2_MP)");
   auto derive = [&](const opir_layout &lay) {
-    return c4 ? opir4::derive(lay) : k2 ? opir::derive_params_k2mp(lay) : opir::derive_params(lay);
+    return is_k1p(p) ? opir::derive_params_k1p(lay)
+           : c4     ? opir4::derive(lay)
+           : k2     ? opir::derive_params_k2mp(lay)
+                    : opir::derive_params(lay);
   };
   if (p.view == OPIR_VIEW_LAYOUT) {
     const opir_params check = derive(opir_layout{p.target_num_pt, p.expansion_height, p.fst_dim_pow2});
@@ -878,6 +889,8 @@ opir_status opir_params_init_config(opir_config config, const opir_layout *layou
   if (config == OPIR_CONFIG_N2048_K1_COMP) return opir_params_init(layout, out);
   if (config == OPIR_CONFIG_N2048_K2_MP)
     return guarded(nullptr, [&] { *out = opir::derive_params_k2mp(*layout); });
+  if (config == OPIR_CONFIG_N2048_K1)
+    return guarded(nullptr, [&] { *out = opir::derive_params_k1p(*layout); });
   if (config != OPIR_CONFIG_N4096_K2_MP) return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] { *out = opir4::derive(*layout); });
 }
@@ -1207,7 +1220,7 @@ opir_status opir_server_create_row_shard(const opir_params *params, uint32_t sha
     checked = checked_params(*params);
     if (checked.view != OPIR_VIEW_LAYOUT)
       throw std::invalid_argument("row shards split a database layout");
-    if (is_k2mp(checked))
+    if (is_k2mp(checked) || is_k1p(checked))
       throw std::invalid_argument(
           "row shards are built for CONFIG_N2048_K1_COMP and CONFIG_N4096_K2_MP");
     rs = opir::row_shard(checked.other_dim_sz, checked.num_dims, shard, num_shards);
@@ -1675,7 +1688,7 @@ opir_status opir_tree_level_create(const opir_params *scheme, const opir_tree_pa
   opir_tree_level_plan plan{};
   const opir_status vs = guarded(nullptr, [&] {
     const opir_params sch = checked_params(*scheme);
-    if (is_k2mp(sch))
+    if (is_k2mp(sch) || is_k1p(sch))
       throw std::invalid_argument("tree PIR is built for CONFIG_N2048_K1_COMP and CONFIG_N4096_K2_MP");
     const auto mods = opir::scheme_moduli(sch);
     opir::validate_tree_params(*tree, mods);
@@ -1900,15 +1913,16 @@ opir_status opir_tree_query(opir_tree *t, uint64_t client_id, const uint64_t *qu
 }
 
 opir_status opir_measure_butterfly_rate(opir_config config, int device, double *per_s) {
-  // CONFIG_N2048_K2_MP runs on the residue-pair NTT of CONFIG_N2048_K1_COMP
+  // CONFIG_N2048_K2_MP runs on the residue-pair NTT of CONFIG_N2048_K1_COMP;
+  // CONFIG_N2048_K1 on 64-bit Shoup butterflies like CONFIG_N4096_K2_MP
   if (!per_s || (config != OPIR_CONFIG_N2048_K1_COMP && config != OPIR_CONFIG_N4096_K2_MP &&
-                 config != OPIR_CONFIG_N2048_K2_MP))
+                 config != OPIR_CONFIG_N2048_K2_MP && config != OPIR_CONFIG_N2048_K1))
     return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] {
     DeviceGuard g(device);
     int sms = 0;
     ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
-    const bool c4 = config == OPIR_CONFIG_N4096_K2_MP;
+    const bool c4 = config == OPIR_CONFIG_N4096_K2_MP || config == OPIR_CONFIG_N2048_K1;
     const uint32_t blocks = c4 ? opir4::bfly_rate_blocks(sms) : opir::bfly_rate_blocks(sms);
     const uint32_t iters = c4 ? 256 : 1024;
     DevBuf<uint64_t> sink;

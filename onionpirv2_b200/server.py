@@ -6,9 +6,9 @@ Names, argument meaning and error behaviour follow the reference
 ValueError (std::invalid_argument), unknown clients raise KeyError-compatible
 IndexError subclass OutOfRange (std::out_of_range), device failures raise
 RuntimeError. Ciphertexts are numpy uint64 arrays shaped (2, N) = (c0, c1)
-under CONFIG_N2048_K1_COMP and (2, 2, N) = (poly, RNS limb, coefficient)
-under CONFIG_N2048_K2_MP and CONFIG_N4096_K2_MP; responses are (2, N) mod
-small_q under all three.
+under CONFIG_N2048_K1_COMP and CONFIG_N2048_K1 and (2, 2, N) = (poly, RNS
+limb, coefficient) under CONFIG_N2048_K2_MP and CONFIG_N4096_K2_MP; responses
+are (2, N) mod small_q under all four.
 """
 from __future__ import annotations
 
@@ -54,14 +54,15 @@ def _ptr(a: np.ndarray, t=C.c_uint64):
     return a.ctypes.data_as(C.POINTER(t))
 
 
-CONFIGS = {"CONFIG_N2048_K1_COMP": 0, "CONFIG_N4096_K2_MP": 1, "CONFIG_N2048_K2_MP": 2}
+CONFIGS = {"CONFIG_N2048_K1_COMP": 0, "CONFIG_N4096_K2_MP": 1, "CONFIG_N2048_K2_MP": 2,
+           "CONFIG_N2048_K1": 3}
 
 
 class PirParams:
     """PirParams().with_layout({target_num_pt, expansion_height, fst_dim_pow2})
     under one ACTIVE_CONFIG (includes/database_constants.h:31-40):
-    "CONFIG_N2048_K1_COMP" (default), "CONFIG_N2048_K2_MP" or
-    "CONFIG_N4096_K2_MP"."""
+    "CONFIG_N2048_K1_COMP" (default), "CONFIG_N2048_K1" (the reference's own
+    default: one 60-bit prime), "CONFIG_N2048_K2_MP" or "CONFIG_N4096_K2_MP"."""
 
     def __init__(self, target_num_pt: int = 43690, expansion_height: int = 10,
                  fst_dim_pow2: bool = True, config: str = "CONFIG_N2048_K1_COMP"):

@@ -84,17 +84,21 @@ GSWCt gsw_of(const std::vector<uint64_t> &g, size_t rows, size_t kn) {
   return out;
 }
 
-// ---------------------------------------------------------- CONFIG_N2048_K1_COMP
-void test_pir_k1() {
+// ------------------------------------- CONFIG_N2048_K1_COMP and CONFIG_N2048_K1
+// The one-limb sets: the oracle's routines take either set's parameters
+// (init picks the set; CONFIG_N2048_K1 has one 60-bit prime).
+void test_pir_one_limb(opir_config config,
+                       int (*init)(uint64_t, uint32_t, int, opir_oracle_params *),
+                       const std::string &label) {
   const uint64_t seed_db = 11;
   const size_t target = 16384, height = 9;
-  PirParams pir_params = PirParams().with_layout({target, height, true});
+  PirParams pir_params = PirParams(config).with_layout({target, height, true});
   opir_oracle_params op;
-  oracle_params_init(target, height, 1, &op);
+  init(target, height, 1, &op);
   const size_t N = pir_params.get_poly_degree(), kn = pir_params.get_coeff_val_cnt();
   const size_t h = pir_params.get_expan_height(), l_ks = op.l_ks;
   require_test(pir_params.get_num_pt() == op.num_pt && pir_params.get_fst_dim_sz() == op.fst_dim_sz,
-               "k1 layout");
+               label + " layout");
 
   PirServer server(pir_params);
   std::vector<size_t> query_indices = {0, 12345, target - 1};
@@ -133,7 +137,7 @@ void test_pir_k1() {
 
     std::vector<uint64_t> want(2 * N);
     oracle_server_make_query(ref, q.data(), want.data());
-    require_test(flat(response) == want, "k1 response bit-exact, index " + std::to_string(query_pt_idx));
+    require_test(flat(response) == want, label + " response bit-exact, index " + std::to_string(query_pt_idx));
 
     std::stringstream resp_stream;
     const size_t resp_size = server.save_resp_to_stream(response, resp_stream);
@@ -143,13 +147,13 @@ void test_pir_k1() {
     const std::vector<uint8_t> got_bytes(s.begin(), s.end());
     want_bytes.resize(want_size);
     require_test(resp_size == 11264 && resp_size == want_size && got_bytes == want_bytes,
-                 "k1 serialized response");
+                 label + " serialized response");
 
     std::vector<uint64_t> decrypted(N);
     std::vector<uint64_t> r = flat(response);
     oracle_client_decrypt(client, r.data(), decrypted.data());
     RlwePt actual_plaintext = server.direct_get_original_plaintext(query_pt_idx);
-    require_test(decrypted == actual_plaintext.data, "k1 decrypts to the recorded plaintext");
+    require_test(decrypted == actual_plaintext.data, label + " decrypts to the recorded plaintext");
     if (last) oracle_client_free(last);
     last = client;
     last_query = q;
@@ -167,7 +171,7 @@ void test_pir_k1() {
     const auto f = flat(ct);
     e_got.insert(e_got.end(), f.begin(), f.end());
   }
-  require_test(expanded.size() == useful && e_got == e_want, "expand_query");
+  require_test(expanded.size() == useful && e_got == e_want, label + " expand_query");
 
   std::vector<GSWCt> selectors = server.complete_selectors(client_id, expanded);
   std::vector<uint64_t> s_want((op.num_dims - 1) * 2 * op.l_ep * 2 * kn);
@@ -175,7 +179,7 @@ void test_pir_k1() {
   std::vector<uint64_t> s_got;
   for (const auto &gct : selectors)
     for (const auto &row : gct) s_got.insert(s_got.end(), row.begin(), row.end());
-  require_test(s_got == s_want, "complete_selectors");
+  require_test(s_got == s_want, label + " complete_selectors");
 
   std::vector<RlweCt> mid = server.evaluate_first_dim(expanded);
   std::vector<uint64_t> m_want(op.other_dim_sz * 2 * kn);
@@ -185,19 +189,19 @@ void test_pir_k1() {
     const auto f = flat(ct);
     m_got.insert(m_got.end(), f.begin(), f.end());
   }
-  require_test(m_got == m_want, "evaluate_first_dim");
+  require_test(m_got == m_want, label + " evaluate_first_dim");
 
   RlweCt mux;
   server.ext_prod_mux(mid[0], mid[1], selectors[0], mux);
   std::vector<uint64_t> x(m_want.begin(), m_want.begin() + 2 * kn),
       y(m_want.begin() + 2 * kn, m_want.begin() + 4 * kn), mux_want(2 * kn);
   oracle_ext_prod_mux(&op, x.data(), y.data(), s_want.data(), mux_want.data());
-  require_test(flat(mux) == mux_want, "ext_prod_mux");
+  require_test(flat(mux) == mux_want, label + " ext_prod_mux");
 
   RlweCt fin = server.evaluate_other_dim(mid, selectors);
   std::vector<uint64_t> f_want(2 * kn);
   oracle_server_other_dim(ref, m_want.data(), s_want.data(), f_want.data());
-  require_test(flat(fin) == f_want, "evaluate_other_dim");
+  require_test(flat(fin) == f_want, label + " evaluate_other_dim");
 
   // error behaviour of the reference
   require_throws<std::out_of_range>([&] { server.make_query(999, query); }, "unknown client");
@@ -295,7 +299,8 @@ void test_pir_two_limb(opir_config config,
 }  // namespace
 
 int main() {
-  test_pir_k1();
+  test_pir_one_limb(OPIR_CONFIG_N2048_K1_COMP, oracle_params_init, "CONFIG_N2048_K1_COMP");
+  test_pir_one_limb(OPIR_CONFIG_N2048_K1, oracle_k1p_params_init, "CONFIG_N2048_K1");
   test_pir_two_limb(OPIR_CONFIG_N4096_K2_MP, oracle_c4_params_init, 2048, 7, 777, 51200,
                     "CONFIG_N4096_K2_MP");
   test_pir_two_limb(OPIR_CONFIG_N2048_K2_MP, oracle_k2mp_params_init, 1000, 7, 777, 11264,
