@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--sweep", default=None,
                     help="batch sizes timed after the headline (default 1,8,32,128 for k1, "
                          "1,8,32,64 for c4; 'none' to skip)")
+    ap.add_argument("--concurrent", action="store_true",
+                    help="also time two batches in flight at once (two handles on the same "
+                         "database layout, two streams): the served form's overlap")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default scan tiling (or OPIR_SCAN_TILE)")
     ap.add_argument("--tree-config", choices=["k1", "c4"], default="k1",
@@ -515,6 +518,42 @@ def bench_ours(args, world, rank, local):
                       "p50_ms": float(np.percentile(s_per, 50)),
                       "scan_ms": round(s_stages["Core"], 4)})
 
+    # two batches in flight: a second handle on its own stream (the serving
+    # loop's overlap of batches), device-timed around both streams
+    conc = None
+    if args.concurrent and world == 1:
+        srv2 = PirServer(params, device=local)
+        srv2.load_data_seeded(args.target, DB_SEED)
+        for b, (bv, gsw) in enumerate(keys):
+            srv2.set_client_keys(b, bv, gsw)
+        if not args.no_autotune:
+            srv2.autotune(nq)
+        s2 = torch.cuda.Stream(device)
+        qb, rb = d_q[:B].contiguous(), d_r[:B].contiguous()
+        rb2 = torch.empty_like(rb)
+
+        def both():
+            srv.make_query_batch_device(ids[:B], qb.data_ptr(), rb.data_ptr(), stream.cuda_stream)
+            srv2.make_query_batch_device(ids[:B], qb.data_ptr(), rb2.data_ptr(), s2.cuda_stream)
+        for _ in range(args.warmup):
+            both()
+        torch.cuda.synchronize(device)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        s2.wait_event(e0)
+        for _ in range(args.steps):
+            both()
+        e2.record(s2)
+        stream.wait_event(e2)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1)
+        conc = {"batches_in_flight": 2, "batch": B, "steps": args.steps,
+                "queries_per_s": 2 * B * args.steps / (ms / 1e3),
+                "ms_per_pair": ms / args.steps,
+                "same_responses": bool(torch.equal(rb, rb2))}
+        srv2.close()
+
     if rank != 0:
         srv.close()
         if world > 1:
@@ -579,6 +618,7 @@ def bench_ours(args, world, rank, local):
         "int_pipe": int_pipe_roofline(params, config, stages, B, local),
         "batch_sweep": sweep,
         "clocks": clk.summary(),
+        **({"concurrent": conc} if conc else {}),
         "gpu_launches": launches,
         "setup": {"db_load_s": round(load_s, 3), "autotune_s": round(tune_s, 3),
                   "scan_tile": srv.scan_tile(B), "scan_tile_plain": srv.scan_tile(1),

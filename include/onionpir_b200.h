@@ -343,15 +343,25 @@ opir_status opir_server_reserve(opir_server *server, uint32_t max_batch);
  * blocking). Times the tilings of the tensor-core first-dimension scan --
  * query columns per tile (16, 32, 64), K bytes per pipeline stage (128 with
  * 128-byte swizzle, 64 with 64-byte swizzle) and pipeline depth -- on this
- * handle's database for batches of 1, 2, 4, ... up to max_batch queries, and
- * keeps the fastest per batch-size bucket. Every tiling computes the same
- * result; only the speed differs. Synchronises the handle's stream and
- * overwrites its scratch arena: no query may be in flight on the handle. */
+ * handle's database, and the cluster width of every expansion level (1, 2, 4
+ * or 8 CTAs per key switch) and MUX level (1, 2 or, with an even digit
+ * count, 4 CTAs per MUX), for batches of 1, 2, 4, ... up to max_batch
+ * queries, and keeps the fastest per batch-size bucket. Every tiling and
+ * width computes the same result; only the speed differs. Synchronises the
+ * handle's stream and overwrites its scratch arena: no query may be in
+ * flight on the handle. The residue-pair sets only (CONFIG_N2048_K1_COMP,
+ * CONFIG_N2048_K2_MP); a no-op on the 64-bit-limb sets. */
 opir_status opir_server_autotune(opir_server *server, uint32_t max_batch);
 /* The scan tiling a batch of n queries uses (autotuned, else the default). */
 opir_status opir_server_scan_tile(const opir_server *server, uint32_t n,
                                   uint32_t *ntile, uint32_t *kt,
                                   uint32_t *stages);
+/* No counterpart in the reference. The cluster widths a batch of n queries
+ * uses: expand[d] for expansion level d (16 entries), mux[a] for MUX level a
+ * (32 entries); 0 means the default rule (split while a level has fewer CTAs
+ * than the GPU has slots), else the autotuned width. */
+opir_status opir_server_level_splits(const opir_server *server, uint32_t n, uint8_t *expand,
+                                     uint8_t *mux);
 
 /* No counterpart in the reference. Moves the handle's work to a new CUDA
  * stream of the given priority (cudaStreamCreateWithPriority: lower numbers

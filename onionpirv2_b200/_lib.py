@@ -125,6 +125,8 @@ _SIGS = {
     "opir_server_reserve": ([C.c_void_p, C.c_uint32], C.c_int),
     "opir_server_set_priority": ([C.c_void_p, C.c_int], C.c_int),
     "opir_server_set_scan_wait_limit": ([C.c_void_p, C.c_uint64], C.c_int),
+    "opir_server_level_splits": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint8),
+                                  C.POINTER(C.c_uint8)], C.c_int),
     "opir_server_autotune": ([C.c_void_p, C.c_uint32], C.c_int),
     "opir_server_scan_tile": ([C.c_void_p, C.c_uint32, u32p, u32p, u32p], C.c_int),
     "opir_server_set_stage_timing": ([C.c_void_p, C.c_int], C.c_int),

@@ -1337,8 +1337,13 @@ static void expand_level_impl(const DevParams &P, const Shape &s, uint32_t d, co
   // levels with fewer nodes than CTA slots (2 per SM) split each key switch
   // over a cluster of 2, 4 or 8 CTAs (k_expand_level_split)
   const uint64_t ctas = 2ull * nodes * batch, slots = 2ull * sm_count();
-  const int split = !split_enabled() ? 1
-                    : 8 * ctas <= slots ? 8 : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
+  int split = !split_enabled() ? 1
+              : 8 * ctas <= slots ? 8 : 4 * ctas <= slots ? 4 : 2 * ctas <= slots ? 2 : 1;
+  if (d < 16 && s.split_exp[d]) {  // autotuned width
+    split = s.split_exp[d];
+    if (split != 1 && split != 2 && split != 4 && split != 8)
+      throw std::invalid_argument("expansion cluster width must be 1, 2, 4 or 8");
+  }
   if (split == 1) {
     dim3 grid(nodes, 2, batch);
     k_expand_level<G><<<grid, kThreads, smem, st>>>(P, galois_inv, k, s.base_ks, s.l_ks, in,
@@ -1518,8 +1523,13 @@ static void mux_level_impl(const DevParams &P, const Shape &s, uint32_t level, u
   // polynomial's digits halve evenly
   constexpr bool four = G::lep % 2 == 0;
   const uint64_t ctas = 2ull * n_pairs * batch, slots = 2ull * sm_count();
-  const int split = (copies != 0 || !split_enabled()) ? 1
-                    : (four && 4 * ctas <= slots) ? 4 : 2 * ctas <= slots ? 2 : 1;
+  int split = (copies != 0 || !split_enabled()) ? 1
+              : (four && 4 * ctas <= slots) ? 4 : 2 * ctas <= slots ? 2 : 1;
+  if (level < 32 && s.split_mux[level] && copies == 0) {  // autotuned width
+    split = s.split_mux[level];
+    if (split != 1 && split != 2 && (split != 4 || !four))
+      throw std::invalid_argument("MUX cluster width must be 1, 2 or (even digit counts) 4");
+  }
   if (split == 1) {
     set_smem(k_mux_level<G>, smem);
     dim3 grid(n_pairs + copies, 2, batch);

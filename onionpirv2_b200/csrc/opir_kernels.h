@@ -21,6 +21,11 @@ struct Shape {
   uint32_t n0p;         // n0 rounded up to 16 (byte-plane row length)
   uint32_t gadget;      // 0: CONFIG_N2048_K1_COMP gadgets, 1: CONFIG_N2048_K2_MP gadgets
   uint64_t num_pt;
+  // cluster width per expansion level d / MUX level a (1, 2, 4 or 8 CTAs
+  // per key switch or MUX); 0 = the default rule (split while the level has
+  // fewer CTAs than the GPU has slots). Set by the handle's autotuner.
+  uint8_t split_exp[16];
+  uint8_t split_mux[32];
 };
 
 // Number of heap nodes processed at expansion level d (nodes whose leftmost

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <iterator>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -76,6 +77,19 @@ int tile_bucket(uint32_t n) {
   return b;
 }
 
+// Cluster widths of the expansion and MUX levels for one batch bucket
+// (opir_server_autotune); 0 = the launchers' default rule.
+struct LevelSplits {
+  uint8_t exp[16] = {};
+  uint8_t mux[32] = {};
+};
+
+// OPIR_SPLIT=0 turns every cluster split off (tuned widths included).
+bool splits_allowed() {
+  const char *e = std::getenv("OPIR_SPLIT");
+  return !(e && std::strcmp(e, "0") == 0);
+}
+
 }  // namespace
 
 struct opir_server {
@@ -89,6 +103,7 @@ struct opir_server {
   bool db_loaded = false;
   CUtensorMap map_db[2]{};   // TMA views of db8 for the tensor-core scan: 128 B / 64 B swizzle
   ScanTile tile[kTileBuckets];  // tensor-core scan tiling per batch bucket (autotuned)
+  LevelSplits split[kTileBuckets];  // level cluster widths per batch bucket (autotuned)
   int sm_count = 148;
   int scan_mode = 0;         // 0 auto, 1 tensor cores, 2 CUDA cores
   DevBuf<uint32_t> err;      // device error word of the tensor-core scan
@@ -429,8 +444,19 @@ bool is_c4(const opir_params &p) {
 
 // Expansion (Algorithm 2) over n queries whose residue pairs sit in slot 0 of
 // lvl[0]; returns the buffer holding the leaves.
+// The handle's shape with the cluster widths tuned for a batch of n.
+opir::Shape level_shape(const opir_server *s, uint32_t n) {
+  opir::Shape sh = s->shape;
+  if (splits_allowed()) {
+    const LevelSplits &ls = s->split[tile_bucket(n)];
+    std::copy(std::begin(ls.exp), std::end(ls.exp), sh.split_exp);
+    std::copy(std::begin(ls.mux), std::end(ls.mux), sh.split_mux);
+  }
+  return sh;
+}
+
 uint32_t *run_expand(opir_server *s, uint32_t n) {
-  const opir::Shape &sh = s->shape;
+  const opir::Shape sh = level_shape(s, n);
   const uint64_t bv_level_stride = static_cast<uint64_t>(sh.l_ks) * 4 * kN;
   for (uint32_t d = 0; d < sh.h; ++d)
     opir::launch_expand_level(s->dp, sh, d, s->lvl[d & 1].p, s->lvl_slots, s->lvl[(d + 1) & 1].p,
@@ -518,7 +544,7 @@ void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n) {
 
 // Remaining dimensions: returns the buffer whose slot 0 holds the result.
 uint32_t *run_other_dims(opir_server *s, uint32_t n) {
-  const opir::Shape &sh = s->shape;
+  const opir::Shape sh = level_shape(s, n);
   const uint32_t levels = s->tree_h;
   for (uint32_t a = 0; a < levels; ++a)
     opir::launch_mux_level(s->dp, sh, a, levels, s->mid[a & 1].p, s->mid[(a + 1) & 1].p, sh.other,
@@ -870,6 +896,81 @@ void signal_user(opir_server *s, cudaStream_t user) {
   ck(cudaEventRecord(e, s->stream), "event record");
   ck(cudaStreamWaitEvent(user, e, 0), "wait");
   cudaEventDestroy(e);
+}
+
+}  // namespace
+
+namespace {
+
+// Times `launch` (one warm-up, then three back to back) on the handle's stream.
+template <typename F>
+float time_launches(opir_server *s, cudaEvent_t e0, cudaEvent_t e1, F &&launch) {
+  launch();
+  ck(cudaEventRecord(e0, s->stream), "event record");
+  for (int r = 0; r < 3; ++r) launch();
+  ck(cudaEventRecord(e1, s->stream), "event record");
+  ck(cudaEventSynchronize(e1), "autotune");
+  float ms = 0;
+  ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+  return ms;
+}
+
+// Cluster width of every expansion level (1, 2, 4, 8 CTAs per key switch)
+// and MUX level (1, 2, 4 CTAs per MUX) per batch bucket: each width timed on
+// the handle's scratch buffers with zero ciphertexts and zero key rows (the
+// kernels' work does not depend on the values), the fastest kept. Every
+// width computes the same result bit for bit.
+void tune_levels(opir_server *s, uint32_t max_batch, cudaEvent_t e0, cudaEvent_t e1) {
+  const opir::Shape base = s->shape;
+  const uint64_t bv_words = std::max<uint64_t>(1, static_cast<uint64_t>(base.h) * base.l_ks * 4 * kN);
+  const uint64_t gsw_words = 2ull * base.l_key * 4 * kN;
+  DevBuf<uint32_t> zkeys;
+  zkeys.alloc(bv_words + gsw_words);
+  ck(cudaMemsetAsync(zkeys.p, 0, zkeys.n * 4, s->stream), "memset");
+  for (auto *b : {&s->lvl[0], &s->lvl[1], &s->mid[0], &s->mid[1], &s->sel})
+    ck(cudaMemsetAsync(b->p, 0, b->n * 4, s->stream), "memset");
+  std::vector<const uint32_t *> ptrs(2ull * max_batch);
+  for (uint32_t i = 0; i < max_batch; ++i) {
+    ptrs[i] = zkeys.p;
+    ptrs[max_batch + i] = zkeys.p + bv_words;
+  }
+  ck(cudaMemcpyAsync(s->keyptrs.p, ptrs.data(), ptrs.size() * sizeof(void *), cudaMemcpyHostToDevice,
+                     s->stream), "key pointers");
+  const uint64_t bv_level_stride = static_cast<uint64_t>(base.l_ks) * 4 * kN;
+  for (int b = 0; b < kTileBuckets; ++b) {
+    const uint32_t n = std::min<uint32_t>(1u << b, max_batch);
+    LevelSplits ls;
+    for (uint32_t d = 0; d < base.h && d < 16; ++d) {
+      float best = 1e30f;
+      for (uint8_t c : {1, 2, 4, 8}) {
+        opir::Shape sh = base;
+        sh.split_exp[d] = c;
+        const float ms = time_launches(s, e0, e1, [&] {
+          opir::launch_expand_level(s->dp, sh, d, s->lvl[d & 1].p, s->lvl_slots,
+                                    s->lvl[(d + 1) & 1].p, s->lvl_slots, s->keyptrs.p,
+                                    bv_level_stride, n, s->stream);
+        });
+        if (ms < best) { best = ms; ls.exp[d] = c; }
+      }
+    }
+    for (uint32_t a = 0; a < s->tree_h && a < 32; ++a) {
+      float best = 1e30f;
+      for (uint8_t c : {1, 2, 4}) {
+        if (c == 4 && base.l_ep % 2 != 0) continue;  // digits do not halve
+        opir::Shape sh = base;
+        sh.split_mux[a] = c;
+        const float ms = time_launches(s, e0, e1, [&] {
+          opir::launch_mux_level(s->dp, sh, a, s->tree_h, s->mid[a & 1].p, s->mid[(a + 1) & 1].p,
+                                 base.other, s->sel.p, n, s->stream);
+        });
+        if (ms < best) { best = ms; ls.mux[a] = c; }
+      }
+    }
+    s->split[b] = ls;
+    if (n == max_batch) break;
+  }
+  ck(cudaStreamSynchronize(s->stream), "autotune");
+  clear_graphs(s);
 }
 
 }  // namespace
@@ -1389,10 +1490,25 @@ opir_status opir_server_autotune(opir_server *s, uint32_t max_batch) {
     if (!(s->c4 ? s->c4->db_loaded() : s->db_loaded))
       throw std::runtime_error("autotune before load_data");
     if (max_batch == 0) throw std::invalid_argument("max_batch must be positive");
-    if (s->c4) return;  // the two-limb scan has no tiling to tune
-    if (s->shape.n0p > 8192) return;  // the CUDA-core scan has no tiling to tune
+    if (s->c4) return;  // the 64-bit-limb scan has no tiling to tune
     DeviceGuard g(s->device);
     ensure_capacity(s, max_batch);
+    grow_keyptr_slots(s, 2ull * max_batch);
+    if (s->shape.n0p > 8192) {  // the CUDA-core scan has no tiling to tune
+      cudaEvent_t e0, e1;
+      ck(cudaEventCreate(&e0), "event");
+      ck(cudaEventCreate(&e1), "event");
+      try {
+        tune_levels(s, max_batch, e0, e1);
+      } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return;
+    }
     std::vector<ScanTile> cands;
     for (uint32_t kt : {128u, 64u})
       for (uint32_t nt : {16u, 32u, 64u}) {
@@ -1421,6 +1537,7 @@ opir_status opir_server_autotune(opir_server *s, uint32_t max_batch) {
         check_device_error(s);
         if (n == max_batch) break;
       }
+      tune_levels(s, max_batch, e0, e1);
     } catch (...) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
@@ -1429,6 +1546,20 @@ opir_status opir_server_autotune(opir_server *s, uint32_t max_batch) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   });
+}
+
+opir_status opir_server_level_splits(const opir_server *s, uint32_t n, uint8_t *expand,
+                                     uint8_t *mux) {
+  if (!s || !expand || !mux || n == 0) return OPIR_ERR_INVALID_ARGUMENT;
+  if (s->c4) {  // the 64-bit-limb levels have fixed widths
+    std::fill(expand, expand + 16, 0);
+    std::fill(mux, mux + 32, 0);
+    return OPIR_OK;
+  }
+  const LevelSplits &ls = s->split[tile_bucket(n)];
+  std::copy(std::begin(ls.exp), std::end(ls.exp), expand);
+  std::copy(std::begin(ls.mux), std::end(ls.mux), mux);
+  return OPIR_OK;
 }
 
 opir_status opir_server_scan_tile(const opir_server *s, uint32_t n, uint32_t *ntile, uint32_t *kt,

@@ -286,6 +286,14 @@ class PirServer:
         scheduled first); results are unchanged."""
         self._check(self._lib.opir_server_set_priority(self._h, int(priority)))
 
+    def level_splits(self, n: int) -> dict:
+        """Cluster widths a batch of n uses per expansion and MUX level
+        (0 = the default rule, else the autotuned width)."""
+        e = (C.c_uint8 * 16)()
+        m = (C.c_uint8 * 32)()
+        self._check(self._lib.opir_server_level_splits(self._h, int(n), e, m))
+        return {"expand": list(e), "mux": list(m)}
+
     def set_scan_wait_limit(self, cycles: int):
         """Limit (SM clock cycles) of each wait inside the tensor-core scan;
         0 restores the default of about one second. A wait that runs out

@@ -225,6 +225,9 @@ def test_autotune_keeps_results():
         for n in (1, 2, 5, 8):
             t = s2.scan_tile(n)
             assert t["ntile"] in (16, 32, 64) and t["kt"] in (64, 128) and t["stages"] >= 2
+            sp = s2.level_splits(n)
+            assert all(w in (1, 2, 4, 8) for w in sp["expand"][:gp.expansion_height])
+            assert all(w in (1, 2, 4) for w in sp["mux"][:gp.num_dims - 1])
         _check_response(c, cl, op, s2.make_query(7, q))
         out = s2.make_query_batch([7] * 5, np.stack([q] * 5))
         for i in range(5):
