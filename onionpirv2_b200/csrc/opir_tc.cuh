@@ -30,6 +30,23 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// Non-blocking test of a phase (mbarrier.test_wait returns at once, where
+// try_wait may suspend the thread for a while before it answers).
+__device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(sa(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Limits below this many cycles poll with test_wait, so that a short limit
+// is measured in cycles rather than in try_wait's own suspension time.
+constexpr long long kPollBelow = 1ll << 20;
+
 // Bounded wait, called by all 32 lanes of a warp together: false on timeout
 // (`limit` cycles) or when another role aborted. The answer is the same on
 // every lane (a lane whose phase completed still reports false when another
@@ -40,9 +57,10 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag,
                                           long long limit = kWaitCycles) {
   const long long t0 = clock64();
+  const bool poll = limit < kPollBelow;
   bool done = false;
   for (;;) {
-    done = done || mbar_try(b, parity);
+    done = done || (poll ? mbar_test(b, parity) : mbar_try(b, parity));
     const bool stop = done || *abort_flag != 0 || clock64() - t0 > limit;
     if (__all_sync(0xffffffffu, stop)) break;
   }
