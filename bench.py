@@ -47,7 +47,10 @@ C4_TARGET, C4_HEIGHT = 1 << 20, 11
 C4_CONFIG = "CONFIG_N4096_K2_MP"
 K2_CONFIG = "CONFIG_N2048_K2_MP"
 # the parameter set of each workload (tree: its own scheme)
-CONFIGS = {"k1": "CONFIG_N2048_K1_COMP", "c4": C4_CONFIG, "k2mp": K2_CONFIG}
+K1P_CONFIG = "CONFIG_N2048_K1"
+CONFIGS = {"k1": "CONFIG_N2048_K1_COMP", "c4": C4_CONFIG, "k2mp": K2_CONFIG, "k1p": K1P_CONFIG}
+# suffix of the reference binaries built with each workload's configuration
+REF_SUFFIX = {"k1": "", "k2mp": "_k2mp", "k1p": "_k1"}
 # two timed layouts of the reference under CONFIG_N4096_K2_MP with the full
 # workload's first dimension (1024) and expansion height (11): 4 and 32
 # candidate rows
@@ -64,9 +67,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-queries", type=int, default=3)
-    ap.add_argument("--workload", choices=["k1", "c4", "k2mp", "tree"], default="k1",
+    ap.add_argument("--workload", choices=["k1", "c4", "k2mp", "k1p", "tree"], default="k1",
                     help="k1: CONFIG_N2048_K1_COMP at 2^18 plaintexts; c4: CONFIG_N4096_K2_MP at 2^20; "
-                         "k2mp: CONFIG_N2048_K2_MP at 2^18; "
+                         "k2mp: CONFIG_N2048_K2_MP at 2^18; k1p: CONFIG_N2048_K1 at 2^18; "
                          "tree: tree PIR path selection (L = 16, a = 3)")
     ap.add_argument("--target", type=int, default=None,
                     help="plaintexts (smaller layouts are for profiling captures)")
@@ -209,11 +212,13 @@ def ntt_butterflies(params) -> dict:
     gsw.cpp:119-250, server.cpp:652-722). One butterfly = one Shoup product."""
     N = params.N
     per_ntt = (N // 2) * (N.bit_length() - 1)
+    # NTTs run per residue (k1_comp) or RNS limb; CONFIG_N2048_K1 has one prime
+    planes = 1 if (params._p.num_limbs == 1 and params._p.q1 == 0) else 2
     h = params.expansion_height
     useful = params.fst_dim_sz + params.l_ep * (params.num_dims - 1)
     nodes = sum(-(-useful // (1 << (h - d))) for d in range(h))
-    return {"Expand": nodes * (params.l_ks + 2) * per_ntt * 2,
-            "Other dim": (params.other_dim_sz - 1) * (2 * params.l_ep + 2) * per_ntt * 2}
+    return {"Expand": nodes * (params.l_ks + 2) * per_ntt * planes,
+            "Other dim": (params.other_dim_sz - 1) * (2 * params.l_ep + 2) * per_ntt * planes}
 
 
 def int_pipe_roofline(params, config: str, stages: dict, batch: int, device: int) -> dict:
@@ -337,7 +342,7 @@ def bench_reference(args, world, rank):
     n_q, n_w = min(args.steps, 8), min(args.warmup, 1)
     k2 = args.workload == "k2mp"
     try:
-        res = run_reference(n_q, n_w, procs, 7, "_k2mp" if k2 else "")
+        res = run_reference(n_q, n_w, procs, 7, REF_SUFFIX[args.workload])
     except Exception as e:  # reference binary missing or failed
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU server: {e}"}))
         return
@@ -347,7 +352,7 @@ def bench_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": res["mean_ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": (f"{'CONFIG_N2048_K2_MP' if k2 else 'k1_comp'} N=2048, {TARGET} "
+        "config": {"workload": (f"{CONFIGS[args.workload] if args.workload != 'k1' else 'k1_comp'} N=2048, {TARGET} "
                                 f"plaintexts, first dim 512 x 9 binary dims"),
                    "batch": 1, "parallelism": f"{procs} host processes"},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": procs, "kind": "reference",
@@ -579,7 +584,9 @@ def bench_ours(args, world, rank, local):
     if c4:
         workload = c4_workload_name(params)
     else:
-        workload = (f"{'CONFIG_N2048_K2_MP N=2048 two 29-bit limbs' if k2 else 'k1_comp N=2048'}, "
+        set_name = {"k1": "k1_comp N=2048", "k2mp": "CONFIG_N2048_K2_MP N=2048 two 29-bit limbs",
+                    "k1p": "CONFIG_N2048_K1 N=2048 one 60-bit prime"}[args.workload]
+        workload = (f"{set_name}, "
                     f"{args.target} plaintexts ({logical_db / 1e6:.1f} MB at 13 bits, "
                     f"{db_phys} B NTT form), first dim {params.fst_dim_sz} x "
                     f"{params.num_dims - 1} binary dims")
@@ -587,7 +594,7 @@ def bench_ours(args, world, rank, local):
         "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u64" if c4 else "u32",
+        "dtype": "u64" if (c4 or args.workload == "k1p") else "u32",
         "data": "synthetic (seeded DB coefficients < t generated on device; seeded uniform "
                 "ciphertexts and keys mod q -- the path is data-independent)",
         "config": {"workload": workload,
@@ -609,7 +616,7 @@ def bench_ours(args, world, rank, local):
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * ct_words * 8,
                 "d2h_bytes_per_step": B * 2 * N * 8},
         "roofline": {"bound": "hbm",
-                     "kernel": ("k4_scan_tc (first-dimension scan, tcgen05)" if c4
+                     "kernel": ("k4_scan_tc (first-dimension scan, tcgen05)" if (c4 or args.workload == "k1p")
                                 else "k_scan (first-dimension scan)"),
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
@@ -634,7 +641,7 @@ def bench_ours(args, world, rank, local):
                                     "kind": "reference", "sample": f"unavailable: {e}"}
     if world == 1 and not args.no_cpu_baseline and not c4 and args.target == TARGET:
         try:
-            res = run_reference(args.cpu_queries, 0, 1, 7, "_k2mp" if k2 else "")
+            res = run_reference(args.cpu_queries, 0, 1, 7, REF_SUFFIX[args.workload])
             line["cpu_baseline"] = {
                 "value": 1000.0 / res["mean_ms"], "unit": "queries/s", "cores": 1,
                 "kind": "reference",
