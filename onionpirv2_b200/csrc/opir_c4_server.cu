@@ -104,6 +104,7 @@ Server::Server(const opir_params &p, cudaStream_t stream, const opir::RowShard *
     sh_.other = static_cast<uint32_t>(rs->rows.size());
     sh_.num_pt = static_cast<uint64_t>(sh_.other) * sh_.n0;
     out_words_ = ct_;
+    shard_ = true;
     row_map_.alloc(rs->rows.size());
     ck(cudaMemcpy(row_map_.p, rs->rows.data(), rs->rows.size() * 4, cudaMemcpyHostToDevice),
        "row map");
@@ -527,7 +528,7 @@ void Server::enqueue_core(uint32_t n, const uint64_t *d_queries, uint64_t *d_res
   mark(ev, 3);
   const uint64_t *res = run_other_dims(n);
   mark(ev, 4);
-  if (out_words_ == ct_)  // row shard: the partial ciphertext, before the last levels
+  if (shard_)  // row shard: the partial ciphertext, before the last levels
     ck(cudaMemcpy2DAsync(d_resp, ct_ * 8, res, static_cast<size_t>(sh_.other) * ct_ * 8, ct_ * 8, n,
                          cudaMemcpyDeviceToDevice, st_), "partial copy");
   else
@@ -628,7 +629,7 @@ void Server::make_query_batch(uint32_t n, const uint64_t *ids, const uint64_t *q
 }
 
 void Server::combine_device(uint32_t n, const uint64_t *d_partials, uint64_t *d_responses) {
-  if (out_words_ != ct_) throw std::invalid_argument("combine_shards needs a row shard");
+  if (!shard_) throw std::invalid_argument("combine_shards needs a row shard");
   const uint32_t G = num_shards_, h = sh_.num_dims - 1;
   const uint64_t words = static_cast<uint64_t>(n) * G * ct_;
   for (auto &b : comb_)

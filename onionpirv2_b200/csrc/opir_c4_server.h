@@ -165,7 +165,8 @@ class Server {
   std::vector<uint32_t> host_rows_;
   opir::DevBuf<uint32_t> row_map_;
   opir::DevBuf<uint64_t> comb_[2];
-  uint64_t out_words_ = 2ull * kN;  // per query out of make_query: 2N, or 4N on a shard
+  uint64_t out_words_ = 2ull * kN;  // per query out of make_query: 2N, or a ciphertext on a shard
+  bool shard_ = false;              // a row shard (opir_shard.h) of the layout
   std::unordered_map<uint64_t, Keys> clients_;
   uint32_t cap_ = 0;
   uint64_t lvl_slots_ = 1;
