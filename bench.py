@@ -237,7 +237,25 @@ def int_pipe_roofline(params, config: str, stages: dict, batch: int, device: int
         achieved = per_query * batch / (ms / 1e3) / 1e9
         out["stages"][name] = {"achieved": achieved, "frac": achieved / peak,
                                "butterflies_per_query": per_query}
+    if config in ("CONFIG_N2048_K1_COMP", "CONFIG_N2048_K2_MP"):
+        out["tc_ntt_bound"] = tc_ntt_bound(peak, params.N, device)
     return out
+
+
+def tc_ntt_bound(bfly_peak_g: float, N: int, device: int) -> dict:
+    """Coefficients per second of a digit NTT on the register butterflies
+    (each coefficient takes part in log2 N butterflies, two per butterfly)
+    against the most a byte-sliced int8 tensor-core four-step NTT could
+    finish with a free MMA: one 5-class epilogue (2-plane digits x 4-plane
+    twiddles) and one 7-class epilogue (4 x 4 planes) per coefficient, each
+    at the measured register-resident recombination rate."""
+    from onionpirv2_b200.server import measure_recombine_rate
+    r5 = measure_recombine_rate(5, device) / 1e9
+    r7 = measure_recombine_rate(7, device) / 1e9
+    reg = bfly_peak_g * 2 / (N.bit_length() - 1)
+    tc = 1.0 / (1.0 / r5 + 1.0 / r7)
+    return {"unit": "G coefficients/s", "recombine_5": r5, "recombine_7": r7,
+            "register_ntt": reg, "tc_ntt_epilogue_only": tc, "register_over_tc": reg / tc}
 
 
 def synthetic_inputs(params, batch: int, seed: int):
@@ -617,11 +635,15 @@ def bench_ours(args, world, rank, local):
                 "d2h_bytes_per_step": B * 2 * N * 8},
         "roofline": {"bound": "hbm",
                      "kernel": ("k4_scan_tc (first-dimension scan, tcgen05)" if (c4 or args.workload == "k1p")
-                                else "k_scan (first-dimension scan)"),
+                                else "k_scan_tc (first-dimension scan, tcgen05)"),
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "algorithmic_bytes": alg_bytes,
-                     "traffic": (traffic or {}).get(f"{'c4_' if c4 else ''}batch_{B}")},
+                     # k2mp runs the k1_comp scan kernel on the same byte counts;
+                     # the one-prime set's scan has no capture of its own
+                     "traffic": (traffic or {}).get(
+                         {"k1": "", "k2mp": "", "c4": "c4_", "k1p": "k1p_"}[args.workload]
+                         + f"batch_{B}")},
         "int_pipe": int_pipe_roofline(params, config, stages, B, local),
         "batch_sweep": sweep,
         "clocks": clk.summary(),

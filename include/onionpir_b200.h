@@ -405,6 +405,17 @@ opir_status opir_server_stage_times(opir_server *server, float *ms_out,
  * of probe kernels on `device`. */
 opir_status opir_measure_butterfly_rate(opir_config config, int device, double *per_s);
 
+/* No counterpart in the reference. The rate (outputs per second) at which
+ * the device finishes one output of an int8 tensor-core product of
+ * byte-sliced 29-bit residues: `classes` (5 or 7) int32 shift-class sums
+ * S_s combined as sum_s S_s (2^(8s) mod q) in 64 bits and Barrett-reduced
+ * mod q -- the first-dimension scan's epilogue arithmetic -- on
+ * register-resident sums over every SM, without the accumulator loads and
+ * stores. A byte-sliced tensor-core NTT pays this once per coefficient per
+ * matrix step, so the rate bounds such an NTT from above whatever the MMA
+ * speed. Runs about a millisecond of probe kernels on `device`. */
+opir_status opir_measure_recombine_rate(int classes, int device, double *per_s);
+
 /* Total kernel launches issued by this library in this process. */
 uint64_t opir_launch_count(void);
 

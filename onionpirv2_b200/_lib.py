@@ -133,6 +133,7 @@ _SIGS = {
     "opir_server_stage_times": ([C.c_void_p, C.POINTER(C.c_float), u32p], C.c_int),
     "opir_launch_count": ([], C.c_uint64),
     "opir_measure_butterfly_rate": ([C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "opir_measure_recombine_rate": ([C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "opir_server_expand_query": ([C.c_void_p, C.c_uint64, u64p, u64p], C.c_int),
     "opir_server_complete_selectors": ([C.c_void_p, C.c_uint64, u64p, u64p], C.c_int),
     "opir_server_evaluate_first_dim": ([C.c_void_p, u64p, u64p], C.c_int),

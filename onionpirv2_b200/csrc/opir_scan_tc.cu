@@ -321,6 +321,41 @@ void configure_scan_tc() {
   done.insert(dev);
 }
 
+// Recombination-rate probe: the epilogue arithmetic above (NC shift-class
+// sums S_s < 2^31 -> sum_s S_s (2^(8s) mod q) in 64 bits -> reduce64_tc)
+// on register-resident sums, 8 outputs per thread per iteration, without the
+// TMEM loads and stores: the rate at which an SM finishes one output of an
+// int8 product of byte-sliced 29-bit residues when nothing else is in the
+// way. The multipliers take one bit of the running result after every
+// iteration (NC adds per 8 outputs), so no product can be computed once for
+// several iterations; the values are not meaningful and `sink` keeps the
+// work alive.
+template <int NC>
+__global__ void __launch_bounds__(256)
+k_recombine_rate(uint32_t *__restrict__ sink, uint32_t iters, uint32_t q, uint64_t mu, uint32_t w0) {
+  uint32_t P[NC][8];
+  uint32_t w[NC];
+#pragma unroll
+  for (int s = 0; s < NC; ++s) {
+    w[s] = (w0 + 977u * s) % q;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) P[s][c] = (threadIdx.x * 64 + s * 8 + c + blockIdx.x) & 0x7fffffffu;
+  }
+  uint32_t acc = 0;
+  for (uint32_t it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      uint64_t x = static_cast<uint64_t>(P[0][c]) * w[0];
+#pragma unroll
+      for (int s = 1; s < NC; ++s) x += static_cast<uint64_t>(P[s][c]) * w[s];
+      acc ^= reduce64_tc(x, q, mu);
+    }
+#pragma unroll
+    for (int s = 0; s < NC; ++s) w[s] += acc & 1u;  // stays below 2^29 + iters
+  }
+  sink[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
 }  // namespace
 
 // 3-D byte tensor [planes][rows][k] (k innermost, row stride = k_bytes),
@@ -373,6 +408,31 @@ void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcSc
   note_launches(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw std::runtime_error(std::string("k_scan_tc: ") + cudaGetErrorString(e));
+}
+
+uint32_t recombine_rate_blocks(int sms, int classes) {
+  int occ = 0;
+  const cudaError_t e =
+      classes == 5 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_recombine_rate<5>, 256, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_recombine_rate<7>, 256, 0);
+  if (e != cudaSuccess || occ < 1) occ = 1;
+  return static_cast<uint32_t>(sms) * static_cast<uint32_t>(occ);
+}
+
+uint64_t launch_recombine_rate(uint32_t *sink, uint32_t blocks, uint32_t iters, int classes,
+                               cudaStream_t st) {
+  if (classes != 5 && classes != 7) throw std::invalid_argument("recombine probe: 5 or 7 classes");
+  const uint32_t q = 536813569u;  // the first k1_comp residue
+  const uint64_t mu = ~0ull / q;
+  if (classes == 5)
+    k_recombine_rate<5><<<blocks, 256, 0, st>>>(sink, iters, q, mu, 123456789u);
+  else
+    k_recombine_rate<7><<<blocks, 256, 0, st>>>(sink, iters, q, mu, 123456789u);
+  note_launches(1);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("k_recombine_rate: ") + cudaGetErrorString(e));
+  return static_cast<uint64_t>(blocks) * 256 * iters * 8;
 }
 
 }  // namespace opir

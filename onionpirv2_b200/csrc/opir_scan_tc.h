@@ -39,4 +39,12 @@ uint32_t scan_tc_max_stages(uint32_t ntile, uint32_t kt);
 void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcScanArgs &args,
                     int sm_count, cudaStream_t st);
 
+// Recombination-rate probe (the scan epilogue's arithmetic on register
+// values, `classes` = 5 or 7 shift classes): blocks of 256 threads that fill
+// `sms` SMs, and a launch of `iters` iterations into sink (blocks x 256 u32).
+// Returns the outputs the launch finishes.
+uint32_t recombine_rate_blocks(int sms, int classes);
+uint64_t launch_recombine_rate(uint32_t *sink, uint32_t blocks, uint32_t iters, int classes,
+                               cudaStream_t st);
+
 }  // namespace opir

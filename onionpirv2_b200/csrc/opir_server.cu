@@ -973,6 +973,42 @@ void tune_levels(opir_server *s, uint32_t max_batch, cudaEvent_t e0, cudaEvent_t
   clear_graphs(s);
 }
 
+// Device rate of a register-resident probe kernel: one warm-up launch, then
+// three timed launches on a private stream; `launch(sink, st)` returns the
+// units (butterflies, outputs) one launch performs.
+template <class F>
+double probe_rate(int device, size_t sink_words, F &&launch) {
+  DeviceGuard g(device);
+  DevBuf<uint64_t> sink;
+  sink.alloc(sink_words);
+  cudaStream_t st = nullptr;
+  ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double rate = 0;
+  try {
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    launch(sink.p, st);  // warm-up
+    ck(cudaEventRecord(e0, st), "event record");
+    uint64_t units = 0;
+    for (int r = 0; r < 3; ++r) units += launch(sink.p, st);
+    ck(cudaEventRecord(e1, st), "event record");
+    ck(cudaEventSynchronize(e1), "probe");
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+    rate = static_cast<double>(units) / (static_cast<double>(ms) / 1e3);
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  return rate;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2050,42 +2086,27 @@ opir_status opir_measure_butterfly_rate(opir_config config, int device, double *
                  config != OPIR_CONFIG_N2048_K2_MP && config != OPIR_CONFIG_N2048_K1))
     return OPIR_ERR_INVALID_ARGUMENT;
   return guarded(nullptr, [&] {
-    DeviceGuard g(device);
     int sms = 0;
     ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
     const bool c4 = config == OPIR_CONFIG_N4096_K2_MP || config == OPIR_CONFIG_N2048_K1;
     const uint32_t blocks = c4 ? opir4::bfly_rate_blocks(sms) : opir::bfly_rate_blocks(sms);
     const uint32_t iters = c4 ? 256 : 1024;
-    DevBuf<uint64_t> sink;
-    sink.alloc(static_cast<size_t>(blocks) * 256);
-    cudaStream_t st = nullptr;
-    ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    auto launch = [&] {
-      return c4 ? opir4::launch_bfly_rate(sink.p, blocks, iters, st)
-                : opir::launch_bfly_rate(reinterpret_cast<uint32_t *>(sink.p), blocks, iters, st);
-    };
-    try {
-      ck(cudaEventCreate(&e0), "event");
-      ck(cudaEventCreate(&e1), "event");
-      launch();  // warm-up
-      ck(cudaEventRecord(e0, st), "event record");
-      uint64_t bfly = 0;
-      for (int r = 0; r < 3; ++r) bfly += launch();
-      ck(cudaEventRecord(e1, st), "event record");
-      ck(cudaEventSynchronize(e1), "probe");
-      float ms = 0;
-      ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
-      *per_s = static_cast<double>(bfly) / (static_cast<double>(ms) / 1e3);
-    } catch (...) {
-      if (e0) cudaEventDestroy(e0);
-      if (e1) cudaEventDestroy(e1);
-      cudaStreamDestroy(st);
-      throw;
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaStreamDestroy(st);
+    *per_s = probe_rate(device, static_cast<size_t>(blocks) * 256, [&](uint64_t *sink, cudaStream_t st) {
+      return c4 ? opir4::launch_bfly_rate(sink, blocks, iters, st)
+                : opir::launch_bfly_rate(reinterpret_cast<uint32_t *>(sink), blocks, iters, st);
+    });
+  });
+}
+
+opir_status opir_measure_recombine_rate(int classes, int device, double *per_s) {
+  if (!per_s || (classes != 5 && classes != 7)) return OPIR_ERR_INVALID_ARGUMENT;
+  return guarded(nullptr, [&] {
+    int sms = 0;
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "sm count");
+    const uint32_t blocks = opir::recombine_rate_blocks(sms, classes);
+    *per_s = probe_rate(device, static_cast<size_t>(blocks) * 128, [&](uint64_t *sink, cudaStream_t st) {
+      return opir::launch_recombine_rate(reinterpret_cast<uint32_t *>(sink), blocks, 512, classes, st);
+    });
   });
 }
 

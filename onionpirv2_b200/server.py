@@ -478,6 +478,17 @@ def measure_butterfly_rate(config: str = "CONFIG_N2048_K1_COMP", device: int = 0
     return float(out.value)
 
 
+def measure_recombine_rate(classes: int = 7, device: int = 0) -> float:
+    """Outputs per second the device finishes for an int8 tensor-core product
+    of byte-sliced 29-bit residues: `classes` shift-class sums recombined and
+    reduced mod q, register-resident (opir_measure_recombine_rate)."""
+    out = C.c_double()
+    rc = L.load().opir_measure_recombine_rate(classes, device, C.byref(out))
+    if rc != OPIR_OK:
+        _raise(rc, "opir_measure_recombine_rate failed")
+    return float(out.value)
+
+
 def launch_count() -> int:
     """Kernel launches issued by the library in this process."""
     return int(L.load().opir_launch_count())
