@@ -651,6 +651,11 @@ def bench_ours(args, world, rank, local):
         "gpu_launches": launches,
         "setup": {"db_load_s": round(load_s, 3), "autotune_s": round(tune_s, 3),
                   "scan_tile": srv.scan_tile(B), "scan_tile_plain": srv.scan_tile(1),
+                  # cluster width per expansion / MUX level (0: the fixed rule)
+                  "level_splits": {str(n): {k: v[:h] for k, v, h in
+                                            (("expand", ls["expand"], params.expansion_height),
+                                             ("mux", ls["mux"], params.num_dims - 1))}
+                                   for n, ls in ((1, srv.level_splits(1)), (B, srv.level_splits(B)))},
                   "gpu": torch.cuda.get_device_name(device)},
     }
     if world == 1 and not args.no_cpu_baseline and c4 and args.target == C4_TARGET:

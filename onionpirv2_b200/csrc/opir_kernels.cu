@@ -263,9 +263,8 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
   __syncthreads();
   fwd_mid_r<RES>(sm, G::lks, T.fwt);
   // inner product with the key rows (row t encrypts sigma(s) B^t), D-order;
-  // digit NTT values stay in [0, 4q) when l_ks <= 8 (sum < 2^64), else canonical
+  // L_KS products per coefficient (mac_in)
   const uint32_t *key = bv_keys[b] + bv_level_off + RES * kN;
-  constexpr bool lazy = G::lks <= 8;
   uint64_t ab[8], aa[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) ab[k] = aa[k] = 0;
@@ -277,7 +276,7 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
       ld_plane<3>(sm + i * kPad, v, tid);
       fD<RES>(v, wd);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = lazy ? to4q<RES>(v[k]) : canon8<RES>(v[k]);
+      for (int k = 0; k < 8; ++k) v[k] = mac_in<RES, G::lks>(v[k]);
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int j0 = 4 * (tid + 256 * h);
@@ -296,7 +295,7 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
     iload_d(wd, T.iwt, tid);
     uint32_t v[8], w[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { v[k] = red64<RES>(ab[k]); w[k] = red64<RES>(aa[k]); }
+    for (int k = 0; k < 8; ++k) { v[k] = red64_lazy<RES>(ab[k]); w[k] = red64_lazy<RES>(aa[k]); }
     iD<RES>(v, wd);
     iD<RES>(w, wd);
     st_plane<3>(sm, v, tid);
@@ -404,7 +403,7 @@ __device__ __forceinline__ void expand_split_body(const DevParams &P, uint32_t g
       ld_plane<3>(sm + i * kPad, v, tid);
       fD<RES>(v, wd);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = to4q<RES>(v[k]);
+      for (int k = 0; k < 8; ++k) v[k] = mac_in<RES, G::lks>(v[k]);  // L_KS products over the cluster
       const int row = i0 + i;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -445,7 +444,7 @@ __device__ __forceinline__ void expand_split_body(const DevParams &P, uint32_t g
     iload_d(wd, T.iwt, tid);
     uint32_t v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = red64<RES>(tot[k]);
+    for (int k = 0; k < 8; ++k) v[k] = red64_lazy<RES>(tot[k]);
     iD<RES>(v, wd);
     st_plane<3>(sm, v, tid);
   }
@@ -497,8 +496,10 @@ k_expand_level_split(DevParams P, uint32_t galois_inv, uint32_t kshift,
 // null) against NTT-form RGSW rows: acc_k += sum_rows digit * rgsw[row][k],
 // accumulated at this thread's D-order positions. Digit i (LSB first) of
 // poly p meets row p*l + (l - 1 - i) (gsw.cpp:283-293). Uses l padded planes.
-// Digit NTT values enter the MAC in [0, 4q) when 2 l <= 16 (a sum of 2 l
-// products below 4q x q < 2^60 stays below 2^64), else canonical.
+// The accumulators start at zero and take 2 l products of mac_in values;
+// when 2 l > 16 they are reduced to [0, 2q] after the first polynomial, so
+// at most 16 products (plus that carry) build up between reductions, below
+// 2^64.
 template <int RES, int L, int B, int KIND>
 __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x,
                                            const uint32_t *y, const uint32_t *rgsw,
@@ -506,7 +507,8 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x
                                            uint64_t (&acc1)[8]) {
   constexpr uint32_t q = Res<RES>::q;
   constexpr int l = L;
-  constexpr bool lazy = L <= 8;
+  constexpr bool mid = 2 * L > 16;            // reduce after the first polynomial
+  constexpr int kProducts = mid ? L : 2 * L;  // products between reductions
   const ResidueTables &T = P.r[RES];
   const int tid = threadIdx.x;
 #pragma unroll 1
@@ -539,7 +541,7 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x
       ld_plane<3>(sm + i * kPad, v, tid);
       fD<RES>(v, wd);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = lazy ? to4q<RES>(v[k]) : canon8<RES>(v[k]);
+      for (int k = 0; k < 8; ++k) v[k] = mac_in<RES, kProducts>(v[k]);
       const int row = p * l + (l - 1 - i);
       const uint32_t *R0 = rgsw + (uint64_t)row * kCtWords + RES * kN;
 #pragma unroll
@@ -551,6 +553,13 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x
         acc0[4 * h + 1] += (uint64_t)v[4 * h + 1] * r0.y; acc1[4 * h + 1] += (uint64_t)v[4 * h + 1] * r1.y;
         acc0[4 * h + 2] += (uint64_t)v[4 * h + 2] * r0.z; acc1[4 * h + 2] += (uint64_t)v[4 * h + 2] * r1.z;
         acc0[4 * h + 3] += (uint64_t)v[4 * h + 3] * r0.w; acc1[4 * h + 3] += (uint64_t)v[4 * h + 3] * r1.w;
+      }
+    }
+    if (mid && p == 0) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        acc0[k] = red64_lazy<RES>(acc0[k]);
+        acc1[k] = red64_lazy<RES>(acc1[k]);
       }
     }
     __syncthreads();
@@ -918,7 +927,7 @@ __device__ __forceinline__ void mux_level_body(const DevParams &P, const Shape &
     iload_d(wd, T.iwt, tid);
     uint32_t v[8], w[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { v[k] = red64<RES>(acc0[k]); w[k] = red64<RES>(acc1[k]); }
+    for (int k = 0; k < 8; ++k) { v[k] = red64_lazy<RES>(acc0[k]); w[k] = red64_lazy<RES>(acc1[k]); }
     iD<RES>(v, wd);
     iD<RES>(w, wd);
     st_plane<3>(sm, v, tid);
@@ -970,7 +979,6 @@ __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32
                                                 uint64_t (&acc0)[8], uint64_t (&acc1)[8]) {
   constexpr uint32_t q = Res<RES>::q;
   constexpr int l = L;
-  constexpr bool lazy = L <= 8;
   const ResidueTables &T = P.r[RES];
   const int tid = threadIdx.x;
   uint64_t d[8];
@@ -1001,7 +1009,7 @@ __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32
     ld_plane<3>(sm + i * kPad, v, tid);
     fD<RES>(v, wd);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = lazy ? to4q<RES>(v[k]) : canon8<RES>(v[k]);
+    for (int k = 0; k < 8; ++k) v[k] = mac_in<RES, 2 * L>(v[k]);  // 2 l products over the cluster
     const int row = p * l + (l - 1 - (i0 + i));
     const uint32_t *R0 = rgsw + (uint64_t)row * kCtWords + RES * kN;
 #pragma unroll
@@ -1074,7 +1082,7 @@ __device__ __forceinline__ void mux_split_body(const DevParams &P, const Shape &
     iload_d(wd, T.iwt, tid);
     uint32_t v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = red64<RES>(tot[k]);
+    for (int k = 0; k < 8; ++k) v[k] = red64_lazy<RES>(tot[k]);
     iD<RES>(v, wd);
     st_plane<3>(sm, v, tid);
   }

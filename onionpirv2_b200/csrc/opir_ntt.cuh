@@ -9,11 +9,12 @@
 //     twiddles of passes C and D are loaded once per plane loop instead of
 //     once per plane;
 //   * forward butterflies correct X only where the bound needs it. With
-//     canonical inputs and Shoup products t in [0, 2q), an uncorrected
-//     butterfly maps [0, b q) to [0, (b + 2) q) and a corrected one (X taken
-//     to [0, 4q) first) maps [0, 8q) to [0, 6q); correcting stages 4, 6, 8
-//     and 10 keeps every value below 8q < 2^32 (q < 2^29), and the output
-//     lies in [0, 8q).
+//     inputs below 2q (canonical values, or gadget digits as r + q) and
+//     Shoup products t in [0, 2q), an uncorrected butterfly maps [0, b q)
+//     to [0, (b + 2) q) and a corrected one (X taken to [0, 4q) first) maps
+//     [0, 8q) to [0, 6q); the three uncorrected stages of the first pass end
+//     below 8q, and correcting stages 4, 6, 8 and 10 keeps every later value
+//     below 8q < 2^32 (8 q1 = 4294508552), so the output lies in [0, 8q).
 // This header defines constant-memory arrays and is included by one
 // translation unit only (opir_kernels.cu), which uploads them per device.
 #pragma once
@@ -37,12 +38,33 @@ static __constant__ uint2 c_iwt[2][64];
 // {N^-1, its Shoup companion, iw[1] N^-1, its Shoup companion} per residue
 static __constant__ uint4 c_nscale[2];
 
+// floor(x mu / 2^64) - e with 0 <= e < 3, mod 2^32, from one high product:
+// mu = floor((2^64 - 1) / q) = 8 2^32 + ml for both residues, so with x =
+// xh 2^32 + xl, x mu / 2^64 = 8 xh + xh ml / 2^32 + xl / 2^29 + xl ml / 2^64,
+// and the estimate drops three fractions, each below 1.
+template <int RES>
+__device__ __forceinline__ uint32_t quot64(uint64_t x) {
+  constexpr uint64_t mu = Res<RES>::mu;
+  static_assert((mu >> 32) == 8, "quot64 assumes floor(2^64 / q) = 8 2^32 + ml");
+  const uint32_t xh = static_cast<uint32_t>(x >> 32), xl = static_cast<uint32_t>(x);
+  return (xh << 3) + __umulhi(xh, static_cast<uint32_t>(mu)) + (xl >> 29);
+}
+// any x -> [0, 2q]: x mu / 2^64 > x / q - 1 - 1/q, so the estimate exceeds
+// x / q - 4 - 1/q and x - quot64(x) q <= 4q (< 2^32, so 32-bit arithmetic is
+// exact); one correction maps [0, 4q] to [0, 2q]. The inverse NTT's passes
+// take inputs up to 2q inclusive (X + Y <= 4q < 2^32; their min correction
+// maps [0, 4q] to [0, 2q]).
+template <int RES>
+__device__ __forceinline__ uint32_t red64_lazy(uint64_t x) {
+  constexpr uint32_t Q = Res<RES>::q;
+  const uint32_t r = static_cast<uint32_t>(x) - quot64<RES>(x) * Q;
+  return min(r, r - 2 * Q);
+}
 template <int RES>
 __device__ __forceinline__ uint32_t red64(uint64_t x) {  // any x -> [0, q)
   constexpr uint32_t Q = Res<RES>::q;
-  const uint64_t qhat = __umul64hi(x, Res<RES>::mu);
-  uint32_t r = static_cast<uint32_t>(x - qhat * Q);  // < 3q < 2^32
-  r = min(r, r - 2 * Q);
+  uint32_t r = red64_lazy<RES>(x);  // [0, 2q]
+  r = min(r, r - Q);                // [0, q]
   return min(r, r - Q);
 }
 template <int RES>
@@ -55,6 +77,17 @@ __device__ __forceinline__ uint32_t canon8(uint32_t x) {  // [0, 8q) -> [0, q)
 template <int RES>
 __device__ __forceinline__ uint32_t to4q(uint32_t x) {  // [0, 8q) -> [0, 4q)
   return min(x, x - 4 * Res<RES>::q);
+}
+// A digit NTT value leaves the forward transform in [0, 8q) and enters a
+// 64-bit multiply-accumulate with canonical key / RGSW values. P products
+// (plus a carried value below 2q) stay below 2^64 uncorrected when P <= 8
+// (8 8q q < 64 q1^2 = 0.99979 2^64), with values taken to [0, 4q) when
+// P <= 16, and canonical beyond.
+template <int RES, int P>
+__device__ __forceinline__ uint32_t mac_in(uint32_t v) {
+  if (P <= 8) return v;
+  if (P <= 16) return to4q<RES>(v);
+  return canon8<RES>(v);
 }
 
 // ------------------------------------------------------ gadget digits
@@ -120,7 +153,9 @@ __device__ __forceinline__ uint64_t digit_source(uint64_t v) {
   for (int i = 0; i < L; ++i) C += static_cast<uint64_t>(digit_offset<B, KIND>()) << (B * i);
   return v + C - (v > kQ / 2 ? kQ : 0);
 }
-// r_i as a residue mod Q (r_i + Q for negative r_i).
+// r_i as a residue mod Q below 2Q: r_i + Q for every balanced digit (in
+// [Q - o, Q - o + 2^B), not reduced: the forward NTT's first pass takes
+// inputs below 2q), the digit itself for unsigned digits.
 template <uint32_t Q, int B, int KIND = kDigitsLow>
 __device__ __forceinline__ uint32_t digit_res(uint64_t u, int i) {
   const int o = B * i;  // a constant once the caller's digit loop is unrolled
@@ -131,8 +166,7 @@ __device__ __forceinline__ uint32_t digit_res(uint64_t u, int i) {
   else f = __funnelshift_r(lo, hi, o);
   f &= (1u << B) - 1;
   if (KIND == kDigitsUnsigned) return f;  // f < 2^B < Q
-  const uint32_t t = f + (Q - digit_offset<B, KIND>());
-  return min(t, t - Q);
+  return f + (Q - digit_offset<B, KIND>());
 }
 
 // --------------------------------------------------------------- forward
@@ -153,7 +187,8 @@ __device__ __forceinline__ void fpass8(uint32_t (&v)[8], const uint2 (&w)[7]) {
   fbf<Q, C3>(v[0], v[1], w[3]); fbf<Q, C3>(v[2], v[3], w[4]);
   fbf<Q, C3>(v[4], v[5], w[5]); fbf<Q, C3>(v[6], v[7], w[6]);
 }
-// pass A (stages 1-3), canonical input; twiddles 1..7 from constant memory
+// pass A (stages 1-3), inputs below 2q, outputs below 8q; twiddles 1..7
+// from constant memory
 template <int RES>
 __device__ __forceinline__ void fA(uint32_t (&v)[8]) {
   const uint2 w[7] = {c_fwt[RES][1], c_fwt[RES][2], c_fwt[RES][3], c_fwt[RES][4],
@@ -231,7 +266,8 @@ __device__ __forceinline__ void fwd_mid_r(uint32_t *sm, int np, const uint2 *fwt
 }
 
 // --------------------------------------------------------------- inverse
-// Gentleman-Sande, inputs and outputs in [0, 2q) between passes.
+// Gentleman-Sande, inputs and outputs in [0, 2q] between passes (X + Y and
+// X - Y + 2q stay within [0, 4q], and the min maps [0, 4q] to [0, 2q]).
 template <uint32_t Q>
 __device__ __forceinline__ void ibf(uint32_t &X, uint32_t &Y, uint2 w) {
   uint32_t u = X + Y;
