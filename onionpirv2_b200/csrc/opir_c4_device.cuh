@@ -172,6 +172,7 @@ __device__ __forceinline__ void fwd_mid(uint64_t *sm, int np, const Tables &T) {
   {
     ulonglong2 w[7];
     tw_const<L, true>(w, 8, t >> 6);
+#pragma unroll
     for (int i = 0; i < np; ++i) {
       uint64_t v[8];
       ld_plane<1>(sm + i * kPad, v, t);
@@ -183,6 +184,7 @@ __device__ __forceinline__ void fwd_mid(uint64_t *sm, int np, const Tables &T) {
   {
     ulonglong2 w[7];
     tw_global(w, T.fwt[L], 64, t >> 3);
+#pragma unroll
     for (int i = 0; i < np; ++i) {
       uint64_t v[8];
       ld_plane<2>(sm + i * kPad, v, t);
@@ -220,6 +222,7 @@ __device__ __forceinline__ void inv_mid(uint64_t *sm, int np, const Tables &T) {
   {
     ulonglong2 w[7];
     tw_global(w, T.iwt[L], 64, t >> 3);
+#pragma unroll
     for (int i = 0; i < np; ++i) {
       uint64_t v[8];
       ld_plane<2>(sm + i * kPad, v, t);
@@ -231,6 +234,7 @@ __device__ __forceinline__ void inv_mid(uint64_t *sm, int np, const Tables &T) {
   {
     ulonglong2 w[7];
     tw_const<L, false>(w, 8, t >> 6);
+#pragma unroll
     for (int i = 0; i < np; ++i) {
       uint64_t v[8];
       ld_plane<1>(sm + i * kPad, v, t);

@@ -190,28 +190,44 @@ __device__ __forceinline__ void fD(uint64_t (&v)[8], const ulonglong2 (&w)[6]) {
   }
 }
 // passes B and C over np planes stored in A-order after fA (up to a
-// __syncthreads); ends synchronised
+// __syncthreads); ends synchronised. Full = true unrolls the plane loops
+// (faster in the expansion and MUX levels; the selector kernel keeps the
+// compiler's choice, which is faster there).
+__device__ __forceinline__ void ipass8(uint64_t (&v)[8], const ulonglong2 (&w)[7]);
+template <int PASS, bool FWD>
+__device__ __forceinline__ void mid_plane(uint64_t *pl, const ulonglong2 (&w)[7], int t) {
+  uint64_t v[8];
+  ld_plane<PASS>(pl, v, t);
+  if (FWD) {
+    if (PASS == 1) fpass8<true, false, true>(v, w);
+    else fpass8<false, true, false>(v, w);
+  } else {
+    ipass8(v, w);
+  }
+  st_plane<PASS>(pl, v, t);
+}
+template <bool Full = true>
 __device__ __forceinline__ void fwd_mid(uint64_t *sm, int np, const ulonglong2 *fwt) {
   const int t = threadIdx.x;
   {
     ulonglong2 w[7];
     load_b(w, c1_fwt, t);
-    for (int i = 0; i < np; ++i) {
-      uint64_t v[8];
-      ld_plane<1>(sm + i * kPad, v, t);
-      fpass8<true, false, true>(v, w);
-      st_plane<1>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane<1, true>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane<1, true>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
   {
     ulonglong2 w[7];
     load_c(w, fwt, t);
-    for (int i = 0; i < np; ++i) {
-      uint64_t v[8];
-      ld_plane<2>(sm + i * kPad, v, t);
-      fpass8<false, true, false>(v, w);
-      st_plane<2>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane<2, true>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane<2, true>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
@@ -244,28 +260,29 @@ __device__ __forceinline__ void iD(uint64_t (&v)[8], const ulonglong2 (&w)[6]) {
   }
 }
 // passes C and B over np planes holding D-order values after iD (up to a
-// __syncthreads); ends synchronised
+// __syncthreads); ends synchronised. Full as in fwd_mid.
+template <bool Full = true>
 __device__ __forceinline__ void inv_mid(uint64_t *sm, int np, const ulonglong2 *iwt) {
   const int t = threadIdx.x;
   {
     ulonglong2 w[7];
     load_c(w, iwt, t);
-    for (int i = 0; i < np; ++i) {
-      uint64_t v[8];
-      ld_plane<2>(sm + i * kPad, v, t);
-      ipass8(v, w);
-      st_plane<2>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane<2, false>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane<2, false>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
   {
     ulonglong2 w[7];
     load_b(w, c1_iwt, t);
-    for (int i = 0; i < np; ++i) {
-      uint64_t v[8];
-      ld_plane<1>(sm + i * kPad, v, t);
-      ipass8(v, w);
-      st_plane<1>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane<1, false>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane<1, false>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
@@ -475,7 +492,7 @@ k1p_expand_level(Dev1 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *_
 // null) split into L balanced base-2^B digits; digit d of poly p meets row
 // p L + (L - 1 - d) (MSB-first rows). Digit planes in groups of up to 5;
 // sums folded below 2q after each group.
-template <int L, int B>
+template <int L, int B, bool Full = true>
 __device__ __forceinline__ void gadget_mac(const Dev1 &P, const uint64_t *x, const uint64_t *y,
                                            const uint64_t *rgsw, uint64_t *sm,
                                            uint64_t (&acc0)[8], uint64_t (&acc1)[8]) {
@@ -503,7 +520,7 @@ __device__ __forceinline__ void gadget_mac(const Dev1 &P, const uint64_t *x, con
         st_plane<0>(sm + e * kPad, v, tid);
       }
       __syncthreads();
-      fwd_mid(sm, G, P.fwt);
+      fwd_mid<Full>(sm, G, P.fwt);
       ulonglong2 wd[6];
       load_d(wd, P.fwt, tid);
       for (int e = 0; e < G; ++e) {
@@ -537,7 +554,7 @@ k1p_selectors(Dev1 P, Shape1 S, const uint64_t *__restrict__ leaves, uint64_t le
   uint64_t acc0[8], acc1[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc0[k] = acc1[k] = 0;
-  gadget_mac<kLKey, kBaseKey>(P, ct, nullptr, gsw_keys[b], sm1, acc0, acc1);
+  gadget_mac<kLKey, kBaseKey, false>(P, ct, nullptr, gsw_keys[b], sm1, acc0, acc1);
   uint64_t *bot = outs + static_cast<uint64_t>(S.l_ep + r) * kRowWords;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -557,7 +574,7 @@ k1p_selectors(Dev1 P, Shape1 S, const uint64_t *__restrict__ leaves, uint64_t le
     st_plane<0>(sm1 + p * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid(sm1, 2, P.fwt);
+  fwd_mid<false>(sm1, 2, P.fwt);
   ulonglong2 wd[6];
   load_d(wd, P.fwt, tid);
   uint64_t *top = outs + static_cast<uint64_t>(r) * kRowWords;

@@ -271,6 +271,7 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
   {
     uint2 wd[6];
     fload_d(wd, T.fwt, tid);
+#pragma unroll
     for (int i = 0; i < G::lks; ++i) {
       uint32_t v[8];
       ld_plane<3>(sm + i * kPad, v, tid);
@@ -390,7 +391,7 @@ __device__ __forceinline__ void expand_split_body(const DevParams &P, uint32_t g
     st_plane<0>(sm + i * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid_r<RES>(sm, D, T.fwt);
+  fwd_mid_r<RES, false>(sm, D, T.fwt);
   const uint32_t *key = bv_keys[b] + bv_level_off + RES * kN;
   uint64_t ab[8], aa[8];
 #pragma unroll
@@ -536,6 +537,7 @@ __device__ __forceinline__ void gadget_mac(const DevParams &P, const uint32_t *x
     fwd_mid_r<RES>(sm, l, T.fwt);
     uint2 wd[6];
     fload_d(wd, T.fwt, tid);
+#pragma unroll
     for (int i = 0; i < l; ++i) {
       uint32_t v[8];
       ld_plane<3>(sm + i * kPad, v, tid);
@@ -1001,7 +1003,7 @@ __device__ __forceinline__ void gadget_mac_part(const DevParams &P, const uint32
     st_plane<0>(sm + i * kPad, v, tid);
   }
   __syncthreads();
-  fwd_mid_r<RES>(sm, D, T.fwt);
+  fwd_mid_r<RES, false>(sm, D, T.fwt);
   uint2 wd[6];
   fload_d(wd, T.fwt, tid);
   for (int i = 0; i < D; ++i) {

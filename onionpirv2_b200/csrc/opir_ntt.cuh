@@ -235,31 +235,47 @@ __device__ __forceinline__ void fD(uint32_t (&v)[8], const uint2 (&w)[6]) {
     fbf<Q, false>(u[2], u[3], w[3 * h + 2]);
   }
 }
+template <uint32_t Q>
+__device__ __forceinline__ void ipass8(uint32_t (&v)[8], const uint2 (&w)[7]);
+// One radix-8 pass over the padded plane `pl`: load in pass order PASS,
+// butterflies, store back.
+template <int RES, int PASS, bool FWD>
+__device__ __forceinline__ void mid_plane_r(uint32_t *pl, const uint2 (&w)[7], int t) {
+  constexpr uint32_t Q = Res<RES>::q;
+  uint32_t v[8];
+  ld_plane<PASS>(pl, v, t);
+  if (!FWD) ipass8<Q>(v, w);
+  else if (PASS == 1) fpass8<Q, true, false, true>(v, w);
+  else fpass8<Q, false, true, false>(v, w);
+  st_plane<PASS>(pl, v, t);
+}
 // Passes B and C over `np` padded planes stored in A-order after fA, up to a
 // __syncthreads; ends synchronised. The caller then loads D-order and runs fD.
-template <int RES>
+// Full = true unrolls the plane loops (faster in the one-CTA-per-step
+// kernels; the cluster-split kernels, with 1 to 4 planes per CTA, keep the
+// compiler's choice, which is faster there).
+template <int RES, bool Full = true>
 __device__ __forceinline__ void fwd_mid_r(uint32_t *sm, int np, const uint2 *fwt) {
-  constexpr uint32_t Q = Res<RES>::q;
   const int t = threadIdx.x;
   {
     uint2 w[7];
     fload_b<RES>(w, t);
-    for (int i = 0; i < np; ++i) {
-      uint32_t v[8];
-      ld_plane<1>(sm + i * kPad, v, t);
-      fpass8<Q, true, false, true>(v, w);
-      st_plane<1>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 1, true>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 1, true>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
   {
     uint2 w[7];
     fload_c(w, fwt, t);
-    for (int i = 0; i < np; ++i) {
-      uint32_t v[8];
-      ld_plane<2>(sm + i * kPad, v, t);
-      fpass8<Q, false, true, false>(v, w);
-      st_plane<2>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 2, true>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 2, true>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
@@ -347,29 +363,28 @@ __device__ __forceinline__ void iA(uint32_t (&v)[8]) {
 }
 // Passes C and B over `np` planes holding D-order values after iD, up to a
 // __syncthreads; ends synchronised. The caller then loads A-order and runs iA.
-template <int RES>
+template <int RES, bool Full = true>
 __device__ __forceinline__ void inv_mid_r(uint32_t *sm, int np, const uint2 *iwt) {
-  constexpr uint32_t Q = Res<RES>::q;
   const int t = threadIdx.x;
   {
     uint2 w[7];
     iload_c(w, iwt, t);
-    for (int i = 0; i < np; ++i) {
-      uint32_t v[8];
-      ld_plane<2>(sm + i * kPad, v, t);
-      ipass8<Q>(v, w);
-      st_plane<2>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 2, false>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 2, false>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
   {
     uint2 w[7];
     iload_b<RES>(w, t);
-    for (int i = 0; i < np; ++i) {
-      uint32_t v[8];
-      ld_plane<1>(sm + i * kPad, v, t);
-      ipass8<Q>(v, w);
-      st_plane<1>(sm + i * kPad, v, t);
+    if constexpr (Full) {
+#pragma unroll
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 1, false>(sm + i * kPad, w, t);
+    } else {
+      for (int i = 0; i < np; ++i) mid_plane_r<RES, 1, false>(sm + i * kPad, w, t);
     }
   }
   __syncthreads();
