@@ -29,6 +29,7 @@ struct ResidueTables {
   const uint32_t *fw, *fw_sh;   // psi^brv(k), Shoup companions (forward)
   const uint32_t *iw, *iw_sh;   // psi^-brv(k), Shoup companions (inverse)
   const uint2 *fwt, *iwt;       // the same, interleaved (w, w_sh) pairs
+  const uint2 *pwt;             // (psi^m, Shoup companion) for m < 2N
   uint32_t q;
   uint32_t n_inv, n_inv_sh;
   uint32_t w1_ninv, w1_ninv_sh; // iw[1] * N^-1 (last inverse stage)

@@ -222,16 +222,90 @@ k_db_preprocess(DevParams P, const uint16_t *__restrict__ coeffs,
 // ciphertext (bv_keyswitch.cpp:296-367) then the two children
 // (server.cpp:794-809): left = c + c', right = (c - c') X^-k.
 // sigma_k is applied as a gather: sigma(c)[j] = +-c[j k^-1 mod 2N].
-template <int RES, class G>
+// Children of the last level in NTT form (the first-dimension leaves), from
+// the key switch's sums still in NTT form: with NTT slot i holding the value
+// at psi^e_i, e_i = 2 brev(i) + 1 (the reference's bit-reversed order),
+// sigma_g(c)^[i] = c^[j] for e_j = e_i g mod 2N, and (f X^-k)^[i] =
+// psi^(-k e_i) f^[i]. So left = c^ + sigma(c0)^ + delta^ and right =
+// (c^ - sigma(c0)^ - delta^) psi^(-k e), the same values fst_ntt would
+// compute from the coefficient-form children, with the two inverse NTTs of
+// the key switch replaced by forward NTTs of the parent (c0, c1).
+template <int RES>
+__device__ __forceinline__ void expand_tail_ntt(const ResidueTables &T, uint32_t galois,
+                                                uint32_t kshift, const uint32_t *ct,
+                                                const uint32_t (&vb)[8], const uint32_t (&va)[8],
+                                                uint32_t *sm, uint32_t *out, uint64_t out_stride,
+                                                uint32_t node) {
+  constexpr uint32_t q = Res<RES>::q;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = ct[(p * 2 + RES) * kN + posA(tid, k)];
+    fA<RES>(v);
+    st_plane<0>(sm + p * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid_r<RES>(sm, 2, T.fwt);
+  uint32_t h0[8], h1[8];
+  {
+    uint2 wd[6];
+    fload_d(wd, T.fwt, tid);
+    ld_plane<3>(sm, h0, tid);
+    ld_plane<3>(sm + kPad, h1, tid);
+    fD<RES>(h0, wd);
+    fD<RES>(h1, wd);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    h0[k] = canon8<RES>(h0[k]);
+    h1[k] = canon8<RES>(h1[k]);
+  }
+  st_plane<3>(sm + 2 * kPad, h0, tid);  // c0^ by slot, for the sigma gather
+  __syncthreads();
+  // children, four coefficients (one uint4 per polynomial) at a time
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint32_t l0[4], l1[4], r0[4], r1[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int k = 4 * h + c;
+      const uint32_t i = posD(tid, k);
+      const uint32_t e = 2 * (__brev(i) >> 21) + 1;  // 11-bit reversal (N = 2048)
+      const uint32_t j = __brev(((e * galois) & (2 * kN - 1)) >> 1) >> 21;
+      const uint32_t n0v = add_mod(sm[2 * kPad + padi(j)], vb[k], q);
+      const uint32_t n1v = va[k];
+      l0[c] = add_mod(h0[k], n0v, q);
+      l1[c] = add_mod(h1[k], n1v, q);
+      const uint2 lam = __ldg(T.pwt + ((2 * kN - ((kshift * e) & (2 * kN - 1))) & (2 * kN - 1)));
+      const uint32_t d0 = sub_mod(h0[k], n0v, q), d1 = sub_mod(h1[k], n1v, q);
+      const uint32_t t0 = d0 * lam.x - __umulhi(d0, lam.y) * q;
+      const uint32_t t1 = d1 * lam.x - __umulhi(d1, lam.y) * q;
+      r0[c] = min(t0, t0 - q);
+      r1[c] = min(t1, t1 - q);
+    }
+    const int j0 = 4 * (tid + 256 * h);
+    uint32_t *outL = out + ((uint64_t)blockIdx.z * out_stride + 2 * (uint64_t)node) * kCtWords;
+    uint32_t *outR = outL + kCtWords;
+    *reinterpret_cast<uint4 *>(outL + RES * kN + j0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+    *reinterpret_cast<uint4 *>(outL + 2 * kN + RES * kN + j0) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+    *reinterpret_cast<uint4 *>(outR + RES * kN + j0) = make_uint4(r0[0], r0[1], r0[2], r0[3]);
+    *reinterpret_cast<uint4 *>(outR + 2 * kN + RES * kN + j0) = make_uint4(r1[0], r1[1], r1[2], r1[3]);
+  }
+}
+
+template <int RES, class G, bool NTT_OUT = false>
 __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t galois_inv,
                                                   uint32_t kshift, int base_ks, int l_ks,
                                                   const uint32_t *in, uint64_t in_stride,
                                                   uint32_t *out, uint64_t out_stride,
                                                   const uint32_t *const *bv_keys,
-                                                  uint64_t bv_level_off) {
+                                                  uint64_t bv_level_off, uint32_t galois = 0,
+                                                  uint32_t node0 = 0) {
   extern __shared__ uint32_t sm[];
   constexpr uint32_t q = Res<RES>::q;
-  const int node = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
+  const int node = node0 + blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
   const ResidueTables &T = P.r[RES];
   const uint32_t *ct = in + ((uint64_t)b * in_stride + node) * kCtWords;
   const uint32_t *c0 = ct + RES * kN;
@@ -291,6 +365,18 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
     }
   }
   __syncthreads();
+  if constexpr (NTT_OUT) {
+    uint32_t vb[8], va[8];  // the key switch's delta in NTT form, canonical
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      vb[k] = red64<RES>(ab[k]);
+      va[k] = red64<RES>(aa[k]);
+    }
+    expand_tail_ntt<RES>(T, galois, kshift, ct, vb, va, sm, out, out_stride, node);
+    return;
+  }
+  uint32_t *outL = out + ((uint64_t)b * out_stride + 2 * (uint64_t)node) * kCtWords;
+  uint32_t *outR = outL + kCtWords;
   {
     uint2 wd[6];
     iload_d(wd, T.iwt, tid);
@@ -309,8 +395,6 @@ __device__ __forceinline__ void expand_level_body(const DevParams &P, uint32_t g
   ld_plane<0>(sm + kPad, da, tid);
   iA<RES>(db_);
   iA<RES>(da);
-  uint32_t *outL = out + ((uint64_t)b * out_stride + 2 * (uint64_t)node) * kCtWords;
-  uint32_t *outR = outL + kCtWords;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int j = posA(tid, k);
@@ -333,13 +417,32 @@ __global__ void __launch_bounds__(kThreads, 2)
 k_expand_level(DevParams P, uint32_t galois_inv, uint32_t kshift, int base_ks, int l_ks,
                const uint32_t *__restrict__ in, uint64_t in_stride,
                uint32_t *__restrict__ out, uint64_t out_stride,
-               const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+               const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off,
+               uint32_t node0) {
   if (blockIdx.y == 0)
     expand_level_body<0, G>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
-                            bv_keys, bv_level_off);
+                            bv_keys, bv_level_off, 0, node0);
   else
     expand_level_body<1, G>(P, galois_inv, kshift, base_ks, l_ks, in, in_stride, out, out_stride,
-                            bv_keys, bv_level_off);
+                            bv_keys, bv_level_off, 0, node0);
+}
+
+// The last expansion level's nodes below ntt_nodes when the
+// first-dimension leaves are wanted in NTT form: their children (leaves
+// < n0) are written in NTT form (expand_tail_ntt); k_expand_level takes the
+// remaining nodes.
+template <class G>
+__global__ void __launch_bounds__(kThreads, 2)
+k_expand_level_ntt(DevParams P, uint32_t galois, uint32_t galois_inv, uint32_t kshift,
+                   const uint32_t *__restrict__ in, uint64_t in_stride,
+                   uint32_t *__restrict__ out, uint64_t out_stride,
+                   const uint32_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  if (blockIdx.y == 0)
+    expand_level_body<0, G, true>(P, galois_inv, kshift, 0, 0, in, in_stride, out, out_stride,
+                                  bv_keys, bv_level_off, galois);
+  else
+    expand_level_body<1, G, true>(P, galois_inv, kshift, 0, 0, in, in_stride, out, out_stride,
+                                  bv_keys, bv_level_off, galois);
 }
 
 // Expansion level, cluster split: a level with fewer nodes than the GPU
@@ -1336,14 +1439,30 @@ template <class G>
 static void expand_level_impl(const DevParams &P, const Shape &s, uint32_t d, const uint32_t *in,
                               uint64_t in_stride, uint32_t *out, uint64_t out_stride,
                               const uint32_t *const *bv_keys, uint64_t bv_level_stride,
-                              uint32_t batch, cudaStream_t st) {
+                              uint32_t batch, cudaStream_t st, uint32_t ntt_nodes) {
   const uint32_t nodes = expand_nodes(s, d);
   const size_t smem = s.l_ks * kPad * sizeof(uint32_t);
-  set_smem(k_expand_level<G>, smem);
   const uint32_t k = 1u << d;
   const uint32_t galois = kN / k + 1;
   uint32_t galois_inv = 1;  // galois^-1 mod 2N (galois is odd)
   while (((galois_inv * galois) & (2 * kN - 1)) != 1) galois_inv += 2;
+  if (ntt_nodes > 0) {
+    if (d + 1 != s.h || ntt_nodes > nodes || G::lks < 3)  // NTT tail uses planes 0..2
+      throw std::invalid_argument("NTT-form children only at the last expansion level");
+    set_smem(k_expand_level_ntt<G>, smem);
+    k_expand_level_ntt<G><<<dim3(ntt_nodes, 2, batch), kThreads, smem, st>>>(
+        P, galois, galois_inv, k, in, in_stride, out, out_stride, bv_keys, d * bv_level_stride);
+    check_launch("k_expand_level_ntt");
+    if (ntt_nodes < nodes) {
+      set_smem(k_expand_level<G>, smem);
+      k_expand_level<G><<<dim3(nodes - ntt_nodes, 2, batch), kThreads, smem, st>>>(
+          P, galois_inv, k, s.base_ks, s.l_ks, in, in_stride, out, out_stride, bv_keys,
+          d * bv_level_stride, ntt_nodes);
+      check_launch("k_expand_level");
+    }
+    return;
+  }
+  set_smem(k_expand_level<G>, smem);
   // levels with fewer nodes than CTA slots (2 per SM) split each key switch
   // over a cluster of 2, 4 or 8 CTAs (k_expand_level_split)
   const uint64_t ctas = 2ull * nodes * batch, slots = 2ull * sm_count();
@@ -1358,7 +1477,7 @@ static void expand_level_impl(const DevParams &P, const Shape &s, uint32_t d, co
     dim3 grid(nodes, 2, batch);
     k_expand_level<G><<<grid, kThreads, smem, st>>>(P, galois_inv, k, s.base_ks, s.l_ks, in,
                                                      in_stride, out, out_stride, bv_keys,
-                                                     d * bv_level_stride);
+                                                     d * bv_level_stride, 0u);
     check_launch("k_expand_level");
     return;
   }
@@ -1400,14 +1519,14 @@ static void expand_level_impl(const DevParams &P, const Shape &s, uint32_t d, co
 void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d, const uint32_t *in,
                          uint64_t in_stride, uint32_t *out, uint64_t out_stride,
                          const uint32_t *const *bv_keys, uint64_t bv_level_stride,
-                         uint32_t batch, cudaStream_t st) {
+                         uint32_t batch, cudaStream_t st, uint32_t ntt_nodes) {
   check_gadgets(s);
   if (s.gadget == 1)
     expand_level_impl<GadgetsK2Mp>(P, s, d, in, in_stride, out, out_stride, bv_keys,
-                                   bv_level_stride, batch, st);
+                                   bv_level_stride, batch, st, ntt_nodes);
   else
     expand_level_impl<GadgetsK1Comp>(P, s, d, in, in_stride, out, out_stride, bv_keys,
-                                     bv_level_stride, batch, st);
+                                     bv_level_stride, batch, st, ntt_nodes);
 }
 
 template <class G>
@@ -1464,6 +1583,11 @@ void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
   dim3 grid((s.n0 + kFstTile - 1) / kFstTile, 2, batch);
   k_fst_ntt<<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, ntt, ntt_stride);
   check_launch("k_fst_ntt");
+  launch_fst_pack(s, ntt, ntt_stride, qb, batch, st);
+}
+
+void launch_fst_pack(const Shape &s, const uint32_t *ntt, uint64_t ntt_stride, uint8_t *qb,
+                     uint32_t batch, cudaStream_t st) {
   dim3 pgrid((s.n0p + kPackK - 1) / kPackK, 2 * kN / kPackZ, 2 * batch);
   k_fst_pack<<<pgrid, kThreads, 0, st>>>(ntt, ntt_stride, s.n0, s.n0p, qb, 2 * batch);
   check_launch("k_fst_pack");

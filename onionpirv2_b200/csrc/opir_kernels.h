@@ -62,10 +62,14 @@ void launch_db_preprocess(const DevParams &P, const Shape &s, const uint16_t *co
 // One expansion level d over `batch` queries. in: batch x in_stride cts,
 // out: batch x out_stride cts. bv_level[b] points at the (galois level d) key
 // block of query b: L_KS x [b|a] x 2 residues x N u32, NTT form.
+// ntt_nodes > 0 (the last level only): the children of nodes below ntt_nodes
+// are written in NTT form (canonical, the layout k_fst_ntt writes), the
+// others in coefficient form; the level then runs one CTA per key switch.
 void launch_expand_level(const DevParams &P, const Shape &s, uint32_t d,
                          const uint32_t *in, uint64_t in_stride, uint32_t *out,
                          uint64_t out_stride, const uint32_t *const *bv_keys,
-                         uint64_t bv_level_stride, uint32_t batch, cudaStream_t st);
+                         uint64_t bv_level_stride, uint32_t batch, cudaStream_t st,
+                         uint32_t ntt_nodes = 0);
 
 // Selector completion (src/server.cpp:823-855, src/gsw.cpp:317-357).
 // leaves: batch x leaf_stride cts; gsw[b]: 2 L_KEY rows x 2 polys x 2 res x N;
@@ -88,6 +92,10 @@ void upload_ntt_constants(const uint32_t q[2], const uint32_t *const fw[2],
 // qb[((res N + level) 4 + plane) 2 batch + column][n0p], column = 2 b + poly.
 void launch_fst_prep(const DevParams &P, const Shape &s, const uint32_t *leaves,
                      uint64_t leaf_stride, uint32_t *ntt, uint64_t ntt_stride, uint8_t *qb,
+                     uint32_t batch, cudaStream_t st);
+// The byte-plane transpose alone, for leaves already in NTT form (the last
+// expansion level's NTT-form children).
+void launch_fst_pack(const Shape &s, const uint32_t *ntt, uint64_t ntt_stride, uint8_t *qb,
                      uint32_t batch, cudaStream_t st);
 
 // First-dimension scan on CUDA cores (matrix.cpp:240-350): per residue and

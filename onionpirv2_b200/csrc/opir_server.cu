@@ -273,11 +273,25 @@ void setup_device_params(opir_server *s) {
   const auto t1 = opir::make_limb_tables(kN, static_cast<uint32_t>(p.q1), static_cast<uint32_t>(p.w1));
   const auto t2 = opir::make_limb_tables(kN, static_cast<uint32_t>(p.q2), static_cast<uint32_t>(p.w2));
   // per residue: fw, fw_sh, iw, iw_sh (kN each), then (fw, fw_sh) and
-  // (iw, iw_sh) interleaved (2 kN each)
-  std::vector<uint32_t> host(16 * kN);
+  // (iw, iw_sh) interleaved (2 kN each), then (psi^m, Shoup) for m < 2N
+  // (4 kN)
+  constexpr int kResWords = 12 * kN;
+  std::vector<uint32_t> host(2 * kResWords);
   const opir::LimbTables *ts[2] = {&t1, &t2};
   for (int r = 0; r < 2; ++r) {
-    uint32_t *h = host.data() + r * 8 * kN;
+    uint32_t *h = host.data() + r * kResWords;
+    {
+      // psi = fw[brev(1)] = fw[N / 2] (fw[k] = psi^brev(k))
+      const uint64_t q = ts[r]->q, psi = ts[r]->fw[kN / 2];
+      uint64_t pw = 1;
+      for (int m = 0; m < 2 * kN; ++m) {
+        h[8 * kN + 2 * m] = static_cast<uint32_t>(pw);
+        h[8 * kN + 2 * m + 1] = static_cast<uint32_t>((pw << 32) / q);
+        pw = pw * psi % q;
+      }
+      if (pw != 1 || h[8 * kN + 2 * kN] != q - 1)
+        throw std::runtime_error("psi is not a primitive 2N-th root of unity");
+    }
     std::copy(ts[r]->fw.begin(), ts[r]->fw.end(), h + 0 * kN);
     std::copy(ts[r]->fw_sh.begin(), ts[r]->fw_sh.end(), h + 1 * kN);
     std::copy(ts[r]->iw.begin(), ts[r]->iw.end(), h + 2 * kN);
@@ -293,13 +307,14 @@ void setup_device_params(opir_server *s) {
   ck(cudaMemcpy(s->tables.p, host.data(), host.size() * 4, cudaMemcpyHostToDevice), "tables");
   opir::DevParams &d = s->dp;
   for (int r = 0; r < 2; ++r) {
-    uint32_t *base = s->tables.p + r * 8 * kN;
+    uint32_t *base = s->tables.p + r * kResWords;
     d.r[r].fw = base + 0 * kN;
     d.r[r].fw_sh = base + 1 * kN;
     d.r[r].iw = base + 2 * kN;
     d.r[r].iw_sh = base + 3 * kN;
     d.r[r].fwt = reinterpret_cast<const uint2 *>(base + 4 * kN);
     d.r[r].iwt = reinterpret_cast<const uint2 *>(base + 6 * kN);
+    d.r[r].pwt = reinterpret_cast<const uint2 *>(base + 8 * kN);
     d.r[r].q = ts[r]->q;
     d.r[r].n_inv = ts[r]->n_inv;
     d.r[r].n_inv_sh = ts[r]->n_inv_sh;
@@ -455,12 +470,27 @@ opir::Shape level_shape(const opir_server *s, uint32_t n) {
   return sh;
 }
 
-uint32_t *run_expand(opir_server *s, uint32_t n) {
+// OPIR_NTT_LEAVES=0 keeps every leaf in coefficient form (the first
+// dimension then runs its own forward NTT of the leaves).
+bool ntt_leaves_allowed() {
+  const char *e = std::getenv("OPIR_NTT_LEAVES");
+  return !(e && e[0] == '0');
+}
+
+// When ntt_first is given and the layout allows it (an even first dimension
+// under at least one expansion level), the last level writes the first n0
+// leaves in NTT form and *ntt_first is set; the other leaves stay in
+// coefficient form.
+uint32_t *run_expand(opir_server *s, uint32_t n, bool *ntt_first = nullptr) {
   const opir::Shape sh = level_shape(s, n);
   const uint64_t bv_level_stride = static_cast<uint64_t>(sh.l_ks) * 4 * kN;
+  const bool ntt = ntt_first && ntt_leaves_allowed() && sh.h >= 1 && sh.n0 % 2 == 0 &&
+                   sh.n0 / 2 <= opir::expand_nodes(sh, sh.h - 1);
   for (uint32_t d = 0; d < sh.h; ++d)
     opir::launch_expand_level(s->dp, sh, d, s->lvl[d & 1].p, s->lvl_slots, s->lvl[(d + 1) & 1].p,
-                              s->lvl_slots, s->keyptrs.p, bv_level_stride, n, s->stream);
+                              s->lvl_slots, s->keyptrs.p, bv_level_stride, n, s->stream,
+                              ntt && d + 1 == sh.h ? sh.n0 / 2 : 0);
+  if (ntt_first) *ntt_first = ntt;
   return s->lvl[sh.h & 1].p;
 }
 
@@ -530,12 +560,18 @@ void launch_scan_any(opir_server *s, uint32_t n) {
   launch_scan_tc_tile(s, n, effective_tile(s, n));
 }
 
-// First dimension: NTT + transpose of the first n0 leaves, scan, gather + INTT.
-void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n) {
+// First dimension: NTT + transpose of the first n0 leaves (the transpose
+// alone when the leaves are already in NTT form), scan, gather + INTT.
+void run_first_dim(opir_server *s, const uint32_t *leaves, uint32_t n, bool leaves_ntt = false) {
   const opir::Shape &sh = s->shape;
-  // the NTT-form leaves go to whichever expansion buffer does not hold them
-  uint32_t *ntt = leaves == s->lvl[0].p ? s->lvl[1].p : s->lvl[0].p;
-  opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, ntt, s->lvl_slots, s->qb.p, n, s->stream);
+  if (leaves_ntt) {
+    opir::launch_fst_pack(sh, leaves, s->lvl_slots, s->qb.p, n, s->stream);
+  } else {
+    // the NTT-form leaves go to whichever expansion buffer does not hold them
+    uint32_t *ntt = leaves == s->lvl[0].p ? s->lvl[1].p : s->lvl[0].p;
+    opir::launch_fst_prep(s->dp, sh, leaves, s->lvl_slots, ntt, s->lvl_slots, s->qb.p, n,
+                          s->stream);
+  }
   mark(s, kStages + 1);
   launch_scan_any(s, n);
   mark(s, kStages + 2);
@@ -562,11 +598,12 @@ void enqueue_core(opir_server *s, uint32_t n, const uint64_t *d_queries, uint64_
   const opir::Shape &sh = s->shape;
   mark(s, 0);
   opir::launch_split_u64(s->dp, d_queries, s->lvl[0].p, n, 2, s->lvl_slots * kCtWords, s->stream);
-  const uint32_t *leaves = run_expand(s, n);
+  bool leaves_ntt = false;
+  const uint32_t *leaves = run_expand(s, n, &leaves_ntt);
   mark(s, 1);
   opir::launch_selectors(s->dp, sh, leaves, s->lvl_slots, s->keyptrs.p + n, s->sel.p, n, s->stream);
   mark(s, 2);
-  run_first_dim(s, leaves, n);
+  run_first_dim(s, leaves, n, leaves_ntt);
   mark(s, 3);
   const uint32_t *res = run_other_dims(s, n);
   mark(s, 4);

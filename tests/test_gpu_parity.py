@@ -283,3 +283,28 @@ def test_stream_priority_leaves_results_unchanged():
     for prio in (-1, 0, -100):
         srv.set_priority(prio)
         _check_response(c, cl, op, srv.make_query(7, q))
+
+
+@pytest.mark.parametrize("name", SMALL + LARGE[:1])
+def test_ntt_form_leaves_match_coefficient_leaves(name, monkeypatch):
+    """The make_query pipeline's last expansion level writes the
+    first-dimension leaves in NTT form (sigma and X^-k applied in the NTT
+    domain); with OPIR_NTT_LEAVES=0 every leaf stays in coefficient form and
+    the first dimension runs its own forward NTT. Both give the golden
+    response, single and batched (eager, captured, replayed)."""
+    c, op, cl, bv, gsw, q, gp, _ = setup(name)
+    qs = np.stack([q, q, q])
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("OPIR_NTT_LEAVES", flag)
+        with PirServer(gp) as srv:
+            srv.load_data_seeded(c["target_num_pt"], c["db_seed"])
+            srv.set_client_keys(7, bv, gsw)
+            for _ in range(3):
+                r = srv.make_query(7, q)
+                _check_response(c, cl, op, r)
+            out[flag] = [srv.make_query_batch([7, 7, 7], qs) for _ in range(3)]
+    for a, b in zip(out["1"], out["0"]):
+        for ra, rb in zip(a, b):
+            assert np.array_equal(ra, rb)
+            assert G.sha256(ra) == c["sha256_response_u64"]
