@@ -241,14 +241,85 @@ k4_db_preprocess(Dev4 P, const uint64_t *__restrict__ coeffs, uint64_t coeff_pt_
 // so eight rows sum below 16q in 64 bits.
 constexpr int kExpGroup = 4;  // digit planes per group
 
+// Children of the last level in NTT form (the first-dimension leaves), from
+// the key switch's sums still in NTT form: with NTT slot i holding the value
+// at psi^e_i, e_i = 2 brev(i) + 1 (the reference's bit-reversed order),
+// sigma_g(c)^[i] = c^[j] for e_j = e_i g mod 2N, and (f X^-k)^[i] =
+// psi^(-k e_i) f^[i]. So left = c^ + sigma(c0)^ + delta^ and right =
+// (c^ - sigma(c0)^ - delta^) psi^(-k e), the values k4_fst_ntt would compute
+// from the coefficient-form children; the key switch's two inverse NTTs are
+// replaced by forward NTTs of the parent's c0 and c1 (this limb).
 template <int L>
+__device__ __forceinline__ void expand_tail_ntt(const Dev4 &P, uint32_t galois, uint32_t kshift,
+                                                const uint64_t *ct, const uint64_t (&vb)[8],
+                                                const uint64_t (&va)[8], uint64_t *outL,
+                                                uint64_t *outR) {
+  extern __shared__ uint64_t sm4[];
+  constexpr uint64_t Q = Limb<L>::q;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    uint64_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = ct[p * 2 * kN + L * kN + posA(tid, k)];
+    fA<L>(v);
+    st_plane<0>(sm4 + p * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid<L>(sm4, 2, P.T);
+  uint64_t h0[8], h1[8];
+  {
+    ulonglong2 wd[7];
+    fload_d<L>(wd, P.T);
+    ld_plane<3>(sm4, h0, tid);
+    ld_plane<3>(sm4 + kPad, h1, tid);
+    fD<L>(h0, wd);
+    fD<L>(h1, wd);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    h0[k] = canon8<Q>(h0[k]);
+    h1[k] = canon8<Q>(h1[k]);
+  }
+  st_plane<3>(sm4 + 2 * kPad, h0, tid);  // c0^ by slot, for the sigma gather
+  __syncthreads();
+  uint64_t l0[8], l1[8], r0[8], r1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t i = posD(tid, k);
+    const uint32_t e = 2 * (__brev(i) >> 20) + 1;  // 12-bit reversal (N = 4096)
+    const uint32_t j = __brev(((e * galois) & (2 * kN - 1)) >> 1) >> 20;
+    const uint64_t n0v = add_mod<Q>(sm4[2 * kPad + pad(j)], vb[k]), n1v = va[k];
+    l0[k] = add_mod<Q>(h0[k], n0v);
+    l1[k] = add_mod<Q>(h1[k], n1v);
+    const ulonglong2 lam =
+        __ldg(P.T.pwt[L] + ((2 * kN - ((kshift * e) & (2 * kN - 1))) & (2 * kN - 1)));
+    const uint64_t t0 = mul_shoup<Q>(sub_mod<Q>(h0[k], n0v), lam.x, lam.y);
+    const uint64_t t1 = mul_shoup<Q>(sub_mod<Q>(h1[k], n1v), lam.x, lam.y);
+    r0[k] = min(t0, t0 - Q);
+    r1[k] = min(t1, t1 - Q);
+  }
+  const int j0 = posD(tid, 0);  // eight consecutive slots
+#pragma unroll
+  for (int c = 0; c < 8; c += 2) {
+    *reinterpret_cast<ulonglong2 *>(outL + L * kN + j0 + c) = make_ulonglong2(l0[c], l0[c + 1]);
+    *reinterpret_cast<ulonglong2 *>(outL + 2 * kN + L * kN + j0 + c) =
+        make_ulonglong2(l1[c], l1[c + 1]);
+    *reinterpret_cast<ulonglong2 *>(outR + L * kN + j0 + c) = make_ulonglong2(r0[c], r0[c + 1]);
+    *reinterpret_cast<ulonglong2 *>(outR + 2 * kN + L * kN + j0 + c) =
+        make_ulonglong2(r1[c], r1[c + 1]);
+  }
+}
+
+template <int L, bool NTT_OUT = false>
 __device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, uint32_t kshift,
                                             const uint64_t *in, uint64_t in_stride, uint64_t *out,
                                             uint64_t out_stride, const uint64_t *const *bv_keys,
-                                            uint64_t bv_level_off) {
+                                            uint64_t bv_level_off, uint32_t node0 = 0,
+                                            uint32_t galois = 0) {
   extern __shared__ uint64_t sm4[];
   constexpr uint64_t Q = Limb<L>::q;
-  const int node = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
+  const int node = node0 + blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
   const uint64_t *ct = in + (static_cast<uint64_t>(b) * in_stride + node) * kCtWords;
   const uint64_t *key = bv_keys[b] + bv_level_off;  // [row][b][a][b'][a']
   uint64_t ab[8], aa[8];
@@ -307,6 +378,20 @@ __device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, 
     }
     __syncthreads();
   }
+  uint64_t *outL = out + (static_cast<uint64_t>(b) * out_stride + 2ull * node) * kCtWords;
+  uint64_t *outR = outL + kCtWords;
+  if constexpr (NTT_OUT) {
+    uint64_t vb[8], va[8];  // the key switch's delta in NTT form, canonical
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      vb[k] = fold16<Q>(ab[k]);
+      vb[k] = min(vb[k], vb[k] - Q);
+      va[k] = fold16<Q>(aa[k]);
+      va[k] = min(va[k], va[k] - Q);
+    }
+    expand_tail_ntt<L>(P, galois, kshift, ct, vb, va, outL, outR);
+    return;
+  }
   {
     ulonglong2 wd[7];
     iload_d<L>(wd, P.T);
@@ -325,8 +410,6 @@ __device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, 
   ld_plane<0>(sm4 + kPad, da, tid);
   iA<L>(db_);
   iA<L>(da);
-  uint64_t *outL = out + (static_cast<uint64_t>(b) * out_stride + 2ull * node) * kCtWords;
-  uint64_t *outR = outL + kCtWords;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const uint32_t j = posA(tid, k);
@@ -349,11 +432,29 @@ __device__ __forceinline__ void expand_body(const Dev4 &P, uint32_t galois_inv, 
 __global__ void __launch_bounds__(kThreads, 1)
 k4_expand_level(Dev4 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *__restrict__ in,
                 uint64_t in_stride, uint64_t *__restrict__ out, uint64_t out_stride,
-                const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+                const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off,
+                uint32_t node0) {
   if (blockIdx.y == 0)
-    expand_body<0>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off);
+    expand_body<0>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off,
+                   node0);
   else
-    expand_body<1>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off);
+    expand_body<1>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys, bv_level_off,
+                   node0);
+}
+
+// The last level's nodes below ntt_nodes when the first-dimension leaves are
+// wanted in NTT form (expand_tail_ntt); k4_expand_level takes the others.
+__global__ void __launch_bounds__(kThreads, 1)
+k4_expand_level_ntt(Dev4 P, uint32_t galois, uint32_t galois_inv, uint32_t kshift,
+                    const uint64_t *__restrict__ in, uint64_t in_stride,
+                    uint64_t *__restrict__ out, uint64_t out_stride,
+                    const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  if (blockIdx.y == 0)
+    expand_body<0, true>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                         bv_level_off, 0, galois);
+  else
+    expand_body<1, true>(P, galois_inv, kshift, in, in_stride, out, out_stride, bv_keys,
+                         bv_level_off, 0, galois);
 }
 
 // Expansion level, cluster split: with fewer nodes than SMs (the top of the
@@ -710,18 +811,22 @@ k4_fst_ntt(Dev4 P, Shape4 S, const uint64_t *__restrict__ leaves, uint64_t leaf_
 // run reads (8 runs x 4 z) touch every bank pair at most twice.
 constexpr int kPackZ = 32, kPackK = 128, kRunPitch = 18, kRowPitch = 145;
 __global__ void __launch_bounds__(256)
-k4_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t ncols,
+k4_fst_pack(const uint64_t *__restrict__ qm, uint64_t q_stride, uint64_t p_stride,
+            uint64_t k_stride, uint32_t n0, uint32_t n0p, uint32_t ncols,
             uint8_t *__restrict__ qb) {
   __shared__ uint64_t tile[(kPackZ - 1) * kRowPitch + (kPackK / 16 - 1) * kRunPitch + 16];
   const uint32_t z0 = blockIdx.x * kPackZ, col = blockIdx.y, k0 = blockIdx.z * kPackK;
   const int t = threadIdx.x;
-  const uint64_t *src = qm + static_cast<uint64_t>(col) * n0 * (2 * kN) + z0;
+  // column col = 2 query + poly: qm (q_stride = 2 p_stride, p_stride = n0 2N,
+  // k_stride = 2N) or NTT-form leaves (q_stride = slots 4N, p_stride = 2N,
+  // k_stride = 4N)
+  const uint64_t *src = qm + (col >> 1) * q_stride + (col & 1) * p_stride + z0;
 #pragma unroll 4
   for (int i = t; i < kPackK * kPackZ; i += 256) {
     const int kk = i / kPackZ, zz = i % kPackZ;
     const uint32_t k = k0 + kk;
     tile[zz * kRowPitch + (kk / 16) * kRunPitch + kk % 16] =
-        k < n0 ? src[static_cast<uint64_t>(k) * (2 * kN) + zz] : 0;
+        k < n0 ? src[static_cast<uint64_t>(k) * k_stride + zz] : 0;
   }
   __syncthreads();
   const int chunk = t % (kPackK / 16), zz = t / (kPackK / 16);
@@ -1123,7 +1228,7 @@ uint32_t expand_nodes(const Shape4 &s, uint32_t d) {
 void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint64_t *in,
                          uint64_t in_stride, uint64_t *out, uint64_t out_stride,
                          const uint64_t *const *bv_keys, uint64_t bv_level_stride, uint32_t batch,
-                         cudaStream_t st) {
+                         cudaStream_t st, uint32_t ntt_nodes) {
   const uint32_t nodes = expand_nodes(s, d);
   if (nodes == 0) return;
   const size_t smem = plane_bytes(kExpGroup);
@@ -1137,6 +1242,21 @@ void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint6
   // nodes of level d are heap slots k .. k + nodes - 1, stored from slot 0;
   // children of node i go to slots 2 i, 2 i + 1 of the next buffer
   const uint64_t koff = static_cast<uint64_t>(d) * bv_level_stride;
+  if (ntt_nodes > 0) {  // NTT tail: planes 0..2 of the kExpGroup-plane area
+    static_assert(kExpGroup >= 3, "the NTT-form tail uses three planes");
+    if (d + 1 != s.h || ntt_nodes > nodes)
+      throw std::invalid_argument("NTT-form children only at the last expansion level");
+    set_smem(k4_expand_level_ntt, smem);
+    k4_expand_level_ntt<<<dim3(ntt_nodes, 2, batch), kThreads, smem, st>>>(
+        P, galois, inv, k, in, in_stride, out, out_stride, bv_keys, koff);
+    check_launch("k4_expand_level_ntt");
+    if (ntt_nodes < nodes) {
+      k4_expand_level<<<dim3(nodes - ntt_nodes, 2, batch), kThreads, smem, st>>>(
+          P, inv, k, in, in_stride, out, out_stride, bv_keys, koff, ntt_nodes);
+      check_launch("k4_expand_level");
+    }
+    return;
+  }
   // fewer nodes than SMs (one CTA each): a cluster of 2, 4 or 8 CTAs per node
   const uint64_t ctas = 2ull * nodes * batch, slots = sm_count();
   const int split = !split_enabled() ? 1
@@ -1144,7 +1264,7 @@ void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint6
   if (split == 1) {
     dim3 grid(nodes, 2, batch);
     k4_expand_level<<<grid, kThreads, smem, st>>>(P, inv, k, in, in_stride, out, out_stride,
-                                                   bv_keys, koff);
+                                                   bv_keys, koff, 0u);
     check_launch("k4_expand_level");
     return;
   }
@@ -1188,7 +1308,17 @@ void launch_fst_pack(const Shape4 &s, const uint64_t *qm, uint8_t *qb, uint32_t 
                      cudaStream_t st) {
   const uint32_t ncols = 2 * batch;
   const dim3 grid(2 * kN / kPackZ, ncols, (s.n0p + kPackK - 1) / kPackK);
-  k4_fst_pack<<<grid, 256, 0, st>>>(qm, s.n0, s.n0p, ncols, qb);
+  const uint64_t p_stride = static_cast<uint64_t>(s.n0) * 2 * kN;
+  k4_fst_pack<<<grid, 256, 0, st>>>(qm, 2 * p_stride, p_stride, 2 * kN, s.n0, s.n0p, ncols, qb);
+  check_launch("k4_fst_pack");
+}
+
+void launch_fst_pack_leaves(const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                            uint8_t *qb, uint32_t batch, cudaStream_t st) {
+  const uint32_t ncols = 2 * batch;
+  const dim3 grid(2 * kN / kPackZ, ncols, (s.n0p + kPackK - 1) / kPackK);
+  k4_fst_pack<<<grid, 256, 0, st>>>(leaves, leaf_stride * kCtWords, 2 * kN, kCtWords, s.n0, s.n0p,
+                                     ncols, qb);
   check_launch("k4_fst_pack");
 }
 

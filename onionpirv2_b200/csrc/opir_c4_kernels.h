@@ -34,6 +34,7 @@ constexpr int kRowWords = 8 * kN; // a key / RGSW row: ciphertext + Shoup compan
 // Full twiddle tables in global memory, (w, floor(w 2^64 / q)) pairs per limb
 struct Tables {
   const ulonglong2 *fwt[2], *iwt[2];
+  const ulonglong2 *pwt[2];  // (psi^m, floor(psi^m 2^64 / q)) for m < 2N
 };
 
 struct Dev4 {
@@ -72,10 +73,13 @@ void launch_db_preprocess(const Dev4 &P, const Shape4 &s, const uint64_t *coeffs
                           uint8_t *db8, cudaStream_t st);
 // One expansion level for `batch` queries; bv_keys: device array of per-query
 // key pointers.
+// ntt_nodes > 0 (the last level only): the children of nodes below
+// ntt_nodes (the first-dimension leaves) are written in NTT form, canonical,
+// in the ciphertext layout; the other nodes' children in coefficient form.
 void launch_expand_level(const Dev4 &P, const Shape4 &s, uint32_t d, const uint64_t *in,
                          uint64_t in_stride, uint64_t *out, uint64_t out_stride,
                          const uint64_t *const *bv_keys, uint64_t bv_level_stride, uint32_t batch,
-                         cudaStream_t st);
+                         cudaStream_t st, uint32_t ntt_nodes = 0);
 void launch_selectors(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
                       const uint64_t *const *gsw_keys, uint64_t *sel, uint32_t batch,
                       cudaStream_t st);
@@ -83,6 +87,11 @@ void launch_fst_ntt(const Dev4 &P, const Shape4 &s, const uint64_t *leaves, uint
                     uint64_t *qm, uint32_t batch, cudaStream_t st);
 void launch_fst_pack(const Shape4 &s, const uint64_t *qm, uint8_t *qb, uint32_t batch,
                      cudaStream_t st);
+// The same byte planes from NTT-form leaves in the ciphertext layout
+// (leaves: batch x leaf_stride ciphertexts, the last expansion level's
+// NTT-form children).
+void launch_fst_pack_leaves(const Shape4 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                            uint8_t *qb, uint32_t batch, cudaStream_t st);
 void launch_epilogue(const Dev4 &P, const Shape4 &s, const uint64_t *cmat, uint64_t *mid,
                      uint64_t mid_stride, uint32_t batch, cudaStream_t st);
 // One MUX level in a selector tree of height tree_h (num_dims - 1 for a

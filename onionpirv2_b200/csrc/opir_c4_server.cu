@@ -146,6 +146,7 @@ void Server::setup_k1_tables() {
      "twiddle tables");
   dp_.T.fwt[0] = dp_.T.fwt[1] = tables_.p;
   dp_.T.iwt[0] = dp_.T.iwt[1] = tables_.p + n_;
+  dp_.T.pwt[0] = dp_.T.pwt[1] = nullptr;  // CONFIG_N2048_K1 keeps coefficient-form leaves
   const uint64_t ninv[2] = {t.n_inv, t.n_inv_sh}, w1n[2] = {t.w1_ninv, t.w1_ninv_sh};
   opir1::upload_constants(t.fw.data(), t.fw_sh.data(), t.iw.data(), t.iw_sh.data(), ninv, w1n);
 }
@@ -159,19 +160,31 @@ void Server::setup_c4_tables() {
   const opir::LimbTables64 t[2] = {opir::make_limb_tables64(kN, p_.q1, p_.w1),
                                    opir::make_limb_tables64(kN, p_.q2, p_.w2)};
   if (t[0].q != kQ0 || t[1].q != kQ1) throw std::invalid_argument("unexpected RNS limbs");
-  // [limb][forward N][inverse N] (w, Shoup) pairs
-  std::vector<ulonglong2> host(4ull * kN);
-  for (int l = 0; l < 2; ++l)
+  // [limb][forward N][inverse N] (w, Shoup) pairs, then [limb][psi^m, m < 2N]
+  std::vector<ulonglong2> host(8ull * kN);
+  for (int l = 0; l < 2; ++l) {
     for (int i = 0; i < kN; ++i) {
       host[l * 2 * kN + i] = make_ulonglong2(t[l].fw[i], t[l].fw_sh[i]);
       host[l * 2 * kN + kN + i] = make_ulonglong2(t[l].iw[i], t[l].iw_sh[i]);
     }
+    // psi = fw[brev(1)] = fw[N / 2] (fw[k] = psi^brev(k))
+    const uint64_t q = t[l].q, psi = t[l].fw[kN / 2];
+    uint64_t pw = 1;
+    for (int m = 0; m < 2 * kN; ++m) {
+      const uint64_t sh = static_cast<uint64_t>((static_cast<unsigned __int128>(pw) << 64) / q);
+      host[4 * kN + l * 2 * kN + m] = make_ulonglong2(pw, sh);
+      pw = static_cast<uint64_t>(static_cast<unsigned __int128>(pw) * psi % q);
+    }
+    if (pw != 1 || host[4 * kN + l * 2 * kN + kN].x != q - 1)
+      throw std::runtime_error("psi is not a primitive 2N-th root of unity");
+  }
   tables_.alloc(host.size());
   ck(cudaMemcpy(tables_.p, host.data(), host.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice),
      "twiddle tables");
   for (int l = 0; l < 2; ++l) {
     dp_.T.fwt[l] = tables_.p + l * 2 * kN;
     dp_.T.iwt[l] = tables_.p + l * 2 * kN + kN;
+    dp_.T.pwt[l] = tables_.p + 4 * kN + l * 2 * kN;
   }
   const uint64_t *fw[2] = {t[0].fw.data(), t[1].fw.data()};
   const uint64_t *fw_sh[2] = {t[0].fw_sh.data(), t[1].fw_sh.data()};
@@ -427,15 +440,24 @@ void Server::stage_in(const uint64_t *d_queries, uint32_t n) {
                        cudaMemcpyDeviceToDevice, st_), "query staging");
 }
 
-const uint64_t *Server::run_expand(uint32_t n) {
+// When ntt_first is given and the layout allows it (CONFIG_N4096_K2_MP, an
+// even first dimension under at least one expansion level;
+// OPIR_NTT_LEAVES=0 turns it off), the last level writes the first n0
+// leaves in NTT form and *ntt_first is set.
+const uint64_t *Server::run_expand(uint32_t n, bool *ntt_first) {
   const uint64_t level_stride = static_cast<uint64_t>(kLKsRows) * row_;
+  const char *env = std::getenv("OPIR_NTT_LEAVES");
+  const bool ntt = ntt_first && !k1_ && !(env && env[0] == '0') && sh_.h >= 1 &&
+                   sh_.n0 % 2 == 0 && sh_.n0 / 2 <= expand_nodes(sh_, sh_.h - 1);
   for (uint32_t d = 0; d < sh_.h; ++d)
     if (k1_)
       opir1::launch_expand_level(d1(), sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p,
                                  lvl_slots_, keyptrs_.p, level_stride, n, st_);
     else
       launch_expand_level(dp_, sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p, lvl_slots_,
-                          keyptrs_.p, level_stride, n, st_);
+                          keyptrs_.p, level_stride, n, st_,
+                          ntt && d + 1 == sh_.h ? sh_.n0 / 2 : 0);
+  if (ntt_first) *ntt_first = ntt;
   return lvl_[sh_.h & 1].p;
 }
 
@@ -489,12 +511,18 @@ void Server::mark(Events ev, int i) {
     ck(cudaEventRecord(ev[i], st_), "event record");
 }
 
-void Server::run_first_dim(const uint64_t *leaves, uint32_t n, Events ev) {
+void Server::run_first_dim(const uint64_t *leaves, uint32_t n, Events ev, bool leaves_ntt) {
   const int li = leaves == lvl_[0].p ? 0 : 1;
   uint64_t *qm = lvl_[li ^ 1].p;
   uint8_t *qb = reinterpret_cast<uint8_t *>(lvl_[li].p);
   uint64_t *cmat = lvl_[li ^ 1].p;
-  if (k1_) {
+  if (leaves_ntt) {
+    // NTT-form leaves: byte planes into the other buffer (the last
+    // expansion level's input, dead now), the scan's output over the leaves
+    qb = reinterpret_cast<uint8_t *>(lvl_[li ^ 1].p);
+    cmat = lvl_[li].p;
+    launch_fst_pack_leaves(sh_, leaves, lvl_slots_, qb, n, st_);
+  } else if (k1_) {
     opir1::launch_fst_ntt(d1(), sh_, leaves, lvl_slots_, qm, n, st_);
     opir1::launch_fst_pack(sh_, qm, qb, n, st_);
   } else {
@@ -520,11 +548,12 @@ const uint64_t *Server::run_other_dims(uint32_t n) {
 void Server::enqueue_core(uint32_t n, const uint64_t *d_queries, uint64_t *d_resp, Events ev) {
   mark(ev, 0);
   stage_in(d_queries, n);
-  const uint64_t *leaves = run_expand(n);
+  bool leaves_ntt = false;
+  const uint64_t *leaves = run_expand(n, &leaves_ntt);
   mark(ev, 1);
   run_selectors(leaves, keyptrs_.p + n, n);
   mark(ev, 2);
-  run_first_dim(leaves, n, ev);
+  run_first_dim(leaves, n, ev, leaves_ntt);
   mark(ev, 3);
   const uint64_t *res = run_other_dims(n);
   mark(ev, 4);

@@ -121,8 +121,8 @@ class Server {
   void grow_ptr_slots(size_t entries);
   void check_ct_values(const uint64_t *v, size_t cts) const;
   void stage_in(const uint64_t *d_queries, uint32_t n);
-  const uint64_t *run_expand(uint32_t n);
-  void run_first_dim(const uint64_t *leaves, uint32_t n, Events ev);
+  const uint64_t *run_expand(uint32_t n, bool *ntt_first = nullptr);
+  void run_first_dim(const uint64_t *leaves, uint32_t n, Events ev, bool leaves_ntt = false);
   const uint64_t *run_other_dims(uint32_t n);
   void run_pipeline(uint32_t n, const uint64_t *ids, const uint64_t *d_queries,
                     uint64_t *d_resp, Events ev);
