@@ -136,23 +136,36 @@ Server::Server(const opir_params &p, cudaStream_t stream, const opir::RowShard *
 // the one limb, the first 64 of each to constant memory.
 void Server::setup_k1_tables() {
   const opir::LimbTables64 t = opir::make_limb_tables64(n_, p_.q, p_.w1);
-  std::vector<ulonglong2> host(2ull * n_);
+  // [forward N][inverse N] (w, Shoup) pairs, then (psi^m, Shoup) for m < 2N
+  std::vector<ulonglong2> host(4ull * n_);
   for (uint32_t i = 0; i < n_; ++i) {
     host[i] = make_ulonglong2(t.fw[i], t.fw_sh[i]);
     host[n_ + i] = make_ulonglong2(t.iw[i], t.iw_sh[i]);
+  }
+  {
+    // psi = fw[brev(1)] = fw[N / 2] (fw[k] = psi^brev(k))
+    const uint64_t q = t.q, psi = t.fw[n_ / 2];
+    uint64_t pw = 1;
+    for (uint32_t m = 0; m < 2 * n_; ++m) {
+      const uint64_t sh = static_cast<uint64_t>((static_cast<unsigned __int128>(pw) << 64) / q);
+      host[2 * n_ + m] = make_ulonglong2(pw, sh);
+      pw = static_cast<uint64_t>(static_cast<unsigned __int128>(pw) * psi % q);
+    }
+    if (pw != 1 || host[2 * n_ + n_].x != q - 1)
+      throw std::runtime_error("psi is not a primitive 2N-th root of unity");
   }
   tables_.alloc(host.size());
   ck(cudaMemcpy(tables_.p, host.data(), host.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice),
      "twiddle tables");
   dp_.T.fwt[0] = dp_.T.fwt[1] = tables_.p;
   dp_.T.iwt[0] = dp_.T.iwt[1] = tables_.p + n_;
-  dp_.T.pwt[0] = dp_.T.pwt[1] = nullptr;  // CONFIG_N2048_K1 keeps coefficient-form leaves
+  dp_.T.pwt[0] = dp_.T.pwt[1] = tables_.p + 2 * n_;
   const uint64_t ninv[2] = {t.n_inv, t.n_inv_sh}, w1n[2] = {t.w1_ninv, t.w1_ninv_sh};
   opir1::upload_constants(t.fw.data(), t.fw_sh.data(), t.iw.data(), t.iw_sh.data(), ninv, w1n);
 }
 
 opir1::Dev1 Server::d1() const {
-  return opir1::Dev1{dp_.T.fwt[0], dp_.T.iwt[0], dp_.small_q, dp_.small_q_width};
+  return opir1::Dev1{dp_.T.fwt[0], dp_.T.iwt[0], dp_.small_q, dp_.small_q_width, dp_.T.pwt[0]};
 }
 
 // Twiddle tables of CONFIG_N4096_K2_MP: [limb][forward N][inverse N].
@@ -440,19 +453,23 @@ void Server::stage_in(const uint64_t *d_queries, uint32_t n) {
                        cudaMemcpyDeviceToDevice, st_), "query staging");
 }
 
-// When ntt_first is given and the layout allows it (CONFIG_N4096_K2_MP, an
-// even first dimension under at least one expansion level;
+// When ntt_first is given and the batch and layout allow it (two or more
+// queries, an even first dimension under at least one expansion level;
 // OPIR_NTT_LEAVES=0 turns it off), the last level writes the first n0
 // leaves in NTT form and *ntt_first is set.
 const uint64_t *Server::run_expand(uint32_t n, bool *ntt_first) {
   const uint64_t level_stride = static_cast<uint64_t>(kLKsRows) * row_;
   const char *env = std::getenv("OPIR_NTT_LEAVES");
-  const bool ntt = ntt_first && !k1_ && !(env && env[0] == '0') && sh_.h >= 1 &&
+  // a single query keeps the coefficient path: its last level is too
+  // small for the NTT-form tail to pay for itself (CONFIG_N2048_K1 batch 1:
+  // 561 vs 550 q/s)
+  const bool ntt = ntt_first && n >= 2 && !(env && env[0] == '0') && sh_.h >= 1 &&
                    sh_.n0 % 2 == 0 && sh_.n0 / 2 <= expand_nodes(sh_, sh_.h - 1);
   for (uint32_t d = 0; d < sh_.h; ++d)
     if (k1_)
       opir1::launch_expand_level(d1(), sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p,
-                                 lvl_slots_, keyptrs_.p, level_stride, n, st_);
+                                 lvl_slots_, keyptrs_.p, level_stride, n, st_,
+                                 ntt && d + 1 == sh_.h ? sh_.n0 / 2 : 0);
     else
       launch_expand_level(dp_, sh_, d, lvl_[d & 1].p, lvl_slots_, lvl_[(d + 1) & 1].p, lvl_slots_,
                           keyptrs_.p, level_stride, n, st_,
@@ -521,7 +538,8 @@ void Server::run_first_dim(const uint64_t *leaves, uint32_t n, Events ev, bool l
     // expansion level's input, dead now), the scan's output over the leaves
     qb = reinterpret_cast<uint8_t *>(lvl_[li ^ 1].p);
     cmat = lvl_[li].p;
-    launch_fst_pack_leaves(sh_, leaves, lvl_slots_, qb, n, st_);
+    if (k1_) opir1::launch_fst_pack_leaves(sh_, leaves, lvl_slots_, qb, n, st_);
+    else launch_fst_pack_leaves(sh_, leaves, lvl_slots_, qb, n, st_);
   } else if (k1_) {
     opir1::launch_fst_ntt(d1(), sh_, leaves, lvl_slots_, qm, n, st_);
     opir1::launch_fst_pack(sh_, qm, qb, n, st_);

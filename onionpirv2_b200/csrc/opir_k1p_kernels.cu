@@ -59,6 +59,24 @@ void set_smem(K kernel, size_t bytes) {
 
 constexpr size_t plane_bytes(int np) { return static_cast<size_t>(np) * kPad * sizeof(uint64_t); }
 
+// SMs of the current device (cached per device).
+int sms() {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    n = 1;
+  }
+  cache[dev] = n;
+  return n;
+}
+
 // ------------------------------------------------------------ arithmetic
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {  // splitmix64 finaliser
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -406,12 +424,84 @@ k1p_db_preprocess(Dev1 P, const uint64_t *__restrict__ coeffs, uint64_t coeff_pt
 // planes; Shoup key products summed below 2q after each group.
 constexpr int kGroup = 4;
 
-__global__ void __launch_bounds__(kThreads)
-k1p_expand_level(Dev1 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *__restrict__ in,
-                 uint64_t in_stride, uint64_t *__restrict__ out, uint64_t out_stride,
-                 const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+// Children of the last level in NTT form (the first-dimension leaves), from
+// the key switch's sums still in NTT form: with NTT slot i holding the value
+// at psi^e_i, e_i = 2 brev(i) + 1 (the reference's bit-reversed order),
+// sigma_g(c)^[i] = c^[j] for e_j = e_i g mod 2N, and (f X^-k)^[i] =
+// psi^(-k e_i) f^[i]. So left = c^ + sigma(c0)^ + delta^ and right =
+// (c^ - sigma(c0)^ - delta^) psi^(-k e), the values k1p_fst_ntt would
+// compute from the coefficient-form children; the key switch's two inverse
+// NTTs are replaced by forward NTTs of the parent's c0 and c1.
+__device__ __forceinline__ void expand_tail_ntt(const Dev1 &P, uint32_t galois, uint32_t kshift,
+                                                const uint64_t *ct, const uint64_t (&vb)[8],
+                                                const uint64_t (&va)[8], uint64_t *outL,
+                                                uint64_t *outR) {
   extern __shared__ uint64_t sm1[];
-  const int node = blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    uint64_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = ct[p * kN + posA(tid, k)];
+    fA(v);
+    st_plane<0>(sm1 + p * kPad, v, tid);
+  }
+  __syncthreads();
+  fwd_mid(sm1, 2, P.fwt);
+  uint64_t h0[8], h1[8];
+  {
+    ulonglong2 wd[6];
+    load_d(wd, P.fwt, tid);
+    ld_plane<3>(sm1, h0, tid);
+    ld_plane<3>(sm1 + kPad, h1, tid);
+    fD(h0, wd);
+    fD(h1, wd);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    h0[k] = canon8(h0[k]);
+    h1[k] = canon8(h1[k]);
+  }
+  st_plane<3>(sm1 + 2 * kPad, h0, tid);  // c0^ by slot, for the sigma gather
+  __syncthreads();
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint64_t l0[4], l1[4], r0[4], r1[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int k = 4 * h + c;
+      const uint32_t i = posD(tid, k);
+      const uint32_t e = 2 * (__brev(i) >> 21) + 1;  // 11-bit reversal (N = 2048)
+      const uint32_t j = __brev(((e * galois) & (2 * kN - 1)) >> 1) >> 21;
+      const uint64_t n0v = add_q(sm1[2 * kPad + padi(j)], vb[k]), n1v = va[k];
+      l0[c] = add_q(h0[k], n0v);
+      l1[c] = add_q(h1[k], n1v);
+      const ulonglong2 lam =
+          __ldg(P.pwt + ((2 * kN - ((kshift * e) & (2 * kN - 1))) & (2 * kN - 1)));
+      r0[c] = fold2(mulsh(sub_q(h0[k], n0v), lam.x, lam.y));
+      r1[c] = fold2(mulsh(sub_q(h1[k], n1v), lam.x, lam.y));
+    }
+    const int j0 = posD(tid, 4 * h);  // four consecutive slots
+    *reinterpret_cast<ulonglong2 *>(outL + j0) = make_ulonglong2(l0[0], l0[1]);
+    *reinterpret_cast<ulonglong2 *>(outL + j0 + 2) = make_ulonglong2(l0[2], l0[3]);
+    *reinterpret_cast<ulonglong2 *>(outL + kN + j0) = make_ulonglong2(l1[0], l1[1]);
+    *reinterpret_cast<ulonglong2 *>(outL + kN + j0 + 2) = make_ulonglong2(l1[2], l1[3]);
+    *reinterpret_cast<ulonglong2 *>(outR + j0) = make_ulonglong2(r0[0], r0[1]);
+    *reinterpret_cast<ulonglong2 *>(outR + j0 + 2) = make_ulonglong2(r0[2], r0[3]);
+    *reinterpret_cast<ulonglong2 *>(outR + kN + j0) = make_ulonglong2(r1[0], r1[1]);
+    *reinterpret_cast<ulonglong2 *>(outR + kN + j0 + 2) = make_ulonglong2(r1[2], r1[3]);
+  }
+}
+
+// One key switch (node node0 + blockIdx.x); NTT_OUT: children in NTT form.
+template <bool NTT_OUT>
+__device__ __forceinline__ void expand_body(const Dev1 &P, uint32_t galois_inv, uint32_t kshift,
+                                            uint32_t galois, uint32_t node0, const uint64_t *in,
+                                            uint64_t in_stride, uint64_t *out, uint64_t out_stride,
+                                            const uint64_t *const *bv_keys,
+                                            uint64_t bv_level_off) {
+  extern __shared__ uint64_t sm1[];
+  const int node = node0 + blockIdx.x, b = blockIdx.z, tid = threadIdx.x;
   const uint64_t *ct = in + (static_cast<uint64_t>(b) * in_stride + node) * kCtWords;
   const uint64_t *key = bv_keys[b] + bv_level_off;  // rows [b][a][b'][a']
   uint64_t u[8];
@@ -450,6 +540,18 @@ k1p_expand_level(Dev1 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *_
     for (int k = 0; k < 8; ++k) { ab[k] = fold16(ab[k]); aa[k] = fold16(aa[k]); }
     __syncthreads();
   }
+  uint64_t *outL = out + (static_cast<uint64_t>(b) * out_stride + 2ull * node) * kCtWords;
+  uint64_t *outR = outL + kCtWords;
+  if constexpr (NTT_OUT) {
+    uint64_t vb[8], va[8];  // the key switch's delta in NTT form, canonical
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      vb[k] = fold2(ab[k]);
+      va[k] = fold2(aa[k]);
+    }
+    expand_tail_ntt(P, galois, kshift, ct, vb, va, outL, outR);
+    return;
+  }
   {
     ulonglong2 wd[6];
     load_d(wd, P.iwt, tid);
@@ -465,8 +567,6 @@ k1p_expand_level(Dev1 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *_
   ld_plane<0>(sm1 + kPad, da, tid);
   iA(db_);
   iA(da);
-  uint64_t *outL = out + (static_cast<uint64_t>(b) * out_stride + 2ull * node) * kCtWords;
-  uint64_t *outR = outL + kCtWords;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const uint32_t j = posA(tid, k);
@@ -484,6 +584,29 @@ k1p_expand_level(Dev1 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *_
     outR[dst] = wrap ? neg_q(d0) : d0;
     outR[kN + dst] = wrap ? neg_q(d1) : d1;
   }
+}
+
+// MINB CTAs per SM: 2 (128 registers, a few spilled) when a level fills
+// the GPU twice over, else 1 (no spills, lower latency per CTA).
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+k1p_expand_level(Dev1 P, uint32_t galois_inv, uint32_t kshift, const uint64_t *__restrict__ in,
+                 uint64_t in_stride, uint64_t *__restrict__ out, uint64_t out_stride,
+                 const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off,
+                 uint32_t node0) {
+  expand_body<false>(P, galois_inv, kshift, 0, node0, in, in_stride, out, out_stride, bv_keys,
+                     bv_level_off);
+}
+// The last level's nodes below ntt_nodes when the first-dimension leaves are
+// wanted in NTT form (expand_tail_ntt); k1p_expand_level takes the others.
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+k1p_expand_level_ntt(Dev1 P, uint32_t galois, uint32_t galois_inv, uint32_t kshift,
+                     const uint64_t *__restrict__ in, uint64_t in_stride,
+                     uint64_t *__restrict__ out, uint64_t out_stride,
+                     const uint64_t *const *__restrict__ bv_keys, uint64_t bv_level_off) {
+  expand_body<true>(P, galois_inv, kshift, galois, 0, in, in_stride, out, out_stride, bv_keys,
+                    bv_level_off);
 }
 
 // ------------------------------------------------------------ gadget product
@@ -543,7 +666,8 @@ __device__ __forceinline__ void gadget_mac(const Dev1 &P, const uint64_t *x, con
 // complete_selectors / query_to_gsw (server.cpp:823-855, gsw.cpp:317-357):
 // the top row is the expanded row itself in NTT form, the bottom row its
 // external product with RGSW(s); both stored with Shoup companions.
-__global__ void __launch_bounds__(kThreads)
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 k1p_selectors(Dev1 P, Shape1 S, const uint64_t *__restrict__ leaves, uint64_t leaf_stride,
               const uint64_t *const *__restrict__ gsw_keys, uint64_t *__restrict__ sel) {
   extern __shared__ uint64_t sm1[];
@@ -644,18 +768,22 @@ k1p_fst_ntt(Dev1 P, Shape1 S, const uint64_t *__restrict__ leaves, uint64_t leaf
 // planes, 16 bytes each; k in [n0, n0p) reads as zero.
 constexpr int kPackZ = 32, kPackK = 128, kRunPitch = 18, kRowPitch = 145;
 __global__ void __launch_bounds__(256)
-k1p_fst_pack(const uint64_t *__restrict__ qm, uint32_t n0, uint32_t n0p, uint32_t ncols,
+k1p_fst_pack(const uint64_t *__restrict__ qm, uint64_t q_stride, uint64_t p_stride,
+             uint64_t k_stride, uint32_t n0, uint32_t n0p, uint32_t ncols,
              uint8_t *__restrict__ qb) {
   __shared__ uint64_t tile[(kPackZ - 1) * kRowPitch + (kPackK / 16 - 1) * kRunPitch + 16];
   const uint32_t z0 = blockIdx.x * kPackZ, col = blockIdx.y, k0 = blockIdx.z * kPackK;
   const int t = threadIdx.x;
-  const uint64_t *src = qm + static_cast<uint64_t>(col) * n0 * kN + z0;
+  // column col = 2 query + poly: qm (q_stride = 2 p_stride, p_stride = n0 N,
+  // k_stride = N) or NTT-form leaves (q_stride = slots 2N, p_stride = N,
+  // k_stride = 2N)
+  const uint64_t *src = qm + (col >> 1) * q_stride + (col & 1) * p_stride + z0;
 #pragma unroll 4
   for (int i = t; i < kPackK * kPackZ; i += 256) {
     const int kk = i / kPackZ, zz = i % kPackZ;
     const uint32_t k = k0 + kk;
     tile[zz * kRowPitch + (kk / 16) * kRunPitch + kk % 16] =
-        k < n0 ? src[static_cast<uint64_t>(k) * kN + zz] : 0;
+        k < n0 ? src[static_cast<uint64_t>(k) * k_stride + zz] : 0;
   }
   __syncthreads();
   const int chunk = t % (kPackK / 16), zz = t / (kPackK / 16);
@@ -857,16 +985,44 @@ void launch_db_preprocess(const Dev1 &P, const Shape1 &s, const uint64_t *coeffs
 void launch_expand_level(const Dev1 &P, const Shape1 &s, uint32_t d, const uint64_t *in,
                          uint64_t in_stride, uint64_t *out, uint64_t out_stride,
                          const uint64_t *const *bv_keys, uint64_t bv_level_stride, uint32_t batch,
-                         cudaStream_t st) {
+                         cudaStream_t st, uint32_t ntt_nodes) {
   const uint32_t nodes = opir4::expand_nodes(s, d);
   const size_t smem = plane_bytes(kGroup);
-  set_smem(k1p_expand_level, smem);
   const uint32_t k = 1u << d;
   const uint32_t galois = kN / k + 1;
   uint32_t galois_inv = 1;  // galois^-1 mod 2N (galois is odd)
   while (((galois_inv * galois) & (2 * kN - 1)) != 1) galois_inv += 2;
-  k1p_expand_level<<<dim3(nodes, 1, batch), kThreads, smem, st>>>(
-      P, galois_inv, k, in, in_stride, out, out_stride, bv_keys, d * bv_level_stride);
+  const uint64_t koff = d * bv_level_stride;
+  static_assert(kGroup >= 3, "the NTT-form tail uses three planes");
+  if (ntt_nodes > nodes || (ntt_nodes > 0 && d + 1 != s.h))
+    throw std::invalid_argument("NTT-form children only at the last expansion level");
+  if (ntt_nodes > 0) {
+    const dim3 grid(ntt_nodes, 1, batch);
+    if (static_cast<uint64_t>(ntt_nodes) * batch >= 2ull * sms()) {
+      set_smem(k1p_expand_level_ntt<2>, smem);
+      k1p_expand_level_ntt<2><<<grid, kThreads, smem, st>>>(P, galois, galois_inv, k, in,
+                                                             in_stride, out, out_stride, bv_keys,
+                                                             koff);
+    } else {
+      set_smem(k1p_expand_level_ntt<1>, smem);
+      k1p_expand_level_ntt<1><<<grid, kThreads, smem, st>>>(P, galois, galois_inv, k, in,
+                                                             in_stride, out, out_stride, bv_keys,
+                                                             koff);
+    }
+    check_launch("k1p_expand_level_ntt");
+  }
+  const uint32_t rest = nodes - ntt_nodes;  // coefficient-form children
+  if (rest == 0) return;
+  const dim3 grid(rest, 1, batch);
+  if (static_cast<uint64_t>(rest) * batch >= 2ull * sms()) {
+    set_smem(k1p_expand_level<2>, smem);
+    k1p_expand_level<2><<<grid, kThreads, smem, st>>>(P, galois_inv, k, in, in_stride, out,
+                                                       out_stride, bv_keys, koff, ntt_nodes);
+  } else {
+    set_smem(k1p_expand_level<1>, smem);
+    k1p_expand_level<1><<<grid, kThreads, smem, st>>>(P, galois_inv, k, in, in_stride, out,
+                                                       out_stride, bv_keys, koff, ntt_nodes);
+  }
   check_launch("k1p_expand_level");
 }
 
@@ -875,10 +1031,15 @@ void launch_selectors(const Dev1 &P, const Shape1 &s, const uint64_t *leaves, ui
                       cudaStream_t st) {
   if (s.num_dims <= 1) return;
   const size_t smem = plane_bytes(kGroup);
-  set_smem(k1p_selectors, smem);
   const uint32_t rows = (s.num_dims - 1) * s.l_ep;
-  k1p_selectors<<<dim3(rows, 1, batch), kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys,
-                                                             sel);
+  const dim3 grid(rows, 1, batch);
+  if (static_cast<uint64_t>(rows) * batch >= 2ull * sms()) {
+    set_smem(k1p_selectors<2>, smem);
+    k1p_selectors<2><<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
+  } else {
+    set_smem(k1p_selectors<1>, smem);
+    k1p_selectors<1><<<grid, kThreads, smem, st>>>(P, s, leaves, leaf_stride, gsw_keys, sel);
+  }
   check_launch("k1p_selectors");
 }
 
@@ -895,7 +1056,17 @@ void launch_fst_pack(const Shape1 &s, const uint64_t *qm, uint8_t *qb, uint32_t 
                      cudaStream_t st) {
   const uint32_t ncols = 2 * batch;
   const dim3 grid(kN / kPackZ, ncols, (s.n0p + kPackK - 1) / kPackK);
-  k1p_fst_pack<<<grid, 256, 0, st>>>(qm, s.n0, s.n0p, ncols, qb);
+  const uint64_t p_stride = static_cast<uint64_t>(s.n0) * kN;
+  k1p_fst_pack<<<grid, 256, 0, st>>>(qm, 2 * p_stride, p_stride, kN, s.n0, s.n0p, ncols, qb);
+  check_launch("k1p_fst_pack");
+}
+
+void launch_fst_pack_leaves(const Shape1 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                            uint8_t *qb, uint32_t batch, cudaStream_t st) {
+  const uint32_t ncols = 2 * batch;
+  const dim3 grid(kN / kPackZ, ncols, (s.n0p + kPackK - 1) / kPackK);
+  k1p_fst_pack<<<grid, 256, 0, st>>>(leaves, leaf_stride * kCtWords, kN, kCtWords, s.n0, s.n0p,
+                                      ncols, qb);
   check_launch("k1p_fst_pack");
 }
 

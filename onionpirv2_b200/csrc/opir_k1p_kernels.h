@@ -43,6 +43,7 @@ struct Dev1 {
   const ulonglong2 *fwt, *iwt;  // (w, floor(w 2^64 / q)), bit-reversed order
   uint64_t small_q;
   uint32_t small_q_width;
+  const ulonglong2 *pwt;        // (psi^m, floor(psi^m 2^64 / q)) for m < 2N
 };
 
 // the layout fields the kernels read (the two-limb set's shape struct)
@@ -63,7 +64,7 @@ void launch_db_preprocess(const Dev1 &P, const Shape1 &s, const uint64_t *coeffs
 void launch_expand_level(const Dev1 &P, const Shape1 &s, uint32_t d, const uint64_t *in,
                          uint64_t in_stride, uint64_t *out, uint64_t out_stride,
                          const uint64_t *const *bv_keys, uint64_t bv_level_stride, uint32_t batch,
-                         cudaStream_t st);
+                         cudaStream_t st, uint32_t ntt_nodes = 0);
 void launch_selectors(const Dev1 &P, const Shape1 &s, const uint64_t *leaves, uint64_t leaf_stride,
                       const uint64_t *const *gsw_keys, uint64_t *sel, uint32_t batch,
                       cudaStream_t st);
@@ -71,6 +72,10 @@ void launch_fst_ntt(const Dev1 &P, const Shape1 &s, const uint64_t *leaves, uint
                     uint64_t *qm, uint32_t batch, cudaStream_t st);
 void launch_fst_pack(const Shape1 &s, const uint64_t *qm, uint8_t *qb, uint32_t batch,
                      cudaStream_t st);
+// The same byte planes from NTT-form leaves in the ciphertext layout (the
+// last expansion level's NTT-form children; batch x leaf_stride cts).
+void launch_fst_pack_leaves(const Shape1 &s, const uint64_t *leaves, uint64_t leaf_stride,
+                            uint8_t *qb, uint32_t batch, cudaStream_t st);
 void launch_epilogue(const Dev1 &P, const Shape1 &s, const uint64_t *cmat, uint64_t *mid,
                      uint64_t mid_stride, uint32_t batch, cudaStream_t st);
 // One MUX level of a selector tree of height tree_h: level 0 carries the

@@ -231,3 +231,29 @@ def test_k1p_stream_priority_leaves_results_unchanged():
     resp = srv.make_query(7, q)
     assert G.sha256(resp) == c["sha256_response_u64"]
     srv.set_priority(0)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_k1p_ntt_form_leaves_match_coefficient_leaves(name, monkeypatch):
+    """make_query's last expansion level writes the first-dimension leaves
+    in NTT form (sigma and X^-k in the NTT domain); OPIR_NTT_LEAVES=0 keeps
+    every leaf in coefficient form and runs k1p_fst_ntt. Both give the
+    golden response, single and batched (1 and 2 CTAs per SM), eager and
+    replayed."""
+    c, op, cl, bv, gsw, q, gp, _ = setup(name)
+    qs = np.stack([q] * 40)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("OPIR_NTT_LEAVES", flag)
+        with PirServer(gp) as srv:
+            srv.load_data_seeded(c["target_num_pt"], c["db_seed"])
+            srv.set_client_keys(7, bv, gsw)
+            for _ in range(3):
+                r = srv.make_query(7, q)
+                assert G.sha256(r) == c["sha256_response_u64"]
+            out[flag] = [srv.make_query_batch([7] * 40, qs) for _ in range(2)]
+    for a, b in zip(out["1"], out["0"]):
+        for ra, rb in zip(a, b):
+            assert np.array_equal(ra, rb)
+            assert G.sha256(ra) == c["sha256_response_u64"]
+    assert np.array_equal(cl.decrypt(out["1"][0][0]), _plaintext(c, op))
