@@ -60,12 +60,19 @@ constexpr int kEpilogueThreads = 256;
 constexpr size_t kBarrierBytes = 256;  // mbarriers, TMEM slot, abort flag
 constexpr uint32_t kTmemCols = 512;
 
+// x mod q for any 64-bit x, from one 32-bit high product: mu = floor((2^64
+// - 1) / q) = 8 2^32 + mu_lo for the 29-bit residues (the launcher checks),
+// so with x = xh 2^32 + xl, x mu / 2^64 = 8 xh + xh mu_lo / 2^32 + xl / 2^29
+// + xl mu_lo / 2^64; the estimate drops three fractions below 1 each, so it
+// lies within 3 of floor(x mu / 2^64) > x / q - 2 - 1/q, r = x - est q <= 4q
+// (< 2^32: 32-bit arithmetic is exact), and three corrections finish.
 __device__ __forceinline__ uint32_t reduce64_tc(uint64_t x, uint32_t q, uint64_t mu) {
-  const uint64_t qhat = __umul64hi(x, mu);
-  uint64_t r = x - qhat * q;
-  if (r >= q) r -= q;
-  if (r >= q) r -= q;
-  return static_cast<uint32_t>(r);
+  const uint32_t xh = static_cast<uint32_t>(x >> 32), xl = static_cast<uint32_t>(x);
+  const uint32_t est = (xh << 3) + __umulhi(xh, static_cast<uint32_t>(mu)) + (xl >> 29);
+  uint32_t r = xl - est * q;
+  r = min(r, r - 2 * q);
+  r = min(r, r - q);
+  return min(r, r - q);
 }
 
 template <int KT>
@@ -391,6 +398,8 @@ uint32_t scan_tc_max_stages(uint32_t ntile, uint32_t kt) {
 
 void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcScanArgs &args,
                     int sm_count, cudaStream_t st) {
+  if ((args.mu[0] >> 32) != 8 || (args.mu[1] >> 32) != 8)
+    throw std::invalid_argument("tensor-core scan: floor(2^64 / q) must be 8 2^32 + mu_lo (q in (2^64 / 9 2^32, 2^29])");
   if ((args.kt != 128 && args.kt != 64) || args.stages < 2 ||
       args.stages > scan_tc_max_stages(args.ntile, args.kt) ||
       (args.ntile != 16 && args.ntile != 32 && args.ntile != 64))
