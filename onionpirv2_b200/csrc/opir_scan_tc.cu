@@ -60,8 +60,16 @@ constexpr int kEpilogueThreads = 256;
 constexpr size_t kBarrierBytes = 256;  // mbarriers, TMEM slot, abort flag
 constexpr uint32_t kTmemCols = 512;
 
-// x mod q for any 64-bit x, from one 32-bit high product: mu = floor((2^64
-// - 1) / q) = 8 2^32 + mu_lo for the 29-bit residues (the launcher checks),
+// x mod q with mu = floor((2^64 - 1) / q), by Barrett's 64-bit quotient.
+__device__ __forceinline__ uint32_t reduce64_barrett(uint64_t x, uint32_t q, uint64_t mu) {
+  const uint64_t qhat = __umul64hi(x, mu);
+  uint64_t r = x - qhat * q;
+  if (r >= q) r -= q;
+  if (r >= q) r -= q;
+  return static_cast<uint32_t>(r);
+}
+// x mod q for any 64-bit x, from one 32-bit high product when mu = floor((2^64
+// - 1) / q) = 8 2^32 + mu_lo (the 29-bit residues; the launcher checks),
 // so with x = xh 2^32 + xl, x mu / 2^64 = 8 xh + xh mu_lo / 2^32 + xl / 2^29
 // + xl mu_lo / 2^64; the estimate drops three fractions below 1 each, so it
 // lies within 3 of floor(x mu / 2^64) > x / q - 2 - 1/q, r = x - est q <= 4q
@@ -75,7 +83,9 @@ __device__ __forceinline__ uint32_t reduce64_tc(uint64_t x, uint32_t q, uint64_t
   return min(r, r - q);
 }
 
-template <int KT>
+// FAST: every residue's mu is 8 2^32 + mu_lo (reduce64_tc), else Barrett
+// (the client's one-residue products mod small_q use the same kernel).
+template <int KT, bool FAST>
 __global__ void __launch_bounds__(kThreadsTc, 1)
 k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmQ,
           TcScanArgs a) {
@@ -261,7 +271,8 @@ k_scan_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             for (int s2 = 1; s2 < 7; ++s2) acc[c] += static_cast<uint64_t>(P[s2][c]) * w[s2];
           }
 #pragma unroll
-          for (int c = 0; c < 8; ++c) outv[8 * cc + c] = reduce64_tc(acc[c], q, mu);
+          for (int c = 0; c < 8; ++c)
+            outv[8 * cc + c] = FAST ? reduce64_tc(acc[c], q, mu) : reduce64_barrett(acc[c], q, mu);
         }
         if (last) {  // the accumulators are in registers: hand the TMEM set back first
           fence_before();
@@ -318,8 +329,10 @@ void configure_scan_tc() {
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lock(mu);
   if (done.count(dev)) return;
-  for (const void *k : {reinterpret_cast<const void *>(k_scan_tc<128>),
-                        reinterpret_cast<const void *>(k_scan_tc<64>)}) {
+  for (const void *k : {reinterpret_cast<const void *>(k_scan_tc<128, true>),
+                        reinterpret_cast<const void *>(k_scan_tc<64, true>),
+                        reinterpret_cast<const void *>(k_scan_tc<128, false>),
+                        reinterpret_cast<const void *>(k_scan_tc<64, false>)}) {
     const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(kSmemLimit));
     if (e != cudaSuccess)
@@ -398,8 +411,6 @@ uint32_t scan_tc_max_stages(uint32_t ntile, uint32_t kt) {
 
 void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcScanArgs &args,
                     int sm_count, cudaStream_t st) {
-  if ((args.mu[0] >> 32) != 8 || (args.mu[1] >> 32) != 8)
-    throw std::invalid_argument("tensor-core scan: floor(2^64 / q) must be 8 2^32 + mu_lo (q in (2^64 / 9 2^32, 2^29])");
   if ((args.kt != 128 && args.kt != 64) || args.stages < 2 ||
       args.stages > scan_tc_max_stages(args.ntile, args.kt) ||
       (args.ntile != 16 && args.ntile != 32 && args.ntile != 64))
@@ -410,10 +421,15 @@ void launch_scan_tc(const CUtensorMap &mapA, const CUtensorMap &mapQ, const TcSc
   const unsigned grid = static_cast<unsigned>(items < static_cast<uint64_t>(sm_count) ? items : sm_count);
   TcScanArgs a = args;  // 0: the default limit (~1 s)
   if (a.wait_cycles <= 0) a.wait_cycles = tc::kWaitCycles;
-  if (a.kt == 128)
-    k_scan_tc<128><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
+  const bool fast = (a.mu[0] >> 32) == 8 && (a.mu[1] >> 32) == 8;
+  if (a.kt == 128 && fast)
+    k_scan_tc<128, true><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
+  else if (a.kt == 128)
+    k_scan_tc<128, false><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
+  else if (fast)
+    k_scan_tc<64, true><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
   else
-    k_scan_tc<64><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
+    k_scan_tc<64, false><<<grid, kThreadsTc, smem, st>>>(mapA, mapQ, a);
   note_launches(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw std::runtime_error(std::string("k_scan_tc: ") + cudaGetErrorString(e));
